@@ -1,0 +1,391 @@
+#!/usr/bin/env python
+"""Benchmark: Poisson solve time to ||r||/||b|| <= 1e-8 on one B200.
+
+Workload (default, --config 3): 512x256x256 cells (33.5M) as 4x2x2 blocks of
+128^3, all-Neumann, seeded spectral right-hand side.  One step = one full
+solve from p = 0 to the FP64 relative residual 1e-8 by the FP32-smoothing /
+FP64-refined multigrid (`value`, ms per solve, lower is better).  The plain
+FP64 GPU multigrid (the reference's arithmetic) is timed beside it on the
+same resident inputs, and the solution error of the mixed solve against the
+FP64 one is reported.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference] [--config C]
+
+With N > 1 (torchrun) every rank solves its own replica (the path does not
+shard across GPUs in this build); the value is the whole job's ms per solve
+(max-over-ranks device time / (N*K)).  `--impl reference` times the CPU
+implementation of the same path (the oracle restatement of the reference
+Fortran, OpenMP over all host cores) on a bounded sample.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+TOL = 1e-8
+WORKLOADS = {
+    1: "config1: 64^3 single block, walls, U(-1,1) divergence, 4 levels, V(2,1) RBGS",
+    2: "config2: 192^3 as 2x2x2 blocks of 96^3, periodic x, 6 levels, warm start",
+    3: "config3: 512x256x256 (33.5M cells) as 4x2x2 blocks of 128^3, all-Neumann, k^-5/3 spectral rhs, 7 levels",
+    4: "config4: 27 independent all-Neumann blocks, axes from {32,48,64,96,128}, 4 levels",
+    5: "config5: 256^3 two-phase 1000:1 density (L_LSM coefficients), 8 levels",
+}
+
+
+def dist_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d.get("hbm_gbs", 6650.0)), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+        self.t = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def make_problem(cfg):
+    from hydro3d_b200 import synth
+    return synth.CONFIGS[cfg]()
+
+
+def build_solver(prob, precision, use_graph=True):
+    from hydro3d_b200 import MultigridSolver
+    s = MultigridSolver(prob.blocks, prob.ngrid, precision=precision, var_coef=prob.var_coef, maxcy=400,
+                        use_graph=use_graph)
+    if prob.var_coef:
+        for ib, d in enumerate(prob.dens):
+            s.set_density(ib, d)
+    s.coeff()
+    for ib in range(len(prob.blocks)):
+        s.upload("b", ib, prob.b[ib])
+        s.upload("p", ib, prob.p0[ib])
+    return s
+
+
+def timed_solves(s, prob, steps, warmup, profile=False, barrier=None):
+    """Returns per-step device ms and the last info (inputs resident in HBM)."""
+    def one():
+        if not any(np.any(p) for p in prob.p0):
+            s.zero_field("p")
+        else:
+            for ib in range(len(prob.blocks)):
+                s.upload("p", ib, prob.p0[ib])
+        return s.solve_resident(tol=TOL, maxcy=400)
+    for _ in range(warmup):
+        info = one()
+    s.set_profiling(profile)
+    if barrier:
+        barrier()
+    ms, infos = [], []
+    for _ in range(steps):
+        info = one()
+        if not info["converged"]:
+            raise RuntimeError(f"solve did not converge: {info}")
+        ms.append(info["device_ms"])
+        infos.append(info)
+    s.set_profiling(False)
+    return ms, infos
+
+
+def e2e_solves(s, prob, steps):
+    """newsolv_mg through the public API from pinned host buffers (H2D and D2H
+    inside the timed region)."""
+    import torch
+    pin_b = [torch.from_numpy(x).pin_memory().numpy() for x in prob.b]
+    pin_p = [torch.from_numpy(x).pin_memory().numpy() for x in prob.p0]
+    work = [torch.empty(x.shape, dtype=torch.float64).pin_memory().numpy() for x in prob.p0]
+    times = []
+    for _ in range(steps):
+        for w, p in zip(work, pin_p):
+            w[...] = p
+        t0 = time.perf_counter()
+        info = s.newsolv_mg(work, pin_b, tol=TOL, maxcy=400)
+        times.append((time.perf_counter() - t0) * 1e3)
+        if not info["converged"]:
+            raise RuntimeError("e2e solve did not converge")
+    h2d = sum(x.nbytes for x in prob.b) + sum(x.nbytes for x in prob.p0)
+    d2h = sum(x.nbytes for x in prob.p0)
+    return times, h2d, d2h
+
+
+def mean_removed_error(a_list, b_list, blocks):
+    from hydro3d_b200 import interior
+    a = np.concatenate([interior(x, d).ravel() for x, d in zip(a_list, blocks)])
+    b = np.concatenate([interior(x, d).ravel() for x, d in zip(b_list, blocks)])
+    a = a - a.mean()
+    b = b - b.mean()
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+def cpu_port_sample(prob, fp64_cycles, threads, sample_cycles=2):
+    """Oracle (C restatement of the reference MG, OpenMP) on the full workload:
+    time `sample_cycles` defect-correction V-cycles, project to the cycle count
+    of the identical FP64 algorithm."""
+    from oracle import oracle as O
+    import ctypes as C
+    od = (O.BlockDesc * len(prob.blocks))()
+    C.memmove(od, (type(prob.blocks[0]) * len(prob.blocks))(*prob.blocks), C.sizeof(od))
+    orc = O.Oracle(list(od), prob.ngrid, 3, 2, 1, lsm=prob.var_coef, threads=threads)
+    if prob.var_coef:
+        from hydro3d_b200 import interior
+        for ib, (d, x) in enumerate(zip(prob.blocks, prob.dens)):
+            orc.set_density(ib, np.ascontiguousarray(interior(x, d)))
+    orc.coeff()
+    from hydro3d_b200 import interior, with_ghost
+    b = [np.ascontiguousarray(interior(x, d)) for x, d in zip(prob.b, prob.blocks)]
+    p = [np.ascontiguousarray(with_ghost(x, d)) for x, d in zip(prob.p0, prob.blocks)]
+    t0 = time.perf_counter()
+    res = orc.solve(p, b, tol=0.0, maxcy=sample_cycles)
+    dt = time.perf_counter() - t0
+    orc.close()
+    per_cycle = dt / max(res["cycles"], 1)
+    return per_cycle * 1e3 * fp64_cycles, per_cycle, res
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    prob = make_problem(args.config)
+    threads = os.cpu_count() or 1
+    from oracle import oracle as O
+    O.lib()
+    # cycle count of the reference algorithm on this workload (FP64, to 1e-8)
+    cyc = args.ref_cycles
+    vals = []
+    for _ in range(args.warmup):
+        cpu_port_sample(prob, cyc, threads, sample_cycles=1)
+    for _ in range(args.steps):
+        v, per_cycle, _ = cpu_port_sample(prob, cyc, threads, sample_cycles=args.ref_sample_cycles)
+        vals.append(v)
+    value = statistics.median(vals)
+    line = {
+        "impl": "reference", "metric": "poisson_solve_ms_to_1e-8", "value": round(value, 3), "unit": "ms",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(value, 3),
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOADS[args.config], "solver": "reference V(2,1) RBGS, FP64"},
+        "cpu_baseline": {"value": round(value, 3), "unit": "ms", "cores": threads, "kind": "port",
+                         "sample": f"{args.ref_sample_cycles} FP64 V-cycles per step on the full workload, "
+                                   f"scaled to the {cyc} cycles the identical FP64 algorithm needs to 1e-8"},
+        "e2e": {"value": round(value, 3), "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--config", type=int, default=3)
+    ap.add_argument("--ref-cycles", type=int, default=int(os.environ.get("H3D_REF_CYCLES", "0")) or 0)
+    ap.add_argument("--ref-sample-cycles", type=int, default=2)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        if args.ref_cycles <= 0:
+            args.ref_cycles = REF_CYCLES.get(args.config, 30)
+        return run_reference(args)
+
+    rank, world, local = dist_env()
+    dist = world > 1
+    barrier = None
+    if dist:
+        import torch.distributed as tdist
+        from datetime import timedelta
+        tdist.init_process_group("gloo", timeout=timedelta(seconds=600))
+        barrier = tdist.barrier
+    import hydro3d_b200  # noqa: F401  (loads libh3dmg.so; raises if missing)
+    os.environ.setdefault("CUDA_DEVICE_ORDER", "PCI_BUS_ID")
+    device = local
+    prob = make_problem(args.config)
+    peak, peak_kind = load_peaks()
+
+    mixed = build_solver_dev(prob, "mixed", device)
+    fp64 = build_solver_dev(prob, "fp64", device)
+
+    clocks = ClockSampler(device)
+    clocks.start()
+    ms_mixed, infos_mixed = timed_solves(mixed, prob, args.steps, args.warmup, profile=True, barrier=barrier)
+    clk = clocks.stop()
+    ms_fp64, infos_fp64 = timed_solves(fp64, prob, max(1, min(args.steps, 3)), args.warmup, barrier=barrier)
+
+    total_ms = sum(ms_mixed)
+    if dist:
+        import torch
+        import torch.distributed as tdist
+        t = torch.tensor([total_ms], dtype=torch.float64)
+        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = total_ms / (args.steps * world)
+
+    # solution error of the mixed solve against the FP64 solve (same inputs)
+    from hydro3d_b200 import host_field
+    pm = [host_field(d) for d in prob.blocks]
+    pf = [host_field(d) for d in prob.blocks]
+    for ib in range(len(prob.blocks)):
+        mixed.download("p", ib, pm[ib])
+        fp64.download("p", ib, pf[ib])
+    err = mean_removed_error(pm, pf, prob.blocks)
+
+    # roofline of the dominant kernel (level-1 FP32 smoother)
+    info = infos_mixed[-1]
+    sm_ms = sum(i["smoother_ms"] for i in infos_mixed)
+    sm_n = sum(i["smoother_launches"] for i in infos_mixed)
+    bytes_launch = mixed.smoother_bytes()
+    avg_launch_ms = sm_ms / max(sm_n, 1)
+    achieved = bytes_launch / (avg_launch_ms * 1e-3) / 1e9 if sm_n else None
+    traffic = read_profile_traffic()
+
+    e2e = None
+    if not args.no_e2e:
+        et, h2d, d2h = e2e_solves(mixed, prob, max(1, min(args.steps, 3)))
+        e2e = {"value": round(statistics.median(et), 3), "unit": "ms", "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int(d2h)}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        v, per_cycle, _ = cpu_port_sample(prob, infos_fp64[-1]["cycles"], threads, sample_cycles=2)
+        cpu = {"value": round(v, 1), "unit": "ms", "cores": threads, "kind": "port",
+               "sample": f"2 FP64 V-cycles of the oracle on the full workload ({per_cycle * 1e3:.0f} ms/cycle), "
+                         f"scaled to the {infos_fp64[-1]['cycles']} cycles the FP64 algorithm needs"}
+
+    if rank == 0:
+        fp64_ms = statistics.median(ms_fp64)
+        line = {
+            "metric": "poisson_solve_ms_to_1e-8", "value": round(value, 3), "unit": "ms", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(value, 3),
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
+            "data": "synthetic (seeded; no dataset)",
+            "config": {"workload": WORKLOADS[args.config], "precision": "FP32 V(2,1) RBGS inside FP64 refinement",
+                       "inner_cycles": 2, "tol": TOL, "cells": prob.cells,
+                       "l2": "inputs larger than L2 (one level-1 FP64 field is %.0f MB)" % (prob.cells * 8 / 1e6),
+                       "parallelism": "replicas" if world > 1 else "single GPU"},
+            "fp64_ms": round(fp64_ms, 3), "speedup_vs_fp64": round(fp64_ms / (total_ms / (args.steps * world) * world), 3)
+            if world == 1 else None,
+            "cycles_mixed": info["cycles"], "outer_mixed": info["outer"], "cycles_fp64": infos_fp64[-1]["cycles"],
+            "relres_mixed": info["relres"], "relres_fp64": infos_fp64[-1]["relres"], "error_vs_fp64": err,
+            "mcell_updates_per_s": None,
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1) if achieved else None, "peak": peak,
+                         "unit": "GB/s", "frac": round(achieved / peak, 4) if achieved else None,
+                         "traffic": traffic, "kernel": "k_rbgs<float> level 1",
+                         "bytes_per_launch": bytes_launch, "avg_launch_ms": round(avg_launch_ms, 5),
+                         "peak_source": peak_kind},
+            "cpu_baseline": cpu, "e2e": e2e,
+            "gpu_launches": int(sum(i["kernel_launches"] for i in infos_mixed)),
+            "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    if dist:
+        import torch.distributed as tdist
+        tdist.barrier()
+        tdist.destroy_process_group()
+
+
+# FP64 V-cycle counts to 1e-8 of the reference algorithm per workload (the
+# GPU FP64 path reproduces the reference arithmetic bit for bit, so its count
+# is the reference's count); used to scale the reference arm's bounded sample.
+REF_CYCLES = {1: 45, 2: 30, 3: 30, 4: 60, 5: 60}
+
+
+def read_profile_traffic():
+    """DRAM bytes per smoother launch from the committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", "k_rbgs_fp32_config3_traffic.txt")
+    if not os.path.exists(p):
+        return None
+    for ln in open(p):
+        if ln.startswith("traffic_bytes_per_launch"):
+            try:
+                return float(ln.split("=")[1])
+            except ValueError:
+                return None
+    return None
+
+
+def build_solver_dev(prob, precision, device):
+    from hydro3d_b200 import MultigridSolver
+    s = MultigridSolver(prob.blocks, prob.ngrid, precision=precision, var_coef=prob.var_coef, maxcy=400,
+                        device=device)
+    if prob.var_coef:
+        for ib, d in enumerate(prob.dens):
+            s.set_density(ib, d)
+    s.coeff()
+    for ib in range(len(prob.blocks)):
+        s.upload("b", ib, prob.b[ib])
+        s.upload("p", ib, prob.p0[ib])
+    return s
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,369 @@
+// Halo gather tables: the ghost-cell semantics of the reference's level
+// exchange, resolved on index arrays so the GPU can fill every ghost cell of
+// a level in one order-free gather.
+//
+// The reference fills MG ghosts with a fixed sequence of plane, edge and
+// corner copies: mgbound (mgsolver.for:912-997), then exchangepp
+// (exchangepp.for:44-2826: per direction a pack pass over all blocks then an
+// unpack pass; corners and edges with the z direction), then mgbound again
+// (:2830) and the periodic wrap exchbc_mgpp (:2832, :2837-3454).  Running
+// that sequence on cell *identities* instead of values gives, for every
+// ghost cell, the cell whose value it ends up holding.  When that source is
+// an interior cell the GPU gathers the current value; when it is a ghost (a
+// value the sequence never replaced) the GPU reads the pre-fill value, which
+// the out-of-place smoother keeps in the previous buffer.
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+
+#include "h3d_internal.h"
+
+namespace h3d {
+
+LevelGeom make_level_geom(const std::vector<h3d_block_desc>& blocks, int g) {
+  LevelGeom L;
+  L.g = g;
+  long long off = 0;
+  for (const auto& d : blocks) {
+    int gl = g > d.ngrid ? d.ngrid : g;  // mgsolver.for:392-396
+    BlkLev b{};
+    b.nx = d.n[0] >> (gl - 1);
+    b.ny = d.n[1] >> (gl - 1);
+    b.nz = d.n[2] >> (gl - 1);
+    b.sx = b.nx + 2;
+    b.sxy = (long long)(b.nx + 2) * (b.ny + 2);
+    b.off = off;
+    b.phys = 0;
+    for (int f = 0; f < 6; ++f)
+      if (d.nb_face[f] < 0 && d.bc[f] != 5) b.phys |= 1 << f;
+    double s = (double)(1 << (gl - 1));
+    double ndx = d.h[0] * s, ndy = d.h[1] * s, ndz = d.h[2] * s;
+    double dxx = ndx * ndx, dyy = ndy * ndy, dzz = ndz * ndz;
+    b.ax = 1.0 / dxx;
+    b.ay = 1.0 / dyy;
+    b.az = 1.0 / dzz;
+    b.dv = d.h[0] * d.h[1] * d.h[2];
+    off += b.sxy * (b.nz + 2);
+    L.n_interior += (int64_t)b.nx * b.ny * b.nz;
+    L.bl.push_back(b);
+  }
+  L.n_elems = off;
+  return L;
+}
+
+namespace {
+
+struct Emu {
+  const LevelGeom& L;
+  const std::vector<h3d_block_desc>& D;
+  std::vector<uint32_t> id;
+  Emu(const LevelGeom& l, const std::vector<h3d_block_desc>& d) : L(l), D(d), id((size_t)l.n_elems) {
+    for (size_t q = 0; q < id.size(); ++q) id[q] = (uint32_t)q;
+  }
+  size_t at(int b, int x, int y, int z) const {
+    const BlkLev& B = L.bl[b];
+    return (size_t)(B.off + ((long long)z * (B.ny + 2) + y) * (B.nx + 2) + x);
+  }
+  int n(int b, int a) const { return a == 0 ? L.bl[b].nx : (a == 1 ? L.bl[b].ny : L.bl[b].nz); }
+  // Cell of block b whose coordinate on axis a is c and whose other two
+  // coordinates are (u, v) in axis order.
+  size_t plane_cell(int b, int a, int c, int u, int v) const {
+    if (a == 0) return at(b, c, u, v);
+    if (a == 1) return at(b, u, c, v);
+    return at(b, u, v, c);
+  }
+  void read_plane(int b, int a, int c, std::vector<uint32_t>& buf) const {
+    int o1 = a == 0 ? 1 : 0, o2 = a == 2 ? 1 : 2;
+    int n1 = n(b, o1) + 2, n2 = n(b, o2) + 2;
+    buf.resize((size_t)n1 * n2);
+    for (int v = 0; v < n2; ++v)
+      for (int u = 0; u < n1; ++u) buf[(size_t)v * n1 + u] = id[plane_cell(b, a, c, u, v)];
+  }
+  bool write_plane(int b, int a, int c, const std::vector<uint32_t>& buf) {
+    int o1 = a == 0 ? 1 : 0, o2 = a == 2 ? 1 : 2;
+    int n1 = n(b, o1) + 2, n2 = n(b, o2) + 2;
+    if (buf.size() != (size_t)n1 * n2) return false;  // face neighbours must match
+    for (int v = 0; v < n2; ++v)
+      for (int u = 0; u < n1; ++u) id[plane_cell(b, a, c, u, v)] = buf[(size_t)v * n1 + u];
+    return true;
+  }
+  void copy_plane(int b, int a, int cdst, int csrc) {
+    int o1 = a == 0 ? 1 : 0, o2 = a == 2 ? 1 : 2;
+    int n1 = n(b, o1) + 2, n2 = n(b, o2) + 2;
+    for (int v = 0; v < n2; ++v)
+      for (int u = 0; u < n1; ++u) id[plane_cell(b, a, cdst, u, v)] = id[plane_cell(b, a, csrc, u, v)];
+  }
+
+  // mgbound: zero-gradient ghosts on physical faces, order W,E,S,N,B,T.
+  void mgbound() {
+    for (size_t b = 0; b < L.bl.size(); ++b) {
+      int phys = L.bl[b].phys;
+      for (int a = 0; a < 3; ++a) {
+        if (phys & (1 << (2 * a))) copy_plane((int)b, a, 0, 1);
+        if (phys & (1 << (2 * a + 1))) copy_plane((int)b, a, n((int)b, a) + 1, n((int)b, a));
+      }
+    }
+  }
+
+  // Coordinate codes for corner/edge cells: 0 -> ghost 0, 1 -> first interior,
+  // 2 -> last interior (n), 3 -> ghost n+1, 4 -> running index.
+  int coord(int code, int nn, int running) const {
+    switch (code) {
+      case 0: return 0;
+      case 1: return 1;
+      case 2: return nn;
+      case 3: return nn + 1;
+      default: return running;
+    }
+  }
+
+  bool exchangepp(std::string* err) {
+    // Corner cells (exchangepp.for:441-640, 1400-1600 pack; 2515-2718 unpack),
+    // as (sender cell, receiver cell) for prev #1..4 then next #1..4.
+    static const int csrc[8][3] = {{1, 1, 1}, {1, 2, 1}, {2, 2, 1}, {2, 1, 1},
+                                   {2, 2, 2}, {2, 1, 2}, {1, 1, 2}, {1, 2, 2}};
+    static const int cdst[8][3] = {{0, 0, 0}, {0, 3, 0}, {3, 3, 0}, {3, 0, 0},
+                                   {3, 3, 3}, {3, 0, 3}, {0, 0, 3}, {0, 3, 3}};
+    // Edges (exchangepp.for:646-1100, 1604-2056 pack; 2568-2826 unpack).
+    static const int eaxis[6] = {1, 0, 1, 0, 2, 2};
+    static const int esrc[12][3] = {{1, 4, 1}, {4, 2, 1}, {2, 4, 1}, {4, 1, 1}, {1, 1, 4}, {1, 2, 4},
+                                    {2, 4, 2}, {4, 1, 2}, {1, 4, 2}, {4, 2, 2}, {2, 2, 4}, {2, 1, 4}};
+    static const int edst[12][3] = {{0, 4, 0}, {4, 3, 0}, {3, 4, 0}, {4, 0, 0}, {0, 0, 4}, {0, 3, 4},
+                                    {3, 4, 3}, {4, 0, 3}, {0, 4, 3}, {4, 3, 3}, {3, 3, 4}, {3, 0, 4}};
+    const int nb = (int)L.bl.size();
+    std::vector<std::vector<uint32_t>> rm(nb), rp(nb);
+    std::vector<uint32_t> rc(nb * 8, 0);
+    std::vector<char> rc_set(nb * 8, 0);
+    std::vector<std::vector<uint32_t>> re((size_t)nb * 12);
+    for (int a = 0; a < 3; ++a) {
+      for (int b = 0; b < nb; ++b) {  // pack
+        int prev = D[b].nb_face[2 * a], next = D[b].nb_face[2 * a + 1];
+        if (prev >= 0) read_plane(b, a, 1, rp[prev]);
+        if (a == 2) {
+          for (int c = 0; c < 4; ++c) {
+            int t = D[b].nb_corner[c];
+            if (t < 0) continue;
+            // receiver slot: sender's prev corner c lands in the receiver's next slot c
+            rc[t * 8 + 4 + c] = id[at(b, coord(csrc[c][0], L.bl[b].nx, 0), coord(csrc[c][1], L.bl[b].ny, 0),
+                                      coord(csrc[c][2], L.bl[b].nz, 0))];
+            rc_set[t * 8 + 4 + c] = 1;
+          }
+          for (int e = 0; e < 6; ++e) {
+            int t = D[b].nb_edge[e];
+            if (t < 0) continue;
+            int len = n(b, eaxis[e]);
+            auto& buf = re[(size_t)t * 12 + 6 + e];
+            buf.assign(len + 2, 0);
+            for (int q = 1; q <= len; ++q)
+              buf[q] = id[at(b, coord(esrc[e][0], L.bl[b].nx, q), coord(esrc[e][1], L.bl[b].ny, q),
+                             coord(esrc[e][2], L.bl[b].nz, q))];
+          }
+        }
+        if (next >= 0) read_plane(b, a, n(b, a), rm[next]);
+        if (a == 2) {
+          for (int c = 0; c < 4; ++c) {
+            int t = D[b].nb_corner[4 + c];
+            if (t < 0) continue;
+            rc[t * 8 + c] = id[at(b, coord(csrc[4 + c][0], L.bl[b].nx, 0), coord(csrc[4 + c][1], L.bl[b].ny, 0),
+                                  coord(csrc[4 + c][2], L.bl[b].nz, 0))];
+            rc_set[t * 8 + c] = 1;
+          }
+          for (int e = 0; e < 6; ++e) {
+            int t = D[b].nb_edge[6 + e];
+            if (t < 0) continue;
+            int len = n(b, eaxis[e]);
+            auto& buf = re[(size_t)t * 12 + e];
+            buf.assign(len + 2, 0);
+            for (int q = 1; q <= len; ++q)
+              buf[q] = id[at(b, coord(esrc[6 + e][0], L.bl[b].nx, q), coord(esrc[6 + e][1], L.bl[b].ny, q),
+                             coord(esrc[6 + e][2], L.bl[b].nz, q))];
+          }
+        }
+      }
+      for (int b = 0; b < nb; ++b) {  // unpack
+        int prev = D[b].nb_face[2 * a], next = D[b].nb_face[2 * a + 1];
+        if (prev >= 0 && !write_plane(b, a, 0, rm[b])) {
+          if (err) *err = "face neighbours with different extents";
+          return false;
+        }
+        if (next >= 0 && !write_plane(b, a, n(b, a) + 1, rp[b])) {
+          if (err) *err = "face neighbours with different extents";
+          return false;
+        }
+        if (a == 2) {
+          const BlkLev& B = L.bl[b];
+          for (int c = 0; c < 4; ++c)  // prev corners (filled by the neighbour's next pack)
+            if (D[b].nb_corner[c] >= 0 && rc_set[b * 8 + c])
+              id[at(b, coord(cdst[c][0], B.nx, 0), coord(cdst[c][1], B.ny, 0), coord(cdst[c][2], B.nz, 0))] =
+                  rc[b * 8 + c];
+          for (int e = 0; e < 6; ++e)
+            if (D[b].nb_edge[e] >= 0) {
+              auto& buf = re[(size_t)b * 12 + e];
+              int len = n(b, eaxis[e]);
+              if ((int)buf.size() != len + 2) {
+                if (err) *err = "edge neighbours with different extents";
+                return false;
+              }
+              for (int q = 1; q <= len; ++q)
+                id[at(b, coord(edst[e][0], B.nx, q), coord(edst[e][1], B.ny, q), coord(edst[e][2], B.nz, q))] =
+                    buf[q];
+            }
+          for (int c = 0; c < 4; ++c)  // next corners
+            if (D[b].nb_corner[4 + c] >= 0 && rc_set[b * 8 + 4 + c])
+              id[at(b, coord(cdst[4 + c][0], B.nx, 0), coord(cdst[4 + c][1], B.ny, 0),
+                    coord(cdst[4 + c][2], B.nz, 0))] = rc[b * 8 + 4 + c];
+          for (int e = 0; e < 6; ++e)
+            if (D[b].nb_edge[6 + e] >= 0) {
+              auto& buf = re[(size_t)b * 12 + 6 + e];
+              int len = n(b, eaxis[e]);
+              if ((int)buf.size() != len + 2) {
+                if (err) *err = "edge neighbours with different extents";
+                return false;
+              }
+              for (int q = 1; q <= len; ++q)
+                id[at(b, coord(edst[6 + e][0], B.nx, q), coord(edst[6 + e][1], B.ny, q),
+                      coord(edst[6 + e][2], B.nz, q))] = buf[q];
+            }
+        }
+      }
+    }
+    mgbound();
+    bool periodic = false;
+    for (int b = 0; b < nb; ++b)
+      for (int f = 0; f < 6; ++f)
+        if (D[b].bc[f] == 5) periodic = true;
+    if (periodic) return exchbc(err);
+    return true;
+  }
+
+  bool exchbc(std::string* err) {
+    const int nb = (int)L.bl.size();
+    std::vector<std::vector<uint32_t>> rm(nb), rp(nb);
+    for (int a = 0; a < 3; ++a) {
+      for (int b = 0; b < nb; ++b) {
+        if (!(D[b].bc[2 * a] == 5 || D[b].bc[2 * a + 1] == 5)) continue;
+        int prev = D[b].nb_face[2 * a], next = D[b].nb_face[2 * a + 1];
+        int na = n(b, a);
+        if (prev < 0) {
+          if (next < 0) copy_plane(b, a, 0, na);
+          else if (D[b].nb_periodic[2 * a] >= 0) read_plane(b, a, 1, rp[D[b].nb_periodic[2 * a]]);
+        }
+        if (next < 0) {
+          if (prev < 0) copy_plane(b, a, na + 1, 1);
+          else if (D[b].nb_periodic[2 * a + 1] >= 0) read_plane(b, a, na, rm[D[b].nb_periodic[2 * a + 1]]);
+        }
+      }
+      for (int b = 0; b < nb; ++b) {
+        if (!(D[b].bc[2 * a] == 5 || D[b].bc[2 * a + 1] == 5)) continue;
+        int prev = D[b].nb_face[2 * a], next = D[b].nb_face[2 * a + 1];
+        if (prev < 0 && next >= 0 && D[b].nb_periodic[2 * a] >= 0 && !write_plane(b, a, 0, rm[b])) {
+          if (err) *err = "periodic partners with different extents";
+          return false;
+        }
+        if (next < 0 && prev >= 0 && D[b].nb_periodic[2 * a + 1] >= 0 &&
+            !write_plane(b, a, n(b, a) + 1, rp[b])) {
+          if (err) *err = "periodic partners with different extents";
+          return false;
+        }
+      }
+    }
+    return true;
+  }
+
+  bool is_interior(uint32_t q) const {
+    // find block by offset (blocks are sorted by offset)
+    size_t lo = 0, hi = L.bl.size();
+    while (hi - lo > 1) {
+      size_t mid = (lo + hi) / 2;
+      if ((uint64_t)L.bl[mid].off <= q) lo = mid;
+      else hi = mid;
+    }
+    const BlkLev& B = L.bl[lo];
+    long long r = (long long)q - B.off;
+    int x = (int)(r % (B.nx + 2));
+    long long t = r / (B.nx + 2);
+    int y = (int)(t % (B.ny + 2));
+    int z = (int)(t / (B.ny + 2));
+    return x >= 1 && x <= B.nx && y >= 1 && y <= B.ny && z >= 1 && z <= B.nz;
+  }
+};
+
+}  // namespace
+
+int build_halo_table(const std::vector<h3d_block_desc>& blocks, int g, int kind,
+                     std::vector<uint32_t>& dst, std::vector<uint32_t>& src, std::string* err) {
+  LevelGeom L = make_level_geom(blocks, g);
+  if (L.n_elems >= (int64_t)kOldFlag) {
+    if (err) *err = "level too large for 31-bit halo indices";
+    return H3D_ERR_BAD_CONFIG;
+  }
+  Emu E(L, blocks);
+  bool ok = true;
+  switch (kind) {
+    case kHaloSweep:
+    case kHaloFaces:
+      E.mgbound();
+      ok = E.exchangepp(err);
+      break;
+    case kHaloExchange:
+      ok = E.exchangepp(err);
+      break;
+    case kHaloBound:
+      E.mgbound();
+      break;
+    default:
+      if (err) *err = "unknown halo kind";
+      return H3D_ERR_ARG;
+  }
+  if (!ok) return H3D_ERR_BAD_CONFIG;
+  dst.clear();
+  src.clear();
+  for (size_t b = 0; b < L.bl.size(); ++b) {
+    const BlkLev& B = L.bl[b];
+    for (int z = 0; z <= B.nz + 1; ++z)
+      for (int y = 0; y <= B.ny + 1; ++y)
+        for (int x = 0; x <= B.nx + 1; ++x) {
+          int outside = (x == 0 || x == B.nx + 1) + (y == 0 || y == B.ny + 1) + (z == 0 || z == B.nz + 1);
+          if (outside == 0) {
+            // interior cells are never written by the fill; x jumps across the row
+            if (x == 0) continue;
+            x = B.nx;  // skip to the east ghost
+            continue;
+          }
+          if (kind == kHaloFaces && outside != 1) continue;
+          size_t q = E.at((int)b, x, y, z);
+          uint32_t s = E.id[q];
+          bool inter = E.is_interior(s);
+          if (kind == kHaloFaces) {
+            if (!inter) {
+              if (err) *err = "face ghost without an interior source";
+              return H3D_ERR_INTERNAL;
+            }
+            if (s == (uint32_t)q) continue;
+          }
+          dst.push_back((uint32_t)q);
+          src.push_back(inter ? s : (s | kOldFlag));
+        }
+  }
+  return H3D_OK;
+}
+
+}  // namespace h3d
+
+extern "C" int h3d_halo_table(int32_t nblocks, const h3d_block_desc* blocks, int32_t g, int32_t kind,
+                              uint32_t* dst, uint32_t* src, int64_t cap, int64_t* n) {
+  if (!blocks || nblocks <= 0 || g < 1 || !n) return H3D_ERR_ARG;
+  std::vector<h3d_block_desc> D(blocks, blocks + nblocks);
+  for (auto& d : D)
+    if (g > d.ngrid || d.ngrid < 1) return H3D_ERR_ARG;
+  std::vector<uint32_t> vd, vs;
+  int rc = h3d::build_halo_table(D, g, kind, vd, vs, nullptr);
+  if (rc != H3D_OK) return rc;
+  *n = (int64_t)vd.size();
+  if (dst && src) {
+    if (cap < (int64_t)vd.size()) return H3D_ERR_ARG;
+    std::memcpy(dst, vd.data(), vd.size() * sizeof(uint32_t));
+    std::memcpy(src, vs.data(), vs.size() * sizeof(uint32_t));
+  }
+  return H3D_OK;
+}

@@ -1,0 +1,52 @@
+// Internal declarations shared by the host runtime (h3d_mg.cu), the halo
+// table builder (h3d_halo.cpp) and the kernels (h3d_kernels.cu).
+#pragma once
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/h3d_mg.h"
+
+namespace h3d {
+
+constexpr int kMaxLevels = 16;
+constexpr uint32_t kOldFlag = 0x80000000u;  // halo entry reads the pre-fill value
+constexpr uint32_t kIdxMask = 0x7fffffffu;
+
+// Per-(block, level) geometry as the kernels see it.  Cell (x,y,z), 0-based
+// with the ghost layer at 0 and n+1, lives at off + (z*(ny+2) + y)*(nx+2) + x.
+struct BlkLev {
+  int nx, ny, nz;       // interior cells
+  int sx;               // nx + 2
+  long long sxy;        // (nx+2)*(ny+2)
+  long long off;        // element offset of cell (0,0,0) in the level array
+  int phys;             // bit f set: face f (W,E,S,N,B,T) is a physical non-periodic wall
+  int pad;
+  double ax, ay, az;    // constant coefficients 1/dxx, 1/dyy, 1/dzz (mgsolver.for:54-60,186-191)
+  double dv;            // cell volume at level 1 (dx*dy*dz), for the rmax measure
+};
+
+// Tile of the smoother / cell kernels: block, first interior x, y, z of the tile.
+struct Tile {
+  int b, x0, y0, z0;
+};
+
+// Level geometry in the canonical packed numbering.
+struct LevelGeom {
+  int g = 0;
+  std::vector<BlkLev> bl;
+  int64_t n_elems = 0;      // total cells incl. ghosts
+  int64_t n_interior = 0;   // total interior cells
+};
+
+// Builds the level geometry from block descriptors (level dims with the
+// reference's clamp, mgsolver.for:392-400).
+LevelGeom make_level_geom(const std::vector<h3d_block_desc>& blocks, int g);
+
+// Halo gather tables (see h3d_halo_table in h3d_mg.h).
+enum HaloKind { kHaloSweep = 0, kHaloExchange = 1, kHaloBound = 2, kHaloFaces = 3 };
+int build_halo_table(const std::vector<h3d_block_desc>& blocks, int g, int kind,
+                     std::vector<uint32_t>& dst, std::vector<uint32_t>& src,
+                     std::string* err);
+
+}  // namespace h3d

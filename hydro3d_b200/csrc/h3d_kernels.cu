@@ -1,0 +1,588 @@
+// sm_100a kernels of the multigrid V-cycle.
+//
+// All FP64 arithmetic follows the reference's operand order (mgsolver.for)
+// and the library is compiled with --fmad=false, so the FP64 path reproduces
+// the reference arithmetic bit for bit.  Every kernel is memory bound (a
+// 7-point stencil is not a contraction; no tensor cores are used).
+#include <cstdint>
+
+#include "h3d_kernels.cuh"
+
+namespace h3d {
+
+namespace {
+
+__device__ __forceinline__ int find_block(const int* __restrict__ start, int nb, int cta) {
+  int lo = 0, hi = nb;  // start[lo] <= cta < start[hi]
+  while (hi - lo > 1) {
+    int mid = (lo + hi) >> 1;
+    if (__ldg(start + mid) <= cta) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
+template <typename T>
+struct Coef {
+  T aw, ae, as, an, ab, at;
+};
+
+// Face coefficients of interior cell (x,y,z) (mgsolver.for:186-205).
+template <typename T, bool VAR>
+__device__ __forceinline__ Coef<T> cell_coef(const BlkLev& B, int x, int y, int z, long long i, const T* fx,
+                                             const T* fy, const T* fz) {
+  Coef<T> c;
+  if (VAR) {
+    c.aw = fx[i - 1];
+    c.ae = fx[i];
+    c.as = fy[i - B.sx];
+    c.an = fy[i];
+    c.ab = fz[i - B.sxy];
+    c.at = fz[i];
+  } else {
+    const T ax = (T)B.ax, ay = (T)B.ay, az = (T)B.az;
+    const int ph = B.phys;
+    c.aw = (x == 1 && (ph & 1)) ? T(0) : ax;
+    c.ae = (x == B.nx && (ph & 2)) ? T(0) : ax;
+    c.as = (y == 1 && (ph & 4)) ? T(0) : ay;
+    c.an = (y == B.ny && (ph & 8)) ? T(0) : ay;
+    c.ab = (z == 1 && (ph & 16)) ? T(0) : az;
+    c.at = (z == B.nz && (ph & 32)) ? T(0) : az;
+  }
+  return c;
+}
+
+template <typename T>
+__device__ __forceinline__ T coef_ap(const Coef<T>& c) {
+  return -(c.aw + c.ae + c.as + c.an + c.ab + c.at);  // -1.0*(...), mgsolver.for:207-210
+}
+
+// ---------------------------------------------------------------------------
+// Red-black Gauss-Seidel sweep (mgrelax, mg_itrsch=3, mgsolver.for:551-605).
+//
+// Colour = MOD(i+j+k,2) of the reference's 1-based ghost-inclusive indices,
+// i.e. red (first pass) <=> x+y+z odd in 0-based ghost-inclusive coordinates.
+// The sweep is out of place: every CTA reads the previous iterate `src` and
+// writes `dst`, so tiles can overlap without ordering between CTAs.  A CTA
+// owns a TX x TY column of one block and marches a z range through a ring of
+// four shared-memory planes: at step z it stages plane z+1, updates the red
+// cells of plane z on the tile plus a one-cell ring (their old black
+// neighbours are in the two-cell staged halo), then updates the black cells
+// of plane z-1 from the new red values and stores plane z-1.  Ghost cells are
+// never updated inside a sweep, exactly like the reference, where they change
+// only in the mgbound/exchangepp call after the whole sweep.
+template <typename T, int TX, int TY, int NT, bool VAR, bool ZERO>
+__global__ void __launch_bounds__(NT) k_rbgs(const BlkLev* __restrict__ bls, const Tile* __restrict__ tiles,
+                                             int zc, const T* __restrict__ src, T* __restrict__ dst,
+                                             const T* __restrict__ rhs, const T* __restrict__ fx,
+                                             const T* __restrict__ fy, const T* __restrict__ fz) {
+  constexpr int RX = TX + 4, RY = TY + 4, RN = RX * RY;
+  constexpr int R1X = TX + 2, R1N = (TX + 2) * (TY + 2);
+  __shared__ T ring[4][RN];
+  const Tile t = tiles[blockIdx.x];
+  const BlkLev B = bls[t.b];
+  const int nx = B.nx, ny = B.ny, nz = B.nz;
+  const long long sx = B.sx, sxy = B.sxy;
+  const T* __restrict__ S = src + B.off;
+  T* __restrict__ D = dst + B.off;
+  const T* __restrict__ R = rhs + B.off;
+  const T* FX = VAR ? fx + B.off : nullptr;
+  const T* FY = VAR ? fy + B.off : nullptr;
+  const T* FZ = VAR ? fz + B.off : nullptr;
+  const int x0 = t.x0, y0 = t.y0, zs = t.z0;
+  const int ze = min(zs + zc - 1, nz);
+  const int zlo = max(zs - 1, 1), zhi = min(ze + 1, nz);
+
+  auto stage = [&](int z) {
+    T* P = ring[z & 3];
+    const T* Sz = S + (long long)z * sxy;
+    for (int q = threadIdx.x; q < RN; q += NT) {
+      int ly = q / RX, lx = q - ly * RX;
+      int x = x0 - 2 + lx, y = y0 - 2 + ly;
+      T v = T(0);
+      if (!ZERO && x >= 0 && x <= nx + 1 && y >= 0 && y <= ny + 1) v = Sz[y * sx + x];
+      P[q] = v;
+    }
+  };
+  auto red = [&](int z) {
+    T* P = ring[z & 3];
+    const T* Pm = ring[(z - 1) & 3];
+    const T* Pp = ring[(z + 1) & 3];
+    for (int q = threadIdx.x; q < R1N; q += NT) {
+      int ly = q / R1X, lx = q - ly * R1X;
+      int x = x0 - 1 + lx, y = y0 - 1 + ly;
+      if (x < 1 || x > nx || y < 1 || y > ny || ((x + y + z) & 1) == 0) continue;
+      int s = (ly + 1) * RX + lx + 1;
+      long long i = (long long)z * sxy + y * sx + x;
+      Coef<T> c = cell_coef<T, VAR>(B, x, y, z, i, FX, FY, FZ);
+      T ap = coef_ap(c);
+      P[s] = (R[i] - (c.aw * P[s - 1] + c.ae * P[s + 1] + c.as * P[s - RX] + c.an * P[s + RX] +
+                      c.ab * Pm[s] + c.at * Pp[s])) /
+             ap;
+    }
+  };
+  auto black_store = [&](int z) {
+    const T* P = ring[z & 3];
+    const T* Pm = ring[(z - 1) & 3];
+    const T* Pp = ring[(z + 1) & 3];
+    T* Dz = D + (long long)z * sxy;
+    for (int q = threadIdx.x; q < TX * TY; q += NT) {
+      int ly = q / TX, lx = q - ly * TX;
+      int x = x0 + lx, y = y0 + ly;
+      if (x > nx || y > ny) continue;
+      int s = (ly + 2) * RX + lx + 2;
+      long long i = (long long)z * sxy + y * sx + x;
+      T v;
+      if ((x + y + z) & 1) {
+        v = P[s];  // red, updated at the previous step
+      } else {
+        Coef<T> c = cell_coef<T, VAR>(B, x, y, z, i, FX, FY, FZ);
+        T ap = coef_ap(c);
+        v = (R[i] - (c.aw * P[s - 1] + c.ae * P[s + 1] + c.as * P[s - RX] + c.an * P[s + RX] +
+                     c.ab * Pm[s] + c.at * Pp[s])) /
+            ap;
+      }
+      Dz[y * sx + x] = v;
+    }
+  };
+
+  stage(zlo - 1);
+  stage(zlo);
+  for (int z = zlo; z <= zhi; ++z) {
+    stage(z + 1);
+    __syncthreads();
+    red(z);
+    __syncthreads();
+    if (z - 1 >= zs && z - 1 <= ze) black_store(z - 1);
+    __syncthreads();
+  }
+  if (ze == nz) black_store(nz);
+}
+
+// ---------------------------------------------------------------------------
+template <typename T, bool ZERO_OLD>
+__global__ void k_fill(const uint32_t* __restrict__ dsts, const uint32_t* __restrict__ srcs, int64_t n,
+                       T* __restrict__ out, const T* __restrict__ cur, const T* __restrict__ old) {
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+    uint32_t s = __ldg(srcs + e);
+    T v;
+    if (s & kOldFlag) v = ZERO_OLD ? T(0) : old[s & kIdxMask];
+    else v = cur[s];
+    out[__ldg(dsts + e)] = v;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// mgrestr: resf = su - (A phi) on the fine interior (mgsolver.for:707-714),
+// coarse rhs = 0.125 * sum of the 2x2x2 children, i fastest (:748-752).
+template <typename T, bool VAR, bool ZERO>
+__global__ void __launch_bounds__(256) k_restrict(const BlkLev* __restrict__ fine, const BlkLev* __restrict__ coarse,
+                                                  const int* __restrict__ cta_start, int nb,
+                                                  const T* __restrict__ phi, const T* __restrict__ rhs,
+                                                  T* __restrict__ rhs_c, const T* __restrict__ fx,
+                                                  const T* __restrict__ fy, const T* __restrict__ fz) {
+  const int b = find_block(cta_start, nb, blockIdx.x);
+  const BlkLev C = coarse[b];
+  const BlkLev F = fine[b];
+  const int local = (blockIdx.x - cta_start[b]) * blockDim.x + threadIdx.x;
+  if (local >= C.nx * C.ny * C.nz) return;
+  const int X = local % C.nx + 1;
+  const int Y = (local / C.nx) % C.ny + 1;
+  const int Z = local / (C.nx * C.ny) + 1;
+  const T* P = phi + F.off;
+  const T* Rf = rhs + F.off;
+  T sum = T(0);
+  bool first = true;
+#pragma unroll
+  for (int dk = 0; dk < 2; ++dk)
+#pragma unroll
+    for (int dj = 0; dj < 2; ++dj)
+#pragma unroll
+      for (int di = 0; di < 2; ++di) {
+        int x = 2 * X - 1 + di, y = 2 * Y - 1 + dj, z = 2 * Z - 1 + dk;
+        long long i = (long long)z * F.sxy + (long long)y * F.sx + x;
+        T r;
+        if (ZERO) {
+          r = Rf[i] - T(0);
+        } else {
+          Coef<T> c = cell_coef<T, VAR>(F, x, y, z, i, fx ? fx + F.off : nullptr, fy ? fy + F.off : nullptr,
+                                        fz ? fz + F.off : nullptr);
+          T ap = coef_ap(c);
+          r = Rf[i] - (c.aw * P[i - 1] + c.ae * P[i + 1] + c.as * P[i - F.sx] + c.an * P[i + F.sx] +
+                       c.ab * P[i - F.sxy] + c.at * P[i + F.sxy] + ap * P[i]);
+        }
+        if (first) { sum = r; first = false; }
+        else sum = sum + r;
+      }
+  rhs_c[C.off + (long long)Z * C.sxy + (long long)Y * C.sx + X] = T(0.125) * sum;
+}
+
+// ---------------------------------------------------------------------------
+// mgcorr + mgbound: for every fine cell incl. ghosts, out = old[s] + P[s]/64
+// where s is the cell's mgbound source (ghost coordinates on physical faces
+// clamp to the adjacent interior, W,E,S,N,B,T composition) and P the
+// trilinear (27,9,3,1) sum in the reference's term order (mgsolver.for:838-892).
+template <typename T, bool ZERO_OLD>
+__global__ void __launch_bounds__(256) k_prolong(const BlkLev* __restrict__ fine, const BlkLev* __restrict__ coarse,
+                                                 const int* __restrict__ cta_start, int nb,
+                                                 const T* __restrict__ phi_c, const T* __restrict__ old,
+                                                 T* __restrict__ out) {
+  const int b = find_block(cta_start, nb, blockIdx.x);
+  const BlkLev F = fine[b];
+  const BlkLev C = coarse[b];
+  const int local = (blockIdx.x - cta_start[b]) * blockDim.x + threadIdx.x;
+  const int mx = F.nx + 2, my = F.ny + 2, mz = F.nz + 2;
+  if (local >= mx * my * mz) return;
+  const int x = local % mx, y = (local / mx) % my, z = local / (mx * my);
+  const int ph = F.phys;
+  int sx = x, sy = y, sz = z;
+  if (x == 0 && (ph & 1)) sx = 1;
+  if (x == F.nx + 1 && (ph & 2)) sx = F.nx;
+  if (y == 0 && (ph & 4)) sy = 1;
+  if (y == F.ny + 1 && (ph & 8)) sy = F.ny;
+  if (z == 0 && (ph & 16)) sz = 1;
+  if (z == F.nz + 1 && (ph & 32)) sz = F.nz;
+  const int lx = sx >> 1, ly = sy >> 1, lz = sz >> 1;
+  const T wx0 = (sx & 1) ? T(1) : T(3), wx1 = (sx & 1) ? T(3) : T(1);
+  const T wy0 = (sy & 1) ? T(1) : T(3), wy1 = (sy & 1) ? T(3) : T(1);
+  const T wz0 = (sz & 1) ? T(1) : T(3), wz1 = (sz & 1) ? T(3) : T(1);
+  const T* Pc = phi_c + C.off + (long long)lz * C.sxy + (long long)ly * C.sx + lx;
+  const long long cx = 1, cy = C.sx, cz = C.sxy;
+  // term order (di,dj,dk): 000, 010, 001, 011, 100, 110, 101, 111
+  T s = (wx0 * wy0 * wz0) * Pc[0];
+  s = s + (wx0 * wy1 * wz0) * Pc[cy];
+  s = s + (wx0 * wy0 * wz1) * Pc[cz];
+  s = s + (wx0 * wy1 * wz1) * Pc[cy + cz];
+  s = s + (wx1 * wy0 * wz0) * Pc[cx];
+  s = s + (wx1 * wy1 * wz0) * Pc[cx + cy];
+  s = s + (wx1 * wy0 * wz1) * Pc[cx + cz];
+  s = s + (wx1 * wy1 * wz1) * Pc[cx + cy + cz];
+  const long long is = (long long)sz * F.sxy + (long long)sy * F.sx + sx;
+  const T o = ZERO_OLD ? T(0) : old[F.off + is];
+  out[F.off + (long long)z * F.sxy + (long long)y * F.sx + x] = o + s / T(64);
+}
+
+// ---------------------------------------------------------------------------
+template <int NT>
+__device__ __forceinline__ void block_reduce4(double a0, double a1, double a2, double a3, double* out) {
+  __shared__ double sh[4][NT / 32];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    a0 += __shfl_xor_sync(0xffffffffu, a0, o);
+    a1 += __shfl_xor_sync(0xffffffffu, a1, o);
+    a2 = fmax(a2, __shfl_xor_sync(0xffffffffu, a2, o));
+    a3 += __shfl_xor_sync(0xffffffffu, a3, o);
+  }
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) { sh[0][w] = a0; sh[1][w] = a1; sh[2][w] = a2; sh[3][w] = a3; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+    for (int q = 0; q < NT / 32; ++q) { s0 += sh[0][q]; s1 += sh[1][q]; s2 = fmax(s2, sh[2][q]); s3 += sh[3][q]; }
+    out[0] = s0; out[1] = s1; out[2] = s2; out[3] = s3;
+  }
+}
+
+// newsolv_mg.for:39-55 as defect correction: p += pp over the whole block
+// (ghosts included, :40-48), then r = b - A p (mgrestr's residual form).
+template <typename TE, typename TR, bool HAS_E, bool VAR>
+__global__ void __launch_bounds__(256) k_defect(const BlkLev* __restrict__ bls, const int* __restrict__ cta_start,
+                                                int nb, const double* __restrict__ p, const TE* __restrict__ e,
+                                                double* __restrict__ p_next, const double* __restrict__ bvec,
+                                                TR* __restrict__ rhs_out, double mean_b, double rscale,
+                                                const double* __restrict__ fx, const double* __restrict__ fy,
+                                                const double* __restrict__ fz, double* __restrict__ partials) {
+  const int b = find_block(cta_start, nb, blockIdx.x);
+  const BlkLev B = bls[b];
+  const int local = (blockIdx.x - cta_start[b]) * blockDim.x + threadIdx.x;
+  const int mx = B.nx + 2, my = B.ny + 2, mz = B.nz + 2;
+  double rr = 0, bb = 0, rm = 0, rs = 0;
+  if (local < mx * my * mz) {
+    const int x = local % mx, y = (local / mx) % my, z = local / (mx * my);
+    const long long i = B.off + (long long)z * B.sxy + (long long)y * B.sx + x;
+    auto pv = [&](long long j) -> double {
+      if (HAS_E) return p[j] + (double)e[j];
+      return p[j];
+    };
+    const double pc = pv(i);
+    if (HAS_E) p_next[i] = pc;
+    if (x >= 1 && x <= B.nx && y >= 1 && y <= B.ny && z >= 1 && z <= B.nz) {
+      Coef<double> c = cell_coef<double, VAR>(B, x, y, z, i - B.off, fx ? fx + B.off : nullptr,
+                                              fy ? fy + B.off : nullptr, fz ? fz + B.off : nullptr);
+      double ap = coef_ap(c);
+      const double bv = bvec[i];
+      double r = bv - (c.aw * pv(i - 1) + c.ae * pv(i + 1) + c.as * pv(i - B.sx) + c.an * pv(i + B.sx) +
+                       c.ab * pv(i - B.sxy) + c.at * pv(i + B.sxy) + ap * pc);
+      rhs_out[i] = (TR)(r - mean_b);
+      rr = r * r;
+      bb = bv * bv;
+      rm = fabs(r) * rscale;
+      rs = r;
+    }
+  }
+  block_reduce4<256>(rr, bb, rm, rs, partials + 4 * (size_t)blockIdx.x);
+}
+
+__global__ void __launch_bounds__(256) k_reduce4(const double* __restrict__ partials, int n, double* __restrict__ out) {
+  double a0 = 0, a1 = 0, a2 = 0, a3 = 0;
+  for (int q = threadIdx.x; q < n; q += 256) {
+    a0 += partials[4 * (size_t)q];
+    a1 += partials[4 * (size_t)q + 1];
+    a2 = fmax(a2, partials[4 * (size_t)q + 2]);
+    a3 += partials[4 * (size_t)q + 3];
+  }
+  block_reduce4<256>(a0, a1, a2, a3, out);
+}
+
+__global__ void __launch_bounds__(256) k_sum_interior(const BlkLev* __restrict__ bls, const int* __restrict__ cta_start,
+                                                      int nb, const double* __restrict__ a,
+                                                      double* __restrict__ partials) {
+  const int b = find_block(cta_start, nb, blockIdx.x);
+  const BlkLev B = bls[b];
+  const int local = (blockIdx.x - cta_start[b]) * blockDim.x + threadIdx.x;
+  double s = 0;
+  if (local < B.nx * B.ny * B.nz) {
+    const int x = local % B.nx + 1, y = (local / B.nx) % B.ny + 1, z = local / (B.nx * B.ny) + 1;
+    s = a[B.off + (long long)z * B.sxy + (long long)y * B.sx + x];
+  }
+  block_reduce4<256>(s, 0.0, 0.0, 0.0, partials + 4 * (size_t)blockIdx.x);
+}
+
+__global__ void k_shift(double* __restrict__ a, int64_t n, const double* __restrict__ s, double scale) {
+  const double v = s[0] * scale;
+  for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x)
+    a[q] = a[q] - v;
+}
+
+__global__ void k_d2f(const double* __restrict__ a, float* __restrict__ b, int64_t n) {
+  for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x)
+    b[q] = (float)a[q];
+}
+__global__ void k_f2d(const float* __restrict__ a, double* __restrict__ b, int64_t n) {
+  for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x)
+    b[q] = (double)a[q];
+}
+
+// dens_mg of level g = 0.125 * sum of the 8 children of level g-1 in the
+// order of mgsolver.for:91-104 (j fastest, then i, then k).
+__global__ void __launch_bounds__(256) k_dens_restrict(const BlkLev* __restrict__ fine, const BlkLev* __restrict__ coarse,
+                                                       const int* __restrict__ cta_start, int nb,
+                                                       const double* __restrict__ df, double* __restrict__ dc) {
+  const int b = find_block(cta_start, nb, blockIdx.x);
+  const BlkLev C = coarse[b], F = fine[b];
+  const int local = (blockIdx.x - cta_start[b]) * blockDim.x + threadIdx.x;
+  if (local >= C.nx * C.ny * C.nz) return;
+  const int X = local % C.nx + 1, Y = (local / C.nx) % C.ny + 1, Z = local / (C.nx * C.ny) + 1;
+  const double* P = df + F.off + (long long)(2 * Z - 1) * F.sxy + (long long)(2 * Y - 1) * F.sx + (2 * X - 1);
+  const long long I = 1, J = F.sx, K = F.sxy;
+  double s = P[0] + P[J] + P[I] + P[I + J] + P[K] + P[K + J] + P[K + I] + P[K + I + J];
+  dc[C.off + (long long)Z * C.sxy + (long long)Y * C.sx + X] = 0.125 * s;
+}
+
+// L_LSM face coefficients (mgsolver.for:130-184): face arrays at the cell
+// index of the lower cell; block faces use the cell's own density; the
+// fine-level dx, dy, dz are used at every level; physical faces are zeroed
+// (:194-205).
+__global__ void __launch_bounds__(256) k_face_coef(const BlkLev* __restrict__ bls, const int* __restrict__ cta_start,
+                                                   int nb, const double* __restrict__ dens,
+                                                   const double* __restrict__ h3, double* __restrict__ fx,
+                                                   double* __restrict__ fy, double* __restrict__ fz) {
+  const int b = find_block(cta_start, nb, blockIdx.x);
+  const BlkLev B = bls[b];
+  const int local = (blockIdx.x - cta_start[b]) * blockDim.x + threadIdx.x;
+  const int mx = B.nx + 2, my = B.ny + 2, mz = B.nz + 2;
+  if (local >= mx * my * mz) return;
+  const int x = local % mx, y = (local / mx) % my, z = local / (mx * my);
+  const double dx = h3[3 * b], dy = h3[3 * b + 1], dz = h3[3 * b + 2];
+  const long long i = B.off + (long long)z * B.sxy + (long long)y * B.sx + x;
+  const bool iny = y >= 1 && y <= B.ny, inz = z >= 1 && z <= B.nz, inx = x >= 1 && x <= B.nx;
+  // x faces: x in [0, nx]
+  if (x <= B.nx && iny && inz) {
+    double d;
+    if (x == 0) d = dens[i + 1];
+    else if (x == B.nx) d = dens[i];
+    else d = 0.5 * (dens[i] + dens[i + 1]);
+    double v = dy * dz / dx / d;
+    if ((x == 0 && (B.phys & 1)) || (x == B.nx && (B.phys & 2))) v = 0.0;
+    fx[i] = v;
+  }
+  if (y <= B.ny && inx && inz) {
+    double d;
+    if (y == 0) d = dens[i + B.sx];
+    else if (y == B.ny) d = dens[i];
+    else d = 0.5 * (dens[i] + dens[i + B.sx]);
+    double v = dx * dz / dy / d;
+    if ((y == 0 && (B.phys & 4)) || (y == B.ny && (B.phys & 8))) v = 0.0;
+    fy[i] = v;
+  }
+  if (z <= B.nz && inx && iny) {
+    double d;
+    if (z == 0) d = dens[i + B.sxy];
+    else if (z == B.nz) d = dens[i];
+    else d = 0.5 * (dens[i] + dens[i + B.sxy]);
+    double v = dx * dy / dz / d;
+    if ((z == 0 && (B.phys & 16)) || (z == B.nz && (B.phys & 32))) v = 0.0;
+    fz[i] = v;
+  }
+}
+
+inline int grid_for(int64_t n, int nt) {
+  int64_t g = (n + nt - 1) / nt;
+  if (g > 148 * 32) g = 148 * 32;
+  if (g < 1) g = 1;
+  return (int)g;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+static const TileShape kShapes[] = {
+    {32, 16, 256}, {32, 8, 256}, {64, 8, 256}, {16, 8, 128}, {8, 8, 64}, {8, 4, 32}, {4, 4, 32}, {64, 16, 512},
+};
+int num_tile_shapes() { return (int)(sizeof(kShapes) / sizeof(kShapes[0])); }
+TileShape tile_shape(int v) { return kShapes[v]; }
+
+template <typename T, int TX, int TY, int NT>
+static cudaError_t rbgs_dispatch(bool var, bool zero, const BlkLev* bl, const Tile* tiles, int ntiles, int zc,
+                                 const T* src, T* dst, const T* rhs, const T* fx, const T* fy, const T* fz,
+                                 cudaStream_t st) {
+  if (ntiles <= 0) return cudaSuccess;
+  dim3 grid(ntiles), block(NT);
+  if (var) {
+    if (zero) k_rbgs<T, TX, TY, NT, true, true><<<grid, block, 0, st>>>(bl, tiles, zc, src, dst, rhs, fx, fy, fz);
+    else k_rbgs<T, TX, TY, NT, true, false><<<grid, block, 0, st>>>(bl, tiles, zc, src, dst, rhs, fx, fy, fz);
+  } else {
+    if (zero) k_rbgs<T, TX, TY, NT, false, true><<<grid, block, 0, st>>>(bl, tiles, zc, src, dst, rhs, fx, fy, fz);
+    else k_rbgs<T, TX, TY, NT, false, false><<<grid, block, 0, st>>>(bl, tiles, zc, src, dst, rhs, fx, fy, fz);
+  }
+  return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_rbgs(int variant, bool var, bool zero_src, const BlkLev* bl, const Tile* tiles, int ntiles,
+                        int zc, const T* src, T* dst, const T* rhs, const T* fx, const T* fy, const T* fz,
+                        cudaStream_t st) {
+  switch (variant) {
+    case 0: return rbgs_dispatch<T, 32, 16, 256>(var, zero_src, bl, tiles, ntiles, zc, src, dst, rhs, fx, fy, fz, st);
+    case 1: return rbgs_dispatch<T, 32, 8, 256>(var, zero_src, bl, tiles, ntiles, zc, src, dst, rhs, fx, fy, fz, st);
+    case 2: return rbgs_dispatch<T, 64, 8, 256>(var, zero_src, bl, tiles, ntiles, zc, src, dst, rhs, fx, fy, fz, st);
+    case 3: return rbgs_dispatch<T, 16, 8, 128>(var, zero_src, bl, tiles, ntiles, zc, src, dst, rhs, fx, fy, fz, st);
+    case 4: return rbgs_dispatch<T, 8, 8, 64>(var, zero_src, bl, tiles, ntiles, zc, src, dst, rhs, fx, fy, fz, st);
+    case 5: return rbgs_dispatch<T, 8, 4, 32>(var, zero_src, bl, tiles, ntiles, zc, src, dst, rhs, fx, fy, fz, st);
+    case 6: return rbgs_dispatch<T, 4, 4, 32>(var, zero_src, bl, tiles, ntiles, zc, src, dst, rhs, fx, fy, fz, st);
+    case 7: return rbgs_dispatch<T, 64, 16, 512>(var, zero_src, bl, tiles, ntiles, zc, src, dst, rhs, fx, fy, fz, st);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+template <typename T>
+cudaError_t launch_fill(const uint32_t* dsts, const uint32_t* srcs, int64_t n, T* out, const T* cur, const T* old,
+                        bool zero_old, cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  int g = grid_for(n, 256);
+  if (zero_old) k_fill<T, true><<<g, 256, 0, st>>>(dsts, srcs, n, out, cur, old);
+  else k_fill<T, false><<<g, 256, 0, st>>>(dsts, srcs, n, out, cur, old);
+  return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_restrict(bool var, bool zero_phi, const BlkLev* fine, const BlkLev* coarse, CellTab ct,
+                            const T* phi, const T* rhs, T* rhs_c, const T* fx, const T* fy, const T* fz,
+                            cudaStream_t st) {
+  if (ct.ncta <= 0) return cudaSuccess;
+  if (zero_phi) k_restrict<T, false, true><<<ct.ncta, 256, 0, st>>>(fine, coarse, ct.cta_start, ct.nb, phi, rhs, rhs_c, fx, fy, fz);
+  else if (var) k_restrict<T, true, false><<<ct.ncta, 256, 0, st>>>(fine, coarse, ct.cta_start, ct.nb, phi, rhs, rhs_c, fx, fy, fz);
+  else k_restrict<T, false, false><<<ct.ncta, 256, 0, st>>>(fine, coarse, ct.cta_start, ct.nb, phi, rhs, rhs_c, fx, fy, fz);
+  return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_prolong(bool zero_old, const BlkLev* fine, const BlkLev* coarse, CellTab ct, const T* phi_c,
+                           const T* old, T* out, cudaStream_t st) {
+  if (ct.ncta <= 0) return cudaSuccess;
+  if (zero_old) k_prolong<T, true><<<ct.ncta, 256, 0, st>>>(fine, coarse, ct.cta_start, ct.nb, phi_c, old, out);
+  else k_prolong<T, false><<<ct.ncta, 256, 0, st>>>(fine, coarse, ct.cta_start, ct.nb, phi_c, old, out);
+  return cudaGetLastError();
+}
+
+template <typename TE, typename TR>
+cudaError_t launch_defect(bool var, const BlkLev* bl, CellTab ct, const double* p, const TE* e, double* p_next,
+                          const double* b, TR* rhs_out, double mean_b, double rscale, const double* fx,
+                          const double* fy, const double* fz, double* partials, cudaStream_t st) {
+  if (ct.ncta <= 0) return cudaSuccess;
+  if (e) {
+    if (var) k_defect<TE, TR, true, true><<<ct.ncta, 256, 0, st>>>(bl, ct.cta_start, ct.nb, p, e, p_next, b, rhs_out, mean_b, rscale, fx, fy, fz, partials);
+    else k_defect<TE, TR, true, false><<<ct.ncta, 256, 0, st>>>(bl, ct.cta_start, ct.nb, p, e, p_next, b, rhs_out, mean_b, rscale, fx, fy, fz, partials);
+  } else {
+    if (var) k_defect<TE, TR, false, true><<<ct.ncta, 256, 0, st>>>(bl, ct.cta_start, ct.nb, p, e, p_next, b, rhs_out, mean_b, rscale, fx, fy, fz, partials);
+    else k_defect<TE, TR, false, false><<<ct.ncta, 256, 0, st>>>(bl, ct.cta_start, ct.nb, p, e, p_next, b, rhs_out, mean_b, rscale, fx, fy, fz, partials);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_reduce4(const double* partials, int n, double* out, cudaStream_t st) {
+  k_reduce4<<<1, 256, 0, st>>>(partials, n, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_sum_interior(const BlkLev* bl, CellTab ct, const double* a, double* partials, cudaStream_t st) {
+  if (ct.ncta <= 0) return cudaSuccess;
+  k_sum_interior<<<ct.ncta, 256, 0, st>>>(bl, ct.cta_start, ct.nb, a, partials);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_shift(double* a, int64_t n, const double* s, double scale, cudaStream_t st) {
+  k_shift<<<grid_for(n, 256), 256, 0, st>>>(a, n, s, scale);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_convert_d2f(const double* a, float* b, int64_t n, cudaStream_t st) {
+  k_d2f<<<grid_for(n, 256), 256, 0, st>>>(a, b, n);
+  return cudaGetLastError();
+}
+cudaError_t launch_convert_f2d(const float* a, double* b, int64_t n, cudaStream_t st) {
+  k_f2d<<<grid_for(n, 256), 256, 0, st>>>(a, b, n);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_dens_restrict(const BlkLev* fine, const BlkLev* coarse, CellTab ct, const double* df, double* dc,
+                                 cudaStream_t st) {
+  if (ct.ncta <= 0) return cudaSuccess;
+  k_dens_restrict<<<ct.ncta, 256, 0, st>>>(fine, coarse, ct.cta_start, ct.nb, df, dc);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_face_coef(const BlkLev* bl, CellTab ct, const double* dens, const double* h3, double* fx,
+                             double* fy, double* fz, cudaStream_t st) {
+  if (ct.ncta <= 0) return cudaSuccess;
+  k_face_coef<<<ct.ncta, 256, 0, st>>>(bl, ct.cta_start, ct.nb, dens, h3, fx, fy, fz);
+  return cudaGetLastError();
+}
+
+// explicit instantiations
+template cudaError_t launch_rbgs<double>(int, bool, bool, const BlkLev*, const Tile*, int, int, const double*, double*,
+                                         const double*, const double*, const double*, const double*, cudaStream_t);
+template cudaError_t launch_rbgs<float>(int, bool, bool, const BlkLev*, const Tile*, int, int, const float*, float*,
+                                        const float*, const float*, const float*, const float*, cudaStream_t);
+template cudaError_t launch_fill<double>(const uint32_t*, const uint32_t*, int64_t, double*, const double*,
+                                         const double*, bool, cudaStream_t);
+template cudaError_t launch_fill<float>(const uint32_t*, const uint32_t*, int64_t, float*, const float*, const float*,
+                                        bool, cudaStream_t);
+template cudaError_t launch_restrict<double>(bool, bool, const BlkLev*, const BlkLev*, CellTab, const double*,
+                                             const double*, double*, const double*, const double*, const double*,
+                                             cudaStream_t);
+template cudaError_t launch_restrict<float>(bool, bool, const BlkLev*, const BlkLev*, CellTab, const float*,
+                                            const float*, float*, const float*, const float*, const float*,
+                                            cudaStream_t);
+template cudaError_t launch_prolong<double>(bool, const BlkLev*, const BlkLev*, CellTab, const double*, const double*,
+                                            double*, cudaStream_t);
+template cudaError_t launch_prolong<float>(bool, const BlkLev*, const BlkLev*, CellTab, const float*, const float*,
+                                           float*, cudaStream_t);
+template cudaError_t launch_defect<double, double>(bool, const BlkLev*, CellTab, const double*, const double*, double*,
+                                                   const double*, double*, double, double, const double*,
+                                                   const double*, const double*, double*, cudaStream_t);
+template cudaError_t launch_defect<float, float>(bool, const BlkLev*, CellTab, const double*, const float*, double*,
+                                                 const double*, float*, double, double, const double*, const double*,
+                                                 const double*, double*, cudaStream_t);
+
+}  // namespace h3d

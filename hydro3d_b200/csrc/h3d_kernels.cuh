@@ -1,0 +1,77 @@
+// Device kernels of the multigrid V-cycle (declarations of the launchers).
+#pragma once
+#include <cuda_runtime.h>
+
+#include "h3d_internal.h"
+
+namespace h3d {
+
+// Cell launch table: CTAs of a cell kernel are assigned to blocks by prefix;
+// cta_start[b] is the first CTA of block b, cta_start[nb] the total.
+struct CellTab {
+  const int* cta_start;  // device
+  int nb;
+  int ncta;
+};
+
+// Smoother tile shapes the runtime can choose (autotuned per level).
+struct TileShape {
+  int tx, ty, nt;
+};
+int num_tile_shapes();
+TileShape tile_shape(int variant);
+
+// One out-of-place red-black sweep (both colours) of every block of a level:
+// dst = sweep(src).  zero_src: src is identically zero (not read).
+template <typename T>
+cudaError_t launch_rbgs(int variant, bool var, bool zero_src, const BlkLev* bl, const Tile* tiles,
+                        int ntiles, int zc, const T* src, T* dst, const T* rhs, const T* fx, const T* fy,
+                        const T* fz, cudaStream_t st);
+
+// Ghost gather: out[dst[e]] = (src[e] & old) ? old[src] : cur[src].
+template <typename T>
+cudaError_t launch_fill(const uint32_t* dsts, const uint32_t* srcs, int64_t n, T* out, const T* cur,
+                        const T* old, bool zero_old, cudaStream_t st);
+
+// Residual of the fine level and 8-cell average into the coarse rhs
+// (mgrestr, mgsolver.for:693-756).  zero_phi: fine iterate is zero.
+template <typename T>
+cudaError_t launch_restrict(bool var, bool zero_phi, const BlkLev* fine, const BlkLev* coarse, CellTab ct,
+                            const T* phi, const T* rhs, T* rhs_c, const T* fx, const T* fy, const T* fz,
+                            cudaStream_t st);
+
+// Trilinear correction (mgcorr, mgsolver.for:828-896) with the following
+// mgbound fused: out = old + P(coarse), evaluated at the mgbound source.
+template <typename T>
+cudaError_t launch_prolong(bool zero_old, const BlkLev* fine, const BlkLev* coarse, CellTab ct,
+                           const T* phi_c, const T* old, T* out, cudaStream_t st);
+
+// Level-1 FP64 defect: pn = p + e (all cells, when e != null), r = b - A pn on
+// the interior, rhs_out = r - mean_b (as TR), per-CTA partial sums
+// {sum r^2, sum b^2, max |r|*rscale, sum r} into partials[4*cta].
+template <typename TE, typename TR>
+cudaError_t launch_defect(bool var, const BlkLev* bl, CellTab ct, const double* p, const TE* e,
+                          double* p_next, const double* b, TR* rhs_out, double mean_b, double rscale,
+                          const double* fx, const double* fy, const double* fz, double* partials,
+                          cudaStream_t st);
+// Deterministic reduction of n partial quadruples into out[4].
+cudaError_t launch_reduce4(const double* partials, int n, double* out, cudaStream_t st);
+
+// Interior sum of a level-1 field (per-CTA partials, reduce with launch_reduce4).
+cudaError_t launch_sum_interior(const BlkLev* bl, CellTab ct, const double* a, double* partials,
+                                cudaStream_t st);
+// a -= s on every cell (incl. ghosts); s read from device memory.
+cudaError_t launch_shift(double* a, int64_t n, const double* s, double scale, cudaStream_t st);
+
+// Precision conversions of whole level arrays.
+cudaError_t launch_convert_d2f(const double* a, float* b, int64_t n, cudaStream_t st);
+cudaError_t launch_convert_f2d(const float* a, double* b, int64_t n, cudaStream_t st);
+
+// L_LSM coefficients (mgsolver.for:72-184): dens of the finer level -> dens of
+// level g (8-cell average), and the face coefficient arrays of level g.
+cudaError_t launch_dens_restrict(const BlkLev* fine, const BlkLev* coarse, CellTab ct, const double* df,
+                                 double* dc, cudaStream_t st);
+cudaError_t launch_face_coef(const BlkLev* bl, CellTab ct, const double* dens, const double* h3 /*per block dx,dy,dz*/,
+                             double* fx, double* fy, double* fz, cudaStream_t st);
+
+}  // namespace h3d

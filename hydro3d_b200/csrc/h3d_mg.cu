@@ -1,0 +1,1220 @@
+// Host runtime of the B200 multigrid solver: handle, device layout, V-cycle
+// schedule (the reference's K-cycle control flow, mgsolver.for:272-352),
+// CUDA-graph capture, the FP64 outer defect correction (newsolv_mg.for) and
+// the C ABI declared in include/h3d_mg.h.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "h3d_internal.h"
+#include "h3d_kernels.cuh"
+
+using namespace h3d;
+
+namespace {
+
+thread_local std::string g_create_error;
+
+struct Halo {
+  uint32_t* d_dst = nullptr;
+  uint32_t* d_src = nullptr;
+  int64_t n = 0;
+};
+
+struct Level {
+  LevelGeom geom;
+  BlkLev* d_bl = nullptr;
+  int* d_cta_all = nullptr;  // ghost-inclusive cells
+  int ncta_all = 0;
+  int* d_cta_int = nullptr;  // interior cells
+  int ncta_int = 0;
+  Tile* d_tiles = nullptr;
+  int ntiles = 0;
+  int variant = 0, zc = 1;
+  double* phi64[2] = {nullptr, nullptr};
+  double* rhs64 = nullptr;
+  float* phi32[2] = {nullptr, nullptr};
+  float* rhs32 = nullptr;
+  double *fx64 = nullptr, *fy64 = nullptr, *fz64 = nullptr;
+  float *fx32 = nullptr, *fy32 = nullptr, *fz32 = nullptr;
+  double* dens = nullptr;
+  Halo sweep, faces, exch, bound;
+  int cur64 = 0, cur32 = 0;
+  bool zero64 = false, zero32 = false;
+  double sweep_bytes = 0;  // algorithmic bytes of one sweep (FP64 or FP32 by mode)
+};
+
+struct CachedGraph {
+  cudaGraphExec_t exec = nullptr;
+  std::vector<int> state_after;
+  int64_t kernels = 0;
+  std::vector<cudaEvent_t> events;  // profiling pairs recorded inside the graph
+};
+
+}  // namespace
+
+struct h3d_mg {
+  int device = 0;
+  cudaStream_t st = nullptr;
+  h3d_mg_desc desc{};
+  std::vector<h3d_block_desc> blocks;
+  int L = 1;
+  bool mixed = false, var = false;
+  std::vector<Level> lev;  // index 1..L
+  double* p64[2] = {nullptr, nullptr};
+  int pc = 0;
+  double* b64 = nullptr;
+  double* partials = nullptr;
+  int npartials = 0;
+  double* d_res = nullptr;
+  double* h_res = nullptr;  // pinned, 4 doubles
+  double* d_h3 = nullptr;   // per-block dx,dy,dz
+  double mean_b = 0.0;
+  bool coeffs_ready = false;
+  std::string last_error;
+  // profiling / accounting
+  bool profiling = false;
+  std::vector<cudaEvent_t> ev_eager;  // events of eager (non-graph) iterations
+  int64_t kernels = 0;
+  std::map<std::vector<int>, CachedGraph> graphs;
+  bool capturing = false;
+  std::vector<double> history;
+};
+
+namespace {
+
+int fail(h3d_mg* h, int code, const std::string& msg) {
+  if (h) h->last_error = msg;
+  else g_create_error = msg;
+  return code;
+}
+
+#define CU(...)                                                                                   \
+  do {                                                                                            \
+    cudaError_t _e = (__VA_ARGS__);                                                               \
+    if (_e != cudaSuccess)                                                                        \
+      return fail(h, _e == cudaErrorMemoryAllocation ? H3D_ERR_OOM : H3D_ERR_CUDA,                \
+                  std::string(#__VA_ARGS__).substr(0, 60) + ": " + cudaGetErrorString(_e));       \
+  } while (0)
+
+#define TRY(call)                   \
+  do {                              \
+    int _r = (call);                \
+    if (_r != H3D_OK) return _r;    \
+  } while (0)
+
+template <typename T>
+int dalloc(h3d_mg* h, T** p, size_t n) {
+  *p = nullptr;
+  if (n == 0) return H3D_OK;
+  CU(cudaMalloc((void**)p, n * sizeof(T)));
+  CU(cudaMemsetAsync(*p, 0, n * sizeof(T), h->st));
+  return H3D_OK;
+}
+
+void dfree(void* p) {
+  if (p) cudaFree(p);
+}
+
+int upload_halo(h3d_mg* h, Halo& H, const std::vector<uint32_t>& d, const std::vector<uint32_t>& s) {
+  H.n = (int64_t)d.size();
+  if (H.n == 0) return H3D_OK;
+  TRY(dalloc(h, &H.d_dst, d.size()));
+  TRY(dalloc(h, &H.d_src, s.size()));
+  CU(cudaMemcpy(H.d_dst, d.data(), d.size() * 4, cudaMemcpyHostToDevice));
+  CU(cudaMemcpy(H.d_src, s.data(), s.size() * 4, cudaMemcpyHostToDevice));
+  return H3D_OK;
+}
+
+int build_cta_table(h3d_mg* h, const LevelGeom& G, bool interior, int** d_tab, int* ncta) {
+  std::vector<int> start(G.bl.size() + 1, 0);
+  for (size_t b = 0; b < G.bl.size(); ++b) {
+    const BlkLev& B = G.bl[b];
+    long long cells = interior ? (long long)B.nx * B.ny * B.nz : (long long)(B.nx + 2) * (B.ny + 2) * (B.nz + 2);
+    if (cells >= (1LL << 31)) return fail(h, H3D_ERR_BAD_CONFIG, "block too large");
+    start[b + 1] = start[b] + (int)((cells + 255) / 256);
+  }
+  *ncta = start.back();
+  TRY(dalloc(h, d_tab, start.size()));
+  CU(cudaMemcpy(*d_tab, start.data(), start.size() * sizeof(int), cudaMemcpyHostToDevice));
+  return H3D_OK;
+}
+
+int build_tiles(h3d_mg* h, Level& Lv, int variant, int zc) {
+  TileShape s = tile_shape(variant);
+  std::vector<Tile> t;
+  for (size_t b = 0; b < Lv.geom.bl.size(); ++b) {
+    const BlkLev& B = Lv.geom.bl[b];
+    for (int z0 = 1; z0 <= B.nz; z0 += zc)
+      for (int y0 = 1; y0 <= B.ny; y0 += s.ty)
+        for (int x0 = 1; x0 <= B.nx; x0 += s.tx) t.push_back(Tile{(int)b, x0, y0, z0});
+  }
+  dfree(Lv.d_tiles);
+  Lv.d_tiles = nullptr;
+  TRY(dalloc(h, &Lv.d_tiles, t.size()));
+  CU(cudaMemcpy(Lv.d_tiles, t.data(), t.size() * sizeof(Tile), cudaMemcpyHostToDevice));
+  Lv.ntiles = (int)t.size();
+  Lv.variant = variant;
+  Lv.zc = zc;
+  return H3D_OK;
+}
+
+// Heuristic tile choice (the autotuner refines it on large levels).
+void default_tile(const Level& Lv, int* variant, int* zc) {
+  int nxm = 0, nym = 0, nzm = 0;
+  long long xy_tiles = 0;
+  for (const auto& B : Lv.geom.bl) {
+    nxm = std::max(nxm, B.nx);
+    nym = std::max(nym, B.ny);
+    nzm = std::max(nzm, B.nz);
+  }
+  int v;
+  if (nxm >= 32) v = nym >= 16 ? 0 : 1;
+  else if (nxm >= 16) v = 3;
+  else if (nxm >= 8) v = nym >= 8 ? 4 : 5;
+  else v = 6;
+  TileShape s = tile_shape(v);
+  for (const auto& B : Lv.geom.bl) xy_tiles += (long long)((B.nx + s.tx - 1) / s.tx) * ((B.ny + s.ty - 1) / s.ty);
+  int z = nzm;
+  while (z > 8 && xy_tiles * ((nzm + z - 1) / z) < 148 * 6) z /= 2;
+  *variant = v;
+  *zc = std::max(1, z);
+}
+
+
+// ------------------------------------------------------------------ executor
+// FP32 iterate at level g?  Mixed solves run every level but the coarsest in
+// FP32; the coarsest level (the coarse solve) stays FP64.
+bool f32_level(const h3d_mg* h, int g) { return h->mixed && !(g == h->L && h->L > 1); }
+
+struct Exec {
+  h3d_mg* h;
+  std::vector<cudaEvent_t>* prof = nullptr;  // pre-created events for level-1 sweeps
+  size_t prof_used = 0;
+
+  Level& L(int g) { return h->lev[g]; }
+
+  bool mixed_level(int g) const { return f32_level(h, g); }
+
+  int sweep(int g) {
+    Level& V = L(g);
+    cudaStream_t st = h->st;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (prof && g == 1 && prof_used + 2 <= prof->size()) {
+      e0 = (*prof)[prof_used++];
+      e1 = (*prof)[prof_used++];
+      CU(cudaEventRecord(e0, st));
+    }
+    if (mixed_level(g)) {
+      float* src = V.phi32[V.cur32];
+      float* dst = V.phi32[1 - V.cur32];
+      CU(launch_rbgs<float>(V.variant, h->var, V.zero32, V.d_bl, V.d_tiles, V.ntiles, V.zc, src, dst, V.rhs32,
+                            V.fx32, V.fy32, V.fz32, st));
+      if (e1) CU(cudaEventRecord(e1, st));
+      CU(launch_fill<float>(V.sweep.d_dst, V.sweep.d_src, V.sweep.n, dst, dst, src, V.zero32, st));
+      V.cur32 = 1 - V.cur32;
+      V.zero32 = false;
+    } else {
+      double* src = V.phi64[V.cur64];
+      double* dst = V.phi64[1 - V.cur64];
+      CU(launch_rbgs<double>(V.variant, h->var, V.zero64, V.d_bl, V.d_tiles, V.ntiles, V.zc, src, dst, V.rhs64,
+                             V.fx64, V.fy64, V.fz64, st));
+      if (e1) CU(cudaEventRecord(e1, st));
+      CU(launch_fill<double>(V.sweep.d_dst, V.sweep.d_src, V.sweep.n, dst, dst, src, V.zero64, st));
+      V.cur64 = 1 - V.cur64;
+      V.zero64 = false;
+    }
+    h->kernels += (V.sweep.n > 0) ? 2 : 1;
+    return H3D_OK;
+  }
+
+  int relax(int g, int it) {
+    for (int q = 0; q < it; ++q) TRY(sweep(g));
+    return H3D_OK;
+  }
+
+  // coarse rhs of level gc from the fine level gc-1 (mgrestr(gc))
+  int restrict_to(int gc) {
+    Level& F = L(gc - 1);
+    Level& C = L(gc);
+    CellTab ct{C.d_cta_int, (int)C.geom.bl.size(), C.ncta_int};
+    if (mixed_level(gc - 1)) {
+      // the coarsest level of a mixed solve keeps an FP32 rhs too (converted after)
+      CU(launch_restrict<float>(h->var, F.zero32, F.d_bl, C.d_bl, ct, F.phi32[F.cur32], F.rhs32, C.rhs32, F.fx32,
+                                F.fy32, F.fz32, h->st));
+      C.zero32 = true;
+      if (!mixed_level(gc)) {  // coarsest level solved in FP64
+        CU(launch_convert_f2d(C.rhs32, C.rhs64, C.geom.n_elems, h->st));
+        C.zero64 = true;
+        h->kernels += 1;
+      }
+    } else {
+      CU(launch_restrict<double>(h->var, F.zero64, F.d_bl, C.d_bl, ct, F.phi64[F.cur64], F.rhs64, C.rhs64, F.fx64,
+                                 F.fy64, F.fz64, h->st));
+      C.zero64 = true;
+    }
+    h->kernels += 1;
+    return H3D_OK;
+  }
+
+  // mgcorr(gf): correction from level gf+1 into level gf, with mgbound fused
+  int correct(int gf) {
+    Level& F = L(gf);
+    Level& C = L(gf + 1);
+    CellTab ct{F.d_cta_all, (int)F.geom.bl.size(), F.ncta_all};
+    if (mixed_level(gf)) {
+      const float* pc;
+      if (mixed_level(gf + 1)) {
+        if (C.zero32) TRY(materialize_zero32(gf + 1));
+        pc = C.phi32[C.cur32];
+      } else {  // coarsest solved in FP64: bring its iterate to FP32
+        if (C.zero64) TRY(materialize_zero64(gf + 1));
+        CU(launch_convert_d2f(C.phi64[C.cur64], C.phi32[C.cur32], C.geom.n_elems, h->st));
+        h->kernels += 1;
+        pc = C.phi32[C.cur32];
+      }
+      CU(launch_prolong<float>(F.zero32, F.d_bl, C.d_bl, ct, pc, F.phi32[F.cur32], F.phi32[1 - F.cur32], h->st));
+      F.cur32 = 1 - F.cur32;
+      F.zero32 = false;
+    } else {
+      if (C.zero64) TRY(materialize_zero64(gf + 1));
+      CU(launch_prolong<double>(F.zero64, F.d_bl, C.d_bl, ct, C.phi64[C.cur64], F.phi64[F.cur64],
+                                F.phi64[1 - F.cur64], h->st));
+      F.cur64 = 1 - F.cur64;
+      F.zero64 = false;
+    }
+    h->kernels += 1;
+    return H3D_OK;
+  }
+
+  int materialize_zero64(int g) {
+    Level& V = L(g);
+    CU(cudaMemsetAsync(V.phi64[V.cur64], 0, V.geom.n_elems * sizeof(double), h->st));
+    V.zero64 = false;
+    return H3D_OK;
+  }
+  int materialize_zero32(int g) {
+    Level& V = L(g);
+    CU(cudaMemsetAsync(V.phi32[V.cur32], 0, V.geom.n_elems * sizeof(float), h->st));
+    V.zero32 = false;
+    return H3D_OK;
+  }
+
+  // mgkcyc control flow (mgsolver.for:272-352) with kcycle = 1.
+  int vcycle() {
+    const int Lv = h->L;
+    const int irestr = h->desc.irestr, iproln = h->desc.iproln;
+    const int csw = h->desc.coarse_sweeps;
+    auto relax_at = [&](int g, int it, bool coarsest_first) -> int {
+      if (g == Lv && Lv > 1 && csw > 0) return coarsest_first ? relax(g, csw) : H3D_OK;
+      return relax(g, it);
+    };
+    if (Lv == 1) {
+      if (csw > 0) return relax(1, csw);
+      TRY(relax(1, irestr));
+      return relax(1, iproln);
+    }
+    TRY(relax(1, irestr));
+    TRY(restrict_to(2));
+    int kount[kMaxLevels + 2] = {0};
+    int g = 2, nrel = irestr;
+    for (;;) {
+      if (g == 1) break;
+      kount[g] += 1;
+      TRY(relax_at(g, nrel, true));
+      if (kount[g] == 2) {
+        TRY(correct(g - 1));
+        kount[g] = 0;
+        g -= 1;
+        nrel = iproln;
+      } else if (g < Lv) {
+        TRY(restrict_to(g + 1));
+        g += 1;
+        nrel = irestr;
+      } else {
+        TRY(relax_at(g, iproln, false));
+        TRY(correct(g - 1));
+        nrel = iproln;
+        g = Lv - 1;
+      }
+    }
+    return relax(1, iproln);
+  }
+
+  // FP64 defect on the resident p/b: e = level-1 iterate (or none).
+  int defect(bool with_e) {
+    Level& V = L(1);
+    CellTab ct{V.d_cta_all, (int)V.geom.bl.size(), V.ncta_all};
+    double rscale = h->var ? 1.0 : V.geom.bl[0].dv;
+    const double* fx = h->var ? V.fx64 : nullptr;
+    const double* fy = h->var ? V.fy64 : nullptr;
+    const double* fz = h->var ? V.fz64 : nullptr;
+    double* pin = h->p64[h->pc];
+    double* pout = h->p64[1 - h->pc];
+    if (h->mixed) {
+      const float* e = nullptr;
+      if (with_e) {
+        if (V.zero32) TRY(materialize_zero32(1));
+        e = V.phi32[V.cur32];
+      }
+      CU(launch_defect<float, float>(h->var, V.d_bl, ct, pin, e, pout, h->b64, V.rhs32, h->mean_b, rscale, fx, fy, fz,
+                                     h->partials, h->st));
+    } else {
+      const double* e = nullptr;
+      if (with_e) {
+        if (V.zero64) TRY(materialize_zero64(1));
+        e = V.phi64[V.cur64];
+      }
+      CU(launch_defect<double, double>(h->var, V.d_bl, ct, pin, e, pout, h->b64, V.rhs64, h->mean_b, rscale, fx, fy,
+                                       fz, h->partials, h->st));
+    }
+    if (with_e) h->pc = 1 - h->pc;
+    CU(launch_reduce4(h->partials, ct.ncta, h->d_res, h->st));
+    CU(cudaMemcpyAsync(h->h_res, h->d_res, 4 * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+    h->kernels += 2;
+    return H3D_OK;
+  }
+
+  // One outer iteration: V-cycle(s) on the current defect, then p += e and
+  // the new defect.
+  int iteration(int inner) {
+    Level& V = L(1);
+    if (h->mixed) V.zero32 = true;
+    else V.zero64 = true;
+    for (int q = 0; q < inner; ++q) TRY(vcycle());
+    return defect(true);
+  }
+};
+
+std::vector<int> state_key(h3d_mg* h, int tag) {
+  std::vector<int> k;
+  k.push_back(tag);
+  k.push_back(h->pc);
+  for (int g = 1; g <= h->L; ++g) {
+    k.push_back(h->lev[g].cur64);
+    k.push_back(h->lev[g].cur32);
+    k.push_back(h->lev[g].zero64);
+    k.push_back(h->lev[g].zero32);
+  }
+  return k;
+}
+
+void set_state(h3d_mg* h, const std::vector<int>& k) {
+  size_t q = 1;
+  h->pc = k[q++];
+  for (int g = 1; g <= h->L; ++g) {
+    h->lev[g].cur64 = k[q++];
+    h->lev[g].cur32 = k[q++];
+    h->lev[g].zero64 = k[q++];
+    h->lev[g].zero32 = k[q++];
+  }
+}
+
+int accumulate_events(h3d_mg* h, const std::vector<cudaEvent_t>& ev, double* ms, int64_t* n) {
+  for (size_t q = 0; q + 1 < ev.size(); q += 2) {
+    float t = 0;
+    CU(cudaEventElapsedTime(&t, ev[q], ev[q + 1]));
+    *ms += t;
+    *n += 1;
+  }
+  return H3D_OK;
+}
+
+// Events needed to bracket the level-1 sweeps of one outer iteration.
+size_t events_per_iteration(const h3d_mg* h, int inner) {
+  int sweeps1 = h->desc.irestr + h->desc.iproln;
+  if (h->L == 1 && h->desc.coarse_sweeps > 0) sweeps1 = h->desc.coarse_sweeps;
+  return 2 * (size_t)inner * (size_t)sweeps1;
+}
+
+int make_events(h3d_mg* h, std::vector<cudaEvent_t>& ev, size_t n) {
+  while (ev.size() < n) {
+    cudaEvent_t e;
+    CU(cudaEventCreate(&e));
+    ev.push_back(e);
+  }
+  return H3D_OK;
+}
+
+// Runs one outer iteration through a cached CUDA graph (captured on first use
+// for the current buffer state) or eagerly.
+int run_iteration(h3d_mg* h, int inner, double* prof_ms, int64_t* prof_n) {
+  const size_t nev = h->profiling ? events_per_iteration(h, inner) : 0;
+  if (!h->desc.use_graph) {
+    TRY(make_events(h, h->ev_eager, nev));
+    Exec ex{h, h->profiling ? &h->ev_eager : nullptr};
+    TRY(ex.iteration(inner));
+    CU(cudaStreamSynchronize(h->st));
+    std::vector<cudaEvent_t> used(h->ev_eager.begin(), h->ev_eager.begin() + ex.prof_used);
+    return accumulate_events(h, used, prof_ms, prof_n);
+  }
+  std::vector<int> key = state_key(h, inner * 2 + (h->profiling ? 1 : 0));
+  auto it = h->graphs.find(key);
+  if (it == h->graphs.end()) {
+    CachedGraph cg;
+    TRY(make_events(h, cg.events, nev));
+    Exec ex{h, h->profiling ? &cg.events : nullptr};
+    int64_t k0 = h->kernels;
+    CU(cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal));
+    int rc = ex.iteration(inner);
+    cudaGraph_t graph = nullptr;
+    cudaError_t ce = cudaStreamEndCapture(h->st, &graph);
+    if (rc != H3D_OK) {
+      if (graph) cudaGraphDestroy(graph);
+      for (auto e : cg.events) cudaEventDestroy(e);
+      return rc;
+    }
+    if (ce != cudaSuccess) return fail(h, H3D_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
+    ce = cudaGraphInstantiate(&cg.exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ce != cudaSuccess) return fail(h, H3D_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ce));
+    cg.kernels = h->kernels - k0;
+    h->kernels = k0;
+    cg.events.resize(ex.prof_used);
+    cg.state_after = state_key(h, key[0]);
+    it = h->graphs.emplace(key, cg).first;
+    set_state(h, key);
+  }
+  CU(cudaGraphLaunch(it->second.exec, h->st));
+  h->kernels += it->second.kernels;
+  set_state(h, it->second.state_after);
+  CU(cudaStreamSynchronize(h->st));
+  return accumulate_events(h, it->second.events, prof_ms, prof_n);
+}
+
+bool is_all_neumann(const h3d_mg* h) {
+  for (const auto& d : h->blocks)
+    for (int f = 0; f < 6; ++f)
+      if (d.bc[f] == 5) return false;
+  return true;
+}
+
+int copy_field_3d(h3d_mg* h, bool to_device, double* dev_base, const BlkLev& B, double* host,
+                  const h3d_block_desc& d, bool with_ghosts) {
+  // canonical (x,y,z) <-> host (pl-1+x, pl-1+y, pl-1+z)
+  const int g0 = with_ghosts ? 0 : 1;
+  const int ex = with_ghosts ? B.nx + 2 : B.nx, ey = with_ghosts ? B.ny + 2 : B.ny, ez = with_ghosts ? B.nz + 2 : B.nz;
+  cudaMemcpy3DParms p{};
+  cudaPitchedPtr dptr = make_cudaPitchedPtr(dev_base + B.off, (size_t)(B.nx + 2) * 8, B.nx + 2, B.ny + 2);
+  cudaPitchedPtr hptr = make_cudaPitchedPtr(host, (size_t)d.ttc[0] * 8, d.ttc[0], d.ttc[1]);
+  cudaPos dpos = make_cudaPos((size_t)g0 * 8, g0, g0);
+  cudaPos hpos = make_cudaPos((size_t)(d.pl - 1 + g0) * 8, d.pl - 1 + g0, d.pl - 1 + g0);
+  if (to_device) {
+    p.srcPtr = hptr; p.srcPos = hpos; p.dstPtr = dptr; p.dstPos = dpos; p.kind = cudaMemcpyHostToDevice;
+  } else {
+    p.srcPtr = dptr; p.srcPos = dpos; p.dstPtr = hptr; p.dstPos = hpos; p.kind = cudaMemcpyDeviceToHost;
+  }
+  p.extent = make_cudaExtent((size_t)ex * 8, ey, ez);
+  CU(cudaMemcpy3DAsync(&p, h->st));
+  return H3D_OK;
+}
+
+int check_block_host_dims(h3d_mg* h, const h3d_block_desc& d) {
+  if (d.pl < 1) return fail(h, H3D_ERR_ARG, "pl must be >= 1");
+  for (int a = 0; a < 3; ++a)
+    if (d.ttc[a] < d.n[a] + 2 * d.pl) return fail(h, H3D_ERR_ARG, "ttc smaller than n + 2*pl");
+  return H3D_OK;
+}
+
+int autotune_level(h3d_mg* h, int g) {
+  Level& V = h->lev[g];
+  int best_v = V.variant, best_z = V.zc;
+  if (V.geom.n_interior < (1 << 20)) return H3D_OK;  // small levels: heuristic
+  int nzm = 0, nxm = 0, nym = 0;
+  for (const auto& B : V.geom.bl) { nzm = std::max(nzm, B.nz); nxm = std::max(nxm, B.nx); nym = std::max(nym, B.ny); }
+  cudaEvent_t a, b;
+  CU(cudaEventCreate(&a));
+  CU(cudaEventCreate(&b));
+  float best = 1e30f;
+  const bool f32 = f32_level(h, g);
+  for (int v = 0; v < num_tile_shapes(); ++v) {
+    TileShape s = tile_shape(v);
+    if (s.tx > 2 * nxm || s.ty > 2 * nym || s.tx < 8) continue;
+    for (int zc : {8, 16, 32, 64, 128, 256}) {
+      if (zc > nzm) continue;
+      TRY(build_tiles(h, V, v, zc));
+      float tot = 0;
+      for (int rep = 0; rep < 4; ++rep) {
+        CU(cudaEventRecord(a, h->st));
+        if (f32) CU(launch_rbgs<float>(v, h->var, false, V.d_bl, V.d_tiles, V.ntiles, zc, V.phi32[V.cur32],
+                                       V.phi32[1 - V.cur32], V.rhs32, V.fx32, V.fy32, V.fz32, h->st));
+        else CU(launch_rbgs<double>(v, h->var, false, V.d_bl, V.d_tiles, V.ntiles, zc, V.phi64[V.cur64],
+                                    V.phi64[1 - V.cur64], V.rhs64, V.fx64, V.fy64, V.fz64, h->st));
+        CU(cudaEventRecord(b, h->st));
+        CU(cudaEventSynchronize(b));
+        float t;
+        CU(cudaEventElapsedTime(&t, a, b));
+        if (rep > 0) tot += t;
+      }
+      if (tot < best) { best = tot; best_v = v; best_z = zc; }
+    }
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  return build_tiles(h, V, best_v, best_z);
+}
+
+}  // namespace
+
+// =================================================================== C ABI
+extern "C" {
+
+const char* h3d_mg_strerror(int code) {
+  switch (code) {
+    case H3D_OK: return "ok";
+    case H3D_ERR_BAD_CONFIG: return "configuration not supported";
+    case H3D_ERR_CUDA: return "CUDA error";
+    case H3D_ERR_NOT_CONVERGED: return "not converged";
+    case H3D_ERR_DIVERGED: return "diverged";
+    case H3D_ERR_TIMEOUT: return "device wait timed out";
+    case H3D_ERR_NO_DEVICE: return "no suitable CUDA device";
+    case H3D_ERR_ARG: return "bad argument";
+    case H3D_ERR_OOM: return "out of device memory";
+    case H3D_ERR_INTERNAL: return "internal error";
+    default: return "unknown error";
+  }
+}
+
+const char* h3d_mg_last_error(const h3d_mg* h) { return h ? h->last_error.c_str() : g_create_error.c_str(); }
+
+int h3d_topology(int32_t nblocks, const int32_t* ext, const int32_t* bc, const double* hh, int32_t ngrid,
+                 h3d_block_desc* out) {
+  // read_infodom (alloc_dom.for:524-1200) on integer extents.
+  if (nblocks <= 0 || !ext || !bc || !hh || !out) return H3D_ERR_ARG;
+  auto E = [&](int b, int q) { return ext[6 * b + q]; };
+  int lo[3] = {E(0, 0), E(0, 2), E(0, 4)}, hi[3] = {E(0, 1), E(0, 3), E(0, 5)};
+  for (int b = 1; b < nblocks; ++b)
+    for (int a = 0; a < 3; ++a) {
+      lo[a] = std::min(lo[a], E(b, 2 * a));
+      hi[a] = std::max(hi[a], E(b, 2 * a + 1));
+    }
+  for (int a = 0; a < nblocks; ++a) {
+    h3d_block_desc& d = out[a];
+    std::memset(&d, 0, sizeof(d));
+    for (int q = 0; q < 3; ++q) {
+      d.n[q] = E(a, 2 * q + 1) - E(a, 2 * q);
+      d.origin[q] = E(a, 2 * q);
+      d.ttc[q] = d.n[q] + 2;
+      d.h[q] = hh[q];
+      if (d.n[q] <= 0) return H3D_ERR_ARG;
+    }
+    d.pl = 1;
+    d.ngrid = ngrid;
+    d.rdiv = 1;
+    for (int q = 0; q < 6; ++q) { d.bc[q] = bc[q]; d.nb_face[q] = -1; d.nb_periodic[q] = -1; }
+    for (int q = 0; q < 8; ++q) d.nb_corner[q] = -1;
+    for (int q = 0; q < 12; ++q) d.nb_edge[q] = -1;
+    // side s of axis q: 0 = low face of a touches high face of b; 1 = high touches low
+    auto touch = [&](int b, int q, int s) {
+      return s == 0 ? E(a, 2 * q) == E(b, 2 * q + 1) : E(a, 2 * q + 1) == E(b, 2 * q);
+    };
+    auto same = [&](int b, int q) { return E(a, 2 * q) == E(b, 2 * q) && E(a, 2 * q + 1) == E(b, 2 * q + 1); };
+    int cnt[26] = {0};
+    for (int b = 0; b < nblocks; ++b) {
+      if (b == a) continue;
+      for (int q = 0; q < 3; ++q)
+        for (int s = 0; s < 2; ++s) {
+          int o1 = (q + 1) % 3, o2 = (q + 2) % 3;
+          if (touch(b, q, s) && same(b, o1) && same(b, o2)) { d.nb_face[2 * q + s] = b; cnt[2 * q + s]++; }
+        }
+      // corners: prev #1..4 at z-, next #1..4 at z+ (x,y sides per alloc_dom.for:700-810)
+      static const int csx[8] = {0, 0, 1, 1, 1, 1, 0, 0}, csy[8] = {0, 1, 1, 0, 1, 0, 0, 1},
+                       csz[8] = {0, 0, 0, 0, 1, 1, 1, 1};
+      for (int c = 0; c < 8; ++c)
+        if (touch(b, 0, csx[c]) && touch(b, 1, csy[c]) && touch(b, 2, csz[c])) { d.nb_corner[c] = b; cnt[6 + c]++; }
+      // edges: (axis pair, sides, running axis) per alloc_dom.for:824-1040
+      static const int ea1[12] = {0, 1, 0, 1, 0, 0, 0, 1, 0, 1, 0, 0};
+      static const int es1[12] = {0, 1, 1, 0, 0, 0, 1, 0, 0, 1, 1, 1};
+      static const int ea2[12] = {2, 2, 2, 2, 1, 1, 2, 2, 2, 2, 1, 1};
+      static const int es2[12] = {0, 0, 0, 0, 0, 1, 1, 1, 1, 1, 1, 0};
+      static const int erun[12] = {1, 0, 1, 0, 2, 2, 1, 0, 1, 0, 2, 2};
+      for (int e = 0; e < 12; ++e)
+        if (touch(b, ea1[e], es1[e]) && touch(b, ea2[e], es2[e]) && same(b, erun[e])) {
+          d.nb_edge[e] = b;
+          cnt[14 + e]++;
+        }
+    }
+    for (int q = 0; q < 26; ++q)
+      if (cnt[q] > 1) return H3D_ERR_BAD_CONFIG;
+  }
+  // periodic partners (alloc_dom.for:1042-1200)
+  for (int a = 0; a < nblocks; ++a) {
+    h3d_block_desc& d = out[a];
+    for (int b = 0; b < nblocks; ++b) {
+      if (b == a) continue;
+      for (int q = 0; q < 3; ++q) {
+        int o1 = (q + 1) % 3, o2 = (q + 2) % 3;
+        bool so = E(a, 2 * o1) == E(b, 2 * o1) && E(a, 2 * o1 + 1) == E(b, 2 * o1 + 1) &&
+                  E(a, 2 * o2) == E(b, 2 * o2) && E(a, 2 * o2 + 1) == E(b, 2 * o2 + 1);
+        if (!so) continue;
+        if (bc[2 * q] == 5 && d.nb_face[2 * q] < 0 && E(b, 2 * q + 1) == hi[q]) d.nb_periodic[2 * q] = b;
+        if (bc[2 * q + 1] == 5 && d.nb_face[2 * q + 1] < 0 && E(b, 2 * q) == lo[q]) d.nb_periodic[2 * q + 1] = b;
+      }
+    }
+  }
+  return H3D_OK;
+}
+
+int h3d_mg_destroy(h3d_mg* h) {
+  if (!h) return H3D_OK;
+  cudaSetDevice(h->device);
+  if (h->st) cudaStreamSynchronize(h->st);
+  for (auto& kv : h->graphs) {
+    if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+    for (auto e : kv.second.events) cudaEventDestroy(e);
+  }
+  for (auto e : h->ev_eager) cudaEventDestroy(e);
+  for (size_t g = 1; g < h->lev.size(); ++g) {
+    Level& V = h->lev[g];
+    void* ps[] = {V.d_bl, V.d_cta_all, V.d_cta_int, V.d_tiles, V.phi64[0], V.phi64[1], V.rhs64, V.phi32[0],
+                  V.phi32[1], V.rhs32, V.fx64, V.fy64, V.fz64, V.fx32, V.fy32, V.fz32, V.dens,
+                  V.sweep.d_dst, V.sweep.d_src, V.faces.d_dst, V.faces.d_src, V.exch.d_dst, V.exch.d_src,
+                  V.bound.d_dst, V.bound.d_src};
+    for (void* p : ps) dfree(p);
+  }
+  dfree(h->p64[0]);
+  dfree(h->p64[1]);
+  dfree(h->b64);
+  dfree(h->partials);
+  dfree(h->d_res);
+  dfree(h->d_h3);
+  if (h->h_res) cudaFreeHost(h->h_res);
+  if (h->st) cudaStreamDestroy(h->st);
+  delete h;
+  return H3D_OK;
+}
+
+int h3d_mg_create(h3d_mg** out, const h3d_mg_desc* desc) {
+  h3d_mg* h = nullptr;
+  if (!out || !desc || !desc->blocks || desc->nblocks <= 0) return fail(nullptr, H3D_ERR_ARG, "null descriptor");
+  *out = nullptr;
+  const h3d_mg_desc& D = *desc;
+  if (D.ngrd_gl < 1 || D.ngrd_gl > kMaxLevels) return fail(nullptr, H3D_ERR_BAD_CONFIG, "ngrd_gl out of range");
+  if (D.mg_itrsch != 3)
+    return fail(nullptr, H3D_ERR_BAD_CONFIG, "only mg_itrsch=3 (red-black Gauss-Seidel) runs on the GPU");
+  if (D.irestr < 0 || D.iproln < 0 || D.irestr + D.iproln < 1)
+    return fail(nullptr, H3D_ERR_BAD_CONFIG, "irestr/iproln must be >= 0 with at least one sweep");
+  if (D.precision != H3D_PREC_FP64 && D.precision != H3D_PREC_MIXED)
+    return fail(nullptr, H3D_ERR_BAD_CONFIG, "unknown precision");
+  for (int b = 0; b < D.nblocks; ++b) {
+    const h3d_block_desc& d = D.blocks[b];
+    if (d.ngrid != D.ngrd_gl) return fail(nullptr, H3D_ERR_BAD_CONFIG, "every block needs ngrid == ngrd_gl");
+    if (d.rdiv != 1) return fail(nullptr, H3D_ERR_BAD_CONFIG, "local mesh refinement (rdiv > 1) is not supported");
+    int pow2 = 1 << (d.ngrid - 1);
+    for (int a = 0; a < 3; ++a)
+      if (d.n[a] <= 0 || d.n[a] % pow2 != 0)  // localparameters.for:204-209
+        return fail(nullptr, H3D_ERR_BAD_CONFIG, "block size not divisible by 2**(ngrid-1)");
+    for (int f = 0; f < 6; ++f) {
+      if (d.nb_face[f] >= D.nblocks || d.nb_periodic[f] >= D.nblocks)
+        return fail(nullptr, H3D_ERR_BAD_CONFIG, "neighbour id out of range");
+    }
+  }
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= D.device || D.device < 0)
+    return fail(nullptr, H3D_ERR_NO_DEVICE, "no CUDA device");
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, D.device) != cudaSuccess || prop.major != 10)
+    return fail(nullptr, H3D_ERR_NO_DEVICE, "this library is built for sm_100a (B200)");
+
+  h = new h3d_mg();
+  h->device = D.device;
+  h->desc = D;
+  h->blocks.assign(D.blocks, D.blocks + D.nblocks);
+  h->desc.blocks = nullptr;
+  if (h->desc.maxcy <= 0) h->desc.maxcy = 30;  // control.cin default
+  if (h->desc.inner_cycles <= 0) h->desc.inner_cycles = 2;
+  h->L = D.ngrd_gl;
+  h->mixed = D.precision == H3D_PREC_MIXED;
+  h->var = D.var_coef != 0;
+  int rc = H3D_OK;
+  auto bail = [&](int r) {
+    g_create_error = h->last_error;
+    h3d_mg_destroy(h);
+    return r;
+  };
+  if (cudaSetDevice(h->device) != cudaSuccess) return bail(fail(h, H3D_ERR_NO_DEVICE, "cudaSetDevice failed"));
+  if (cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking) != cudaSuccess)
+    return bail(fail(h, H3D_ERR_CUDA, "stream create failed"));
+  h->lev.resize(h->L + 1);
+  for (int g = 1; g <= h->L; ++g) {
+    Level& V = h->lev[g];
+    V.geom = make_level_geom(h->blocks, g);
+    if ((rc = dalloc(h, &V.d_bl, V.geom.bl.size())) != H3D_OK) return bail(rc);
+    if (cudaMemcpy(V.d_bl, V.geom.bl.data(), V.geom.bl.size() * sizeof(BlkLev), cudaMemcpyHostToDevice) != cudaSuccess)
+      return bail(fail(h, H3D_ERR_CUDA, "copy level geometry"));
+    if ((rc = build_cta_table(h, V.geom, false, &V.d_cta_all, &V.ncta_all)) != H3D_OK) return bail(rc);
+    if ((rc = build_cta_table(h, V.geom, true, &V.d_cta_int, &V.ncta_int)) != H3D_OK) return bail(rc);
+    int var_, zc;
+    default_tile(V, &var_, &zc);
+    if ((rc = build_tiles(h, V, var_, zc)) != H3D_OK) return bail(rc);
+    const size_t n = (size_t)V.geom.n_elems;
+    const bool need64 = !f32_level(h, g);
+    const bool need32 = h->mixed;
+    if (need64) {
+      if ((rc = dalloc(h, &V.phi64[0], n)) || (rc = dalloc(h, &V.phi64[1], n)) || (rc = dalloc(h, &V.rhs64, n)))
+        return bail(rc);
+    }
+    if (need32) {
+      if ((rc = dalloc(h, &V.phi32[0], n)) || (rc = dalloc(h, &V.phi32[1], n)) || (rc = dalloc(h, &V.rhs32, n)))
+        return bail(rc);
+    }
+    if (h->var) {
+      if ((rc = dalloc(h, &V.dens, n)) || (rc = dalloc(h, &V.fx64, n)) || (rc = dalloc(h, &V.fy64, n)) ||
+          (rc = dalloc(h, &V.fz64, n)))
+        return bail(rc);
+      if (h->mixed && ((rc = dalloc(h, &V.fx32, n)) || (rc = dalloc(h, &V.fy32, n)) || (rc = dalloc(h, &V.fz32, n))))
+        return bail(rc);
+      // density defaults to 1 (set_density overrides)
+      std::vector<double> ones(n, 1.0);
+      if (cudaMemcpy(V.dens, ones.data(), n * 8, cudaMemcpyHostToDevice) != cudaSuccess)
+        return bail(fail(h, H3D_ERR_CUDA, "density init"));
+    }
+    std::vector<uint32_t> d, s;
+    std::string err;
+    if ((rc = build_halo_table(h->blocks, g, kHaloSweep, d, s, &err)) != H3D_OK) return bail(fail(h, rc, err));
+    if ((rc = upload_halo(h, V.sweep, d, s)) != H3D_OK) return bail(rc);
+    if (g == 1) {
+      if ((rc = build_halo_table(h->blocks, g, kHaloFaces, d, s, &err)) != H3D_OK) return bail(fail(h, rc, err));
+      if ((rc = upload_halo(h, V.faces, d, s)) != H3D_OK) return bail(rc);
+    }
+    // bytes of one sweep: read phi + rhs, write phi (+3 face arrays when variable)
+    double w = f32_level(h, g) ? 4.0 : 8.0;
+    V.sweep_bytes = (double)V.geom.n_interior * w * (3.0 + (h->var ? 3.0 : 0.0));
+  }
+  const size_t n1 = (size_t)h->lev[1].geom.n_elems;
+  if ((rc = dalloc(h, &h->p64[0], n1)) || (rc = dalloc(h, &h->p64[1], n1)) || (rc = dalloc(h, &h->b64, n1)))
+    return bail(rc);
+  h->npartials = std::max(h->lev[1].ncta_all, h->lev[1].ncta_int);
+  if ((rc = dalloc(h, &h->partials, 4 * (size_t)h->npartials)) || (rc = dalloc(h, &h->d_res, 4))) return bail(rc);
+  if (cudaMallocHost((void**)&h->h_res, 4 * sizeof(double)) != cudaSuccess)
+    return bail(fail(h, H3D_ERR_OOM, "pinned result buffer"));
+  std::vector<double> h3;
+  for (const auto& d : h->blocks) { h3.push_back(d.h[0]); h3.push_back(d.h[1]); h3.push_back(d.h[2]); }
+  if ((rc = dalloc(h, &h->d_h3, h3.size())) != H3D_OK) return bail(rc);
+  if (cudaMemcpy(h->d_h3, h3.data(), h3.size() * 8, cudaMemcpyHostToDevice) != cudaSuccess)
+    return bail(fail(h, H3D_ERR_CUDA, "copy spacings"));
+  if (cudaStreamSynchronize(h->st) != cudaSuccess) return bail(fail(h, H3D_ERR_CUDA, "set-up sync"));
+  if (!h->var) h->coeffs_ready = true;
+  *out = h;
+  return H3D_OK;
+}
+
+int h3d_mg_set_density(h3d_mg* h, int32_t ib, const double* dens) {
+  if (!h || !dens || ib < 0 || ib >= (int)h->blocks.size()) return H3D_ERR_ARG;
+  if (!h->var) return fail(h, H3D_ERR_ARG, "handle was created with var_coef = 0");
+  TRY(check_block_host_dims(h, h->blocks[ib]));
+  CU(cudaSetDevice(h->device));
+  TRY(copy_field_3d(h, true, h->lev[1].dens, h->lev[1].geom.bl[ib], const_cast<double*>(dens), h->blocks[ib], false));
+  CU(cudaStreamSynchronize(h->st));
+  h->coeffs_ready = false;
+  return H3D_OK;
+}
+
+int h3d_mg_coeff(h3d_mg* h) {
+  if (!h) return H3D_ERR_ARG;
+  CU(cudaSetDevice(h->device));
+  if (h->var) {
+    for (int g = 1; g <= h->L; ++g) {
+      Level& V = h->lev[g];
+      if (g > 1) {
+        Level& F = h->lev[g - 1];
+        CellTab ct{V.d_cta_int, (int)V.geom.bl.size(), V.ncta_int};
+        CU(launch_dens_restrict(F.d_bl, V.d_bl, ct, F.dens, V.dens, h->st));
+      }
+      CellTab ca{V.d_cta_all, (int)V.geom.bl.size(), V.ncta_all};
+      CU(launch_face_coef(V.d_bl, ca, V.dens, h->d_h3, V.fx64, V.fy64, V.fz64, h->st));
+      if (h->mixed) {
+        CU(launch_convert_d2f(V.fx64, V.fx32, V.geom.n_elems, h->st));
+        CU(launch_convert_d2f(V.fy64, V.fy32, V.geom.n_elems, h->st));
+        CU(launch_convert_d2f(V.fz64, V.fz32, V.geom.n_elems, h->st));
+      }
+    }
+    CU(cudaStreamSynchronize(h->st));
+  }
+  // autotune the smoother tiles of the large levels once coefficients exist
+  for (int g = 1; g <= h->L; ++g) TRY(autotune_level(h, g));
+  CU(cudaStreamSynchronize(h->st));
+  h->coeffs_ready = true;
+  return H3D_OK;
+}
+
+static int ensure_coeffs(h3d_mg* h) {
+  if (!h->coeffs_ready) return h3d_mg_coeff(h);
+  return H3D_OK;
+}
+
+int h3d_mg_upload(h3d_mg* h, int32_t field, int32_t ib, const double* host) {
+  if (!h || !host || ib < 0 || ib >= (int)h->blocks.size()) return H3D_ERR_ARG;
+  TRY(check_block_host_dims(h, h->blocks[ib]));
+  CU(cudaSetDevice(h->device));
+  const BlkLev& B = h->lev[1].geom.bl[ib];
+  if (field == H3D_FIELD_P) TRY(copy_field_3d(h, true, h->p64[h->pc], B, const_cast<double*>(host), h->blocks[ib], true));
+  else if (field == H3D_FIELD_B) TRY(copy_field_3d(h, true, h->b64, B, const_cast<double*>(host), h->blocks[ib], false));
+  else return H3D_ERR_ARG;
+  return H3D_OK;
+}
+
+int h3d_mg_download(h3d_mg* h, int32_t field, int32_t ib, double* host) {
+  if (!h || !host || ib < 0 || ib >= (int)h->blocks.size()) return H3D_ERR_ARG;
+  TRY(check_block_host_dims(h, h->blocks[ib]));
+  CU(cudaSetDevice(h->device));
+  const BlkLev& B = h->lev[1].geom.bl[ib];
+  if (field == H3D_FIELD_P) TRY(copy_field_3d(h, false, h->p64[h->pc], B, host, h->blocks[ib], true));
+  else if (field == H3D_FIELD_B) TRY(copy_field_3d(h, false, h->b64, B, host, h->blocks[ib], false));
+  else return H3D_ERR_ARG;
+  CU(cudaStreamSynchronize(h->st));
+  return H3D_OK;
+}
+
+int h3d_mg_zero_field(h3d_mg* h, int32_t field) {
+  if (!h || (field != H3D_FIELD_P && field != H3D_FIELD_B)) return H3D_ERR_ARG;
+  CU(cudaSetDevice(h->device));
+  double* a = field == H3D_FIELD_P ? h->p64[h->pc] : h->b64;
+  CU(cudaMemsetAsync(a, 0, (size_t)h->lev[1].geom.n_elems * sizeof(double), h->st));
+  CU(cudaStreamSynchronize(h->st));
+  return H3D_OK;
+}
+
+int h3d_mg_residual(h3d_mg* h, double* rr, double* bb, double* rinf) {
+  if (!h) return H3D_ERR_ARG;
+  CU(cudaSetDevice(h->device));
+  TRY(ensure_coeffs(h));
+  Level& V = h->lev[1];
+  CU(launch_fill<double>(V.faces.d_dst, V.faces.d_src, V.faces.n, h->p64[h->pc], h->p64[h->pc], h->p64[h->pc],
+                         false, h->st));
+  Exec ex{h};
+  double save = h->mean_b;
+  h->mean_b = 0.0;
+  int rc = ex.defect(false);
+  h->mean_b = save;
+  TRY(rc);
+  CU(cudaStreamSynchronize(h->st));
+  if (rr) *rr = h->h_res[0];
+  if (bb) *bb = h->h_res[1];
+  if (rinf) *rinf = h->h_res[2];
+  return H3D_OK;
+}
+
+int h3d_mg_solve_resident(h3d_mg* h, const h3d_solve_opts* opts, h3d_solve_info* info) {
+  if (!h || !opts) return H3D_ERR_ARG;
+  CU(cudaSetDevice(h->device));
+  TRY(ensure_coeffs(h));
+  h3d_solve_info I{};
+  const int maxcy = opts->maxcy > 0 ? opts->maxcy : h->desc.maxcy;
+  const int inner = h->mixed ? h->desc.inner_cycles : 1;
+  h->history.clear();
+  cudaEvent_t t0, t1;
+  CU(cudaEventCreate(&t0));
+  CU(cudaEventCreate(&t1));
+  int64_t k0 = h->kernels;
+  CU(cudaEventRecord(t0, h->st));
+  Level& V = h->lev[1];
+  // pressure halo (exchange(4) + pbound, newsolv_mg.for:51-52)
+  CU(launch_fill<double>(V.faces.d_dst, V.faces.d_src, V.faces.n, h->p64[h->pc], h->p64[h->pc], h->p64[h->pc],
+                         false, h->st));
+  h->kernels += 1;
+  Exec ex{h};
+  h->mean_b = 0.0;
+  if (h->mixed && is_all_neumann(h)) {
+    // FP64 null-space handling: the compatible part of b has zero mean; the
+    // FP32 cycles see the defect with the mean of b removed.
+    CellTab ct{V.d_cta_int, (int)V.geom.bl.size(), V.ncta_int};
+    CU(launch_sum_interior(V.d_bl, ct, h->b64, h->partials, h->st));
+    CU(launch_reduce4(h->partials, ct.ncta, h->d_res, h->st));
+    CU(cudaMemcpyAsync(h->h_res, h->d_res, 4 * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+    CU(cudaStreamSynchronize(h->st));
+    h->mean_b = h->h_res[0] / (double)V.geom.n_interior;
+    h->kernels += 2;
+  }
+  TRY(ex.defect(false));
+  CU(cudaStreamSynchronize(h->st));
+  double bb = h->h_res[1];
+  I.bnorm = std::sqrt(bb);
+  const double bn = I.bnorm > 0 ? I.bnorm : 1.0;
+  double rel = std::sqrt(h->h_res[0]) / bn, rinf = h->h_res[2];
+  if (opts->record_history) h->history.push_back(rel);
+  int status = 1, iter = 0;
+  if (opts->stop_rule == 0 && rel <= opts->tol) status = 0;
+  double prof_ms = 0;
+  int64_t prof_n = 0;
+  while (status != 0 && iter < maxcy) {
+    TRY(run_iteration(h, inner, &prof_ms, &prof_n));
+    iter += 1;
+    I.cycles += inner;
+    rel = std::sqrt(h->h_res[0]) / bn;
+    rinf = h->h_res[2];
+    if (opts->record_history) h->history.push_back(rel);
+    if (!std::isfinite(rel) || rel > 1e8) { status = 2; break; }
+    if (opts->stop_rule == 0 && rel <= opts->tol) status = 0;
+    if (opts->stop_rule == 1 && rinf < opts->tol && iter > 1) status = 0;  // newsolv_mg.for:57
+  }
+  if (opts->remove_mean) {
+    CellTab ct{V.d_cta_int, (int)V.geom.bl.size(), V.ncta_int};
+    CU(launch_sum_interior(V.d_bl, ct, h->p64[h->pc], h->partials, h->st));
+    CU(launch_reduce4(h->partials, ct.ncta, h->d_res, h->st));
+    CU(launch_shift(h->p64[h->pc], V.geom.n_elems, h->d_res, 1.0 / (double)V.geom.n_interior, h->st));
+    h->kernels += 3;
+  }
+  CU(cudaEventRecord(t1, h->st));
+  CU(cudaEventSynchronize(t1));
+  float ms = 0;
+  CU(cudaEventElapsedTime(&ms, t0, t1));
+  cudaEventDestroy(t0);
+  cudaEventDestroy(t1);
+  I.outer = iter;
+  I.relres = rel;
+  I.rmax = rinf;
+  I.device_ms = ms;
+  I.smoother_ms = prof_ms;
+  I.smoother_launches = prof_n;
+  I.kernel_launches = h->kernels - k0;
+  if (info) *info = I;
+  if (status == 2) return fail(h, H3D_ERR_DIVERGED, "residual is not finite or grew beyond 1e8");
+  if (status != 0) return fail(h, H3D_ERR_NOT_CONVERGED, "not converged within maxcy cycles");
+  return H3D_OK;
+}
+
+int h3d_mg_newsolv(h3d_mg* h, double* const* p, const double* const* b, const h3d_solve_opts* opts,
+                   h3d_solve_info* info) {
+  if (!h || !p || !b || !opts) return H3D_ERR_ARG;
+  for (int ib = 0; ib < (int)h->blocks.size(); ++ib) {
+    TRY(h3d_mg_upload(h, H3D_FIELD_P, ib, p[ib]));
+    TRY(h3d_mg_upload(h, H3D_FIELD_B, ib, b[ib]));
+  }
+  int rc = h3d_mg_solve_resident(h, opts, info);
+  if (rc != H3D_OK && rc != H3D_ERR_NOT_CONVERGED) return rc;
+  for (int ib = 0; ib < (int)h->blocks.size(); ++ib) {
+    const BlkLev& B = h->lev[1].geom.bl[ib];
+    TRY(copy_field_3d(h, false, h->p64[h->pc], B, p[ib], h->blocks[ib], true));
+  }
+  CU(cudaStreamSynchronize(h->st));
+  return rc;
+}
+
+int h3d_mg_history(h3d_mg* h, double* out, int32_t cap, int32_t* n) {
+  if (!h || !n) return H3D_ERR_ARG;
+  int k = (int)std::min<size_t>(h->history.size(), (size_t)std::max(cap, 0));
+  if (out)
+    for (int q = 0; q < k; ++q) out[q] = h->history[q];
+  *n = (int)h->history.size();
+  return H3D_OK;
+}
+
+// ---------------------------------------------------------- level hooks
+static int level_ok(h3d_mg* h, int g) { return h && g >= 1 && g <= h->L; }
+
+int h3d_mg_put_level(h3d_mg* h, int32_t g, int32_t field, int32_t ib, const double* a) {
+  if (!level_ok(h, g) || !a || ib < 0 || ib >= (int)h->blocks.size() || field < 0 || field > 1) return H3D_ERR_ARG;
+  CU(cudaSetDevice(h->device));
+  Level& V = h->lev[g];
+  const BlkLev& B = V.geom.bl[ib];
+  const size_t nb = (size_t)(B.nx + 2) * (B.ny + 2) * (B.nz + 2);
+  std::vector<double> buf(nb, 0.0);
+  if (field == 0) {
+    std::memcpy(buf.data(), a, nb * 8);
+  } else {
+    for (int z = 1; z <= B.nz; ++z)
+      for (int y = 1; y <= B.ny; ++y)
+        for (int x = 1; x <= B.nx; ++x)
+          buf[((size_t)z * (B.ny + 2) + y) * (B.nx + 2) + x] = a[((size_t)(z - 1) * B.ny + (y - 1)) * B.nx + (x - 1)];
+  }
+  const bool f32 = f32_level(h, g);
+  if (f32) {
+    std::vector<float> fb(buf.begin(), buf.end());
+    float* dst = field == 0 ? V.phi32[V.cur32] + B.off : V.rhs32 + B.off;
+    if (field == 1) {  // keep the existing ghost entries of the rhs untouched: copy interior rows only
+      for (int z = 1; z <= B.nz; ++z)
+        CU(cudaMemcpy(dst + (size_t)z * B.sxy, fb.data() + (size_t)z * B.sxy, B.sxy * 4, cudaMemcpyHostToDevice));
+    } else {
+      CU(cudaMemcpy(dst, fb.data(), nb * 4, cudaMemcpyHostToDevice));
+      V.zero32 = false;
+    }
+  } else {
+    double* dst = field == 0 ? V.phi64[V.cur64] + B.off : V.rhs64 + B.off;
+    CU(cudaMemcpy(dst, buf.data(), nb * 8, cudaMemcpyHostToDevice));
+    if (field == 0) V.zero64 = false;
+  }
+  return H3D_OK;
+}
+
+int h3d_mg_get_level(h3d_mg* h, int32_t g, int32_t field, int32_t ib, double* a) {
+  if (!level_ok(h, g) || !a || ib < 0 || ib >= (int)h->blocks.size() || field < 0 || field > 1) return H3D_ERR_ARG;
+  CU(cudaSetDevice(h->device));
+  CU(cudaStreamSynchronize(h->st));
+  Level& V = h->lev[g];
+  const BlkLev& B = V.geom.bl[ib];
+  const size_t nb = (size_t)(B.nx + 2) * (B.ny + 2) * (B.nz + 2);
+  std::vector<double> buf(nb, 0.0);
+  const bool f32 = f32_level(h, g);
+  bool zero = f32 ? V.zero32 : V.zero64;
+  if (!(field == 0 && zero)) {
+    if (f32) {
+      std::vector<float> fb(nb);
+      const float* src = field == 0 ? V.phi32[V.cur32] + B.off : V.rhs32 + B.off;
+      CU(cudaMemcpy(fb.data(), src, nb * 4, cudaMemcpyDeviceToHost));
+      for (size_t q = 0; q < nb; ++q) buf[q] = fb[q];
+    } else {
+      const double* src = field == 0 ? V.phi64[V.cur64] + B.off : V.rhs64 + B.off;
+      CU(cudaMemcpy(buf.data(), src, nb * 8, cudaMemcpyDeviceToHost));
+    }
+  }
+  if (field == 0) {
+    std::memcpy(a, buf.data(), nb * 8);
+  } else {
+    for (int z = 1; z <= B.nz; ++z)
+      for (int y = 1; y <= B.ny; ++y)
+        for (int x = 1; x <= B.nx; ++x)
+          a[((size_t)(z - 1) * B.ny + (y - 1)) * B.nx + (x - 1)] = buf[((size_t)z * (B.ny + 2) + y) * (B.nx + 2) + x];
+  }
+  return H3D_OK;
+}
+
+int h3d_mg_mgrelax(h3d_mg* h, int32_t g, int32_t it) {
+  if (!level_ok(h, g) || it < 0) return H3D_ERR_ARG;
+  CU(cudaSetDevice(h->device));
+  TRY(ensure_coeffs(h));
+  Exec ex{h};
+  TRY(ex.relax(g, it));
+  CU(cudaStreamSynchronize(h->st));
+  return H3D_OK;
+}
+
+int h3d_mg_mgrestr(h3d_mg* h, int32_t g) {
+  if (!level_ok(h, g) || g < 2) return H3D_ERR_ARG;
+  CU(cudaSetDevice(h->device));
+  TRY(ensure_coeffs(h));
+  Exec ex{h};
+  TRY(ex.restrict_to(g));
+  // the reference zeroes the coarse iterate including ghosts (mgsolver.for:655-662)
+  Level& C = h->lev[g];
+  if (C.zero64 && C.phi64[0]) TRY(ex.materialize_zero64(g));
+  if (C.zero32 && C.phi32[0]) TRY(ex.materialize_zero32(g));
+  CU(cudaStreamSynchronize(h->st));
+  return H3D_OK;
+}
+
+int h3d_mg_mgcorr(h3d_mg* h, int32_t g) {
+  if (!level_ok(h, g) || g >= h->L) return H3D_ERR_ARG;
+  CU(cudaSetDevice(h->device));
+  Exec ex{h};
+  TRY(ex.correct(g));
+  CU(cudaStreamSynchronize(h->st));
+  return H3D_OK;
+}
+
+// Applies a halo table of `kind` out of place on the current iterate of level g.
+static int apply_table_hook(h3d_mg* h, int g, int kind) {
+  CU(cudaSetDevice(h->device));
+  Level& V = h->lev[g];
+  Halo* H = kind == kHaloExchange ? &V.exch : &V.bound;
+  if (!H->d_dst && !H->d_src) {
+    std::vector<uint32_t> d, s;
+    std::string err;
+    int rc = build_halo_table(h->blocks, g, kind, d, s, &err);
+    if (rc != H3D_OK) return fail(h, rc, err);
+    TRY(upload_halo(h, *H, d, s));
+    if (H->n == 0) { H->d_dst = reinterpret_cast<uint32_t*>(1); }  // mark built (empty)
+  }
+  const bool f32 = f32_level(h, g);
+  const size_t n = (size_t)V.geom.n_elems;
+  if (f32) {
+    if (V.zero32) { Exec ex{h}; TRY(ex.materialize_zero32(g)); }
+    float* cur = V.phi32[V.cur32];
+    float* nxt = V.phi32[1 - V.cur32];
+    CU(cudaMemcpyAsync(nxt, cur, n * 4, cudaMemcpyDeviceToDevice, h->st));
+    if (H->n > 0) CU(launch_fill<float>(H->d_dst, H->d_src, H->n, nxt, cur, cur, false, h->st));
+    V.cur32 = 1 - V.cur32;
+  } else {
+    if (V.zero64) { Exec ex{h}; TRY(ex.materialize_zero64(g)); }
+    double* cur = V.phi64[V.cur64];
+    double* nxt = V.phi64[1 - V.cur64];
+    CU(cudaMemcpyAsync(nxt, cur, n * 8, cudaMemcpyDeviceToDevice, h->st));
+    if (H->n > 0) CU(launch_fill<double>(H->d_dst, H->d_src, H->n, nxt, cur, cur, false, h->st));
+    V.cur64 = 1 - V.cur64;
+  }
+  CU(cudaStreamSynchronize(h->st));
+  return H3D_OK;
+}
+
+int h3d_mg_mgbound(h3d_mg* h, int32_t g) {
+  if (!level_ok(h, g)) return H3D_ERR_ARG;
+  return apply_table_hook(h, g, kHaloBound);
+}
+
+int h3d_mg_exchangepp(h3d_mg* h, int32_t g) {
+  if (!level_ok(h, g)) return H3D_ERR_ARG;
+  return apply_table_hook(h, g, kHaloExchange);
+}
+
+int h3d_mg_vcycle(h3d_mg* h) {
+  if (!h) return H3D_ERR_ARG;
+  CU(cudaSetDevice(h->device));
+  TRY(ensure_coeffs(h));
+  Exec ex{h};
+  TRY(ex.vcycle());
+  CU(cudaStreamSynchronize(h->st));
+  return H3D_OK;
+}
+
+int h3d_mg_mgkcyc(h3d_mg* h, double* const* pp, const double* const* su) {
+  if (!h || !pp || !su) return H3D_ERR_ARG;
+  CU(cudaSetDevice(h->device));
+  TRY(ensure_coeffs(h));
+  Level& V = h->lev[1];
+  // pp (incl. one ghost layer) -> level-1 iterate, su -> level-1 rhs (mgsolver.for:239-266)
+  for (int ib = 0; ib < (int)h->blocks.size(); ++ib) {
+    TRY(check_block_host_dims(h, h->blocks[ib]));
+    const BlkLev& B = V.geom.bl[ib];
+    if (h->mixed) {
+      TRY(copy_field_3d(h, true, h->p64[1 - h->pc], B, pp[ib], h->blocks[ib], true));
+      TRY(copy_field_3d(h, true, h->b64, B, const_cast<double*>(su[ib]), h->blocks[ib], false));
+    } else {
+      TRY(copy_field_3d(h, true, V.phi64[V.cur64], B, pp[ib], h->blocks[ib], true));
+      TRY(copy_field_3d(h, true, V.rhs64, B, const_cast<double*>(su[ib]), h->blocks[ib], false));
+    }
+  }
+  if (h->mixed) {
+    CU(launch_convert_d2f(h->p64[1 - h->pc], V.phi32[V.cur32], V.geom.n_elems, h->st));
+    CU(launch_convert_d2f(h->b64, V.rhs32, V.geom.n_elems, h->st));
+    V.zero32 = false;
+  } else {
+    V.zero64 = false;
+  }
+  Exec ex{h};
+  TRY(ex.vcycle());
+  if (h->mixed) CU(launch_convert_f2d(V.phi32[V.cur32], h->p64[1 - h->pc], V.geom.n_elems, h->st));
+  for (int ib = 0; ib < (int)h->blocks.size(); ++ib) {
+    const BlkLev& B = V.geom.bl[ib];
+    TRY(copy_field_3d(h, false, h->mixed ? h->p64[1 - h->pc] : V.phi64[V.cur64], B, pp[ib], h->blocks[ib], true));
+  }
+  CU(cudaStreamSynchronize(h->st));
+  return H3D_OK;
+}
+
+int h3d_mg_sync(h3d_mg* h) {
+  if (!h) return H3D_ERR_ARG;
+  CU(cudaSetDevice(h->device));
+  CU(cudaStreamSynchronize(h->st));
+  return H3D_OK;
+}
+
+int h3d_mg_set_profiling(h3d_mg* h, int32_t on) {
+  if (!h) return H3D_ERR_ARG;
+  h->profiling = on != 0;
+  return H3D_OK;
+}
+
+int h3d_mg_smoother_bytes(h3d_mg* h, double* bytes) {
+  if (!h || !bytes) return H3D_ERR_ARG;
+  *bytes = h->lev[1].sweep_bytes;
+  return H3D_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,238 @@
+"""Host-side mirror of the reference's multigrid pressure interface.
+
+`MultigridSolver` keeps the subroutine names of Hydro3D v7.0's multigrid path
+and their argument meaning:
+
+    coeff()                        mgsolver.for:2-224
+    mgkcyc(pp, su)                 mgsolver.for:226-372   (one V-cycle)
+    newsolv_mg(p, b, ...)          newsolv_mg.for:2-93    (outer defect correction)
+    mgrelax(g, it) / mgrestr(g) / mgcorr(g) / mgbound(g) / exchangepp(g)
+                                   mgsolver.for:374-997, exchangepp.for:2-2835
+
+Host fields are numpy float64 arrays laid out like the Fortran `dom(ib)` arrays:
+shape (ttc_k, ttc_j, ttc_i) in C order == Fortran (ttc_i, ttc_j, ttc_k), with
+`pl` ghost layers.  Every call goes through the C ABI of libh3dmg.so; there is
+no CPU code path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import List, Optional, Sequence
+
+import numpy as np
+
+from . import _lib
+from ._lib import H3DError, check
+
+
+def host_field(d) -> np.ndarray:
+    """A zero host field for block descriptor d (Fortran dims ttc, pl ghosts)."""
+    return np.zeros((d.ttc[2], d.ttc[1], d.ttc[0]))
+
+
+def interior(a: np.ndarray, d) -> np.ndarray:
+    p = d.pl
+    return a[p:p + d.n[2], p:p + d.n[1], p:p + d.n[0]]
+
+
+def with_ghost(a: np.ndarray, d) -> np.ndarray:
+    """The interior plus the first ghost layer (what the MG path reads/writes)."""
+    p = d.pl
+    return a[p - 1:p + d.n[2] + 1, p - 1:p + d.n[1] + 1, p - 1:p + d.n[0] + 1]
+
+
+def _dp(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _ptrs(arrs):
+    P = C.POINTER(C.c_double)
+    return (P * len(arrs))(*[_dp(a) for a in arrs])
+
+
+class MultigridSolver:
+    """One multi-block pressure-Poisson problem resident on one GPU."""
+
+    def __init__(self, blocks: Sequence, ngrd_gl: int, mg_itrsch: int = 3, irestr: int = 2, iproln: int = 1,
+                 maxcy: int = 30, precision: str = "fp64", var_coef: bool = False, device: int = 0,
+                 coarse_sweeps: int = 0, inner_cycles: int = 0, use_graph: bool = True):
+        self.L = _lib.lib()
+        self.blocks = list(blocks)
+        self._arr = (_lib.BlockDesc * len(self.blocks))(*self.blocks)
+        desc = _lib.MGDesc()
+        desc.nblocks = len(self.blocks)
+        desc.ngrd_gl = ngrd_gl
+        desc.mg_itrsch = mg_itrsch
+        desc.irestr = irestr
+        desc.iproln = iproln
+        desc.maxcy = maxcy
+        desc.precision = {"fp64": _lib.PREC_FP64, "mixed": _lib.PREC_MIXED}[precision]
+        desc.var_coef = int(bool(var_coef))
+        desc.device = device
+        desc.coarse_sweeps = coarse_sweeps
+        desc.inner_cycles = inner_cycles
+        desc.use_graph = int(bool(use_graph))
+        desc.blocks = self._arr
+        self.ngrd = ngrd_gl
+        self.precision = precision
+        self.maxcy = maxcy
+        self._h = C.c_void_p()
+        rc = self.L.h3d_mg_create(C.byref(self._h), C.byref(desc))
+        if rc != _lib.H3D_OK:
+            msg = self.L.h3d_mg_last_error(None).decode()
+            raise H3DError(rc, f"h3d_mg_create: {self.L.h3d_mg_strerror(rc).decode()}: {msg}")
+
+    # life cycle ----------------------------------------------------------
+    def close(self):
+        if getattr(self, "_h", None):
+            self.L.h3d_mg_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _check(self, rc, what):
+        return check(rc, self._h, what)
+
+    # set-up --------------------------------------------------------------
+    def set_density(self, ib: int, dens: np.ndarray):
+        dens = np.ascontiguousarray(dens, dtype=np.float64)
+        self._check(self.L.h3d_mg_set_density(self._h, ib, _dp(dens)), "h3d_mg_set_density")
+
+    def coeff(self):
+        self._check(self.L.h3d_mg_coeff(self._h), "h3d_mg_coeff")
+
+    # drop-in calls -------------------------------------------------------
+    def mgkcyc(self, pp: List[np.ndarray], su: List[np.ndarray]):
+        """One V-cycle: pp (host fields, in/out), su (host fields)."""
+        for a in list(pp) + list(su):
+            assert a.dtype == np.float64 and a.flags.c_contiguous
+        self._check(self.L.h3d_mg_mgkcyc(self._h, _ptrs(pp), _ptrs(su)), "h3d_mg_mgkcyc")
+
+    @staticmethod
+    def _opts(tol, maxcy, stop_rule, remove_mean, history):
+        o = _lib.SolveOpts()
+        o.tol = tol
+        o.maxcy = maxcy
+        o.stop_rule = stop_rule
+        o.remove_mean = int(bool(remove_mean))
+        o.record_history = int(bool(history))
+        return o
+
+    def _info(self, rc, info, history):
+        out = {k: getattr(info, k) for k, _ in _lib.SolveInfo._fields_}
+        out["converged"] = rc == _lib.H3D_OK
+        out["status"] = rc
+        if history:
+            n = C.c_int32()
+            self.L.h3d_mg_history(self._h, None, 0, C.byref(n))
+            buf = np.zeros(n.value)
+            self.L.h3d_mg_history(self._h, _dp(buf), n.value, C.byref(n))
+            out["history"] = buf
+        if rc not in (_lib.H3D_OK, _lib.H3D_ERR_NOT_CONVERGED):
+            self._check(rc, "solve")
+        return out
+
+    def newsolv_mg(self, p: List[np.ndarray], b: List[np.ndarray], tol: float = 1e-8, maxcy: int = 0,
+                   stop_rule: int = 0, remove_mean: bool = False, history: bool = False) -> dict:
+        """Solve A p = b (host fields, p in/out) by FP64 defect correction.
+
+        Like the reference, an exhausted cycle budget is reported (converged
+        False), not raised; a diverged solve raises."""
+        opts = self._opts(tol, maxcy, stop_rule, remove_mean, history)
+        info = _lib.SolveInfo()
+        rc = self.L.h3d_mg_newsolv(self._h, _ptrs(p), _ptrs(b), C.byref(opts), C.byref(info))
+        return self._info(rc, info, history)
+
+    # resident operation --------------------------------------------------
+    def upload(self, field: str, ib: int, host: np.ndarray):
+        f = {"p": _lib.FIELD_P, "b": _lib.FIELD_B}[field]
+        host = np.ascontiguousarray(host, dtype=np.float64)
+        self._check(self.L.h3d_mg_upload(self._h, f, ib, _dp(host)), "h3d_mg_upload")
+
+    def download(self, field: str, ib: int, host: np.ndarray):
+        f = {"p": _lib.FIELD_P, "b": _lib.FIELD_B}[field]
+        assert host.dtype == np.float64 and host.flags.c_contiguous
+        self._check(self.L.h3d_mg_download(self._h, f, ib, _dp(host)), "h3d_mg_download")
+
+    def zero_field(self, field: str):
+        f = {"p": _lib.FIELD_P, "b": _lib.FIELD_B}[field]
+        self._check(self.L.h3d_mg_zero_field(self._h, f), "h3d_mg_zero_field")
+
+    def solve_resident(self, tol: float = 1e-8, maxcy: int = 0, stop_rule: int = 0, remove_mean: bool = False,
+                       history: bool = False) -> dict:
+        opts = self._opts(tol, maxcy, stop_rule, remove_mean, history)
+        info = _lib.SolveInfo()
+        rc = self.L.h3d_mg_solve_resident(self._h, C.byref(opts), C.byref(info))
+        return self._info(rc, info, history)
+
+    def residual(self):
+        rr, bb, ri = C.c_double(), C.c_double(), C.c_double()
+        self._check(self.L.h3d_mg_residual(self._h, C.byref(rr), C.byref(bb), C.byref(ri)), "h3d_mg_residual")
+        return rr.value, bb.value, ri.value
+
+    def set_profiling(self, on: bool):
+        self._check(self.L.h3d_mg_set_profiling(self._h, int(bool(on))), "h3d_mg_set_profiling")
+
+    def smoother_bytes(self) -> float:
+        v = C.c_double()
+        self._check(self.L.h3d_mg_smoother_bytes(self._h, C.byref(v)), "h3d_mg_smoother_bytes")
+        return v.value
+
+    # reference subroutines on the level state ----------------------------
+    def level_dims(self, g: int, ib: int):
+        d = self.blocks[ib]
+        s = 2 ** (g - 1)
+        return d.n[2] // s, d.n[1] // s, d.n[0] // s
+
+    def put_level(self, g: int, field: str, ib: int, a: np.ndarray):
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        f = {"phi": 0, "rhs": 1}[field]
+        self._check(self.L.h3d_mg_put_level(self._h, g, f, ib, _dp(a)), "h3d_mg_put_level")
+
+    def get_level(self, g: int, field: str, ib: int) -> np.ndarray:
+        nz, ny, nx = self.level_dims(g, ib)
+        f = {"phi": 0, "rhs": 1}[field]
+        a = np.empty((nz + 2, ny + 2, nx + 2)) if f == 0 else np.empty((nz, ny, nx))
+        self._check(self.L.h3d_mg_get_level(self._h, g, f, ib, _dp(a)), "h3d_mg_get_level")
+        return a
+
+    def mgrelax(self, g: int, it: int):
+        self._check(self.L.h3d_mg_mgrelax(self._h, g, it), "h3d_mg_mgrelax")
+
+    def mgrestr(self, g: int):
+        self._check(self.L.h3d_mg_mgrestr(self._h, g), "h3d_mg_mgrestr")
+
+    def mgcorr(self, g: int):
+        self._check(self.L.h3d_mg_mgcorr(self._h, g), "h3d_mg_mgcorr")
+
+    def mgbound(self, g: int):
+        self._check(self.L.h3d_mg_mgbound(self._h, g), "h3d_mg_mgbound")
+
+    def exchangepp(self, g: int):
+        self._check(self.L.h3d_mg_exchangepp(self._h, g), "h3d_mg_exchangepp")
+
+    def vcycle(self):
+        self._check(self.L.h3d_mg_vcycle(self._h), "h3d_mg_vcycle")
+
+
+def halo_table(blocks: Sequence, g: int, kind: int):
+    """Ghost gather table of level g (host-only; see h3d_halo_table)."""
+    L = _lib.lib()
+    arr = (_lib.BlockDesc * len(blocks))(*blocks)
+    n = C.c_int64()
+    check(L.h3d_halo_table(len(blocks), arr, g, kind, None, None, 0, C.byref(n)), None, "h3d_halo_table")
+    dst = np.zeros(n.value, dtype=np.uint32)
+    src = np.zeros(n.value, dtype=np.uint32)
+    check(L.h3d_halo_table(len(blocks), arr, g, kind, dst.ctypes.data_as(C.POINTER(C.c_uint32)),
+                           src.ctypes.data_as(C.POINTER(C.c_uint32)), n.value, C.byref(n)), None, "h3d_halo_table")
+    return dst, src

@@ -1,0 +1,176 @@
+/*
+ * h3d_mg.h -- C ABI of the B200 pressure-Poisson multigrid solver.
+ *
+ * Drop-in for Hydro3D v7.0's multigrid pressure path (src_v70/newsolv_mg.for,
+ * src_v70/mgsolver.for, src_v70/exchangepp.for).  The Fortran host keeps its
+ * `dom(ib)` block arrays and calls these entry points through an
+ * ISO_C_BINDING interface; arrays are passed as the address of element
+ * (1,1,1) of the Fortran array (i fastest), sizes as plain integers.
+ *
+ * Conventions
+ *   - Every entry point returns H3D_OK (0) or a negative H3D_ERR_* code and
+ *     never exits the process (the reference prints and STOPs:
+ *     newsolv_mg.for:61-75, localparameters.for:204-208).
+ *   - One handle = one GPU + one CUDA stream; calls on a handle are not
+ *     re-entrant.  Device memory persists across calls.
+ *   - "Host field" = a Fortran array dims ttc[0..2] with pl ghost layers
+ *     (module_multidata.for:52-56: p, pp, su, sup, dens).
+ *   - "Canonical level array" = float64 (nz+2, ny+2, nx+2), x fastest, one
+ *     ghost layer, where n* is the block's interior size at that level;
+ *     a canonical right-hand side is (nz, ny, nx).
+ */
+#ifndef H3D_MG_H
+#define H3D_MG_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define H3D_OK 0
+#define H3D_ERR_BAD_CONFIG (-1)    /* sizes/levels/topology the path does not support */
+#define H3D_ERR_CUDA (-2)          /* a CUDA runtime call failed */
+#define H3D_ERR_NOT_CONVERGED (-3) /* maxcy reached ('not converged!!', newsolv_mg.for:61) */
+#define H3D_ERR_DIVERGED (-4)      /* NaN/Inf or growth ('BIG RMAX', newsolv_mg.for:65-75) */
+#define H3D_ERR_TIMEOUT (-5)       /* a bounded device wait gave up */
+#define H3D_ERR_NO_DEVICE (-6)     /* no CUDA device / wrong architecture */
+#define H3D_ERR_ARG (-7)           /* bad argument (null pointer, index out of range) */
+#define H3D_ERR_OOM (-8)           /* device allocation failed */
+#define H3D_ERR_INTERNAL (-9)
+
+/* One block (`type multidom`, module_multidata.for:16-120). */
+typedef struct h3d_block_desc {
+  int32_t n[3];           /* interior cells iep-isp+1, jep-jsp+1, kep-ksp+1 */
+  int32_t ttc[3];         /* host array dims ttc_i, ttc_j, ttc_k */
+  int32_t pl;             /* host ghost width (localparameters.for:19-23) */
+  int32_t ngrid;          /* dom(ib)%ngrid */
+  double h[3];            /* dx, dy, dz */
+  int32_t nb_face[6];     /* iprev inext jprev jnext kprev knext (-1 = none) */
+  int32_t nb_corner[8];   /* corprev1..4, cornext1..4 */
+  int32_t nb_edge[12];    /* edgprev1..6, edgnext1..6 */
+  int32_t nb_periodic[6]; /* per_ip per_in per_jp per_jn per_kp per_kn */
+  int32_t bc[6];          /* bc_west bc_east bc_south bc_north bc_bottom bc_top; 5 = periodic */
+  int32_t rdiv;           /* local mesh refinement ratio; only 1 is supported */
+  int32_t origin[3];      /* global index of the first interior cell (informational) */
+} h3d_block_desc;
+
+#define H3D_PREC_FP64 0   /* plain FP64 V-cycle (reference arithmetic) */
+#define H3D_PREC_MIXED 1  /* FP32 V-cycle inside FP64 iterative refinement */
+
+typedef struct h3d_mg_desc {
+  int32_t nblocks;
+  int32_t ngrd_gl;        /* MG levels (module_vars.for:8) */
+  int32_t mg_itrsch;      /* smoother; 3 = red-black GS (the only GPU smoother) */
+  int32_t irestr, iproln; /* pre/post sweeps (control.cin line 11) */
+  int32_t maxcy;          /* default cycle cap for h3d_mg_newsolv */
+  int32_t precision;      /* H3D_PREC_* */
+  int32_t var_coef;       /* 0: constant coefficients; 1: L_LSM density coefficients */
+  int32_t device;         /* CUDA ordinal */
+  int32_t coarse_sweeps;  /* sweeps at the coarsest level; 0 = irestr+iproln (reference) */
+  int32_t inner_cycles;   /* MIXED: FP32 V-cycles per FP64 refinement step (0 = 2) */
+  int32_t use_graph;      /* 1: capture each V-cycle as a CUDA graph */
+  const h3d_block_desc* blocks;
+} h3d_mg_desc;
+
+typedef struct h3d_mg h3d_mg;
+
+/* Options and report of a solve. */
+typedef struct h3d_solve_opts {
+  double tol;             /* tolerance (see stop_rule) */
+  int32_t maxcy;          /* cycle cap (0 = desc.maxcy) */
+  int32_t stop_rule;      /* 0: ||b-Ap||2/||b||2 <= tol, checked before each cycle;
+                             1: reference rule rmax < tol .and. iter > 1 (newsolv_mg.for:57) */
+  int32_t remove_mean;    /* 1: subtract the FP64 mean of p at the end (all-Neumann) */
+  int32_t record_history; /* 1: keep ||r||/||b|| per cycle (read with h3d_mg_history) */
+} h3d_solve_opts;
+
+typedef struct h3d_solve_info {
+  int32_t cycles;         /* V-cycles run (inner FP32 cycles for MIXED) */
+  int32_t outer;          /* FP64 defect evaluations after the initial one */
+  double relres;          /* final ||b-Ap||2/||b||2 (FP64) */
+  double rmax;            /* final max|b-Ap| * dV (calmas measure, press.for:61-63) */
+  double bnorm;           /* ||b||2 */
+  double device_ms;       /* device time of the solve, CUDA events on the solve stream */
+  double smoother_ms;     /* device time in level-1 smoother launches (profiling on) */
+  int64_t smoother_launches;
+  int64_t kernel_launches;/* kernels this library launched during the solve */
+} h3d_solve_info;
+
+/* --- set-up (localparameters.for:202-239, initial.for:329-360, coeff) ---- */
+int h3d_mg_create(h3d_mg** out, const h3d_mg_desc* desc);
+int h3d_mg_destroy(h3d_mg* h);
+/* Density of block ib as a host field (ttc dims, pl ghosts); L_LSM only.
+ * Replaces the dom(ib)%dens read in coeff (mgsolver.for:82). */
+int h3d_mg_set_density(h3d_mg* h, int32_t ib, const double* dens);
+/* coeff (mgsolver.for:2-224): per-level coefficients on the device. */
+int h3d_mg_coeff(h3d_mg* h);
+
+/* --- the drop-in calls -------------------------------------------------- */
+/* mgkcyc (mgsolver.for:226-372): one V-cycle.  pp[ib] host field in/out
+ * (interior + first ghost layer used), su[ib] host field (interior read). */
+int h3d_mg_mgkcyc(h3d_mg* h, double* const* pp, const double* const* su);
+/* newsolv_mg (newsolv_mg.for:17-57) as FP64 defect correction on b - A p.
+ * p[ib] host field in/out, b[ib] host field (su, or sup for L_LSM). */
+int h3d_mg_newsolv(h3d_mg* h, double* const* p, const double* const* b,
+                   const h3d_solve_opts* opts, h3d_solve_info* info);
+
+/* --- device-resident operation ------------------------------------------ */
+#define H3D_FIELD_P 0     /* level-1 pressure, FP64, canonical with ghosts */
+#define H3D_FIELD_B 1     /* level-1 right-hand side, FP64, canonical interior */
+/* Copy block ib of a resident field from/to a host field (ttc dims, pl ghosts). */
+int h3d_mg_upload(h3d_mg* h, int32_t field, int32_t ib, const double* host);
+int h3d_mg_download(h3d_mg* h, int32_t field, int32_t ib, double* host);
+/* Zero a resident field on the device (e.g. the initial guess pp = 0,
+ * newsolv_mg.for:20-22). */
+int h3d_mg_zero_field(h3d_mg* h, int32_t field);
+/* Solve with p and b already in device memory. */
+int h3d_mg_solve_resident(h3d_mg* h, const h3d_solve_opts* opts, h3d_solve_info* info);
+/* ||b-Ap||^2, ||b||^2 and max|b-Ap|*dV of the resident fields. */
+int h3d_mg_residual(h3d_mg* h, double* rr, double* bb, double* rinf);
+/* Relative residual history of the last solve (n <= cap entries written). */
+int h3d_mg_history(h3d_mg* h, double* out, int32_t cap, int32_t* n);
+
+/* --- reference subroutines on the resident level state ----------------- */
+/* Canonical level arrays of block ib at level g; field 0 = phi, 1 = rhs. */
+int h3d_mg_put_level(h3d_mg* h, int32_t g, int32_t field, int32_t ib, const double* a);
+int h3d_mg_get_level(h3d_mg* h, int32_t g, int32_t field, int32_t ib, double* a);
+int h3d_mg_mgrelax(h3d_mg* h, int32_t g, int32_t it);   /* mgsolver.for:374-621 */
+int h3d_mg_mgrestr(h3d_mg* h, int32_t g);               /* mgsolver.for:623-766 */
+int h3d_mg_mgcorr(h3d_mg* h, int32_t g);                /* mgsolver.for:768-910 */
+int h3d_mg_mgbound(h3d_mg* h, int32_t g);               /* mgsolver.for:912-997 */
+int h3d_mg_exchangepp(h3d_mg* h, int32_t g);            /* exchangepp.for:2-2835 */
+int h3d_mg_vcycle(h3d_mg* h);                           /* mgkcyc body on level state */
+int h3d_mg_sync(h3d_mg* h);
+
+/* --- profiling ----------------------------------------------------------- */
+/* 1: bracket every level-1 smoother launch with CUDA events on the solve
+ * stream and add its duration to h3d_solve_info.smoother_ms. */
+int h3d_mg_set_profiling(h3d_mg* h, int32_t on);
+/* Algorithmic bytes of one level-1 smoother launch (sum over blocks). */
+int h3d_mg_smoother_bytes(h3d_mg* h, double* bytes_per_launch);
+
+/* --- host-only helpers (no GPU needed) ---------------------------------- */
+/* read_infodom neighbour discovery (alloc_dom.for:524-1200) on integer block
+ * extents ext[6*ib..] = xs,xe,ys,ye,zs,ze (global cell units), global bc[6]. */
+int h3d_topology(int32_t nblocks, const int32_t* ext, const int32_t* bc,
+                 const double* h, int32_t ngrid, h3d_block_desc* out);
+/* Ghost-fill gather table of level g, in the canonical packed numbering
+ * (blocks concatenated, each (nz+2)(ny+2)(nx+2) x fastest).
+ * kind 0: mgbound followed by exchangepp (after every sweep, mgsolver.for:614-615)
+ * kind 1: exchangepp alone;  kind 2: mgbound alone;  kind 3: face ghosts of
+ * kind 0 (the pressure halo of the outer residual).
+ * Entry e: dst[e] <- src[e]; bit 31 of src set = the pre-fill value of that
+ * (ghost) cell, clear = the cell's current (interior) value.
+ * With dst == NULL only *n is returned. */
+int h3d_halo_table(int32_t nblocks, const h3d_block_desc* blocks, int32_t g,
+                   int32_t kind, uint32_t* dst, uint32_t* src, int64_t cap,
+                   int64_t* n);
+
+const char* h3d_mg_strerror(int code);
+/* Text of the last error on this handle (or of the last create failure). */
+const char* h3d_mg_last_error(const h3d_mg* h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,1087 @@
+/*
+ * h3d_oracle.c -- CPU oracle (test infrastructure only; see h3d_oracle.h).
+ *
+ * A restatement in C of the reference multigrid path of Hydro3D v7.0:
+ *   coeff, mgkcyc, mgrelax, mgrestr, mgcorr, mgbound   (src_v70/mgsolver.for)
+ *   exchangepp, exchbc_mgpp (same-rank, equal-resolution branches)
+ *                                                      (src_v70/exchangepp.for)
+ *   newsolv_mg outer loop                              (src_v70/newsolv_mg.for)
+ *   read_infodom neighbour discovery                   (src_v70/alloc_dom.for)
+ * All arithmetic is IEEE FP64 evaluated left to right in the reference's
+ * operand order; build with -ffp-contract=off so no FMA is formed.
+ *
+ * Index conventions follow the reference: i,j,k are 1-based and include the
+ * one ghost layer (interior 2..n-1); `cof` is 1-based and the level-g phi
+ * slab is j-fastest: (k-1)*ni*nj + (i-1)*nj + j + faz(g) - ni*nj*nk
+ * (mgsolver.for:412); coefficient slot s of cell (i,j,k) lives at
+ * faz(g) + (k-2)(ni-2)(nj-2) + (i-2)(nj-2) + (j-1) + s*incr (mgsolver.for:413-420).
+ */
+#include "h3d_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#define MAXLEV 16
+
+typedef struct {
+  or_block_desc d;
+  int ngrid;
+  int64_t faz[MAXLEV + 1];      /* faz(1..ngrd) as in mgsolver.for:23-41 */
+  int64_t nwork;
+  double* cof;                  /* 1-based, cof[1..nwork] */
+  double* dens;                 /* interior density (nz,ny,nx) x-fastest */
+  double* dens_mg;              /* 1-based dens_mg(1..tot) */
+  int64_t ijkp_lsm[MAXLEV + 1]; /* initial.for:203-213 */
+  /* same-rank receive buffers of exchangepp (1-based) */
+  double* recvb_m1;
+  double* recvb_p1;
+  double rc_m[5], rc_p[5];      /* rc1m..rc4m, rc1p..rc4p */
+  double* re_m[7];              /* re1m..re6m */
+  double* re_p[7];              /* re1p..re6p */
+} or_dom;
+
+struct or_mg {
+  int nbp, ngrd_gl, mg_itrsch, irestr, iproln, lsm, periodic;
+  int ngg;                      /* longest line / largest plane */
+  int err;
+  or_dom* dom;
+};
+
+static int g_threads = 1;
+void or_set_threads(int n) { g_threads = n > 0 ? n : 1; }
+
+static int ipow2(int e) { return 1 << e; }
+
+/* Level dims incl. ghosts with the reference's level clamp
+ * (mgsolver.for:392-400). */
+static void lev_dims(const or_dom* d, int g, int* ni, int* nj, int* nk) {
+  int gl = g > d->ngrid ? d->ngrid : g;
+  *ni = d->d.n[0] / ipow2(gl - 1) + 2;
+  *nj = d->d.n[1] / ipow2(gl - 1) + 2;
+  *nk = d->d.n[2] / ipow2(gl - 1) + 2;
+}
+
+/* phi index (1-based) of cell (i,j,k) of level g. */
+#define PHI(i, j, k) ((int64_t)((k)-1) * nij + (int64_t)((i)-1) * nj + (j) + nijk)
+
+or_mg* or_create(int nblocks, const or_block_desc* blocks, int ngrd_gl,
+                 int mg_itrsch, int irestr, int iproln, int lsm) {
+  or_mg* m = (or_mg*)calloc(1, sizeof(or_mg));
+  m->nbp = nblocks;
+  m->ngrd_gl = ngrd_gl;
+  m->mg_itrsch = mg_itrsch;
+  m->irestr = irestr;
+  m->iproln = iproln;
+  m->lsm = lsm;
+  m->dom = (or_dom*)calloc((size_t)nblocks, sizeof(or_dom));
+  if (ngrd_gl < 1 || ngrd_gl > MAXLEV) m->err = 1;
+  int nmax = 0;
+  for (int ib = 0; ib < nblocks; ++ib) {
+    or_dom* d = &m->dom[ib];
+    d->d = blocks[ib];
+    d->ngrid = blocks[ib].ngrid;
+    if (d->ngrid != ngrd_gl || blocks[ib].rdiv != 1) m->err = 1;
+    for (int a = 0; a < 6; ++a)
+      if (d->d.bc[a] == 5) m->periodic = 1; /* alloc_dom.for:1224-1231 */
+    /* divisibility check, localparameters.for:204-209 */
+    int pow2 = ipow2(d->ngrid - 1);
+    for (int a = 0; a < 3; ++a)
+      if (d->d.n[a] <= 0 || d->d.n[a] % pow2 != 0) m->err = 1;
+    if (m->err) continue;
+    /* nwork, localparameters.for:226-236 */
+    int64_t nwork = 0;
+    for (int g = 1; g <= ngrd_gl; ++g) {
+      int ni, nj, nk;
+      lev_dims(d, g, &ni, &nj, &nk);
+      nwork += (int64_t)ni * nj * nk + 8LL * (ni - 2) * (nj - 2) * (nk - 2);
+    }
+    d->nwork = nwork;
+    d->cof = (double*)calloc((size_t)nwork + 1, sizeof(double));
+    int ni = d->d.n[0] + 2, nj = d->d.n[1] + 2, nk = d->d.n[2] + 2;
+    int pmax = ni * nj;
+    if (ni * nk > pmax) pmax = ni * nk;
+    if (nj * nk > pmax) pmax = nj * nk;
+    if (pmax > nmax) nmax = pmax;
+    /* ijkp_lsm, initial.for:203-213 */
+    d->ijkp_lsm[0] = 0;
+    for (int g = 1; g <= d->ngrid; ++g) {
+      int a, b, c;
+      lev_dims(d, g, &a, &b, &c);
+      d->ijkp_lsm[g] = d->ijkp_lsm[g - 1] + (int64_t)(a - 2) * (b - 2) * (c - 2);
+    }
+    d->dens_mg = (double*)calloc((size_t)d->ijkp_lsm[d->ngrid] + 1, sizeof(double));
+    d->dens = (double*)calloc((size_t)d->d.n[0] * d->d.n[1] * d->d.n[2], sizeof(double));
+    for (int64_t q = 0; q < (int64_t)d->d.n[0] * d->d.n[1] * d->d.n[2]; ++q) d->dens[q] = 1.0;
+  }
+  m->ngg = nmax;
+  for (int ib = 0; ib < nblocks && !m->err; ++ib) {
+    or_dom* d = &m->dom[ib];
+    d->recvb_m1 = (double*)calloc((size_t)nmax + 1, sizeof(double));
+    d->recvb_p1 = (double*)calloc((size_t)nmax + 1, sizeof(double));
+    int lmax = d->d.n[0] + 2;
+    if (d->d.n[1] + 2 > lmax) lmax = d->d.n[1] + 2;
+    if (d->d.n[2] + 2 > lmax) lmax = d->d.n[2] + 2;
+    for (int e = 1; e <= 6; ++e) {
+      d->re_m[e] = (double*)calloc((size_t)lmax + 1, sizeof(double));
+      d->re_p[e] = (double*)calloc((size_t)lmax + 1, sizeof(double));
+    }
+  }
+  return m;
+}
+
+int or_error(const or_mg* m) { return m->err; }
+
+void or_destroy(or_mg* m) {
+  if (!m) return;
+  for (int ib = 0; ib < m->nbp; ++ib) {
+    or_dom* d = &m->dom[ib];
+    free(d->cof);
+    free(d->dens);
+    free(d->dens_mg);
+    free(d->recvb_m1);
+    free(d->recvb_p1);
+    for (int e = 1; e <= 6; ++e) {
+      free(d->re_m[e]);
+      free(d->re_p[e]);
+    }
+  }
+  free(m->dom);
+  free(m);
+}
+
+void or_set_density(or_mg* m, int ib, const double* dens) {
+  or_dom* d = &m->dom[ib];
+  memcpy(d->dens, dens, sizeof(double) * (size_t)d->d.n[0] * d->d.n[1] * d->d.n[2]);
+}
+
+/* dens(i+pl-1, j+pl-1, k+pl-1) for the 1-based ghost-inclusive level-1 index
+ * (mgsolver.for:82) == interior cell (i-2, j-2, k-2). */
+static double dens_at(const or_dom* d, int i, int j, int k) {
+  return d->dens[((int64_t)(k - 2) * d->d.n[1] + (j - 2)) * d->d.n[0] + (i - 2)];
+}
+
+/* ------------------------------------------------------------------ coeff */
+void or_coeff(or_mg* m) { /* mgsolver.for:2-224 */
+  for (int ib = 0; ib < m->nbp; ++ib) {
+    or_dom* d = &m->dom[ib];
+    if (m->lsm)
+      for (int64_t q = 0; q <= d->ijkp_lsm[d->ngrid]; ++q) d->dens_mg[q] = 0.0;
+    int pi, pj, pk;
+    lev_dims(d, 1, &pi, &pj, &pk);
+    d->faz[1] = (int64_t)pi * pj * pk; /* :23-28 */
+    for (int glevel = 2; glevel <= m->ngrd_gl; ++glevel) { /* :29-41 */
+      int ci, cj, ck;
+      lev_dims(d, glevel, &ci, &cj, &ck);
+      d->faz[glevel] = d->faz[glevel - 1] + (int64_t)ci * cj * ck +
+                       8LL * (pi - 2) * (pj - 2) * (pk - 2);
+      pi = ci; pj = cj; pk = ck;
+    }
+    const int* nb = d->d.nb_face;
+    const int* bc = d->d.bc;
+    for (int glevel = 1; glevel <= m->ngrd_gl; ++glevel) { /* :44 */
+      int gl = glevel > d->ngrid ? d->ngrid : glevel;
+      int mi, mj, mk;
+      lev_dims(d, glevel, &mi, &mj, &mk);
+      double ndx = d->d.h[0] * ipow2(gl - 1);
+      double ndy = d->d.h[1] * ipow2(gl - 1);
+      double ndz = d->d.h[2] * ipow2(gl - 1);
+      double dxx = ndx * ndx, dyy = ndy * ndy, dzz = ndz * ndz;
+      int64_t cnt = d->faz[glevel] - (int64_t)mi * mj * mk; /* :62-70 */
+      for (int64_t q = 1; q <= (int64_t)mi * mj * mk; ++q) d->cof[cnt + q] = 0.0;
+
+      if (m->lsm) { /* :72-112 dens_mg hierarchy */
+        for (int k = 2; k <= mk - 1; ++k)
+          for (int i = 2; i <= mi - 1; ++i)
+            for (int j = 2; j <= mj - 1; ++j) {
+              if (glevel == 1) {
+                int64_t q = (int64_t)(k - 2) * (mi - 2) * (mj - 2) + (int64_t)(i - 2) * (mj - 2) + (j - 1);
+                d->dens_mg[q] = dens_at(d, i, j, k);
+              } else {
+                int64_t q = d->ijkp_lsm[glevel - 1] + (int64_t)(k - 2) * (mi - 2) * (mj - 2) +
+                            (int64_t)(i - 2) * (mj - 2) + (j - 1);
+                int pni = d->d.n[0] / ipow2(glevel - 2) + 2;
+                int pnj = d->d.n[1] / ipow2(glevel - 2) + 2;
+                int64_t ij1 = (int64_t)(2 * k - 4) * (pni - 2) * (pnj - 2) + (int64_t)(2 * i - 4) * (pnj - 2) +
+                              (2 * j - 3) + d->ijkp_lsm[glevel - 2];
+                int64_t ij2 = ij1 + 1, ij3 = ij1 + (pnj - 2), ij4 = ij1 + (pnj - 2) + 1;
+                int64_t pl2 = (int64_t)(pni - 2) * (pnj - 2);
+                int64_t ij5 = ij1 + pl2, ij6 = ij1 + pl2 + 1, ij7 = ij1 + pl2 + (pnj - 2),
+                        ij8 = ij1 + pl2 + (pnj - 2) + 1;
+                double* dm = d->dens_mg;
+                d->dens_mg[q] = 0.125 * (dm[ij1] + dm[ij2] + dm[ij3] + dm[ij4] + dm[ij5] + dm[ij6] +
+                                         dm[ij7] + dm[ij8]);
+              }
+            }
+      }
+
+      int64_t incr = (int64_t)(mi - 2) * (mj - 2) * (mk - 2); /* :114 */
+      for (int k = 2; k <= mk - 1; ++k)
+        for (int i = 2; i <= mi - 1; ++i)
+          for (int j = 2; j <= mj - 1; ++j) {
+            int64_t ijk = d->faz[glevel] + (int64_t)(k - 2) * (mi - 2) * (mj - 2) +
+                          (int64_t)(i - 2) * (mj - 2) + (j - 1);
+            double* c = d->cof;
+            if (m->lsm) { /* :122-184 */
+              int64_t q = (glevel == 1 ? 0 : d->ijkp_lsm[glevel - 1]) +
+                          (int64_t)(k - 2) * (mi - 2) * (mj - 2) + (int64_t)(i - 2) * (mj - 2) + (j - 1);
+              const double* dm = d->dens_mg;
+              int64_t sx = (mj - 2), sz = (int64_t)(mi - 2) * (mj - 2);
+              double dim = (i == 2) ? dm[q] : 0.5 * (dm[q] + dm[q - sx]);
+              double dip = (i == mi - 1) ? dm[q] : 0.5 * (dm[q] + dm[q + sx]);
+              double djm = (j == 2) ? dm[q] : 0.5 * (dm[q] + dm[q - 1]);
+              double djp = (j == mj - 1) ? dm[q] : 0.5 * (dm[q] + dm[q + 1]);
+              double dkm = (k == 2) ? dm[q] : 0.5 * (dm[q] + dm[q - sz]);
+              double dkp = (k == mk - 1) ? dm[q] : 0.5 * (dm[q] + dm[q + sz]);
+              double dx = d->d.h[0], dy = d->d.h[1], dz = d->d.h[2];
+              c[ijk] = dy * dz / dx / dim;
+              c[ijk + 1 * incr] = dy * dz / dx / dip;
+              c[ijk + 2 * incr] = dx * dz / dy / djm;
+              c[ijk + 3 * incr] = dx * dz / dy / djp;
+              c[ijk + 4 * incr] = dx * dy / dz / dkm;
+              c[ijk + 5 * incr] = dx * dy / dz / dkp;
+            } else { /* :186-191 */
+              c[ijk] = 1.0 / dxx;
+              c[ijk + 1 * incr] = 1.0 / dxx;
+              c[ijk + 2 * incr] = 1.0 / dyy;
+              c[ijk + 3 * incr] = 1.0 / dyy;
+              c[ijk + 4 * incr] = 1.0 / dzz;
+              c[ijk + 5 * incr] = 1.0 / dzz;
+            }
+            /* physical, non-periodic faces, :194-205 */
+            if (nb[0] < 0 && bc[0] != 5 && i == 2) c[ijk] = 0.0;
+            if (nb[1] < 0 && bc[1] != 5 && i == mi - 1) c[ijk + 1 * incr] = 0.0;
+            if (nb[2] < 0 && bc[2] != 5 && j == 2) c[ijk + 2 * incr] = 0.0;
+            if (nb[3] < 0 && bc[3] != 5 && j == mj - 1) c[ijk + 3 * incr] = 0.0;
+            if (nb[4] < 0 && bc[4] != 5 && k == 2) c[ijk + 4 * incr] = 0.0;
+            if (nb[5] < 0 && bc[5] != 5 && k == mk - 1) c[ijk + 5 * incr] = 0.0;
+            c[ijk + 6 * incr] = -1.0 * (c[ijk] + c[ijk + 1 * incr] + c[ijk + 2 * incr] +
+                                        c[ijk + 3 * incr] + c[ijk + 4 * incr] + c[ijk + 5 * incr]);
+            c[ijk + 7 * incr] = 0.0;
+          }
+    }
+  }
+}
+
+/* ------------------------------------------------------------- accessors */
+void or_put_phi(or_mg* m, int g, int ib, const double* a) {
+  or_dom* d = &m->dom[ib];
+  int ni, nj, nk;
+  lev_dims(d, g, &ni, &nj, &nk);
+  int64_t nij = (int64_t)ni * nj, nijk = d->faz[g] - (int64_t)ni * nj * nk;
+  for (int k = 1; k <= nk; ++k)
+    for (int j = 1; j <= nj; ++j)
+      for (int i = 1; i <= ni; ++i)
+        d->cof[PHI(i, j, k)] = a[((int64_t)(k - 1) * nj + (j - 1)) * ni + (i - 1)];
+}
+
+void or_get_phi(const or_mg* m, int g, int ib, double* a) {
+  const or_dom* d = &m->dom[ib];
+  int ni, nj, nk;
+  lev_dims(d, g, &ni, &nj, &nk);
+  int64_t nij = (int64_t)ni * nj, nijk = d->faz[g] - (int64_t)ni * nj * nk;
+  for (int k = 1; k <= nk; ++k)
+    for (int j = 1; j <= nj; ++j)
+      for (int i = 1; i <= ni; ++i)
+        a[((int64_t)(k - 1) * nj + (j - 1)) * ni + (i - 1)] = d->cof[PHI(i, j, k)];
+}
+
+static int64_t cofidx(const or_dom* d, int g, int ni, int nj, int i, int j, int k) {
+  return d->faz[g] + (int64_t)(k - 2) * (ni - 2) * (nj - 2) + (int64_t)(i - 2) * (nj - 2) + (j - 1);
+}
+
+void or_get_coef(const or_mg* m, int g, int ib, int s, double* a) {
+  const or_dom* d = &m->dom[ib];
+  int ni, nj, nk;
+  lev_dims(d, g, &ni, &nj, &nk);
+  int64_t incr = (int64_t)(ni - 2) * (nj - 2) * (nk - 2);
+  for (int k = 2; k <= nk - 1; ++k)
+    for (int j = 2; j <= nj - 1; ++j)
+      for (int i = 2; i <= ni - 1; ++i)
+        a[((int64_t)(k - 2) * (nj - 2) + (j - 2)) * (ni - 2) + (i - 2)] =
+            d->cof[cofidx(d, g, ni, nj, i, j, k) + s * incr];
+}
+
+void or_put_rhs(or_mg* m, int g, int ib, const double* a) {
+  or_dom* d = &m->dom[ib];
+  int ni, nj, nk;
+  lev_dims(d, g, &ni, &nj, &nk);
+  int64_t incr = (int64_t)(ni - 2) * (nj - 2) * (nk - 2);
+  for (int k = 2; k <= nk - 1; ++k)
+    for (int j = 2; j <= nj - 1; ++j)
+      for (int i = 2; i <= ni - 1; ++i)
+        d->cof[cofidx(d, g, ni, nj, i, j, k) + 7 * incr] =
+            a[((int64_t)(k - 2) * (nj - 2) + (j - 2)) * (ni - 2) + (i - 2)];
+}
+
+void or_get_rhs(const or_mg* m, int g, int ib, double* a) {
+  or_get_coef(m, g, ib, 7, a);
+}
+
+/* ---------------------------------------------------------------- mgbound */
+void or_mgbound(or_mg* m, int g) { /* mgsolver.for:912-997 */
+  for (int ib = 0; ib < m->nbp; ++ib) {
+    or_dom* d = &m->dom[ib];
+    int ni, nj, nk;
+    lev_dims(d, g, &ni, &nj, &nk);
+    int64_t nij = (int64_t)ni * nj, nijk = d->faz[g] - (int64_t)ni * nj * nk;
+    double* c = d->cof;
+    const int* nb = d->d.nb_face;
+    const int* bc = d->d.bc;
+    if (nb[0] < 0 && bc[0] != 5)
+      for (int k = 1; k <= nk; ++k)
+        for (int j = 1; j <= nj; ++j) c[PHI(1, j, k)] = c[PHI(1, j, k) + nj];
+    if (nb[1] < 0 && bc[1] != 5)
+      for (int k = 1; k <= nk; ++k)
+        for (int j = 1; j <= nj; ++j) c[PHI(ni, j, k)] = c[PHI(ni, j, k) - nj];
+    if (nb[2] < 0 && bc[2] != 5)
+      for (int k = 1; k <= nk; ++k)
+        for (int i = 1; i <= ni; ++i) c[PHI(i, 1, k)] = c[PHI(i, 1, k) + 1];
+    if (nb[3] < 0 && bc[3] != 5)
+      for (int k = 1; k <= nk; ++k)
+        for (int i = 1; i <= ni; ++i) c[PHI(i, nj, k)] = c[PHI(i, nj, k) - 1];
+    if (nb[4] < 0 && bc[4] != 5)
+      for (int j = 1; j <= nj; ++j)
+        for (int i = 1; i <= ni; ++i) c[PHI(i, j, 1)] = c[PHI(i, j, 1) + nij];
+    if (nb[5] < 0 && bc[5] != 5)
+      for (int j = 1; j <= nj; ++j)
+        for (int i = 1; i <= ni; ++i) c[PHI(i, j, nk)] = c[PHI(i, j, nk) - nij];
+  }
+}
+
+/* ------------------------------------------------------------- exchangepp */
+/* Corner and edge cells: pack position in the sender and unpack position in
+ * the receiver, as 1-based ghost-inclusive (i,j,k) with 0 = "1", -1 = "n-1",
+ * -2 = "n", 2 = "2" and 99 = "running index nn" (exchangepp.for:441-1100,
+ * 1400-2056 pack; 2511-2826 unpack). */
+enum { P2 = 2, PN1 = -1, PN = -2, P1 = 1, RUN = 99 };
+static int pos(int code, int n, int nn) {
+  switch (code) {
+    case P1: return 1;
+    case P2: return 2;
+    case PN1: return n - 1;
+    case PN: return n;
+    default: return nn;
+  }
+}
+/* prev corners #1..4: sender cell -> receiver's rcNp -> receiver cell */
+static const int corprev_src[4][3] = {{P2, P2, P2}, {P2, PN1, P2}, {PN1, PN1, P2}, {PN1, P2, P2}};
+static const int cornext_src[4][3] = {{PN1, PN1, PN1}, {PN1, P2, PN1}, {P2, P2, PN1}, {P2, PN1, PN1}};
+/* unpack of rcNm (prev corners of the receiver), exchangepp.for:2515-2566 */
+static const int corprev_dst[4][3] = {{P1, P1, P1}, {P1, PN, P1}, {PN, PN, P1}, {PN, P1, P1}};
+/* unpack of rcNp (next corners of the receiver), exchangepp.for:2668-2718 */
+static const int cornext_dst[4][3] = {{PN, PN, PN}, {PN, P1, PN}, {P1, P1, PN}, {P1, PN, PN}};
+/* edges: axis that runs (0 i, 1 j, 2 k) and the fixed positions */
+static const int edg_axis[6] = {1, 0, 1, 0, 2, 2};
+static const int edgprev_src[6][3] = {{P2, RUN, P2}, {RUN, PN1, P2}, {PN1, RUN, P2},
+                                      {RUN, P2, P2}, {P2, P2, RUN}, {P2, PN1, RUN}};
+static const int edgnext_src[6][3] = {{PN1, RUN, PN1}, {RUN, P2, PN1}, {P2, RUN, PN1},
+                                      {RUN, PN1, PN1}, {PN1, PN1, RUN}, {PN1, P2, RUN}};
+static const int edgprev_dst[6][3] = {{P1, RUN, P1}, {RUN, PN, P1}, {PN, RUN, P1},
+                                      {RUN, P1, P1}, {P1, P1, RUN}, {P1, PN, RUN}};
+static const int edgnext_dst[6][3] = {{PN, RUN, PN}, {RUN, P1, PN}, {P1, RUN, PN},
+                                      {RUN, PN, PN}, {PN, PN, RUN}, {PN, P1, RUN}};
+
+static int edge_len(int e, int ni, int nj, int nk) {
+  int ax = edg_axis[e];
+  return ax == 0 ? ni : (ax == 1 ? nj : nk);
+}
+
+void or_exchangepp(or_mg* m, int g) { /* exchangepp.for:2-2835 */
+  for (int sync_dir = 1; sync_dir <= 3; ++sync_dir) {
+    /* pack loop, exchangepp.for:48-2063 (same-rank, equal-resolution) */
+    for (int ib = 0; ib < m->nbp; ++ib) {
+      or_dom* d = &m->dom[ib];
+      int ni, nj, nk;
+      lev_dims(d, g, &ni, &nj, &nk);
+      int64_t nij = (int64_t)ni * nj, nijk = d->faz[g] - (int64_t)ni * nj * nk;
+      const double* fi = d->cof;
+      int cprev = d->d.nb_face[2 * (sync_dir - 1)];
+      int cnext = d->d.nb_face[2 * (sync_dir - 1) + 1];
+      if (cprev >= 0) { /* :149-271 */
+        double* rb = m->dom[cprev].recvb_p1;
+        if (sync_dir == 1) {
+          for (int k = 1; k <= nk; ++k)
+            for (int j = 1; j <= nj; ++j) rb[(k - 1) * nj + j] = fi[PHI(2, j, k)];
+        } else if (sync_dir == 2) {
+          for (int k = 1; k <= nk; ++k)
+            for (int i = 1; i <= ni; ++i) rb[(k - 1) * ni + i] = fi[PHI(i, 2, k)];
+        } else {
+          for (int i = 1; i <= ni; ++i)
+            for (int j = 1; j <= nj; ++j) rb[(i - 1) * nj + j] = fi[PHI(i, j, 2)];
+        }
+      }
+      if (sync_dir == 3) { /* prev corners and edges, :435-1100 */
+        for (int c = 0; c < 4; ++c) {
+          int nbr = d->d.nb_corner[c];
+          if (nbr < 0) continue;
+          m->dom[nbr].rc_p[c + 1] =
+              fi[PHI(pos(corprev_src[c][0], ni, 0), pos(corprev_src[c][1], nj, 0),
+                     pos(corprev_src[c][2], nk, 0))];
+        }
+        for (int e = 0; e < 6; ++e) {
+          int nbr = d->d.nb_edge[e];
+          if (nbr < 0) continue;
+          int len = edge_len(e, ni, nj, nk);
+          for (int nn = 2; nn <= len - 1; ++nn)
+            m->dom[nbr].re_p[e + 1][nn] =
+                fi[PHI(pos(edgprev_src[e][0], ni, nn), pos(edgprev_src[e][1], nj, nn),
+                       pos(edgprev_src[e][2], nk, nn))];
+        }
+      }
+      if (cnext >= 0) { /* :1107-1393 */
+        double* rb = m->dom[cnext].recvb_m1;
+        if (sync_dir == 1) {
+          for (int k = 1; k <= nk; ++k)
+            for (int j = 1; j <= nj; ++j) rb[(k - 1) * nj + j] = fi[PHI(ni - 1, j, k)];
+        } else if (sync_dir == 2) {
+          for (int k = 1; k <= nk; ++k)
+            for (int i = 1; i <= ni; ++i) rb[(k - 1) * ni + i] = fi[PHI(i, nj - 1, k)];
+        } else {
+          for (int i = 1; i <= ni; ++i)
+            for (int j = 1; j <= nj; ++j) rb[(i - 1) * nj + j] = fi[PHI(i, j, nk - 1)];
+        }
+      }
+      if (sync_dir == 3) { /* next corners and edges, :1394-2060 */
+        for (int c = 0; c < 4; ++c) {
+          int nbr = d->d.nb_corner[4 + c];
+          if (nbr < 0) continue;
+          m->dom[nbr].rc_m[c + 1] =
+              fi[PHI(pos(cornext_src[c][0], ni, 0), pos(cornext_src[c][1], nj, 0),
+                     pos(cornext_src[c][2], nk, 0))];
+        }
+        for (int e = 0; e < 6; ++e) {
+          int nbr = d->d.nb_edge[6 + e];
+          if (nbr < 0) continue;
+          int len = edge_len(e, ni, nj, nk);
+          for (int nn = 2; nn <= len - 1; ++nn)
+            m->dom[nbr].re_m[e + 1][nn] =
+                fi[PHI(pos(edgnext_src[e][0], ni, nn), pos(edgnext_src[e][1], nj, nn),
+                       pos(edgnext_src[e][2], nk, nn))];
+        }
+      }
+    }
+    /* unpack loop, exchangepp.for:2066-2826 */
+    for (int ib = 0; ib < m->nbp; ++ib) {
+      or_dom* d = &m->dom[ib];
+      int ni, nj, nk;
+      lev_dims(d, g, &ni, &nj, &nk);
+      int64_t nij = (int64_t)ni * nj, nijk = d->faz[g] - (int64_t)ni * nj * nk;
+      double* fi = d->cof;
+      int cprev = d->d.nb_face[2 * (sync_dir - 1)];
+      int cnext = d->d.nb_face[2 * (sync_dir - 1) + 1];
+      if (cprev >= 0) { /* :2101-2196 */
+        const double* rb = d->recvb_m1;
+        if (sync_dir == 1) {
+          for (int k = 1; k <= nk; ++k)
+            for (int j = 1; j <= nj; ++j) fi[PHI(1, j, k)] = rb[(k - 1) * nj + j];
+        } else if (sync_dir == 2) {
+          for (int k = 1; k <= nk; ++k)
+            for (int i = 1; i <= ni; ++i) fi[PHI(i, 1, k)] = rb[(k - 1) * ni + i];
+        } else {
+          for (int i = 1; i <= ni; ++i)
+            for (int j = 1; j <= nj; ++j) fi[PHI(i, j, 1)] = rb[(i - 1) * nj + j];
+        }
+      }
+      if (cnext >= 0) { /* :2306-2402 */
+        const double* rb = d->recvb_p1;
+        if (sync_dir == 1) {
+          for (int k = 1; k <= nk; ++k)
+            for (int j = 1; j <= nj; ++j) fi[PHI(ni, j, k)] = rb[(k - 1) * nj + j];
+        } else if (sync_dir == 2) {
+          for (int k = 1; k <= nk; ++k)
+            for (int i = 1; i <= ni; ++i) fi[PHI(i, nj, k)] = rb[(k - 1) * ni + i];
+        } else {
+          for (int i = 1; i <= ni; ++i)
+            for (int j = 1; j <= nj; ++j) fi[PHI(i, j, nk)] = rb[(i - 1) * nj + j];
+        }
+      }
+      if (sync_dir == 3) { /* :2511-2826 */
+        for (int c = 0; c < 4; ++c)
+          if (d->d.nb_corner[c] >= 0)
+            fi[PHI(pos(corprev_dst[c][0], ni, 0), pos(corprev_dst[c][1], nj, 0),
+                   pos(corprev_dst[c][2], nk, 0))] = d->rc_m[c + 1];
+        for (int e = 0; e < 6; ++e)
+          if (d->d.nb_edge[e] >= 0) {
+            int len = edge_len(e, ni, nj, nk);
+            for (int nn = 2; nn <= len - 1; ++nn)
+              fi[PHI(pos(edgprev_dst[e][0], ni, nn), pos(edgprev_dst[e][1], nj, nn),
+                     pos(edgprev_dst[e][2], nk, nn))] = d->re_m[e + 1][nn];
+          }
+        for (int c = 0; c < 4; ++c)
+          if (d->d.nb_corner[4 + c] >= 0)
+            fi[PHI(pos(cornext_dst[c][0], ni, 0), pos(cornext_dst[c][1], nj, 0),
+                   pos(cornext_dst[c][2], nk, 0))] = d->rc_p[c + 1];
+        for (int e = 0; e < 6; ++e)
+          if (d->d.nb_edge[6 + e] >= 0) {
+            int len = edge_len(e, ni, nj, nk);
+            for (int nn = 2; nn <= len - 1; ++nn)
+              fi[PHI(pos(edgnext_dst[e][0], ni, nn), pos(edgnext_dst[e][1], nj, nn),
+                     pos(edgnext_dst[e][2], nk, nn))] = d->re_p[e + 1][nn];
+          }
+      }
+    }
+  }
+  or_mgbound(m, g);                        /* :2830 */
+  if (m->periodic) or_exchbc_mgpp(m, g);   /* :2832 */
+}
+
+/* ------------------------------------------------------------ exchbc_mgpp */
+void or_exchbc_mgpp(or_mg* m, int g) { /* exchangepp.for:2837-3454 */
+  for (int ax = 0; ax < 3; ++ax) {
+    /* pack (and single-block wrap) loop */
+    for (int ib = 0; ib < m->nbp; ++ib) {
+      or_dom* d = &m->dom[ib];
+      if (!(d->d.bc[2 * ax] == 5 || d->d.bc[2 * ax + 1] == 5)) continue;
+      int ni, nj, nk;
+      lev_dims(d, g, &ni, &nj, &nk);
+      int64_t nij = (int64_t)ni * nj, nijk = d->faz[g] - (int64_t)ni * nj * nk;
+      double* fi = d->cof;
+      int prev = d->d.nb_face[2 * ax], next = d->d.nb_face[2 * ax + 1];
+      if (prev < 0) {
+        if (next < 0) {
+          if (ax == 0) { for (int k = 1; k <= nk; ++k) for (int j = 1; j <= nj; ++j) fi[PHI(1, j, k)] = fi[PHI(ni - 1, j, k)]; }
+          else if (ax == 1) { for (int k = 1; k <= nk; ++k) for (int i = 1; i <= ni; ++i) fi[PHI(i, 1, k)] = fi[PHI(i, nj - 1, k)]; }
+          else { for (int j = 1; j <= nj; ++j) for (int i = 1; i <= ni; ++i) fi[PHI(i, j, 1)] = fi[PHI(i, j, nk - 1)]; }
+        } else {
+          int pc = d->d.nb_periodic[2 * ax];
+          if (pc >= 0) {
+            double* rb = m->dom[pc].recvb_p1;
+            if (ax == 0) { for (int k = 1; k <= nk; ++k) for (int j = 1; j <= nj; ++j) rb[(k - 1) * nj + j] = fi[PHI(2, j, k)]; }
+            else if (ax == 1) { for (int k = 1; k <= nk; ++k) for (int i = 1; i <= ni; ++i) rb[(k - 1) * ni + i] = fi[PHI(i, 2, k)]; }
+            else { for (int j = 1; j <= nj; ++j) for (int i = 1; i <= ni; ++i) rb[(j - 1) * ni + i] = fi[PHI(i, j, 2)]; }
+          }
+        }
+      }
+      if (next < 0) {
+        if (prev < 0) {
+          if (ax == 0) { for (int k = 1; k <= nk; ++k) for (int j = 1; j <= nj; ++j) fi[PHI(ni, j, k)] = fi[PHI(2, j, k)]; }
+          else if (ax == 1) { for (int k = 1; k <= nk; ++k) for (int i = 1; i <= ni; ++i) fi[PHI(i, nj, k)] = fi[PHI(i, 2, k)]; }
+          else { for (int j = 1; j <= nj; ++j) for (int i = 1; i <= ni; ++i) fi[PHI(i, j, nk)] = fi[PHI(i, j, 2)]; }
+        } else {
+          int pc = d->d.nb_periodic[2 * ax + 1];
+          if (pc >= 0) {
+            double* rb = m->dom[pc].recvb_m1;
+            if (ax == 0) { for (int k = 1; k <= nk; ++k) for (int j = 1; j <= nj; ++j) rb[(k - 1) * nj + j] = fi[PHI(ni - 1, j, k)]; }
+            else if (ax == 1) { for (int k = 1; k <= nk; ++k) for (int i = 1; i <= ni; ++i) rb[(k - 1) * ni + i] = fi[PHI(i, nj - 1, k)]; }
+            else { for (int j = 1; j <= nj; ++j) for (int i = 1; i <= ni; ++i) rb[(j - 1) * ni + i] = fi[PHI(i, j, nk - 1)]; }
+          }
+        }
+      }
+    }
+    /* unpack loop */
+    for (int ib = 0; ib < m->nbp; ++ib) {
+      or_dom* d = &m->dom[ib];
+      if (!(d->d.bc[2 * ax] == 5 || d->d.bc[2 * ax + 1] == 5)) continue;
+      int ni, nj, nk;
+      lev_dims(d, g, &ni, &nj, &nk);
+      int64_t nij = (int64_t)ni * nj, nijk = d->faz[g] - (int64_t)ni * nj * nk;
+      double* fi = d->cof;
+      int prev = d->d.nb_face[2 * ax], next = d->d.nb_face[2 * ax + 1];
+      if (prev < 0 && next >= 0 && d->d.nb_periodic[2 * ax] >= 0) {
+        const double* rb = d->recvb_m1;
+        if (ax == 0) { for (int k = 1; k <= nk; ++k) for (int j = 1; j <= nj; ++j) fi[PHI(1, j, k)] = rb[(k - 1) * nj + j]; }
+        else if (ax == 1) { for (int k = 1; k <= nk; ++k) for (int i = 1; i <= ni; ++i) fi[PHI(i, 1, k)] = rb[(k - 1) * ni + i]; }
+        else { for (int j = 1; j <= nj; ++j) for (int i = 1; i <= ni; ++i) fi[PHI(i, j, 1)] = rb[(j - 1) * ni + i]; }
+      }
+      if (next < 0 && prev >= 0 && d->d.nb_periodic[2 * ax + 1] >= 0) {
+        const double* rb = d->recvb_p1;
+        if (ax == 0) { for (int k = 1; k <= nk; ++k) for (int j = 1; j <= nj; ++j) fi[PHI(ni, j, k)] = rb[(k - 1) * nj + j]; }
+        else if (ax == 1) { for (int k = 1; k <= nk; ++k) for (int i = 1; i <= ni; ++i) fi[PHI(i, nj, k)] = rb[(k - 1) * ni + i]; }
+        else { for (int j = 1; j <= nj; ++j) for (int i = 1; i <= ni; ++i) fi[PHI(i, j, nk)] = rb[(j - 1) * ni + i]; }
+      }
+    }
+  }
+}
+
+/* ---------------------------------------------------------------- mgrelax */
+static void relax_block_rbgs(or_dom* d, int g, int colour) {
+  int ni, nj, nk;
+  lev_dims(d, g, &ni, &nj, &nk);
+  int64_t nij = (int64_t)ni * nj, nijk = d->faz[g] - (int64_t)ni * nj * nk;
+  int64_t nij2 = (int64_t)(ni - 2) * (nj - 2), incr = nij2 * (nk - 2);
+  double* c = d->cof;
+  int64_t faz = d->faz[g];
+#pragma omp parallel for num_threads(g_threads) schedule(static) if (g_threads > 1)
+  for (int k = 2; k <= nk - 1; ++k)
+    for (int j = 2; j <= nj - 1; ++j)
+      for (int i = 2; i <= ni - 1; ++i) {
+        if ((i + j + k) % 2 != colour) continue;
+        int64_t ijkphi = PHI(i, j, k);
+        int64_t w = faz + (k - 2) * nij2 + (int64_t)(i - 2) * (nj - 2) + (j - 1);
+        c[ijkphi] = (c[w + 7 * incr] -
+                     (c[w] * c[ijkphi - nj] + c[w + incr] * c[ijkphi + nj] +
+                      c[w + 2 * incr] * c[ijkphi - 1] + c[w + 3 * incr] * c[ijkphi + 1] +
+                      c[w + 4 * incr] * c[ijkphi - nij] + c[w + 5 * incr] * c[ijkphi + nij])) /
+                    c[w + 6 * incr];
+      }
+}
+
+static void relax_block_lex(or_dom* d, int g) { /* mgsolver.for:407-432 */
+  int ni, nj, nk;
+  lev_dims(d, g, &ni, &nj, &nk);
+  int64_t nij = (int64_t)ni * nj, nijk = d->faz[g] - (int64_t)ni * nj * nk;
+  int64_t nij2 = (int64_t)(ni - 2) * (nj - 2), incr = nij2 * (nk - 2);
+  double* c = d->cof;
+  int64_t faz = d->faz[g];
+  for (int k = 2; k <= nk - 1; ++k)
+    for (int j = 2; j <= nj - 1; ++j)
+      for (int i = 2; i <= ni - 1; ++i) {
+        int64_t ijkphi = PHI(i, j, k);
+        int64_t w = faz + (k - 2) * nij2 + (int64_t)(i - 2) * (nj - 2) + (j - 1);
+        c[ijkphi] = (c[w + 7 * incr] -
+                     (c[w] * c[ijkphi - nj] + c[w + incr] * c[ijkphi + nj] +
+                      c[w + 2 * incr] * c[ijkphi - 1] + c[w + 3 * incr] * c[ijkphi + 1] +
+                      c[w + 4 * incr] * c[ijkphi - nij] + c[w + 5 * incr] * c[ijkphi + nij])) /
+                    c[w + 6 * incr];
+      }
+}
+
+static void relax_block_tdma(or_dom* d, int g, double* a, double* cc, int ngg) {
+  /* mgsolver.for:434-549 */
+  int ni, nj, nk;
+  lev_dims(d, g, &ni, &nj, &nk);
+  int64_t nij = (int64_t)ni * nj, nijk = d->faz[g] - (int64_t)ni * nj * nk;
+  int64_t nij2 = (int64_t)(ni - 2) * (nj - 2), incr = nij2 * (nk - 2);
+  double* c = d->cof;
+  int64_t faz = d->faz[g];
+  for (int q = 0; q <= ngg; ++q) { a[q] = 0.0; cc[q] = 0.0; }
+#define WIDX(i, j, k) (faz + (int64_t)((k)-2) * nij2 + (int64_t)((i)-2) * (nj - 2) + ((j)-1))
+  /* j-lines */
+  for (int k = 2; k <= nk - 1; ++k)
+    for (int i = 2; i <= ni - 1; ++i) {
+      cc[1] = c[PHI(i, 1, k)];
+      for (int j = 2; j <= nj - 1; ++j) {
+        int64_t p = PHI(i, j, k), w = WIDX(i, j, k);
+        double apr = 1.0 / (c[w + 6 * incr] - c[w + 2 * incr] * a[j - 1]);
+        a[j] = c[w + 3 * incr] * apr;
+        cc[j] = (c[w + 7 * incr] - c[w + incr] * c[p + nj] - c[w] * c[p - nj] -
+                 c[w + 5 * incr] * c[p + nij] - c[w + 4 * incr] * c[p - nij] -
+                 c[w + 2 * incr] * cc[j - 1]) * apr;
+      }
+      for (int j = nj - 1; j >= 2; --j) {
+        int64_t p = PHI(i, j, k);
+        c[p] = (cc[j] - a[j] * c[p + 1]);
+      }
+    }
+  /* i-lines */
+  for (int k = 2; k <= nk - 1; ++k)
+    for (int j = 2; j <= nj - 1; ++j) {
+      cc[1] = c[PHI(1, j, k)];
+      for (int i = 2; i <= ni - 1; ++i) {
+        int64_t p = PHI(i, j, k), w = WIDX(i, j, k);
+        double apr = 1.0 / (c[w + 6 * incr] - c[w] * a[i - 1]);
+        a[i] = c[w + incr] * apr;
+        cc[i] = (c[w + 7 * incr] - c[w + 3 * incr] * c[p + 1] - c[w + 2 * incr] * c[p - 1] -
+                 c[w + 5 * incr] * c[p + nij] - c[w + 4 * incr] * c[p - nij] -
+                 c[w] * cc[i - 1]) * apr;
+      }
+      for (int i = ni - 1; i >= 2; --i) {
+        int64_t p = PHI(i, j, k);
+        c[p] = (cc[i] - a[i] * c[p + nj]);
+      }
+    }
+  /* k-lines */
+  for (int i = 2; i <= ni - 1; ++i)
+    for (int j = 2; j <= nj - 1; ++j) {
+      cc[1] = c[PHI(i, j, 1)];
+      for (int k = 2; k <= nk - 1; ++k) {
+        int64_t p = PHI(i, j, k), w = WIDX(i, j, k);
+        double apr = 1.0 / (c[w + 6 * incr] - c[w + 4 * incr] * a[k - 1]);
+        a[k] = c[w + 5 * incr] * apr;
+        cc[k] = (c[w + 7 * incr] - c[w + 3 * incr] * c[p + 1] - c[w + 2 * incr] * c[p - 1] -
+                 c[w + incr] * c[p + nj] - c[w] * c[p - nj] - c[w + 4 * incr] * cc[k - 1]) * apr;
+      }
+      for (int k = nk - 1; k >= 2; --k) {
+        int64_t p = PHI(i, j, k);
+        c[p] = (cc[k] - a[k] * c[p + nij]);
+      }
+    }
+#undef WIDX
+}
+
+void or_mgrelax(or_mg* m, int g, int it) { /* mgsolver.for:374-621 */
+  double* a = NULL;
+  double* cc = NULL;
+  if (m->mg_itrsch == 2) {
+    a = (double*)calloc((size_t)m->ngg + 1, sizeof(double));
+    cc = (double*)calloc((size_t)m->ngg + 1, sizeof(double));
+  }
+  for (int itr = 1; itr <= it; ++itr) {
+    for (int ib = 0; ib < m->nbp; ++ib) {
+      or_dom* d = &m->dom[ib];
+      if (m->mg_itrsch == 1) {
+        relax_block_lex(d, g);
+      } else if (m->mg_itrsch == 2) {
+        relax_block_tdma(d, g, a, cc, m->ngg);
+      } else {
+        relax_block_rbgs(d, g, 0); /* MOD(i+j+k,2)==0, :553-578 */
+        relax_block_rbgs(d, g, 1); /* MOD(i+j+k,2)==1, :580-605 */
+      }
+    }
+    or_mgbound(m, g);     /* :614 */
+    or_exchangepp(m, g);  /* :615 */
+  }
+  free(a);
+  free(cc);
+}
+
+/* ---------------------------------------------------------------- mgrestr */
+void or_mgrestr(or_mg* m, int glevel) { /* mgsolver.for:623-766 */
+  for (int ib = 0; ib < m->nbp; ++ib) {
+    or_dom* d = &m->dom[ib];
+    int nic, njc, nkc;
+    lev_dims(d, glevel, &nic, &njc, &nkc);
+    int64_t nijc2 = (int64_t)(nic - 2) * (njc - 2);
+    int64_t incr_c = nijc2 * (nkc - 2);
+    {
+      int64_t base = d->faz[glevel] - (int64_t)nic * njc * nkc;
+      for (int64_t q = 1; q <= (int64_t)nic * njc * nkc; ++q) d->cof[base + q] = 0.0; /* :655-662 */
+      for (int64_t q = 0; q < incr_c; ++q) d->cof[d->faz[glevel] + 1 + q + 7 * incr_c] = 0.0; /* :664-672 */
+    }
+    int nif, njf, nkf;
+    int clamp = glevel > d->ngrid;
+    if (clamp) { nif = nic; njf = njc; nkf = nkc; }
+    else {
+      int gl = glevel;
+      nif = d->d.n[0] / ipow2(gl - 2) + 2;
+      njf = d->d.n[1] / ipow2(gl - 2) + 2;
+      nkf = d->d.n[2] / ipow2(gl - 2) + 2;
+    }
+    int64_t nij = (int64_t)nif * njf, nj = njf;
+    int64_t nijk = d->faz[glevel - 1] - (int64_t)nif * njf * nkf;
+    int64_t nijf2 = (int64_t)(nif - 2) * (njf - 2), incr_f = nijf2 * (nkf - 2);
+    /* resf(nif,njf,nkf), Fortran column-major: (i,j,k) -> i-1 + nif*(j-1 + njf*(k-1)) */
+    double* resf = (double*)calloc((size_t)nif * njf * nkf, sizeof(double));
+#define RESF(i, j, k) resf[((int64_t)((k)-1) * njf + ((j)-1)) * nif + ((i)-1)]
+    const double* c = d->cof;
+    int64_t fazf = d->faz[glevel - 1];
+#pragma omp parallel for num_threads(g_threads) schedule(static) if (g_threads > 1)
+    for (int k = 2; k <= nkf - 1; ++k)
+      for (int i = 2; i <= nif - 1; ++i)
+        for (int j = 2; j <= njf - 1; ++j) {
+          int64_t p = PHI(i, j, k);
+          int64_t w = fazf + (k - 2) * nijf2 + (int64_t)(i - 2) * (njf - 2) + (j - 1);
+          RESF(i, j, k) = c[w + 7 * incr_f] -
+                          (c[w] * c[p - njf] + c[w + incr_f] * c[p + njf] +
+                           c[w + 2 * incr_f] * c[p - 1] + c[w + 3 * incr_f] * c[p + 1] +
+                           c[w + 4 * incr_f] * c[p - nij] + c[w + 5 * incr_f] * c[p + nij] +
+                           c[w + 6 * incr_f] * c[p]);
+        }
+    double* cw = d->cof;
+    for (int k = 2; k <= nkc - 1; ++k)
+      for (int i = 2; i <= nic - 1; ++i)
+        for (int j = 2; j <= njc - 1; ++j) {
+          int64_t su = d->faz[glevel] + (k - 2) * nijc2 + (int64_t)(i - 2) * (njc - 2) + (j - 1) + 7 * incr_c;
+          if (clamp) {
+            cw[su] = RESF(i, j, k); /* :724-737 */
+          } else { /* :741-756 */
+            cw[su] = 0.125 * (RESF(2 * i - 2, 2 * j - 2, 2 * k - 2) + RESF(2 * i - 1, 2 * j - 2, 2 * k - 2) +
+                              RESF(2 * i - 2, 2 * j - 1, 2 * k - 2) + RESF(2 * i - 1, 2 * j - 1, 2 * k - 2) +
+                              RESF(2 * i - 2, 2 * j - 2, 2 * k - 1) + RESF(2 * i - 1, 2 * j - 2, 2 * k - 1) +
+                              RESF(2 * i - 2, 2 * j - 1, 2 * k - 1) + RESF(2 * i - 1, 2 * j - 1, 2 * k - 1));
+          }
+        }
+#undef RESF
+    free(resf);
+  }
+}
+
+/* ----------------------------------------------------------------- mgcorr */
+void or_mgcorr(or_mg* m, int glevel) { /* mgsolver.for:768-910 */
+  for (int ib = 0; ib < m->nbp; ++ib) {
+    or_dom* d = &m->dom[ib];
+    int nif, njf, nkf;
+    lev_dims(d, glevel, &nif, &njf, &nkf);
+    int64_t nijf = (int64_t)nif * njf, nijkf = (int64_t)nif * njf * nkf;
+    int nic, njc, nkc;
+    int clamp = glevel >= d->ngrid;
+    if (clamp) { nic = nif; njc = njf; nkc = nkf; }
+    else {
+      int gl = glevel;
+      nic = d->d.n[0] / ipow2(gl) + 2;
+      njc = d->d.n[1] / ipow2(gl) + 2;
+      nkc = d->d.n[2] / ipow2(gl) + 2;
+    }
+    int64_t nijc = (int64_t)nic * njc, nijkc = (int64_t)nic * njc * nkc;
+    double* c = d->cof;
+    int64_t fazc = d->faz[glevel + 1], fazf = d->faz[glevel];
+    if (clamp) { /* :812-824 */
+      for (int kc = 1; kc <= nkc; ++kc)
+        for (int ic = 1; ic <= nic; ++ic)
+          for (int jc = 1; jc <= njc; ++jc) {
+            int64_t ijkc = (kc - 1) * nijc + (int64_t)(ic - 1) * njc + jc + fazc - nijkc;
+            int64_t ijkf = (kc - 1) * nijf + (int64_t)(ic - 1) * njf + jc + fazf - nijkf;
+            c[ijkf] = c[ijkf] + c[ijkc];
+          }
+    } else { /* :828-896 */
+#pragma omp parallel for num_threads(g_threads) schedule(static) if (g_threads > 1)
+      for (int kc = 1; kc <= nkc - 1; ++kc) {
+        int k = 2 * kc - 1;
+        for (int ic = 1; ic <= nic - 1; ++ic) {
+          int i = 2 * ic - 1;
+          for (int jc = 1; jc <= njc - 1; ++jc) {
+            int j = 2 * jc - 1;
+            int64_t q = (kc - 1) * nijc + (int64_t)(ic - 1) * njc + jc + fazc - nijkc;
+            int64_t f = (int64_t)(k - 1) * nijf + (int64_t)(i - 1) * njf + j + fazf - nijkf;
+            double c0 = c[q], cj = c[q + 1], ck = c[q + nijc], cjk = c[q + nijc + 1];
+            double ci = c[q + njc], cij = c[q + njc + 1], cik = c[q + njc + nijc],
+                   cijk = c[q + 1 + njc + nijc];
+            c[f] = c[f] + (27.0 * c0 + 9.0 * cj + 9.0 * ck + 3.0 * cjk + 9.0 * ci + 3.0 * cij +
+                           3.0 * cik + 1.0 * cijk) / 64.0;
+            c[f + njf] = c[f + njf] + (9.0 * c0 + 3.0 * cj + 3.0 * ck + 1.0 * cjk + 27.0 * ci +
+                                       9.0 * cij + 9.0 * cik + 3.0 * cijk) / 64.0;
+            c[f + 1] = c[f + 1] + (9.0 * c0 + 27.0 * cj + 3.0 * ck + 9.0 * cjk + 3.0 * ci +
+                                   9.0 * cij + 1.0 * cik + 3.0 * cijk) / 64.0;
+            c[f + nijf] = c[f + nijf] + (9.0 * c0 + 3.0 * cj + 27.0 * ck + 9.0 * cjk + 3.0 * ci +
+                                         1.0 * cij + 9.0 * cik + 3.0 * cijk) / 64.0;
+            c[f + njf + 1] = c[f + njf + 1] + (3.0 * c0 + 9.0 * cj + 1.0 * ck + 3.0 * cjk +
+                                               9.0 * ci + 27.0 * cij + 3.0 * cik + 9.0 * cijk) / 64.0;
+            c[f + nijf + njf] = c[f + nijf + njf] + (3.0 * c0 + 1.0 * cj + 9.0 * ck + 3.0 * cjk +
+                                                     9.0 * ci + 3.0 * cij + 27.0 * cik + 9.0 * cijk) / 64.0;
+            c[f + nijf + 1] = c[f + nijf + 1] + (3.0 * c0 + 9.0 * cj + 9.0 * ck + 27.0 * cjk +
+                                                 1.0 * ci + 3.0 * cij + 3.0 * cik + 9.0 * cijk) / 64.0;
+            c[f + nijf + njf + 1] = c[f + nijf + njf + 1] + (1.0 * c0 + 3.0 * cj + 3.0 * ck + 9.0 * cjk +
+                                                             3.0 * ci + 9.0 * cij + 9.0 * cik + 27.0 * cijk) / 64.0;
+          }
+        }
+      }
+    }
+  }
+  or_mgbound(m, glevel); /* :907 */
+}
+
+/* ----------------------------------------------------------------- mgkcyc */
+void or_vcycle(or_mg* m) { /* mgsolver.for:272-352 */
+  int L = m->ngrd_gl;
+  int kount[MAXLEV + 2];
+  int glevel = 1, kcycle = 1, nrel;
+  or_mgrelax(m, 1, m->irestr);
+  if (L == 1) goto post;
+  or_mgrestr(m, glevel + 1);
+  for (int l = 1; l <= L; ++l) kount[l] = 0;
+  glevel = glevel + 1;
+  nrel = m->irestr;
+  for (;;) {
+    if (glevel == 1) goto post;
+    kount[glevel] = kount[glevel] + 1;
+    or_mgrelax(m, glevel, nrel);
+    if (kount[glevel] == kcycle + 1) {
+      or_mgcorr(m, glevel - 1);
+      kount[glevel] = 0;
+      glevel = glevel - 1;
+      nrel = m->iproln;
+    } else if (glevel < L) {
+      or_mgrestr(m, glevel + 1);
+      glevel = glevel + 1;
+      nrel = m->irestr;
+    } else {
+      or_mgrelax(m, glevel, m->iproln);
+      or_mgcorr(m, glevel - 1);
+      nrel = m->iproln;
+      glevel = L - 1;
+    }
+  }
+post:
+  or_mgrelax(m, 1, m->iproln);
+}
+
+void or_mgkcyc(or_mg* m, double* const* pp, const double* const* su) {
+  for (int ib = 0; ib < m->nbp; ++ib) { /* :239-266 */
+    or_put_phi(m, 1, ib, pp[ib]);
+    or_put_rhs(m, 1, ib, su[ib]);
+  }
+  or_vcycle(m);
+  for (int ib = 0; ib < m->nbp; ++ib) or_get_phi(m, 1, ib, pp[ib]); /* :354-367 */
+}
+
+/* -------------------------------------------------------- outer iteration */
+double or_residual(or_mg* m, double* const* p, const double* const* b,
+                   double* const* r, double* bnorm2, double* rinf) {
+  /* p's ghosts: the level-1 exchangepp (faces, then mgbound == pbound,
+   * press.for:146-207) gives every face ghost the value exchange(4) gives;
+   * edge/corner ghosts do not enter the 7-point operator. */
+  for (int ib = 0; ib < m->nbp; ++ib) or_put_phi(m, 1, ib, p[ib]);
+  or_exchangepp(m, 1);
+  double rr = 0.0, bb = 0.0, rmax = 0.0;
+  for (int ib = 0; ib < m->nbp; ++ib) {
+    or_dom* d = &m->dom[ib];
+    or_get_phi(m, 1, ib, p[ib]);
+    int ni, nj, nk;
+    lev_dims(d, 1, &ni, &nj, &nk);
+    int64_t nij = (int64_t)ni * nj, nijk = d->faz[1] - (int64_t)ni * nj * nk;
+    int64_t nij2 = (int64_t)(ni - 2) * (nj - 2), incr = nij2 * (nk - 2);
+    const double* c = d->cof;
+    double dv = d->d.h[0] * d->d.h[1] * d->d.h[2];
+    double brr = 0.0, bbb = 0.0, bmax = 0.0;
+#pragma omp parallel for num_threads(g_threads) schedule(static) reduction(+ : brr, bbb) reduction(max : bmax) if (g_threads > 1)
+    for (int k = 2; k <= nk - 1; ++k)
+      for (int j = 2; j <= nj - 1; ++j)
+        for (int i = 2; i <= ni - 1; ++i) {
+          int64_t ph = PHI(i, j, k);
+          int64_t w = d->faz[1] + (k - 2) * nij2 + (int64_t)(i - 2) * (nj - 2) + (j - 1);
+          int64_t q = ((int64_t)(k - 2) * (nj - 2) + (j - 2)) * (ni - 2) + (i - 2);
+          double bv = b[ib][q];
+          double rv = bv - (c[w] * c[ph - nj] + c[w + incr] * c[ph + nj] + c[w + 2 * incr] * c[ph - 1] +
+                            c[w + 3 * incr] * c[ph + 1] + c[w + 4 * incr] * c[ph - nij] +
+                            c[w + 5 * incr] * c[ph + nij] + c[w + 6 * incr] * c[ph]);
+          if (r) r[ib][q] = rv;
+          brr += rv * rv;
+          bbb += bv * bv;
+          double a = fabs(rv) * dv;
+          if (a > bmax) bmax = a;
+        }
+    rr += brr;
+    bb += bbb;
+    if (bmax > rmax) rmax = bmax;
+  }
+  if (bnorm2) *bnorm2 = bb;
+  if (rinf) *rinf = rmax;
+  return rr;
+}
+
+int or_solve(or_mg* m, double* const* p, const double* const* b, double tol,
+             int maxcy, int stop_rule, int* cycles, double* relres,
+             double* history) {
+  /* newsolv_mg.for:17-57: the outer loop is defect correction.  Each
+   * iteration runs one V-cycle on pp from zero with the current defect as
+   * right-hand side, then p += pp and the defect is recomputed in FP64. */
+  int nb = m->nbp;
+  double** r = (double**)calloc((size_t)nb, sizeof(double*));
+  double** pp = (double**)calloc((size_t)nb, sizeof(double*));
+  for (int ib = 0; ib < nb; ++ib) {
+    const or_dom* d = &m->dom[ib];
+    size_t ni = (size_t)d->d.n[0], nj = (size_t)d->d.n[1], nk = (size_t)d->d.n[2];
+    r[ib] = (double*)calloc(ni * nj * nk, sizeof(double));
+    pp[ib] = (double*)calloc((ni + 2) * (nj + 2) * (nk + 2), sizeof(double));
+  }
+  double bb, rinf;
+  double rr = or_residual(m, p, b, r, &bb, &rinf);
+  double bn = sqrt(bb) > 0 ? sqrt(bb) : 1.0;
+  double rel = sqrt(rr) / bn;
+  if (history) history[0] = rel;
+  int iter = 0, status = 1;
+  if (stop_rule == 0 && rel <= tol) status = 0;
+  while (status != 0 && iter < maxcy) {
+    for (int ib = 0; ib < nb; ++ib) {
+      const or_dom* d = &m->dom[ib];
+      size_t n = (size_t)(d->d.n[0] + 2) * (d->d.n[1] + 2) * (d->d.n[2] + 2);
+      memset(pp[ib], 0, n * sizeof(double)); /* newsolv_mg.for:20-22, :45 */
+    }
+    or_mgkcyc(m, pp, (const double* const*)r);
+    ++iter;
+    for (int ib = 0; ib < nb; ++ib) { /* p = p + (pp - ppref), ppref = 0, :39-49 */
+      const or_dom* d = &m->dom[ib];
+      size_t n = (size_t)(d->d.n[0] + 2) * (d->d.n[1] + 2) * (d->d.n[2] + 2);
+      for (size_t q = 0; q < n; ++q) p[ib][q] = (p[ib][q] + (pp[ib][q] - 0.0));
+    }
+    rr = or_residual(m, p, b, r, NULL, &rinf);
+    rel = sqrt(rr) / bn;
+    if (history) history[iter] = rel;
+    if (stop_rule == 0 && rel <= tol) status = 0;
+    if (stop_rule == 1 && rinf < tol && iter > 1) status = 0; /* :57 */
+    if (!isfinite(rel)) { status = 2; break; }
+  }
+  if (cycles) *cycles = iter;
+  if (relres) *relres = rel;
+  for (int ib = 0; ib < nb; ++ib) { free(r[ib]); free(pp[ib]); }
+  free(r);
+  free(pp);
+  return status;
+}
+
+/* --------------------------------------------------------------- topology */
+int or_topology(int nblocks, const int32_t* ext, const int32_t* bc,
+                or_block_desc* out) {
+  /* read_infodom, alloc_dom.for:524-1200, on exact integer extents.
+   * ext[6*b + (0..5)] = xs, xe, ys, ye, zs, ze. */
+#define XS(b) ext[6 * (b) + 0]
+#define XE(b) ext[6 * (b) + 1]
+#define YS(b) ext[6 * (b) + 2]
+#define YE(b) ext[6 * (b) + 3]
+#define ZS(b) ext[6 * (b) + 4]
+#define ZE(b) ext[6 * (b) + 5]
+  int xst = XS(0), xen = XE(0), yst = YS(0), yen = YE(0), zst = ZS(0), zen = ZE(0);
+  for (int b = 1; b < nblocks; ++b) {
+    if (XS(b) < xst) xst = XS(b);
+    if (XE(b) > xen) xen = XE(b);
+    if (YS(b) < yst) yst = YS(b);
+    if (YE(b) > yen) yen = YE(b);
+    if (ZS(b) < zst) zst = ZS(b);
+    if (ZE(b) > zen) zen = ZE(b);
+  }
+  for (int a = 0; a < nblocks; ++a) {
+    or_block_desc* d = &out[a];
+    d->n[0] = XE(a) - XS(a);
+    d->n[1] = YE(a) - YS(a);
+    d->n[2] = ZE(a) - ZS(a);
+    d->origin[0] = XS(a);
+    d->origin[1] = YS(a);
+    d->origin[2] = ZS(a);
+    for (int q = 0; q < 6; ++q) { d->bc[q] = bc[q]; d->nb_face[q] = -1; d->nb_periodic[q] = -1; }
+    for (int q = 0; q < 8; ++q) d->nb_corner[q] = -1;
+    for (int q = 0; q < 12; ++q) d->nb_edge[q] = -1;
+    int say[6 + 8 + 12] = {0};
+    for (int b = 0; b < nblocks; ++b) {
+      if (b == a) continue;
+      int sy = YS(a) == YS(b) && YE(a) == YE(b), sz = ZS(a) == ZS(b) && ZE(a) == ZE(b),
+          sx = XS(a) == XS(b) && XE(a) == XE(b);
+      /* faces, :545-680 */
+      if (XS(a) == XE(b) && sy && sz) { d->nb_face[0] = b; say[0]++; }
+      if (XE(a) == XS(b) && sy && sz) { d->nb_face[1] = b; say[1]++; }
+      if (YS(a) == YE(b) && sx && sz) { d->nb_face[2] = b; say[2]++; }
+      if (YE(a) == YS(b) && sx && sz) { d->nb_face[3] = b; say[3]++; }
+      if (ZS(a) == ZE(b) && sx && sy) { d->nb_face[4] = b; say[4]++; }
+      if (ZE(a) == ZS(b) && sx && sy) { d->nb_face[5] = b; say[5]++; }
+      /* corners, :700-810 */
+      if (XS(a) == XE(b) && YS(a) == YE(b) && ZS(a) == ZE(b)) { d->nb_corner[0] = b; say[6]++; }
+      if (XS(a) == XE(b) && YE(a) == YS(b) && ZS(a) == ZE(b)) { d->nb_corner[1] = b; say[7]++; }
+      if (XE(a) == XS(b) && YE(a) == YS(b) && ZS(a) == ZE(b)) { d->nb_corner[2] = b; say[8]++; }
+      if (XE(a) == XS(b) && YS(a) == YE(b) && ZS(a) == ZE(b)) { d->nb_corner[3] = b; say[9]++; }
+      if (XE(a) == XS(b) && YE(a) == YS(b) && ZE(a) == ZS(b)) { d->nb_corner[4] = b; say[10]++; }
+      if (XE(a) == XS(b) && YS(a) == YE(b) && ZE(a) == ZS(b)) { d->nb_corner[5] = b; say[11]++; }
+      if (XS(a) == XE(b) && YS(a) == YE(b) && ZE(a) == ZS(b)) { d->nb_corner[6] = b; say[12]++; }
+      if (XS(a) == XE(b) && YE(a) == YS(b) && ZE(a) == ZS(b)) { d->nb_corner[7] = b; say[13]++; }
+      /* edges, :824-1040 */
+      if (XS(a) == XE(b) && ZS(a) == ZE(b) && sy) { d->nb_edge[0] = b; say[14]++; }
+      if (YE(a) == YS(b) && ZS(a) == ZE(b) && sx) { d->nb_edge[1] = b; say[15]++; }
+      if (XE(a) == XS(b) && ZS(a) == ZE(b) && sy) { d->nb_edge[2] = b; say[16]++; }
+      if (YS(a) == YE(b) && ZS(a) == ZE(b) && sx) { d->nb_edge[3] = b; say[17]++; }
+      if (XS(a) == XE(b) && YS(a) == YE(b) && sz) { d->nb_edge[4] = b; say[18]++; }
+      if (XS(a) == XE(b) && YE(a) == YS(b) && sz) { d->nb_edge[5] = b; say[19]++; }
+      if (XE(a) == XS(b) && ZE(a) == ZS(b) && sy) { d->nb_edge[6] = b; say[20]++; }
+      if (YS(a) == YE(b) && ZE(a) == ZS(b) && sx) { d->nb_edge[7] = b; say[21]++; }
+      if (XS(a) == XE(b) && ZE(a) == ZS(b) && sy) { d->nb_edge[8] = b; say[22]++; }
+      if (YE(a) == YS(b) && ZE(a) == ZS(b) && sx) { d->nb_edge[9] = b; say[23]++; }
+      if (XE(a) == XS(b) && YE(a) == YS(b) && sz) { d->nb_edge[10] = b; say[24]++; }
+      if (XE(a) == XS(b) && YS(a) == YE(b) && sz) { d->nb_edge[11] = b; say[25]++; }
+    }
+    for (int q = 0; q < 26; ++q)
+      if (say[q] > 1) return -1;
+  }
+  /* periodic partners, alloc_dom.for:1042-1200 */
+  for (int a = 0; a < nblocks; ++a) {
+    or_block_desc* d = &out[a];
+    for (int b = 0; b < nblocks; ++b) {
+      if (b == a) continue;
+      int sy = YS(a) == YS(b) && YE(a) == YE(b), sz = ZS(a) == ZS(b) && ZE(a) == ZE(b),
+          sx = XS(a) == XS(b) && XE(a) == XE(b);
+      if (bc[0] == 5 && d->nb_face[0] < 0 && xen == XE(b) && sy && sz) d->nb_periodic[0] = b;
+      if (bc[1] == 5 && d->nb_face[1] < 0 && xst == XS(b) && sy && sz) d->nb_periodic[1] = b;
+      if (bc[2] == 5 && d->nb_face[2] < 0 && yen == YE(b) && sx && sz) d->nb_periodic[2] = b;
+      if (bc[3] == 5 && d->nb_face[3] < 0 && yst == YS(b) && sx && sz) d->nb_periodic[3] = b;
+      if (bc[4] == 5 && d->nb_face[4] < 0 && zen == ZE(b) && sx && sy) d->nb_periodic[4] = b;
+      if (bc[5] == 5 && d->nb_face[5] < 0 && zst == ZS(b) && sx && sy) d->nb_periodic[5] = b;
+    }
+  }
+  return 0;
+#undef XS
+#undef XE
+#undef YS
+#undef YE
+#undef ZS
+#undef ZE
+}

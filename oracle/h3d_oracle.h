@@ -1,0 +1,108 @@
+/*
+ * h3d_oracle.h -- CPU oracle for the pressure-Poisson multigrid path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This is a plain-C restatement of the reference
+ * Hydro3D v7.0 multigrid routines, used by tests/, __graft_entry__.smoke()
+ * and the cpu_baseline leg of bench.py as the checker.  It is never linked
+ * into, loaded by, or called from the product library (hydro3d_b200).
+ *
+ * Parity pinning: the reference ships no golden vectors or known-answer
+ * tests for this path and cannot be built here (Fortran, no compiler).  The
+ * oracle is pinned by (a) golden fixtures produced from the reference's own
+ * Fortran source by the mechanical translator in oracle/fortran_ref.py
+ * (see oracle/Makefile target `ref`), and (b) algebraic properties
+ * (manufactured Neumann cosine modes, null space, symmetry).
+ *
+ * Every routine cites the reference file:line it restates.  Storage keeps the
+ * reference's per-block `cof` work array and its j-fastest level layout
+ * (mgsolver.for:62-66, 119-120), so lexicographic and line-TDMA orderings are
+ * the reference's own.
+ */
+#ifndef H3D_ORACLE_H
+#define H3D_ORACLE_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Same byte layout as h3d_block_desc in include/h3d_mg.h (kept separate so
+ * the oracle does not depend on the product headers). */
+typedef struct {
+  int32_t n[3];           /* interior cells i (x), j (y), k (z)              */
+  int32_t ttc[3];         /* host dims incl. ghosts (unused by the oracle)   */
+  int32_t pl;             /* host ghost width (unused by the oracle)         */
+  int32_t ngrid;          /* levels of this block                             */
+  double h[3];            /* dx, dy, dz                                       */
+  int32_t nb_face[6];     /* iprev inext jprev jnext kprev knext              */
+  int32_t nb_corner[8];   /* corprev1..4 cornext1..4                          */
+  int32_t nb_edge[12];    /* edgprev1..6 edgnext1..6                          */
+  int32_t nb_periodic[6]; /* per_ip per_in per_jp per_jn per_kp per_kn        */
+  int32_t bc[6];          /* bc_west bc_east bc_south bc_north bc_bottom bc_top */
+  int32_t rdiv;           /* refinement ratio (only 1 is supported)           */
+  int32_t origin[3];      /* global cell index of the first interior cell     */
+} or_block_desc;
+
+typedef struct or_mg or_mg;
+
+/* Create the solver state (localparameters.for:202-239 sizing). */
+or_mg* or_create(int nblocks, const or_block_desc* blocks, int ngrd_gl,
+                 int mg_itrsch, int irestr, int iproln, int lsm);
+void or_destroy(or_mg* m);
+int or_error(const or_mg* m); /* 0 if the configuration was accepted */
+
+/* Interior density of block ib, x-fastest (n_z, n_y, n_x). LSM only. */
+void or_set_density(or_mg* m, int ib, const double* dens);
+/* coeff, mgsolver.for:2-224 */
+void or_coeff(or_mg* m);
+
+/* Level-g iterate of block ib, canonical x-fastest (nz+2, ny+2, nx+2) incl.
+ * the one ghost layer; rhs is interior only (nz, ny, nx). */
+void or_put_phi(or_mg* m, int g, int ib, const double* a);
+void or_get_phi(const or_mg* m, int g, int ib, double* a);
+void or_put_rhs(or_mg* m, int g, int ib, const double* a);
+void or_get_rhs(const or_mg* m, int g, int ib, double* a);
+/* Coefficient slot s (0 aw,1 ae,2 as,3 an,4 ab,5 at,6 ap) interior-only. */
+void or_get_coef(const or_mg* m, int g, int ib, int s, double* a);
+
+/* Reference subroutines on the resident state. */
+void or_mgrelax(or_mg* m, int g, int it);   /* mgsolver.for:374-621 */
+void or_mgrestr(or_mg* m, int g);           /* mgsolver.for:623-766 */
+void or_mgcorr(or_mg* m, int g);            /* mgsolver.for:768-910 */
+void or_mgbound(or_mg* m, int g);           /* mgsolver.for:912-997 */
+void or_exchangepp(or_mg* m, int g);        /* exchangepp.for:2-2835 */
+void or_exchbc_mgpp(or_mg* m, int g);       /* exchangepp.for:2837-3454 */
+void or_vcycle(or_mg* m);                   /* mgkcyc control flow, mgsolver.for:272-352 */
+
+/* mgkcyc on level-1 arrays: pp (canonical with ghosts) in/out, su interior. */
+void or_mgkcyc(or_mg* m, double* const* pp, const double* const* su);
+
+/* r = b - A p on level 1 (FP64), with p's face ghosts filled first the way
+ * exchange(4)+pbound leave them.  p is canonical with ghosts (ghosts are
+ * rewritten), b and r interior-only.  Returns sum r^2; *bnorm2 = sum b^2;
+ * *rinf = max |r| * dV (the calmas rmax measure, press.for:61-63). */
+double or_residual(or_mg* m, double* const* p, const double* const* b,
+                   double* const* r, double* bnorm2, double* rinf);
+
+/* newsolv_mg outer loop (newsolv_mg.for:17-57) written as defect correction
+ * on b - A p.  stop_rule 0: ||r||2/||b||2 <= tol (checked before each cycle);
+ * stop_rule 1: reference rule rmax < tol .and. iter > 1 (checked after each
+ * cycle).  history (may be NULL) receives maxcy+1 relative residuals. */
+int or_solve(or_mg* m, double* const* p, const double* const* b, double tol,
+             int maxcy, int stop_rule, int* cycles, double* relres,
+             double* history);
+
+/* Block topology from integer extents: read_infodom neighbour discovery
+ * (alloc_dom.for:524-1200).  ext is nblocks x 6 (x0,x1,y0,y1,z0,z1) in global
+ * cell units; bc[6] global codes.  Fills nb_face/nb_corner/nb_edge/
+ * nb_periodic/bc/n/origin of each desc. Returns 0, or -1 on ambiguity. */
+int or_topology(int nblocks, const int32_t* ext, const int32_t* bc,
+                or_block_desc* out);
+
+/* OpenMP thread count used by the colour passes (1 = scalar). */
+void or_set_threads(int nthreads);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,53 @@
+"""CPU: the C-ABI library loads and exports every entry point of include/h3d_mg.h."""
+import os
+import re
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _declared():
+    txt = open(os.path.join(ROOT, "include", "h3d_mg.h")).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    return sorted(set(re.findall(r"\b(h3d_[a-z0-9_]+)\s*\(", txt)))
+
+
+def test_library_exports_every_declared_symbol(h3d):
+    L = h3d.lib()
+    names = _declared()
+    assert len(names) >= 20
+    missing = [n for n in names if not hasattr(L, n)]
+    assert not missing, missing
+
+
+def test_binding_covers_header(h3d):
+    from hydro3d_b200 import _lib
+    assert sorted(_lib.EXPORTS) == _declared()
+
+
+def test_strerror_and_create_errors(h3d):
+    import ctypes as C
+    from hydro3d_b200 import _lib
+    L = h3d.lib()
+    assert L.h3d_mg_strerror(_lib.H3D_ERR_NOT_CONVERGED) == b"not converged"
+    # a bad descriptor is rejected on the host before any device work
+    blocks = h3d.topology.block_grid((1, 1, 1), (12, 12, 12), [4] * 6, [0.1] * 3, 4)
+    d = _lib.MGDesc()
+    arr = (_lib.BlockDesc * 1)(*blocks)
+    d.nblocks, d.ngrd_gl, d.mg_itrsch, d.irestr, d.iproln, d.blocks = 1, 4, 3, 2, 1, arr
+    h = C.c_void_p()
+    assert L.h3d_mg_create(C.byref(h), C.byref(d)) == _lib.H3D_ERR_BAD_CONFIG  # 12 % 8 != 0
+    assert b"divisible" in L.h3d_mg_last_error(None)
+    d.ngrd_gl = 2
+    for b in arr:
+        b.ngrid = 2
+    d.mg_itrsch = 2
+    assert L.h3d_mg_create(C.byref(h), C.byref(d)) == _lib.H3D_ERR_BAD_CONFIG
+
+
+def test_product_does_not_touch_oracle():
+    # the product package must not import, link or load the oracle
+    for dp, _, fs in os.walk(os.path.join(ROOT, "hydro3d_b200")):
+        for f in fs:
+            if f.endswith((".py", ".cu", ".cpp", ".h", ".cuh")):
+                txt = open(os.path.join(dp, f)).read()
+                assert "oracle" not in txt.replace("oracle/", ""), f

@@ -1,0 +1,249 @@
+"""GPU parity: every reference routine on the CUDA path vs the oracle.
+
+The FP64 path is compared bit for bit (the library is built without FMA
+contraction and follows the reference's operand order); the FP32 path of the
+mixed-precision solver is compared with a relative tolerance of 2e-5.
+All calls go through the C ABI (hydro3d_b200 -> libh3dmg.so).
+"""
+import numpy as np
+import pytest
+
+from tests.helpers import mean_removed_rel, to_oracle_descs
+
+pytestmark = pytest.mark.gpu
+
+W, P = 4, 5
+LAYOUTS = [
+    ((1, 1, 1), (16, 16, 16), [W] * 6, 3),
+    ((2, 2, 2), (8, 16, 8), [P, P, W, W, W, W], 3),
+    ((3, 2, 2), (16, 8, 8), [W, W, P, P, W, W], 2),
+    ((2, 1, 3), (8, 8, 16), [P] * 6, 3),
+]
+FP32_RTOL = 2e-5
+
+
+def _pair(O, h3d, layout, precision="fp64", var=False, use_graph=False):
+    nblk, n, bc, ngrid = layout
+    blocks = h3d.topology.block_grid(nblk, n, bc, [1.0 / 32] * 3, ngrid)
+    s = h3d.MultigridSolver(blocks, ngrid, precision=precision, var_coef=var, use_graph=use_graph)
+    orc = O.Oracle(to_oracle_descs(O, blocks), ngrid, 3, 2, 1, lsm=var)
+    return blocks, s, orc
+
+
+def _rand_level(rng, s, orc, g, fields=("phi", "rhs")):
+    for ib in range(len(s.blocks)):
+        nz, ny, nx = s.level_dims(g, ib)
+        if "phi" in fields:
+            a = rng.standard_normal((nz + 2, ny + 2, nx + 2))
+            s.put_level(g, "phi", ib, a)
+            orc.put_phi(g, ib, a)
+        if "rhs" in fields:
+            r = rng.standard_normal((nz, ny, nx))
+            s.put_level(g, "rhs", ib, r)
+            orc.put_rhs(g, ib, r)
+
+
+def _assert_level(s, orc, g, field="phi", exact=True):
+    for ib in range(len(s.blocks)):
+        a = s.get_level(g, field, ib)
+        b = orc.get_phi(g, ib) if field == "phi" else orc.get_rhs(g, ib)
+        if exact:
+            assert np.array_equal(a, b), (g, ib, float(np.abs(a - b).max()))
+        else:
+            np.testing.assert_allclose(a, b, rtol=FP32_RTOL, atol=FP32_RTOL * np.abs(b).max())
+
+
+@pytest.mark.parametrize("layout", LAYOUTS)
+def test_mgrelax_bitexact(oracle_mod, h3d, layout):
+    blocks, s, orc = _pair(oracle_mod, h3d, layout)
+    s.coeff(); orc.coeff()
+    rng = np.random.default_rng(1)
+    for g in range(1, layout[3] + 1):
+        _rand_level(rng, s, orc, g)
+        s.mgrelax(g, 2)
+        orc.mgrelax(g, 2)
+        _assert_level(s, orc, g)
+    s.close()
+
+
+@pytest.mark.parametrize("layout", LAYOUTS)
+def test_mgrestr_mgcorr_bitexact(oracle_mod, h3d, layout):
+    blocks, s, orc = _pair(oracle_mod, h3d, layout)
+    s.coeff(); orc.coeff()
+    rng = np.random.default_rng(2)
+    for g in range(2, layout[3] + 1):
+        _rand_level(rng, s, orc, g - 1)
+        s.mgrestr(g)
+        orc.mgrestr(g)
+        _assert_level(s, orc, g, "rhs")
+        _assert_level(s, orc, g, "phi")
+        _rand_level(rng, s, orc, g, ("phi",))
+        _rand_level(rng, s, orc, g - 1, ("phi",))
+        s.mgcorr(g - 1)
+        orc.mgcorr(g - 1)
+        _assert_level(s, orc, g - 1)
+    s.close()
+
+
+@pytest.mark.parametrize("layout", LAYOUTS)
+def test_mgbound_exchangepp_bitexact(oracle_mod, h3d, layout):
+    blocks, s, orc = _pair(oracle_mod, h3d, layout)
+    s.coeff(); orc.coeff()
+    rng = np.random.default_rng(3)
+    _rand_level(rng, s, orc, 1)
+    s.mgbound(1); orc.mgbound(1)
+    _assert_level(s, orc, 1)
+    _rand_level(rng, s, orc, 2)
+    s.exchangepp(2); orc.exchangepp(2)
+    _assert_level(s, orc, 2)
+    s.close()
+
+
+@pytest.mark.parametrize("layout", LAYOUTS)
+def test_vcycle_bitexact(oracle_mod, h3d, layout):
+    blocks, s, orc = _pair(oracle_mod, h3d, layout)
+    s.coeff(); orc.coeff()
+    rng = np.random.default_rng(4)
+    _rand_level(rng, s, orc, 1)
+    s.vcycle(); orc.vcycle()
+    _assert_level(s, orc, 1)
+    s.vcycle(); orc.vcycle()
+    _assert_level(s, orc, 1)
+    s.close()
+
+
+def test_var_coef_bitexact(oracle_mod, h3d):
+    layout = ((2, 1, 2), (16, 16, 8), [W] * 6, 3)
+    blocks, s, orc = _pair(oracle_mod, h3d, layout, var=True)
+    rng = np.random.default_rng(5)
+    for ib, d in enumerate(blocks):
+        dens = h3d.host_field(d)
+        rho = np.exp(rng.uniform(0, np.log(1000.0), (d.n[2], d.n[1], d.n[0])))
+        h3d.interior(dens, d)[...] = rho
+        s.set_density(ib, dens)
+        orc.set_density(ib, rho)
+    s.coeff(); orc.coeff()
+    for g in (1, 2, 3):
+        _rand_level(rng, s, orc, g)
+        s.mgrelax(g, 1); orc.mgrelax(g, 1)
+        _assert_level(s, orc, g)
+    _rand_level(rng, s, orc, 1)
+    s.mgrestr(2); orc.mgrestr(2)
+    _assert_level(s, orc, 2, "rhs")
+    _rand_level(rng, s, orc, 1)
+    s.vcycle(); orc.vcycle()
+    _assert_level(s, orc, 1)
+    s.close()
+
+
+def test_fp32_kernels_close(oracle_mod, h3d):
+    layout = ((2, 2, 1), (16, 16, 16), [P, P, W, W, W, W], 3)
+    blocks, s, orc = _pair(oracle_mod, h3d, layout, precision="mixed")
+    s.coeff(); orc.coeff()
+    rng = np.random.default_rng(6)
+    _rand_level(rng, s, orc, 1)
+    s.mgrelax(1, 2); orc.mgrelax(1, 2)
+    _assert_level(s, orc, 1, exact=False)
+    _rand_level(rng, s, orc, 1)
+    s.mgrestr(2); orc.mgrestr(2)
+    _assert_level(s, orc, 2, "rhs", exact=False)
+    s.close()
+
+
+def _host_problem(h3d, blocks, seed, pl):
+    rng = np.random.default_rng(seed)
+    b, p, bc_, pc_ = [], [], [], []
+    for d in blocks:
+        bh = h3d.host_field(d)
+        bi = rng.standard_normal((d.n[2], d.n[1], d.n[0]))
+        h3d.interior(bh, d)[...] = bi
+        b.append(bh)
+        p.append(h3d.host_field(d))
+    # all-wall problems need a compatible rhs
+    if all(x != 5 for x in blocks[0].bc):
+        m = np.mean(np.concatenate([h3d.interior(x, d).ravel() for x, d in zip(b, blocks)]))
+        for x, d in zip(b, blocks):
+            h3d.interior(x, d)[...] -= m
+    return b, p
+
+
+@pytest.mark.parametrize("layout", [((1, 1, 1), (32, 32, 32), [W] * 6, 4),
+                                    ((2, 2, 2), (16, 16, 16), [P, P, W, W, W, W], 4)])
+def test_newsolv_matches_oracle(oracle_mod, h3d, layout):
+    nblk, n, bc, ngrid = layout
+    blocks = h3d.topology.block_grid(nblk, n, bc, [1.0 / 32] * 3, ngrid, pl=2)
+    b, p = _host_problem(h3d, blocks, 11, 2)
+    s = h3d.MultigridSolver(blocks, ngrid)
+    info = s.newsolv_mg(p, b, tol=1e-8, maxcy=300, history=True)
+    orc = oracle_mod.Oracle(to_oracle_descs(oracle_mod, blocks), ngrid)
+    orc.coeff()
+    from tests.helpers import canon_from_host, interior_of_host
+    ref = orc.solve([np.zeros((d.n[2] + 2, d.n[1] + 2, d.n[0] + 2)) for d in blocks],
+                    [interior_of_host(x, d) for x, d in zip(b, blocks)], tol=1e-8, maxcy=300)
+    assert info["converged"] and ref["status"] == 0
+    assert abs(info["cycles"] - ref["cycles"]) <= 2
+    got = [interior_of_host(x, d) for x, d in zip(p, blocks)]
+    want = [x[1:-1, 1:-1, 1:-1] for x in ref["p"]]
+    assert mean_removed_rel(got, want) <= 1e-7
+    np.testing.assert_allclose(info["history"], ref["history"], rtol=1e-9, atol=0)
+    s.close()
+
+
+def test_mgkcyc_host_fields(oracle_mod, h3d):
+    blocks = h3d.topology.block_grid((2, 1, 1), (16, 16, 16), [W] * 6, [1.0 / 32] * 3, 3, pl=3)
+    b, _ = _host_problem(h3d, blocks, 12, 3)
+    rng = np.random.default_rng(13)
+    pp = []
+    for d in blocks:
+        a = h3d.host_field(d)
+        a[...] = rng.standard_normal(a.shape)
+        pp.append(a)
+    outer = [a.copy() for a in pp]
+    s = h3d.MultigridSolver(blocks, 3)
+    s.mgkcyc(pp, b)
+    orc = oracle_mod.Oracle(to_oracle_descs(oracle_mod, blocks), 3)
+    orc.coeff()
+    from tests.helpers import canon_from_host, interior_of_host
+    got = orc.mgkcyc([canon_from_host(a, d) for a, d in zip(outer, blocks)],
+                     [interior_of_host(x, d) for x, d in zip(b, blocks)])
+    for a, g, o, d in zip(pp, got, outer, blocks):
+        assert np.array_equal(canon_from_host(a, d), g)
+        # layers beyond the first ghost layer are untouched
+        m = np.ones(a.shape, bool)
+        pl = d.pl
+        m[pl - 1:pl + d.n[2] + 1, pl - 1:pl + d.n[1] + 1, pl - 1:pl + d.n[0] + 1] = False
+        assert np.array_equal(a[m], o[m])
+    s.close()
+
+
+def test_graph_and_eager_identical(h3d):
+    blocks = h3d.topology.block_grid((2, 2, 1), (16, 16, 16), [P, P, W, W, W, W], [1.0 / 32] * 3, 4)
+    b, p = _host_problem(h3d, blocks, 14, 1)
+    out = []
+    for g in (True, False):
+        s = h3d.MultigridSolver(blocks, 4, use_graph=g)
+        pc = [x.copy() for x in p]
+        info = s.newsolv_mg(pc, b, tol=1e-9, maxcy=200)
+        out.append((pc, info["cycles"]))
+        s.close()
+    assert out[0][1] == out[1][1]
+    for a, c in zip(out[0][0], out[1][0]):
+        assert np.array_equal(a, c)
+
+
+def test_mixed_precision_error_vs_fp64(oracle_mod, h3d):
+    blocks = h3d.topology.block_grid((4, 2, 2), (16, 16, 16), [W] * 6, [1.0 / 32] * 3, 5)
+    b, p = _host_problem(h3d, blocks, 15, 1)
+    orc = oracle_mod.Oracle(to_oracle_descs(oracle_mod, blocks), 5)
+    orc.coeff()
+    from tests.helpers import interior_of_host
+    ref = orc.solve([np.zeros((d.n[2] + 2, d.n[1] + 2, d.n[0] + 2)) for d in blocks],
+                    [interior_of_host(x, d) for x, d in zip(b, blocks)], tol=1e-12, maxcy=400)
+    s = h3d.MultigridSolver(blocks, 5, precision="mixed")
+    pm = [x.copy() for x in p]
+    info = s.newsolv_mg(pm, b, tol=1e-12, maxcy=400)
+    assert info["converged"] and info["relres"] <= 1e-12
+    err = mean_removed_rel([interior_of_host(x, d) for x, d in zip(pm, blocks)],
+                           [x[1:-1, 1:-1, 1:-1] for x in ref["p"]])
+    assert err <= 1e-8, err
+    s.close()
