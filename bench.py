@@ -249,6 +249,9 @@ def main():
     ap.add_argument("--ref-sample-cycles", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--ncu-region", action="store_true",
+                    help="profiling driver: mixed solver only, warm-up solves, then one solve inside "
+                         "cudaProfilerStart/Stop (use with ncu --profile-from-start off)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -270,6 +273,19 @@ def main():
     device = local
     prob = make_problem(args.config)
     peak, peak_kind = load_peaks()
+    if args.ncu_region:
+        import torch
+        s = build_solver_dev(prob, "mixed", device)
+        for _ in range(args.warmup):
+            s.zero_field("p")
+            s.solve_resident(tol=TOL, maxcy=400)
+        s.zero_field("p")
+        torch.cuda.profiler.start()
+        info = s.solve_resident(tol=TOL, maxcy=400)
+        torch.cuda.profiler.stop()
+        print(json.dumps({"ncu_region": True, "cycles": info["cycles"], "device_ms": info["device_ms"],
+                          "kernel_launches": info["kernel_launches"]}), flush=True)
+        return
 
     mixed = build_solver_dev(prob, "mixed", device)
     fp64 = build_solver_dev(prob, "fp64", device)

@@ -203,6 +203,16 @@ struct Exec {
 
   bool mixed_level(int g) const { return f32_level(h, g); }
 
+  // Inside stream capture an event must be recorded as an external node to be
+  // timed later; outside capture a plain record.
+  cudaError_t record(cudaEvent_t e) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaError_t r = cudaStreamIsCapturing(h->st, &cs);
+    if (r != cudaSuccess) return r;
+    if (cs == cudaStreamCaptureStatusActive) return cudaEventRecordWithFlags(e, h->st, cudaEventRecordExternal);
+    return cudaEventRecord(e, h->st);
+  }
+
   int sweep(int g) {
     Level& V = L(g);
     cudaStream_t st = h->st;
@@ -210,14 +220,14 @@ struct Exec {
     if (prof && g == 1 && prof_used + 2 <= prof->size()) {
       e0 = (*prof)[prof_used++];
       e1 = (*prof)[prof_used++];
-      CU(cudaEventRecord(e0, st));
+      CU(record(e0));
     }
     if (mixed_level(g)) {
       float* src = V.phi32[V.cur32];
       float* dst = V.phi32[1 - V.cur32];
       CU(launch_rbgs<float>(V.variant, h->var, V.zero32, V.d_bl, V.d_tiles, V.ntiles, V.zc, src, dst, V.rhs32,
                             V.fx32, V.fy32, V.fz32, st));
-      if (e1) CU(cudaEventRecord(e1, st));
+      if (e1) CU(record(e1));
       CU(launch_fill<float>(V.sweep.d_dst, V.sweep.d_src, V.sweep.n, dst, dst, src, V.zero32, st));
       V.cur32 = 1 - V.cur32;
       V.zero32 = false;
@@ -226,7 +236,7 @@ struct Exec {
       double* dst = V.phi64[1 - V.cur64];
       CU(launch_rbgs<double>(V.variant, h->var, V.zero64, V.d_bl, V.d_tiles, V.ntiles, V.zc, src, dst, V.rhs64,
                              V.fx64, V.fy64, V.fz64, st));
-      if (e1) CU(cudaEventRecord(e1, st));
+      if (e1) CU(record(e1));
       CU(launch_fill<double>(V.sweep.d_dst, V.sweep.d_src, V.sweep.n, dst, dst, src, V.zero64, st));
       V.cur64 = 1 - V.cur64;
       V.zero64 = false;

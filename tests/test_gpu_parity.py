@@ -159,11 +159,10 @@ def _host_problem(h3d, blocks, seed, pl):
         h3d.interior(bh, d)[...] = bi
         b.append(bh)
         p.append(h3d.host_field(d))
-    # all-wall problems need a compatible rhs
-    if all(x != 5 for x in blocks[0].bc):
-        m = np.mean(np.concatenate([h3d.interior(x, d).ravel() for x, d in zip(b, blocks)]))
-        for x, d in zip(b, blocks):
-            h3d.interior(x, d)[...] -= m
+    # wall and periodic faces only: the operator is singular, the rhs must have zero mean
+    m = np.mean(np.concatenate([h3d.interior(x, d).ravel() for x, d in zip(b, blocks)]))
+    for x, d in zip(b, blocks):
+        h3d.interior(x, d)[...] -= m
     return b, p
 
 
