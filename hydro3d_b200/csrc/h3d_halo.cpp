@@ -20,7 +20,7 @@
 
 namespace h3d {
 
-LevelGeom make_level_geom(const std::vector<h3d_block_desc>& blocks, int g) {
+LevelGeom make_level_geom(const std::vector<h3d_block_desc>& blocks, int g, bool pad) {
   LevelGeom L;
   L.g = g;
   long long off = 0;
@@ -30,8 +30,11 @@ LevelGeom make_level_geom(const std::vector<h3d_block_desc>& blocks, int g) {
     b.nx = d.n[0] >> (gl - 1);
     b.ny = d.n[1] >> (gl - 1);
     b.nz = d.n[2] >> (gl - 1);
-    b.sx = b.nx + 2;
-    b.sxy = (long long)(b.nx + 2) * (b.ny + 2);
+    // padded layout: rows start on 16-byte boundaries (TMA global strides) and
+    // blocks on 256-byte boundaries; the canonical layout is dense.
+    b.sx = pad ? ((b.nx + 2 + kRowAlign - 1) / kRowAlign) * kRowAlign : b.nx + 2;
+    b.sxy = (long long)b.sx * (b.ny + 2);
+    if (pad) off = (off + kBlockAlign - 1) / kBlockAlign * kBlockAlign;
     b.off = off;
     b.phys = 0;
     for (int f = 0; f < 6; ++f)
@@ -62,7 +65,7 @@ struct Emu {
   }
   size_t at(int b, int x, int y, int z) const {
     const BlkLev& B = L.bl[b];
-    return (size_t)(B.off + ((long long)z * (B.ny + 2) + y) * (B.nx + 2) + x);
+    return (size_t)(B.off + (long long)z * B.sxy + (long long)y * B.sx + x);
   }
   int n(int b, int a) const { return a == 0 ? L.bl[b].nx : (a == 1 ? L.bl[b].ny : L.bl[b].nz); }
   // Cell of block b whose coordinate on axis a is c and whose other two
@@ -280,19 +283,19 @@ struct Emu {
     }
     const BlkLev& B = L.bl[lo];
     long long r = (long long)q - B.off;
-    int x = (int)(r % (B.nx + 2));
-    long long t = r / (B.nx + 2);
-    int y = (int)(t % (B.ny + 2));
-    int z = (int)(t / (B.ny + 2));
+    int z = (int)(r / B.sxy);
+    long long t = r - (long long)z * B.sxy;
+    int y = (int)(t / B.sx);
+    int x = (int)(t - (long long)y * B.sx);
     return x >= 1 && x <= B.nx && y >= 1 && y <= B.ny && z >= 1 && z <= B.nz;
   }
 };
 
 }  // namespace
 
-int build_halo_table(const std::vector<h3d_block_desc>& blocks, int g, int kind,
+int build_halo_table(const std::vector<h3d_block_desc>& blocks, int g, int kind, bool pad,
                      std::vector<uint32_t>& dst, std::vector<uint32_t>& src, std::string* err) {
-  LevelGeom L = make_level_geom(blocks, g);
+  LevelGeom L = make_level_geom(blocks, g, pad);
   if (L.n_elems >= (int64_t)kOldFlag) {
     if (err) *err = "level too large for 31-bit halo indices";
     return H3D_ERR_BAD_CONFIG;
@@ -357,7 +360,7 @@ extern "C" int h3d_halo_table(int32_t nblocks, const h3d_block_desc* blocks, int
   for (auto& d : D)
     if (g > d.ngrid || d.ngrid < 1) return H3D_ERR_ARG;
   std::vector<uint32_t> vd, vs;
-  int rc = h3d::build_halo_table(D, g, kind, vd, vs, nullptr);
+  int rc = h3d::build_halo_table(D, g, kind, false, vd, vs, nullptr);
   if (rc != H3D_OK) return rc;
   *n = (int64_t)vd.size();
   if (dst && src) {

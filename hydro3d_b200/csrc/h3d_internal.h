@@ -12,13 +12,15 @@ namespace h3d {
 constexpr int kMaxLevels = 16;
 constexpr uint32_t kOldFlag = 0x80000000u;  // halo entry reads the pre-fill value
 constexpr uint32_t kIdxMask = 0x7fffffffu;
+constexpr int kRowAlign = 4;     // row pitch multiple (elements): 16 B for FP32, 32 B for FP64
+constexpr int kBlockAlign = 64;  // block base multiple (elements)
 
 // Per-(block, level) geometry as the kernels see it.  Cell (x,y,z), 0-based
-// with the ghost layer at 0 and n+1, lives at off + (z*(ny+2) + y)*(nx+2) + x.
+// with the ghost layer at 0 and n+1, lives at off + z*sxy + y*sx + x.
 struct BlkLev {
   int nx, ny, nz;       // interior cells
-  int sx;               // nx + 2
-  long long sxy;        // (nx+2)*(ny+2)
+  int sx;               // row pitch (>= nx+2; padded on the device)
+  long long sxy;        // plane pitch sx*(ny+2)
   long long off;        // element offset of cell (0,0,0) in the level array
   int phys;             // bit f set: face f (W,E,S,N,B,T) is a physical non-periodic wall
   int pad;
@@ -40,12 +42,13 @@ struct LevelGeom {
 };
 
 // Builds the level geometry from block descriptors (level dims with the
-// reference's clamp, mgsolver.for:392-400).
-LevelGeom make_level_geom(const std::vector<h3d_block_desc>& blocks, int g);
+// reference's clamp, mgsolver.for:392-400).  pad: the device layout (aligned
+// row pitch and block bases); otherwise the canonical dense numbering.
+LevelGeom make_level_geom(const std::vector<h3d_block_desc>& blocks, int g, bool pad);
 
 // Halo gather tables (see h3d_halo_table in h3d_mg.h).
 enum HaloKind { kHaloSweep = 0, kHaloExchange = 1, kHaloBound = 2, kHaloFaces = 3 };
-int build_halo_table(const std::vector<h3d_block_desc>& blocks, int g, int kind,
+int build_halo_table(const std::vector<h3d_block_desc>& blocks, int g, int kind, bool pad,
                      std::vector<uint32_t>& dst, std::vector<uint32_t>& src,
                      std::string* err);
 

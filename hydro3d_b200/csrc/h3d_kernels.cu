@@ -57,6 +57,11 @@ __device__ __forceinline__ T coef_ap(const Coef<T>& c) {
   return -(c.aw + c.ae + c.as + c.an + c.ab + c.at);  // -1.0*(...), mgsolver.for:207-210
 }
 
+// Gauss-Seidel update division: IEEE division in FP64 (the reference's
+// arithmetic); the FP32 inner solve uses the 2-ulp reciprocal division.
+__device__ __forceinline__ double gs_div(double a, double b) { return a / b; }
+__device__ __forceinline__ float gs_div(float a, float b) { return __fdividef(a, b); }
+
 // ---------------------------------------------------------------------------
 // Red-black Gauss-Seidel sweep (mgrelax, mg_itrsch=3, mgsolver.for:551-605).
 //
@@ -116,9 +121,9 @@ __global__ void __launch_bounds__(NT) k_rbgs(const BlkLev* __restrict__ bls, con
       long long i = (long long)z * sxy + y * sx + x;
       Coef<T> c = cell_coef<T, VAR>(B, x, y, z, i, FX, FY, FZ);
       T ap = coef_ap(c);
-      P[s] = (R[i] - (c.aw * P[s - 1] + c.ae * P[s + 1] + c.as * P[s - RX] + c.an * P[s + RX] +
-                      c.ab * Pm[s] + c.at * Pp[s])) /
-             ap;
+      P[s] = gs_div(R[i] - (c.aw * P[s - 1] + c.ae * P[s + 1] + c.as * P[s - RX] + c.an * P[s + RX] +
+                            c.ab * Pm[s] + c.at * Pp[s]),
+                    ap);
     }
   };
   auto black_store = [&](int z) {
@@ -138,9 +143,9 @@ __global__ void __launch_bounds__(NT) k_rbgs(const BlkLev* __restrict__ bls, con
       } else {
         Coef<T> c = cell_coef<T, VAR>(B, x, y, z, i, FX, FY, FZ);
         T ap = coef_ap(c);
-        v = (R[i] - (c.aw * P[s - 1] + c.ae * P[s + 1] + c.as * P[s - RX] + c.an * P[s + RX] +
-                     c.ab * Pm[s] + c.at * Pp[s])) /
-            ap;
+        v = gs_div(R[i] - (c.aw * P[s - 1] + c.ae * P[s + 1] + c.as * P[s - RX] + c.an * P[s + RX] +
+                           c.ab * Pm[s] + c.at * Pp[s]),
+                   ap);
       }
       Dz[y * sx + x] = v;
     }
@@ -159,6 +164,313 @@ __global__ void __launch_bounds__(NT) k_rbgs(const BlkLev* __restrict__ bls, con
   if (ze == nz) black_store(nz);
 }
 
+
+// ---------------------------------------------------------------------------
+// Row-tile red-black sweep.  A CTA owns TY whole rows (x = 0..nx+1) of one
+// block and marches a z range; because a tile spans the whole row there is no
+// x halo, only one red halo row above and below.  Thread (tr, tc) owns the
+// cell pairs p = tc + k*TPR (x = 2p+1, 2p+2) of row y0-1+tr: of every pair
+// exactly one cell is red and one black, so neither colour phase diverges.
+// Shared memory holds four staged planes of rows y0-2 .. y0+TY+1; column c
+// holds x = c-1.  Same out-of-place contract and arithmetic as k_rbgs.
+template <typename T, int TPR, int CP, int TY, bool VAR, bool ZERO>
+__global__ void __launch_bounds__(TPR*(TY + 2)) k_rbgs_rows(const BlkLev* __restrict__ bls,
+                                                           const Tile* __restrict__ tiles, int zc,
+                                                           const T* __restrict__ src, T* __restrict__ dst,
+                                                           const T* __restrict__ rhs, const T* __restrict__ fx,
+                                                           const T* __restrict__ fy, const T* __restrict__ fz) {
+  constexpr int SP = 2 * CP * TPR + 4;
+  constexpr int SR = TY + 4;
+  constexpr int PL = SR * SP;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* ring = reinterpret_cast<T*>(smem_raw);
+  const Tile t = tiles[blockIdx.x];
+  const BlkLev B = bls[t.b];
+  const int nx = B.nx, ny = B.ny, nz = B.nz;
+  const long long sx = B.sx, sxy = B.sxy;
+  const T* __restrict__ S = src + B.off;
+  T* __restrict__ D = dst + B.off;
+  const T* __restrict__ R = rhs + B.off;
+  const T* FX = VAR ? fx + B.off : nullptr;
+  const T* FY = VAR ? fy + B.off : nullptr;
+  const T* FZ = VAR ? fz + B.off : nullptr;
+  const int y0 = t.y0, zs = t.z0;
+  const int ze = min(zs + zc - 1, nz);
+  const int zlo = max(zs - 1, 1), zhi = min(ze + 1, nz);
+  const int tr = threadIdx.x / TPR, tc = threadIdx.x - (threadIdx.x / TPR) * TPR;
+  const int y = y0 - 1 + tr;
+  const int srow = (tr + 1) * SP;
+  const bool row_in = y >= 1 && y <= ny;
+  const bool row_own = tr >= 1 && tr <= TY && y <= ny;
+  const int ph = B.phys;
+  const T ax = (T)B.ax, ay = (T)B.ay, az = (T)B.az;
+  const T as_c = (y == 1 && (ph & 4)) ? T(0) : ay;
+  const T an_c = (y == ny && (ph & 8)) ? T(0) : ay;
+
+  auto stage = [&](int z) {
+    T* P = ring + (z & 3) * PL;
+    const T* Sz = S + (long long)z * sxy;
+    for (int r = tr; r < SR; r += TY + 2) {
+      const int yy = y0 - 2 + r;
+      const bool yok = yy >= 0 && yy <= ny + 1;
+      const T* Srow = Sz + (long long)yy * sx;
+      T* Prow = P + r * SP + 1;
+      for (int c = tc; c <= nx + 1; c += TPR) {
+        T v = T(0);
+        if (!ZERO && yok) v = Srow[c];
+        Prow[c] = v;
+      }
+    }
+  };
+  // one cell update in plane z (P), neighbours in Pm (z-1), Pp (z+1)
+  auto update = [&](T* P, const T* Pm, const T* Pp, int x, int z, long long rowg) -> T {
+    const int s = srow + x + 1;
+    T aw, ae, as, an, ab, at;
+    if (VAR) {
+      const long long i = rowg + x;
+      aw = FX[i - 1]; ae = FX[i]; as = FY[i - sx]; an = FY[i]; ab = FZ[i - sxy]; at = FZ[i];
+    } else {
+      aw = (x == 1 && (ph & 1)) ? T(0) : ax;
+      ae = (x == nx && (ph & 2)) ? T(0) : ax;
+      as = as_c;
+      an = an_c;
+      ab = (z == 1 && (ph & 16)) ? T(0) : az;
+      at = (z == nz && (ph & 32)) ? T(0) : az;
+    }
+    const T ap = -(aw + ae + as + an + ab + at);
+    return gs_div(R[rowg + x] - (aw * P[s - 1] + ae * P[s + 1] + as * P[s - SP] + an * P[s + SP] + ab * Pm[s] +
+                                 at * Pp[s]),
+                  ap);
+  };
+  auto red = [&](int z) {
+    if (!row_in) return;
+    T* P = ring + (z & 3) * PL;
+    const T* Pm = ring + ((z - 1) & 3) * PL;
+    const T* Pp = ring + ((z + 1) & 3) * PL;
+    const long long rowg = (long long)z * sxy + (long long)y * sx;
+    const int j = (y + z) & 1;
+#pragma unroll
+    for (int k = 0; k < CP; ++k) {
+      const int x = 2 * (tc + k * TPR) + 1 + j;
+      if (x <= nx) P[srow + x + 1] = update(P, Pm, Pp, x, z, rowg);
+    }
+  };
+  auto black_store = [&](int z) {
+    if (!row_own) return;
+    T* P = ring + (z & 3) * PL;
+    const T* Pm = ring + ((z - 1) & 3) * PL;
+    const T* Pp = ring + ((z + 1) & 3) * PL;
+    const long long rowg = (long long)z * sxy + (long long)y * sx;
+    const int jb = (y + z + 1) & 1;
+#pragma unroll
+    for (int k = 0; k < CP; ++k) {
+      const int xp = 2 * (tc + k * TPR) + 1;
+      if (xp > nx) continue;
+      const int xb = xp + jb, xr = xp + 1 - jb;
+      const T vr = P[srow + xr + 1];
+      const T vb = update(P, Pm, Pp, xb, z, rowg);
+      D[rowg + xr] = vr;
+      D[rowg + xb] = vb;
+    }
+  };
+
+  stage(zlo - 1);
+  stage(zlo);
+  for (int z = zlo; z <= zhi; ++z) {
+    stage(z + 1);
+    __syncthreads();
+    red(z);
+    __syncthreads();
+    if (z - 1 >= zs && z - 1 <= ze) black_store(z - 1);
+    __syncthreads();
+  }
+  if (ze == nz) black_store(nz);
+}
+
+
+// ---------------------------------------------------------------------------
+// TMA-staged row-tile sweep (the production smoother on sm_100a).
+//
+// Same cell mapping and arithmetic as k_rbgs_rows, but the z planes are
+// brought into shared memory by the Tensor Memory Accelerator: one elected
+// thread issues a 3-D bulk tensor copy (box = whole padded row width x TY+4
+// rows x 1 plane, rows outside the block read as zero) into a ring of five
+// plane slots, two planes ahead of the computation, each slot completing on
+// its own mbarrier.  Every wait is bounded; a wait that gives up sets *err
+// and the sweep finishes without hanging (the host reports a timeout).
+// No multicast is used.
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// Bounded wait on an mbarrier phase: gives up after ~2^26 SM clocks (tens of
+// ms; a plane copy takes microseconds), records the failure in *err and makes
+// every later wait of this thread return at once, so a failed copy can never
+// hang the kernel.
+__device__ __forceinline__ void mbar_wait(uint32_t bar, uint32_t parity, int* err, bool& bad) {
+  if (bad) return;
+  const long long t0 = clock64();
+  for (;;) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (done) return;
+    if (clock64() - t0 > (1LL << 26)) {
+      bad = true;
+      atomicExch(err, 1);
+      return;
+    }
+  }
+}
+
+template <typename T, int TPR, int CP, int TY, bool VAR>
+__global__ void __launch_bounds__(TPR*(TY + 2)) k_rbgs_tma(const BlkLev* __restrict__ bls,
+                                                          const Tile* __restrict__ tiles, int zc,
+                                                          const CUtensorMap* __restrict__ maps,
+                                                          T* __restrict__ dst, const T* __restrict__ rhs,
+                                                          const T* __restrict__ fx, const T* __restrict__ fy,
+                                                          const T* __restrict__ fz, int* err) {
+  constexpr int NS = 5;
+  constexpr int VEC = 16 / (int)sizeof(T);
+  constexpr int SPMAX = ((2 * CP * TPR + 2 + VEC - 1) / VEC) * VEC;
+  constexpr int SLOT = ((SPMAX * (TY + 4) * (int)sizeof(T) + 127) / 128) * 128;
+  extern __shared__ unsigned char smem_raw[];
+  unsigned char* base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
+  uint64_t* bars = reinterpret_cast<uint64_t*>(base + NS * SLOT);
+
+  const Tile t = tiles[blockIdx.x];
+  const BlkLev B = bls[t.b];
+  const CUtensorMap* map = maps + t.b;
+  const int nx = B.nx, ny = B.ny, nz = B.nz;
+  const int sx = B.sx;
+  const long long sxy = B.sxy;
+  T* __restrict__ D = dst + B.off;
+  const T* __restrict__ R = rhs + B.off;
+  const T* FX = VAR ? fx + B.off : nullptr;
+  const T* FY = VAR ? fy + B.off : nullptr;
+  const T* FZ = VAR ? fz + B.off : nullptr;
+  const int y0 = t.y0, zs = t.z0;
+  const int ze = min(zs + zc - 1, nz);
+  const int zlo = max(zs - 1, 1), zhi = min(ze + 1, nz);
+  const int BX = ((nx + 2 + VEC - 1) / VEC) * VEC;  // smem row pitch == TMA box width
+  const uint32_t box_bytes = (uint32_t)(BX * (TY + 4) * (int)sizeof(T));
+  const int tr = threadIdx.x / TPR, tc = threadIdx.x - (threadIdx.x / TPR) * TPR;
+  const int y = y0 - 1 + tr;
+  const int srow = (tr + 1) * BX;
+  const bool row_in = y >= 1 && y <= ny;
+  const bool row_own = tr >= 1 && tr <= TY && y <= ny;
+  const int ph = B.phys;
+  const T ax = (T)B.ax, ay = (T)B.ay, az = (T)B.az;
+  const T as_c = (y == 1 && (ph & 4)) ? T(0) : ay;
+  const T an_c = (y == ny && (ph & 8)) ? T(0) : ay;
+  const bool leader = threadIdx.x == 0;
+  bool bad = false;
+
+  if (leader) {
+    for (int q = 0; q < NS; ++q)
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(bars + q)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  __syncthreads();
+
+  auto slot = [&](int z) -> T* { return reinterpret_cast<T*>(base + (z % NS) * SLOT); };
+  auto issue = [&](int z) {  // leader only
+    const uint32_t bar = smem_u32(bars + (z % NS));
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(box_bytes) : "memory");
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];\n" ::
+            "r"(smem_u32(slot(z))),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(0), "r"(y0 - 2), "r"(z), "r"(bar)
+        : "memory");
+  };
+  auto wait_plane = [&](int z) {
+    const uint32_t parity = (uint32_t)(((z - zlo + 1) / NS) & 1);
+    mbar_wait(smem_u32(bars + (z % NS)), parity, err, bad);
+  };
+  auto update = [&](T* P, const T* Pm, const T* Pp, int x, int z, const T* Rrow, int io) -> T {
+    const int s = srow + x;
+    T aw, ae, as, an, ab, at;
+    if (VAR) {
+      const long long i = (long long)z * sxy + io + x;
+      aw = FX[i - 1]; ae = FX[i]; as = FY[i - sx]; an = FY[i]; ab = FZ[i - sxy]; at = FZ[i];
+    } else {
+      aw = (x == 1 && (ph & 1)) ? T(0) : ax;
+      ae = (x == nx && (ph & 2)) ? T(0) : ax;
+      as = as_c;
+      an = an_c;
+      ab = (z == 1 && (ph & 16)) ? T(0) : az;
+      at = (z == nz && (ph & 32)) ? T(0) : az;
+    }
+    const T ap = -(aw + ae + as + an + ab + at);
+    return gs_div(Rrow[x] - (aw * P[s - 1] + ae * P[s + 1] + as * P[s - BX] + an * P[s + BX] + ab * Pm[s] +
+                             at * Pp[s]),
+                  ap);
+  };
+  auto red = [&](int z) {
+    if (!row_in) return;
+    T* P = slot(z);
+    const T* Pm = slot(z - 1);
+    const T* Pp = slot(z + 1);
+    const int io = y * sx;
+    const T* Rrow = R + (long long)z * sxy + io;
+    const int j = (y + z) & 1;
+#pragma unroll
+    for (int k = 0; k < CP; ++k) {
+      const int x = 2 * (tc + k * TPR) + 1 + j;
+      if (x <= nx) P[srow + x] = update(P, Pm, Pp, x, z, Rrow, io);
+    }
+  };
+  auto black_store = [&](int z) {
+    if (!row_own) return;
+    T* P = slot(z);
+    const T* Pm = slot(z - 1);
+    const T* Pp = slot(z + 1);
+    const int io = y * sx;
+    const T* Rrow = R + (long long)z * sxy + io;
+    T* Drow = D + (long long)z * sxy + io;
+    const int jb = (y + z + 1) & 1;
+#pragma unroll
+    for (int k = 0; k < CP; ++k) {
+      const int xp = 2 * (tc + k * TPR) + 1;
+      if (xp > nx) continue;
+      const int xb = xp + jb, xr = xp + 1 - jb;
+      const T vr = P[srow + xr];
+      const T vb = update(P, Pm, Pp, xb, z, Rrow, io);
+      Drow[xr] = vr;
+      Drow[xb] = vb;
+    }
+  };
+
+  if (leader) {
+    issue(zlo - 1);
+    issue(zlo);
+    issue(zlo + 1);
+  }
+  wait_plane(zlo - 1);
+  wait_plane(zlo);
+  for (int z = zlo; z <= zhi; ++z) {
+    if (leader && z + 2 <= zhi + 1) issue(z + 2);
+    wait_plane(z + 1);
+    red(z);
+    __syncthreads();
+    if (z - 1 >= zs && z - 1 <= ze) black_store(z - 1);
+    __syncthreads();
+  }
+  if (ze == nz) black_store(nz);
+}
+
+template <typename T, int TPR, int CP, int TY>
+constexpr size_t tma_smem() {
+  constexpr int VEC = 16 / (int)sizeof(T);
+  constexpr int SPMAX = ((2 * CP * TPR + 2 + VEC - 1) / VEC) * VEC;
+  constexpr int SLOT = ((SPMAX * (TY + 4) * (int)sizeof(T) + 127) / 128) * 128;
+  return (size_t)5 * SLOT + 128 + 5 * 8;
+}
+
 // ---------------------------------------------------------------------------
 template <typename T, bool ZERO_OLD>
 __global__ void k_fill(const uint32_t* __restrict__ dsts, const uint32_t* __restrict__ srcs, int64_t n,
@@ -173,48 +485,68 @@ __global__ void k_fill(const uint32_t* __restrict__ dsts, const uint32_t* __rest
 }
 
 // ---------------------------------------------------------------------------
+// Row work: one warp per row (b, y, z) of a row table, grid-stride over rows.
+// rows_start[b] is the first row of block b; a block has (ny+2)*(nz+2) rows
+// (all rows) or ny*nz rows (interior rows).
+struct RowRef {
+  int b, y, z;
+};
+__device__ __forceinline__ RowRef row_of(const BlkLev* __restrict__ bls, const int* __restrict__ start, int nb,
+                                         int rid, bool interior) {
+  RowRef r;
+  r.b = find_block(start, nb, rid);
+  const int local = rid - __ldg(start + r.b);
+  const BlkLev& B = bls[r.b];
+  const int my = interior ? B.ny : B.ny + 2;
+  r.z = local / my;
+  r.y = local - r.z * my;
+  if (interior) { r.y += 1; r.z += 1; }
+  return r;
+}
+
 // mgrestr: resf = su - (A phi) on the fine interior (mgsolver.for:707-714),
 // coarse rhs = 0.125 * sum of the 2x2x2 children, i fastest (:748-752).
 template <typename T, bool VAR, bool ZERO>
 __global__ void __launch_bounds__(256) k_restrict(const BlkLev* __restrict__ fine, const BlkLev* __restrict__ coarse,
-                                                  const int* __restrict__ cta_start, int nb,
+                                                  const int* __restrict__ row_start, int nb, int nrows,
                                                   const T* __restrict__ phi, const T* __restrict__ rhs,
                                                   T* __restrict__ rhs_c, const T* __restrict__ fx,
                                                   const T* __restrict__ fy, const T* __restrict__ fz) {
-  const int b = find_block(cta_start, nb, blockIdx.x);
-  const BlkLev C = coarse[b];
-  const BlkLev F = fine[b];
-  const int local = (blockIdx.x - cta_start[b]) * blockDim.x + threadIdx.x;
-  if (local >= C.nx * C.ny * C.nz) return;
-  const int X = local % C.nx + 1;
-  const int Y = (local / C.nx) % C.ny + 1;
-  const int Z = local / (C.nx * C.ny) + 1;
-  const T* P = phi + F.off;
-  const T* Rf = rhs + F.off;
-  T sum = T(0);
-  bool first = true;
+  const int lane = threadIdx.x & 31;
+  for (int rid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; rid < nrows; rid += (gridDim.x * blockDim.x) >> 5) {
+    const RowRef rr = row_of(coarse, row_start, nb, rid, true);
+    const BlkLev C = coarse[rr.b];
+    const BlkLev F = fine[rr.b];
+    const T* P = phi + F.off;
+    const T* Rf = rhs + F.off;
+    const T* FX = VAR ? fx + F.off : nullptr;
+    const T* FY = VAR ? fy + F.off : nullptr;
+    const T* FZ = VAR ? fz + F.off : nullptr;
+    const int Y = rr.y, Z = rr.z;
+    for (int X = 1 + lane; X <= C.nx; X += 32) {
+      T sum = T(0);
 #pragma unroll
-  for (int dk = 0; dk < 2; ++dk)
+      for (int dk = 0; dk < 2; ++dk)
 #pragma unroll
-    for (int dj = 0; dj < 2; ++dj)
+        for (int dj = 0; dj < 2; ++dj)
 #pragma unroll
-      for (int di = 0; di < 2; ++di) {
-        int x = 2 * X - 1 + di, y = 2 * Y - 1 + dj, z = 2 * Z - 1 + dk;
-        long long i = (long long)z * F.sxy + (long long)y * F.sx + x;
-        T r;
-        if (ZERO) {
-          r = Rf[i] - T(0);
-        } else {
-          Coef<T> c = cell_coef<T, VAR>(F, x, y, z, i, fx ? fx + F.off : nullptr, fy ? fy + F.off : nullptr,
-                                        fz ? fz + F.off : nullptr);
-          T ap = coef_ap(c);
-          r = Rf[i] - (c.aw * P[i - 1] + c.ae * P[i + 1] + c.as * P[i - F.sx] + c.an * P[i + F.sx] +
-                       c.ab * P[i - F.sxy] + c.at * P[i + F.sxy] + ap * P[i]);
-        }
-        if (first) { sum = r; first = false; }
-        else sum = sum + r;
-      }
-  rhs_c[C.off + (long long)Z * C.sxy + (long long)Y * C.sx + X] = T(0.125) * sum;
+          for (int di = 0; di < 2; ++di) {
+            const int x = 2 * X - 1 + di, y = 2 * Y - 1 + dj, z = 2 * Z - 1 + dk;
+            const long long i = (long long)z * F.sxy + (long long)y * F.sx + x;
+            T r;
+            if (ZERO) {
+              r = Rf[i] - T(0);
+            } else {
+              Coef<T> c = cell_coef<T, VAR>(F, x, y, z, i, FX, FY, FZ);
+              const T ap = coef_ap(c);
+              r = Rf[i] - (c.aw * P[i - 1] + c.ae * P[i + 1] + c.as * P[i - F.sx] + c.an * P[i + F.sx] +
+                           c.ab * P[i - F.sxy] + c.at * P[i + F.sxy] + ap * P[i]);
+            }
+            sum = (di | dj | dk) ? sum + r : r;
+          }
+      rhs_c[C.off + (long long)Z * C.sxy + (long long)Y * C.sx + X] = T(0.125) * sum;
+    }
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -224,42 +556,48 @@ __global__ void __launch_bounds__(256) k_restrict(const BlkLev* __restrict__ fin
 // trilinear (27,9,3,1) sum in the reference's term order (mgsolver.for:838-892).
 template <typename T, bool ZERO_OLD>
 __global__ void __launch_bounds__(256) k_prolong(const BlkLev* __restrict__ fine, const BlkLev* __restrict__ coarse,
-                                                 const int* __restrict__ cta_start, int nb,
+                                                 const int* __restrict__ row_start, int nb, int nrows,
                                                  const T* __restrict__ phi_c, const T* __restrict__ old,
                                                  T* __restrict__ out) {
-  const int b = find_block(cta_start, nb, blockIdx.x);
-  const BlkLev F = fine[b];
-  const BlkLev C = coarse[b];
-  const int local = (blockIdx.x - cta_start[b]) * blockDim.x + threadIdx.x;
-  const int mx = F.nx + 2, my = F.ny + 2, mz = F.nz + 2;
-  if (local >= mx * my * mz) return;
-  const int x = local % mx, y = (local / mx) % my, z = local / (mx * my);
-  const int ph = F.phys;
-  int sx = x, sy = y, sz = z;
-  if (x == 0 && (ph & 1)) sx = 1;
-  if (x == F.nx + 1 && (ph & 2)) sx = F.nx;
-  if (y == 0 && (ph & 4)) sy = 1;
-  if (y == F.ny + 1 && (ph & 8)) sy = F.ny;
-  if (z == 0 && (ph & 16)) sz = 1;
-  if (z == F.nz + 1 && (ph & 32)) sz = F.nz;
-  const int lx = sx >> 1, ly = sy >> 1, lz = sz >> 1;
-  const T wx0 = (sx & 1) ? T(1) : T(3), wx1 = (sx & 1) ? T(3) : T(1);
-  const T wy0 = (sy & 1) ? T(1) : T(3), wy1 = (sy & 1) ? T(3) : T(1);
-  const T wz0 = (sz & 1) ? T(1) : T(3), wz1 = (sz & 1) ? T(3) : T(1);
-  const T* Pc = phi_c + C.off + (long long)lz * C.sxy + (long long)ly * C.sx + lx;
-  const long long cx = 1, cy = C.sx, cz = C.sxy;
-  // term order (di,dj,dk): 000, 010, 001, 011, 100, 110, 101, 111
-  T s = (wx0 * wy0 * wz0) * Pc[0];
-  s = s + (wx0 * wy1 * wz0) * Pc[cy];
-  s = s + (wx0 * wy0 * wz1) * Pc[cz];
-  s = s + (wx0 * wy1 * wz1) * Pc[cy + cz];
-  s = s + (wx1 * wy0 * wz0) * Pc[cx];
-  s = s + (wx1 * wy1 * wz0) * Pc[cx + cy];
-  s = s + (wx1 * wy0 * wz1) * Pc[cx + cz];
-  s = s + (wx1 * wy1 * wz1) * Pc[cx + cy + cz];
-  const long long is = (long long)sz * F.sxy + (long long)sy * F.sx + sx;
-  const T o = ZERO_OLD ? T(0) : old[F.off + is];
-  out[F.off + (long long)z * F.sxy + (long long)y * F.sx + x] = o + s / T(64);
+  const int lane = threadIdx.x & 31;
+  for (int rid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; rid < nrows; rid += (gridDim.x * blockDim.x) >> 5) {
+    const RowRef rr = row_of(fine, row_start, nb, rid, false);
+    const BlkLev F = fine[rr.b];
+    const BlkLev C = coarse[rr.b];
+    const int ph = F.phys;
+    const int y = rr.y, z = rr.z;
+    int sy = y, sz = z;
+    if (y == 0 && (ph & 4)) sy = 1;
+    if (y == F.ny + 1 && (ph & 8)) sy = F.ny;
+    if (z == 0 && (ph & 16)) sz = 1;
+    if (z == F.nz + 1 && (ph & 32)) sz = F.nz;
+    const int ly = sy >> 1, lz = sz >> 1;
+    const T wy0 = (sy & 1) ? T(1) : T(3), wy1 = (sy & 1) ? T(3) : T(1);
+    const T wz0 = (sz & 1) ? T(1) : T(3), wz1 = (sz & 1) ? T(3) : T(1);
+    const T* Pc = phi_c + C.off + (long long)lz * C.sxy + (long long)ly * C.sx;
+    const long long cy = C.sx, cz = C.sxy;
+    const T* Orow = old + F.off + (long long)sz * F.sxy + (long long)sy * F.sx;
+    T* Out = out + F.off + (long long)z * F.sxy + (long long)y * F.sx;
+    for (int x = lane; x <= F.nx + 1; x += 32) {
+      int sx = x;
+      if (x == 0 && (ph & 1)) sx = 1;
+      if (x == F.nx + 1 && (ph & 2)) sx = F.nx;
+      const int lx = sx >> 1;
+      const T wx0 = (sx & 1) ? T(1) : T(3), wx1 = (sx & 1) ? T(3) : T(1);
+      const T* Q = Pc + lx;
+      // term order (di,dj,dk): 000, 010, 001, 011, 100, 110, 101, 111
+      T s = (wx0 * wy0 * wz0) * Q[0];
+      s = s + (wx0 * wy1 * wz0) * Q[cy];
+      s = s + (wx0 * wy0 * wz1) * Q[cz];
+      s = s + (wx0 * wy1 * wz1) * Q[cy + cz];
+      s = s + (wx1 * wy0 * wz0) * Q[1];
+      s = s + (wx1 * wy1 * wz0) * Q[1 + cy];
+      s = s + (wx1 * wy0 * wz1) * Q[1 + cz];
+      s = s + (wx1 * wy1 * wz1) * Q[1 + cy + cz];
+      const T o = ZERO_OLD ? T(0) : Orow[sx];
+      Out[x] = o + s / T(64);
+    }
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -285,39 +623,44 @@ __device__ __forceinline__ void block_reduce4(double a0, double a1, double a2, d
 
 // newsolv_mg.for:39-55 as defect correction: p += pp over the whole block
 // (ghosts included, :40-48), then r = b - A p (mgrestr's residual form).
+// One warp per level-1 row (all rows incl. ghosts); per-CTA partial sums.
 template <typename TE, typename TR, bool HAS_E, bool VAR>
-__global__ void __launch_bounds__(256) k_defect(const BlkLev* __restrict__ bls, const int* __restrict__ cta_start,
-                                                int nb, const double* __restrict__ p, const TE* __restrict__ e,
-                                                double* __restrict__ p_next, const double* __restrict__ bvec,
-                                                TR* __restrict__ rhs_out, double mean_b, double rscale,
-                                                const double* __restrict__ fx, const double* __restrict__ fy,
-                                                const double* __restrict__ fz, double* __restrict__ partials) {
-  const int b = find_block(cta_start, nb, blockIdx.x);
-  const BlkLev B = bls[b];
-  const int local = (blockIdx.x - cta_start[b]) * blockDim.x + threadIdx.x;
-  const int mx = B.nx + 2, my = B.ny + 2, mz = B.nz + 2;
+__global__ void __launch_bounds__(256) k_defect(const BlkLev* __restrict__ bls, const int* __restrict__ row_start,
+                                                int nb, int nrows, const double* __restrict__ p,
+                                                const TE* __restrict__ e, double* __restrict__ p_next,
+                                                const double* __restrict__ bvec, TR* __restrict__ rhs_out,
+                                                double mean_b, double rscale, const double* __restrict__ fx,
+                                                const double* __restrict__ fy, const double* __restrict__ fz,
+                                                double* __restrict__ partials) {
+  const int lane = threadIdx.x & 31;
   double rr = 0, bb = 0, rm = 0, rs = 0;
-  if (local < mx * my * mz) {
-    const int x = local % mx, y = (local / mx) % my, z = local / (mx * my);
-    const long long i = B.off + (long long)z * B.sxy + (long long)y * B.sx + x;
+  for (int rid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; rid < nrows; rid += (gridDim.x * blockDim.x) >> 5) {
+    const RowRef ref = row_of(bls, row_start, nb, rid, false);
+    const BlkLev B = bls[ref.b];
+    const int y = ref.y, z = ref.z;
+    const bool row_in = y >= 1 && y <= B.ny && z >= 1 && z <= B.nz;
+    const long long rowg = B.off + (long long)z * B.sxy + (long long)y * B.sx;
     auto pv = [&](long long j) -> double {
       if (HAS_E) return p[j] + (double)e[j];
       return p[j];
     };
-    const double pc = pv(i);
-    if (HAS_E) p_next[i] = pc;
-    if (x >= 1 && x <= B.nx && y >= 1 && y <= B.ny && z >= 1 && z <= B.nz) {
-      Coef<double> c = cell_coef<double, VAR>(B, x, y, z, i - B.off, fx ? fx + B.off : nullptr,
-                                              fy ? fy + B.off : nullptr, fz ? fz + B.off : nullptr);
-      double ap = coef_ap(c);
-      const double bv = bvec[i];
-      double r = bv - (c.aw * pv(i - 1) + c.ae * pv(i + 1) + c.as * pv(i - B.sx) + c.an * pv(i + B.sx) +
-                       c.ab * pv(i - B.sxy) + c.at * pv(i + B.sxy) + ap * pc);
-      rhs_out[i] = (TR)(r - mean_b);
-      rr = r * r;
-      bb = bv * bv;
-      rm = fabs(r) * rscale;
-      rs = r;
+    for (int x = lane; x <= B.nx + 1; x += 32) {
+      const long long i = rowg + x;
+      const double pc = pv(i);
+      if (HAS_E) p_next[i] = pc;
+      if (row_in && x >= 1 && x <= B.nx) {
+        Coef<double> c = cell_coef<double, VAR>(B, x, y, z, i - B.off, VAR ? fx + B.off : nullptr,
+                                                VAR ? fy + B.off : nullptr, VAR ? fz + B.off : nullptr);
+        const double ap = coef_ap(c);
+        const double bv = bvec[i];
+        const double r = bv - (c.aw * pv(i - 1) + c.ae * pv(i + 1) + c.as * pv(i - B.sx) + c.an * pv(i + B.sx) +
+                               c.ab * pv(i - B.sxy) + c.at * pv(i + B.sxy) + ap * pc);
+        rhs_out[i] = (TR)(r - mean_b);
+        rr += r * r;
+        bb += bv * bv;
+        rm = fmax(rm, fabs(r) * rscale);
+        rs += r;
+      }
     }
   }
   block_reduce4<256>(rr, bb, rm, rs, partials + 4 * (size_t)blockIdx.x);
@@ -436,9 +779,25 @@ inline int grid_for(int64_t n, int nt) {
 }  // namespace
 
 // ---------------------------------------------------------------------------
+// Smoother variants: 0-7 generic tiles (k_rbgs), 8+ row tiles (k_rbgs_rows,
+// tx = largest supported nx).
 static const TileShape kShapes[] = {
-    {32, 16, 256}, {32, 8, 256}, {64, 8, 256}, {16, 8, 128}, {8, 8, 64}, {8, 4, 32}, {4, 4, 32}, {64, 16, 512},
+    {32, 16, 256, false, 0, 0, false, -1}, {32, 8, 256, false, 0, 0, false, -1},
+    {64, 8, 256, false, 0, 0, false, -1},  {16, 8, 128, false, 0, 0, false, -1},
+    {8, 8, 64, false, 0, 0, false, -1},    {8, 4, 32, false, 0, 0, false, -1},
+    {4, 4, 32, false, 0, 0, false, -1},    {64, 16, 512, false, 0, 0, false, -1},
+    {128, 8, 640, true, 64, 1, false, -1}, {128, 8, 320, true, 32, 2, false, -1},   // 8, 9
+    {64, 8, 320, true, 32, 1, false, -1},  {64, 16, 576, true, 32, 1, false, -1},   // 10, 11
+    {32, 16, 288, true, 16, 1, false, -1}, {16, 16, 144, true, 8, 1, false, -1},    // 12, 13
+    {256, 8, 640, true, 64, 2, false, -1}, {128, 4, 384, true, 64, 1, false, -1},   // 14, 15
+    {256, 4, 768, true, 128, 1, false, -1}, {128, 4, 192, true, 32, 2, false, -1},  // 16, 17
+    {256, 8, 320, true, 32, 4, false, -1},                                          // 18
+    {128, 8, 640, true, 64, 1, true, 8},   {128, 8, 320, true, 32, 2, true, 9},     // 19, 20
+    {64, 8, 320, true, 32, 1, true, 10},   {64, 16, 576, true, 32, 1, true, 11},    // 21, 22
+    {32, 16, 288, true, 16, 1, true, 12},  {16, 16, 144, true, 8, 1, true, 13},     // 23, 24
+    {128, 4, 384, true, 64, 1, true, 15},  {128, 4, 192, true, 32, 2, true, 17},    // 25, 26
 };
+int tma_ty_index(int ty) { return ty == 4 ? 0 : ty == 8 ? 1 : ty == 16 ? 2 : -1; }
 int num_tile_shapes() { return (int)(sizeof(kShapes) / sizeof(kShapes[0])); }
 TileShape tile_shape(int v) { return kShapes[v]; }
 
@@ -458,10 +817,104 @@ static cudaError_t rbgs_dispatch(bool var, bool zero, const BlkLev* bl, const Ti
   return cudaGetLastError();
 }
 
+template <typename T, int TPR, int CP, int TY>
+static constexpr size_t rows_smem() {
+  return 4 * (size_t)(TY + 4) * (size_t)(2 * CP * TPR + 4) * sizeof(T);
+}
+
+template <typename T, int TPR, int CP, int TY>
+static cudaError_t rows_attr() {
+  const int sm = (int)rows_smem<T, TPR, CP, TY>();
+  cudaError_t e;
+  if ((e = cudaFuncSetAttribute(k_rbgs_rows<T, TPR, CP, TY, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm))) return e;
+  if ((e = cudaFuncSetAttribute(k_rbgs_rows<T, TPR, CP, TY, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm))) return e;
+  if ((e = cudaFuncSetAttribute(k_rbgs_rows<T, TPR, CP, TY, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm))) return e;
+  return cudaFuncSetAttribute(k_rbgs_rows<T, TPR, CP, TY, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+}
+
+template <typename T, int TPR, int CP, int TY>
+static cudaError_t rows_dispatch(bool var, bool zero, const BlkLev* bl, const Tile* tiles, int ntiles, int zc,
+                                 const T* src, T* dst, const T* rhs, const T* fx, const T* fy, const T* fz,
+                                 cudaStream_t st) {
+  if (ntiles <= 0) return cudaSuccess;
+  constexpr int NT = TPR * (TY + 2);
+  constexpr size_t SM = rows_smem<T, TPR, CP, TY>();
+  dim3 grid(ntiles), block(NT);
+  if (var) {
+    if (zero) k_rbgs_rows<T, TPR, CP, TY, true, true><<<grid, block, SM, st>>>(bl, tiles, zc, src, dst, rhs, fx, fy, fz);
+    else k_rbgs_rows<T, TPR, CP, TY, true, false><<<grid, block, SM, st>>>(bl, tiles, zc, src, dst, rhs, fx, fy, fz);
+  } else {
+    if (zero) k_rbgs_rows<T, TPR, CP, TY, false, true><<<grid, block, SM, st>>>(bl, tiles, zc, src, dst, rhs, fx, fy, fz);
+    else k_rbgs_rows<T, TPR, CP, TY, false, false><<<grid, block, SM, st>>>(bl, tiles, zc, src, dst, rhs, fx, fy, fz);
+  }
+  return cudaGetLastError();
+}
+
+template <typename T, int TPR, int CP, int TY>
+static cudaError_t tma_attr() {
+  const int sm = (int)tma_smem<T, TPR, CP, TY>();
+  cudaError_t e;
+  if ((e = cudaFuncSetAttribute(k_rbgs_tma<T, TPR, CP, TY, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm))) return e;
+  return cudaFuncSetAttribute(k_rbgs_tma<T, TPR, CP, TY, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+}
+
+template <typename T, int TPR, int CP, int TY>
+static cudaError_t tma_dispatch(bool var, const BlkLev* bl, const Tile* tiles, int ntiles, int zc,
+                                const CUtensorMap* maps, int* err, T* dst, const T* rhs, const T* fx, const T* fy,
+                                const T* fz, cudaStream_t st) {
+  if (ntiles <= 0) return cudaSuccess;
+  constexpr int NT = TPR * (TY + 2);
+  constexpr size_t SM = tma_smem<T, TPR, CP, TY>();
+  if (var) k_rbgs_tma<T, TPR, CP, TY, true><<<ntiles, NT, SM, st>>>(bl, tiles, zc, maps, dst, rhs, fx, fy, fz, err);
+  else k_rbgs_tma<T, TPR, CP, TY, false><<<ntiles, NT, SM, st>>>(bl, tiles, zc, maps, dst, rhs, fx, fy, fz, err);
+  return cudaGetLastError();
+}
+
+#define H3D_TMA_SHAPES(X) \
+  X(19, 64, 1, 8)         \
+  X(20, 32, 2, 8)         \
+  X(21, 32, 1, 8)         \
+  X(22, 32, 1, 16)        \
+  X(23, 16, 1, 16)        \
+  X(24, 8, 1, 16)         \
+  X(25, 64, 1, 4)         \
+  X(26, 32, 2, 4)
+
+#define H3D_ROW_SHAPES(X)  \
+  X(8, 64, 1, 8)           \
+  X(9, 32, 2, 8)           \
+  X(10, 32, 1, 8)          \
+  X(11, 32, 1, 16)         \
+  X(12, 16, 1, 16)         \
+  X(13, 8, 1, 16)          \
+  X(14, 64, 2, 8)          \
+  X(15, 64, 1, 4)          \
+  X(16, 128, 1, 4)         \
+  X(17, 32, 2, 4)          \
+  X(18, 32, 4, 8)
+
+cudaError_t init_kernel_attributes() {
+  cudaError_t e = cudaSuccess;
+#define X(v, tpr, cp, ty)                                                  \
+  if ((e = rows_attr<float, tpr, cp, ty>()) != cudaSuccess) return e;      \
+  if ((e = rows_attr<double, tpr, cp, ty>()) != cudaSuccess) return e;
+  H3D_ROW_SHAPES(X)
+#undef X
+#define X(v, tpr, cp, ty)                                                  \
+  if ((e = tma_attr<float, tpr, cp, ty>()) != cudaSuccess) return e;       \
+  if ((e = tma_attr<double, tpr, cp, ty>()) != cudaSuccess) return e;
+  H3D_TMA_SHAPES(X)
+#undef X
+  return e;
+}
+
 template <typename T>
 cudaError_t launch_rbgs(int variant, bool var, bool zero_src, const BlkLev* bl, const Tile* tiles, int ntiles,
-                        int zc, const T* src, T* dst, const T* rhs, const T* fx, const T* fy, const T* fz,
-                        cudaStream_t st) {
+                        int zc, const CUtensorMap* maps, int* err, const T* src, T* dst, const T* rhs, const T* fx,
+                        const T* fy, const T* fz, cudaStream_t st) {
+  if (variant >= 0 && variant < num_tile_shapes() && kShapes[variant].tma) {
+    if (zero_src || !maps) variant = kShapes[variant].alt;  // nothing to stage: plain zero-fill kernel
+  }
   switch (variant) {
     case 0: return rbgs_dispatch<T, 32, 16, 256>(var, zero_src, bl, tiles, ntiles, zc, src, dst, rhs, fx, fy, fz, st);
     case 1: return rbgs_dispatch<T, 32, 8, 256>(var, zero_src, bl, tiles, ntiles, zc, src, dst, rhs, fx, fy, fz, st);
@@ -471,6 +924,14 @@ cudaError_t launch_rbgs(int variant, bool var, bool zero_src, const BlkLev* bl, 
     case 5: return rbgs_dispatch<T, 8, 4, 32>(var, zero_src, bl, tiles, ntiles, zc, src, dst, rhs, fx, fy, fz, st);
     case 6: return rbgs_dispatch<T, 4, 4, 32>(var, zero_src, bl, tiles, ntiles, zc, src, dst, rhs, fx, fy, fz, st);
     case 7: return rbgs_dispatch<T, 64, 16, 512>(var, zero_src, bl, tiles, ntiles, zc, src, dst, rhs, fx, fy, fz, st);
+#define X(v, tpr, cp, ty) \
+    case v: return rows_dispatch<T, tpr, cp, ty>(var, zero_src, bl, tiles, ntiles, zc, src, dst, rhs, fx, fy, fz, st);
+    H3D_ROW_SHAPES(X)
+#undef X
+#define X(v, tpr, cp, ty) \
+    case v: return tma_dispatch<T, tpr, cp, ty>(var, bl, tiles, ntiles, zc, maps, err, dst, rhs, fx, fy, fz, st);
+    H3D_TMA_SHAPES(X)
+#undef X
     default: return cudaErrorInvalidValue;
   }
 }
@@ -485,37 +946,50 @@ cudaError_t launch_fill(const uint32_t* dsts, const uint32_t* srcs, int64_t n, T
   return cudaGetLastError();
 }
 
+static inline int row_grid(int nrows) {
+  int g = (nrows + 7) / 8;  // 8 warps (rows) per CTA
+  return g < 1 ? 1 : (g > 148 * 16 ? 148 * 16 : g);
+}
+
 template <typename T>
-cudaError_t launch_restrict(bool var, bool zero_phi, const BlkLev* fine, const BlkLev* coarse, CellTab ct,
+cudaError_t launch_restrict(bool var, bool zero_phi, const BlkLev* fine, const BlkLev* coarse, RowTab rt,
                             const T* phi, const T* rhs, T* rhs_c, const T* fx, const T* fy, const T* fz,
                             cudaStream_t st) {
-  if (ct.ncta <= 0) return cudaSuccess;
-  if (zero_phi) k_restrict<T, false, true><<<ct.ncta, 256, 0, st>>>(fine, coarse, ct.cta_start, ct.nb, phi, rhs, rhs_c, fx, fy, fz);
-  else if (var) k_restrict<T, true, false><<<ct.ncta, 256, 0, st>>>(fine, coarse, ct.cta_start, ct.nb, phi, rhs, rhs_c, fx, fy, fz);
-  else k_restrict<T, false, false><<<ct.ncta, 256, 0, st>>>(fine, coarse, ct.cta_start, ct.nb, phi, rhs, rhs_c, fx, fy, fz);
+  if (rt.nrows <= 0) return cudaSuccess;
+  const int g = row_grid(rt.nrows);
+  if (zero_phi) k_restrict<T, false, true><<<g, 256, 0, st>>>(fine, coarse, rt.start, rt.nb, rt.nrows, phi, rhs, rhs_c, fx, fy, fz);
+  else if (var) k_restrict<T, true, false><<<g, 256, 0, st>>>(fine, coarse, rt.start, rt.nb, rt.nrows, phi, rhs, rhs_c, fx, fy, fz);
+  else k_restrict<T, false, false><<<g, 256, 0, st>>>(fine, coarse, rt.start, rt.nb, rt.nrows, phi, rhs, rhs_c, fx, fy, fz);
   return cudaGetLastError();
 }
 
 template <typename T>
-cudaError_t launch_prolong(bool zero_old, const BlkLev* fine, const BlkLev* coarse, CellTab ct, const T* phi_c,
+cudaError_t launch_prolong(bool zero_old, const BlkLev* fine, const BlkLev* coarse, RowTab rt, const T* phi_c,
                            const T* old, T* out, cudaStream_t st) {
-  if (ct.ncta <= 0) return cudaSuccess;
-  if (zero_old) k_prolong<T, true><<<ct.ncta, 256, 0, st>>>(fine, coarse, ct.cta_start, ct.nb, phi_c, old, out);
-  else k_prolong<T, false><<<ct.ncta, 256, 0, st>>>(fine, coarse, ct.cta_start, ct.nb, phi_c, old, out);
+  if (rt.nrows <= 0) return cudaSuccess;
+  const int g = row_grid(rt.nrows);
+  if (zero_old) k_prolong<T, true><<<g, 256, 0, st>>>(fine, coarse, rt.start, rt.nb, rt.nrows, phi_c, old, out);
+  else k_prolong<T, false><<<g, 256, 0, st>>>(fine, coarse, rt.start, rt.nb, rt.nrows, phi_c, old, out);
   return cudaGetLastError();
+}
+
+int defect_grid(int nrows) {
+  int g = (nrows + 7) / 8;
+  return g < 1 ? 1 : (g > kDefectCtas ? kDefectCtas : g);
 }
 
 template <typename TE, typename TR>
-cudaError_t launch_defect(bool var, const BlkLev* bl, CellTab ct, const double* p, const TE* e, double* p_next,
+cudaError_t launch_defect(bool var, const BlkLev* bl, RowTab rt, const double* p, const TE* e, double* p_next,
                           const double* b, TR* rhs_out, double mean_b, double rscale, const double* fx,
                           const double* fy, const double* fz, double* partials, cudaStream_t st) {
-  if (ct.ncta <= 0) return cudaSuccess;
+  if (rt.nrows <= 0) return cudaSuccess;
+  const int g = defect_grid(rt.nrows);
   if (e) {
-    if (var) k_defect<TE, TR, true, true><<<ct.ncta, 256, 0, st>>>(bl, ct.cta_start, ct.nb, p, e, p_next, b, rhs_out, mean_b, rscale, fx, fy, fz, partials);
-    else k_defect<TE, TR, true, false><<<ct.ncta, 256, 0, st>>>(bl, ct.cta_start, ct.nb, p, e, p_next, b, rhs_out, mean_b, rscale, fx, fy, fz, partials);
+    if (var) k_defect<TE, TR, true, true><<<g, 256, 0, st>>>(bl, rt.start, rt.nb, rt.nrows, p, e, p_next, b, rhs_out, mean_b, rscale, fx, fy, fz, partials);
+    else k_defect<TE, TR, true, false><<<g, 256, 0, st>>>(bl, rt.start, rt.nb, rt.nrows, p, e, p_next, b, rhs_out, mean_b, rscale, fx, fy, fz, partials);
   } else {
-    if (var) k_defect<TE, TR, false, true><<<ct.ncta, 256, 0, st>>>(bl, ct.cta_start, ct.nb, p, e, p_next, b, rhs_out, mean_b, rscale, fx, fy, fz, partials);
-    else k_defect<TE, TR, false, false><<<ct.ncta, 256, 0, st>>>(bl, ct.cta_start, ct.nb, p, e, p_next, b, rhs_out, mean_b, rscale, fx, fy, fz, partials);
+    if (var) k_defect<TE, TR, false, true><<<g, 256, 0, st>>>(bl, rt.start, rt.nb, rt.nrows, p, e, p_next, b, rhs_out, mean_b, rscale, fx, fy, fz, partials);
+    else k_defect<TE, TR, false, false><<<g, 256, 0, st>>>(bl, rt.start, rt.nb, rt.nrows, p, e, p_next, b, rhs_out, mean_b, rscale, fx, fy, fz, partials);
   }
   return cudaGetLastError();
 }
@@ -560,28 +1034,30 @@ cudaError_t launch_face_coef(const BlkLev* bl, CellTab ct, const double* dens, c
 }
 
 // explicit instantiations
-template cudaError_t launch_rbgs<double>(int, bool, bool, const BlkLev*, const Tile*, int, int, const double*, double*,
-                                         const double*, const double*, const double*, const double*, cudaStream_t);
-template cudaError_t launch_rbgs<float>(int, bool, bool, const BlkLev*, const Tile*, int, int, const float*, float*,
-                                        const float*, const float*, const float*, const float*, cudaStream_t);
+template cudaError_t launch_rbgs<double>(int, bool, bool, const BlkLev*, const Tile*, int, int, const CUtensorMap*,
+                                         int*, const double*, double*, const double*, const double*, const double*,
+                                         const double*, cudaStream_t);
+template cudaError_t launch_rbgs<float>(int, bool, bool, const BlkLev*, const Tile*, int, int, const CUtensorMap*,
+                                        int*, const float*, float*, const float*, const float*, const float*,
+                                        const float*, cudaStream_t);
 template cudaError_t launch_fill<double>(const uint32_t*, const uint32_t*, int64_t, double*, const double*,
                                          const double*, bool, cudaStream_t);
 template cudaError_t launch_fill<float>(const uint32_t*, const uint32_t*, int64_t, float*, const float*, const float*,
                                         bool, cudaStream_t);
-template cudaError_t launch_restrict<double>(bool, bool, const BlkLev*, const BlkLev*, CellTab, const double*,
+template cudaError_t launch_restrict<double>(bool, bool, const BlkLev*, const BlkLev*, RowTab, const double*,
                                              const double*, double*, const double*, const double*, const double*,
                                              cudaStream_t);
-template cudaError_t launch_restrict<float>(bool, bool, const BlkLev*, const BlkLev*, CellTab, const float*,
+template cudaError_t launch_restrict<float>(bool, bool, const BlkLev*, const BlkLev*, RowTab, const float*,
                                             const float*, float*, const float*, const float*, const float*,
                                             cudaStream_t);
-template cudaError_t launch_prolong<double>(bool, const BlkLev*, const BlkLev*, CellTab, const double*, const double*,
+template cudaError_t launch_prolong<double>(bool, const BlkLev*, const BlkLev*, RowTab, const double*, const double*,
                                             double*, cudaStream_t);
-template cudaError_t launch_prolong<float>(bool, const BlkLev*, const BlkLev*, CellTab, const float*, const float*,
+template cudaError_t launch_prolong<float>(bool, const BlkLev*, const BlkLev*, RowTab, const float*, const float*,
                                            float*, cudaStream_t);
-template cudaError_t launch_defect<double, double>(bool, const BlkLev*, CellTab, const double*, const double*, double*,
+template cudaError_t launch_defect<double, double>(bool, const BlkLev*, RowTab, const double*, const double*, double*,
                                                    const double*, double*, double, double, const double*,
                                                    const double*, const double*, double*, cudaStream_t);
-template cudaError_t launch_defect<float, float>(bool, const BlkLev*, CellTab, const double*, const float*, double*,
+template cudaError_t launch_defect<float, float>(bool, const BlkLev*, RowTab, const double*, const float*, double*,
                                                  const double*, float*, double, double, const double*, const double*,
                                                  const double*, double*, cudaStream_t);
 

@@ -1,5 +1,6 @@
 // Device kernels of the multigrid V-cycle (declarations of the launchers).
 #pragma once
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include "h3d_internal.h"
@@ -14,18 +15,43 @@ struct CellTab {
   int ncta;
 };
 
-// Smoother tile shapes the runtime can choose (autotuned per level).
+// Row table: one warp per row; start[b] is the first row of block b,
+// start[nb] == nrows.
+struct RowTab {
+  const int* start;  // device
+  int nb;
+  int nrows;
+};
+
+// Smoother tile shapes the runtime can choose (autotuned per level).  Row
+// shapes (rows == true) span whole rows: usable when every block's nx is even
+// and <= tx.
 struct TileShape {
   int tx, ty, nt;
+  bool rows;
+  int tpr, cp;
+  bool tma;  // planes staged by TMA (needs tensor maps of the source buffer)
+  int alt;   // for TMA shapes: the equivalent row shape (used for zero sources)
 };
+// TMA box heights (TY+4) are one of these; tensor maps are built per height.
+constexpr int kNumTmaTy = 3;
+int tma_ty_index(int ty);  // 0,1,2 for TY = 4, 8, 16; -1 otherwise
+constexpr int kDefectCtas = 148 * 4;  // CTAs (and partial sums) of the defect kernel
+int defect_grid(int nrows);
+// Sets the dynamic shared-memory limits of the row-tile smoothers (call once
+// per device before any launch or capture).
+cudaError_t init_kernel_attributes();
 int num_tile_shapes();
 TileShape tile_shape(int variant);
 
 // One out-of-place red-black sweep (both colours) of every block of a level:
 // dst = sweep(src).  zero_src: src is identically zero (not read).
+// maps: tensor maps of src for every block (TMA variants); err: device flag
+// set when a bounded wait gives up.
 template <typename T>
 cudaError_t launch_rbgs(int variant, bool var, bool zero_src, const BlkLev* bl, const Tile* tiles,
-                        int ntiles, int zc, const T* src, T* dst, const T* rhs, const T* fx, const T* fy,
+                        int ntiles, int zc, const CUtensorMap* maps, int* err, const T* src, T* dst,
+                        const T* rhs, const T* fx, const T* fy,
                         const T* fz, cudaStream_t st);
 
 // Ghost gather: out[dst[e]] = (src[e] & old) ? old[src] : cur[src].
@@ -36,21 +62,21 @@ cudaError_t launch_fill(const uint32_t* dsts, const uint32_t* srcs, int64_t n, T
 // Residual of the fine level and 8-cell average into the coarse rhs
 // (mgrestr, mgsolver.for:693-756).  zero_phi: fine iterate is zero.
 template <typename T>
-cudaError_t launch_restrict(bool var, bool zero_phi, const BlkLev* fine, const BlkLev* coarse, CellTab ct,
+cudaError_t launch_restrict(bool var, bool zero_phi, const BlkLev* fine, const BlkLev* coarse, RowTab rt,
                             const T* phi, const T* rhs, T* rhs_c, const T* fx, const T* fy, const T* fz,
                             cudaStream_t st);
 
 // Trilinear correction (mgcorr, mgsolver.for:828-896) with the following
 // mgbound fused: out = old + P(coarse), evaluated at the mgbound source.
 template <typename T>
-cudaError_t launch_prolong(bool zero_old, const BlkLev* fine, const BlkLev* coarse, CellTab ct,
+cudaError_t launch_prolong(bool zero_old, const BlkLev* fine, const BlkLev* coarse, RowTab rt,
                            const T* phi_c, const T* old, T* out, cudaStream_t st);
 
 // Level-1 FP64 defect: pn = p + e (all cells, when e != null), r = b - A pn on
 // the interior, rhs_out = r - mean_b (as TR), per-CTA partial sums
 // {sum r^2, sum b^2, max |r|*rscale, sum r} into partials[4*cta].
 template <typename TE, typename TR>
-cudaError_t launch_defect(bool var, const BlkLev* bl, CellTab ct, const double* p, const TE* e,
+cudaError_t launch_defect(bool var, const BlkLev* bl, RowTab rt, const double* p, const TE* e,
                           double* p_next, const double* b, TR* rhs_out, double mean_b, double rscale,
                           const double* fx, const double* fy, const double* fz, double* partials,
                           cudaStream_t st);

@@ -2,6 +2,8 @@
 // schedule (the reference's K-cycle control flow, mgsolver.for:272-352),
 // CUDA-graph capture, the FP64 outer defect correction (newsolv_mg.for) and
 // the C ABI declared in include/h3d_mg.h.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -26,6 +28,7 @@ struct Halo {
   uint32_t* d_dst = nullptr;
   uint32_t* d_src = nullptr;
   int64_t n = 0;
+  bool built = false;
 };
 
 struct Level {
@@ -35,6 +38,10 @@ struct Level {
   int ncta_all = 0;
   int* d_cta_int = nullptr;  // interior cells
   int ncta_int = 0;
+  int* d_rows_all = nullptr;  // all rows (y, z incl. ghosts)
+  int nrows_all = 0;
+  int* d_rows_int = nullptr;  // interior rows
+  int nrows_int = 0;
   Tile* d_tiles = nullptr;
   int ntiles = 0;
   int variant = 0, zc = 1;
@@ -46,6 +53,8 @@ struct Level {
   float *fx32 = nullptr, *fy32 = nullptr, *fz32 = nullptr;
   double* dens = nullptr;
   Halo sweep, faces, exch, bound;
+  CUtensorMap* d_maps = nullptr;  // [ty index][buffer][block] tensor maps of the iterate
+  bool tma_ok = false;
   int cur64 = 0, cur32 = 0;
   bool zero64 = false, zero32 = false;
   double sweep_bytes = 0;  // algorithmic bytes of one sweep (FP64 or FP32 by mode)
@@ -76,6 +85,7 @@ struct h3d_mg {
   double* d_res = nullptr;
   double* h_res = nullptr;  // pinned, 4 doubles
   double* d_h3 = nullptr;   // per-block dx,dy,dz
+  int* d_err = nullptr;     // set by a device wait that gave up
   double mean_b = 0.0;
   bool coeffs_ready = false;
   std::string last_error;
@@ -147,6 +157,30 @@ int build_cta_table(h3d_mg* h, const LevelGeom& G, bool interior, int** d_tab, i
   return H3D_OK;
 }
 
+int build_row_table(h3d_mg* h, const LevelGeom& G, bool interior, int** d_tab, int* nrows) {
+  std::vector<int> start(G.bl.size() + 1, 0);
+  for (size_t b = 0; b < G.bl.size(); ++b) {
+    const BlkLev& B = G.bl[b];
+    long long rows = interior ? (long long)B.ny * B.nz : (long long)(B.ny + 2) * (B.nz + 2);
+    if ((long long)start[b] + rows >= (1LL << 31)) return fail(h, H3D_ERR_BAD_CONFIG, "too many rows");
+    start[b + 1] = start[b] + (int)rows;
+  }
+  *nrows = start.back();
+  TRY(dalloc(h, d_tab, start.size()));
+  CU(cudaMemcpy(*d_tab, start.data(), start.size() * sizeof(int), cudaMemcpyHostToDevice));
+  return H3D_OK;
+}
+
+// A row-tile smoother variant needs every block's nx even and within its row.
+bool variant_fits(const Level& Lv, int variant) {
+  TileShape s = tile_shape(variant);
+  if (!s.rows) return true;
+  if (s.tma && !Lv.tma_ok) return false;
+  for (const auto& B : Lv.geom.bl)
+    if ((B.nx & 1) || B.nx > s.tx) return false;
+  return true;
+}
+
 int build_tiles(h3d_mg* h, Level& Lv, int variant, int zc) {
   TileShape s = tile_shape(variant);
   std::vector<Tile> t;
@@ -180,6 +214,12 @@ void default_tile(const Level& Lv, int* variant, int* zc) {
   else if (nxm >= 16) v = 3;
   else if (nxm >= 8) v = nym >= 8 ? 4 : 5;
   else v = 6;
+  // whole-row tiles when every block allows them (TMA-staged first)
+  const int pref[] = {24, 23, 21, 20, 13, 12, 10, 8, 14, 16};
+  for (int cand : pref) {
+    TileShape c = tile_shape(cand);
+    if (nxm <= c.tx && nxm * 2 > c.tx / 2 && variant_fits(Lv, cand) && nym >= 4) { v = cand; break; }
+  }
   TileShape s = tile_shape(v);
   for (const auto& B : Lv.geom.bl) xy_tiles += (long long)((B.nx + s.tx - 1) / s.tx) * ((B.ny + s.ty - 1) / s.ty);
   int z = nzm;
@@ -190,6 +230,15 @@ void default_tile(const Level& Lv, int* variant, int* zc) {
 
 
 // ------------------------------------------------------------------ executor
+// Tensor maps of buffer `buf` for the level's smoother variant (or null).
+const CUtensorMap* sweep_maps(const Level& V, int buf) {
+  TileShape s = tile_shape(V.variant);
+  if (!s.tma || !V.tma_ok) return nullptr;
+  int ti = tma_ty_index(s.ty);
+  if (ti < 0) return nullptr;
+  return V.d_maps + ((size_t)ti * 2 + buf) * V.geom.bl.size();
+}
+
 // FP32 iterate at level g?  Mixed solves run every level but the coarsest in
 // FP32; the coarsest level (the coarse solve) stays FP64.
 bool f32_level(const h3d_mg* h, int g) { return h->mixed && !(g == h->L && h->L > 1); }
@@ -225,7 +274,8 @@ struct Exec {
     if (mixed_level(g)) {
       float* src = V.phi32[V.cur32];
       float* dst = V.phi32[1 - V.cur32];
-      CU(launch_rbgs<float>(V.variant, h->var, V.zero32, V.d_bl, V.d_tiles, V.ntiles, V.zc, src, dst, V.rhs32,
+      CU(launch_rbgs<float>(V.variant, h->var, V.zero32, V.d_bl, V.d_tiles, V.ntiles, V.zc, sweep_maps(V, V.cur32),
+                            h->d_err, src, dst, V.rhs32,
                             V.fx32, V.fy32, V.fz32, st));
       if (e1) CU(record(e1));
       CU(launch_fill<float>(V.sweep.d_dst, V.sweep.d_src, V.sweep.n, dst, dst, src, V.zero32, st));
@@ -234,7 +284,8 @@ struct Exec {
     } else {
       double* src = V.phi64[V.cur64];
       double* dst = V.phi64[1 - V.cur64];
-      CU(launch_rbgs<double>(V.variant, h->var, V.zero64, V.d_bl, V.d_tiles, V.ntiles, V.zc, src, dst, V.rhs64,
+      CU(launch_rbgs<double>(V.variant, h->var, V.zero64, V.d_bl, V.d_tiles, V.ntiles, V.zc, sweep_maps(V, V.cur64),
+                             h->d_err, src, dst, V.rhs64,
                              V.fx64, V.fy64, V.fz64, st));
       if (e1) CU(record(e1));
       CU(launch_fill<double>(V.sweep.d_dst, V.sweep.d_src, V.sweep.n, dst, dst, src, V.zero64, st));
@@ -254,7 +305,7 @@ struct Exec {
   int restrict_to(int gc) {
     Level& F = L(gc - 1);
     Level& C = L(gc);
-    CellTab ct{C.d_cta_int, (int)C.geom.bl.size(), C.ncta_int};
+    RowTab ct{C.d_rows_int, (int)C.geom.bl.size(), C.nrows_int};
     if (mixed_level(gc - 1)) {
       // the coarsest level of a mixed solve keeps an FP32 rhs too (converted after)
       CU(launch_restrict<float>(h->var, F.zero32, F.d_bl, C.d_bl, ct, F.phi32[F.cur32], F.rhs32, C.rhs32, F.fx32,
@@ -278,7 +329,7 @@ struct Exec {
   int correct(int gf) {
     Level& F = L(gf);
     Level& C = L(gf + 1);
-    CellTab ct{F.d_cta_all, (int)F.geom.bl.size(), F.ncta_all};
+    RowTab ct{F.d_rows_all, (int)F.geom.bl.size(), F.nrows_all};
     if (mixed_level(gf)) {
       const float* pc;
       if (mixed_level(gf + 1)) {
@@ -361,7 +412,7 @@ struct Exec {
   // FP64 defect on the resident p/b: e = level-1 iterate (or none).
   int defect(bool with_e) {
     Level& V = L(1);
-    CellTab ct{V.d_cta_all, (int)V.geom.bl.size(), V.ncta_all};
+    RowTab ct{V.d_rows_all, (int)V.geom.bl.size(), V.nrows_all};
     double rscale = h->var ? 1.0 : V.geom.bl[0].dv;
     const double* fx = h->var ? V.fx64 : nullptr;
     const double* fy = h->var ? V.fy64 : nullptr;
@@ -386,7 +437,7 @@ struct Exec {
                                        fz, h->partials, h->st));
     }
     if (with_e) h->pc = 1 - h->pc;
-    CU(launch_reduce4(h->partials, ct.ncta, h->d_res, h->st));
+    CU(launch_reduce4(h->partials, defect_grid(ct.nrows), h->d_res, h->st));
     CU(cudaMemcpyAsync(h->h_res, h->d_res, 4 * sizeof(double), cudaMemcpyDeviceToHost, h->st));
     h->kernels += 2;
     return H3D_OK;
@@ -512,7 +563,7 @@ int copy_field_3d(h3d_mg* h, bool to_device, double* dev_base, const BlkLev& B, 
   const int g0 = with_ghosts ? 0 : 1;
   const int ex = with_ghosts ? B.nx + 2 : B.nx, ey = with_ghosts ? B.ny + 2 : B.ny, ez = with_ghosts ? B.nz + 2 : B.nz;
   cudaMemcpy3DParms p{};
-  cudaPitchedPtr dptr = make_cudaPitchedPtr(dev_base + B.off, (size_t)(B.nx + 2) * 8, B.nx + 2, B.ny + 2);
+  cudaPitchedPtr dptr = make_cudaPitchedPtr(dev_base + B.off, (size_t)B.sx * 8, B.nx + 2, B.ny + 2);
   cudaPitchedPtr hptr = make_cudaPitchedPtr(host, (size_t)d.ttc[0] * 8, d.ttc[0], d.ttc[1]);
   cudaPos dpos = make_cudaPos((size_t)g0 * 8, g0, g0);
   cudaPos hpos = make_cudaPos((size_t)(d.pl - 1 + g0) * 8, d.pl - 1 + g0, d.pl - 1 + g0);
@@ -533,6 +584,66 @@ int check_block_host_dims(h3d_mg* h, const h3d_block_desc& d) {
   return H3D_OK;
 }
 
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }
+  return fn;
+}
+
+// Tensor maps of both iterate buffers of level g for every TMA box height:
+// dims (nx+2, ny+2, nz+2), strides (sx, sxy) elements, box (BX, TY+4, 1),
+// out-of-bounds rows read as zero.  Levels whose row width exceeds one box
+// (BX > 256) or with an odd nx keep the plain-load smoothers.
+int build_tensor_maps(h3d_mg* h, int g) {
+  Level& V = h->lev[g];
+  const bool f32 = f32_level(h, g);
+  const int es = f32 ? 4 : 8, vec = 16 / es;
+  for (const auto& B : V.geom.bl) {
+    int bx = (B.nx + 2 + vec - 1) / vec * vec;
+    if ((B.nx & 1) || bx > 256) return H3D_OK;
+  }
+  auto enc = encode_fn();
+  if (!enc) return H3D_OK;
+  const size_t nb = V.geom.bl.size();
+  std::vector<CUtensorMap> maps((size_t)kNumTmaTy * 2 * nb);
+  const int tys[kNumTmaTy] = {4, 8, 16};
+  for (int ti = 0; ti < kNumTmaTy; ++ti)
+    for (int buf = 0; buf < 2; ++buf)
+      for (size_t b = 0; b < nb; ++b) {
+        const BlkLev& B = V.geom.bl[b];
+        void* base = f32 ? (void*)(V.phi32[buf] + B.off) : (void*)(V.phi64[buf] + B.off);
+        cuuint64_t dims[3] = {(cuuint64_t)B.nx + 2, (cuuint64_t)B.ny + 2, (cuuint64_t)B.nz + 2};
+        cuuint64_t strides[2] = {(cuuint64_t)B.sx * es, (cuuint64_t)B.sxy * es};
+        cuuint32_t box[3] = {(cuuint32_t)((B.nx + 2 + vec - 1) / vec * vec), (cuuint32_t)(tys[ti] + 4), 1};
+        cuuint32_t estr[3] = {1, 1, 1};
+        CUresult r = enc(&maps[((size_t)ti * 2 + buf) * nb + b], f32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32
+                                                                     : CU_TENSOR_MAP_DATA_TYPE_FLOAT64,
+                         3, base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                         CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if (r != CUDA_SUCCESS) return H3D_OK;  // keep the plain-load smoothers
+      }
+  TRY(dalloc(h, &V.d_maps, maps.size()));
+  CU(cudaMemcpy(V.d_maps, maps.data(), maps.size() * sizeof(CUtensorMap), cudaMemcpyHostToDevice));
+  V.tma_ok = true;
+  return H3D_OK;
+}
+
+int check_device_error(h3d_mg* h) {
+  int e = 0;
+  CU(cudaMemcpy(&e, h->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (e) {
+    CU(cudaMemset(h->d_err, 0, sizeof(int)));
+    return fail(h, H3D_ERR_TIMEOUT, "a bounded device wait gave up (TMA copy did not complete)");
+  }
+  return H3D_OK;
+}
+
 int autotune_level(h3d_mg* h, int g) {
   Level& V = h->lev[g];
   int best_v = V.variant, best_z = V.zc;
@@ -546,16 +657,19 @@ int autotune_level(h3d_mg* h, int g) {
   const bool f32 = f32_level(h, g);
   for (int v = 0; v < num_tile_shapes(); ++v) {
     TileShape s = tile_shape(v);
-    if (s.tx > 2 * nxm || s.ty > 2 * nym || s.tx < 8) continue;
+    if (!variant_fits(V, v)) continue;
+    if (s.rows ? (s.tx >= 4 * nxm) : (s.tx > 2 * nxm || s.ty > 2 * nym || s.tx < 8)) continue;
     for (int zc : {8, 16, 32, 64, 128, 256}) {
       if (zc > nzm) continue;
       TRY(build_tiles(h, V, v, zc));
       float tot = 0;
       for (int rep = 0; rep < 4; ++rep) {
         CU(cudaEventRecord(a, h->st));
-        if (f32) CU(launch_rbgs<float>(v, h->var, false, V.d_bl, V.d_tiles, V.ntiles, zc, V.phi32[V.cur32],
+        if (f32) CU(launch_rbgs<float>(v, h->var, false, V.d_bl, V.d_tiles, V.ntiles, zc, sweep_maps(V, V.cur32),
+                                       h->d_err, V.phi32[V.cur32],
                                        V.phi32[1 - V.cur32], V.rhs32, V.fx32, V.fy32, V.fz32, h->st));
-        else CU(launch_rbgs<double>(v, h->var, false, V.d_bl, V.d_tiles, V.ntiles, zc, V.phi64[V.cur64],
+        else CU(launch_rbgs<double>(v, h->var, false, V.d_bl, V.d_tiles, V.ntiles, zc, sweep_maps(V, V.cur64),
+                                    h->d_err, V.phi64[V.cur64],
                                     V.phi64[1 - V.cur64], V.rhs64, V.fx64, V.fy64, V.fz64, h->st));
         CU(cudaEventRecord(b, h->st));
         CU(cudaEventSynchronize(b));
@@ -683,10 +797,10 @@ int h3d_mg_destroy(h3d_mg* h) {
   for (auto e : h->ev_eager) cudaEventDestroy(e);
   for (size_t g = 1; g < h->lev.size(); ++g) {
     Level& V = h->lev[g];
-    void* ps[] = {V.d_bl, V.d_cta_all, V.d_cta_int, V.d_tiles, V.phi64[0], V.phi64[1], V.rhs64, V.phi32[0],
+    void* ps[] = {V.d_bl, V.d_cta_all, V.d_cta_int, V.d_rows_all, V.d_rows_int, V.d_tiles, V.phi64[0], V.phi64[1], V.rhs64, V.phi32[0],
                   V.phi32[1], V.rhs32, V.fx64, V.fy64, V.fz64, V.fx32, V.fy32, V.fz32, V.dens,
                   V.sweep.d_dst, V.sweep.d_src, V.faces.d_dst, V.faces.d_src, V.exch.d_dst, V.exch.d_src,
-                  V.bound.d_dst, V.bound.d_src};
+                  V.bound.d_dst, V.bound.d_src, V.d_maps};
     for (void* p : ps) dfree(p);
   }
   dfree(h->p64[0]);
@@ -695,6 +809,7 @@ int h3d_mg_destroy(h3d_mg* h) {
   dfree(h->partials);
   dfree(h->d_res);
   dfree(h->d_h3);
+  dfree(h->d_err);
   if (h->h_res) cudaFreeHost(h->h_res);
   if (h->st) cudaStreamDestroy(h->st);
   delete h;
@@ -752,18 +867,18 @@ int h3d_mg_create(h3d_mg** out, const h3d_mg_desc* desc) {
   if (cudaSetDevice(h->device) != cudaSuccess) return bail(fail(h, H3D_ERR_NO_DEVICE, "cudaSetDevice failed"));
   if (cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking) != cudaSuccess)
     return bail(fail(h, H3D_ERR_CUDA, "stream create failed"));
+  if (init_kernel_attributes() != cudaSuccess) return bail(fail(h, H3D_ERR_CUDA, "kernel attributes"));
   h->lev.resize(h->L + 1);
   for (int g = 1; g <= h->L; ++g) {
     Level& V = h->lev[g];
-    V.geom = make_level_geom(h->blocks, g);
+    V.geom = make_level_geom(h->blocks, g, true);
     if ((rc = dalloc(h, &V.d_bl, V.geom.bl.size())) != H3D_OK) return bail(rc);
     if (cudaMemcpy(V.d_bl, V.geom.bl.data(), V.geom.bl.size() * sizeof(BlkLev), cudaMemcpyHostToDevice) != cudaSuccess)
       return bail(fail(h, H3D_ERR_CUDA, "copy level geometry"));
     if ((rc = build_cta_table(h, V.geom, false, &V.d_cta_all, &V.ncta_all)) != H3D_OK) return bail(rc);
     if ((rc = build_cta_table(h, V.geom, true, &V.d_cta_int, &V.ncta_int)) != H3D_OK) return bail(rc);
-    int var_, zc;
-    default_tile(V, &var_, &zc);
-    if ((rc = build_tiles(h, V, var_, zc)) != H3D_OK) return bail(rc);
+    if ((rc = build_row_table(h, V.geom, false, &V.d_rows_all, &V.nrows_all)) != H3D_OK) return bail(rc);
+    if ((rc = build_row_table(h, V.geom, true, &V.d_rows_int, &V.nrows_int)) != H3D_OK) return bail(rc);
     const size_t n = (size_t)V.geom.n_elems;
     const bool need64 = !f32_level(h, g);
     const bool need32 = h->mixed;
@@ -788,12 +903,16 @@ int h3d_mg_create(h3d_mg** out, const h3d_mg_desc* desc) {
     }
     std::vector<uint32_t> d, s;
     std::string err;
-    if ((rc = build_halo_table(h->blocks, g, kHaloSweep, d, s, &err)) != H3D_OK) return bail(fail(h, rc, err));
+    if ((rc = build_halo_table(h->blocks, g, kHaloSweep, true, d, s, &err)) != H3D_OK) return bail(fail(h, rc, err));
     if ((rc = upload_halo(h, V.sweep, d, s)) != H3D_OK) return bail(rc);
     if (g == 1) {
-      if ((rc = build_halo_table(h->blocks, g, kHaloFaces, d, s, &err)) != H3D_OK) return bail(fail(h, rc, err));
+      if ((rc = build_halo_table(h->blocks, g, kHaloFaces, true, d, s, &err)) != H3D_OK) return bail(fail(h, rc, err));
       if ((rc = upload_halo(h, V.faces, d, s)) != H3D_OK) return bail(rc);
     }
+    if ((rc = build_tensor_maps(h, g)) != H3D_OK) return bail(rc);
+    int var_, zc;
+    default_tile(V, &var_, &zc);
+    if ((rc = build_tiles(h, V, var_, zc)) != H3D_OK) return bail(rc);
     // bytes of one sweep: read phi + rhs, write phi (+3 face arrays when variable)
     double w = f32_level(h, g) ? 4.0 : 8.0;
     V.sweep_bytes = (double)V.geom.n_interior * w * (3.0 + (h->var ? 3.0 : 0.0));
@@ -801,13 +920,14 @@ int h3d_mg_create(h3d_mg** out, const h3d_mg_desc* desc) {
   const size_t n1 = (size_t)h->lev[1].geom.n_elems;
   if ((rc = dalloc(h, &h->p64[0], n1)) || (rc = dalloc(h, &h->p64[1], n1)) || (rc = dalloc(h, &h->b64, n1)))
     return bail(rc);
-  h->npartials = std::max(h->lev[1].ncta_all, h->lev[1].ncta_int);
+  h->npartials = std::max(std::max(h->lev[1].ncta_all, h->lev[1].ncta_int), kDefectCtas);
   if ((rc = dalloc(h, &h->partials, 4 * (size_t)h->npartials)) || (rc = dalloc(h, &h->d_res, 4))) return bail(rc);
   if (cudaMallocHost((void**)&h->h_res, 4 * sizeof(double)) != cudaSuccess)
     return bail(fail(h, H3D_ERR_OOM, "pinned result buffer"));
   std::vector<double> h3;
   for (const auto& d : h->blocks) { h3.push_back(d.h[0]); h3.push_back(d.h[1]); h3.push_back(d.h[2]); }
   if ((rc = dalloc(h, &h->d_h3, h3.size())) != H3D_OK) return bail(rc);
+  if ((rc = dalloc(h, &h->d_err, 1)) != H3D_OK) return bail(rc);
   if (cudaMemcpy(h->d_h3, h3.data(), h3.size() * 8, cudaMemcpyHostToDevice) != cudaSuccess)
     return bail(fail(h, H3D_ERR_CUDA, "copy spacings"));
   if (cudaStreamSynchronize(h->st) != cudaSuccess) return bail(fail(h, H3D_ERR_CUDA, "set-up sync"));
@@ -986,6 +1106,7 @@ int h3d_mg_solve_resident(h3d_mg* h, const h3d_solve_opts* opts, h3d_solve_info*
   I.smoother_launches = prof_n;
   I.kernel_launches = h->kernels - k0;
   if (info) *info = I;
+  TRY(check_device_error(h));
   if (status == 2) return fail(h, H3D_ERR_DIVERGED, "residual is not finite or grew beyond 1e8");
   if (status != 0) return fail(h, H3D_ERR_NOT_CONVERGED, "not converged within maxcy cycles");
   return H3D_OK;
@@ -1020,9 +1141,29 @@ int h3d_mg_history(h3d_mg* h, double* out, int32_t cap, int32_t* n) {
 // ---------------------------------------------------------- level hooks
 static int level_ok(h3d_mg* h, int g) { return h && g >= 1 && g <= h->L; }
 
+}  // extern "C"
+
+// Copies a dense canonical block array (nz+2, ny+2, nx+2) of element type T
+// to/from the padded device layout of block B.
+template <typename T>
+static int copy_canonical(h3d_mg* h, bool to_device, T* dev_level, const BlkLev& B, T* host) {
+  cudaMemcpy3DParms p{};
+  cudaPitchedPtr dptr = make_cudaPitchedPtr(dev_level + B.off, (size_t)B.sx * sizeof(T), B.nx + 2, B.ny + 2);
+  cudaPitchedPtr hptr = make_cudaPitchedPtr(host, (size_t)(B.nx + 2) * sizeof(T), B.nx + 2, B.ny + 2);
+  if (to_device) { p.srcPtr = hptr; p.dstPtr = dptr; p.kind = cudaMemcpyHostToDevice; }
+  else { p.srcPtr = dptr; p.dstPtr = hptr; p.kind = cudaMemcpyDeviceToHost; }
+  p.extent = make_cudaExtent((size_t)(B.nx + 2) * sizeof(T), B.ny + 2, B.nz + 2);
+  CU(cudaMemcpy3DAsync(&p, h->st));
+  CU(cudaStreamSynchronize(h->st));
+  return H3D_OK;
+}
+
+extern "C" {
+
 int h3d_mg_put_level(h3d_mg* h, int32_t g, int32_t field, int32_t ib, const double* a) {
   if (!level_ok(h, g) || !a || ib < 0 || ib >= (int)h->blocks.size() || field < 0 || field > 1) return H3D_ERR_ARG;
   CU(cudaSetDevice(h->device));
+  CU(cudaStreamSynchronize(h->st));
   Level& V = h->lev[g];
   const BlkLev& B = V.geom.bl[ib];
   const size_t nb = (size_t)(B.nx + 2) * (B.ny + 2) * (B.nz + 2);
@@ -1038,17 +1179,10 @@ int h3d_mg_put_level(h3d_mg* h, int32_t g, int32_t field, int32_t ib, const doub
   const bool f32 = f32_level(h, g);
   if (f32) {
     std::vector<float> fb(buf.begin(), buf.end());
-    float* dst = field == 0 ? V.phi32[V.cur32] + B.off : V.rhs32 + B.off;
-    if (field == 1) {  // keep the existing ghost entries of the rhs untouched: copy interior rows only
-      for (int z = 1; z <= B.nz; ++z)
-        CU(cudaMemcpy(dst + (size_t)z * B.sxy, fb.data() + (size_t)z * B.sxy, B.sxy * 4, cudaMemcpyHostToDevice));
-    } else {
-      CU(cudaMemcpy(dst, fb.data(), nb * 4, cudaMemcpyHostToDevice));
-      V.zero32 = false;
-    }
+    TRY(copy_canonical<float>(h, true, field == 0 ? V.phi32[V.cur32] : V.rhs32, B, fb.data()));
+    if (field == 0) V.zero32 = false;
   } else {
-    double* dst = field == 0 ? V.phi64[V.cur64] + B.off : V.rhs64 + B.off;
-    CU(cudaMemcpy(dst, buf.data(), nb * 8, cudaMemcpyHostToDevice));
+    TRY(copy_canonical<double>(h, true, field == 0 ? V.phi64[V.cur64] : V.rhs64, B, buf.data()));
     if (field == 0) V.zero64 = false;
   }
   return H3D_OK;
@@ -1067,12 +1201,10 @@ int h3d_mg_get_level(h3d_mg* h, int32_t g, int32_t field, int32_t ib, double* a)
   if (!(field == 0 && zero)) {
     if (f32) {
       std::vector<float> fb(nb);
-      const float* src = field == 0 ? V.phi32[V.cur32] + B.off : V.rhs32 + B.off;
-      CU(cudaMemcpy(fb.data(), src, nb * 4, cudaMemcpyDeviceToHost));
+      TRY(copy_canonical<float>(h, false, field == 0 ? V.phi32[V.cur32] : V.rhs32, B, fb.data()));
       for (size_t q = 0; q < nb; ++q) buf[q] = fb[q];
     } else {
-      const double* src = field == 0 ? V.phi64[V.cur64] + B.off : V.rhs64 + B.off;
-      CU(cudaMemcpy(buf.data(), src, nb * 8, cudaMemcpyDeviceToHost));
+      TRY(copy_canonical<double>(h, false, field == 0 ? V.phi64[V.cur64] : V.rhs64, B, buf.data()));
     }
   }
   if (field == 0) {
@@ -1093,7 +1225,7 @@ int h3d_mg_mgrelax(h3d_mg* h, int32_t g, int32_t it) {
   Exec ex{h};
   TRY(ex.relax(g, it));
   CU(cudaStreamSynchronize(h->st));
-  return H3D_OK;
+  return check_device_error(h);
 }
 
 int h3d_mg_mgrestr(h3d_mg* h, int32_t g) {
@@ -1124,13 +1256,13 @@ static int apply_table_hook(h3d_mg* h, int g, int kind) {
   CU(cudaSetDevice(h->device));
   Level& V = h->lev[g];
   Halo* H = kind == kHaloExchange ? &V.exch : &V.bound;
-  if (!H->d_dst && !H->d_src) {
+  if (!H->built) {
     std::vector<uint32_t> d, s;
     std::string err;
-    int rc = build_halo_table(h->blocks, g, kind, d, s, &err);
+    int rc = build_halo_table(h->blocks, g, kind, true, d, s, &err);
     if (rc != H3D_OK) return fail(h, rc, err);
     TRY(upload_halo(h, *H, d, s));
-    if (H->n == 0) { H->d_dst = reinterpret_cast<uint32_t*>(1); }  // mark built (empty)
+    H->built = true;
   }
   const bool f32 = f32_level(h, g);
   const size_t n = (size_t)V.geom.n_elems;
@@ -1170,7 +1302,7 @@ int h3d_mg_vcycle(h3d_mg* h) {
   Exec ex{h};
   TRY(ex.vcycle());
   CU(cudaStreamSynchronize(h->st));
-  return H3D_OK;
+  return check_device_error(h);
 }
 
 int h3d_mg_mgkcyc(h3d_mg* h, double* const* pp, const double* const* su) {
@@ -1218,6 +1350,24 @@ int h3d_mg_sync(h3d_mg* h) {
 int h3d_mg_set_profiling(h3d_mg* h, int32_t on) {
   if (!h) return H3D_ERR_ARG;
   h->profiling = on != 0;
+  return H3D_OK;
+}
+
+int h3d_mg_set_smoother(h3d_mg* h, int32_t g, int32_t variant, int32_t zchunk) {
+  if (!level_ok(h, g) || variant < 0 || variant >= num_tile_shapes() || zchunk < 1) return H3D_ERR_ARG;
+  Level& V = h->lev[g];
+  if (!variant_fits(V, variant)) return fail(h, H3D_ERR_ARG, "smoother variant does not fit this level");
+  CU(cudaSetDevice(h->device));
+  TRY(build_tiles(h, V, variant, zchunk));
+  h->graphs.clear();  // captured graphs refer to the old tiles
+  return H3D_OK;
+}
+
+int h3d_mg_get_smoother(h3d_mg* h, int32_t g, int32_t* variant, int32_t* zchunk, int32_t* nvariants) {
+  if (!level_ok(h, g)) return H3D_ERR_ARG;
+  if (variant) *variant = h->lev[g].variant;
+  if (zchunk) *zchunk = h->lev[g].zc;
+  if (nvariants) *nvariants = num_tile_shapes();
   return H3D_OK;
 }
 

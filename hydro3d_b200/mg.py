@@ -188,6 +188,19 @@ class MultigridSolver:
         self._check(self.L.h3d_mg_smoother_bytes(self._h, C.byref(v)), "h3d_mg_smoother_bytes")
         return v.value
 
+    def set_smoother(self, g: int, variant: int, zchunk: int) -> bool:
+        """Force smoother variant / z-chunk of level g; False if it cannot run there."""
+        rc = self.L.h3d_mg_set_smoother(self._h, g, variant, zchunk)
+        if rc == _lib.H3D_ERR_ARG:
+            return False
+        self._check(rc, "h3d_mg_set_smoother")
+        return True
+
+    def get_smoother(self, g: int):
+        v, z, n = C.c_int32(), C.c_int32(), C.c_int32()
+        self._check(self.L.h3d_mg_get_smoother(self._h, g, C.byref(v), C.byref(z), C.byref(n)), "h3d_mg_get_smoother")
+        return v.value, z.value, n.value
+
     # reference subroutines on the level state ----------------------------
     def level_dims(self, g: int, ib: int):
         d = self.blocks[ib]

@@ -146,6 +146,11 @@ int h3d_mg_sync(h3d_mg* h);
 /* 1: bracket every level-1 smoother launch with CUDA events on the solve
  * stream and add its duration to h3d_solve_info.smoother_ms. */
 int h3d_mg_set_profiling(h3d_mg* h, int32_t on);
+/* Smoother kernel variant and z-chunk of level g (the autotuner's choice is
+ * the default; H3D_ERR_ARG if the variant cannot run this level).  *nvariants
+ * receives the number of variants. */
+int h3d_mg_set_smoother(h3d_mg* h, int32_t g, int32_t variant, int32_t zchunk);
+int h3d_mg_get_smoother(h3d_mg* h, int32_t g, int32_t* variant, int32_t* zchunk, int32_t* nvariants);
 /* Algorithmic bytes of one level-1 smoother launch (sum over blocks). */
 int h3d_mg_smoother_bytes(h3d_mg* h, double* bytes_per_launch);
 

@@ -246,3 +246,27 @@ def test_mixed_precision_error_vs_fp64(oracle_mod, h3d):
                            [x[1:-1, 1:-1, 1:-1] for x in ref["p"]])
     assert err <= 1e-8, err
     s.close()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_every_smoother_variant(oracle_mod, h3d, precision):
+    """Each smoother kernel variant (generic tiles, whole-row tiles, TMA-staged
+    row tiles) and several z-chunks give the reference sweep: bit-exact in
+    FP64, within the FP32 tolerance in the mixed solver's FP32 levels."""
+    layout = ((2, 2, 1), (32, 16, 16), [P, P, W, W, W, W], 3)
+    blocks, s, orc = _pair(oracle_mod, h3d, layout, precision=precision)
+    s.coeff(); orc.coeff()
+    _, _, nvar = s.get_smoother(1)
+    rng = np.random.default_rng(7)
+    tried = 0
+    for v in range(nvar):
+        for zc in (3, 16):
+            if not s.set_smoother(1, v, zc):
+                continue
+            tried += 1
+            _rand_level(rng, s, orc, 1)
+            s.mgrelax(1, 2)
+            orc.mgrelax(1, 2)
+            _assert_level(s, orc, 1, exact=(precision == "fp64"))
+    assert tried >= 20
+    s.close()
