@@ -165,6 +165,67 @@ __global__ void __launch_bounds__(NT) k_rbgs(const BlkLev* __restrict__ bls, con
 }
 
 
+// Per-thread stencil state of the row-tile smoothers.  A thread's cells are
+// fixed for the whole z march (pair k, member m: x = 2(tc + k*TPR) + 1 + m),
+// so the constant coefficients of mgsolver.for:186-205 are selected once.
+// FP64 keeps the reference's operand order and IEEE division (bit-exact);
+// the FP32 inner solve uses fused multiply-adds and a reciprocal of the
+// diagonal computed once per cell column.
+template <typename T, int CP, bool VAR>
+struct RowGs {
+  T cw[CP][2], ce[CP][2], cinv[CP][2], cxy[CP][2];
+  T cs, cn, az;
+  int ph, nz;
+
+  __device__ __forceinline__ void init(const BlkLev& B, int y, int tc, int tpr) {
+    ph = B.phys;
+    nz = B.nz;
+    const T ax = (T)B.ax, ay = (T)B.ay;
+    az = (T)B.az;
+    cs = (y == 1 && (ph & 4)) ? T(0) : ay;
+    cn = (y == B.ny && (ph & 8)) ? T(0) : ay;
+#pragma unroll
+    for (int k = 0; k < CP; ++k)
+#pragma unroll
+      for (int m = 0; m < 2; ++m) {
+        const int x = 2 * (tc + k * tpr) + 1 + m;
+        cw[k][m] = (x == 1 && (ph & 1)) ? T(0) : ax;
+        ce[k][m] = (x == B.nx && (ph & 2)) ? T(0) : ax;
+        cxy[k][m] = cw[k][m] + ce[k][m] + cs + cn;
+        cinv[k][m] = T(1) / (-(cxy[k][m] + az + az));
+      }
+  }
+
+  // New value of the cell at smem index s (row pitch sp) of plane z, pair k,
+  // member m; rv = its right-hand side; i = its offset in the block (VAR).
+  __device__ __forceinline__ T update(const T* P, const T* Pm, const T* Pp, int s, int sp, int k, int m, int z,
+                                      T rv, const T* FX, const T* FY, const T* FZ, long long i, int sx,
+                                      long long sxy) const {
+    T aw, ae, as, an, ab, at;
+    if (VAR) {
+      aw = FX[i - 1]; ae = FX[i]; as = FY[i - sx]; an = FY[i]; ab = FZ[i - sxy]; at = FZ[i];
+    } else {
+      aw = m ? cw[k][1] : cw[k][0];
+      ae = m ? ce[k][1] : ce[k][0];
+      as = cs;
+      an = cn;
+      ab = (z == 1 && (ph & 16)) ? T(0) : az;
+      at = (z == nz && (ph & 32)) ? T(0) : az;
+    }
+    const T w = P[s - 1], e = P[s + 1], so = P[s - sp], no = P[s + sp], bo = Pm[s], to = Pp[s];
+    if (sizeof(T) == 8) {
+      const T ap = -(aw + ae + as + an + ab + at);
+      return gs_div(rv - (aw * w + ae * e + as * so + an * no + ab * bo + at * to), ap);
+    } else {
+      const T sum = fma(at, to, fma(ab, bo, fma(an, no, fma(as, so, fma(ae, e, aw * w)))));
+      T inv;
+      if (!VAR && z > 1 && z < nz) inv = m ? cinv[k][1] : cinv[k][0];
+      else inv = T(1) / (-(aw + ae + as + an + ab + at));
+      return (rv - sum) * inv;
+    }
+  }
+};
+
 // ---------------------------------------------------------------------------
 // Row-tile red-black sweep.  A CTA owns TY whole rows (x = 0..nx+1) of one
 // block and marches a z range; because a tile spans the whole row there is no
@@ -223,25 +284,8 @@ __global__ void __launch_bounds__(TPR*(TY + 2)) k_rbgs_rows(const BlkLev* __rest
     }
   };
   // one cell update in plane z (P), neighbours in Pm (z-1), Pp (z+1)
-  auto update = [&](T* P, const T* Pm, const T* Pp, int x, int z, long long rowg) -> T {
-    const int s = srow + x + 1;
-    T aw, ae, as, an, ab, at;
-    if (VAR) {
-      const long long i = rowg + x;
-      aw = FX[i - 1]; ae = FX[i]; as = FY[i - sx]; an = FY[i]; ab = FZ[i - sxy]; at = FZ[i];
-    } else {
-      aw = (x == 1 && (ph & 1)) ? T(0) : ax;
-      ae = (x == nx && (ph & 2)) ? T(0) : ax;
-      as = as_c;
-      an = an_c;
-      ab = (z == 1 && (ph & 16)) ? T(0) : az;
-      at = (z == nz && (ph & 32)) ? T(0) : az;
-    }
-    const T ap = -(aw + ae + as + an + ab + at);
-    return gs_div(R[rowg + x] - (aw * P[s - 1] + ae * P[s + 1] + as * P[s - SP] + an * P[s + SP] + ab * Pm[s] +
-                                 at * Pp[s]),
-                  ap);
-  };
+  RowGs<T, CP, VAR> gs;
+  gs.init(B, y, tc, TPR);
   auto red = [&](int z) {
     if (!row_in) return;
     T* P = ring + (z & 3) * PL;
@@ -252,7 +296,8 @@ __global__ void __launch_bounds__(TPR*(TY + 2)) k_rbgs_rows(const BlkLev* __rest
 #pragma unroll
     for (int k = 0; k < CP; ++k) {
       const int x = 2 * (tc + k * TPR) + 1 + j;
-      if (x <= nx) P[srow + x + 1] = update(P, Pm, Pp, x, z, rowg);
+      if (x <= nx)
+        P[srow + x + 1] = gs.update(P, Pm, Pp, srow + x + 1, SP, k, j, z, R[rowg + x], FX, FY, FZ, rowg + x, (int)sx, sxy);
     }
   };
   auto black_store = [&](int z) {
@@ -268,7 +313,7 @@ __global__ void __launch_bounds__(TPR*(TY + 2)) k_rbgs_rows(const BlkLev* __rest
       if (xp > nx) continue;
       const int xb = xp + jb, xr = xp + 1 - jb;
       const T vr = P[srow + xr + 1];
-      const T vb = update(P, Pm, Pp, xb, z, rowg);
+      const T vb = gs.update(P, Pm, Pp, srow + xb + 1, SP, k, jb, z, R[rowg + xb], FX, FY, FZ, rowg + xb, (int)sx, sxy);
       D[rowg + xr] = vr;
       D[rowg + xb] = vb;
     }
@@ -391,25 +436,8 @@ __global__ void __launch_bounds__(TPR*(TY + 2)) k_rbgs_tma(const BlkLev* __restr
     const uint32_t parity = (uint32_t)(((z - zlo + 1) / NS) & 1);
     mbar_wait(smem_u32(bars + (z % NS)), parity, err, bad);
   };
-  auto update = [&](T* P, const T* Pm, const T* Pp, int x, int z, const T* Rrow, int io) -> T {
-    const int s = srow + x;
-    T aw, ae, as, an, ab, at;
-    if (VAR) {
-      const long long i = (long long)z * sxy + io + x;
-      aw = FX[i - 1]; ae = FX[i]; as = FY[i - sx]; an = FY[i]; ab = FZ[i - sxy]; at = FZ[i];
-    } else {
-      aw = (x == 1 && (ph & 1)) ? T(0) : ax;
-      ae = (x == nx && (ph & 2)) ? T(0) : ax;
-      as = as_c;
-      an = an_c;
-      ab = (z == 1 && (ph & 16)) ? T(0) : az;
-      at = (z == nz && (ph & 32)) ? T(0) : az;
-    }
-    const T ap = -(aw + ae + as + an + ab + at);
-    return gs_div(Rrow[x] - (aw * P[s - 1] + ae * P[s + 1] + as * P[s - BX] + an * P[s + BX] + ab * Pm[s] +
-                             at * Pp[s]),
-                  ap);
-  };
+  RowGs<T, CP, VAR> gs;
+  gs.init(B, y, tc, TPR);
   auto red = [&](int z) {
     if (!row_in) return;
     T* P = slot(z);
@@ -418,10 +446,11 @@ __global__ void __launch_bounds__(TPR*(TY + 2)) k_rbgs_tma(const BlkLev* __restr
     const int io = y * sx;
     const T* Rrow = R + (long long)z * sxy + io;
     const int j = (y + z) & 1;
+    const long long zo = (long long)z * sxy + io;
 #pragma unroll
     for (int k = 0; k < CP; ++k) {
       const int x = 2 * (tc + k * TPR) + 1 + j;
-      if (x <= nx) P[srow + x] = update(P, Pm, Pp, x, z, Rrow, io);
+      if (x <= nx) P[srow + x] = gs.update(P, Pm, Pp, srow + x, BX, k, j, z, Rrow[x], FX, FY, FZ, zo + x, sx, sxy);
     }
   };
   auto black_store = [&](int z) {
@@ -439,7 +468,8 @@ __global__ void __launch_bounds__(TPR*(TY + 2)) k_rbgs_tma(const BlkLev* __restr
       if (xp > nx) continue;
       const int xb = xp + jb, xr = xp + 1 - jb;
       const T vr = P[srow + xr];
-      const T vb = update(P, Pm, Pp, xb, z, Rrow, io);
+      const T vb = gs.update(P, Pm, Pp, srow + xb, BX, k, jb, z, Rrow[xb], FX, FY, FZ, (long long)z * sxy + io + xb, sx,
+                             sxy);
       Drow[xr] = vr;
       Drow[xb] = vb;
     }
@@ -664,6 +694,224 @@ __global__ void __launch_bounds__(256) k_defect(const BlkLev* __restrict__ bls, 
     }
   }
   block_reduce4<256>(rr, bb, rm, rs, partials + 4 * (size_t)blockIdx.x);
+}
+
+
+// ---------------------------------------------------------------------------
+// Tile restriction (mgrestr, mgsolver.for:693-756).  A CTA owns TYC coarse
+// rows x all coarse x of one block and marches the fine planes of a coarse z
+// range, staging fine iterate planes (rows 2Y0-2 .. 2Y0+2TYC-1) in a 3-plane
+// ring.  Each thread keeps the running sum of its coarse cells and adds the
+// eight child residuals in the reference order (i fastest, then j, then k).
+template <typename T, bool VAR, bool ZERO, int TPR, int CPX, int TYC>
+__global__ void __launch_bounds__(TPR* TYC) k_restrict_tile(const BlkLev* __restrict__ fine,
+                                                           const BlkLev* __restrict__ coarse,
+                                                           const Tile* __restrict__ tiles, int zc,
+                                                           const T* __restrict__ phi, const T* __restrict__ rhs,
+                                                           T* __restrict__ rhs_c, const T* __restrict__ fx,
+                                                           const T* __restrict__ fy, const T* __restrict__ fz) {
+  constexpr int SP = 2 * CPX * TPR + 4;
+  constexpr int SR = 2 * TYC + 2;
+  constexpr int PL = SR * SP;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* ring = reinterpret_cast<T*>(smem_raw);
+  const Tile t = tiles[blockIdx.x];
+  const BlkLev F = fine[t.b];
+  const BlkLev C = coarse[t.b];
+  const T* P = phi + F.off;
+  const T* Rf = rhs + F.off;
+  const T* FX = VAR ? fx + F.off : nullptr;
+  const T* FY = VAR ? fy + F.off : nullptr;
+  const T* FZ = VAR ? fz + F.off : nullptr;
+  const int Y0 = t.y0, Z0 = t.z0;
+  const int Z1 = min(Z0 + zc - 1, C.nz);
+  const int tr = threadIdx.x / TPR, tc = threadIdx.x - (threadIdx.x / TPR) * TPR;
+  const int Y = Y0 + tr;
+  const int fy0 = 2 * Y0 - 2;  // fine row held in smem row 0
+  auto stage = [&](int zf) {
+    T* S = ring + (zf % 3) * PL;
+    const T* Pz = P + (long long)zf * F.sxy;
+    for (int r = tr; r < SR; r += TYC) {
+      const int yy = fy0 + r;
+      if (yy < 0 || yy > F.ny + 1) continue;
+      const T* row = Pz + (long long)yy * F.sx;
+      T* srow = S + r * SP;
+      for (int x = tc; x <= F.nx + 1; x += TPR) srow[x] = ZERO ? T(0) : row[x];
+    }
+  };
+  T sum[CPX];
+#pragma unroll
+  for (int k = 0; k < CPX; ++k) sum[k] = T(0);
+  stage(2 * Z0 - 2);
+  stage(2 * Z0 - 1);
+  for (int zf = 2 * Z0 - 1; zf <= 2 * Z1; ++zf) {
+    stage(zf + 1);
+    __syncthreads();
+    if (Y <= C.ny) {
+      const T* S = ring + (zf % 3) * PL;
+      const T* Sm = ring + ((zf - 1) % 3) * PL;
+      const T* Sp = ring + ((zf + 1) % 3) * PL;
+#pragma unroll
+      for (int k = 0; k < CPX; ++k) {
+        const int X = 1 + tc + k * TPR;
+        if (X > C.nx) continue;
+#pragma unroll
+        for (int dj = 0; dj < 2; ++dj)
+#pragma unroll
+          for (int di = 0; di < 2; ++di) {
+            const int x = 2 * X - 1 + di, y = 2 * Y - 1 + dj;
+            const long long i = (long long)zf * F.sxy + (long long)y * F.sx + x;
+            T r;
+            if (ZERO) {
+              r = Rf[i] - T(0);
+            } else {
+              const int q = (y - fy0) * SP + x;
+              Coef<T> c = cell_coef<T, VAR>(F, x, y, zf, i, FX, FY, FZ);
+              const T ap = coef_ap(c);
+              r = Rf[i] - (c.aw * S[q - 1] + c.ae * S[q + 1] + c.as * S[q - SP] + c.an * S[q + SP] +
+                           c.ab * Sm[q] + c.at * Sp[q] + ap * S[q]);
+            }
+            sum[k] = ((zf & 1) && dj == 0 && di == 0) ? r : sum[k] + r;
+          }
+        if (!(zf & 1))
+          rhs_c[C.off + (long long)(zf >> 1) * C.sxy + (long long)Y * C.sx + X] = T(0.125) * sum[k];
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// mgcorr + mgbound with one thread per fine cell pair (2q, 2q+1) of a row:
+// both cells of a pair interpolate from the same eight coarse cells.
+template <typename T, bool ZERO_OLD>
+__global__ void __launch_bounds__(256) k_prolong_pairs(const BlkLev* __restrict__ fine,
+                                                       const BlkLev* __restrict__ coarse,
+                                                       const int* __restrict__ row_start, int nb, int nrows,
+                                                       const T* __restrict__ phi_c, const T* __restrict__ old,
+                                                       T* __restrict__ out) {
+  const int lane = threadIdx.x & 31;
+  for (int rid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; rid < nrows; rid += (gridDim.x * blockDim.x) >> 5) {
+    const RowRef rr = row_of(fine, row_start, nb, rid, false);
+    const BlkLev F = fine[rr.b];
+    const BlkLev C = coarse[rr.b];
+    const int ph = F.phys;
+    const int y = rr.y, z = rr.z;
+    int sy = y, sz = z;
+    if (y == 0 && (ph & 4)) sy = 1;
+    if (y == F.ny + 1 && (ph & 8)) sy = F.ny;
+    if (z == 0 && (ph & 16)) sz = 1;
+    if (z == F.nz + 1 && (ph & 32)) sz = F.nz;
+    const T wy0 = (sy & 1) ? T(1) : T(3), wy1 = (sy & 1) ? T(3) : T(1);
+    const T wz0 = (sz & 1) ? T(1) : T(3), wz1 = (sz & 1) ? T(3) : T(1);
+    const T w00 = wy0 * wz0, w10 = wy1 * wz0, w01 = wy0 * wz1, w11 = wy1 * wz1;  // [dj][dk]
+    const T* Pc = phi_c + C.off + (long long)(sz >> 1) * C.sxy + (long long)(sy >> 1) * C.sx;
+    const long long cy = C.sx, cz = C.sxy;
+    const T* Orow = old + F.off + (long long)sz * F.sxy + (long long)sy * F.sx;
+    T* Out = out + F.off + (long long)z * F.sxy + (long long)y * F.sx;
+    const int npairs = (F.nx + 2) >> 1;
+    for (int q = lane; q < npairs; q += 32) {
+      const T* Q = Pc + q;
+      const T c000 = Q[0], c010 = Q[cy], c001 = Q[cz], c011 = Q[cy + cz];
+      const T c100 = Q[1], c110 = Q[1 + cy], c101 = Q[1 + cz], c111 = Q[1 + cy + cz];
+#pragma unroll
+      for (int m = 0; m < 2; ++m) {
+        const int x = 2 * q + m;
+        int sx = x;
+        if (x == 0 && (ph & 1)) sx = 1;
+        if (x == F.nx + 1 && (ph & 2)) sx = F.nx;
+        const T wx0 = (sx & 1) ? T(1) : T(3), wx1 = (sx & 1) ? T(3) : T(1);
+        // term order (di,dj,dk): 000, 010, 001, 011, 100, 110, 101, 111 (mgsolver.for:838-892)
+        T s = (wx0 * w00) * c000;
+        s = s + (wx0 * w10) * c010;
+        s = s + (wx0 * w01) * c001;
+        s = s + (wx0 * w11) * c011;
+        s = s + (wx1 * w00) * c100;
+        s = s + (wx1 * w10) * c110;
+        s = s + (wx1 * w01) * c101;
+        s = s + (wx1 * w11) * c111;
+        const T o = ZERO_OLD ? T(0) : Orow[sx];
+        Out[x] = o + s / T(64);
+      }
+    }
+  }
+}
+
+// Tile defect (newsolv_mg.for:39-55): stages pn = p + e for rows y0-1 ..
+// y0+TY of a z range through a 3-plane ring (writing p_next for the cells
+// this tile owns, ghosts included), then r = b - A pn on the tile's interior
+// cells; per-CTA partial sums {r^2, b^2, max|r|*rscale, r}.
+template <typename TE, typename TR, bool HAS_E, bool VAR, int TPR, int TY>
+__global__ void __launch_bounds__(TPR* TY) k_defect_tile(const BlkLev* __restrict__ bls, const Tile* __restrict__ tiles,
+                                                        int zc, const double* __restrict__ p,
+                                                        const TE* __restrict__ e, double* __restrict__ p_next,
+                                                        const double* __restrict__ bvec, TR* __restrict__ rhs_out,
+                                                        double mean_b, double rscale, const double* __restrict__ fx,
+                                                        const double* __restrict__ fy, const double* __restrict__ fz,
+                                                        double* __restrict__ partials, int sp) {
+  constexpr int SR = TY + 2;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double* ring = reinterpret_cast<double*>(smem_raw);
+  const int PL = SR * sp;
+  const Tile t = tiles[blockIdx.x];
+  const BlkLev B = bls[t.b];
+  const int nx = B.nx, ny = B.ny, nz = B.nz;
+  const int y0 = t.y0, zs = t.z0, ze = min(zs + zc - 1, nz);
+  const int tr = threadIdx.x / TPR, tc = threadIdx.x - (threadIdx.x / TPR) * TPR;
+  const double* Pb = p + B.off;
+  const TE* Eb = HAS_E ? e + B.off : nullptr;
+  double* Nb = HAS_E ? p_next + B.off : nullptr;
+  const int ylast = min(y0 + TY - 1, ny);
+  auto owns_row = [&](int yy) {
+    return (yy >= y0 && yy <= ylast) || (yy == 0 && y0 == 1) || (yy == ny + 1 && ylast == ny);
+  };
+  auto stage = [&](int z) {
+    double* S = ring + (z % 3) * PL;
+    const long long zo = (long long)z * B.sxy;
+    const bool oz = (z >= zs && z <= ze) || (z == 0 && zs == 1) || (z == nz + 1 && ze == nz);
+    for (int r = tr; r < SR; r += TY) {
+      const int yy = y0 - 1 + r;
+      if (yy < 0 || yy > ny + 1) continue;
+      const long long ro = zo + (long long)yy * B.sx;
+      const bool own = HAS_E && oz && owns_row(yy);
+      double* srow = S + r * sp;
+      for (int x = tc; x <= nx + 1; x += TPR) {
+        double v = Pb[ro + x];
+        if (HAS_E) v = v + (double)Eb[ro + x];
+        if (own) Nb[ro + x] = v;
+        srow[x] = v;
+      }
+    }
+  };
+  double rr = 0, bb = 0, rm = 0, rs = 0;
+  stage(zs - 1);
+  stage(zs);
+  for (int z = zs; z <= ze; ++z) {
+    stage(z + 1);
+    __syncthreads();
+    const int y = y0 + tr;
+    if (y <= ny) {
+      const double* S = ring + (z % 3) * PL;
+      const double* Sm = ring + ((z - 1) % 3) * PL;
+      const double* Sp = ring + ((z + 1) % 3) * PL;
+      const long long ro = B.off + (long long)z * B.sxy + (long long)y * B.sx;
+      for (int x = 1 + tc; x <= nx; x += TPR) {
+        const int q = (tr + 1) * sp + x;
+        Coef<double> c = cell_coef<double, VAR>(B, x, y, z, ro - B.off + x, VAR ? fx + B.off : nullptr,
+                                                VAR ? fy + B.off : nullptr, VAR ? fz + B.off : nullptr);
+        const double ap = coef_ap(c);
+        const double bv = bvec[ro + x];
+        const double r = bv - (c.aw * S[q - 1] + c.ae * S[q + 1] + c.as * S[q - sp] + c.an * S[q + sp] +
+                               c.ab * Sm[q] + c.at * Sp[q] + ap * S[q]);
+        rhs_out[ro + x] = (TR)(r - mean_b);
+        rr += r * r;
+        bb += bv * bv;
+        rm = fmax(rm, fabs(r) * rscale);
+        rs += r;
+      }
+    }
+    __syncthreads();
+  }
+  block_reduce4<TPR * TY>(rr, bb, rm, rs, partials + 4 * (size_t)blockIdx.x);
 }
 
 __global__ void __launch_bounds__(256) k_reduce4(const double* __restrict__ partials, int n, double* __restrict__ out) {
@@ -908,6 +1156,8 @@ cudaError_t init_kernel_attributes() {
   return e;
 }
 
+
+
 template <typename T>
 cudaError_t launch_rbgs(int variant, bool var, bool zero_src, const BlkLev* bl, const Tile* tiles, int ntiles,
                         int zc, const CUtensorMap* maps, int* err, const T* src, T* dst, const T* rhs, const T* fx,
@@ -968,8 +1218,8 @@ cudaError_t launch_prolong(bool zero_old, const BlkLev* fine, const BlkLev* coar
                            const T* old, T* out, cudaStream_t st) {
   if (rt.nrows <= 0) return cudaSuccess;
   const int g = row_grid(rt.nrows);
-  if (zero_old) k_prolong<T, true><<<g, 256, 0, st>>>(fine, coarse, rt.start, rt.nb, rt.nrows, phi_c, old, out);
-  else k_prolong<T, false><<<g, 256, 0, st>>>(fine, coarse, rt.start, rt.nb, rt.nrows, phi_c, old, out);
+  if (zero_old) k_prolong_pairs<T, true><<<g, 256, 0, st>>>(fine, coarse, rt.start, rt.nb, rt.nrows, phi_c, old, out);
+  else k_prolong_pairs<T, false><<<g, 256, 0, st>>>(fine, coarse, rt.start, rt.nb, rt.nrows, phi_c, old, out);
   return cudaGetLastError();
 }
 
@@ -993,6 +1243,112 @@ cudaError_t launch_defect(bool var, const BlkLev* bl, RowTab rt, const double* p
   }
   return cudaGetLastError();
 }
+
+
+// ---- tile restriction ------------------------------------------------------
+static const RestrictShape kRShapes[] = {{16, 1, 8}, {32, 1, 8}, {32, 2, 4}, {32, 4, 4}};
+int num_restrict_shapes() { return (int)(sizeof(kRShapes) / sizeof(kRShapes[0])); }
+RestrictShape restrict_shape(int v) { return kRShapes[v]; }
+
+template <typename T, int TPR, int CPX, int TYC>
+static constexpr size_t rtile_smem() {
+  return 3 * (size_t)(2 * TYC + 2) * (size_t)(2 * CPX * TPR + 4) * sizeof(T);
+}
+
+template <typename T, int TPR, int CPX, int TYC>
+static cudaError_t rtile_attr() {
+  const int sm = (int)rtile_smem<T, TPR, CPX, TYC>();
+  cudaError_t e;
+  if ((e = cudaFuncSetAttribute(k_restrict_tile<T, true, false, TPR, CPX, TYC>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm))) return e;
+  if ((e = cudaFuncSetAttribute(k_restrict_tile<T, false, false, TPR, CPX, TYC>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm))) return e;
+  return cudaFuncSetAttribute(k_restrict_tile<T, false, true, TPR, CPX, TYC>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+}
+
+template <typename T, int TPR, int CPX, int TYC>
+static cudaError_t rtile_dispatch(bool var, bool zero, const BlkLev* fine, const BlkLev* coarse, const Tile* tiles,
+                                  int ntiles, int zc, const T* phi, const T* rhs, T* rhs_c, const T* fx, const T* fy,
+                                  const T* fz, cudaStream_t st) {
+  if (ntiles <= 0) return cudaSuccess;
+  constexpr size_t SM = rtile_smem<T, TPR, CPX, TYC>();
+  if (zero) k_restrict_tile<T, false, true, TPR, CPX, TYC><<<ntiles, TPR * TYC, SM, st>>>(fine, coarse, tiles, zc, phi, rhs, rhs_c, fx, fy, fz);
+  else if (var) k_restrict_tile<T, true, false, TPR, CPX, TYC><<<ntiles, TPR * TYC, SM, st>>>(fine, coarse, tiles, zc, phi, rhs, rhs_c, fx, fy, fz);
+  else k_restrict_tile<T, false, false, TPR, CPX, TYC><<<ntiles, TPR * TYC, SM, st>>>(fine, coarse, tiles, zc, phi, rhs, rhs_c, fx, fy, fz);
+  return cudaGetLastError();
+}
+
+#define H3D_RSHAPES(X) X(0, 16, 1, 8) X(1, 32, 1, 8) X(2, 32, 2, 4) X(3, 32, 4, 4)
+
+template <typename T>
+cudaError_t launch_restrict_tile(int variant, bool var, bool zero_phi, const BlkLev* fine, const BlkLev* coarse,
+                                 const Tile* tiles, int ntiles, int zc, const T* phi, const T* rhs, T* rhs_c,
+                                 const T* fx, const T* fy, const T* fz, cudaStream_t st) {
+  switch (variant) {
+#define X(v, tpr, cpx, tyc) \
+    case v: return rtile_dispatch<T, tpr, cpx, tyc>(var, zero_phi, fine, coarse, tiles, ntiles, zc, phi, rhs, rhs_c, fx, fy, fz, st);
+    H3D_RSHAPES(X)
+#undef X
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+// ---- tile defect ------------------------------------------------------------
+constexpr int kDefTPR = 32, kDefTY = 8;
+size_t defect_tile_smem(int sp) { return 3 * (size_t)(kDefTY + 2) * (size_t)sp * sizeof(double); }
+
+template <typename TE, typename TR>
+static cudaError_t dtile_attr() {
+  const int sm = 200 * 1024;
+  cudaError_t e;
+  if ((e = cudaFuncSetAttribute(k_defect_tile<TE, TR, true, true, kDefTPR, kDefTY>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm))) return e;
+  if ((e = cudaFuncSetAttribute(k_defect_tile<TE, TR, true, false, kDefTPR, kDefTY>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm))) return e;
+  if ((e = cudaFuncSetAttribute(k_defect_tile<TE, TR, false, true, kDefTPR, kDefTY>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm))) return e;
+  return cudaFuncSetAttribute(k_defect_tile<TE, TR, false, false, kDefTPR, kDefTY>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+}
+
+template <typename TE, typename TR>
+cudaError_t launch_defect_tile(bool var, const BlkLev* bl, const Tile* tiles, int ntiles, int zc, int sp,
+                               const double* p, const TE* e, double* p_next, const double* b, TR* rhs_out,
+                               double mean_b, double rscale, const double* fx, const double* fy, const double* fz,
+                               double* partials, cudaStream_t st) {
+  if (ntiles <= 0) return cudaSuccess;
+  const size_t SM = defect_tile_smem(sp);
+  constexpr int NT = kDefTPR * kDefTY;
+  if (e) {
+    if (var) k_defect_tile<TE, TR, true, true, kDefTPR, kDefTY><<<ntiles, NT, SM, st>>>(bl, tiles, zc, p, e, p_next, b, rhs_out, mean_b, rscale, fx, fy, fz, partials, sp);
+    else k_defect_tile<TE, TR, true, false, kDefTPR, kDefTY><<<ntiles, NT, SM, st>>>(bl, tiles, zc, p, e, p_next, b, rhs_out, mean_b, rscale, fx, fy, fz, partials, sp);
+  } else {
+    if (var) k_defect_tile<TE, TR, false, true, kDefTPR, kDefTY><<<ntiles, NT, SM, st>>>(bl, tiles, zc, p, e, p_next, b, rhs_out, mean_b, rscale, fx, fy, fz, partials, sp);
+    else k_defect_tile<TE, TR, false, false, kDefTPR, kDefTY><<<ntiles, NT, SM, st>>>(bl, tiles, zc, p, e, p_next, b, rhs_out, mean_b, rscale, fx, fy, fz, partials, sp);
+  }
+  return cudaGetLastError();
+}
+int defect_tile_rows() { return kDefTY; }
+
+cudaError_t init_kernel_attributes_2() {
+  cudaError_t e = cudaSuccess;
+#define X(v, tpr, cpx, tyc)                                                    \
+  if ((e = rtile_attr<float, tpr, cpx, tyc>()) != cudaSuccess) return e;       \
+  if ((e = rtile_attr<double, tpr, cpx, tyc>()) != cudaSuccess) return e;
+  H3D_RSHAPES(X)
+#undef X
+  if ((e = dtile_attr<double, double>()) != cudaSuccess) return e;
+  return dtile_attr<float, float>();
+}
+
+template cudaError_t launch_restrict_tile<double>(int, bool, bool, const BlkLev*, const BlkLev*, const Tile*, int, int,
+                                                  const double*, const double*, double*, const double*, const double*,
+                                                  const double*, cudaStream_t);
+template cudaError_t launch_restrict_tile<float>(int, bool, bool, const BlkLev*, const BlkLev*, const Tile*, int, int,
+                                                 const float*, const float*, float*, const float*, const float*,
+                                                 const float*, cudaStream_t);
+template cudaError_t launch_defect_tile<double, double>(bool, const BlkLev*, const Tile*, int, int, int, const double*,
+                                                        const double*, double*, const double*, double*, double, double,
+                                                        const double*, const double*, const double*, double*,
+                                                        cudaStream_t);
+template cudaError_t launch_defect_tile<float, float>(bool, const BlkLev*, const Tile*, int, int, int, const double*,
+                                                      const float*, double*, const double*, float*, double, double,
+                                                      const double*, const double*, const double*, double*,
+                                                      cudaStream_t);
 
 cudaError_t launch_reduce4(const double* partials, int n, double* out, cudaStream_t st) {
   k_reduce4<<<1, 256, 0, st>>>(partials, n, out);

@@ -54,6 +54,8 @@ struct Level {
   double* dens = nullptr;
   Halo sweep, faces, exch, bound;
   CUtensorMap* d_maps = nullptr;  // [ty index][buffer][block] tensor maps of the iterate
+  Tile* d_rtiles = nullptr;       // restriction tiles (this level as the coarse level)
+  int nrtiles = 0, rvariant = 0, rzc = 1;
   bool tma_ok = false;
   int cur64 = 0, cur32 = 0;
   bool zero64 = false, zero32 = false;
@@ -86,6 +88,8 @@ struct h3d_mg {
   double* h_res = nullptr;  // pinned, 4 doubles
   double* d_h3 = nullptr;   // per-block dx,dy,dz
   int* d_err = nullptr;     // set by a device wait that gave up
+  Tile* d_dtiles = nullptr; // level-1 defect tiles
+  int ndtiles = 0, dzc = 1, dsp = 0;
   double mean_b = 0.0;
   bool coeffs_ready = false;
   std::string last_error;
@@ -200,6 +204,48 @@ int build_tiles(h3d_mg* h, Level& Lv, int variant, int zc) {
   return H3D_OK;
 }
 
+// Tiles of (TY rows x all x) x zc planes over every block of geometry G.
+std::vector<Tile> row_tiles(const LevelGeom& G, int ty, int zc) {
+  std::vector<Tile> t;
+  for (size_t b = 0; b < G.bl.size(); ++b)
+    for (int z0 = 1; z0 <= G.bl[b].nz; z0 += zc)
+      for (int y0 = 1; y0 <= G.bl[b].ny; y0 += ty) t.push_back(Tile{(int)b, 1, y0, z0});
+  return t;
+}
+
+// z chunk giving at least ~3 CTAs per SM.
+int pick_zc(const LevelGeom& G, int ty) {
+  int nzm = 1;
+  long long xy = 0;
+  for (const auto& B : G.bl) {
+    nzm = std::max(nzm, B.nz);
+    xy += (B.ny + ty - 1) / ty;
+  }
+  int zc = nzm;
+  while (zc > 4 && xy * ((nzm + zc - 1) / zc) < 148 * 3) zc = (zc + 1) / 2;
+  return zc;
+}
+
+int build_restrict_tiles(h3d_mg* h, Level& C) {
+  int nxm = 0;
+  for (const auto& B : C.geom.bl) nxm = std::max(nxm, B.nx);
+  int v = -1;
+  for (int q = 0; q < num_restrict_shapes(); ++q) {
+    RestrictShape r = restrict_shape(q);
+    if (r.tpr * r.cpx >= nxm) { v = q; break; }
+  }
+  if (v < 0) return fail(h, H3D_ERR_BAD_CONFIG, "block too wide for the restriction kernels (nx > 512)");
+  RestrictShape r = restrict_shape(v);
+  int zc = pick_zc(C.geom, r.tyc);
+  std::vector<Tile> t = row_tiles(C.geom, r.tyc, zc);
+  TRY(dalloc(h, &C.d_rtiles, t.size()));
+  CU(cudaMemcpy(C.d_rtiles, t.data(), t.size() * sizeof(Tile), cudaMemcpyHostToDevice));
+  C.nrtiles = (int)t.size();
+  C.rvariant = v;
+  C.rzc = zc;
+  return H3D_OK;
+}
+
 // Heuristic tile choice (the autotuner refines it on large levels).
 void default_tile(const Level& Lv, int* variant, int* zc) {
   int nxm = 0, nym = 0, nzm = 0;
@@ -305,11 +351,10 @@ struct Exec {
   int restrict_to(int gc) {
     Level& F = L(gc - 1);
     Level& C = L(gc);
-    RowTab ct{C.d_rows_int, (int)C.geom.bl.size(), C.nrows_int};
     if (mixed_level(gc - 1)) {
       // the coarsest level of a mixed solve keeps an FP32 rhs too (converted after)
-      CU(launch_restrict<float>(h->var, F.zero32, F.d_bl, C.d_bl, ct, F.phi32[F.cur32], F.rhs32, C.rhs32, F.fx32,
-                                F.fy32, F.fz32, h->st));
+      CU(launch_restrict_tile<float>(C.rvariant, h->var, F.zero32, F.d_bl, C.d_bl, C.d_rtiles, C.nrtiles, C.rzc,
+                                     F.phi32[F.cur32], F.rhs32, C.rhs32, F.fx32, F.fy32, F.fz32, h->st));
       C.zero32 = true;
       if (!mixed_level(gc)) {  // coarsest level solved in FP64
         CU(launch_convert_f2d(C.rhs32, C.rhs64, C.geom.n_elems, h->st));
@@ -317,8 +362,8 @@ struct Exec {
         h->kernels += 1;
       }
     } else {
-      CU(launch_restrict<double>(h->var, F.zero64, F.d_bl, C.d_bl, ct, F.phi64[F.cur64], F.rhs64, C.rhs64, F.fx64,
-                                 F.fy64, F.fz64, h->st));
+      CU(launch_restrict_tile<double>(C.rvariant, h->var, F.zero64, F.d_bl, C.d_bl, C.d_rtiles, C.nrtiles, C.rzc,
+                                      F.phi64[F.cur64], F.rhs64, C.rhs64, F.fx64, F.fy64, F.fz64, h->st));
       C.zero64 = true;
     }
     h->kernels += 1;
@@ -412,7 +457,6 @@ struct Exec {
   // FP64 defect on the resident p/b: e = level-1 iterate (or none).
   int defect(bool with_e) {
     Level& V = L(1);
-    RowTab ct{V.d_rows_all, (int)V.geom.bl.size(), V.nrows_all};
     double rscale = h->var ? 1.0 : V.geom.bl[0].dv;
     const double* fx = h->var ? V.fx64 : nullptr;
     const double* fy = h->var ? V.fy64 : nullptr;
@@ -425,19 +469,19 @@ struct Exec {
         if (V.zero32) TRY(materialize_zero32(1));
         e = V.phi32[V.cur32];
       }
-      CU(launch_defect<float, float>(h->var, V.d_bl, ct, pin, e, pout, h->b64, V.rhs32, h->mean_b, rscale, fx, fy, fz,
-                                     h->partials, h->st));
+      CU(launch_defect_tile<float, float>(h->var, V.d_bl, h->d_dtiles, h->ndtiles, h->dzc, h->dsp, pin, e, pout,
+                                          h->b64, V.rhs32, h->mean_b, rscale, fx, fy, fz, h->partials, h->st));
     } else {
       const double* e = nullptr;
       if (with_e) {
         if (V.zero64) TRY(materialize_zero64(1));
         e = V.phi64[V.cur64];
       }
-      CU(launch_defect<double, double>(h->var, V.d_bl, ct, pin, e, pout, h->b64, V.rhs64, h->mean_b, rscale, fx, fy,
-                                       fz, h->partials, h->st));
+      CU(launch_defect_tile<double, double>(h->var, V.d_bl, h->d_dtiles, h->ndtiles, h->dzc, h->dsp, pin, e, pout,
+                                            h->b64, V.rhs64, h->mean_b, rscale, fx, fy, fz, h->partials, h->st));
     }
     if (with_e) h->pc = 1 - h->pc;
-    CU(launch_reduce4(h->partials, defect_grid(ct.nrows), h->d_res, h->st));
+    CU(launch_reduce4(h->partials, h->ndtiles, h->d_res, h->st));
     CU(cudaMemcpyAsync(h->h_res, h->d_res, 4 * sizeof(double), cudaMemcpyDeviceToHost, h->st));
     h->kernels += 2;
     return H3D_OK;
@@ -800,7 +844,7 @@ int h3d_mg_destroy(h3d_mg* h) {
     void* ps[] = {V.d_bl, V.d_cta_all, V.d_cta_int, V.d_rows_all, V.d_rows_int, V.d_tiles, V.phi64[0], V.phi64[1], V.rhs64, V.phi32[0],
                   V.phi32[1], V.rhs32, V.fx64, V.fy64, V.fz64, V.fx32, V.fy32, V.fz32, V.dens,
                   V.sweep.d_dst, V.sweep.d_src, V.faces.d_dst, V.faces.d_src, V.exch.d_dst, V.exch.d_src,
-                  V.bound.d_dst, V.bound.d_src, V.d_maps};
+                  V.bound.d_dst, V.bound.d_src, V.d_maps, V.d_rtiles};
     for (void* p : ps) dfree(p);
   }
   dfree(h->p64[0]);
@@ -810,6 +854,7 @@ int h3d_mg_destroy(h3d_mg* h) {
   dfree(h->d_res);
   dfree(h->d_h3);
   dfree(h->d_err);
+  dfree(h->d_dtiles);
   if (h->h_res) cudaFreeHost(h->h_res);
   if (h->st) cudaStreamDestroy(h->st);
   delete h;
@@ -867,7 +912,8 @@ int h3d_mg_create(h3d_mg** out, const h3d_mg_desc* desc) {
   if (cudaSetDevice(h->device) != cudaSuccess) return bail(fail(h, H3D_ERR_NO_DEVICE, "cudaSetDevice failed"));
   if (cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking) != cudaSuccess)
     return bail(fail(h, H3D_ERR_CUDA, "stream create failed"));
-  if (init_kernel_attributes() != cudaSuccess) return bail(fail(h, H3D_ERR_CUDA, "kernel attributes"));
+  if (init_kernel_attributes() != cudaSuccess || init_kernel_attributes_2() != cudaSuccess)
+    return bail(fail(h, H3D_ERR_CUDA, "kernel attributes"));
   h->lev.resize(h->L + 1);
   for (int g = 1; g <= h->L; ++g) {
     Level& V = h->lev[g];
@@ -910,6 +956,7 @@ int h3d_mg_create(h3d_mg** out, const h3d_mg_desc* desc) {
       if ((rc = upload_halo(h, V.faces, d, s)) != H3D_OK) return bail(rc);
     }
     if ((rc = build_tensor_maps(h, g)) != H3D_OK) return bail(rc);
+    if (g >= 2 && (rc = build_restrict_tiles(h, V)) != H3D_OK) return bail(rc);
     int var_, zc;
     default_tile(V, &var_, &zc);
     if ((rc = build_tiles(h, V, var_, zc)) != H3D_OK) return bail(rc);
@@ -920,7 +967,20 @@ int h3d_mg_create(h3d_mg** out, const h3d_mg_desc* desc) {
   const size_t n1 = (size_t)h->lev[1].geom.n_elems;
   if ((rc = dalloc(h, &h->p64[0], n1)) || (rc = dalloc(h, &h->p64[1], n1)) || (rc = dalloc(h, &h->b64, n1)))
     return bail(rc);
-  h->npartials = std::max(std::max(h->lev[1].ncta_all, h->lev[1].ncta_int), kDefectCtas);
+  {
+    const LevelGeom& G1 = h->lev[1].geom;
+    int nxm = 0;
+    for (const auto& B : G1.bl) nxm = std::max(nxm, B.nx);
+    h->dsp = (nxm + 2 + 1) & ~1;
+    if (defect_tile_smem(h->dsp) > 200 * 1024) return bail(fail(h, H3D_ERR_BAD_CONFIG, "block rows too long"));
+    h->dzc = pick_zc(G1, defect_tile_rows());
+    std::vector<Tile> dt = row_tiles(G1, defect_tile_rows(), h->dzc);
+    h->ndtiles = (int)dt.size();
+    if ((rc = dalloc(h, &h->d_dtiles, dt.size())) != H3D_OK) return bail(rc);
+    if (cudaMemcpy(h->d_dtiles, dt.data(), dt.size() * sizeof(Tile), cudaMemcpyHostToDevice) != cudaSuccess)
+      return bail(fail(h, H3D_ERR_CUDA, "copy defect tiles"));
+  }
+  h->npartials = std::max(std::max(std::max(h->lev[1].ncta_all, h->lev[1].ncta_int), kDefectCtas), h->ndtiles);
   if ((rc = dalloc(h, &h->partials, 4 * (size_t)h->npartials)) || (rc = dalloc(h, &h->d_res, 4))) return bail(rc);
   if (cudaMallocHost((void**)&h->h_res, 4 * sizeof(double)) != cudaSuccess)
     return bail(fail(h, H3D_ERR_OOM, "pinned result buffer"));
