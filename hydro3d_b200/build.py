@@ -49,29 +49,39 @@ def _stale(target, deps):
 
 
 def build(verbose: bool = False, ptxas_info: bool = False) -> str:
+    """Compile (incrementally) and link libh3dmg.so.  H3D_BOUNDS_CHECK=1 in the
+    environment builds the bounds-checked debug variant."""
     os.makedirs(BUILD, exist_ok=True)
     nvcc = _nvcc()
     ccbin = _host_cxx()
     base = [nvcc] + ARCH + NVFLAGS + (["-ccbin", ccbin] if ccbin else [])
     if ptxas_info:
         base += ["-Xptxas", "-v"]
+    debug = os.environ.get("H3D_BOUNDS_CHECK") == "1"
+    if debug:
+        base += ["-DH3D_BOUNDS_CHECK"]
     hdrs = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(ROOT, "include", "h3d_mg.h")]
     objs = []
     for src in SOURCES:
         s = os.path.join(CSRC, src)
-        o = os.path.join(BUILD, src + ".o")
+        o = os.path.join(BUILD, src + (".dbg.o" if debug else ".o"))
         objs.append(o)
-        if ptxas_info or _stale(o, [s, __file__] + hdrs):
+        if ptxas_info or debug or _stale(o, [s, __file__] + hdrs):
             cmd = base + ["-c", s, "-o", o]
             if verbose:
                 print(" ".join(cmd))
             subprocess.run(cmd, check=True)
-    if _stale(OUT, objs):
+    stamp = os.path.join(BUILD, "flavor")
+    flavor = "debug" if debug else "release"
+    last = open(stamp).read() if os.path.exists(stamp) else ""
+    if last != flavor or _stale(OUT, objs):
         cmd = [nvcc] + ARCH + ["-shared", "-o", OUT] + objs + (["-ccbin", ccbin] if ccbin else []) + \
             ["-cudart", "static"]
         if verbose:
             print(" ".join(cmd))
         subprocess.run(cmd, check=True)
+        with open(stamp, "w") as f:
+            f.write(flavor)
     return OUT
 
 

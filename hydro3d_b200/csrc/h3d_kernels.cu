@@ -22,6 +22,26 @@ __device__ __forceinline__ int find_block(const int* __restrict__ start, int nb,
   return lo;
 }
 
+// Bounds-checked debug builds (-DH3D_BOUNDS_CHECK): accesses of the tile
+// kernels are checked against their block / shared-memory extents; the first
+// violation (kernel id, block, index, limit) is recorded and the access
+// skipped, so a wrong index shows up as a record instead of a fault.
+#ifdef H3D_BOUNDS_CHECK
+__device__ unsigned long long g_h3d_bad[4];
+__device__ __noinline__ bool h3d_oob(int kid, int b, long long idx, long long lim) {
+  if (idx >= 0 && idx < lim) return false;
+  if (atomicCAS(&g_h3d_bad[0], 0ull, (unsigned long long)(kid + 1)) == 0ull) {
+    g_h3d_bad[1] = (unsigned long long)b;
+    g_h3d_bad[2] = (unsigned long long)idx;
+    g_h3d_bad[3] = (unsigned long long)lim;
+  }
+  return true;
+}
+#define H3D_IN(kid, b, idx, lim) (!h3d_oob((kid), (b), (long long)(idx), (long long)(lim)))
+#else
+#define H3D_IN(kid, b, idx, lim) true
+#endif
+
 template <typename T>
 struct Coef {
   T aw, ae, as, an, ab, at;
@@ -296,7 +316,7 @@ __global__ void __launch_bounds__(TPR*(TY + 2)) k_rbgs_rows(const BlkLev* __rest
 #pragma unroll
     for (int k = 0; k < CP; ++k) {
       const int x = 2 * (tc + k * TPR) + 1 + j;
-      if (x <= nx)
+      if (x <= nx && H3D_IN(50, t.b, rowg + x, sxy * (nz + 2)) && H3D_IN(52, t.b, srow + x + 1 - SP, PL - 2 * SP))
         P[srow + x + 1] = gs.update(P, Pm, Pp, srow + x + 1, SP, k, j, z, R[rowg + x], FX, FY, FZ, rowg + x, (int)sx, sxy);
     }
   };
@@ -312,6 +332,7 @@ __global__ void __launch_bounds__(TPR*(TY + 2)) k_rbgs_rows(const BlkLev* __rest
       const int xp = 2 * (tc + k * TPR) + 1;
       if (xp > nx) continue;
       const int xb = xp + jb, xr = xp + 1 - jb;
+      if (!H3D_IN(51, t.b, rowg + xb, sxy * (nz + 2)) || !H3D_IN(53, t.b, srow + xb + 1 - SP, PL - 2 * SP)) continue;
       const T vr = P[srow + xr + 1];
       const T vb = gs.update(P, Pm, Pp, srow + xb + 1, SP, k, jb, z, R[rowg + xb], FX, FY, FZ, rowg + xb, (int)sx, sxy);
       D[rowg + xr] = vr;
@@ -450,7 +471,8 @@ __global__ void __launch_bounds__(TPR*(TY + 2)) k_rbgs_tma(const BlkLev* __restr
 #pragma unroll
     for (int k = 0; k < CP; ++k) {
       const int x = 2 * (tc + k * TPR) + 1 + j;
-      if (x <= nx) P[srow + x] = gs.update(P, Pm, Pp, srow + x, BX, k, j, z, Rrow[x], FX, FY, FZ, zo + x, sx, sxy);
+      if (x <= nx && H3D_IN(40, t.b, zo + x, sxy * (nz + 2)) && H3D_IN(42, t.b, srow + x - BX, SLOT / (int)sizeof(T) - 2 * BX))
+        P[srow + x] = gs.update(P, Pm, Pp, srow + x, BX, k, j, z, Rrow[x], FX, FY, FZ, zo + x, sx, sxy);
     }
   };
   auto black_store = [&](int z) {
@@ -467,6 +489,9 @@ __global__ void __launch_bounds__(TPR*(TY + 2)) k_rbgs_tma(const BlkLev* __restr
       const int xp = 2 * (tc + k * TPR) + 1;
       if (xp > nx) continue;
       const int xb = xp + jb, xr = xp + 1 - jb;
+      if (!H3D_IN(41, t.b, (long long)z * sxy + io + xb, sxy * (nz + 2)) ||
+          !H3D_IN(43, t.b, srow + xb - BX, SLOT / (int)sizeof(T) - 2 * BX))
+        continue;
       const T vr = P[srow + xr];
       const T vb = gs.update(P, Pm, Pp, srow + xb, BX, k, jb, z, Rrow[xb], FX, FY, FZ, (long long)z * sxy + io + xb, sx,
                              sxy);
@@ -736,7 +761,10 @@ __global__ void __launch_bounds__(TPR* TYC) k_restrict_tile(const BlkLev* __rest
       if (yy < 0 || yy > F.ny + 1) continue;
       const T* row = Pz + (long long)yy * F.sx;
       T* srow = S + r * SP;
-      for (int x = tc; x <= F.nx + 1; x += TPR) srow[x] = ZERO ? T(0) : row[x];
+      for (int x = tc; x <= F.nx + 1; x += TPR)
+        if (H3D_IN(10, t.b, (S - ring) + r * SP + x, 3 * PL) &&
+            H3D_IN(11, t.b, (long long)zf * F.sxy + (long long)yy * F.sx + x, F.sxy * (F.nz + 2)))
+          srow[x] = ZERO ? T(0) : row[x];
     }
   };
   T sum[CPX];
@@ -761,9 +789,11 @@ __global__ void __launch_bounds__(TPR* TYC) k_restrict_tile(const BlkLev* __rest
           for (int di = 0; di < 2; ++di) {
             const int x = 2 * X - 1 + di, y = 2 * Y - 1 + dj;
             const long long i = (long long)zf * F.sxy + (long long)y * F.sx + x;
-            T r;
-            if (ZERO) {
+            T r = T(0);
+            if (!H3D_IN(12, t.b, i, F.sxy * (F.nz + 2))) {
+            } else if (ZERO) {
               r = Rf[i] - T(0);
+            } else if (!H3D_IN(13, t.b, (y - fy0) * SP + x - SP, PL - 2 * SP)) {
             } else {
               const int q = (y - fy0) * SP + x;
               Coef<T> c = cell_coef<T, VAR>(F, x, y, zf, i, FX, FY, FZ);
@@ -773,7 +803,7 @@ __global__ void __launch_bounds__(TPR* TYC) k_restrict_tile(const BlkLev* __rest
             }
             sum[k] = ((zf & 1) && dj == 0 && di == 0) ? r : sum[k] + r;
           }
-        if (!(zf & 1))
+        if (!(zf & 1) && H3D_IN(14, t.b, (long long)(zf >> 1) * C.sxy + (long long)Y * C.sx + X, C.sxy * (C.nz + 2)))
           rhs_c[C.off + (long long)(zf >> 1) * C.sxy + (long long)Y * C.sx + X] = T(0.125) * sum[k];
       }
     }
@@ -811,6 +841,9 @@ __global__ void __launch_bounds__(256) k_prolong_pairs(const BlkLev* __restrict_
     const int npairs = (F.nx + 2) >> 1;
     for (int q = lane; q < npairs; q += 32) {
       const T* Q = Pc + q;
+      if (!H3D_IN(20, rr.b, (long long)(sz >> 1) * C.sxy + (long long)(sy >> 1) * C.sx + q + 1 + cy + cz,
+                  C.sxy * (C.nz + 2)))
+        continue;
       const T c000 = Q[0], c010 = Q[cy], c001 = Q[cz], c011 = Q[cy + cz];
       const T c100 = Q[1], c110 = Q[1 + cy], c101 = Q[1 + cz], c111 = Q[1 + cy + cz];
 #pragma unroll
@@ -829,89 +862,14 @@ __global__ void __launch_bounds__(256) k_prolong_pairs(const BlkLev* __restrict_
         s = s + (wx1 * w10) * c110;
         s = s + (wx1 * w01) * c101;
         s = s + (wx1 * w11) * c111;
+        if (!H3D_IN(21, rr.b, (long long)sz * F.sxy + (long long)sy * F.sx + sx, F.sxy * (F.nz + 2)) ||
+            !H3D_IN(22, rr.b, (long long)z * F.sxy + (long long)y * F.sx + x, F.sxy * (F.nz + 2)))
+          continue;
         const T o = ZERO_OLD ? T(0) : Orow[sx];
         Out[x] = o + s / T(64);
       }
     }
   }
-}
-
-// Tile defect (newsolv_mg.for:39-55): stages pn = p + e for rows y0-1 ..
-// y0+TY of a z range through a 3-plane ring (writing p_next for the cells
-// this tile owns, ghosts included), then r = b - A pn on the tile's interior
-// cells; per-CTA partial sums {r^2, b^2, max|r|*rscale, r}.
-template <typename TE, typename TR, bool HAS_E, bool VAR, int TPR, int TY>
-__global__ void __launch_bounds__(TPR* TY) k_defect_tile(const BlkLev* __restrict__ bls, const Tile* __restrict__ tiles,
-                                                        int zc, const double* __restrict__ p,
-                                                        const TE* __restrict__ e, double* __restrict__ p_next,
-                                                        const double* __restrict__ bvec, TR* __restrict__ rhs_out,
-                                                        double mean_b, double rscale, const double* __restrict__ fx,
-                                                        const double* __restrict__ fy, const double* __restrict__ fz,
-                                                        double* __restrict__ partials, int sp) {
-  constexpr int SR = TY + 2;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  double* ring = reinterpret_cast<double*>(smem_raw);
-  const int PL = SR * sp;
-  const Tile t = tiles[blockIdx.x];
-  const BlkLev B = bls[t.b];
-  const int nx = B.nx, ny = B.ny, nz = B.nz;
-  const int y0 = t.y0, zs = t.z0, ze = min(zs + zc - 1, nz);
-  const int tr = threadIdx.x / TPR, tc = threadIdx.x - (threadIdx.x / TPR) * TPR;
-  const double* Pb = p + B.off;
-  const TE* Eb = HAS_E ? e + B.off : nullptr;
-  double* Nb = HAS_E ? p_next + B.off : nullptr;
-  const int ylast = min(y0 + TY - 1, ny);
-  auto owns_row = [&](int yy) {
-    return (yy >= y0 && yy <= ylast) || (yy == 0 && y0 == 1) || (yy == ny + 1 && ylast == ny);
-  };
-  auto stage = [&](int z) {
-    double* S = ring + (z % 3) * PL;
-    const long long zo = (long long)z * B.sxy;
-    const bool oz = (z >= zs && z <= ze) || (z == 0 && zs == 1) || (z == nz + 1 && ze == nz);
-    for (int r = tr; r < SR; r += TY) {
-      const int yy = y0 - 1 + r;
-      if (yy < 0 || yy > ny + 1) continue;
-      const long long ro = zo + (long long)yy * B.sx;
-      const bool own = HAS_E && oz && owns_row(yy);
-      double* srow = S + r * sp;
-      for (int x = tc; x <= nx + 1; x += TPR) {
-        double v = Pb[ro + x];
-        if (HAS_E) v = v + (double)Eb[ro + x];
-        if (own) Nb[ro + x] = v;
-        srow[x] = v;
-      }
-    }
-  };
-  double rr = 0, bb = 0, rm = 0, rs = 0;
-  stage(zs - 1);
-  stage(zs);
-  for (int z = zs; z <= ze; ++z) {
-    stage(z + 1);
-    __syncthreads();
-    const int y = y0 + tr;
-    if (y <= ny) {
-      const double* S = ring + (z % 3) * PL;
-      const double* Sm = ring + ((z - 1) % 3) * PL;
-      const double* Sp = ring + ((z + 1) % 3) * PL;
-      const long long ro = B.off + (long long)z * B.sxy + (long long)y * B.sx;
-      for (int x = 1 + tc; x <= nx; x += TPR) {
-        const int q = (tr + 1) * sp + x;
-        Coef<double> c = cell_coef<double, VAR>(B, x, y, z, ro - B.off + x, VAR ? fx + B.off : nullptr,
-                                                VAR ? fy + B.off : nullptr, VAR ? fz + B.off : nullptr);
-        const double ap = coef_ap(c);
-        const double bv = bvec[ro + x];
-        const double r = bv - (c.aw * S[q - 1] + c.ae * S[q + 1] + c.as * S[q - sp] + c.an * S[q + sp] +
-                               c.ab * Sm[q] + c.at * Sp[q] + ap * S[q]);
-        rhs_out[ro + x] = (TR)(r - mean_b);
-        rr += r * r;
-        bb += bv * bv;
-        rm = fmax(rm, fabs(r) * rscale);
-        rs += r;
-      }
-    }
-    __syncthreads();
-  }
-  block_reduce4<TPR * TY>(rr, bb, rm, rs, partials + 4 * (size_t)blockIdx.x);
 }
 
 __global__ void __launch_bounds__(256) k_reduce4(const double* __restrict__ partials, int n, double* __restrict__ out) {
@@ -1045,6 +1003,13 @@ static const TileShape kShapes[] = {
     {32, 16, 288, true, 16, 1, true, 12},  {16, 16, 144, true, 8, 1, true, 13},     // 23, 24
     {128, 4, 384, true, 64, 1, true, 15},  {128, 4, 192, true, 32, 2, true, 17},    // 25, 26
 };
+#ifdef H3D_BOUNDS_CHECK
+// Debug builds only: first recorded out-of-bounds access {kernel id + 1, block, index, limit}.
+extern "C" int h3d_debug_bounds(unsigned long long* out) {
+  if (cudaMemcpyFromSymbol(out, g_h3d_bad, 4 * sizeof(unsigned long long)) != cudaSuccess) return -2;
+  return 0;
+}
+#endif
 int tma_ty_index(int ty) { return ty == 4 ? 0 : ty == 8 ? 1 : ty == 16 ? 2 : -1; }
 int num_tile_shapes() { return (int)(sizeof(kShapes) / sizeof(kShapes[0])); }
 TileShape tile_shape(int v) { return kShapes[v]; }
@@ -1291,38 +1256,7 @@ cudaError_t launch_restrict_tile(int variant, bool var, bool zero_phi, const Blk
   }
 }
 
-// ---- tile defect ------------------------------------------------------------
-constexpr int kDefTPR = 32, kDefTY = 8;
-size_t defect_tile_smem(int sp) { return 3 * (size_t)(kDefTY + 2) * (size_t)sp * sizeof(double); }
 
-template <typename TE, typename TR>
-static cudaError_t dtile_attr() {
-  const int sm = 200 * 1024;
-  cudaError_t e;
-  if ((e = cudaFuncSetAttribute(k_defect_tile<TE, TR, true, true, kDefTPR, kDefTY>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm))) return e;
-  if ((e = cudaFuncSetAttribute(k_defect_tile<TE, TR, true, false, kDefTPR, kDefTY>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm))) return e;
-  if ((e = cudaFuncSetAttribute(k_defect_tile<TE, TR, false, true, kDefTPR, kDefTY>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm))) return e;
-  return cudaFuncSetAttribute(k_defect_tile<TE, TR, false, false, kDefTPR, kDefTY>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-}
-
-template <typename TE, typename TR>
-cudaError_t launch_defect_tile(bool var, const BlkLev* bl, const Tile* tiles, int ntiles, int zc, int sp,
-                               const double* p, const TE* e, double* p_next, const double* b, TR* rhs_out,
-                               double mean_b, double rscale, const double* fx, const double* fy, const double* fz,
-                               double* partials, cudaStream_t st) {
-  if (ntiles <= 0) return cudaSuccess;
-  const size_t SM = defect_tile_smem(sp);
-  constexpr int NT = kDefTPR * kDefTY;
-  if (e) {
-    if (var) k_defect_tile<TE, TR, true, true, kDefTPR, kDefTY><<<ntiles, NT, SM, st>>>(bl, tiles, zc, p, e, p_next, b, rhs_out, mean_b, rscale, fx, fy, fz, partials, sp);
-    else k_defect_tile<TE, TR, true, false, kDefTPR, kDefTY><<<ntiles, NT, SM, st>>>(bl, tiles, zc, p, e, p_next, b, rhs_out, mean_b, rscale, fx, fy, fz, partials, sp);
-  } else {
-    if (var) k_defect_tile<TE, TR, false, true, kDefTPR, kDefTY><<<ntiles, NT, SM, st>>>(bl, tiles, zc, p, e, p_next, b, rhs_out, mean_b, rscale, fx, fy, fz, partials, sp);
-    else k_defect_tile<TE, TR, false, false, kDefTPR, kDefTY><<<ntiles, NT, SM, st>>>(bl, tiles, zc, p, e, p_next, b, rhs_out, mean_b, rscale, fx, fy, fz, partials, sp);
-  }
-  return cudaGetLastError();
-}
-int defect_tile_rows() { return kDefTY; }
 
 cudaError_t init_kernel_attributes_2() {
   cudaError_t e = cudaSuccess;
@@ -1331,8 +1265,7 @@ cudaError_t init_kernel_attributes_2() {
   if ((e = rtile_attr<double, tpr, cpx, tyc>()) != cudaSuccess) return e;
   H3D_RSHAPES(X)
 #undef X
-  if ((e = dtile_attr<double, double>()) != cudaSuccess) return e;
-  return dtile_attr<float, float>();
+  return e;
 }
 
 template cudaError_t launch_restrict_tile<double>(int, bool, bool, const BlkLev*, const BlkLev*, const Tile*, int, int,
@@ -1341,14 +1274,7 @@ template cudaError_t launch_restrict_tile<double>(int, bool, bool, const BlkLev*
 template cudaError_t launch_restrict_tile<float>(int, bool, bool, const BlkLev*, const BlkLev*, const Tile*, int, int,
                                                  const float*, const float*, float*, const float*, const float*,
                                                  const float*, cudaStream_t);
-template cudaError_t launch_defect_tile<double, double>(bool, const BlkLev*, const Tile*, int, int, int, const double*,
-                                                        const double*, double*, const double*, double*, double, double,
-                                                        const double*, const double*, const double*, double*,
-                                                        cudaStream_t);
-template cudaError_t launch_defect_tile<float, float>(bool, const BlkLev*, const Tile*, int, int, int, const double*,
-                                                      const float*, double*, const double*, float*, double, double,
-                                                      const double*, const double*, const double*, double*,
-                                                      cudaStream_t);
+
 
 cudaError_t launch_reduce4(const double* partials, int n, double* out, cudaStream_t st) {
   k_reduce4<<<1, 256, 0, st>>>(partials, n, out);

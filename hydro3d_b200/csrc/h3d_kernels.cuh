@@ -41,7 +41,7 @@ int defect_grid(int nrows);
 // Sets the dynamic shared-memory limits of the row-tile smoothers (call once
 // per device before any launch or capture).
 cudaError_t init_kernel_attributes();
-cudaError_t init_kernel_attributes_2();  // restriction / defect tiles
+cudaError_t init_kernel_attributes_2();  // restriction tiles
 
 // Tile restriction shapes: TPR threads per coarse row, CPX coarse cells per
 // thread (coarse nx <= TPR*CPX), TYC coarse rows per CTA.
@@ -54,15 +54,7 @@ template <typename T>
 cudaError_t launch_restrict_tile(int variant, bool var, bool zero_phi, const BlkLev* fine, const BlkLev* coarse,
                                  const Tile* tiles, int ntiles, int zc, const T* phi, const T* rhs, T* rhs_c,
                                  const T* fx, const T* fy, const T* fz, cudaStream_t st);
-// Tile defect: tiles of defect_tile_rows() rows; sp = smem row pitch
-// (>= max nx + 2 of the level); dynamic shared memory defect_tile_smem(sp).
-int defect_tile_rows();
-size_t defect_tile_smem(int sp);
-template <typename TE, typename TR>
-cudaError_t launch_defect_tile(bool var, const BlkLev* bl, const Tile* tiles, int ntiles, int zc, int sp,
-                               const double* p, const TE* e, double* p_next, const double* b, TR* rhs_out,
-                               double mean_b, double rscale, const double* fx, const double* fy, const double* fz,
-                               double* partials, cudaStream_t st);
+
 int num_tile_shapes();
 TileShape tile_shape(int variant);
 

@@ -9,6 +9,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -88,8 +89,6 @@ struct h3d_mg {
   double* h_res = nullptr;  // pinned, 4 doubles
   double* d_h3 = nullptr;   // per-block dx,dy,dz
   int* d_err = nullptr;     // set by a device wait that gave up
-  Tile* d_dtiles = nullptr; // level-1 defect tiles
-  int ndtiles = 0, dzc = 1, dsp = 0;
   double mean_b = 0.0;
   bool coeffs_ready = false;
   std::string last_error;
@@ -99,6 +98,7 @@ struct h3d_mg {
   int64_t kernels = 0;
   std::map<std::vector<int>, CachedGraph> graphs;
   bool capturing = false;
+  bool debug_sync = false;  // H3D_DEBUG_SYNC=1: synchronize and check after every launch
   std::vector<double> history;
 };
 
@@ -298,6 +298,15 @@ struct Exec {
 
   bool mixed_level(int g) const { return f32_level(h, g); }
 
+  // Debug mode: synchronize after a launch and name the failing operation.
+  int chk(const char* what, int g) {
+    if (!h->debug_sync) return H3D_OK;
+    cudaError_t e = cudaStreamSynchronize(h->st);
+    if (e != cudaSuccess)
+      return fail(h, H3D_ERR_CUDA, std::string(what) + " (level " + std::to_string(g) + "): " + cudaGetErrorString(e));
+    return H3D_OK;
+  }
+
   // Inside stream capture an event must be recorded as an external node to be
   // timed later; outside capture a plain record.
   cudaError_t record(cudaEvent_t e) {
@@ -323,8 +332,10 @@ struct Exec {
       CU(launch_rbgs<float>(V.variant, h->var, V.zero32, V.d_bl, V.d_tiles, V.ntiles, V.zc, sweep_maps(V, V.cur32),
                             h->d_err, src, dst, V.rhs32,
                             V.fx32, V.fy32, V.fz32, st));
+      TRY(chk("sweep fp32", g));
       if (e1) CU(record(e1));
       CU(launch_fill<float>(V.sweep.d_dst, V.sweep.d_src, V.sweep.n, dst, dst, src, V.zero32, st));
+      TRY(chk("fill fp32", g));
       V.cur32 = 1 - V.cur32;
       V.zero32 = false;
     } else {
@@ -333,8 +344,10 @@ struct Exec {
       CU(launch_rbgs<double>(V.variant, h->var, V.zero64, V.d_bl, V.d_tiles, V.ntiles, V.zc, sweep_maps(V, V.cur64),
                              h->d_err, src, dst, V.rhs64,
                              V.fx64, V.fy64, V.fz64, st));
+      TRY(chk("sweep fp64", g));
       if (e1) CU(record(e1));
       CU(launch_fill<double>(V.sweep.d_dst, V.sweep.d_src, V.sweep.n, dst, dst, src, V.zero64, st));
+      TRY(chk("fill fp64", g));
       V.cur64 = 1 - V.cur64;
       V.zero64 = false;
     }
@@ -355,15 +368,18 @@ struct Exec {
       // the coarsest level of a mixed solve keeps an FP32 rhs too (converted after)
       CU(launch_restrict_tile<float>(C.rvariant, h->var, F.zero32, F.d_bl, C.d_bl, C.d_rtiles, C.nrtiles, C.rzc,
                                      F.phi32[F.cur32], F.rhs32, C.rhs32, F.fx32, F.fy32, F.fz32, h->st));
+      TRY(chk("restrict fp32", gc));
       C.zero32 = true;
       if (!mixed_level(gc)) {  // coarsest level solved in FP64
         CU(launch_convert_f2d(C.rhs32, C.rhs64, C.geom.n_elems, h->st));
+        TRY(chk("convert rhs f2d", gc));
         C.zero64 = true;
         h->kernels += 1;
       }
     } else {
       CU(launch_restrict_tile<double>(C.rvariant, h->var, F.zero64, F.d_bl, C.d_bl, C.d_rtiles, C.nrtiles, C.rzc,
                                       F.phi64[F.cur64], F.rhs64, C.rhs64, F.fx64, F.fy64, F.fz64, h->st));
+      TRY(chk("restrict fp64", gc));
       C.zero64 = true;
     }
     h->kernels += 1;
@@ -383,16 +399,19 @@ struct Exec {
       } else {  // coarsest solved in FP64: bring its iterate to FP32
         if (C.zero64) TRY(materialize_zero64(gf + 1));
         CU(launch_convert_d2f(C.phi64[C.cur64], C.phi32[C.cur32], C.geom.n_elems, h->st));
+        TRY(chk("convert phi d2f", gf + 1));
         h->kernels += 1;
         pc = C.phi32[C.cur32];
       }
       CU(launch_prolong<float>(F.zero32, F.d_bl, C.d_bl, ct, pc, F.phi32[F.cur32], F.phi32[1 - F.cur32], h->st));
+      TRY(chk("prolong fp32", gf));
       F.cur32 = 1 - F.cur32;
       F.zero32 = false;
     } else {
       if (C.zero64) TRY(materialize_zero64(gf + 1));
       CU(launch_prolong<double>(F.zero64, F.d_bl, C.d_bl, ct, C.phi64[C.cur64], F.phi64[F.cur64],
                                 F.phi64[1 - F.cur64], h->st));
+      TRY(chk("prolong fp64", gf));
       F.cur64 = 1 - F.cur64;
       F.zero64 = false;
     }
@@ -457,6 +476,7 @@ struct Exec {
   // FP64 defect on the resident p/b: e = level-1 iterate (or none).
   int defect(bool with_e) {
     Level& V = L(1);
+    RowTab ct{V.d_rows_all, (int)V.geom.bl.size(), V.nrows_all};
     double rscale = h->var ? 1.0 : V.geom.bl[0].dv;
     const double* fx = h->var ? V.fx64 : nullptr;
     const double* fy = h->var ? V.fy64 : nullptr;
@@ -469,19 +489,21 @@ struct Exec {
         if (V.zero32) TRY(materialize_zero32(1));
         e = V.phi32[V.cur32];
       }
-      CU(launch_defect_tile<float, float>(h->var, V.d_bl, h->d_dtiles, h->ndtiles, h->dzc, h->dsp, pin, e, pout,
-                                          h->b64, V.rhs32, h->mean_b, rscale, fx, fy, fz, h->partials, h->st));
+      CU(launch_defect<float, float>(h->var, V.d_bl, ct, pin, e, pout, h->b64, V.rhs32, h->mean_b, rscale, fx, fy, fz,
+                                     h->partials, h->st));
     } else {
       const double* e = nullptr;
       if (with_e) {
         if (V.zero64) TRY(materialize_zero64(1));
         e = V.phi64[V.cur64];
       }
-      CU(launch_defect_tile<double, double>(h->var, V.d_bl, h->d_dtiles, h->ndtiles, h->dzc, h->dsp, pin, e, pout,
-                                            h->b64, V.rhs64, h->mean_b, rscale, fx, fy, fz, h->partials, h->st));
+      CU(launch_defect<double, double>(h->var, V.d_bl, ct, pin, e, pout, h->b64, V.rhs64, h->mean_b, rscale, fx, fy,
+                                       fz, h->partials, h->st));
     }
+    TRY(chk("defect", 1));
     if (with_e) h->pc = 1 - h->pc;
-    CU(launch_reduce4(h->partials, h->ndtiles, h->d_res, h->st));
+    CU(launch_reduce4(h->partials, defect_grid(ct.nrows), h->d_res, h->st));
+    TRY(chk("reduce", 1));
     CU(cudaMemcpyAsync(h->h_res, h->d_res, 4 * sizeof(double), cudaMemcpyDeviceToHost, h->st));
     h->kernels += 2;
     return H3D_OK;
@@ -854,7 +876,6 @@ int h3d_mg_destroy(h3d_mg* h) {
   dfree(h->d_res);
   dfree(h->d_h3);
   dfree(h->d_err);
-  dfree(h->d_dtiles);
   if (h->h_res) cudaFreeHost(h->h_res);
   if (h->st) cudaStreamDestroy(h->st);
   delete h;
@@ -901,6 +922,11 @@ int h3d_mg_create(h3d_mg** out, const h3d_mg_desc* desc) {
   if (h->desc.maxcy <= 0) h->desc.maxcy = 30;  // control.cin default
   if (h->desc.inner_cycles <= 0) h->desc.inner_cycles = 2;
   h->L = D.ngrd_gl;
+  {
+    const char* dbg = std::getenv("H3D_DEBUG_SYNC");
+    h->debug_sync = dbg && dbg[0] == '1';
+    if (h->debug_sync) h->desc.use_graph = 0;
+  }
   h->mixed = D.precision == H3D_PREC_MIXED;
   h->var = D.var_coef != 0;
   int rc = H3D_OK;
@@ -967,20 +993,7 @@ int h3d_mg_create(h3d_mg** out, const h3d_mg_desc* desc) {
   const size_t n1 = (size_t)h->lev[1].geom.n_elems;
   if ((rc = dalloc(h, &h->p64[0], n1)) || (rc = dalloc(h, &h->p64[1], n1)) || (rc = dalloc(h, &h->b64, n1)))
     return bail(rc);
-  {
-    const LevelGeom& G1 = h->lev[1].geom;
-    int nxm = 0;
-    for (const auto& B : G1.bl) nxm = std::max(nxm, B.nx);
-    h->dsp = (nxm + 2 + 1) & ~1;
-    if (defect_tile_smem(h->dsp) > 200 * 1024) return bail(fail(h, H3D_ERR_BAD_CONFIG, "block rows too long"));
-    h->dzc = pick_zc(G1, defect_tile_rows());
-    std::vector<Tile> dt = row_tiles(G1, defect_tile_rows(), h->dzc);
-    h->ndtiles = (int)dt.size();
-    if ((rc = dalloc(h, &h->d_dtiles, dt.size())) != H3D_OK) return bail(rc);
-    if (cudaMemcpy(h->d_dtiles, dt.data(), dt.size() * sizeof(Tile), cudaMemcpyHostToDevice) != cudaSuccess)
-      return bail(fail(h, H3D_ERR_CUDA, "copy defect tiles"));
-  }
-  h->npartials = std::max(std::max(std::max(h->lev[1].ncta_all, h->lev[1].ncta_int), kDefectCtas), h->ndtiles);
+  h->npartials = std::max(std::max(h->lev[1].ncta_all, h->lev[1].ncta_int), kDefectCtas);
   if ((rc = dalloc(h, &h->partials, 4 * (size_t)h->npartials)) || (rc = dalloc(h, &h->d_res, 4))) return bail(rc);
   if (cudaMallocHost((void**)&h->h_res, 4 * sizeof(double)) != cudaSuccess)
     return bail(fail(h, H3D_ERR_OOM, "pinned result buffer"));
@@ -1111,13 +1124,16 @@ int h3d_mg_solve_resident(h3d_mg* h, const h3d_solve_opts* opts, h3d_solve_info*
                          false, h->st));
   h->kernels += 1;
   Exec ex{h};
+  TRY(ex.chk("pressure halo", 1));
   h->mean_b = 0.0;
   if (h->mixed && is_all_neumann(h)) {
     // FP64 null-space handling: the compatible part of b has zero mean; the
     // FP32 cycles see the defect with the mean of b removed.
     CellTab ct{V.d_cta_int, (int)V.geom.bl.size(), V.ncta_int};
     CU(launch_sum_interior(V.d_bl, ct, h->b64, h->partials, h->st));
+    TRY(ex.chk("sum b", 1));
     CU(launch_reduce4(h->partials, ct.ncta, h->d_res, h->st));
+    TRY(ex.chk("reduce sum b", 1));
     CU(cudaMemcpyAsync(h->h_res, h->d_res, 4 * sizeof(double), cudaMemcpyDeviceToHost, h->st));
     CU(cudaStreamSynchronize(h->st));
     h->mean_b = h->h_res[0] / (double)V.geom.n_interior;
