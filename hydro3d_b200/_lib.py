@@ -98,7 +98,7 @@ EXPORTS = [
     "h3d_mg_history", "h3d_mg_put_level", "h3d_mg_get_level", "h3d_mg_mgrelax", "h3d_mg_mgrestr",
     "h3d_mg_mgcorr", "h3d_mg_mgbound", "h3d_mg_exchangepp", "h3d_mg_vcycle", "h3d_mg_sync",
     "h3d_mg_set_profiling", "h3d_mg_smoother_bytes", "h3d_mg_set_smoother", "h3d_mg_get_smoother", "h3d_topology", "h3d_halo_table",
-    "h3d_mg_strerror", "h3d_mg_last_error",
+    "h3d_mg_strerror", "h3d_mg_last_error", "h3d_residual_noalloc",
 ]
 
 _lib = None
@@ -150,6 +150,7 @@ def lib():
         "h3d_mg_get_smoother": (i32, [vp, i32, C.POINTER(i32), C.POINTER(i32), C.POINTER(i32)]),
         "h3d_topology": (i32, [i32, C.POINTER(C.c_int32), C.POINTER(C.c_int32), pd, i32, C.POINTER(BlockDesc)]),
         "h3d_halo_table": (i32, [i32, C.POINTER(BlockDesc), i32, i32, pu32, pu32, i64, C.POINTER(i64)]),
+        "h3d_residual_noalloc": (i32, [C.c_void_p, C.c_void_p, i32, i32, i32, pd, i32, pd, C.c_void_p]),
         "h3d_mg_strerror": (C.c_char_p, [C.c_int]),
         "h3d_mg_last_error": (C.c_char_p, [vp]),
     }

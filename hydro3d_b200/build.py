@@ -19,7 +19,7 @@ CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libh3dmg.so")
 BUILD = os.path.join(ROOT, "_build")
 
-SOURCES = ["h3d_halo.cpp", "h3d_kernels.cu", "h3d_mg.cu"]
+SOURCES = ["h3d_halo.cpp", "h3d_kernels.cu", "h3d_mg.cu", "h3d_noalloc.cu"]
 HEADERS = ["h3d_internal.h", "h3d_kernels.cuh"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

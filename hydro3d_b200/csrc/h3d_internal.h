@@ -52,4 +52,7 @@ int build_halo_table(const std::vector<h3d_block_desc>& blocks, int g, int kind,
                      std::vector<uint32_t>& dst, std::vector<uint32_t>& src,
                      std::string* err);
 
+// Error text of a call that has no handle (read with h3d_mg_last_error(NULL)).
+void set_call_error(const std::string& msg);
+
 }  // namespace h3d

@@ -25,6 +25,12 @@ namespace {
 
 thread_local std::string g_create_error;
 
+}  // namespace
+
+void h3d::set_call_error(const std::string& msg) { g_create_error = msg; }
+
+namespace {
+
 struct Halo {
   uint32_t* d_dst = nullptr;
   uint32_t* d_src = nullptr;

@@ -1,0 +1,93 @@
+"""h3d_residual_noalloc (allocation-free residual norms) against h3d_mg_residual.
+
+Both are called through the C ABI on the same fields; the allocation-free
+entry point is called twice in a row on the same arrays and must give the
+same answer both times.  The two sum in different orders, so the norms are
+compared with a relative tolerance of 1e-12.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+W, P = 4, 5
+RTOL = 1e-12
+
+
+def _call(lib, p_dev, b_dev, n, h, phys):
+    import torch
+    out = (C.c_double * 4)()
+    hh = (C.c_double * 3)(*h)
+    rc = lib.h3d_residual_noalloc(C.c_void_p(p_dev.data_ptr()), C.c_void_p(b_dev.data_ptr()),
+                                  n[0], n[1], n[2], hh, phys, out, None)
+    assert rc == 0, lib.h3d_mg_last_error(None)
+    torch.cuda.synchronize()
+    return np.array(out[:])
+
+
+def _numpy_residual(p, b, n, h, phys):
+    nx, ny, nz = n
+    ax, ay, az = (1.0 / (x * x) for x in h)
+    c = p[1:-1, 1:-1, 1:-1]
+    acc = np.zeros_like(c)
+    for (sl, a, bit) in (((slice(1, -1), slice(1, -1), slice(0, -2)), ax, 1),
+                         ((slice(1, -1), slice(1, -1), slice(2, None)), ax, 2),
+                         ((slice(1, -1), slice(0, -2), slice(1, -1)), ay, 4),
+                         ((slice(1, -1), slice(2, None), slice(1, -1)), ay, 8),
+                         ((slice(0, -2), slice(1, -1), slice(1, -1)), az, 16),
+                         ((slice(2, None), slice(1, -1), slice(1, -1)), az, 32)):
+        coef = np.full(c.shape, a)
+        if phys & bit:
+            edge = {1: (..., 0), 2: (..., -1), 4: (slice(None), 0), 8: (slice(None), -1),
+                    16: (0,), 32: (-1,)}[bit]
+            coef[edge] = 0.0
+        acc += coef * (p[sl] - c)
+    return b[1:-1, 1:-1, 1:-1] - acc
+
+
+@pytest.mark.parametrize("bc,phys", [([W] * 6, 63), ([P, P, W, W, W, W], 60)])
+def test_noalloc_matches_solver_residual(h3d, bc, phys):
+    import torch
+    n = (40, 24, 32)
+    h = (0.025, 0.04, 0.03)
+    blocks = h3d.topology.block_grid((1, 1, 1), n, bc, list(h), 3)
+    rng = np.random.default_rng(77)
+    shape = (n[2] + 2, n[1] + 2, n[0] + 2)
+    p = rng.standard_normal(shape)
+    b = np.zeros(shape)
+    b[1:-1, 1:-1, 1:-1] = rng.standard_normal((n[2], n[1], n[0]))
+    if not phys & 1:  # periodic x: ghosts hold the opposite interior plane
+        p[:, :, 0] = p[:, :, n[0]]
+        p[:, :, n[0] + 1] = p[:, :, 1]
+
+    s = h3d.MultigridSolver(blocks, 3)
+    s.upload("p", 0, p)
+    s.upload("b", 0, b)
+    rr, bb, rinf = s.residual()
+    s.close()
+
+    lib = h3d.lib()
+    p_dev = torch.from_numpy(p).cuda()
+    b_dev = torch.from_numpy(b).cuda()
+    first = _call(lib, p_dev, b_dev, n, h, phys)
+    second = _call(lib, p_dev, b_dev, n, h, phys)
+    assert np.array_equal(first, second)
+    for got, want in ((first[0], rr), (first[1], bb), (first[2], rinf)):
+        assert abs(got - want) <= RTOL * abs(want), (got, want)
+    r = _numpy_residual(p, b, n, h, phys)
+    assert abs(first[3] - r.sum()) <= 1e-10 * np.abs(r).sum()
+    assert np.array_equal(p_dev.cpu().numpy(), p) and np.array_equal(b_dev.cpu().numpy(), b)
+
+
+def test_noalloc_rejects_oversize(h3d):
+    import torch
+    lib = h3d.lib()
+    dummy = torch.zeros(8, dtype=torch.float64, device="cuda")
+    out = (C.c_double * 4)()
+    hh = (C.c_double * 3)(1.0, 1.0, 1.0)
+    rc = lib.h3d_residual_noalloc(C.c_void_p(dummy.data_ptr()), C.c_void_p(dummy.data_ptr()),
+                                  8, 257, 256, hh, 63, out, None)
+    assert rc == h3d._lib.H3D_ERR_ARG
+    assert b"65536" in lib.h3d_mg_last_error(None)
