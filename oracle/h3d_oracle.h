@@ -7,11 +7,14 @@
  * into, loaded by, or called from the product library (hydro3d_b200).
  *
  * Parity pinning: the reference ships no golden vectors or known-answer
- * tests for this path and cannot be built here (Fortran, no compiler).  The
- * oracle is pinned by (a) golden fixtures produced from the reference's own
- * Fortran source by the mechanical translator in oracle/fortran_ref.py
- * (see oracle/Makefile target `ref`), and (b) algebraic properties
- * (manufactured Neumann cosine modes, null space, symmetry).
+ * tests for this path and cannot be compiled here (Fortran and MPI; neither
+ * toolchain is in the image).  The oracle is pinned by (a) golden fixtures
+ * made by running the reference's own Fortran source (coeff, mgkcyc,
+ * mgrelax, mgrestr, mgcorr, mgbound, exchangepp, exchbc_mgpp,
+ * localparameters) through the statement-by-statement translator in
+ * oracle/fortran_ref.py (tests/golden/make_golden.py; the oracle reproduces
+ * every fixture bit for bit, tests/test_golden.py), and (b) algebraic
+ * properties (manufactured Neumann cosine modes, null space, symmetry).
  *
  * Every routine cites the reference file:line it restates.  Storage keeps the
  * reference's per-block `cof` work array and its j-fastest level layout
