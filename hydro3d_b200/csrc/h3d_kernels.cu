@@ -518,6 +518,154 @@ __global__ void __launch_bounds__(TPR*(TY + 2)) k_rbgs_tma(const BlkLev* __restr
   if (ze == nz) black_store(nz);
 }
 
+// ---------------------------------------------------------------------------
+// Single-barrier TMA sweep (k_rbgs_tma2).
+//
+// Same cell mapping, arithmetic and out-of-place contract as k_rbgs_tma, with
+// two changes that take the latency of global loads off the z march:
+//  * the right-hand side of rows y0-1 .. y0+TY of each plane comes in by TMA
+//    too (its own tensor map, box TY+2 rows), in the same ring slot and on
+//    the same mbarrier as the iterate's plane;
+//  * the black update trails the red update by two planes, so one barrier
+//    per plane suffices: phase z updates red cells of plane z (reading planes
+//    z-1..z+1, writing plane z in shared memory) and black cells of plane
+//    z-2 (reading only the red-updated planes z-3..z-1, writing global
+//    memory).  The two never touch the same plane.
+// A plane p is last read in phase p+3, so a ring of D+4 slots lets the copy
+// of plane z+D+1 be issued right after the barrier that ends phase z.
+template <typename T, int TPR, int CP, int TY, int D>
+struct Tma2Cfg {
+  static constexpr int NS = D + 4;
+  static constexpr int VEC = 16 / (int)sizeof(T);
+  static constexpr int SPMAX = ((2 * CP * TPR + 2 + VEC - 1) / VEC) * VEC;
+  static constexpr int PSLOT = ((SPMAX * (TY + 4) * (int)sizeof(T) + 127) / 128) * 128;
+  static constexpr int RSLOT = ((SPMAX * (TY + 2) * (int)sizeof(T) + 127) / 128) * 128;
+  static constexpr int SLOT = PSLOT + RSLOT;
+  static constexpr size_t SMEM = (size_t)NS * SLOT + 128 + NS * 8;
+};
+
+template <typename T, int TPR, int CP, int TY, int D, bool VAR>
+__global__ void __launch_bounds__(TPR*(TY + 2)) k_rbgs_tma2(const BlkLev* __restrict__ bls,
+                                                           const Tile* __restrict__ tiles, int zc,
+                                                           const CUtensorMap* __restrict__ maps,
+                                                           const CUtensorMap* __restrict__ rmaps,
+                                                           T* __restrict__ dst, const T* __restrict__ fx,
+                                                           const T* __restrict__ fy, const T* __restrict__ fz,
+                                                           int* err) {
+  using C = Tma2Cfg<T, TPR, CP, TY, D>;
+  constexpr int NS = C::NS;
+  extern __shared__ unsigned char smem_raw[];
+  unsigned char* base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
+  uint64_t* bars = reinterpret_cast<uint64_t*>(base + NS * C::SLOT);
+
+  const Tile t = tiles[blockIdx.x];
+  const BlkLev B = bls[t.b];
+  const CUtensorMap* map = maps + t.b;
+  const CUtensorMap* rmap = rmaps + t.b;
+  const int nx = B.nx, ny = B.ny, nz = B.nz;
+  const int sx = B.sx;
+  const long long sxy = B.sxy;
+  T* __restrict__ Dst = dst + B.off;
+  const T* FX = VAR ? fx + B.off : nullptr;
+  const T* FY = VAR ? fy + B.off : nullptr;
+  const T* FZ = VAR ? fz + B.off : nullptr;
+  const int y0 = t.y0, zs = t.z0;
+  const int ze = min(zs + zc - 1, nz);
+  const int zlo = max(zs - 1, 1), zhi = min(ze + 1, nz);
+  const int BX = ((nx + 2 + C::VEC - 1) / C::VEC) * C::VEC;  // smem row pitch == TMA box width
+  const uint32_t tx_bytes = (uint32_t)(BX * (2 * TY + 6) * (int)sizeof(T));
+  const int tr = threadIdx.x / TPR, tc = threadIdx.x - (threadIdx.x / TPR) * TPR;
+  const int y = y0 - 1 + tr;
+  const int prow = (tr + 1) * BX;  // row y in an iterate slot (slot row 0 = y0-2)
+  const int rrow = tr * BX;        // row y in a right-hand-side slot (slot row 0 = y0-1)
+  const bool row_in = y >= 1 && y <= ny;
+  const bool row_own = tr >= 1 && tr <= TY && y <= ny;
+  const bool leader = threadIdx.x == 0;
+  bool bad = false;
+
+  if (leader) {
+    for (int q = 0; q < NS; ++q)
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(bars + q)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  __syncthreads();
+
+  auto pslot = [&](int z) -> T* { return reinterpret_cast<T*>(base + (z % NS) * C::SLOT); };
+  auto rslot = [&](int z) -> const T* { return reinterpret_cast<const T*>(base + (z % NS) * C::SLOT + C::PSLOT); };
+  auto issue = [&](int z) {  // leader only
+    const uint32_t bar = smem_u32(bars + (z % NS));
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(tx_bytes) : "memory");
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];\n" ::
+            "r"(smem_u32(pslot(z))),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(0), "r"(y0 - 2), "r"(z), "r"(bar)
+        : "memory");
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];\n" ::
+            "r"(smem_u32(rslot(z))),
+        "l"(reinterpret_cast<uint64_t>(rmap)), "r"(0), "r"(y0 - 1), "r"(z), "r"(bar)
+        : "memory");
+  };
+  auto wait_plane = [&](int z) {
+    const uint32_t parity = (uint32_t)(((z - zlo + 1) / NS) & 1);
+    mbar_wait(smem_u32(bars + (z % NS)), parity, err, bad);
+  };
+  RowGs<T, CP, VAR> gs;
+  gs.init(B, y, tc, TPR);
+  auto red = [&](int z) {
+    if (!row_in) return;
+    T* P = pslot(z);
+    const T* Pm = pslot(z - 1);
+    const T* Pp = pslot(z + 1);
+    const T* Rr = rslot(z) + rrow;
+    const int j = (y + z) & 1;
+    const long long zo = (long long)z * sxy + (long long)y * sx;
+#pragma unroll
+    for (int k = 0; k < CP; ++k) {
+      const int x = 2 * (tc + k * TPR) + 1 + j;
+      if (x <= nx && H3D_IN(44, t.b, prow + x - BX, C::PSLOT / (int)sizeof(T) - 2 * BX))
+        P[prow + x] = gs.update(P, Pm, Pp, prow + x, BX, k, j, z, Rr[x], FX, FY, FZ, zo + x, sx, sxy);
+    }
+  };
+  auto black_store = [&](int z) {
+    if (!row_own) return;
+    const T* P = pslot(z);
+    const T* Pm = pslot(z - 1);
+    const T* Pp = pslot(z + 1);
+    const T* Rr = rslot(z) + rrow;
+    const long long zo = (long long)z * sxy + (long long)y * sx;
+    T* Drow = Dst + zo;
+    const int jb = (y + z + 1) & 1;
+#pragma unroll
+    for (int k = 0; k < CP; ++k) {
+      const int xp = 2 * (tc + k * TPR) + 1;
+      if (xp > nx) continue;
+      const int xb = xp + jb, xr = xp + 1 - jb;
+      if (!H3D_IN(45, t.b, zo + xb, sxy * (nz + 2)) || !H3D_IN(46, t.b, prow + xb - BX, C::PSLOT / (int)sizeof(T) - 2 * BX))
+        continue;
+      const T vr = P[prow + xr];
+      const T vb = gs.update(P, Pm, Pp, prow + xb, BX, k, jb, z, Rr[xb], FX, FY, FZ, zo + xb, sx, sxy);
+      Drow[xr] = vr;
+      Drow[xb] = vb;
+    }
+  };
+
+  if (leader)
+    for (int q = zlo - 1; q <= min(zlo + D, zhi + 1); ++q) issue(q);
+  wait_plane(zlo - 1);
+  wait_plane(zlo);
+  for (int z = zlo; z <= ze + 2; ++z) {
+    if (z <= zhi) {
+      wait_plane(z + 1);
+      red(z);
+    }
+    if (z - 2 >= zs && z - 2 <= ze) black_store(z - 2);
+    __syncthreads();
+    if (leader && z + D + 1 <= zhi + 1) issue(z + D + 1);
+  }
+}
+
 template <typename T, int TPR, int CP, int TY>
 constexpr size_t tma_smem() {
   constexpr int VEC = 16 / (int)sizeof(T);
@@ -988,20 +1136,26 @@ inline int grid_for(int64_t n, int nt) {
 // Smoother variants: 0-7 generic tiles (k_rbgs), 8+ row tiles (k_rbgs_rows,
 // tx = largest supported nx).
 static const TileShape kShapes[] = {
-    {32, 16, 256, false, 0, 0, false, -1}, {32, 8, 256, false, 0, 0, false, -1},
-    {64, 8, 256, false, 0, 0, false, -1},  {16, 8, 128, false, 0, 0, false, -1},
-    {8, 8, 64, false, 0, 0, false, -1},    {8, 4, 32, false, 0, 0, false, -1},
-    {4, 4, 32, false, 0, 0, false, -1},    {64, 16, 512, false, 0, 0, false, -1},
-    {128, 8, 640, true, 64, 1, false, -1}, {128, 8, 320, true, 32, 2, false, -1},   // 8, 9
-    {64, 8, 320, true, 32, 1, false, -1},  {64, 16, 576, true, 32, 1, false, -1},   // 10, 11
-    {32, 16, 288, true, 16, 1, false, -1}, {16, 16, 144, true, 8, 1, false, -1},    // 12, 13
-    {256, 8, 640, true, 64, 2, false, -1}, {128, 4, 384, true, 64, 1, false, -1},   // 14, 15
-    {256, 4, 768, true, 128, 1, false, -1}, {128, 4, 192, true, 32, 2, false, -1},  // 16, 17
-    {256, 8, 320, true, 32, 4, false, -1},                                          // 18
-    {128, 8, 640, true, 64, 1, true, 8},   {128, 8, 320, true, 32, 2, true, 9},     // 19, 20
-    {64, 8, 320, true, 32, 1, true, 10},   {64, 16, 576, true, 32, 1, true, 11},    // 21, 22
-    {32, 16, 288, true, 16, 1, true, 12},  {16, 16, 144, true, 8, 1, true, 13},     // 23, 24
-    {128, 4, 384, true, 64, 1, true, 15},  {128, 4, 192, true, 32, 2, true, 17},    // 25, 26
+    {32, 16, 256, false, 0, 0, 0, -1}, {32, 8, 256, false, 0, 0, 0, -1},
+    {64, 8, 256, false, 0, 0, 0, -1},  {16, 8, 128, false, 0, 0, 0, -1},
+    {8, 8, 64, false, 0, 0, 0, -1},    {8, 4, 32, false, 0, 0, 0, -1},
+    {4, 4, 32, false, 0, 0, 0, -1},    {64, 16, 512, false, 0, 0, 0, -1},
+    {128, 8, 640, true, 64, 1, 0, -1}, {128, 8, 320, true, 32, 2, 0, -1},   // 8, 9
+    {64, 8, 320, true, 32, 1, 0, -1},  {64, 16, 576, true, 32, 1, 0, -1},   // 10, 11
+    {32, 16, 288, true, 16, 1, 0, -1}, {16, 16, 144, true, 8, 1, 0, -1},    // 12, 13
+    {256, 8, 640, true, 64, 2, 0, -1}, {128, 4, 384, true, 64, 1, 0, -1},   // 14, 15
+    {256, 4, 768, true, 128, 1, 0, -1}, {128, 4, 192, true, 32, 2, 0, -1},  // 16, 17
+    {256, 8, 320, true, 32, 4, 0, -1},                                          // 18
+    {128, 8, 640, true, 64, 1, 1, 8},   {128, 8, 320, true, 32, 2, 1, 9},     // 19, 20
+    {64, 8, 320, true, 32, 1, 1, 10},   {64, 16, 576, true, 32, 1, 1, 11},    // 21, 22
+    {32, 16, 288, true, 16, 1, 1, 12},  {16, 16, 144, true, 8, 1, 1, 13},     // 23, 24
+    {128, 4, 384, true, 64, 1, 1, 15},  {128, 4, 192, true, 32, 2, 1, 17},          // 25, 26
+    {128, 4, 192, true, 32, 2, 2, 17},  {128, 8, 320, true, 32, 2, 2, 9},           // 27, 28
+    {128, 4, 384, true, 64, 1, 2, 15},  {128, 8, 640, true, 64, 1, 2, 8},           // 29, 30
+    {64, 8, 320, true, 32, 1, 2, 10},   {64, 16, 576, true, 32, 1, 2, 11},          // 31, 32
+    {32, 16, 288, true, 16, 1, 2, 12},  {128, 16, 576, true, 32, 2, 2, 37},         // 33, 34
+    {128, 8, 320, true, 32, 2, 2, 9},   {16, 16, 144, true, 8, 1, 2, 13},           // 35, 36
+    {128, 16, 576, true, 32, 2, 0, -1},                                             // 37
 };
 #ifdef H3D_BOUNDS_CHECK
 // Debug builds only: first recorded out-of-bounds access {kernel id + 1, block, index, limit}.
@@ -1010,7 +1164,7 @@ extern "C" int h3d_debug_bounds(unsigned long long* out) {
   return 0;
 }
 #endif
-int tma_ty_index(int ty) { return ty == 4 ? 0 : ty == 8 ? 1 : ty == 16 ? 2 : -1; }
+int tma_ty_index(int ty) { return ty == 4 ? 0 : ty == 8 ? 1 : ty == 16 ? 2 : ty == 32 ? 3 : -1; }
 int num_tile_shapes() { return (int)(sizeof(kShapes) / sizeof(kShapes[0])); }
 TileShape tile_shape(int v) { return kShapes[v]; }
 
@@ -1083,6 +1237,50 @@ static cudaError_t tma_dispatch(bool var, const BlkLev* bl, const Tile* tiles, i
   return cudaGetLastError();
 }
 
+// Prefetch depth actually used: the requested D, lowered until the ring fits
+// in the 227 KB of shared memory a CTA may have.
+template <typename T, int TPR, int CP, int TY, int D>
+constexpr int tma2_depth() {
+  if constexpr (D <= 1 || Tma2Cfg<T, TPR, CP, TY, D>::SMEM <= 232448) return D;
+  else return tma2_depth<T, TPR, CP, TY, D - 1>();
+}
+
+template <typename T, int TPR, int CP, int TY, int D0>
+static cudaError_t tma2_attr() {
+  constexpr int D = tma2_depth<T, TPR, CP, TY, D0>();
+  static_assert(Tma2Cfg<T, TPR, CP, TY, D>::SMEM <= 232448, "TMA ring exceeds shared memory");
+  const int sm = (int)Tma2Cfg<T, TPR, CP, TY, D>::SMEM;
+  cudaError_t e;
+  if ((e = cudaFuncSetAttribute(k_rbgs_tma2<T, TPR, CP, TY, D, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm))) return e;
+  return cudaFuncSetAttribute(k_rbgs_tma2<T, TPR, CP, TY, D, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+}
+
+template <typename T, int TPR, int CP, int TY, int D0>
+static cudaError_t tma2_dispatch(bool var, const BlkLev* bl, const Tile* tiles, int ntiles, int zc,
+                                 const CUtensorMap* maps, const CUtensorMap* rmaps, int* err, T* dst, const T* fx,
+                                 const T* fy, const T* fz, cudaStream_t st) {
+  if (ntiles <= 0) return cudaSuccess;
+  constexpr int D = tma2_depth<T, TPR, CP, TY, D0>();
+  constexpr int NT = TPR * (TY + 2);
+  constexpr size_t SM = Tma2Cfg<T, TPR, CP, TY, D>::SMEM;
+  if (var) k_rbgs_tma2<T, TPR, CP, TY, D, true><<<ntiles, NT, SM, st>>>(bl, tiles, zc, maps, rmaps, dst, fx, fy, fz, err);
+  else k_rbgs_tma2<T, TPR, CP, TY, D, false><<<ntiles, NT, SM, st>>>(bl, tiles, zc, maps, rmaps, dst, fx, fy, fz, err);
+  return cudaGetLastError();
+}
+
+// (variant, threads per row, pairs per thread, rows, prefetch depth)
+#define H3D_TMA2_SHAPES(X) \
+  X(27, 32, 2, 4, 3)       \
+  X(28, 32, 2, 8, 3)       \
+  X(29, 64, 1, 4, 3)       \
+  X(30, 64, 1, 8, 3)       \
+  X(31, 32, 1, 8, 3)       \
+  X(32, 32, 1, 16, 2)      \
+  X(33, 16, 1, 16, 2)      \
+  X(34, 32, 2, 16, 2)      \
+  X(35, 32, 2, 8, 2)       \
+  X(36, 8, 1, 16, 2)
+
 #define H3D_TMA_SHAPES(X) \
   X(19, 64, 1, 8)         \
   X(20, 32, 2, 8)         \
@@ -1104,7 +1302,8 @@ static cudaError_t tma_dispatch(bool var, const BlkLev* bl, const Tile* tiles, i
   X(15, 64, 1, 4)          \
   X(16, 128, 1, 4)         \
   X(17, 32, 2, 4)          \
-  X(18, 32, 4, 8)
+  X(18, 32, 4, 8)          \
+  X(37, 32, 2, 16)
 
 cudaError_t init_kernel_attributes() {
   cudaError_t e = cudaSuccess;
@@ -1118,6 +1317,11 @@ cudaError_t init_kernel_attributes() {
   if ((e = tma_attr<double, tpr, cp, ty>()) != cudaSuccess) return e;
   H3D_TMA_SHAPES(X)
 #undef X
+#define X(v, tpr, cp, ty, d)                                                 \
+  if ((e = tma2_attr<float, tpr, cp, ty, d>()) != cudaSuccess) return e;     \
+  if ((e = tma2_attr<double, tpr, cp, ty, d>()) != cudaSuccess) return e;
+  H3D_TMA2_SHAPES(X)
+#undef X
   return e;
 }
 
@@ -1125,10 +1329,11 @@ cudaError_t init_kernel_attributes() {
 
 template <typename T>
 cudaError_t launch_rbgs(int variant, bool var, bool zero_src, const BlkLev* bl, const Tile* tiles, int ntiles,
-                        int zc, const CUtensorMap* maps, int* err, const T* src, T* dst, const T* rhs, const T* fx,
-                        const T* fy, const T* fz, cudaStream_t st) {
+                        int zc, const CUtensorMap* maps, const CUtensorMap* rmaps, int* err, const T* src, T* dst,
+                        const T* rhs, const T* fx, const T* fy, const T* fz, cudaStream_t st) {
   if (variant >= 0 && variant < num_tile_shapes() && kShapes[variant].tma) {
-    if (zero_src || !maps) variant = kShapes[variant].alt;  // nothing to stage: plain zero-fill kernel
+    // nothing to stage from a zero source: the equivalent plain-load kernel zero-fills
+    if (zero_src || !maps || (kShapes[variant].tma == 2 && !rmaps)) variant = kShapes[variant].alt;
   }
   switch (variant) {
     case 0: return rbgs_dispatch<T, 32, 16, 256>(var, zero_src, bl, tiles, ntiles, zc, src, dst, rhs, fx, fy, fz, st);
@@ -1146,6 +1351,10 @@ cudaError_t launch_rbgs(int variant, bool var, bool zero_src, const BlkLev* bl, 
 #define X(v, tpr, cp, ty) \
     case v: return tma_dispatch<T, tpr, cp, ty>(var, bl, tiles, ntiles, zc, maps, err, dst, rhs, fx, fy, fz, st);
     H3D_TMA_SHAPES(X)
+#undef X
+#define X(v, tpr, cp, ty, d) \
+    case v: return tma2_dispatch<T, tpr, cp, ty, d>(var, bl, tiles, ntiles, zc, maps, rmaps, err, dst, fx, fy, fz, st);
+    H3D_TMA2_SHAPES(X)
 #undef X
     default: return cudaErrorInvalidValue;
   }
@@ -1317,10 +1526,10 @@ cudaError_t launch_face_coef(const BlkLev* bl, CellTab ct, const double* dens, c
 
 // explicit instantiations
 template cudaError_t launch_rbgs<double>(int, bool, bool, const BlkLev*, const Tile*, int, int, const CUtensorMap*,
-                                         int*, const double*, double*, const double*, const double*, const double*,
+                                         const CUtensorMap*, int*, const double*, double*, const double*, const double*, const double*,
                                          const double*, cudaStream_t);
 template cudaError_t launch_rbgs<float>(int, bool, bool, const BlkLev*, const Tile*, int, int, const CUtensorMap*,
-                                        int*, const float*, float*, const float*, const float*, const float*,
+                                        const CUtensorMap*, int*, const float*, float*, const float*, const float*, const float*,
                                         const float*, cudaStream_t);
 template cudaError_t launch_fill<double>(const uint32_t*, const uint32_t*, int64_t, double*, const double*,
                                          const double*, bool, cudaStream_t);

@@ -30,12 +30,12 @@ struct TileShape {
   int tx, ty, nt;
   bool rows;
   int tpr, cp;
-  bool tma;  // planes staged by TMA (needs tensor maps of the source buffer)
+  int tma;   // 0 plain loads; 1 iterate planes staged by TMA; 2 iterate and right-hand side by TMA
   int alt;   // for TMA shapes: the equivalent row shape (used for zero sources)
 };
 // TMA box heights (TY+4) are one of these; tensor maps are built per height.
-constexpr int kNumTmaTy = 3;
-int tma_ty_index(int ty);  // 0,1,2 for TY = 4, 8, 16; -1 otherwise
+constexpr int kNumTmaTy = 4;
+int tma_ty_index(int ty);  // 0,1,2,3 for TY = 4, 8, 16, 32; -1 otherwise
 constexpr int kDefectCtas = 148 * 4;  // CTAs (and partial sums) of the defect kernel
 int defect_grid(int nrows);
 // Sets the dynamic shared-memory limits of the row-tile smoothers (call once
@@ -60,11 +60,13 @@ TileShape tile_shape(int variant);
 
 // One out-of-place red-black sweep (both colours) of every block of a level:
 // dst = sweep(src).  zero_src: src is identically zero (not read).
-// maps: tensor maps of src for every block (TMA variants); err: device flag
-// set when a bounded wait gives up.
+// maps: tensor maps of src for every block (TMA variants); rmaps: tensor maps
+// of rhs (variants that stage it); err: device flag set when a bounded wait
+// gives up.
 template <typename T>
 cudaError_t launch_rbgs(int variant, bool var, bool zero_src, const BlkLev* bl, const Tile* tiles,
-                        int ntiles, int zc, const CUtensorMap* maps, int* err, const T* src, T* dst,
+                        int ntiles, int zc, const CUtensorMap* maps, const CUtensorMap* rmaps, int* err,
+                        const T* src, T* dst,
                         const T* rhs, const T* fx, const T* fy,
                         const T* fz, cudaStream_t st);
 

@@ -60,7 +60,7 @@ struct Level {
   float *fx32 = nullptr, *fy32 = nullptr, *fz32 = nullptr;
   double* dens = nullptr;
   Halo sweep, faces, exch, bound;
-  CUtensorMap* d_maps = nullptr;  // [ty index][buffer][block] tensor maps of the iterate
+  CUtensorMap* d_maps = nullptr;  // [ty index][0,1: iterate buffer, 2: rhs][block] tensor maps
   Tile* d_rtiles = nullptr;       // restriction tiles (this level as the coarse level)
   int nrtiles = 0, rvariant = 0, rzc = 1;
   bool tma_ok = false;
@@ -267,7 +267,7 @@ void default_tile(const Level& Lv, int* variant, int* zc) {
   else if (nxm >= 8) v = nym >= 8 ? 4 : 5;
   else v = 6;
   // whole-row tiles when every block allows them (TMA-staged first)
-  const int pref[] = {24, 23, 21, 20, 13, 12, 10, 8, 14, 16};
+  const int pref[] = {36, 33, 32, 28, 24, 23, 21, 20, 13, 12, 10, 8, 14, 16};
   for (int cand : pref) {
     TileShape c = tile_shape(cand);
     if (nxm <= c.tx && nxm * 2 > c.tx / 2 && variant_fits(Lv, cand) && nym >= 4) { v = cand; break; }
@@ -288,7 +288,16 @@ const CUtensorMap* sweep_maps(const Level& V, int buf) {
   if (!s.tma || !V.tma_ok) return nullptr;
   int ti = tma_ty_index(s.ty);
   if (ti < 0) return nullptr;
-  return V.d_maps + ((size_t)ti * 2 + buf) * V.geom.bl.size();
+  return V.d_maps + ((size_t)ti * 3 + buf) * V.geom.bl.size();
+}
+
+// Tensor maps of the level's right-hand side (box TY+2 rows), or null.
+const CUtensorMap* rhs_maps(const Level& V) {
+  TileShape s = tile_shape(V.variant);
+  if (s.tma != 2 || !V.tma_ok) return nullptr;
+  int ti = tma_ty_index(s.ty);
+  if (ti < 0) return nullptr;
+  return V.d_maps + ((size_t)ti * 3 + 2) * V.geom.bl.size();
 }
 
 // FP32 iterate at level g?  Mixed solves run every level but the coarsest in
@@ -336,7 +345,7 @@ struct Exec {
       float* src = V.phi32[V.cur32];
       float* dst = V.phi32[1 - V.cur32];
       CU(launch_rbgs<float>(V.variant, h->var, V.zero32, V.d_bl, V.d_tiles, V.ntiles, V.zc, sweep_maps(V, V.cur32),
-                            h->d_err, src, dst, V.rhs32,
+                            rhs_maps(V), h->d_err, src, dst, V.rhs32,
                             V.fx32, V.fy32, V.fz32, st));
       TRY(chk("sweep fp32", g));
       if (e1) CU(record(e1));
@@ -348,7 +357,7 @@ struct Exec {
       double* src = V.phi64[V.cur64];
       double* dst = V.phi64[1 - V.cur64];
       CU(launch_rbgs<double>(V.variant, h->var, V.zero64, V.d_bl, V.d_tiles, V.ntiles, V.zc, sweep_maps(V, V.cur64),
-                             h->d_err, src, dst, V.rhs64,
+                             rhs_maps(V), h->d_err, src, dst, V.rhs64,
                              V.fx64, V.fy64, V.fz64, st));
       TRY(chk("sweep fp64", g));
       if (e1) CU(record(e1));
@@ -683,18 +692,21 @@ int build_tensor_maps(h3d_mg* h, int g) {
   auto enc = encode_fn();
   if (!enc) return H3D_OK;
   const size_t nb = V.geom.bl.size();
-  std::vector<CUtensorMap> maps((size_t)kNumTmaTy * 2 * nb);
-  const int tys[kNumTmaTy] = {4, 8, 16};
+  std::vector<CUtensorMap> maps((size_t)kNumTmaTy * 3 * nb);
+  const int tys[kNumTmaTy] = {4, 8, 16, 32};
   for (int ti = 0; ti < kNumTmaTy; ++ti)
-    for (int buf = 0; buf < 2; ++buf)
+    for (int buf = 0; buf < 3; ++buf)
       for (size_t b = 0; b < nb; ++b) {
         const BlkLev& B = V.geom.bl[b];
-        void* base = f32 ? (void*)(V.phi32[buf] + B.off) : (void*)(V.phi64[buf] + B.off);
+        void* base = buf == 2 ? (f32 ? (void*)(V.rhs32 + B.off) : (void*)(V.rhs64 + B.off))
+                              : (f32 ? (void*)(V.phi32[buf] + B.off) : (void*)(V.phi64[buf] + B.off));
         cuuint64_t dims[3] = {(cuuint64_t)B.nx + 2, (cuuint64_t)B.ny + 2, (cuuint64_t)B.nz + 2};
         cuuint64_t strides[2] = {(cuuint64_t)B.sx * es, (cuuint64_t)B.sxy * es};
-        cuuint32_t box[3] = {(cuuint32_t)((B.nx + 2 + vec - 1) / vec * vec), (cuuint32_t)(tys[ti] + 4), 1};
+        // iterate: rows y0-2 .. y0+TY+1; right-hand side: rows y0-1 .. y0+TY
+        cuuint32_t box[3] = {(cuuint32_t)((B.nx + 2 + vec - 1) / vec * vec),
+                             (cuuint32_t)(tys[ti] + (buf == 2 ? 2 : 4)), 1};
         cuuint32_t estr[3] = {1, 1, 1};
-        CUresult r = enc(&maps[((size_t)ti * 2 + buf) * nb + b], f32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32
+        CUresult r = enc(&maps[((size_t)ti * 3 + buf) * nb + b], f32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32
                                                                      : CU_TENSOR_MAP_DATA_TYPE_FLOAT64,
                          3, base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                          CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
@@ -738,10 +750,10 @@ int autotune_level(h3d_mg* h, int g) {
       for (int rep = 0; rep < 4; ++rep) {
         CU(cudaEventRecord(a, h->st));
         if (f32) CU(launch_rbgs<float>(v, h->var, false, V.d_bl, V.d_tiles, V.ntiles, zc, sweep_maps(V, V.cur32),
-                                       h->d_err, V.phi32[V.cur32],
+                                       rhs_maps(V), h->d_err, V.phi32[V.cur32],
                                        V.phi32[1 - V.cur32], V.rhs32, V.fx32, V.fy32, V.fz32, h->st));
         else CU(launch_rbgs<double>(v, h->var, false, V.d_bl, V.d_tiles, V.ntiles, zc, sweep_maps(V, V.cur64),
-                                    h->d_err, V.phi64[V.cur64],
+                                    rhs_maps(V), h->d_err, V.phi64[V.cur64],
                                     V.phi64[1 - V.cur64], V.rhs64, V.fx64, V.fy64, V.fz64, h->st));
         CU(cudaEventRecord(b, h->st));
         CU(cudaEventSynchronize(b));
