@@ -30,11 +30,12 @@ LevelGeom make_level_geom(const std::vector<h3d_block_desc>& blocks, int g, bool
     b.nx = d.n[0] >> (gl - 1);
     b.ny = d.n[1] >> (gl - 1);
     b.nz = d.n[2] >> (gl - 1);
-    // padded layout: rows start on 16-byte boundaries (TMA global strides) and
-    // blocks on 256-byte boundaries; the canonical layout is dense.
-    b.sx = pad ? ((b.nx + 2 + kRowAlign - 1) / kRowAlign) * kRowAlign : b.nx + 2;
+    // padded layout: row pitch a multiple of 16 bytes (TMA global strides),
+    // x = 1 of every row on a 16-byte boundary (block base = 256-byte boundary
+    // + kXOff); the canonical layout is dense.
+    b.sx = pad ? ((b.nx + 2 + kXOff + kRowAlign - 1) / kRowAlign) * kRowAlign : b.nx + 2;
     b.sxy = (long long)b.sx * (b.ny + 2);
-    if (pad) off = (off + kBlockAlign - 1) / kBlockAlign * kBlockAlign;
+    if (pad) off = (off + kBlockAlign - 1) / kBlockAlign * kBlockAlign + kXOff;
     b.off = off;
     b.phys = 0;
     for (int f = 0; f < 6; ++f)

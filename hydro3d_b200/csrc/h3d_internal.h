@@ -14,6 +14,10 @@ constexpr uint32_t kOldFlag = 0x80000000u;  // halo entry reads the pre-fill val
 constexpr uint32_t kIdxMask = 0x7fffffffu;
 constexpr int kRowAlign = 4;     // row pitch multiple (elements): 16 B for FP32, 32 B for FP64
 constexpr int kBlockAlign = 64;  // block base multiple (elements)
+// Padded device layout: x = 0 of every row sits kXOff elements after a 16-byte
+// boundary, so the first interior cell x = 1 starts on one (vector loads and
+// stores of 4 FP32 / 2 FP64 cells).  TMA boxes start at that boundary (x = -3).
+constexpr int kXOff = 3;
 
 // Per-(block, level) geometry as the kernels see it.  Cell (x,y,z), 0-based
 // with the ghost layer at 0 and n+1, lives at off + z*sxy + y*sx + x.

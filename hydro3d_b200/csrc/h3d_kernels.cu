@@ -355,16 +355,8 @@ __global__ void __launch_bounds__(TPR*(TY + 2)) k_rbgs_rows(const BlkLev* __rest
 
 
 // ---------------------------------------------------------------------------
-// TMA-staged row-tile sweep (the production smoother on sm_100a).
-//
-// Same cell mapping and arithmetic as k_rbgs_rows, but the z planes are
-// brought into shared memory by the Tensor Memory Accelerator: one elected
-// thread issues a 3-D bulk tensor copy (box = whole padded row width x TY+4
-// rows x 1 plane, rows outside the block read as zero) into a ring of five
-// plane slots, two planes ahead of the computation, each slot completing on
-// its own mbarrier.  Every wait is bounded; a wait that gives up sets *err
-// and the sweep finishes without hanging (the host reports a timeout).
-// No multicast is used.
+// Helpers of the TMA-staged sweeps: shared-memory addresses and bounded
+// mbarrier waits.  No multicast is used anywhere.
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
@@ -392,152 +384,30 @@ __device__ __forceinline__ void mbar_wait(uint32_t bar, uint32_t parity, int* er
   }
 }
 
-template <typename T, int TPR, int CP, int TY, bool VAR>
-__global__ void __launch_bounds__(TPR*(TY + 2)) k_rbgs_tma(const BlkLev* __restrict__ bls,
-                                                          const Tile* __restrict__ tiles, int zc,
-                                                          const CUtensorMap* __restrict__ maps,
-                                                          T* __restrict__ dst, const T* __restrict__ rhs,
-                                                          const T* __restrict__ fx, const T* __restrict__ fy,
-                                                          const T* __restrict__ fz, int* err) {
-  constexpr int NS = 5;
-  constexpr int VEC = 16 / (int)sizeof(T);
-  constexpr int SPMAX = ((2 * CP * TPR + 2 + VEC - 1) / VEC) * VEC;
-  constexpr int SLOT = ((SPMAX * (TY + 4) * (int)sizeof(T) + 127) / 128) * 128;
-  extern __shared__ unsigned char smem_raw[];
-  unsigned char* base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
-  uint64_t* bars = reinterpret_cast<uint64_t*>(base + NS * SLOT);
-
-  const Tile t = tiles[blockIdx.x];
-  const BlkLev B = bls[t.b];
-  const CUtensorMap* map = maps + t.b;
-  const int nx = B.nx, ny = B.ny, nz = B.nz;
-  const int sx = B.sx;
-  const long long sxy = B.sxy;
-  T* __restrict__ D = dst + B.off;
-  const T* __restrict__ R = rhs + B.off;
-  const T* FX = VAR ? fx + B.off : nullptr;
-  const T* FY = VAR ? fy + B.off : nullptr;
-  const T* FZ = VAR ? fz + B.off : nullptr;
-  const int y0 = t.y0, zs = t.z0;
-  const int ze = min(zs + zc - 1, nz);
-  const int zlo = max(zs - 1, 1), zhi = min(ze + 1, nz);
-  const int BX = ((nx + 2 + VEC - 1) / VEC) * VEC;  // smem row pitch == TMA box width
-  const uint32_t box_bytes = (uint32_t)(BX * (TY + 4) * (int)sizeof(T));
-  const int tr = threadIdx.x / TPR, tc = threadIdx.x - (threadIdx.x / TPR) * TPR;
-  const int y = y0 - 1 + tr;
-  const int srow = (tr + 1) * BX;
-  const bool row_in = y >= 1 && y <= ny;
-  const bool row_own = tr >= 1 && tr <= TY && y <= ny;
-  const int ph = B.phys;
-  const T ax = (T)B.ax, ay = (T)B.ay, az = (T)B.az;
-  const T as_c = (y == 1 && (ph & 4)) ? T(0) : ay;
-  const T an_c = (y == ny && (ph & 8)) ? T(0) : ay;
-  const bool leader = threadIdx.x == 0;
-  bool bad = false;
-
-  if (leader) {
-    for (int q = 0; q < NS; ++q)
-      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(bars + q)) : "memory");
-    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
-  }
-  __syncthreads();
-
-  auto slot = [&](int z) -> T* { return reinterpret_cast<T*>(base + (z % NS) * SLOT); };
-  auto issue = [&](int z) {  // leader only
-    const uint32_t bar = smem_u32(bars + (z % NS));
-    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(box_bytes) : "memory");
-    asm volatile(
-        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];\n" ::
-            "r"(smem_u32(slot(z))),
-        "l"(reinterpret_cast<uint64_t>(map)), "r"(0), "r"(y0 - 2), "r"(z), "r"(bar)
-        : "memory");
-  };
-  auto wait_plane = [&](int z) {
-    const uint32_t parity = (uint32_t)(((z - zlo + 1) / NS) & 1);
-    mbar_wait(smem_u32(bars + (z % NS)), parity, err, bad);
-  };
-  RowGs<T, CP, VAR> gs;
-  gs.init(B, y, tc, TPR);
-  auto red = [&](int z) {
-    if (!row_in) return;
-    T* P = slot(z);
-    const T* Pm = slot(z - 1);
-    const T* Pp = slot(z + 1);
-    const int io = y * sx;
-    const T* Rrow = R + (long long)z * sxy + io;
-    const int j = (y + z) & 1;
-    const long long zo = (long long)z * sxy + io;
-#pragma unroll
-    for (int k = 0; k < CP; ++k) {
-      const int x = 2 * (tc + k * TPR) + 1 + j;
-      if (x <= nx && H3D_IN(40, t.b, zo + x, sxy * (nz + 2)) && H3D_IN(42, t.b, srow + x - BX, SLOT / (int)sizeof(T) - 2 * BX))
-        P[srow + x] = gs.update(P, Pm, Pp, srow + x, BX, k, j, z, Rrow[x], FX, FY, FZ, zo + x, sx, sxy);
-    }
-  };
-  auto black_store = [&](int z) {
-    if (!row_own) return;
-    T* P = slot(z);
-    const T* Pm = slot(z - 1);
-    const T* Pp = slot(z + 1);
-    const int io = y * sx;
-    const T* Rrow = R + (long long)z * sxy + io;
-    T* Drow = D + (long long)z * sxy + io;
-    const int jb = (y + z + 1) & 1;
-#pragma unroll
-    for (int k = 0; k < CP; ++k) {
-      const int xp = 2 * (tc + k * TPR) + 1;
-      if (xp > nx) continue;
-      const int xb = xp + jb, xr = xp + 1 - jb;
-      if (!H3D_IN(41, t.b, (long long)z * sxy + io + xb, sxy * (nz + 2)) ||
-          !H3D_IN(43, t.b, srow + xb - BX, SLOT / (int)sizeof(T) - 2 * BX))
-        continue;
-      const T vr = P[srow + xr];
-      const T vb = gs.update(P, Pm, Pp, srow + xb, BX, k, jb, z, Rrow[xb], FX, FY, FZ, (long long)z * sxy + io + xb, sx,
-                             sxy);
-      Drow[xr] = vr;
-      Drow[xb] = vb;
-    }
-  };
-
-  if (leader) {
-    issue(zlo - 1);
-    issue(zlo);
-    issue(zlo + 1);
-  }
-  wait_plane(zlo - 1);
-  wait_plane(zlo);
-  for (int z = zlo; z <= zhi; ++z) {
-    if (leader && z + 2 <= zhi + 1) issue(z + 2);
-    wait_plane(z + 1);
-    red(z);
-    __syncthreads();
-    if (z - 1 >= zs && z - 1 <= ze) black_store(z - 1);
-    __syncthreads();
-  }
-  if (ze == nz) black_store(nz);
-}
-
 // ---------------------------------------------------------------------------
 // Single-barrier TMA sweep (k_rbgs_tma2).
 //
-// Same cell mapping, arithmetic and out-of-place contract as k_rbgs_tma, with
-// two changes that take the latency of global loads off the z march:
-//  * the right-hand side of rows y0-1 .. y0+TY of each plane comes in by TMA
-//    too (its own tensor map, box TY+2 rows), in the same ring slot and on
-//    the same mbarrier as the iterate's plane;
+// Same cell mapping, arithmetic and out-of-place contract as k_rbgs_rows, but
+// the global loads are off the z march:
+//  * one elected thread brings each plane in by the Tensor Memory Accelerator:
+//    a 3-D bulk tensor copy of the iterate (box = whole padded row width x
+//    TY+4 rows from y0-2, rows outside the block read as zero) and one of the
+//    right-hand side (rows y0-1 .. y0+TY) into a ring slot, both completing
+//    on the slot's mbarrier, D planes ahead of the computation;
 //  * the black update trails the red update by two planes, so one barrier
 //    per plane suffices: phase z updates red cells of plane z (reading planes
 //    z-1..z+1, writing plane z in shared memory) and black cells of plane
 //    z-2 (reading only the red-updated planes z-3..z-1, writing global
 //    memory).  The two never touch the same plane.
+// Every wait is bounded; a wait that gives up sets *err and the sweep
+// finishes without hanging (the host reports a timeout).
 // A plane p is last read in phase p+3, so a ring of D+4 slots lets the copy
 // of plane z+D+1 be issued right after the barrier that ends phase z.
 template <typename T, int TPR, int CP, int TY, int D>
 struct Tma2Cfg {
   static constexpr int NS = D + 4;
   static constexpr int VEC = 16 / (int)sizeof(T);
-  static constexpr int SPMAX = ((2 * CP * TPR + 2 + VEC - 1) / VEC) * VEC;
+  static constexpr int SPMAX = ((2 * CP * TPR + 2 + kXOff + VEC - 1) / VEC) * VEC;
   static constexpr int PSLOT = ((SPMAX * (TY + 4) * (int)sizeof(T) + 127) / 128) * 128;
   static constexpr int RSLOT = ((SPMAX * (TY + 2) * (int)sizeof(T) + 127) / 128) * 128;
   static constexpr int SLOT = PSLOT + RSLOT;
@@ -572,12 +442,12 @@ __global__ void __launch_bounds__(TPR*(TY + 2)) k_rbgs_tma2(const BlkLev* __rest
   const int y0 = t.y0, zs = t.z0;
   const int ze = min(zs + zc - 1, nz);
   const int zlo = max(zs - 1, 1), zhi = min(ze + 1, nz);
-  const int BX = ((nx + 2 + C::VEC - 1) / C::VEC) * C::VEC;  // smem row pitch == TMA box width
+  const int BX = ((nx + 2 + kXOff + C::VEC - 1) / C::VEC) * C::VEC;  // smem row pitch == TMA box width
   const uint32_t tx_bytes = (uint32_t)(BX * (2 * TY + 6) * (int)sizeof(T));
   const int tr = threadIdx.x / TPR, tc = threadIdx.x - (threadIdx.x / TPR) * TPR;
   const int y = y0 - 1 + tr;
-  const int prow = (tr + 1) * BX;  // row y in an iterate slot (slot row 0 = y0-2)
-  const int rrow = tr * BX;        // row y in a right-hand-side slot (slot row 0 = y0-1)
+  const int prow = (tr + 1) * BX + kXOff;  // cell (x, y) of an iterate slot (slot row 0 = y0-2)
+  const int rrow = tr * BX + kXOff;        // cell (x, y) of a right-hand-side slot (slot row 0 = y0-1)
   const bool row_in = y >= 1 && y <= ny;
   const bool row_own = tr >= 1 && tr <= TY && y <= ny;
   const bool leader = threadIdx.x == 0;
@@ -666,13 +536,160 @@ __global__ void __launch_bounds__(TPR*(TY + 2)) k_rbgs_tma2(const BlkLev* __rest
   }
 }
 
-template <typename T, int TPR, int CP, int TY>
-constexpr size_t tma_smem() {
-  constexpr int VEC = 16 / (int)sizeof(T);
-  constexpr int SPMAX = ((2 * CP * TPR + 2 + VEC - 1) / VEC) * VEC;
-  constexpr int SLOT = ((SPMAX * (TY + 4) * (int)sizeof(T) + 127) / 128) * 128;
-  return (size_t)5 * SLOT + 128 + 5 * 8;
+// ---------------------------------------------------------------------------
+// Vectorised single-barrier TMA sweep (k_rbgs_vec), FP32 with constant
+// coefficients: the production smoother of the mixed solver's FP32 levels.
+//
+// Same phases as k_rbgs_tma2 (red of plane z and black of plane z-2 between
+// two barriers, iterate and right-hand side staged by TMA), but a thread owns
+// a group of four consecutive cells x0 .. x0+3 (x0 = 1 + 4j) of one row, two
+// of each colour, and moves it with 16-byte shared-memory loads and stores;
+// the black phase writes the finished group to global memory as one 16-byte
+// store (x0 is 16-byte aligned in the padded layout).  The ring has eight
+// slots, so slot indices are masks.  Needs nx a multiple of 4 and nx <= 4*TPR.
+template <int TPR, int TY, int D>
+struct VecCfg {
+  static constexpr int NS = 8;
+  static constexpr int SPMAX = 4 * TPR + 8;  // >= roundup(nx + 2 + kXOff, 4)
+  static constexpr int PSLOT = ((SPMAX * (TY + 4) * 4 + 127) / 128) * 128;
+  static constexpr int RSLOT = ((SPMAX * (TY + 2) * 4 + 127) / 128) * 128;
+  static constexpr int SLOT = PSLOT + RSLOT;
+  static constexpr size_t SMEM = (size_t)NS * SLOT + 128 + NS * 8;
+  static_assert(D + 4 <= NS, "a plane is read until three phases after its own");
+  static_assert(SMEM <= 232448, "ring exceeds shared memory");
+};
+
+template <int TPR, int TY, int D>
+__global__ void __launch_bounds__(TPR*(TY + 2)) k_rbgs_vec(const BlkLev* __restrict__ bls,
+                                                          const Tile* __restrict__ tiles, int zc,
+                                                          const CUtensorMap* __restrict__ maps,
+                                                          const CUtensorMap* __restrict__ rmaps,
+                                                          float* __restrict__ dst, int* err) {
+  using C = VecCfg<TPR, TY, D>;
+  constexpr int NS = C::NS;
+  extern __shared__ unsigned char smem_raw[];
+  unsigned char* base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
+  uint64_t* bars = reinterpret_cast<uint64_t*>(base + NS * C::SLOT);
+
+  const Tile t = tiles[blockIdx.x];
+  const BlkLev B = bls[t.b];
+  const CUtensorMap* map = maps + t.b;
+  const CUtensorMap* rmap = rmaps + t.b;
+  const int nx = B.nx, ny = B.ny, nz = B.nz;
+  const long long sx = B.sx, sxy = B.sxy;
+  float* __restrict__ Dst = dst + B.off;
+  const int y0 = t.y0, zs = t.z0;
+  const int ze = min(zs + zc - 1, nz);
+  const int zlo = max(zs - 1, 1), zhi = min(ze + 1, nz);
+  const int BX = (nx + 2 + kXOff + 3) & ~3;  // smem row pitch == TMA box width
+  const uint32_t tx_bytes = (uint32_t)(BX * (2 * TY + 6) * 4);
+  const int tr = threadIdx.x / TPR, j = threadIdx.x % TPR;
+  const int y = y0 - 1 + tr;
+  const int x0 = 1 + 4 * j;
+  const bool row_in = x0 <= nx && y >= 1 && y <= ny;
+  const bool row_own = row_in && tr >= 1 && tr <= TY;
+  const int pc = (tr + 1) * BX + kXOff + x0;  // cell x0 of row y in an iterate slot (16-byte aligned)
+  const int rc = tr * BX + kXOff + x0;        // cell x0 of row y in a right-hand-side slot
+  const bool leader = threadIdx.x == 0;
+  bool bad = false;
+
+  // constant coefficients (mgsolver.for:186-205): walls zero the face term
+  const int ph = B.phys;
+  const float ax = (float)B.ax, ay = (float)B.ay, az = (float)B.az;
+  const float as = (y == 1 && (ph & 4)) ? 0.f : ay;
+  const float an = (y == ny && (ph & 8)) ? 0.f : ay;
+  float aw[4], ae[4], inv[4];
+#pragma unroll
+  for (int p = 0; p < 4; ++p) {
+    const int x = x0 + p;
+    aw[p] = (x == 1 && (ph & 1)) ? 0.f : ax;
+    ae[p] = (x == nx && (ph & 2)) ? 0.f : ax;
+    inv[p] = 1.f / (-(aw[p] + ae[p] + as + an + az + az));
+  }
+
+  if (leader) {
+    for (int q = 0; q < NS; ++q)
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(bars + q)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  __syncthreads();
+
+  auto pslot = [&](int z) -> float* { return reinterpret_cast<float*>(base + (z & (NS - 1)) * C::SLOT); };
+  auto rslot = [&](int z) -> const float* {
+    return reinterpret_cast<const float*>(base + (z & (NS - 1)) * C::SLOT + C::PSLOT);
+  };
+  auto issue = [&](int z) {  // leader only
+    const uint32_t bar = smem_u32(bars + (z & (NS - 1)));
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(tx_bytes) : "memory");
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];\n" ::
+            "r"(smem_u32(pslot(z))),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(0), "r"(y0 - 2), "r"(z), "r"(bar)
+        : "memory");
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];\n" ::
+            "r"(smem_u32(rslot(z))),
+        "l"(reinterpret_cast<uint64_t>(rmap)), "r"(0), "r"(y0 - 1), "r"(z), "r"(bar)
+        : "memory");
+  };
+  auto wait_plane = [&](int z) {
+    const uint32_t parity = (uint32_t)(((z - zlo + 1) / NS) & 1);
+    mbar_wait(smem_u32(bars + (z & (NS - 1))), parity, err, bad);
+  };
+  // New values of the cells of colour q (positions q and q+2) of the group in
+  // plane slot P, with the planes below/above in Pm/Pp; c returns the group.
+  auto group = [&](const float* P, const float* Pm, const float* Pp, const float* Rr, int z, int q, float4& c) {
+    c = *reinterpret_cast<const float4*>(P + pc);
+    const float4 u = *reinterpret_cast<const float4*>(P + pc - BX);
+    const float4 dn = *reinterpret_cast<const float4*>(P + pc + BX);
+    const float4 bz = *reinterpret_cast<const float4*>(Pm + pc);
+    const float4 tz = *reinterpret_cast<const float4*>(Pp + pc);
+    const float4 rh = *reinterpret_cast<const float4*>(Rr + rc);
+    const bool wlo = z == 1 && (ph & 16), whi = z == nz && (ph & 32);
+    const float ab = wlo ? 0.f : az, at = whi ? 0.f : az;
+    const bool edge = wlo || whi;
+    auto upd = [&](float w, float e, float s, float n, float b, float tt, float rv, int p) -> float {
+      const float sum = fmaf(at, tt, fmaf(ab, b, fmaf(an, n, fmaf(as, s, fmaf(ae[p], e, aw[p] * w)))));
+      const float iv = edge ? 1.f / (-(aw[p] + ae[p] + as + an + ab + at)) : inv[p];
+      return (rv - sum) * iv;
+    };
+    if (q == 0) {
+      const float l = P[pc - 1];
+      c.x = upd(l, c.y, u.x, dn.x, bz.x, tz.x, rh.x, 0);
+      c.z = upd(c.y, c.w, u.z, dn.z, bz.z, tz.z, rh.z, 2);
+    } else {
+      const float r = P[pc + 4];
+      c.y = upd(c.x, c.z, u.y, dn.y, bz.y, tz.y, rh.y, 1);
+      c.w = upd(c.z, r, u.w, dn.w, bz.w, tz.w, rh.w, 3);
+    }
+  };
+
+  if (leader)
+    for (int q = zlo - 1; q <= min(zlo + D, zhi + 1); ++q) issue(q);
+  wait_plane(zlo - 1);
+  wait_plane(zlo);
+  for (int z = zlo; z <= ze + 2; ++z) {
+    if (z <= zhi) {
+      wait_plane(z + 1);
+      if (row_in) {  // red cells (x + y + z odd) of plane z
+        float* P = pslot(z);
+        float4 c;
+        group(P, pslot(z - 1), pslot(z + 1), rslot(z), z, (y + z) & 1, c);
+        *reinterpret_cast<float4*>(P + pc) = c;
+      }
+    }
+    const int zb = z - 2;
+    if (zb >= zs && zb <= ze && row_own) {  // black cells of plane z-2, then the whole group out
+      float4 c;
+      group(pslot(zb), pslot(zb - 1), pslot(zb + 1), rslot(zb), zb, (y + zb + 1) & 1, c);
+      *reinterpret_cast<float4*>(Dst + (long long)zb * sxy + (long long)y * sx + x0) = c;
+    }
+    __syncthreads();
+    if (leader && z + D + 1 <= zhi + 1) issue(z + D + 1);
+  }
 }
+
 
 // ---------------------------------------------------------------------------
 template <typename T, bool ZERO_OLD>
@@ -1146,16 +1163,17 @@ static const TileShape kShapes[] = {
     {256, 8, 640, true, 64, 2, 0, -1}, {128, 4, 384, true, 64, 1, 0, -1},   // 14, 15
     {256, 4, 768, true, 128, 1, 0, -1}, {128, 4, 192, true, 32, 2, 0, -1},  // 16, 17
     {256, 8, 320, true, 32, 4, 0, -1},                                          // 18
-    {128, 8, 640, true, 64, 1, 1, 8},   {128, 8, 320, true, 32, 2, 1, 9},     // 19, 20
-    {64, 8, 320, true, 32, 1, 1, 10},   {64, 16, 576, true, 32, 1, 1, 11},    // 21, 22
-    {32, 16, 288, true, 16, 1, 1, 12},  {16, 16, 144, true, 8, 1, 1, 13},     // 23, 24
-    {128, 4, 384, true, 64, 1, 1, 15},  {128, 4, 192, true, 32, 2, 1, 17},          // 25, 26
-    {128, 4, 192, true, 32, 2, 2, 17},  {128, 8, 320, true, 32, 2, 2, 9},           // 27, 28
-    {128, 4, 384, true, 64, 1, 2, 15},  {128, 8, 640, true, 64, 1, 2, 8},           // 29, 30
-    {64, 8, 320, true, 32, 1, 2, 10},   {64, 16, 576, true, 32, 1, 2, 11},          // 31, 32
-    {32, 16, 288, true, 16, 1, 2, 12},  {128, 16, 576, true, 32, 2, 2, 37},         // 33, 34
-    {128, 8, 320, true, 32, 2, 2, 9},   {16, 16, 144, true, 8, 1, 2, 13},           // 35, 36
-    {128, 16, 576, true, 32, 2, 0, -1},                                             // 37
+    {128, 4, 192, true, 32, 2, 2, 17},  {128, 8, 320, true, 32, 2, 2, 9},           // 19, 20
+    {128, 4, 384, true, 64, 1, 2, 15},  {128, 8, 640, true, 64, 1, 2, 8},           // 21, 22
+    {64, 8, 320, true, 32, 1, 2, 10},   {64, 16, 576, true, 32, 1, 2, 11},          // 23, 24
+    {32, 16, 288, true, 16, 1, 2, 12},  {128, 16, 576, true, 32, 2, 2, 29},         // 25, 26
+    {128, 8, 320, true, 32, 2, 2, 9},   {16, 16, 144, true, 8, 1, 2, 13},           // 27, 28
+    {128, 16, 576, true, 32, 2, 0, -1},                                             // 29
+    // vectorised FP32 sweeps (k_rbgs_vec); tpr = groups of four cells per row
+    {128, 4, 192, true, 32, 1, 3, 17},  {128, 8, 320, true, 32, 1, 3, 9},           // 30, 31
+    {128, 16, 576, true, 32, 1, 3, 29}, {64, 8, 160, true, 16, 1, 3, 10},           // 32, 33
+    {64, 16, 288, true, 16, 1, 3, 11},  {32, 16, 144, true, 8, 1, 3, 12},           // 34, 35
+    {16, 16, 72, true, 4, 1, 3, 13},    {128, 8, 320, true, 32, 1, 3, 9},           // 36, 37
 };
 #ifdef H3D_BOUNDS_CHECK
 // Debug builds only: first recorded out-of-bounds access {kernel id + 1, block, index, limit}.
@@ -1217,25 +1235,6 @@ static cudaError_t rows_dispatch(bool var, bool zero, const BlkLev* bl, const Ti
   return cudaGetLastError();
 }
 
-template <typename T, int TPR, int CP, int TY>
-static cudaError_t tma_attr() {
-  const int sm = (int)tma_smem<T, TPR, CP, TY>();
-  cudaError_t e;
-  if ((e = cudaFuncSetAttribute(k_rbgs_tma<T, TPR, CP, TY, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm))) return e;
-  return cudaFuncSetAttribute(k_rbgs_tma<T, TPR, CP, TY, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-}
-
-template <typename T, int TPR, int CP, int TY>
-static cudaError_t tma_dispatch(bool var, const BlkLev* bl, const Tile* tiles, int ntiles, int zc,
-                                const CUtensorMap* maps, int* err, T* dst, const T* rhs, const T* fx, const T* fy,
-                                const T* fz, cudaStream_t st) {
-  if (ntiles <= 0) return cudaSuccess;
-  constexpr int NT = TPR * (TY + 2);
-  constexpr size_t SM = tma_smem<T, TPR, CP, TY>();
-  if (var) k_rbgs_tma<T, TPR, CP, TY, true><<<ntiles, NT, SM, st>>>(bl, tiles, zc, maps, dst, rhs, fx, fy, fz, err);
-  else k_rbgs_tma<T, TPR, CP, TY, false><<<ntiles, NT, SM, st>>>(bl, tiles, zc, maps, dst, rhs, fx, fy, fz, err);
-  return cudaGetLastError();
-}
 
 // Prefetch depth actually used: the requested D, lowered until the ring fits
 // in the 227 KB of shared memory a CTA may have.
@@ -1270,26 +1269,41 @@ static cudaError_t tma2_dispatch(bool var, const BlkLev* bl, const Tile* tiles, 
 
 // (variant, threads per row, pairs per thread, rows, prefetch depth)
 #define H3D_TMA2_SHAPES(X) \
-  X(27, 32, 2, 4, 3)       \
-  X(28, 32, 2, 8, 3)       \
-  X(29, 64, 1, 4, 3)       \
-  X(30, 64, 1, 8, 3)       \
-  X(31, 32, 1, 8, 3)       \
-  X(32, 32, 1, 16, 2)      \
-  X(33, 16, 1, 16, 2)      \
-  X(34, 32, 2, 16, 2)      \
-  X(35, 32, 2, 8, 2)       \
-  X(36, 8, 1, 16, 2)
+  X(19, 32, 2, 4, 3)       \
+  X(20, 32, 2, 8, 3)       \
+  X(21, 64, 1, 4, 3)       \
+  X(22, 64, 1, 8, 3)       \
+  X(23, 32, 1, 8, 3)       \
+  X(24, 32, 1, 16, 2)      \
+  X(25, 16, 1, 16, 2)      \
+  X(26, 32, 2, 16, 2)      \
+  X(27, 32, 2, 8, 2)       \
+  X(28, 8, 1, 16, 2)
 
-#define H3D_TMA_SHAPES(X) \
-  X(19, 64, 1, 8)         \
-  X(20, 32, 2, 8)         \
-  X(21, 32, 1, 8)         \
-  X(22, 32, 1, 16)        \
-  X(23, 16, 1, 16)        \
-  X(24, 8, 1, 16)         \
-  X(25, 64, 1, 4)         \
-  X(26, 32, 2, 4)
+template <int TPR, int TY, int D>
+static cudaError_t vec_attr() {
+  return cudaFuncSetAttribute(k_rbgs_vec<TPR, TY, D>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)VecCfg<TPR, TY, D>::SMEM);
+}
+
+template <int TPR, int TY, int D>
+static cudaError_t vec_dispatch(const BlkLev* bl, const Tile* tiles, int ntiles, int zc, const CUtensorMap* maps,
+                                const CUtensorMap* rmaps, int* err, float* dst, cudaStream_t st) {
+  if (ntiles <= 0) return cudaSuccess;
+  k_rbgs_vec<TPR, TY, D><<<ntiles, TPR * (TY + 2), VecCfg<TPR, TY, D>::SMEM, st>>>(bl, tiles, zc, maps, rmaps, dst, err);
+  return cudaGetLastError();
+}
+
+// (variant, groups of four cells per row, rows, prefetch depth)
+#define H3D_VEC_SHAPES(X) \
+  X(30, 32, 4, 4)         \
+  X(31, 32, 8, 4)         \
+  X(32, 32, 16, 4)        \
+  X(33, 16, 8, 4)         \
+  X(34, 16, 16, 4)        \
+  X(35, 8, 16, 4)         \
+  X(36, 4, 16, 4)         \
+  X(37, 32, 8, 2)
 
 #define H3D_ROW_SHAPES(X)  \
   X(8, 64, 1, 8)           \
@@ -1303,7 +1317,7 @@ static cudaError_t tma2_dispatch(bool var, const BlkLev* bl, const Tile* tiles, 
   X(16, 128, 1, 4)         \
   X(17, 32, 2, 4)          \
   X(18, 32, 4, 8)          \
-  X(37, 32, 2, 16)
+  X(29, 32, 2, 16)
 
 cudaError_t init_kernel_attributes() {
   cudaError_t e = cudaSuccess;
@@ -1312,15 +1326,14 @@ cudaError_t init_kernel_attributes() {
   if ((e = rows_attr<double, tpr, cp, ty>()) != cudaSuccess) return e;
   H3D_ROW_SHAPES(X)
 #undef X
-#define X(v, tpr, cp, ty)                                                  \
-  if ((e = tma_attr<float, tpr, cp, ty>()) != cudaSuccess) return e;       \
-  if ((e = tma_attr<double, tpr, cp, ty>()) != cudaSuccess) return e;
-  H3D_TMA_SHAPES(X)
-#undef X
 #define X(v, tpr, cp, ty, d)                                                 \
   if ((e = tma2_attr<float, tpr, cp, ty, d>()) != cudaSuccess) return e;     \
   if ((e = tma2_attr<double, tpr, cp, ty, d>()) != cudaSuccess) return e;
   H3D_TMA2_SHAPES(X)
+#undef X
+#define X(v, tpr, ty, d) \
+  if ((e = vec_attr<tpr, ty, d>()) != cudaSuccess) return e;
+  H3D_VEC_SHAPES(X)
 #undef X
   return e;
 }
@@ -1332,8 +1345,20 @@ cudaError_t launch_rbgs(int variant, bool var, bool zero_src, const BlkLev* bl, 
                         int zc, const CUtensorMap* maps, const CUtensorMap* rmaps, int* err, const T* src, T* dst,
                         const T* rhs, const T* fx, const T* fy, const T* fz, cudaStream_t st) {
   if (variant >= 0 && variant < num_tile_shapes() && kShapes[variant].tma) {
-    // nothing to stage from a zero source: the equivalent plain-load kernel zero-fills
-    if (zero_src || !maps || (kShapes[variant].tma == 2 && !rmaps)) variant = kShapes[variant].alt;
+    // nothing to stage from a zero source: the equivalent plain-load kernel zero-fills;
+    // the vectorised sweep is FP32 with constant coefficients only
+    const int tk = kShapes[variant].tma;
+    if (zero_src || !maps || (tk >= 2 && !rmaps) || (tk == 3 && (var || sizeof(T) != 4)))
+      variant = kShapes[variant].alt;
+  }
+  if constexpr (sizeof(T) == 4) {
+    switch (variant) {
+#define X(v, tpr, ty, d) \
+      case v: return vec_dispatch<tpr, ty, d>(bl, tiles, ntiles, zc, maps, rmaps, err, reinterpret_cast<float*>(dst), st);
+      H3D_VEC_SHAPES(X)
+#undef X
+      default: break;
+    }
   }
   switch (variant) {
     case 0: return rbgs_dispatch<T, 32, 16, 256>(var, zero_src, bl, tiles, ntiles, zc, src, dst, rhs, fx, fy, fz, st);
@@ -1347,10 +1372,6 @@ cudaError_t launch_rbgs(int variant, bool var, bool zero_src, const BlkLev* bl, 
 #define X(v, tpr, cp, ty) \
     case v: return rows_dispatch<T, tpr, cp, ty>(var, zero_src, bl, tiles, ntiles, zc, src, dst, rhs, fx, fy, fz, st);
     H3D_ROW_SHAPES(X)
-#undef X
-#define X(v, tpr, cp, ty) \
-    case v: return tma_dispatch<T, tpr, cp, ty>(var, bl, tiles, ntiles, zc, maps, err, dst, rhs, fx, fy, fz, st);
-    H3D_TMA_SHAPES(X)
 #undef X
 #define X(v, tpr, cp, ty, d) \
     case v: return tma2_dispatch<T, tpr, cp, ty, d>(var, bl, tiles, ntiles, zc, maps, rmaps, err, dst, fx, fy, fz, st);

@@ -30,7 +30,8 @@ struct TileShape {
   int tx, ty, nt;
   bool rows;
   int tpr, cp;
-  int tma;   // 0 plain loads; 1 iterate planes staged by TMA; 2 iterate and right-hand side by TMA
+  int tma;   // 0 plain loads; 1 iterate planes staged by TMA; 2 iterate and right-hand side by TMA;
+             // 3 as 2, vectorised (FP32, constant coefficients, nx a multiple of 4 and <= tx)
   int alt;   // for TMA shapes: the equivalent row shape (used for zero sources)
 };
 // TMA box heights (TY+4) are one of these; tensor maps are built per height.

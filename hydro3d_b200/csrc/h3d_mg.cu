@@ -64,6 +64,7 @@ struct Level {
   Tile* d_rtiles = nullptr;       // restriction tiles (this level as the coarse level)
   int nrtiles = 0, rvariant = 0, rzc = 1;
   bool tma_ok = false;
+  bool f32 = false, var = false;  // iterate precision of the level's smoother; variable coefficients
   int cur64 = 0, cur32 = 0;
   bool zero64 = false, zero32 = false;
   double sweep_bytes = 0;  // algorithmic bytes of one sweep (FP64 or FP32 by mode)
@@ -186,8 +187,9 @@ bool variant_fits(const Level& Lv, int variant) {
   TileShape s = tile_shape(variant);
   if (!s.rows) return true;
   if (s.tma && !Lv.tma_ok) return false;
+  if (s.tma == 3 && (!Lv.f32 || Lv.var)) return false;
   for (const auto& B : Lv.geom.bl)
-    if ((B.nx & 1) || B.nx > s.tx) return false;
+    if ((B.nx & 1) || B.nx > s.tx || (s.tma == 3 && (B.nx & 3))) return false;
   return true;
 }
 
@@ -267,7 +269,7 @@ void default_tile(const Level& Lv, int* variant, int* zc) {
   else if (nxm >= 8) v = nym >= 8 ? 4 : 5;
   else v = 6;
   // whole-row tiles when every block allows them (TMA-staged first)
-  const int pref[] = {36, 33, 32, 28, 24, 23, 21, 20, 13, 12, 10, 8, 14, 16};
+  const int pref[] = {36, 35, 34, 31, 28, 25, 24, 20, 13, 12, 10, 8, 14, 16};
   for (int cand : pref) {
     TileShape c = tile_shape(cand);
     if (nxm <= c.tx && nxm * 2 > c.tx / 2 && variant_fits(Lv, cand) && nym >= 4) { v = cand; break; }
@@ -294,7 +296,7 @@ const CUtensorMap* sweep_maps(const Level& V, int buf) {
 // Tensor maps of the level's right-hand side (box TY+2 rows), or null.
 const CUtensorMap* rhs_maps(const Level& V) {
   TileShape s = tile_shape(V.variant);
-  if (s.tma != 2 || !V.tma_ok) return nullptr;
+  if (s.tma < 2 || !V.tma_ok) return nullptr;
   int ti = tma_ty_index(s.ty);
   if (ti < 0) return nullptr;
   return V.d_maps + ((size_t)ti * 3 + 2) * V.geom.bl.size();
@@ -677,16 +679,17 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
   return fn;
 }
 
-// Tensor maps of both iterate buffers of level g for every TMA box height:
-// dims (nx+2, ny+2, nz+2), strides (sx, sxy) elements, box (BX, TY+4, 1),
-// out-of-bounds rows read as zero.  Levels whose row width exceeds one box
-// (BX > 256) or with an odd nx keep the plain-load smoothers.
+// Tensor maps of both iterate buffers and of the right-hand side of level g
+// for every TMA box height: origin kXOff elements before x = 0, dims
+// (nx+2+kXOff, ny+2, nz+2), strides (sx, sxy) elements, box (BX, TY+4 or
+// TY+2, 1), out-of-bounds rows read as zero.  Levels whose row width exceeds
+// one box (BX > 256) or with an odd nx keep the plain-load smoothers.
 int build_tensor_maps(h3d_mg* h, int g) {
   Level& V = h->lev[g];
   const bool f32 = f32_level(h, g);
   const int es = f32 ? 4 : 8, vec = 16 / es;
   for (const auto& B : V.geom.bl) {
-    int bx = (B.nx + 2 + vec - 1) / vec * vec;
+    int bx = (B.nx + 2 + kXOff + vec - 1) / vec * vec;
     if ((B.nx & 1) || bx > 256) return H3D_OK;
   }
   auto enc = encode_fn();
@@ -698,12 +701,14 @@ int build_tensor_maps(h3d_mg* h, int g) {
     for (int buf = 0; buf < 3; ++buf)
       for (size_t b = 0; b < nb; ++b) {
         const BlkLev& B = V.geom.bl[b];
-        void* base = buf == 2 ? (f32 ? (void*)(V.rhs32 + B.off) : (void*)(V.rhs64 + B.off))
-                              : (f32 ? (void*)(V.phi32[buf] + B.off) : (void*)(V.phi64[buf] + B.off));
-        cuuint64_t dims[3] = {(cuuint64_t)B.nx + 2, (cuuint64_t)B.ny + 2, (cuuint64_t)B.nz + 2};
+        // the box starts kXOff elements before x = 0, on the row's 16-byte boundary
+        const long long o = B.off - kXOff;
+        void* base = buf == 2 ? (f32 ? (void*)(V.rhs32 + o) : (void*)(V.rhs64 + o))
+                              : (f32 ? (void*)(V.phi32[buf] + o) : (void*)(V.phi64[buf] + o));
+        cuuint64_t dims[3] = {(cuuint64_t)B.nx + 2 + kXOff, (cuuint64_t)B.ny + 2, (cuuint64_t)B.nz + 2};
         cuuint64_t strides[2] = {(cuuint64_t)B.sx * es, (cuuint64_t)B.sxy * es};
         // iterate: rows y0-2 .. y0+TY+1; right-hand side: rows y0-1 .. y0+TY
-        cuuint32_t box[3] = {(cuuint32_t)((B.nx + 2 + vec - 1) / vec * vec),
+        cuuint32_t box[3] = {(cuuint32_t)((B.nx + 2 + kXOff + vec - 1) / vec * vec),
                              (cuuint32_t)(tys[ti] + (buf == 2 ? 2 : 4)), 1};
         cuuint32_t estr[3] = {1, 1, 1};
         CUresult r = enc(&maps[((size_t)ti * 3 + buf) * nb + b], f32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32
@@ -756,7 +761,16 @@ int autotune_level(h3d_mg* h, int g) {
                                     rhs_maps(V), h->d_err, V.phi64[V.cur64],
                                     V.phi64[1 - V.cur64], V.rhs64, V.fx64, V.fy64, V.fz64, h->st));
         CU(cudaEventRecord(b, h->st));
-        CU(cudaEventSynchronize(b));
+        {
+          cudaError_t e = cudaEventSynchronize(b);
+          int werr = 0;
+          if (e == cudaSuccess) e = cudaMemcpy(&werr, h->d_err, sizeof(int), cudaMemcpyDeviceToHost);
+          if (e != cudaSuccess || werr)
+            return fail(h, e != cudaSuccess ? H3D_ERR_CUDA : H3D_ERR_TIMEOUT,
+                        "smoother autotuning (level " + std::to_string(g) + ", variant " + std::to_string(v) +
+                            ", z-chunk " + std::to_string(zc) + "): " +
+                            (e != cudaSuccess ? cudaGetErrorString(e) : "a bounded device wait gave up"));
+        }
         float t;
         CU(cudaEventElapsedTime(&t, a, b));
         if (rep > 0) tot += t;
@@ -999,6 +1013,8 @@ int h3d_mg_create(h3d_mg** out, const h3d_mg_desc* desc) {
       if ((rc = build_halo_table(h->blocks, g, kHaloFaces, true, d, s, &err)) != H3D_OK) return bail(fail(h, rc, err));
       if ((rc = upload_halo(h, V.faces, d, s)) != H3D_OK) return bail(rc);
     }
+    V.f32 = f32_level(h, g);
+    V.var = h->var;
     if ((rc = build_tensor_maps(h, g)) != H3D_OK) return bail(rc);
     if (g >= 2 && (rc = build_restrict_tiles(h, V)) != H3D_OK) return bail(rc);
     int var_, zc;
