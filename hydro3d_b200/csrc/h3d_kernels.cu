@@ -365,17 +365,21 @@ __device__ __forceinline__ uint32_t smem_u32(const void* p) {
 // ms; a plane copy takes microseconds), records the failure in *err and makes
 // every later wait of this thread return at once, so a failed copy can never
 // hang the kernel.
+__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
+  uint32_t done;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(done)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+
 __device__ __forceinline__ void mbar_wait(uint32_t bar, uint32_t parity, int* err, bool& bad) {
-  if (bad) return;
+  if (bad || mbar_try(bar, parity)) return;
   const long long t0 = clock64();
   for (;;) {
-    uint32_t done;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(done)
-        : "r"(bar), "r"(parity)
-        : "memory");
-    if (done) return;
+    if (mbar_try(bar, parity)) return;
     if (clock64() - t0 > (1LL << 26)) {
       bad = true;
       atomicExch(err, 1);
@@ -541,32 +545,33 @@ __global__ void __launch_bounds__(TPR*(TY + 2)) k_rbgs_tma2(const BlkLev* __rest
 // coefficients: the production smoother of the mixed solver's FP32 levels.
 //
 // Same phases as k_rbgs_tma2 (red of plane z and black of plane z-2 between
-// two barriers, iterate and right-hand side staged by TMA), but a thread owns
-// a group of four consecutive cells x0 .. x0+3 (x0 = 1 + 4j) of one row, two
-// of each colour, and moves it with 16-byte shared-memory loads and stores;
+// two barriers, iterate and right-hand side staged by TMA into an NS-slot
+// ring D planes ahead), but a thread owns GPT groups of four consecutive
+// cells x0 .. x0+3 (x0 = 1 + 4g, g = j + k*TPR) of one row, two of each
+// colour, and moves each group with 16-byte shared-memory loads and stores;
 // the black phase writes the finished group to global memory as one 16-byte
-// store (x0 is 16-byte aligned in the padded layout).  The ring has eight
-// slots, so slot indices are masks.  Needs nx a multiple of 4 and nx <= 4*TPR.
-template <int TPR, int TY, int D>
+// store (x0 is 16-byte aligned in the padded layout).  Only x0 can be a west
+// wall cell and x0+3 an east wall cell (nx is a multiple of 4), so a group
+// keeps two face coefficients and three diagonal reciprocals in registers.
+// Needs nx a multiple of 4 and nx <= 4*TPR*GPT.
+template <int TPR, int GPT, int TY, int NS, int D>
 struct VecCfg {
-  static constexpr int NS = 8;
-  static constexpr int SPMAX = 4 * TPR + 8;  // >= roundup(nx + 2 + kXOff, 4)
+  static constexpr int SPMAX = 4 * TPR * GPT + 8;  // >= roundup(nx + 2 + kXOff, 4)
   static constexpr int PSLOT = ((SPMAX * (TY + 4) * 4 + 127) / 128) * 128;
   static constexpr int RSLOT = ((SPMAX * (TY + 2) * 4 + 127) / 128) * 128;
   static constexpr int SLOT = PSLOT + RSLOT;
   static constexpr size_t SMEM = (size_t)NS * SLOT + 128 + NS * 8;
-  static_assert(D + 4 <= NS, "a plane is read until three phases after its own");
   static_assert(SMEM <= 232448, "ring exceeds shared memory");
 };
 
-template <int TPR, int TY, int D>
+template <int TPR, int GPT, int TY, int NS, int D>
 __global__ void __launch_bounds__(TPR*(TY + 2)) k_rbgs_vec(const BlkLev* __restrict__ bls,
                                                           const Tile* __restrict__ tiles, int zc,
                                                           const CUtensorMap* __restrict__ maps,
                                                           const CUtensorMap* __restrict__ rmaps,
                                                           float* __restrict__ dst, int* err) {
-  using C = VecCfg<TPR, TY, D>;
-  constexpr int NS = C::NS;
+  using C = VecCfg<TPR, GPT, TY, NS, D>;
+  static_assert(D + 4 <= NS, "a plane is read until three phases after its own");
   extern __shared__ unsigned char smem_raw[];
   unsigned char* base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
   uint64_t* bars = reinterpret_cast<uint64_t*>(base + NS * C::SLOT);
@@ -577,7 +582,6 @@ __global__ void __launch_bounds__(TPR*(TY + 2)) k_rbgs_vec(const BlkLev* __restr
   const CUtensorMap* rmap = rmaps + t.b;
   const int nx = B.nx, ny = B.ny, nz = B.nz;
   const long long sx = B.sx, sxy = B.sxy;
-  float* __restrict__ Dst = dst + B.off;
   const int y0 = t.y0, zs = t.z0;
   const int ze = min(zs + zc - 1, nz);
   const int zlo = max(zs - 1, 1), zhi = min(ze + 1, nz);
@@ -585,11 +589,11 @@ __global__ void __launch_bounds__(TPR*(TY + 2)) k_rbgs_vec(const BlkLev* __restr
   const uint32_t tx_bytes = (uint32_t)(BX * (2 * TY + 6) * 4);
   const int tr = threadIdx.x / TPR, j = threadIdx.x % TPR;
   const int y = y0 - 1 + tr;
-  const int x0 = 1 + 4 * j;
-  const bool row_in = x0 <= nx && y >= 1 && y <= ny;
-  const bool row_own = row_in && tr >= 1 && tr <= TY;
-  const int pc = (tr + 1) * BX + kXOff + x0;  // cell x0 of row y in an iterate slot (16-byte aligned)
-  const int rc = tr * BX + kXOff + x0;        // cell x0 of row y in a right-hand-side slot
+  const bool yin = y >= 1 && y <= ny;
+  const bool yown = yin && tr >= 1 && tr <= TY;
+  const int prow = (tr + 1) * BX + kXOff;  // cell (x, y) of an iterate slot sits at prow + x
+  const int rrow = tr * BX + kXOff;        // ... of a right-hand-side slot at rrow + x
+  float* __restrict__ Drow = dst + B.off + (long long)y * sx;
   const bool leader = threadIdx.x == 0;
   bool bad = false;
 
@@ -598,13 +602,15 @@ __global__ void __launch_bounds__(TPR*(TY + 2)) k_rbgs_vec(const BlkLev* __restr
   const float ax = (float)B.ax, ay = (float)B.ay, az = (float)B.az;
   const float as = (y == 1 && (ph & 4)) ? 0.f : ay;
   const float an = (y == ny && (ph & 8)) ? 0.f : ay;
-  float aw[4], ae[4], inv[4];
+  float aw0[GPT], ae3[GPT], inv0[GPT], inv3[GPT];
+  const float inv12 = 1.f / (-(ax + ax + as + an + az + az));
 #pragma unroll
-  for (int p = 0; p < 4; ++p) {
-    const int x = x0 + p;
-    aw[p] = (x == 1 && (ph & 1)) ? 0.f : ax;
-    ae[p] = (x == nx && (ph & 2)) ? 0.f : ax;
-    inv[p] = 1.f / (-(aw[p] + ae[p] + as + an + az + az));
+  for (int k = 0; k < GPT; ++k) {
+    const int x0 = 1 + 4 * (j + k * TPR);
+    aw0[k] = (x0 == 1 && (ph & 1)) ? 0.f : ax;
+    ae3[k] = (x0 + 3 == nx && (ph & 2)) ? 0.f : ax;
+    inv0[k] = 1.f / (-(aw0[k] + ax + as + an + az + az));
+    inv3[k] = 1.f / (-(ax + ae3[k] + as + an + az + az));
   }
 
   if (leader) {
@@ -614,54 +620,69 @@ __global__ void __launch_bounds__(TPR*(TY + 2)) k_rbgs_vec(const BlkLev* __restr
   }
   __syncthreads();
 
-  auto pslot = [&](int z) -> float* { return reinterpret_cast<float*>(base + (z & (NS - 1)) * C::SLOT); };
-  auto rslot = [&](int z) -> const float* {
-    return reinterpret_cast<const float*>(base + (z & (NS - 1)) * C::SLOT + C::PSLOT);
-  };
+  auto slot_of = [&](int z) { return z % NS; };
+  auto pslot = [&](int s) -> float* { return reinterpret_cast<float*>(base + s * C::SLOT); };
+  auto rslot = [&](int s) -> const float* { return reinterpret_cast<const float*>(base + s * C::SLOT + C::PSLOT); };
   auto issue = [&](int z) {  // leader only
-    const uint32_t bar = smem_u32(bars + (z & (NS - 1)));
+    const int sl = slot_of(z);
+    const uint32_t bar = smem_u32(bars + sl);
     asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(tx_bytes) : "memory");
     asm volatile(
         "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];\n" ::
-            "r"(smem_u32(pslot(z))),
+            "r"(smem_u32(pslot(sl))),
         "l"(reinterpret_cast<uint64_t>(map)), "r"(0), "r"(y0 - 2), "r"(z), "r"(bar)
         : "memory");
     asm volatile(
         "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];\n" ::
-            "r"(smem_u32(rslot(z))),
+            "r"(smem_u32(rslot(sl))),
         "l"(reinterpret_cast<uint64_t>(rmap)), "r"(0), "r"(y0 - 1), "r"(z), "r"(bar)
         : "memory");
   };
   auto wait_plane = [&](int z) {
     const uint32_t parity = (uint32_t)(((z - zlo + 1) / NS) & 1);
-    mbar_wait(smem_u32(bars + (z & (NS - 1))), parity, err, bad);
+    mbar_wait(smem_u32(bars + slot_of(z)), parity, err, bad);
   };
-  // New values of the cells of colour q (positions q and q+2) of the group in
-  // plane slot P, with the planes below/above in Pm/Pp; c returns the group.
-  auto group = [&](const float* P, const float* Pm, const float* Pp, const float* Rr, int z, int q, float4& c) {
-    c = *reinterpret_cast<const float4*>(P + pc);
-    const float4 u = *reinterpret_cast<const float4*>(P + pc - BX);
-    const float4 dn = *reinterpret_cast<const float4*>(P + pc + BX);
-    const float4 bz = *reinterpret_cast<const float4*>(Pm + pc);
-    const float4 tz = *reinterpret_cast<const float4*>(Pp + pc);
-    const float4 rh = *reinterpret_cast<const float4*>(Rr + rc);
+  auto upd = [](float w, float e, float s, float n, float b, float tt, float rv, float aw, float ae, float as_,
+                float an_, float ab, float at, float iv) -> float {
+    const float sum = fmaf(at, tt, fmaf(ab, b, fmaf(an_, n, fmaf(as_, s, fmaf(ae, e, aw * w)))));
+    return (rv - sum) * iv;
+  };
+  // The inputs of one group update: the group, its row neighbours above and
+  // below, the planes below and above, the right-hand side, and the cell left
+  // (colour 0) or right (colour 1) of the group.
+  struct In {
+    float4 c, u, dn, bz, tz, rh;
+    float side;
+  };
+  auto load = [&](In& in, int sp, int sm, int su, int x0, int q) {
+    const float* P = pslot(sp);
+    const int pc = prow + x0;
+    in.c = *reinterpret_cast<const float4*>(P + pc);
+    in.u = *reinterpret_cast<const float4*>(P + pc - BX);
+    in.dn = *reinterpret_cast<const float4*>(P + pc + BX);
+    in.bz = *reinterpret_cast<const float4*>(pslot(sm) + pc);
+    in.tz = *reinterpret_cast<const float4*>(pslot(su) + pc);
+    in.rh = *reinterpret_cast<const float4*>(rslot(sp) + rrow + x0);
+    in.side = q == 0 ? P[pc - 1] : P[pc + 4];
+  };
+  // New values of the cells of colour q (positions q and q+2) of group k.
+  auto compute = [&](In& in, int k, int z, int q) {
     const bool wlo = z == 1 && (ph & 16), whi = z == nz && (ph & 32);
     const float ab = wlo ? 0.f : az, at = whi ? 0.f : az;
-    const bool edge = wlo || whi;
-    auto upd = [&](float w, float e, float s, float n, float b, float tt, float rv, int p) -> float {
-      const float sum = fmaf(at, tt, fmaf(ab, b, fmaf(an, n, fmaf(as, s, fmaf(ae[p], e, aw[p] * w)))));
-      const float iv = edge ? 1.f / (-(aw[p] + ae[p] + as + an + ab + at)) : inv[p];
-      return (rv - sum) * iv;
-    };
+    float i0 = inv0[k], i3 = inv3[k], i12 = inv12;
+    if (wlo || whi) {  // wall plane: the diagonal changes
+      i0 = 1.f / (-(aw0[k] + ax + as + an + ab + at));
+      i3 = 1.f / (-(ax + ae3[k] + as + an + ab + at));
+      i12 = 1.f / (-(ax + ax + as + an + ab + at));
+    }
+    float4& c = in.c;
     if (q == 0) {
-      const float l = P[pc - 1];
-      c.x = upd(l, c.y, u.x, dn.x, bz.x, tz.x, rh.x, 0);
-      c.z = upd(c.y, c.w, u.z, dn.z, bz.z, tz.z, rh.z, 2);
+      c.x = upd(in.side, c.y, in.u.x, in.dn.x, in.bz.x, in.tz.x, in.rh.x, aw0[k], ax, as, an, ab, at, i0);
+      c.z = upd(c.y, c.w, in.u.z, in.dn.z, in.bz.z, in.tz.z, in.rh.z, ax, ax, as, an, ab, at, i12);
     } else {
-      const float r = P[pc + 4];
-      c.y = upd(c.x, c.z, u.y, dn.y, bz.y, tz.y, rh.y, 1);
-      c.w = upd(c.z, r, u.w, dn.w, bz.w, tz.w, rh.w, 3);
+      c.y = upd(c.x, c.z, in.u.y, in.dn.y, in.bz.y, in.tz.y, in.rh.y, ax, ax, as, an, ab, at, i12);
+      c.w = upd(c.z, in.side, in.u.w, in.dn.w, in.bz.w, in.tz.w, in.rh.w, ax, ae3[k], as, an, ab, at, i3);
     }
   };
 
@@ -669,27 +690,33 @@ __global__ void __launch_bounds__(TPR*(TY + 2)) k_rbgs_vec(const BlkLev* __restr
     for (int q = zlo - 1; q <= min(zlo + D, zhi + 1); ++q) issue(q);
   wait_plane(zlo - 1);
   wait_plane(zlo);
+  int s0 = slot_of(zlo);  // slot of plane z
+  auto wrap = [](int i) { return i < 0 ? i + NS : (i >= NS ? i - NS : i); };
   for (int z = zlo; z <= ze + 2; ++z) {
-    if (z <= zhi) {
-      wait_plane(z + 1);
-      if (row_in) {  // red cells (x + y + z odd) of plane z
-        float* P = pslot(z);
-        float4 c;
-        group(P, pslot(z - 1), pslot(z + 1), rslot(z), z, (y + z) & 1, c);
-        *reinterpret_cast<float4*>(P + pc) = c;
-      }
-    }
+    const bool red = z <= zhi && yin;                    // red cells of plane z
     const int zb = z - 2;
-    if (zb >= zs && zb <= ze && row_own) {  // black cells of plane z-2, then the whole group out
-      float4 c;
-      group(pslot(zb), pslot(zb - 1), pslot(zb + 1), rslot(zb), zb, (y + zb + 1) & 1, c);
-      *reinterpret_cast<float4*>(Dst + (long long)zb * sxy + (long long)y * sx + x0) = c;
+    const bool blk = zb >= zs && zb <= ze && yown;      // black cells of plane z-2
+    if (z <= zhi) wait_plane(z + 1);
+    const int qr = (y + z) & 1, qb = (y + zb + 1) & 1;
+    const int sr = s0, sb = wrap(s0 - 2);
+#pragma unroll
+    for (int k = 0; k < GPT; ++k) {
+      const int x0 = 1 + 4 * (j + k * TPR);
+      if (x0 > nx) continue;
+      // every load of the phase first, then the arithmetic, then the stores
+      In ir, ib;
+      if (red) load(ir, sr, wrap(sr - 1), wrap(sr + 1), x0, qr);
+      if (blk) load(ib, sb, wrap(sb - 1), wrap(sb + 1), x0, qb);
+      if (red) compute(ir, k, z, qr);
+      if (blk) compute(ib, k, zb, qb);
+      if (red) *reinterpret_cast<float4*>(pslot(sr) + prow + x0) = ir.c;
+      if (blk) *reinterpret_cast<float4*>(Drow + (long long)zb * sxy + x0) = ib.c;
     }
     __syncthreads();
     if (leader && z + D + 1 <= zhi + 1) issue(z + D + 1);
+    s0 = wrap(s0 + 1);
   }
 }
-
 
 // ---------------------------------------------------------------------------
 template <typename T, bool ZERO_OLD>
@@ -1169,11 +1196,17 @@ static const TileShape kShapes[] = {
     {32, 16, 288, true, 16, 1, 2, 12},  {128, 16, 576, true, 32, 2, 2, 29},         // 25, 26
     {128, 8, 320, true, 32, 2, 2, 9},   {16, 16, 144, true, 8, 1, 2, 13},           // 27, 28
     {128, 16, 576, true, 32, 2, 0, -1},                                             // 29
-    // vectorised FP32 sweeps (k_rbgs_vec); tpr = groups of four cells per row
+    // vectorised FP32 sweeps (k_rbgs_vec); tpr = threads per row, cp = groups of four cells per thread
     {128, 4, 192, true, 32, 1, 3, 17},  {128, 8, 320, true, 32, 1, 3, 9},           // 30, 31
-    {128, 16, 576, true, 32, 1, 3, 29}, {64, 8, 160, true, 16, 1, 3, 10},           // 32, 33
-    {64, 16, 288, true, 16, 1, 3, 11},  {32, 16, 144, true, 8, 1, 3, 12},           // 34, 35
-    {16, 16, 72, true, 4, 1, 3, 13},    {128, 8, 320, true, 32, 1, 3, 9},           // 36, 37
+    {128, 8, 320, true, 32, 1, 3, 9},   {128, 16, 576, true, 32, 1, 3, 29},         // 32, 33
+    {128, 8, 160, true, 16, 2, 3, 9},   {128, 16, 288, true, 16, 2, 3, 29},         // 34, 35
+    {64, 8, 160, true, 16, 1, 3, 10},   {64, 16, 288, true, 16, 1, 3, 11},          // 36, 37
+    {32, 16, 144, true, 8, 1, 3, 12},   {16, 16, 72, true, 4, 1, 3, 13},            // 38, 39
+    // register-window FP32 sweeps (k_rbgs_win); tpr = lanes per row, one group each
+    {128, 4, 192, true, 32, 1, 3, 17},  {128, 8, 320, true, 32, 1, 3, 9},           // 40, 41
+    {128, 16, 576, true, 32, 1, 3, 29}, {128, 8, 320, true, 32, 1, 3, 9},           // 42, 43
+    {64, 8, 160, true, 16, 1, 3, 10},   {64, 16, 288, true, 16, 1, 3, 11},          // 44, 45
+    {32, 16, 144, true, 8, 1, 3, 12},   {16, 16, 72, true, 4, 1, 3, 13},            // 46, 47
 };
 #ifdef H3D_BOUNDS_CHECK
 // Debug builds only: first recorded out-of-bounds access {kernel id + 1, block, index, limit}.
@@ -1280,30 +1313,234 @@ static cudaError_t tma2_dispatch(bool var, const BlkLev* bl, const Tile* tiles, 
   X(27, 32, 2, 8, 2)       \
   X(28, 8, 1, 16, 2)
 
-template <int TPR, int TY, int D>
-static cudaError_t vec_attr() {
-  return cudaFuncSetAttribute(k_rbgs_vec<TPR, TY, D>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)VecCfg<TPR, TY, D>::SMEM);
+// ---------------------------------------------------------------------------
+// Register-window TMA sweep (k_rbgs_win), FP32 with constant coefficients.
+//
+// Same phases, staging and results as k_rbgs_vec (GPT = 1), but a thread keeps
+// its own group of planes z-3 .. z+1 in registers for the whole z march, so a
+// phase reads from shared memory only the group of the new plane z+1, the
+// rows y-1 and y+1 at planes z (red) and z-2 (black) and the right-hand side;
+// the cells left and right of the group come from the neighbouring lanes by
+// warp shuffles (a row is TPR consecutive lanes), the ghost columns from
+// shared memory.  A plane is last read two phases after its own, so the ring
+// needs D+3 slots.
+template <int TPR, int TY, int NS, int D>
+__global__ void __launch_bounds__(TPR*(TY + 2)) k_rbgs_win(const BlkLev* __restrict__ bls,
+                                                          const Tile* __restrict__ tiles, int zc,
+                                                          const CUtensorMap* __restrict__ maps,
+                                                          const CUtensorMap* __restrict__ rmaps,
+                                                          float* __restrict__ dst, int* err) {
+  using C = VecCfg<TPR, 1, TY, NS, D>;
+  static_assert(TPR <= 32 && (TPR & (TPR - 1)) == 0, "a row is a power-of-two lane segment of one warp");
+  extern __shared__ unsigned char smem_raw[];
+  unsigned char* base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
+  uint64_t* bars = reinterpret_cast<uint64_t*>(base + NS * C::SLOT);
+
+  const Tile t = tiles[blockIdx.x];
+  const BlkLev B = bls[t.b];
+  const CUtensorMap* map = maps + t.b;
+  const CUtensorMap* rmap = rmaps + t.b;
+  const int nx = B.nx, ny = B.ny, nz = B.nz;
+  const long long sx = B.sx, sxy = B.sxy;
+  const int y0 = t.y0, zs = t.z0;
+  const int ze = min(zs + zc - 1, nz);
+  const int zlo = max(zs - 1, 1), zhi = min(ze + 1, nz);
+  const int BX = (nx + 2 + kXOff + 3) & ~3;  // smem row pitch == TMA box width
+  const uint32_t tx_bytes = (uint32_t)(BX * (2 * TY + 6) * 4);
+  const int tr = threadIdx.x / TPR, j = threadIdx.x % TPR;
+  const int y = y0 - 1 + tr;
+  const int x0 = 1 + 4 * j;
+  const bool gin = x0 <= nx;
+  const bool yin = gin && y >= 1 && y <= ny;
+  const bool yown = yin && tr >= 1 && tr <= TY;
+  const bool lft = j == 0, rgt = x0 + 3 == nx;  // groups next to the ghost columns
+  const int pc = (tr + 1) * BX + kXOff + x0;    // own group in an iterate slot
+  const int rcol = tr * BX + kXOff + x0;        // own group in a right-hand-side slot
+  float* __restrict__ Drow = dst + B.off + (long long)y * sx + x0;
+  const bool leader = threadIdx.x == 0;
+  bool bad = false;
+
+  // constant coefficients (mgsolver.for:186-205): walls zero the face term
+  const int ph = B.phys;
+  const float ax = (float)B.ax, ay = (float)B.ay, az = (float)B.az;
+  const float as = (y == 1 && (ph & 4)) ? 0.f : ay;
+  const float an = (y == ny && (ph & 8)) ? 0.f : ay;
+  const float aw0 = (x0 == 1 && (ph & 1)) ? 0.f : ax;
+  const float ae3 = (rgt && (ph & 2)) ? 0.f : ax;
+  const float inv0 = 1.f / (-(aw0 + ax + as + an + az + az));
+  const float inv3 = 1.f / (-(ax + ae3 + as + an + az + az));
+  const float inv12 = 1.f / (-(ax + ax + as + an + az + az));
+
+  if (leader) {
+    for (int q = 0; q < NS; ++q)
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(bars + q)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  __syncthreads();
+
+  auto pslot = [&](int s) -> float* { return reinterpret_cast<float*>(base + s * C::SLOT); };
+  auto rslot = [&](int s) -> const float* { return reinterpret_cast<const float*>(base + s * C::SLOT + C::PSLOT); };
+  auto issue = [&](int z) {  // leader only
+    const int sl = z % NS;
+    const uint32_t bar = smem_u32(bars + sl);
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(tx_bytes) : "memory");
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];\n" ::
+            "r"(smem_u32(pslot(sl))),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(0), "r"(y0 - 2), "r"(z), "r"(bar)
+        : "memory");
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];\n" ::
+            "r"(smem_u32(rslot(sl))),
+        "l"(reinterpret_cast<uint64_t>(rmap)), "r"(0), "r"(y0 - 1), "r"(z), "r"(bar)
+        : "memory");
+  };
+  auto wait_plane = [&](int z) {
+    const uint32_t parity = (uint32_t)(((z - zlo + 1) / NS) & 1);
+    mbar_wait(smem_u32(bars + z % NS), parity, err, bad);
+  };
+  auto wrap = [](int i) { return i < 0 ? i + NS : (i >= NS ? i - NS : i); };
+  auto upd = [](float w, float e, float s, float n, float b, float tt, float rv, float aw, float ae, float as_,
+                float an_, float ab, float at, float iv) -> float {
+    const float sum = fmaf(at, tt, fmaf(ab, b, fmaf(an_, n, fmaf(as_, s, fmaf(ae, e, aw * w)))));
+    return (rv - sum) * iv;
+  };
+  // Cells of colour q (positions q, q+2) of the own group c in plane z, with
+  // the group below (bz) and above (tz), rows y-1 (u) and y+1 (dn), rhs rh,
+  // and the cells left (l) and right (r) of the group.
+  auto colour = [&](float4& c, const float4& bz, const float4& tz, const float4& u, const float4& dn,
+                    const float4& rh, float l, float r, int z, int q) {
+    const bool wlo = z == 1 && (ph & 16), whi = z == nz && (ph & 32);
+    const float ab = wlo ? 0.f : az, at = whi ? 0.f : az;
+    float i0 = inv0, i3 = inv3, i12 = inv12;
+    if (wlo || whi) {  // wall plane: the diagonal changes
+      i0 = 1.f / (-(aw0 + ax + as + an + ab + at));
+      i3 = 1.f / (-(ax + ae3 + as + an + ab + at));
+      i12 = 1.f / (-(ax + ax + as + an + ab + at));
+    }
+    if (q == 0) {
+      c.x = upd(l, c.y, u.x, dn.x, bz.x, tz.x, rh.x, aw0, ax, as, an, ab, at, i0);
+      c.z = upd(c.y, c.w, u.z, dn.z, bz.z, tz.z, rh.z, ax, ax, as, an, ab, at, i12);
+    } else {
+      c.y = upd(c.x, c.z, u.y, dn.y, bz.y, tz.y, rh.y, ax, ax, as, an, ab, at, i12);
+      c.w = upd(c.z, r, u.w, dn.w, bz.w, tz.w, rh.w, ax, ae3, as, an, ab, at, i3);
+    }
+  };
+  auto ld4 = [](const float* p) { return *reinterpret_cast<const float4*>(p); };
+  // lanes of this warp that exist (the last warp of a CTA can be partial)
+  const int wlanes = min(32, (int)blockDim.x - (int)(threadIdx.x & ~31u));
+  const unsigned FULL = wlanes == 32 ? 0xffffffffu : ((1u << wlanes) - 1u);
+
+  if (leader)
+    for (int q = zlo - 1; q <= min(zlo + D, zhi + 1); ++q) issue(q);
+  wait_plane(zlo - 1);
+  wait_plane(zlo);
+  int s0 = zlo % NS;  // slot of plane z
+  // own group of planes z-3 .. z+1 (planes below z hold their red updates)
+  float4 m3 = make_float4(0.f, 0.f, 0.f, 0.f), m2 = m3, p1 = m3;
+  float4 m1 = ld4(pslot(wrap(s0 - 1)) + pc), c0 = ld4(pslot(s0) + pc);
+  for (int z = zlo; z <= ze + 2; ++z) {
+    const int zb = z - 2;
+    const bool red = z <= zhi && yin;              // red cells of plane z
+    const bool blk = zb >= zs && zb <= ze && yown;  // black cells of plane z-2
+    const int sb = wrap(s0 - 2);
+    if (z <= zhi) {
+      wait_plane(z + 1);
+      p1 = ld4(pslot(wrap(s0 + 1)) + pc);
+    }
+    // neighbours across the group's ends: lanes of the same row, ghost columns at the row ends
+    float rl = __shfl_up_sync(FULL, c0.w, 1, TPR), rr = __shfl_down_sync(FULL, c0.x, 1, TPR);
+    float bl = __shfl_up_sync(FULL, m2.w, 1, TPR), br = __shfl_down_sync(FULL, m2.x, 1, TPR);
+    float4 ur, dr, hr, ub, db, hb;
+    if (red) {
+      const float* P = pslot(s0);
+      ur = ld4(P + pc - BX);
+      dr = ld4(P + pc + BX);
+      hr = ld4(rslot(s0) + rcol);
+      if (lft) rl = P[pc - 1];
+      if (rgt) rr = P[pc + 4];
+    }
+    if (blk) {
+      const float* P = pslot(sb);
+      ub = ld4(P + pc - BX);
+      db = ld4(P + pc + BX);
+      hb = ld4(rslot(sb) + rcol);
+      if (lft) bl = P[pc - 1];
+      if (rgt) br = P[pc + 4];
+    }
+    if (red) {
+      colour(c0, m1, p1, ur, dr, hr, rl, rr, z, (y + z) & 1);
+      *reinterpret_cast<float4*>(pslot(s0) + pc) = c0;
+    }
+    if (blk) {
+      colour(m2, m3, m1, ub, db, hb, bl, br, zb, (y + zb + 1) & 1);
+      *reinterpret_cast<float4*>(Drow + (long long)zb * sxy) = m2;
+    }
+    __syncthreads();
+    if (leader && z + D + 1 <= zhi + 1) issue(z + D + 1);
+    m3 = m2;
+    m2 = m1;
+    m1 = c0;
+    c0 = p1;
+    s0 = wrap(s0 + 1);
+  }
 }
 
-template <int TPR, int TY, int D>
+template <int TPR, int GPT, int TY, int NS, int D>
+static cudaError_t vec_attr() {
+  return cudaFuncSetAttribute(k_rbgs_vec<TPR, GPT, TY, NS, D>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)VecCfg<TPR, GPT, TY, NS, D>::SMEM);
+}
+
+template <int TPR, int GPT, int TY, int NS, int D>
 static cudaError_t vec_dispatch(const BlkLev* bl, const Tile* tiles, int ntiles, int zc, const CUtensorMap* maps,
                                 const CUtensorMap* rmaps, int* err, float* dst, cudaStream_t st) {
   if (ntiles <= 0) return cudaSuccess;
-  k_rbgs_vec<TPR, TY, D><<<ntiles, TPR * (TY + 2), VecCfg<TPR, TY, D>::SMEM, st>>>(bl, tiles, zc, maps, rmaps, dst, err);
+  k_rbgs_vec<TPR, GPT, TY, NS, D><<<ntiles, TPR * (TY + 2), VecCfg<TPR, GPT, TY, NS, D>::SMEM, st>>>(
+      bl, tiles, zc, maps, rmaps, dst, err);
   return cudaGetLastError();
 }
 
-// (variant, groups of four cells per row, rows, prefetch depth)
-#define H3D_VEC_SHAPES(X) \
-  X(30, 32, 4, 4)         \
-  X(31, 32, 8, 4)         \
-  X(32, 32, 16, 4)        \
-  X(33, 16, 8, 4)         \
-  X(34, 16, 16, 4)        \
-  X(35, 8, 16, 4)         \
-  X(36, 4, 16, 4)         \
-  X(37, 32, 8, 2)
+template <int TPR, int TY, int NS, int D>
+static cudaError_t win_attr() {
+  return cudaFuncSetAttribute(k_rbgs_win<TPR, TY, NS, D>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)VecCfg<TPR, 1, TY, NS, D>::SMEM);
+}
+
+template <int TPR, int TY, int NS, int D>
+static cudaError_t win_dispatch(const BlkLev* bl, const Tile* tiles, int ntiles, int zc, const CUtensorMap* maps,
+                                const CUtensorMap* rmaps, int* err, float* dst, cudaStream_t st) {
+  static_assert(D + 3 <= NS, "a plane is read until two phases after its own");
+  if (ntiles <= 0) return cudaSuccess;
+  k_rbgs_win<TPR, TY, NS, D><<<ntiles, TPR * (TY + 2), VecCfg<TPR, 1, TY, NS, D>::SMEM, st>>>(bl, tiles, zc, maps,
+                                                                                            rmaps, dst, err);
+  return cudaGetLastError();
+}
+
+// (variant, lanes per row, rows, ring slots, prefetch depth)
+#define H3D_WIN_SHAPES(X) \
+  X(40, 32, 4, 6, 3)      \
+  X(41, 32, 8, 6, 3)      \
+  X(42, 32, 16, 5, 2)     \
+  X(43, 32, 8, 8, 5)      \
+  X(44, 16, 8, 6, 3)      \
+  X(45, 16, 16, 6, 3)     \
+  X(46, 8, 16, 6, 3)      \
+  X(47, 4, 16, 6, 3)
+
+// (variant, threads per row, groups of four cells per thread, rows, ring slots, prefetch depth)
+#define H3D_VEC_SHAPES(X)  \
+  X(30, 32, 1, 4, 8, 4)    \
+  X(31, 32, 1, 8, 8, 4)    \
+  X(32, 32, 1, 8, 6, 2)    \
+  X(33, 32, 1, 16, 6, 2)   \
+  X(34, 16, 2, 8, 6, 2)    \
+  X(35, 16, 2, 16, 6, 2)   \
+  X(36, 16, 1, 8, 8, 4)    \
+  X(37, 16, 1, 16, 6, 2)   \
+  X(38, 8, 1, 16, 6, 2)    \
+  X(39, 4, 1, 16, 6, 2)
 
 #define H3D_ROW_SHAPES(X)  \
   X(8, 64, 1, 8)           \
@@ -1331,9 +1568,13 @@ cudaError_t init_kernel_attributes() {
   if ((e = tma2_attr<double, tpr, cp, ty, d>()) != cudaSuccess) return e;
   H3D_TMA2_SHAPES(X)
 #undef X
-#define X(v, tpr, ty, d) \
-  if ((e = vec_attr<tpr, ty, d>()) != cudaSuccess) return e;
+#define X(v, tpr, gpt, ty, ns, d) \
+  if ((e = vec_attr<tpr, gpt, ty, ns, d>()) != cudaSuccess) return e;
   H3D_VEC_SHAPES(X)
+#undef X
+#define X(v, tpr, ty, ns, d) \
+  if ((e = win_attr<tpr, ty, ns, d>()) != cudaSuccess) return e;
+  H3D_WIN_SHAPES(X)
 #undef X
   return e;
 }
@@ -1353,9 +1594,13 @@ cudaError_t launch_rbgs(int variant, bool var, bool zero_src, const BlkLev* bl, 
   }
   if constexpr (sizeof(T) == 4) {
     switch (variant) {
-#define X(v, tpr, ty, d) \
-      case v: return vec_dispatch<tpr, ty, d>(bl, tiles, ntiles, zc, maps, rmaps, err, reinterpret_cast<float*>(dst), st);
+#define X(v, tpr, gpt, ty, ns, d) \
+      case v: return vec_dispatch<tpr, gpt, ty, ns, d>(bl, tiles, ntiles, zc, maps, rmaps, err, reinterpret_cast<float*>(dst), st);
       H3D_VEC_SHAPES(X)
+#undef X
+#define X(v, tpr, ty, ns, d) \
+      case v: return win_dispatch<tpr, ty, ns, d>(bl, tiles, ntiles, zc, maps, rmaps, err, reinterpret_cast<float*>(dst), st);
+      H3D_WIN_SHAPES(X)
 #undef X
       default: break;
     }

@@ -269,7 +269,7 @@ void default_tile(const Level& Lv, int* variant, int* zc) {
   else if (nxm >= 8) v = nym >= 8 ? 4 : 5;
   else v = 6;
   // whole-row tiles when every block allows them (TMA-staged first)
-  const int pref[] = {36, 35, 34, 31, 28, 25, 24, 20, 13, 12, 10, 8, 14, 16};
+  const int pref[] = {47, 46, 45, 41, 28, 25, 24, 20, 13, 12, 10, 8, 14, 16};
   for (int cand : pref) {
     TileShape c = tile_shape(cand);
     if (nxm <= c.tx && nxm * 2 > c.tx / 2 && variant_fits(Lv, cand) && nym >= 4) { v = cand; break; }
