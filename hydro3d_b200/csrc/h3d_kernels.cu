@@ -6,6 +6,8 @@
 // 7-point stencil is not a contraction; no tensor cores are used).
 #include <cstdint>
 
+#include <type_traits>
+
 #include "h3d_kernels.cuh"
 
 namespace h3d {
@@ -1685,8 +1687,162 @@ cudaError_t launch_defect(bool var, const BlkLev* bl, RowTab rt, const double* p
 }
 
 
+// ---------------------------------------------------------------------------
+// TMA-staged restriction (mgrestr, mgsolver.for:623-766): fine residuals
+// summed into the coarse right-hand side, with the arithmetic of
+// k_restrict_tile (same residual operand order, same child order: i fastest,
+// then j, then k), so FP64 stays bit-exact.  A CTA owns TYC coarse rows of a
+// block (whole rows) and a range of coarse planes; fine planes arrive by TMA
+// (iterate: fine rows 2Y0-2 .. 2Y0+2TYC-1, right-hand side: rows 2Y0-1 ..
+// 2Y0+2TYC-2) into an NS-slot ring, D planes ahead, one barrier per fine
+// plane.  Thread (tr, tc) owns coarse cells X = 1 + tc + k*TPR of coarse row
+// Y0 + tr and reads each pair of fine children (x = 2X-1, 2X) with one
+// 8- (FP32) or 16-byte (FP64) shared-memory load.
+template <typename T, int TPR, int CPX, int TYC, int NS>
+struct RTmaCfg {
+  static constexpr int VEC = 16 / (int)sizeof(T);
+  static constexpr int SPMAX = ((2 * CPX * TPR + 2 + kXOff + VEC - 1) / VEC) * VEC;
+  static constexpr int PSLOT = ((SPMAX * (2 * TYC + 2) * (int)sizeof(T) + 127) / 128) * 128;
+  static constexpr int RSLOT = ((SPMAX * (2 * TYC) * (int)sizeof(T) + 127) / 128) * 128;
+  static constexpr int SLOT = PSLOT + RSLOT;
+  static constexpr size_t SMEM = (size_t)NS * SLOT + 128 + NS * 8;
+  static_assert(SMEM <= 232448, "ring exceeds shared memory");
+};
+
+template <typename T>
+struct Pair {
+  T x, y;
+};
+
+template <typename T, int TPR, int CPX, int TYC, int NS, int D, bool VAR, bool ZERO>
+__global__ void __launch_bounds__(TPR* TYC) k_restrict_tma(const BlkLev* __restrict__ fine,
+                                                          const BlkLev* __restrict__ coarse,
+                                                          const Tile* __restrict__ tiles, int zc,
+                                                          const CUtensorMap* __restrict__ pmaps,
+                                                          const CUtensorMap* __restrict__ rmaps,
+                                                          T* __restrict__ rhs_c, const T* __restrict__ fx,
+                                                          const T* __restrict__ fy, const T* __restrict__ fz,
+                                                          int* err) {
+  using C = RTmaCfg<T, TPR, CPX, TYC, NS>;
+  static_assert(D + 2 <= NS, "a fine plane is read until the phase after its own");
+  using P2 = typename std::conditional<sizeof(T) == 4, float2, double2>::type;
+  extern __shared__ unsigned char smem_raw[];
+  unsigned char* base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
+  uint64_t* bars = reinterpret_cast<uint64_t*>(base + NS * C::SLOT);
+
+  const Tile t = tiles[blockIdx.x];
+  const BlkLev F = fine[t.b];
+  const BlkLev Cc = coarse[t.b];
+  const CUtensorMap* pmap = pmaps + t.b;
+  const CUtensorMap* rmap = rmaps + t.b;
+  const T* FX = VAR ? fx + F.off : nullptr;
+  const T* FY = VAR ? fy + F.off : nullptr;
+  const T* FZ = VAR ? fz + F.off : nullptr;
+  const int Y0 = t.y0, Z0 = t.z0;
+  const int Z1 = min(Z0 + zc - 1, Cc.nz);
+  const int zfa = 2 * Z0 - 1, zfb = 2 * Z1;  // fine planes of the chunk
+  const int BX = ((F.nx + 2 + kXOff + C::VEC - 1) / C::VEC) * C::VEC;
+  const uint32_t pbytes = ZERO ? 0u : (uint32_t)(BX * (2 * TYC + 2) * (int)sizeof(T));
+  const uint32_t tx_bytes = pbytes + (uint32_t)(BX * 2 * TYC * (int)sizeof(T));
+  const int tr = threadIdx.x / TPR, tc = threadIdx.x - (threadIdx.x / TPR) * TPR;
+  const int Y = Y0 + tr;
+  const bool yok = Y <= Cc.ny;
+  const bool leader = threadIdx.x == 0;
+  bool bad = false;
+
+  if (leader) {
+    for (int q = 0; q < NS; ++q)
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(bars + q)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  __syncthreads();
+
+  auto pslot = [&](int q) -> const T* { return reinterpret_cast<const T*>(base + (q % NS) * C::SLOT); };
+  auto rslot = [&](int q) -> const T* { return reinterpret_cast<const T*>(base + (q % NS) * C::SLOT + C::PSLOT); };
+  auto issue = [&](int q) {  // leader only
+    const uint32_t bar = smem_u32(bars + q % NS);
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(tx_bytes) : "memory");
+    if (!ZERO)
+      asm volatile(
+          "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];\n" ::
+              "r"(smem_u32(pslot(q))),
+          "l"(reinterpret_cast<uint64_t>(pmap)), "r"(0), "r"(2 * Y0 - 2), "r"(q), "r"(bar)
+          : "memory");
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];\n" ::
+            "r"(smem_u32(rslot(q))),
+        "l"(reinterpret_cast<uint64_t>(rmap)), "r"(0), "r"(2 * Y0 - 1), "r"(q), "r"(bar)
+        : "memory");
+  };
+  auto wait_plane = [&](int q) {
+    const uint32_t parity = (uint32_t)(((q - zfa + 1) / NS) & 1);
+    mbar_wait(smem_u32(bars + q % NS), parity, err, bad);
+  };
+
+  T sum[CPX];
+#pragma unroll
+  for (int k = 0; k < CPX; ++k) sum[k] = T(0);
+  if (leader)
+    for (int q = zfa - 1; q <= min(zfa + D, zfb + 1); ++q) issue(q);
+  wait_plane(zfa - 1);
+  wait_plane(zfa);
+  for (int zf = zfa; zf <= zfb; ++zf) {
+    wait_plane(zf + 1);
+    if (yok) {
+      const T* S = pslot(zf);
+      const T* Sm = pslot(zf - 1);
+      const T* Sp = pslot(zf + 1);
+      const T* R = rslot(zf);
+#pragma unroll
+      for (int k = 0; k < CPX; ++k) {
+        const int X = 1 + tc + k * TPR;
+        if (X > Cc.nx) continue;
+        const int ca = 2 * X - 1 + kXOff;  // smem column of the first child (even: aligned pair)
+#pragma unroll
+        for (int dj = 0; dj < 2; ++dj) {
+          const int y = 2 * Y - 1 + dj;
+          const int ro = (2 * tr + 1 + dj) * BX + ca;  // iterate slot offset of the pair
+          const P2 rh = *reinterpret_cast<const P2*>(R + (2 * tr + dj) * BX + ca);
+          T ra, rb;
+          if (ZERO) {
+            ra = rh.x - T(0);
+            rb = rh.y - T(0);
+          } else {
+            const P2 cen = *reinterpret_cast<const P2*>(S + ro);
+            const P2 up = *reinterpret_cast<const P2*>(S + ro - BX);
+            const P2 dn = *reinterpret_cast<const P2*>(S + ro + BX);
+            const P2 bo = *reinterpret_cast<const P2*>(Sm + ro);
+            const P2 to = *reinterpret_cast<const P2*>(Sp + ro);
+            const T wa = S[ro - 1], eb = S[ro + 2];
+            const int xa = 2 * X - 1;
+            const long long ia = (long long)zf * F.sxy + (long long)y * F.sx + xa;
+            const Coef<T> c0 = cell_coef<T, VAR>(F, xa, y, zf, ia, FX, FY, FZ);
+            const Coef<T> c1 = cell_coef<T, VAR>(F, xa + 1, y, zf, ia + 1, FX, FY, FZ);
+            const T ap0 = coef_ap(c0), ap1 = coef_ap(c1);
+            ra = rh.x - (c0.aw * wa + c0.ae * cen.y + c0.as * up.x + c0.an * dn.x + c0.ab * bo.x + c0.at * to.x +
+                         ap0 * cen.x);
+            rb = rh.y - (c1.aw * cen.x + c1.ae * eb + c1.as * up.y + c1.an * dn.y + c1.ab * bo.y + c1.at * to.y +
+                         ap1 * cen.y);
+          }
+          sum[k] = ((zf & 1) && dj == 0) ? ra : sum[k] + ra;
+          sum[k] = sum[k] + rb;
+        }
+        if (!(zf & 1))
+          rhs_c[Cc.off + (long long)(zf >> 1) * Cc.sxy + (long long)Y * Cc.sx + X] = T(0.125) * sum[k];
+      }
+    }
+    __syncthreads();
+    if (leader && zf + D + 1 <= zfb + 1) issue(zf + D + 1);
+  }
+}
+
 // ---- tile restriction ------------------------------------------------------
-static const RestrictShape kRShapes[] = {{16, 1, 8}, {32, 1, 8}, {32, 2, 4}, {32, 4, 4}};
+// 0-3 plain-load tiles (k_restrict_tile); 4+ TMA-staged (k_restrict_tma)
+static const RestrictShape kRShapes[] = {{16, 1, 8, 0}, {32, 1, 8, 0}, {32, 2, 4, 0}, {32, 4, 4, 0},
+                                          {32, 2, 4, 1},  {32, 2, 8, 1}, {16, 2, 8, 1}, {32, 1, 8, 1},
+                                          {16, 1, 8, 1},  {32, 4, 4, 1}, {64, 1, 4, 1}};
+int rtma_tyc_index(int tyc) { return tyc == 4 ? 0 : tyc == 8 ? 1 : -1; }
 int num_restrict_shapes() { return (int)(sizeof(kRShapes) / sizeof(kRShapes[0])); }
 RestrictShape restrict_shape(int v) { return kRShapes[v]; }
 
@@ -1718,14 +1874,59 @@ static cudaError_t rtile_dispatch(bool var, bool zero, const BlkLev* fine, const
 
 #define H3D_RSHAPES(X) X(0, 16, 1, 8) X(1, 32, 1, 8) X(2, 32, 2, 4) X(3, 32, 4, 4)
 
+template <typename T, int TPR, int CPX, int TYC>
+static constexpr int rtma_ns() {
+  return RTmaCfg<T, TPR, CPX, TYC, 5>::SMEM <= 232448 / 2 ? 5 : 4;
+}
+
+template <typename T, int TPR, int CPX, int TYC>
+static cudaError_t rtma_attr() {
+  constexpr int NS = rtma_ns<T, TPR, CPX, TYC>();
+  const int sm = (int)RTmaCfg<T, TPR, CPX, TYC, NS>::SMEM;
+  cudaError_t e;
+  if ((e = cudaFuncSetAttribute(k_restrict_tma<T, TPR, CPX, TYC, NS, NS - 2, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm))) return e;
+  if ((e = cudaFuncSetAttribute(k_restrict_tma<T, TPR, CPX, TYC, NS, NS - 2, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm))) return e;
+  if ((e = cudaFuncSetAttribute(k_restrict_tma<T, TPR, CPX, TYC, NS, NS - 2, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm))) return e;
+  return cudaFuncSetAttribute(k_restrict_tma<T, TPR, CPX, TYC, NS, NS - 2, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+}
+
+template <typename T, int TPR, int CPX, int TYC>
+static cudaError_t rtma_dispatch(bool var, bool zero, const BlkLev* fine, const BlkLev* coarse, const Tile* tiles,
+                                 int ntiles, int zc, const CUtensorMap* pmaps, const CUtensorMap* rmaps, T* rhs_c,
+                                 const T* fx, const T* fy, const T* fz, int* err, cudaStream_t st) {
+  if (ntiles <= 0) return cudaSuccess;
+  constexpr int NS = rtma_ns<T, TPR, CPX, TYC>();
+  constexpr int D = NS - 2;
+  constexpr size_t SM = RTmaCfg<T, TPR, CPX, TYC, NS>::SMEM;
+  constexpr int NT = TPR * TYC;
+  if (var) {
+    if (zero) k_restrict_tma<T, TPR, CPX, TYC, NS, D, true, true><<<ntiles, NT, SM, st>>>(fine, coarse, tiles, zc, pmaps, rmaps, rhs_c, fx, fy, fz, err);
+    else k_restrict_tma<T, TPR, CPX, TYC, NS, D, true, false><<<ntiles, NT, SM, st>>>(fine, coarse, tiles, zc, pmaps, rmaps, rhs_c, fx, fy, fz, err);
+  } else {
+    if (zero) k_restrict_tma<T, TPR, CPX, TYC, NS, D, false, true><<<ntiles, NT, SM, st>>>(fine, coarse, tiles, zc, pmaps, rmaps, rhs_c, fx, fy, fz, err);
+    else k_restrict_tma<T, TPR, CPX, TYC, NS, D, false, false><<<ntiles, NT, SM, st>>>(fine, coarse, tiles, zc, pmaps, rmaps, rhs_c, fx, fy, fz, err);
+  }
+  return cudaGetLastError();
+}
+
+#define H3D_RTMA_SHAPES(X) \
+  X(4, 32, 2, 4) X(5, 32, 2, 8) X(6, 16, 2, 8) X(7, 32, 1, 8) X(8, 16, 1, 8) X(9, 32, 4, 4) X(10, 64, 1, 4)
+
 template <typename T>
 cudaError_t launch_restrict_tile(int variant, bool var, bool zero_phi, const BlkLev* fine, const BlkLev* coarse,
                                  const Tile* tiles, int ntiles, int zc, const T* phi, const T* rhs, T* rhs_c,
-                                 const T* fx, const T* fy, const T* fz, cudaStream_t st) {
+                                 const T* fx, const T* fy, const T* fz, const CUtensorMap* pmaps,
+                                 const CUtensorMap* rmaps, int* err, cudaStream_t st) {
   switch (variant) {
 #define X(v, tpr, cpx, tyc) \
     case v: return rtile_dispatch<T, tpr, cpx, tyc>(var, zero_phi, fine, coarse, tiles, ntiles, zc, phi, rhs, rhs_c, fx, fy, fz, st);
     H3D_RSHAPES(X)
+#undef X
+#define X(v, tpr, cpx, tyc)                                                                                   \
+    case v:                                                                                                   \
+      if (!rmaps || (!pmaps && !zero_phi)) return cudaErrorInvalidValue;                                     \
+      return rtma_dispatch<T, tpr, cpx, tyc>(var, zero_phi, fine, coarse, tiles, ntiles, zc, pmaps, rmaps, rhs_c, fx, fy, fz, err, st);
+    H3D_RTMA_SHAPES(X)
 #undef X
     default: return cudaErrorInvalidValue;
   }
@@ -1740,15 +1941,20 @@ cudaError_t init_kernel_attributes_2() {
   if ((e = rtile_attr<double, tpr, cpx, tyc>()) != cudaSuccess) return e;
   H3D_RSHAPES(X)
 #undef X
+#define X(v, tpr, cpx, tyc)                                                   \
+  if ((e = rtma_attr<float, tpr, cpx, tyc>()) != cudaSuccess) return e;       \
+  if ((e = rtma_attr<double, tpr, cpx, tyc>()) != cudaSuccess) return e;
+  H3D_RTMA_SHAPES(X)
+#undef X
   return e;
 }
 
 template cudaError_t launch_restrict_tile<double>(int, bool, bool, const BlkLev*, const BlkLev*, const Tile*, int, int,
-                                                  const double*, const double*, double*, const double*, const double*,
-                                                  const double*, cudaStream_t);
+    const double*, const double*, double*, const double*, const double*, const double*, const CUtensorMap*, const CUtensorMap*, int*,
+    cudaStream_t);
 template cudaError_t launch_restrict_tile<float>(int, bool, bool, const BlkLev*, const BlkLev*, const Tile*, int, int,
-                                                 const float*, const float*, float*, const float*, const float*,
-                                                 const float*, cudaStream_t);
+    const float*, const float*, float*, const float*, const float*, const float*, const CUtensorMap*, const CUtensorMap*, int*,
+    cudaStream_t);
 
 
 cudaError_t launch_reduce4(const double* partials, int n, double* out, cudaStream_t st) {

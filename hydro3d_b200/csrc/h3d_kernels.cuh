@@ -45,16 +45,22 @@ cudaError_t init_kernel_attributes();
 cudaError_t init_kernel_attributes_2();  // restriction tiles
 
 // Tile restriction shapes: TPR threads per coarse row, CPX coarse cells per
-// thread (coarse nx <= TPR*CPX), TYC coarse rows per CTA.
+// thread (coarse nx <= TPR*CPX), TYC coarse rows per CTA; tma: fine planes
+// staged by TMA (needs the fine level's restriction tensor maps for TYC).
 struct RestrictShape {
-  int tpr, cpx, tyc;
+  int tpr, cpx, tyc, tma;
 };
 int num_restrict_shapes();
 RestrictShape restrict_shape(int v);
+constexpr int kNumRTmaTyc = 2;
+int rtma_tyc_index(int tyc);  // 0, 1 for TYC = 4, 8; -1 otherwise
+// pmaps: tensor maps of the fine iterate (box 2*TYC+2 fine rows); rmaps: of the
+// fine right-hand side (box 2*TYC rows); both only for TMA shapes.
 template <typename T>
 cudaError_t launch_restrict_tile(int variant, bool var, bool zero_phi, const BlkLev* fine, const BlkLev* coarse,
                                  const Tile* tiles, int ntiles, int zc, const T* phi, const T* rhs, T* rhs_c,
-                                 const T* fx, const T* fy, const T* fz, cudaStream_t st);
+                                 const T* fx, const T* fy, const T* fz, const CUtensorMap* pmaps,
+                                 const CUtensorMap* rmaps, int* err, cudaStream_t st);
 
 int num_tile_shapes();
 TileShape tile_shape(int variant);

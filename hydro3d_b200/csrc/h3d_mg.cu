@@ -61,6 +61,7 @@ struct Level {
   double* dens = nullptr;
   Halo sweep, faces, exch, bound;
   CUtensorMap* d_maps = nullptr;  // [ty index][0,1: iterate buffer, 2: rhs][block] tensor maps
+  CUtensorMap* d_rmaps = nullptr;  // as the fine level of a restriction: [tyc index][0,1: iterate, 2: rhs][block]
   Tile* d_rtiles = nullptr;       // restriction tiles (this level as the coarse level)
   int nrtiles = 0, rvariant = 0, rzc = 1;
   bool tma_ok = false;
@@ -240,7 +241,7 @@ int build_restrict_tiles(h3d_mg* h, Level& C) {
   int v = -1;
   for (int q = 0; q < num_restrict_shapes(); ++q) {
     RestrictShape r = restrict_shape(q);
-    if (r.tpr * r.cpx >= nxm) { v = q; break; }
+    if (!r.tma && r.tpr * r.cpx >= nxm) { v = q; break; }
   }
   if (v < 0) return fail(h, H3D_ERR_BAD_CONFIG, "block too wide for the restriction kernels (nx > 512)");
   RestrictShape r = restrict_shape(v);
@@ -291,6 +292,16 @@ const CUtensorMap* sweep_maps(const Level& V, int buf) {
   int ti = tma_ty_index(s.ty);
   if (ti < 0) return nullptr;
   return V.d_maps + ((size_t)ti * 3 + buf) * V.geom.bl.size();
+}
+
+// Restriction tensor maps of fine level F for the coarse level's restriction
+// variant: iterate buffer `buf` (rhs = false) or right-hand side, or null.
+const CUtensorMap* restrict_maps(const Level& F, int variant, int buf, bool rhs) {
+  RestrictShape r = restrict_shape(variant);
+  if (!r.tma || !F.d_rmaps) return nullptr;
+  int ti = rtma_tyc_index(r.tyc);
+  if (ti < 0) return nullptr;
+  return F.d_rmaps + ((size_t)ti * 3 + (rhs ? 2 : buf)) * F.geom.bl.size();
 }
 
 // Tensor maps of the level's right-hand side (box TY+2 rows), or null.
@@ -384,7 +395,9 @@ struct Exec {
     if (mixed_level(gc - 1)) {
       // the coarsest level of a mixed solve keeps an FP32 rhs too (converted after)
       CU(launch_restrict_tile<float>(C.rvariant, h->var, F.zero32, F.d_bl, C.d_bl, C.d_rtiles, C.nrtiles, C.rzc,
-                                     F.phi32[F.cur32], F.rhs32, C.rhs32, F.fx32, F.fy32, F.fz32, h->st));
+                                     F.phi32[F.cur32], F.rhs32, C.rhs32, F.fx32, F.fy32, F.fz32,
+                                     restrict_maps(F, C.rvariant, F.cur32, false),
+                                     restrict_maps(F, C.rvariant, 0, true), h->d_err, h->st));
       TRY(chk("restrict fp32", gc));
       C.zero32 = true;
       if (!mixed_level(gc)) {  // coarsest level solved in FP64
@@ -395,7 +408,9 @@ struct Exec {
       }
     } else {
       CU(launch_restrict_tile<double>(C.rvariant, h->var, F.zero64, F.d_bl, C.d_bl, C.d_rtiles, C.nrtiles, C.rzc,
-                                      F.phi64[F.cur64], F.rhs64, C.rhs64, F.fx64, F.fy64, F.fz64, h->st));
+                                      F.phi64[F.cur64], F.rhs64, C.rhs64, F.fx64, F.fy64, F.fz64,
+                                      restrict_maps(F, C.rvariant, F.cur64, false),
+                                      restrict_maps(F, C.rvariant, 0, true), h->d_err, h->st));
       TRY(chk("restrict fp64", gc));
       C.zero64 = true;
     }
@@ -719,6 +734,32 @@ int build_tensor_maps(h3d_mg* h, int g) {
       }
   TRY(dalloc(h, &V.d_maps, maps.size()));
   CU(cudaMemcpy(V.d_maps, maps.data(), maps.size() * sizeof(CUtensorMap), cudaMemcpyHostToDevice));
+  // restriction from this level: iterate boxes of 2*TYC+2 fine rows, rhs boxes of 2*TYC rows
+  std::vector<CUtensorMap> rm((size_t)kNumRTmaTyc * 3 * nb);
+  const int tycs[kNumRTmaTyc] = {4, 8};
+  for (int ti = 0; ti < kNumRTmaTyc; ++ti)
+    for (int buf = 0; buf < 3; ++buf)
+      for (size_t b = 0; b < nb; ++b) {
+        const BlkLev& B = V.geom.bl[b];
+        const long long o = B.off - kXOff;
+        void* base = buf == 2 ? (f32 ? (void*)(V.rhs32 + o) : (void*)(V.rhs64 + o))
+                              : (f32 ? (void*)(V.phi32[buf] + o) : (void*)(V.phi64[buf] + o));
+        cuuint64_t dims[3] = {(cuuint64_t)B.nx + 2 + kXOff, (cuuint64_t)B.ny + 2, (cuuint64_t)B.nz + 2};
+        cuuint64_t strides[2] = {(cuuint64_t)B.sx * es, (cuuint64_t)B.sxy * es};
+        cuuint32_t box[3] = {(cuuint32_t)((B.nx + 2 + kXOff + vec - 1) / vec * vec),
+                             (cuuint32_t)(2 * tycs[ti] + (buf == 2 ? 0 : 2)), 1};
+        cuuint32_t estr[3] = {1, 1, 1};
+        CUresult r = enc(&rm[((size_t)ti * 3 + buf) * nb + b],
+                         f32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, base, dims,
+                         strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                         CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if (r != CUDA_SUCCESS) {
+          V.tma_ok = true;  // smoother maps are fine; restriction keeps the plain-load kernels
+          return H3D_OK;
+        }
+      }
+  TRY(dalloc(h, &V.d_rmaps, rm.size()));
+  CU(cudaMemcpy(V.d_rmaps, rm.data(), rm.size() * sizeof(CUtensorMap), cudaMemcpyHostToDevice));
   V.tma_ok = true;
   return H3D_OK;
 }
@@ -781,6 +822,75 @@ int autotune_level(h3d_mg* h, int g) {
   cudaEventDestroy(a);
   cudaEventDestroy(b);
   return build_tiles(h, V, best_v, best_z);
+}
+
+// Times every restriction variant and coarse z-chunk that fits the level
+// pair (fine level gc-1 with at least 2^20 cells) and keeps the fastest.
+int autotune_restrict(h3d_mg* h, int gc) {
+  Level& F = h->lev[gc - 1];
+  Level& C = h->lev[gc];
+  if (F.geom.n_interior < (1 << 20)) return H3D_OK;
+  int nxm = 0, nzm = 0;
+  for (const auto& B : C.geom.bl) { nxm = std::max(nxm, B.nx); nzm = std::max(nzm, B.nz); }
+  const bool f32 = F.f32;
+  cudaEvent_t a, b;
+  CU(cudaEventCreate(&a));
+  CU(cudaEventCreate(&b));
+  float best = 1e30f;
+  int best_v = C.rvariant, best_z = C.rzc;
+  for (int v = 0; v < num_restrict_shapes(); ++v) {
+    RestrictShape r = restrict_shape(v);
+    if (r.tpr * r.cpx < nxm) continue;
+    if (r.tma && (!F.tma_ok || !F.d_rmaps)) continue;
+    for (int zc : {2, 4, 8, 16, 32, 64}) {
+      if (zc > nzm) continue;
+      std::vector<Tile> t = row_tiles(C.geom, r.tyc, zc);
+      dfree(C.d_rtiles);
+      C.d_rtiles = nullptr;
+      TRY(dalloc(h, &C.d_rtiles, t.size()));
+      CU(cudaMemcpy(C.d_rtiles, t.data(), t.size() * sizeof(Tile), cudaMemcpyHostToDevice));
+      C.nrtiles = (int)t.size();
+      float tot = 0;
+      for (int rep = 0; rep < 4; ++rep) {
+        CU(cudaEventRecord(a, h->st));
+        if (f32)
+          CU(launch_restrict_tile<float>(v, h->var, false, F.d_bl, C.d_bl, C.d_rtiles, C.nrtiles, zc,
+                                         F.phi32[F.cur32], F.rhs32, C.rhs32, F.fx32, F.fy32, F.fz32,
+                                         restrict_maps(F, v, F.cur32, false), restrict_maps(F, v, 0, true), h->d_err,
+                                         h->st));
+        else
+          CU(launch_restrict_tile<double>(v, h->var, false, F.d_bl, C.d_bl, C.d_rtiles, C.nrtiles, zc,
+                                          F.phi64[F.cur64], F.rhs64, C.rhs64, F.fx64, F.fy64, F.fz64,
+                                          restrict_maps(F, v, F.cur64, false), restrict_maps(F, v, 0, true),
+                                          h->d_err, h->st));
+        CU(cudaEventRecord(b, h->st));
+        cudaError_t e = cudaEventSynchronize(b);
+        int werr = 0;
+        if (e == cudaSuccess) e = cudaMemcpy(&werr, h->d_err, sizeof(int), cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess || werr)
+          return fail(h, e != cudaSuccess ? H3D_ERR_CUDA : H3D_ERR_TIMEOUT,
+                      "restriction autotuning (level " + std::to_string(gc) + ", variant " + std::to_string(v) +
+                          ", z-chunk " + std::to_string(zc) + "): " +
+                          (e != cudaSuccess ? cudaGetErrorString(e) : "a bounded device wait gave up"));
+        float ms;
+        CU(cudaEventElapsedTime(&ms, a, b));
+        if (rep > 0) tot += ms;
+      }
+      if (tot < best) { best = tot; best_v = v; best_z = zc; }
+    }
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  RestrictShape r = restrict_shape(best_v);
+  std::vector<Tile> t = row_tiles(C.geom, r.tyc, best_z);
+  dfree(C.d_rtiles);
+  C.d_rtiles = nullptr;
+  TRY(dalloc(h, &C.d_rtiles, t.size()));
+  CU(cudaMemcpy(C.d_rtiles, t.data(), t.size() * sizeof(Tile), cudaMemcpyHostToDevice));
+  C.nrtiles = (int)t.size();
+  C.rvariant = best_v;
+  C.rzc = best_z;
+  return H3D_OK;
 }
 
 }  // namespace
@@ -898,7 +1008,7 @@ int h3d_mg_destroy(h3d_mg* h) {
     void* ps[] = {V.d_bl, V.d_cta_all, V.d_cta_int, V.d_rows_all, V.d_rows_int, V.d_tiles, V.phi64[0], V.phi64[1], V.rhs64, V.phi32[0],
                   V.phi32[1], V.rhs32, V.fx64, V.fy64, V.fz64, V.fx32, V.fy32, V.fz32, V.dens,
                   V.sweep.d_dst, V.sweep.d_src, V.faces.d_dst, V.faces.d_src, V.exch.d_dst, V.exch.d_src,
-                  V.bound.d_dst, V.bound.d_src, V.d_maps, V.d_rtiles};
+                  V.bound.d_dst, V.bound.d_src, V.d_maps, V.d_rmaps, V.d_rtiles};
     for (void* p : ps) dfree(p);
   }
   dfree(h->p64[0]);
@@ -1077,6 +1187,7 @@ int h3d_mg_coeff(h3d_mg* h) {
   }
   // autotune the smoother tiles of the large levels once coefficients exist
   for (int g = 1; g <= h->L; ++g) TRY(autotune_level(h, g));
+  for (int g = 2; g <= h->L; ++g) TRY(autotune_restrict(h, g));
   CU(cudaStreamSynchronize(h->st));
   h->coeffs_ready = true;
   return H3D_OK;
@@ -1478,6 +1589,37 @@ int h3d_mg_get_smoother(h3d_mg* h, int32_t g, int32_t* variant, int32_t* zchunk,
   if (variant) *variant = h->lev[g].variant;
   if (zchunk) *zchunk = h->lev[g].zc;
   if (nvariants) *nvariants = num_tile_shapes();
+  return H3D_OK;
+}
+
+int h3d_mg_set_restriction(h3d_mg* h, int32_t g, int32_t variant, int32_t zchunk) {
+  if (!level_ok(h, g) || g < 2 || variant < 0 || variant >= num_restrict_shapes() || zchunk < 1)
+    return H3D_ERR_ARG;
+  Level& F = h->lev[g - 1];
+  Level& C = h->lev[g];
+  RestrictShape r = restrict_shape(variant);
+  int nxm = 0;
+  for (const auto& B : C.geom.bl) nxm = std::max(nxm, B.nx);
+  if (r.tpr * r.cpx < nxm || (r.tma && (!F.tma_ok || !F.d_rmaps)))
+    return fail(h, H3D_ERR_ARG, "restriction variant does not fit this level");
+  CU(cudaSetDevice(h->device));
+  std::vector<Tile> t = row_tiles(C.geom, r.tyc, zchunk);
+  dfree(C.d_rtiles);
+  C.d_rtiles = nullptr;
+  TRY(dalloc(h, &C.d_rtiles, t.size()));
+  CU(cudaMemcpy(C.d_rtiles, t.data(), t.size() * sizeof(Tile), cudaMemcpyHostToDevice));
+  C.nrtiles = (int)t.size();
+  C.rvariant = variant;
+  C.rzc = zchunk;
+  h->graphs.clear();  // captured graphs refer to the old tiles
+  return H3D_OK;
+}
+
+int h3d_mg_get_restriction(h3d_mg* h, int32_t g, int32_t* variant, int32_t* zchunk, int32_t* nvariants) {
+  if (!level_ok(h, g) || g < 2) return H3D_ERR_ARG;
+  if (variant) *variant = h->lev[g].rvariant;
+  if (zchunk) *zchunk = h->lev[g].rzc;
+  if (nvariants) *nvariants = num_restrict_shapes();
   return H3D_OK;
 }
 

@@ -196,6 +196,20 @@ class MultigridSolver:
         self._check(rc, "h3d_mg_set_smoother")
         return True
 
+    def set_restriction(self, g: int, variant: int, zchunk: int) -> bool:
+        """Force the restriction variant / coarse z-chunk into level g; False if it cannot run there."""
+        rc = self.L.h3d_mg_set_restriction(self._h, g, variant, zchunk)
+        if rc == _lib.H3D_ERR_ARG:
+            return False
+        self._check(rc, "h3d_mg_set_restriction")
+        return True
+
+    def get_restriction(self, g: int):
+        v, z, n = C.c_int32(), C.c_int32(), C.c_int32()
+        self._check(self.L.h3d_mg_get_restriction(self._h, g, C.byref(v), C.byref(z), C.byref(n)),
+                    "h3d_mg_get_restriction")
+        return v.value, z.value, n.value
+
     def get_smoother(self, g: int):
         v, z, n = C.c_int32(), C.c_int32(), C.c_int32()
         self._check(self.L.h3d_mg_get_smoother(self._h, g, C.byref(v), C.byref(z), C.byref(n)), "h3d_mg_get_smoother")

@@ -151,6 +151,11 @@ int h3d_mg_set_profiling(h3d_mg* h, int32_t on);
  * receives the number of variants. */
 int h3d_mg_set_smoother(h3d_mg* h, int32_t g, int32_t variant, int32_t zchunk);
 int h3d_mg_get_smoother(h3d_mg* h, int32_t g, int32_t* variant, int32_t* zchunk, int32_t* nvariants);
+/* Restriction kernel variant and coarse z-chunk used into level g (g >= 2);
+ * chosen by timing on large levels in h3d_mg_coeff.  H3D_ERR_ARG if the
+ * variant cannot run there.  Tuning controls; no counterpart in the reference. */
+int h3d_mg_set_restriction(h3d_mg* h, int32_t g, int32_t variant, int32_t zchunk);
+int h3d_mg_get_restriction(h3d_mg* h, int32_t g, int32_t* variant, int32_t* zchunk, int32_t* nvariants);
 /* Algorithmic bytes of one level-1 smoother launch (sum over blocks). */
 int h3d_mg_smoother_bytes(h3d_mg* h, double* bytes_per_launch);
 

@@ -272,3 +272,36 @@ def test_every_smoother_variant(oracle_mod, h3d, precision):
                 _assert_level(s, orc, 1, exact=(precision == "fp64"))
         assert tried >= need
         s.close()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_every_restriction_variant(oracle_mod, h3d, precision):
+    """Each restriction kernel variant (plain-load tiles and TMA-staged tiles)
+    and several coarse z-chunks give the reference mgrestr, also from a zero
+    iterate (the level just restricted into) and with ragged row tiles:
+    bit-exact in FP64, within the FP32 tolerance on the mixed solver's FP32
+    levels."""
+    rng = np.random.default_rng(11)
+    exact = precision == "fp64"
+    for layout in (((2, 2, 1), (32, 16, 16), [P, P, W, W, W, W], 3),
+                   ((2, 1, 1), (32, 24, 12), [W, W, P, P, W, W], 3)):
+        blocks, s, orc = _pair(oracle_mod, h3d, layout, precision=precision)
+        s.coeff(); orc.coeff()
+        _, _, nvar = s.get_restriction(2)
+        tried = tma = 0
+        for v in range(nvar):
+            for zc in (1, 3, 8):
+                if not s.set_restriction(2, v, zc):
+                    continue
+                tried += 1
+                tma += v >= 4
+                _rand_level(rng, s, orc, 1)
+                s.mgrestr(2)
+                orc.mgrestr(2)
+                _assert_level(s, orc, 2, "rhs", exact=exact)
+                if s.set_restriction(3, v, zc):  # from the zero iterate of level 2
+                    s.mgrestr(3)
+                    orc.mgrestr(3)
+                    _assert_level(s, orc, 3, "rhs", exact=exact)
+        assert tried >= 12 and tma >= 6
+        s.close()
