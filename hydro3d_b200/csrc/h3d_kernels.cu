@@ -4,6 +4,7 @@
 // and the library is compiled with --fmad=false, so the FP64 path reproduces
 // the reference arithmetic bit for bit.  Every kernel is memory bound (a
 // 7-point stencil is not a contraction; no tensor cores are used).
+#include <algorithm>
 #include <cstdint>
 
 #include <type_traits>
@@ -1956,6 +1957,42 @@ template cudaError_t launch_restrict_tile<float>(int, bool, bool, const BlkLev*,
     const float*, const float*, float*, const float*, const float*, const float*, const CUtensorMap*, const CUtensorMap*, int*,
     cudaStream_t);
 
+
+// ---------------------------------------------------------------------------
+// Host-field staging: a host block array (Fortran dims tx, ty, tz with pl
+// ghost layers, x fastest) is copied whole and contiguously between host and
+// a device staging buffer; these kernels move the region g0 .. (extent) of
+// the canonical block (ghost layer included when g0 = 0) between staging and
+// the padded device layout.
+__global__ void k_stage_scatter(const double* __restrict__ stg, int tx, int ty, int pl, int g0, int ex, int ey,
+                                int ez, double* __restrict__ dev, int sx, long long sxy) {
+  const long long n = (long long)ex * ey * ez;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+    const int x = (int)(e % ex), y = (int)((e / ex) % ey), z = (int)(e / ((long long)ex * ey));
+    const int hx = pl - 1 + g0 + x, hy = pl - 1 + g0 + y, hz = pl - 1 + g0 + z;
+    dev[(long long)(g0 + z) * sxy + (long long)(g0 + y) * sx + g0 + x] = stg[((long long)hz * ty + hy) * tx + hx];
+  }
+}
+
+__global__ void k_stage_gather(double* __restrict__ stg, int tx, int ty, int pl, int g0, int ex, int ey, int ez,
+                               const double* __restrict__ dev, int sx, long long sxy) {
+  const long long n = (long long)ex * ey * ez;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+    const int x = (int)(e % ex), y = (int)((e / ex) % ey), z = (int)(e / ((long long)ex * ey));
+    const int hx = pl - 1 + g0 + x, hy = pl - 1 + g0 + y, hz = pl - 1 + g0 + z;
+    stg[((long long)hz * ty + hy) * tx + hx] = dev[(long long)(g0 + z) * sxy + (long long)(g0 + y) * sx + g0 + x];
+  }
+}
+
+cudaError_t launch_stage(bool to_device, double* stg, int tx, int ty, int pl, int g0, int ex, int ey, int ez,
+                         double* dev, int sx, long long sxy, cudaStream_t st) {
+  const long long n = (long long)ex * ey * ez;
+  if (n <= 0) return cudaSuccess;
+  const int grid = (int)std::min<long long>((n + 255) / 256, 148LL * 16);
+  if (to_device) k_stage_scatter<<<grid, 256, 0, st>>>(stg, tx, ty, pl, g0, ex, ey, ez, dev, sx, sxy);
+  else k_stage_gather<<<grid, 256, 0, st>>>(stg, tx, ty, pl, g0, ex, ey, ez, dev, sx, sxy);
+  return cudaGetLastError();
+}
 
 cudaError_t launch_reduce4(const double* partials, int n, double* out, cudaStream_t st) {
   k_reduce4<<<1, 256, 0, st>>>(partials, n, out);

@@ -62,6 +62,12 @@ cudaError_t launch_restrict_tile(int variant, bool var, bool zero_phi, const Blk
                                  const T* fx, const T* fy, const T* fz, const CUtensorMap* pmaps,
                                  const CUtensorMap* rmaps, int* err, cudaStream_t st);
 
+// Moves the region (ex, ey, ez) starting at canonical (g0, g0, g0) of one
+// block between a whole host block array staged on the device (dims tx, ty,
+// tz, pl ghost layers) and the padded device layout (block base dev).
+cudaError_t launch_stage(bool to_device, double* stg, int tx, int ty, int pl, int g0, int ex, int ey, int ez,
+                         double* dev, int sx, long long sxy, cudaStream_t st);
+
 int num_tile_shapes();
 TileShape tile_shape(int variant);
 
