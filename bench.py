@@ -318,9 +318,10 @@ def main():
     info = infos_mixed[-1]
     sm_ms = sum(i["smoother_ms"] for i in infos_mixed)
     sm_n = sum(i["smoother_launches"] for i in infos_mixed)
-    bytes_launch = mixed.smoother_bytes()
+    sm_bytes = sum(i["smoother_bytes"] for i in infos_mixed)  # sweeps from a zero iterate move 8 B/cell, others 12
+    bytes_launch = sm_bytes / max(sm_n, 1)
     avg_launch_ms = sm_ms / max(sm_n, 1)
-    achieved = bytes_launch / (avg_launch_ms * 1e-3) / 1e9 if sm_n else None
+    achieved = sm_bytes / (sm_ms * 1e-3) / 1e9 if sm_n else None
     traffic = read_profile_traffic()
 
     e2e = None
@@ -355,7 +356,7 @@ def main():
             "mcell_updates_per_s": None,
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1) if achieved else None, "peak": peak,
                          "unit": "GB/s", "frac": round(achieved / peak, 4) if achieved else None,
-                         "traffic": traffic, "kernel": "k_rbgs<float> level 1",
+                         "traffic": traffic, "kernel": "level-1 FP32 smoother (autotuned variant %d)" % mixed.get_smoother(1)[0],
                          "bytes_per_launch": bytes_launch, "avg_launch_ms": round(avg_launch_ms, 5),
                          "peak_source": peak_kind},
             "cpu_baseline": cpu, "e2e": e2e,

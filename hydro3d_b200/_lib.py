@@ -88,6 +88,7 @@ class SolveInfo(C.Structure):
         ("smoother_ms", C.c_double),
         ("smoother_launches", C.c_int64),
         ("kernel_launches", C.c_int64),
+        ("smoother_bytes", C.c_double),
     ]
 
 

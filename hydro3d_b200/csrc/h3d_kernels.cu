@@ -1327,7 +1327,7 @@ static cudaError_t tma2_dispatch(bool var, const BlkLev* bl, const Tile* tiles, 
 // warp shuffles (a row is TPR consecutive lanes), the ghost columns from
 // shared memory.  A plane is last read two phases after its own, so the ring
 // needs D+3 slots.
-template <int TPR, int TY, int NS, int D>
+template <int TPR, int TY, int NS, int D, bool ZERO>
 __global__ void __launch_bounds__(TPR*(TY + 2)) k_rbgs_win(const BlkLev* __restrict__ bls,
                                                           const Tile* __restrict__ tiles, int zc,
                                                           const CUtensorMap* __restrict__ maps,
@@ -1349,7 +1349,7 @@ __global__ void __launch_bounds__(TPR*(TY + 2)) k_rbgs_win(const BlkLev* __restr
   const int ze = min(zs + zc - 1, nz);
   const int zlo = max(zs - 1, 1), zhi = min(ze + 1, nz);
   const int BX = (nx + 2 + kXOff + 3) & ~3;  // smem row pitch == TMA box width
-  const uint32_t tx_bytes = (uint32_t)(BX * (2 * TY + 6) * 4);
+  const uint32_t tx_bytes = (uint32_t)(BX * ((ZERO ? 0 : TY + 4) + TY + 2) * 4);
   const int tr = threadIdx.x / TPR, j = threadIdx.x % TPR;
   const int y = y0 - 1 + tr;
   const int x0 = 1 + 4 * j;
@@ -1388,11 +1388,12 @@ __global__ void __launch_bounds__(TPR*(TY + 2)) k_rbgs_win(const BlkLev* __restr
     const uint32_t bar = smem_u32(bars + sl);
     asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(tx_bytes) : "memory");
-    asm volatile(
-        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];\n" ::
-            "r"(smem_u32(pslot(sl))),
-        "l"(reinterpret_cast<uint64_t>(map)), "r"(0), "r"(y0 - 2), "r"(z), "r"(bar)
-        : "memory");
+    if (!ZERO)
+      asm volatile(
+          "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];\n" ::
+              "r"(smem_u32(pslot(sl))),
+          "l"(reinterpret_cast<uint64_t>(map)), "r"(0), "r"(y0 - 2), "r"(z), "r"(bar)
+          : "memory");
     asm volatile(
         "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];\n" ::
             "r"(smem_u32(rslot(sl))),
@@ -1441,8 +1442,9 @@ __global__ void __launch_bounds__(TPR*(TY + 2)) k_rbgs_win(const BlkLev* __restr
   wait_plane(zlo);
   int s0 = zlo % NS;  // slot of plane z
   // own group of planes z-3 .. z+1 (planes below z hold their red updates)
-  float4 m3 = make_float4(0.f, 0.f, 0.f, 0.f), m2 = m3, p1 = m3;
-  float4 m1 = ld4(pslot(wrap(s0 - 1)) + pc), c0 = ld4(pslot(s0) + pc);
+  const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f);
+  float4 m3 = zero4, m2 = zero4, p1 = zero4;
+  float4 m1 = ZERO ? zero4 : ld4(pslot(wrap(s0 - 1)) + pc), c0 = ZERO ? zero4 : ld4(pslot(s0) + pc);
   for (int z = zlo; z <= ze + 2; ++z) {
     const int zb = z - 2;
     const bool red = z <= zhi && yin;              // red cells of plane z
@@ -1450,27 +1452,36 @@ __global__ void __launch_bounds__(TPR*(TY + 2)) k_rbgs_win(const BlkLev* __restr
     const int sb = wrap(s0 - 2);
     if (z <= zhi) {
       wait_plane(z + 1);
-      p1 = ld4(pslot(wrap(s0 + 1)) + pc);
+      p1 = ZERO ? zero4 : ld4(pslot(wrap(s0 + 1)) + pc);
     }
     // neighbours across the group's ends: lanes of the same row, ghost columns at the row ends
     float rl = __shfl_up_sync(FULL, c0.w, 1, TPR), rr = __shfl_down_sync(FULL, c0.x, 1, TPR);
     float bl = __shfl_up_sync(FULL, m2.w, 1, TPR), br = __shfl_down_sync(FULL, m2.x, 1, TPR);
-    float4 ur, dr, hr, ub, db, hb;
+    float4 ur = zero4, dr = zero4, hr, ub = zero4, db = zero4, hb;
     if (red) {
       const float* P = pslot(s0);
-      ur = ld4(P + pc - BX);
-      dr = ld4(P + pc + BX);
       hr = ld4(rslot(s0) + rcol);
-      if (lft) rl = P[pc - 1];
-      if (rgt) rr = P[pc + 4];
+      if (!ZERO) {
+        ur = ld4(P + pc - BX);
+        dr = ld4(P + pc + BX);
+        if (lft) rl = P[pc - 1];
+        if (rgt) rr = P[pc + 4];
+      }
     }
     if (blk) {
       const float* P = pslot(sb);
-      ub = ld4(P + pc - BX);
-      db = ld4(P + pc + BX);
       hb = ld4(rslot(sb) + rcol);
-      if (lft) bl = P[pc - 1];
-      if (rgt) br = P[pc + 4];
+      if (!ZERO) {
+        ub = ld4(P + pc - BX);
+        db = ld4(P + pc + BX);
+        if (lft) bl = P[pc - 1];
+        if (rgt) br = P[pc + 4];
+      } else {  // red neighbours inside the block; the zero source outside it
+        if (y > 1) ub = ld4(P + pc - BX);
+        if (y < ny) db = ld4(P + pc + BX);
+        if (lft) bl = 0.f;
+        if (rgt) br = 0.f;
+      }
     }
     if (red) {
       colour(c0, m1, p1, ur, dr, hr, rl, rr, z, (y + z) & 1);
@@ -1507,20 +1518,26 @@ static cudaError_t vec_dispatch(const BlkLev* bl, const Tile* tiles, int ntiles,
 
 template <int TPR, int TY, int NS, int D>
 static cudaError_t win_attr() {
-  return cudaFuncSetAttribute(k_rbgs_win<TPR, TY, NS, D>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  cudaError_t e = cudaFuncSetAttribute(k_rbgs_win<TPR, TY, NS, D, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)VecCfg<TPR, 1, TY, NS, D>::SMEM);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(k_rbgs_win<TPR, TY, NS, D, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               (int)VecCfg<TPR, 1, TY, NS, D>::SMEM);
 }
 
 template <int TPR, int TY, int NS, int D>
-static cudaError_t win_dispatch(const BlkLev* bl, const Tile* tiles, int ntiles, int zc, const CUtensorMap* maps,
-                                const CUtensorMap* rmaps, int* err, float* dst, cudaStream_t st) {
+static cudaError_t win_dispatch(bool zero, const BlkLev* bl, const Tile* tiles, int ntiles, int zc,
+                                const CUtensorMap* maps, const CUtensorMap* rmaps, int* err, float* dst,
+                                cudaStream_t st) {
   static_assert(D + 3 <= NS, "a plane is read until two phases after its own");
   if (ntiles <= 0) return cudaSuccess;
-  k_rbgs_win<TPR, TY, NS, D><<<ntiles, TPR * (TY + 2), VecCfg<TPR, 1, TY, NS, D>::SMEM, st>>>(bl, tiles, zc, maps,
-                                                                                            rmaps, dst, err);
+  constexpr size_t SM = VecCfg<TPR, 1, TY, NS, D>::SMEM;
+  if (zero) k_rbgs_win<TPR, TY, NS, D, true><<<ntiles, TPR * (TY + 2), SM, st>>>(bl, tiles, zc, maps, rmaps, dst, err);
+  else k_rbgs_win<TPR, TY, NS, D, false><<<ntiles, TPR * (TY + 2), SM, st>>>(bl, tiles, zc, maps, rmaps, dst, err);
   return cudaGetLastError();
 }
 
+constexpr int kFirstWinShape = 40;
 // (variant, lanes per row, rows, ring slots, prefetch depth)
 #define H3D_WIN_SHAPES(X) \
   X(40, 32, 4, 6, 3)      \
@@ -1592,7 +1609,9 @@ cudaError_t launch_rbgs(int variant, bool var, bool zero_src, const BlkLev* bl, 
     // nothing to stage from a zero source: the equivalent plain-load kernel zero-fills;
     // the vectorised sweep is FP32 with constant coefficients only
     const int tk = kShapes[variant].tma;
-    if (zero_src || !maps || (tk >= 2 && !rmaps) || (tk == 3 && (var || sizeof(T) != 4)))
+    const bool win = variant >= kFirstWinShape;  // register-window sweeps handle a zero source themselves
+    if ((zero_src && !(win && sizeof(T) == 4 && !var)) || !maps || (tk >= 2 && !rmaps) ||
+        (tk == 3 && (var || sizeof(T) != 4)))
       variant = kShapes[variant].alt;
   }
   if constexpr (sizeof(T) == 4) {
@@ -1602,7 +1621,7 @@ cudaError_t launch_rbgs(int variant, bool var, bool zero_src, const BlkLev* bl, 
       H3D_VEC_SHAPES(X)
 #undef X
 #define X(v, tpr, ty, ns, d) \
-      case v: return win_dispatch<tpr, ty, ns, d>(bl, tiles, ntiles, zc, maps, rmaps, err, reinterpret_cast<float*>(dst), st);
+      case v: return win_dispatch<tpr, ty, ns, d>(zero_src, bl, tiles, ntiles, zc, maps, rmaps, err, reinterpret_cast<float*>(dst), st);
       H3D_WIN_SHAPES(X)
 #undef X
       default: break;
@@ -1655,6 +1674,113 @@ cudaError_t launch_restrict(bool var, bool zero_phi, const BlkLev* fine, const B
   else k_restrict<T, false, false><<<g, 256, 0, st>>>(fine, coarse, rt.start, rt.nb, rt.nrows, phi, rhs, rhs_c, fx, fy, fz);
   return cudaGetLastError();
 }
+
+// mgcorr + mgbound, tiled and vectorised: a CTA owns 8 consecutive fine rows
+// (y0 .. y0+7, ghost rows included) of one plane z of one block, a warp one
+// row; a lane takes groups of VEC = 16/sizeof(T) interior cells (x0 = 1 +
+// VEC*g, a 16-byte aligned address in the padded layout: one vector load of
+// the old iterate and one vector store), lanes 0 and 1 the ghost columns.
+// Same interpolation, term order and mgbound source as k_prolong_pairs.
+// Needs nx a multiple of VEC.
+template <typename T, bool ZERO_OLD>
+__global__ void __launch_bounds__(256) k_prolong_vec(const BlkLev* __restrict__ fine, const BlkLev* __restrict__ coarse,
+                                                     const Tile* __restrict__ tiles, const T* __restrict__ phi_c,
+                                                     const T* __restrict__ old, T* __restrict__ out) {
+  constexpr int VEC = 16 / (int)sizeof(T);
+  constexpr int NC = VEC / 2 + 2;  // coarse columns a group reads
+  using V = typename std::conditional<sizeof(T) == 4, float4, double2>::type;
+  const Tile t = tiles[blockIdx.x];
+  const BlkLev F = fine[t.b];
+  const BlkLev C = coarse[t.b];
+  const int lane = threadIdx.x & 31;
+  const int y = t.y0 + (threadIdx.x >> 5), z = t.z0;
+  if (y > F.ny + 1) return;
+  const int ph = F.phys;
+  int sy = y, sz = z;
+  if (y == 0 && (ph & 4)) sy = 1;
+  if (y == F.ny + 1 && (ph & 8)) sy = F.ny;
+  if (z == 0 && (ph & 16)) sz = 1;
+  if (z == F.nz + 1 && (ph & 32)) sz = F.nz;
+  const T wy0 = (sy & 1) ? T(1) : T(3), wy1 = (sy & 1) ? T(3) : T(1);
+  const T wz0 = (sz & 1) ? T(1) : T(3), wz1 = (sz & 1) ? T(3) : T(1);
+  const T w00 = wy0 * wz0, w10 = wy1 * wz0, w01 = wy0 * wz1, w11 = wy1 * wz1;  // [dj][dk]
+  const T* Pc = phi_c + C.off + (long long)(sz >> 1) * C.sxy + (long long)(sy >> 1) * C.sx;
+  const long long cy = C.sx, cz = C.sxy;
+  const T* Orow = old + F.off + (long long)sz * F.sxy + (long long)sy * F.sx;
+  T* Out = out + F.off + (long long)z * F.sxy + (long long)y * F.sx;
+  // value of fine cell x whose mgbound source column is sx (pair index q = x >> 1)
+  auto interp = [&](const T* Q, int sx, T o) -> T {
+    const T wx0 = (sx & 1) ? T(1) : T(3), wx1 = (sx & 1) ? T(3) : T(1);
+    // term order (di,dj,dk): 000, 010, 001, 011, 100, 110, 101, 111 (mgsolver.for:838-892)
+    T s = (wx0 * w00) * Q[0];
+    s = s + (wx0 * w10) * Q[cy];
+    s = s + (wx0 * w01) * Q[cz];
+    s = s + (wx0 * w11) * Q[cy + cz];
+    s = s + (wx1 * w00) * Q[1];
+    s = s + (wx1 * w10) * Q[1 + cy];
+    s = s + (wx1 * w01) * Q[1 + cz];
+    s = s + (wx1 * w11) * Q[1 + cy + cz];
+    return o + s / T(64);
+  };
+  const int ng = F.nx / VEC;
+  for (int g = lane; g < ng; g += 32) {
+    const int x0 = 1 + VEC * g;
+    V ov;
+    if (ZERO_OLD) {
+      ov = V{};
+    } else {
+      ov = *reinterpret_cast<const V*>(Orow + x0);
+    }
+    T o[VEC], r[VEC];
+    *reinterpret_cast<V*>(o) = ov;
+    // the group's coarse values: columns (x0 >> 1) .. +NC-1 of the 2x2 coarse rows/planes
+    T cq[4][NC];
+    const T* Q0 = Pc + (x0 >> 1);
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+      cq[0][c] = Q0[c];
+      cq[1][c] = Q0[c + cy];
+      cq[2][c] = Q0[c + cz];
+      cq[3][c] = Q0[c + cy + cz];
+    }
+#pragma unroll
+    for (int m = 0; m < VEC; ++m) {
+      const int x = x0 + m;
+      const int kq = (x >> 1) - (x0 >> 1);
+      const T wx0 = (x & 1) ? T(1) : T(3), wx1 = (x & 1) ? T(3) : T(1);
+      T s = (wx0 * w00) * cq[0][kq];
+      s = s + (wx0 * w10) * cq[1][kq];
+      s = s + (wx0 * w01) * cq[2][kq];
+      s = s + (wx0 * w11) * cq[3][kq];
+      s = s + (wx1 * w00) * cq[0][kq + 1];
+      s = s + (wx1 * w10) * cq[1][kq + 1];
+      s = s + (wx1 * w01) * cq[2][kq + 1];
+      s = s + (wx1 * w11) * cq[3][kq + 1];
+      r[m] = o[m] + s / T(64);
+    }
+    *reinterpret_cast<V*>(Out + x0) = *reinterpret_cast<const V*>(r);
+  }
+  if (lane < 2) {  // ghost columns, evaluated at their mgbound source
+    const int x = lane ? F.nx + 1 : 0;
+    int sx = x;
+    if (x == 0 && (ph & 1)) sx = 1;
+    if (x == F.nx + 1 && (ph & 2)) sx = F.nx;
+    Out[x] = interp(Pc + (x >> 1), sx, ZERO_OLD ? T(0) : Orow[sx]);
+  }
+}
+
+template <typename T>
+cudaError_t launch_prolong_vec(bool zero_old, const BlkLev* fine, const BlkLev* coarse, const Tile* tiles, int ntiles,
+                               const T* phi_c, const T* old, T* out, cudaStream_t st) {
+  if (ntiles <= 0) return cudaSuccess;
+  if (zero_old) k_prolong_vec<T, true><<<ntiles, 256, 0, st>>>(fine, coarse, tiles, phi_c, old, out);
+  else k_prolong_vec<T, false><<<ntiles, 256, 0, st>>>(fine, coarse, tiles, phi_c, old, out);
+  return cudaGetLastError();
+}
+template cudaError_t launch_prolong_vec<double>(bool, const BlkLev*, const BlkLev*, const Tile*, int, const double*,
+                                                const double*, double*, cudaStream_t);
+template cudaError_t launch_prolong_vec<float>(bool, const BlkLev*, const BlkLev*, const Tile*, int, const float*,
+                                               const float*, float*, cudaStream_t);
 
 template <typename T>
 cudaError_t launch_prolong(bool zero_old, const BlkLev* fine, const BlkLev* coarse, RowTab rt, const T* phi_c,

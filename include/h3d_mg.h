@@ -94,6 +94,7 @@ typedef struct h3d_solve_info {
   double smoother_ms;     /* device time in level-1 smoother launches (profiling on) */
   int64_t smoother_launches;
   int64_t kernel_launches;/* kernels this library launched during the solve */
+  double smoother_bytes;  /* algorithmic bytes of the profiled level-1 smoother launches */
 } h3d_solve_info;
 
 /* --- set-up (localparameters.for:202-239, initial.for:329-360, coeff) ---- */

@@ -305,3 +305,28 @@ def test_every_restriction_variant(oracle_mod, h3d, precision):
                     _assert_level(s, orc, 3, "rhs", exact=exact)
         assert tried >= 12 and tma >= 6
         s.close()
+
+
+def test_mixed_vcycle_every_level2_smoother(oracle_mod, h3d):
+    """A mixed-precision V-cycle (FP32 levels, FP64 coarsest) against the FP64
+    oracle V-cycle, with every smoother variant on level 2.  Level 2 starts
+    each cycle from the zero iterate left by the restriction, so this runs the
+    zero-source sweeps too.  Tolerance: 1e-4 of the largest value."""
+    layout = ((2, 2, 1), (32, 32, 32), [P, P, W, W, W, W], 4)
+    blocks, s, orc = _pair(oracle_mod, h3d, layout, precision="mixed")
+    s.coeff(); orc.coeff()
+    _, _, nvar = s.get_smoother(2)
+    rng = np.random.default_rng(21)
+    tried = 0
+    for v in range(nvar):
+        if not s.set_smoother(2, v, 5):
+            continue
+        tried += 1
+        _rand_level(rng, s, orc, 1)
+        s.vcycle()
+        orc.vcycle()
+        for ib in range(len(blocks)):
+            a, b = s.get_level(1, "phi", ib), orc.get_phi(1, ib)
+            np.testing.assert_allclose(a, b, rtol=0, atol=1e-4 * np.abs(b).max(), err_msg="variant %d" % v)
+    assert tried >= 15
+    s.close()
