@@ -1067,15 +1067,15 @@ __global__ void __launch_bounds__(256) k_prolong_pairs(const BlkLev* __restrict_
   }
 }
 
-__global__ void __launch_bounds__(256) k_reduce4(const double* __restrict__ partials, int n, double* __restrict__ out) {
+__global__ void __launch_bounds__(1024) k_reduce4(const double* __restrict__ partials, int n, double* __restrict__ out) {
   double a0 = 0, a1 = 0, a2 = 0, a3 = 0;
-  for (int q = threadIdx.x; q < n; q += 256) {
+  for (int q = threadIdx.x; q < n; q += 1024) {
     a0 += partials[4 * (size_t)q];
     a1 += partials[4 * (size_t)q + 1];
     a2 = fmax(a2, partials[4 * (size_t)q + 2]);
     a3 += partials[4 * (size_t)q + 3];
   }
-  block_reduce4<256>(a0, a1, a2, a3, out);
+  block_reduce4<1024>(a0, a1, a2, a3, out);
 }
 
 __global__ void __launch_bounds__(256) k_sum_interior(const BlkLev* __restrict__ bls, const int* __restrict__ cta_start,
@@ -1370,9 +1370,19 @@ __global__ void __launch_bounds__(TPR*(TY + 2)) k_rbgs_win(const BlkLev* __restr
   const float an = (y == ny && (ph & 8)) ? 0.f : ay;
   const float aw0 = (x0 == 1 && (ph & 1)) ? 0.f : ax;
   const float ae3 = (rgt && (ph & 2)) ? 0.f : ax;
-  const float inv0 = 1.f / (-(aw0 + ax + as + an + az + az));
-  const float inv3 = 1.f / (-(ax + ae3 + as + an + az + az));
-  const float inv12 = 1.f / (-(ax + ax + as + an + az + az));
+  // diagonal reciprocals of the three kinds of cells of a group, on interior
+  // planes [0], the bottom wall plane [1], the top wall plane [2] and a plane
+  // that is both [3] (nz = 1); no division inside the z march
+  auto rcp3 = [&](float ab, float at, float& i0, float& i3, float& i12) {
+    i0 = 1.f / (-(aw0 + ax + as + an + ab + at));
+    i3 = 1.f / (-(ax + ae3 + as + an + ab + at));
+    i12 = 1.f / (-(ax + ax + as + an + ab + at));
+  };
+  float inv0, inv3, inv12, inv0b, inv3b, inv12b, inv0t, inv3t, inv12t, inv0bt, inv3bt, inv12bt;
+  rcp3(az, az, inv0, inv3, inv12);
+  rcp3(0.f, az, inv0b, inv3b, inv12b);
+  rcp3(az, 0.f, inv0t, inv3t, inv12t);
+  rcp3(0.f, 0.f, inv0bt, inv3bt, inv12bt);
 
   if (leader) {
     for (int q = 0; q < NS; ++q)
@@ -1417,12 +1427,10 @@ __global__ void __launch_bounds__(TPR*(TY + 2)) k_rbgs_win(const BlkLev* __restr
                     const float4& rh, float l, float r, int z, int q) {
     const bool wlo = z == 1 && (ph & 16), whi = z == nz && (ph & 32);
     const float ab = wlo ? 0.f : az, at = whi ? 0.f : az;
-    float i0 = inv0, i3 = inv3, i12 = inv12;
-    if (wlo || whi) {  // wall plane: the diagonal changes
-      i0 = 1.f / (-(aw0 + ax + as + an + ab + at));
-      i3 = 1.f / (-(ax + ae3 + as + an + ab + at));
-      i12 = 1.f / (-(ax + ax + as + an + ab + at));
-    }
+    // wall planes change the diagonal
+    const float i0 = wlo ? (whi ? inv0bt : inv0b) : (whi ? inv0t : inv0);
+    const float i3 = wlo ? (whi ? inv3bt : inv3b) : (whi ? inv3t : inv3);
+    const float i12 = wlo ? (whi ? inv12bt : inv12b) : (whi ? inv12t : inv12);
     if (q == 0) {
       c.x = upd(l, c.y, u.x, dn.x, bz.x, tz.x, rh.x, aw0, ax, as, an, ab, at, i0);
       c.z = upd(c.y, c.w, u.z, dn.z, bz.z, tz.z, rh.z, ax, ax, as, an, ab, at, i12);
@@ -1540,14 +1548,14 @@ static cudaError_t win_dispatch(bool zero, const BlkLev* bl, const Tile* tiles, 
 constexpr int kFirstWinShape = 40;
 // (variant, lanes per row, rows, ring slots, prefetch depth)
 #define H3D_WIN_SHAPES(X) \
-  X(40, 32, 4, 6, 3)      \
-  X(41, 32, 8, 6, 3)      \
-  X(42, 32, 16, 5, 2)     \
+  X(40, 32, 4, 8, 5)      \
+  X(41, 32, 8, 8, 4)      \
+  X(42, 32, 16, 8, 4)     \
   X(43, 32, 8, 8, 5)      \
-  X(44, 16, 8, 6, 3)      \
-  X(45, 16, 16, 6, 3)     \
-  X(46, 8, 16, 6, 3)      \
-  X(47, 4, 16, 6, 3)
+  X(44, 16, 8, 8, 5)      \
+  X(45, 16, 16, 8, 4)     \
+  X(46, 8, 16, 8, 5)      \
+  X(47, 4, 16, 8, 5)
 
 // (variant, threads per row, groups of four cells per thread, rows, ring slots, prefetch depth)
 #define H3D_VEC_SHAPES(X)  \
@@ -1675,9 +1683,9 @@ cudaError_t launch_restrict(bool var, bool zero_phi, const BlkLev* fine, const B
   return cudaGetLastError();
 }
 
-// mgcorr + mgbound, tiled and vectorised: a CTA owns 8 consecutive fine rows
-// (y0 .. y0+7, ghost rows included) of one plane z of one block, a warp one
-// row; a lane takes groups of VEC = 16/sizeof(T) interior cells (x0 = 1 +
+// mgcorr + mgbound, tiled and vectorised: a CTA owns kProlongRows (32)
+// consecutive fine rows (ghost rows included) of one plane z of one block, a
+// warp every eighth row; a lane takes groups of VEC = 16/sizeof(T) interior cells (x0 = 1 +
 // VEC*g, a 16-byte aligned address in the padded layout: one vector load of
 // the old iterate and one vector store), lanes 0 and 1 the ghost columns.
 // Same interpolation, term order and mgbound source as k_prolong_pairs.
@@ -1693,9 +1701,9 @@ __global__ void __launch_bounds__(256) k_prolong_vec(const BlkLev* __restrict__ 
   const BlkLev F = fine[t.b];
   const BlkLev C = coarse[t.b];
   const int lane = threadIdx.x & 31;
-  const int y = t.y0 + (threadIdx.x >> 5), z = t.z0;
-  if (y > F.ny + 1) return;
+  const int z = t.z0;
   const int ph = F.phys;
+  for (int y = t.y0 + (threadIdx.x >> 5); y <= min(t.y0 + kProlongRows - 1, F.ny + 1); y += 8) {
   int sy = y, sz = z;
   if (y == 0 && (ph & 4)) sy = 1;
   if (y == F.ny + 1 && (ph & 8)) sy = F.ny;
@@ -1722,6 +1730,23 @@ __global__ void __launch_bounds__(256) k_prolong_vec(const BlkLev* __restrict__ 
     s = s + (wx1 * w11) * Q[1 + cy + cz];
     return o + s / T(64);
   };
+  // the eight interpolation weights of odd (x0 = 1 + VEC*g + even m) and even
+  // fine columns, products of small integers, exact in either precision
+  T wo[8], we[8];
+  {
+    const T a[4] = {w00, w10, w01, w11};
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      wo[q] = T(1) * a[q];
+      wo[4 + q] = T(3) * a[q];
+      we[q] = T(3) * a[q];
+      we[4 + q] = T(1) * a[q];
+    }
+  }
+  const T* R00 = Pc;
+  const T* R10 = Pc + cy;
+  const T* R01 = Pc + cz;
+  const T* R11 = Pc + cy + cz;
   const int ng = F.nx / VEC;
   for (int g = lane; g < ng; g += 32) {
     const int x0 = 1 + VEC * g;
@@ -1735,28 +1760,41 @@ __global__ void __launch_bounds__(256) k_prolong_vec(const BlkLev* __restrict__ 
     *reinterpret_cast<V*>(o) = ov;
     // the group's coarse values: columns (x0 >> 1) .. +NC-1 of the 2x2 coarse rows/planes
     T cq[4][NC];
-    const T* Q0 = Pc + (x0 >> 1);
+    const int c0 = x0 >> 1;
 #pragma unroll
     for (int c = 0; c < NC; ++c) {
-      cq[0][c] = Q0[c];
-      cq[1][c] = Q0[c + cy];
-      cq[2][c] = Q0[c + cz];
-      cq[3][c] = Q0[c + cy + cz];
+      cq[0][c] = R00[c0 + c];
+      cq[1][c] = R10[c0 + c];
+      cq[2][c] = R01[c0 + c];
+      cq[3][c] = R11[c0 + c];
     }
 #pragma unroll
     for (int m = 0; m < VEC; ++m) {
-      const int x = x0 + m;
-      const int kq = (x >> 1) - (x0 >> 1);
-      const T wx0 = (x & 1) ? T(1) : T(3), wx1 = (x & 1) ? T(3) : T(1);
-      T s = (wx0 * w00) * cq[0][kq];
-      s = s + (wx0 * w10) * cq[1][kq];
-      s = s + (wx0 * w01) * cq[2][kq];
-      s = s + (wx0 * w11) * cq[3][kq];
-      s = s + (wx1 * w00) * cq[0][kq + 1];
-      s = s + (wx1 * w10) * cq[1][kq + 1];
-      s = s + (wx1 * w01) * cq[2][kq + 1];
-      s = s + (wx1 * w11) * cq[3][kq + 1];
-      r[m] = o[m] + s / T(64);
+      const int kq = (m + 1) >> 1;  // (x >> 1) - (x0 >> 1) for x = x0 + m, x0 odd
+      const T* W = (m & 1) ? we : wo;  // x0 + m odd for even m
+      // term order (di,dj,dk): 000, 010, 001, 011, 100, 110, 101, 111 (mgsolver.for:838-892)
+      T s;
+      if (sizeof(T) == 8) {
+        s = W[0] * cq[0][kq];
+        s = s + W[1] * cq[1][kq];
+        s = s + W[2] * cq[2][kq];
+        s = s + W[3] * cq[3][kq];
+        s = s + W[4] * cq[0][kq + 1];
+        s = s + W[5] * cq[1][kq + 1];
+        s = s + W[6] * cq[2][kq + 1];
+        s = s + W[7] * cq[3][kq + 1];
+        r[m] = o[m] + s / T(64);
+      } else {  // FP32 inner solve: fused multiply-adds
+        s = W[0] * cq[0][kq];
+        s = fma(W[1], cq[1][kq], s);
+        s = fma(W[2], cq[2][kq], s);
+        s = fma(W[3], cq[3][kq], s);
+        s = fma(W[4], cq[0][kq + 1], s);
+        s = fma(W[5], cq[1][kq + 1], s);
+        s = fma(W[6], cq[2][kq + 1], s);
+        s = fma(W[7], cq[3][kq + 1], s);
+        r[m] = fma(s, T(1.0 / 64), o[m]);
+      }
     }
     *reinterpret_cast<V*>(Out + x0) = *reinterpret_cast<const V*>(r);
   }
@@ -1766,6 +1804,7 @@ __global__ void __launch_bounds__(256) k_prolong_vec(const BlkLev* __restrict__ 
     if (x == 0 && (ph & 1)) sx = 1;
     if (x == F.nx + 1 && (ph & 2)) sx = F.nx;
     Out[x] = interp(Pc + (x >> 1), sx, ZERO_OLD ? T(0) : Orow[sx]);
+  }
   }
 }
 
@@ -1796,6 +1835,97 @@ int defect_grid(int nrows) {
   int g = (nrows + 7) / 8;
   return g < 1 ? 1 : (g > kDefectCtas ? kDefectCtas : g);
 }
+
+// The same defect, tiled and vectorised: one CTA per tile (kProlongRows
+// consecutive rows of one plane, ghost rows and planes included; a warp every
+// eighth row), a lane pairs of cells (x0, x0+1), x0 = 1 + 2g, with 16-byte
+// loads of p and b (8-byte of e) and stores of p_next and rhs_out; the cells
+// left and right of a pair are read singly, the ghost columns by lanes 0, 1.
+// Same residual arithmetic as k_defect; per-CTA partial sums in a fixed order.
+// Needs nx even and constant coefficients.
+template <typename TE, typename TR, bool HAS_E>
+__global__ void __launch_bounds__(256) k_defect_vec(const BlkLev* __restrict__ bls, const Tile* __restrict__ tiles,
+                                                    int ntiles, const double* __restrict__ p,
+                                                    const TE* __restrict__ e, double* __restrict__ p_next,
+                                                    const double* __restrict__ bvec, TR* __restrict__ rhs_out,
+                                                    double mean_b, double rscale, double* __restrict__ partials) {
+  using E2 = typename std::conditional<sizeof(TE) == 4, float2, double2>::type;
+  using R2 = typename std::conditional<sizeof(TR) == 4, float2, double2>::type;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  double rr = 0, bb = 0, rm = 0, rs = 0;
+  const Tile t = tiles[blockIdx.x];
+  const BlkLev B = bls[t.b];
+  const int z = t.z0;
+  for (int y = t.y0 + w; y <= min(t.y0 + kProlongRows - 1, B.ny + 1); y += 8) {
+    const bool row_in = y >= 1 && y <= B.ny && z >= 1 && z <= B.nz;
+    const long long rowg = B.off + (long long)z * B.sxy + (long long)y * B.sx;
+    auto pv = [&](long long j) -> double {
+      if (HAS_E) return p[j] + (double)e[j];
+      return p[j];
+    };
+    auto pv2 = [&](long long j) -> double2 {  // j: 16-byte aligned pair
+      double2 a = *reinterpret_cast<const double2*>(p + j);
+      if (HAS_E) {
+        const E2 d = *reinterpret_cast<const E2*>(e + j);
+        a.x = a.x + (double)d.x;
+        a.y = a.y + (double)d.y;
+      }
+      return a;
+    };
+    const int ng = B.nx >> 1;
+    for (int g = lane; g < ng; g += 32) {
+      const int x0 = 1 + 2 * g;
+      const long long i = rowg + x0;
+      const double2 pc = pv2(i);
+      if (HAS_E) *reinterpret_cast<double2*>(p_next + i) = pc;
+      if (!row_in) continue;
+      const double2 so = pv2(i - B.sx), no = pv2(i + B.sx), bo = pv2(i - B.sxy), to = pv2(i + B.sxy);
+      const double wv = pv(i - 1), ev = pv(i + 2);
+      const double2 bv = *reinterpret_cast<const double2*>(bvec + i);
+      const Coef<double> c0 = cell_coef<double, false>(B, x0, y, z, i - B.off, nullptr, nullptr, nullptr);
+      const Coef<double> c1 = cell_coef<double, false>(B, x0 + 1, y, z, i + 1 - B.off, nullptr, nullptr, nullptr);
+      const double ap0 = coef_ap(c0), ap1 = coef_ap(c1);
+      const double r0 = bv.x - (c0.aw * wv + c0.ae * pc.y + c0.as * so.x + c0.an * no.x + c0.ab * bo.x +
+                                c0.at * to.x + ap0 * pc.x);
+      const double r1 = bv.y - (c1.aw * pc.x + c1.ae * ev + c1.as * so.y + c1.an * no.y + c1.ab * bo.y +
+                                c1.at * to.y + ap1 * pc.y);
+      R2 ro;
+      ro.x = (TR)(r0 - mean_b);
+      ro.y = (TR)(r1 - mean_b);
+      *reinterpret_cast<R2*>(rhs_out + i) = ro;
+      rr += r0 * r0;
+      rr += r1 * r1;
+      bb += bv.x * bv.x;
+      bb += bv.y * bv.y;
+      rm = fmax(rm, fabs(r0) * rscale);
+      rm = fmax(rm, fabs(r1) * rscale);
+      rs += r0;
+      rs += r1;
+    }
+    if (HAS_E && lane < 2) {  // ghost columns: p += e only
+      const long long i = rowg + (lane ? B.nx + 1 : 0);
+      p_next[i] = pv(i);
+    }
+  }
+  block_reduce4<256>(rr, bb, rm, rs, partials + 4 * (size_t)blockIdx.x);
+}
+
+template <typename TE, typename TR>
+cudaError_t launch_defect_vec(const BlkLev* bl, const Tile* tiles, int ntiles, const double* p, const TE* e,
+                              double* p_next, const double* b, TR* rhs_out, double mean_b, double rscale,
+                              double* partials, int grid, cudaStream_t st) {
+  if (ntiles <= 0) return cudaSuccess;
+  grid = ntiles;  // one tile per CTA (partials holds one quadruple per tile)
+  if (e) k_defect_vec<TE, TR, true><<<grid, 256, 0, st>>>(bl, tiles, ntiles, p, e, p_next, b, rhs_out, mean_b, rscale, partials);
+  else k_defect_vec<TE, TR, false><<<grid, 256, 0, st>>>(bl, tiles, ntiles, p, e, p_next, b, rhs_out, mean_b, rscale, partials);
+  return cudaGetLastError();
+}
+template cudaError_t launch_defect_vec<double, double>(const BlkLev*, const Tile*, int, const double*, const double*,
+                                                       double*, const double*, double*, double, double, double*, int,
+                                                       cudaStream_t);
+template cudaError_t launch_defect_vec<float, float>(const BlkLev*, const Tile*, int, const double*, const float*,
+                                                     double*, const double*, float*, double, double, double*, int,
+                                                     cudaStream_t);
 
 template <typename TE, typename TR>
 cudaError_t launch_defect(bool var, const BlkLev* bl, RowTab rt, const double* p, const TE* e, double* p_next,
@@ -2121,7 +2251,7 @@ cudaError_t launch_stage(bool to_device, double* stg, int tx, int ty, int pl, in
 }
 
 cudaError_t launch_reduce4(const double* partials, int n, double* out, cudaStream_t st) {
-  k_reduce4<<<1, 256, 0, st>>>(partials, n, out);
+  k_reduce4<<<1, 1024, 0, st>>>(partials, n, out);
   return cudaGetLastError();
 }
 

@@ -100,11 +100,19 @@ cudaError_t launch_restrict(bool var, bool zero_phi, const BlkLev* fine, const B
 template <typename T>
 cudaError_t launch_prolong(bool zero_old, const BlkLev* fine, const BlkLev* coarse, RowTab rt,
                            const T* phi_c, const T* old, T* out, cudaStream_t st);
-// Same, tiled: tiles (b, 0, y0, z) of 8 fine rows (ghost rows included) of
-// plane z; needs every block's nx to be a multiple of 16/sizeof(T).
+// Same, tiled: tiles (b, 0, y0, z) of kProlongRows fine rows (ghost rows
+// included) of plane z; needs every block's nx to be a multiple of 16/sizeof(T).
+constexpr int kProlongRows = 32;
 template <typename T>
 cudaError_t launch_prolong_vec(bool zero_old, const BlkLev* fine, const BlkLev* coarse, const Tile* tiles, int ntiles,
                                const T* phi_c, const T* old, T* out, cudaStream_t st);
+
+// Tiled defect (constant coefficients, nx even): tiles of kProlongRows rows of
+// one plane (the level's prolongation tiles), one CTA and partial sum each.
+template <typename TE, typename TR>
+cudaError_t launch_defect_vec(const BlkLev* bl, const Tile* tiles, int ntiles, const double* p, const TE* e,
+                              double* p_next, const double* b, TR* rhs_out, double mean_b, double rscale,
+                              double* partials, int grid, cudaStream_t st);
 
 // Level-1 FP64 defect: pn = p + e (all cells, when e != null), r = b - A pn on
 // the interior, rhs_out = r - mean_b (as TR), per-CTA partial sums

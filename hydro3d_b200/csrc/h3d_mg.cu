@@ -63,7 +63,7 @@ struct Level {
   CUtensorMap* d_maps = nullptr;  // [ty index][0,1: iterate buffer, 2: rhs][block] tensor maps
   CUtensorMap* d_rmaps = nullptr;  // as the fine level of a restriction: [tyc index][0,1: iterate, 2: rhs][block]
   Tile* d_rtiles = nullptr;       // restriction tiles (this level as the coarse level)
-  Tile* d_ptiles = nullptr;       // prolongation tiles (8 rows of one plane, ghosts included; this level as the fine one)
+  Tile* d_ptiles = nullptr;       // prolongation / defect tiles (kProlongRows rows of one plane, ghosts included)
   int nptiles = 0;
   bool pvec32 = false, pvec64 = false;  // every block's nx a multiple of 4 (FP32) / 2 (FP64) cells
   int nrtiles = 0, rvariant = 0, rzc = 1;
@@ -534,26 +534,37 @@ struct Exec {
     const double* fz = h->var ? V.fz64 : nullptr;
     double* pin = h->p64[h->pc];
     double* pout = h->p64[1 - h->pc];
+    // the tiled kernel needs the level's 8-row tiles and constant coefficients
+    const bool tiled = V.d_ptiles && V.pvec64 && !h->var;
+    const int ngrid = tiled ? V.nptiles : defect_grid(ct.nrows);
     if (h->mixed) {
       const float* e = nullptr;
       if (with_e) {
         if (V.zero32) TRY(materialize_zero32(1));
         e = V.phi32[V.cur32];
       }
-      CU(launch_defect<float, float>(h->var, V.d_bl, ct, pin, e, pout, h->b64, V.rhs32, h->mean_b, rscale, fx, fy, fz,
-                                     h->partials, h->st));
+      if (tiled)
+        CU(launch_defect_vec<float, float>(V.d_bl, V.d_ptiles, V.nptiles, pin, e, pout, h->b64, V.rhs32, h->mean_b,
+                                           rscale, h->partials, ngrid, h->st));
+      else
+        CU(launch_defect<float, float>(h->var, V.d_bl, ct, pin, e, pout, h->b64, V.rhs32, h->mean_b, rscale, fx, fy,
+                                       fz, h->partials, h->st));
     } else {
       const double* e = nullptr;
       if (with_e) {
         if (V.zero64) TRY(materialize_zero64(1));
         e = V.phi64[V.cur64];
       }
-      CU(launch_defect<double, double>(h->var, V.d_bl, ct, pin, e, pout, h->b64, V.rhs64, h->mean_b, rscale, fx, fy,
-                                       fz, h->partials, h->st));
+      if (tiled)
+        CU(launch_defect_vec<double, double>(V.d_bl, V.d_ptiles, V.nptiles, pin, e, pout, h->b64, V.rhs64,
+                                             h->mean_b, rscale, h->partials, ngrid, h->st));
+      else
+        CU(launch_defect<double, double>(h->var, V.d_bl, ct, pin, e, pout, h->b64, V.rhs64, h->mean_b, rscale, fx,
+                                         fy, fz, h->partials, h->st));
     }
     TRY(chk("defect", 1));
     if (with_e) h->pc = 1 - h->pc;
-    CU(launch_reduce4(h->partials, defect_grid(ct.nrows), h->d_res, h->st));
+    CU(launch_reduce4(h->partials, ngrid, h->d_res, h->st));
     TRY(chk("reduce", 1));
     CU(cudaMemcpyAsync(h->h_res, h->d_res, 4 * sizeof(double), cudaMemcpyDeviceToHost, h->st));
     h->kernels += 2;
@@ -1207,7 +1218,7 @@ int h3d_mg_create(h3d_mg** out, const h3d_mg_desc* desc) {
     }
     V.f32 = f32_level(h, g);
     V.var = h->var;
-    if (g < h->L) {  // prolongation tiles: 8 fine rows of one plane, ghost rows and planes included
+    if (g < h->L) {  // prolongation tiles: kProlongRows fine rows of one plane, ghost rows and planes included
       std::vector<Tile> pt;
       V.pvec32 = V.pvec64 = true;
       for (size_t b = 0; b < V.geom.bl.size(); ++b) {
@@ -1215,7 +1226,7 @@ int h3d_mg_create(h3d_mg** out, const h3d_mg_desc* desc) {
         V.pvec32 = V.pvec32 && B.nx % 4 == 0;
         V.pvec64 = V.pvec64 && B.nx % 2 == 0;
         for (int z = 0; z <= B.nz + 1; ++z)
-          for (int y0 = 0; y0 <= B.ny + 1; y0 += 8) pt.push_back(Tile{(int)b, 0, y0, z});
+          for (int y0 = 0; y0 <= B.ny + 1; y0 += kProlongRows) pt.push_back(Tile{(int)b, 0, y0, z});
       }
       if ((rc = dalloc(h, &V.d_ptiles, pt.size())) != H3D_OK) return bail(rc);
       if (cudaMemcpy(V.d_ptiles, pt.data(), pt.size() * sizeof(Tile), cudaMemcpyHostToDevice) != cudaSuccess)
@@ -1235,7 +1246,7 @@ int h3d_mg_create(h3d_mg** out, const h3d_mg_desc* desc) {
   const size_t n1 = (size_t)h->lev[1].geom.n_elems;
   if ((rc = dalloc(h, &h->p64[0], n1)) || (rc = dalloc(h, &h->p64[1], n1)) || (rc = dalloc(h, &h->b64, n1)))
     return bail(rc);
-  h->npartials = std::max(std::max(h->lev[1].ncta_all, h->lev[1].ncta_int), kDefectCtas);
+  h->npartials = std::max(std::max(std::max(h->lev[1].ncta_all, h->lev[1].ncta_int), kDefectCtas), h->lev[1].nptiles);
   if ((rc = dalloc(h, &h->partials, 4 * (size_t)h->npartials)) || (rc = dalloc(h, &h->d_res, 4))) return bail(rc);
   if (cudaMallocHost((void**)&h->h_res, 4 * sizeof(double)) != cudaSuccess)
     return bail(fail(h, H3D_ERR_OOM, "pinned result buffer"));
