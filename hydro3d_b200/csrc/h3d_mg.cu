@@ -866,7 +866,7 @@ int flush_l2(h3d_mg* h) {
 int autotune_level(h3d_mg* h, int g) {
   Level& V = h->lev[g];
   int best_v = V.variant, best_z = V.zc;
-  if (V.geom.n_interior < (1 << 12)) return H3D_OK;  // tiny levels: heuristic
+  if (V.geom.n_interior < 64) return H3D_OK;  // a handful of cells: heuristic
   int nzm = 0, nxm = 0, nym = 0;
   for (const auto& B : V.geom.bl) { nzm = std::max(nzm, B.nz); nxm = std::max(nxm, B.nx); nym = std::max(nym, B.ny); }
   cudaEvent_t a, b;
@@ -877,8 +877,8 @@ int autotune_level(h3d_mg* h, int g) {
   for (int v = 0; v < num_tile_shapes(); ++v) {
     TileShape s = tile_shape(v);
     if (!variant_fits(V, v)) continue;
-    if (s.rows ? (s.tx >= 4 * nxm) : (s.tx > 2 * nxm || s.ty > 2 * nym || s.tx < 8)) continue;
-    for (int zc : {2, 4, 8, 16, 32, 64, 128, 256}) {
+    if (s.rows ? (s.tx >= 4 * nxm) : (s.tx > 2 * nxm || s.ty > 2 * nym || (s.tx < 8 && nxm >= 32))) continue;
+    for (int zc : {1, 2, 4, 8, 16, 32, 64, 128, 256}) {
       if (zc > nzm || (zc < 8 && V.geom.n_interior >= (1 << 20))) continue;
       TRY(build_tiles(h, V, v, zc));
       float tot = 1e30f;  // fastest of the timed repetitions (robust to interference)
@@ -915,11 +915,11 @@ int autotune_level(h3d_mg* h, int g) {
 }
 
 // Times every restriction variant and coarse z-chunk that fits the level
-// pair (fine level gc-1 with at least 2^12 cells) and keeps the fastest.
+// pair (fine level gc-1 with at least 64 cells) and keeps the fastest.
 int autotune_restrict(h3d_mg* h, int gc) {
   Level& F = h->lev[gc - 1];
   Level& C = h->lev[gc];
-  if (F.geom.n_interior < (1 << 12)) return H3D_OK;
+  if (F.geom.n_interior < 64) return H3D_OK;
   int nxm = 0, nzm = 0;
   for (const auto& B : C.geom.bl) { nxm = std::max(nxm, B.nx); nzm = std::max(nzm, B.nz); }
   const bool f32 = F.f32;
