@@ -379,7 +379,7 @@ REF_CYCLES = {1: 45, 2: 30, 3: 54, 4: 60, 5: 60}
 
 def read_profile_traffic():
     """DRAM bytes per smoother launch from the committed ncu summary, if any."""
-    p = os.path.join(ROOT, "profiles", "k_rbgs_tma_fp32_config3.md")
+    p = os.path.join(ROOT, "profiles", "k_rbgs_win_fp32_config3.md")
     if not os.path.exists(p):
         return None
     for ln in open(p):
