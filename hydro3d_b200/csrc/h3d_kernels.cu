@@ -6,6 +6,7 @@
 // 7-point stencil is not a contraction; no tensor cores are used).
 #include <algorithm>
 #include <cstdint>
+#include <cstdlib>
 
 #include <type_traits>
 
@@ -14,6 +15,40 @@
 namespace h3d {
 
 namespace {
+
+// Programmatic dependent launch (opt-in, H3D_PDL=1 in the environment): every
+// kernel lets the next one on the stream start launching at once
+// (griddepcontrol.launch_dependents) and waits for its predecessors to
+// complete (griddepcontrol.wait) before it touches data they write.  Both are
+// no-ops for a kernel launched without the attribute.  Off by default: on the
+// 33.5M-cell solve it measured 60.1 ms against 56.1 ms without (the early
+// launched grids hold SM resources the running ones need).
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory"); }
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
+
+static bool pdl_enabled() {
+  static const bool on = [] {
+    const char* v = std::getenv("H3D_PDL");
+    return v && v[0] == '1';
+  }();
+  return on;
+}
+
+template <typename... KArgs, typename... Args>
+static cudaError_t pdl_launch(void (*k)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+                              Args... args) {
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = pdl_enabled() ? 1 : 0;
+  return cudaLaunchKernelEx(&cfg, k, static_cast<KArgs>(args)...);
+}
 
 __device__ __forceinline__ int find_block(const int* __restrict__ start, int nb, int cta) {
   int lo = 0, hi = nb;  // start[lo] <= cta < start[hi]
@@ -104,6 +139,8 @@ __global__ void __launch_bounds__(NT) k_rbgs(const BlkLev* __restrict__ bls, con
                                              int zc, const T* __restrict__ src, T* __restrict__ dst,
                                              const T* __restrict__ rhs, const T* __restrict__ fx,
                                              const T* __restrict__ fy, const T* __restrict__ fz) {
+  pdl_trigger();
+  pdl_wait();
   constexpr int RX = TX + 4, RY = TY + 4, RN = RX * RY;
   constexpr int R1X = TX + 2, R1N = (TX + 2) * (TY + 2);
   __shared__ T ring[4][RN];
@@ -263,6 +300,8 @@ __global__ void __launch_bounds__(TPR*(TY + 2)) k_rbgs_rows(const BlkLev* __rest
                                                            const T* __restrict__ src, T* __restrict__ dst,
                                                            const T* __restrict__ rhs, const T* __restrict__ fx,
                                                            const T* __restrict__ fy, const T* __restrict__ fz) {
+  pdl_trigger();
+  pdl_wait();
   constexpr int SP = 2 * CP * TPR + 4;
   constexpr int SR = TY + 4;
   constexpr int PL = SR * SP;
@@ -429,6 +468,8 @@ __global__ void __launch_bounds__(TPR*(TY + 2)) k_rbgs_tma2(const BlkLev* __rest
                                                            T* __restrict__ dst, const T* __restrict__ fx,
                                                            const T* __restrict__ fy, const T* __restrict__ fz,
                                                            int* err) {
+  pdl_trigger();
+  pdl_wait();
   using C = Tma2Cfg<T, TPR, CP, TY, D>;
   constexpr int NS = C::NS;
   extern __shared__ unsigned char smem_raw[];
@@ -573,6 +614,8 @@ __global__ void __launch_bounds__(TPR*(TY + 2)) k_rbgs_vec(const BlkLev* __restr
                                                           const CUtensorMap* __restrict__ maps,
                                                           const CUtensorMap* __restrict__ rmaps,
                                                           float* __restrict__ dst, int* err) {
+  pdl_trigger();
+  pdl_wait();
   using C = VecCfg<TPR, GPT, TY, NS, D>;
   static_assert(D + 4 <= NS, "a plane is read until three phases after its own");
   extern __shared__ unsigned char smem_raw[];
@@ -725,6 +768,8 @@ __global__ void __launch_bounds__(TPR*(TY + 2)) k_rbgs_vec(const BlkLev* __restr
 template <typename T, bool ZERO_OLD>
 __global__ void k_fill(const uint32_t* __restrict__ dsts, const uint32_t* __restrict__ srcs, int64_t n,
                        T* __restrict__ out, const T* __restrict__ cur, const T* __restrict__ old) {
+  pdl_trigger();
+  pdl_wait();
   for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
     uint32_t s = __ldg(srcs + e);
     T v;
@@ -762,6 +807,8 @@ __global__ void __launch_bounds__(256) k_restrict(const BlkLev* __restrict__ fin
                                                   const T* __restrict__ phi, const T* __restrict__ rhs,
                                                   T* __restrict__ rhs_c, const T* __restrict__ fx,
                                                   const T* __restrict__ fy, const T* __restrict__ fz) {
+  pdl_trigger();
+  pdl_wait();
   const int lane = threadIdx.x & 31;
   for (int rid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; rid < nrows; rid += (gridDim.x * blockDim.x) >> 5) {
     const RowRef rr = row_of(coarse, row_start, nb, rid, true);
@@ -809,6 +856,8 @@ __global__ void __launch_bounds__(256) k_prolong(const BlkLev* __restrict__ fine
                                                  const int* __restrict__ row_start, int nb, int nrows,
                                                  const T* __restrict__ phi_c, const T* __restrict__ old,
                                                  T* __restrict__ out) {
+  pdl_trigger();
+  pdl_wait();
   const int lane = threadIdx.x & 31;
   for (int rid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; rid < nrows; rid += (gridDim.x * blockDim.x) >> 5) {
     const RowRef rr = row_of(fine, row_start, nb, rid, false);
@@ -882,6 +931,8 @@ __global__ void __launch_bounds__(256) k_defect(const BlkLev* __restrict__ bls, 
                                                 double mean_b, double rscale, const double* __restrict__ fx,
                                                 const double* __restrict__ fy, const double* __restrict__ fz,
                                                 double* __restrict__ partials) {
+  pdl_trigger();
+  pdl_wait();
   const int lane = threadIdx.x & 31;
   double rr = 0, bb = 0, rm = 0, rs = 0;
   for (int rid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; rid < nrows; rid += (gridDim.x * blockDim.x) >> 5) {
@@ -930,6 +981,8 @@ __global__ void __launch_bounds__(TPR* TYC) k_restrict_tile(const BlkLev* __rest
                                                            const T* __restrict__ phi, const T* __restrict__ rhs,
                                                            T* __restrict__ rhs_c, const T* __restrict__ fx,
                                                            const T* __restrict__ fy, const T* __restrict__ fz) {
+  pdl_trigger();
+  pdl_wait();
   constexpr int SP = 2 * CPX * TPR + 4;
   constexpr int SR = 2 * TYC + 2;
   constexpr int PL = SR * SP;
@@ -1014,6 +1067,8 @@ __global__ void __launch_bounds__(256) k_prolong_pairs(const BlkLev* __restrict_
                                                        const int* __restrict__ row_start, int nb, int nrows,
                                                        const T* __restrict__ phi_c, const T* __restrict__ old,
                                                        T* __restrict__ out) {
+  pdl_trigger();
+  pdl_wait();
   const int lane = threadIdx.x & 31;
   for (int rid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; rid < nrows; rid += (gridDim.x * blockDim.x) >> 5) {
     const RowRef rr = row_of(fine, row_start, nb, rid, false);
@@ -1068,6 +1123,8 @@ __global__ void __launch_bounds__(256) k_prolong_pairs(const BlkLev* __restrict_
 }
 
 __global__ void __launch_bounds__(1024) k_reduce4(const double* __restrict__ partials, int n, double* __restrict__ out) {
+  pdl_trigger();
+  pdl_wait();
   double a0 = 0, a1 = 0, a2 = 0, a3 = 0;
   for (int q = threadIdx.x; q < n; q += 1024) {
     a0 += partials[4 * (size_t)q];
@@ -1081,6 +1138,8 @@ __global__ void __launch_bounds__(1024) k_reduce4(const double* __restrict__ par
 __global__ void __launch_bounds__(256) k_sum_interior(const BlkLev* __restrict__ bls, const int* __restrict__ cta_start,
                                                       int nb, const double* __restrict__ a,
                                                       double* __restrict__ partials) {
+  pdl_trigger();
+  pdl_wait();
   const int b = find_block(cta_start, nb, blockIdx.x);
   const BlkLev B = bls[b];
   const int local = (blockIdx.x - cta_start[b]) * blockDim.x + threadIdx.x;
@@ -1093,16 +1152,22 @@ __global__ void __launch_bounds__(256) k_sum_interior(const BlkLev* __restrict__
 }
 
 __global__ void k_shift(double* __restrict__ a, int64_t n, const double* __restrict__ s, double scale) {
+  pdl_trigger();
+  pdl_wait();
   const double v = s[0] * scale;
   for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x)
     a[q] = a[q] - v;
 }
 
 __global__ void k_d2f(const double* __restrict__ a, float* __restrict__ b, int64_t n) {
+  pdl_trigger();
+  pdl_wait();
   for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x)
     b[q] = (float)a[q];
 }
 __global__ void k_f2d(const float* __restrict__ a, double* __restrict__ b, int64_t n) {
+  pdl_trigger();
+  pdl_wait();
   for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x)
     b[q] = (double)a[q];
 }
@@ -1112,6 +1177,8 @@ __global__ void k_f2d(const float* __restrict__ a, double* __restrict__ b, int64
 __global__ void __launch_bounds__(256) k_dens_restrict(const BlkLev* __restrict__ fine, const BlkLev* __restrict__ coarse,
                                                        const int* __restrict__ cta_start, int nb,
                                                        const double* __restrict__ df, double* __restrict__ dc) {
+  pdl_trigger();
+  pdl_wait();
   const int b = find_block(cta_start, nb, blockIdx.x);
   const BlkLev C = coarse[b], F = fine[b];
   const int local = (blockIdx.x - cta_start[b]) * blockDim.x + threadIdx.x;
@@ -1131,6 +1198,8 @@ __global__ void __launch_bounds__(256) k_face_coef(const BlkLev* __restrict__ bl
                                                    int nb, const double* __restrict__ dens,
                                                    const double* __restrict__ h3, double* __restrict__ fx,
                                                    double* __restrict__ fy, double* __restrict__ fz) {
+  pdl_trigger();
+  pdl_wait();
   const int b = find_block(cta_start, nb, blockIdx.x);
   const BlkLev B = bls[b];
   const int local = (blockIdx.x - cta_start[b]) * blockDim.x + threadIdx.x;
@@ -1229,11 +1298,11 @@ static cudaError_t rbgs_dispatch(bool var, bool zero, const BlkLev* bl, const Ti
   if (ntiles <= 0) return cudaSuccess;
   dim3 grid(ntiles), block(NT);
   if (var) {
-    if (zero) k_rbgs<T, TX, TY, NT, true, true><<<grid, block, 0, st>>>(bl, tiles, zc, src, dst, rhs, fx, fy, fz);
-    else k_rbgs<T, TX, TY, NT, true, false><<<grid, block, 0, st>>>(bl, tiles, zc, src, dst, rhs, fx, fy, fz);
+    if (zero) pdl_launch(k_rbgs<T, TX, TY, NT, true, true>, grid, block, 0, st, bl, tiles, zc, src, dst, rhs, fx, fy, fz);
+    else pdl_launch(k_rbgs<T, TX, TY, NT, true, false>, grid, block, 0, st, bl, tiles, zc, src, dst, rhs, fx, fy, fz);
   } else {
-    if (zero) k_rbgs<T, TX, TY, NT, false, true><<<grid, block, 0, st>>>(bl, tiles, zc, src, dst, rhs, fx, fy, fz);
-    else k_rbgs<T, TX, TY, NT, false, false><<<grid, block, 0, st>>>(bl, tiles, zc, src, dst, rhs, fx, fy, fz);
+    if (zero) pdl_launch(k_rbgs<T, TX, TY, NT, false, true>, grid, block, 0, st, bl, tiles, zc, src, dst, rhs, fx, fy, fz);
+    else pdl_launch(k_rbgs<T, TX, TY, NT, false, false>, grid, block, 0, st, bl, tiles, zc, src, dst, rhs, fx, fy, fz);
   }
   return cudaGetLastError();
 }
@@ -1262,11 +1331,11 @@ static cudaError_t rows_dispatch(bool var, bool zero, const BlkLev* bl, const Ti
   constexpr size_t SM = rows_smem<T, TPR, CP, TY>();
   dim3 grid(ntiles), block(NT);
   if (var) {
-    if (zero) k_rbgs_rows<T, TPR, CP, TY, true, true><<<grid, block, SM, st>>>(bl, tiles, zc, src, dst, rhs, fx, fy, fz);
-    else k_rbgs_rows<T, TPR, CP, TY, true, false><<<grid, block, SM, st>>>(bl, tiles, zc, src, dst, rhs, fx, fy, fz);
+    if (zero) pdl_launch(k_rbgs_rows<T, TPR, CP, TY, true, true>, grid, block, SM, st, bl, tiles, zc, src, dst, rhs, fx, fy, fz);
+    else pdl_launch(k_rbgs_rows<T, TPR, CP, TY, true, false>, grid, block, SM, st, bl, tiles, zc, src, dst, rhs, fx, fy, fz);
   } else {
-    if (zero) k_rbgs_rows<T, TPR, CP, TY, false, true><<<grid, block, SM, st>>>(bl, tiles, zc, src, dst, rhs, fx, fy, fz);
-    else k_rbgs_rows<T, TPR, CP, TY, false, false><<<grid, block, SM, st>>>(bl, tiles, zc, src, dst, rhs, fx, fy, fz);
+    if (zero) pdl_launch(k_rbgs_rows<T, TPR, CP, TY, false, true>, grid, block, SM, st, bl, tiles, zc, src, dst, rhs, fx, fy, fz);
+    else pdl_launch(k_rbgs_rows<T, TPR, CP, TY, false, false>, grid, block, SM, st, bl, tiles, zc, src, dst, rhs, fx, fy, fz);
   }
   return cudaGetLastError();
 }
@@ -1298,8 +1367,8 @@ static cudaError_t tma2_dispatch(bool var, const BlkLev* bl, const Tile* tiles, 
   constexpr int D = tma2_depth<T, TPR, CP, TY, D0>();
   constexpr int NT = TPR * (TY + 2);
   constexpr size_t SM = Tma2Cfg<T, TPR, CP, TY, D>::SMEM;
-  if (var) k_rbgs_tma2<T, TPR, CP, TY, D, true><<<ntiles, NT, SM, st>>>(bl, tiles, zc, maps, rmaps, dst, fx, fy, fz, err);
-  else k_rbgs_tma2<T, TPR, CP, TY, D, false><<<ntiles, NT, SM, st>>>(bl, tiles, zc, maps, rmaps, dst, fx, fy, fz, err);
+  if (var) pdl_launch(k_rbgs_tma2<T, TPR, CP, TY, D, true>, ntiles, NT, SM, st, bl, tiles, zc, maps, rmaps, dst, fx, fy, fz, err);
+  else pdl_launch(k_rbgs_tma2<T, TPR, CP, TY, D, false>, ntiles, NT, SM, st, bl, tiles, zc, maps, rmaps, dst, fx, fy, fz, err);
   return cudaGetLastError();
 }
 
@@ -1333,6 +1402,8 @@ __global__ void __launch_bounds__(TPR*(TY + 2)) k_rbgs_win(const BlkLev* __restr
                                                           const CUtensorMap* __restrict__ maps,
                                                           const CUtensorMap* __restrict__ rmaps,
                                                           float* __restrict__ dst, int* err) {
+  pdl_trigger();
+  pdl_wait();
   using C = VecCfg<TPR, 1, TY, NS, D>;
   static_assert(TPR <= 32 && (TPR & (TPR - 1)) == 0, "a row is a power-of-two lane segment of one warp");
   extern __shared__ unsigned char smem_raw[];
@@ -1519,7 +1590,7 @@ template <int TPR, int GPT, int TY, int NS, int D>
 static cudaError_t vec_dispatch(const BlkLev* bl, const Tile* tiles, int ntiles, int zc, const CUtensorMap* maps,
                                 const CUtensorMap* rmaps, int* err, float* dst, cudaStream_t st) {
   if (ntiles <= 0) return cudaSuccess;
-  k_rbgs_vec<TPR, GPT, TY, NS, D><<<ntiles, TPR * (TY + 2), VecCfg<TPR, GPT, TY, NS, D>::SMEM, st>>>(
+  pdl_launch(k_rbgs_vec<TPR, GPT, TY, NS, D>, ntiles, TPR * (TY + 2), VecCfg<TPR, GPT, TY, NS, D>::SMEM, st, 
       bl, tiles, zc, maps, rmaps, dst, err);
   return cudaGetLastError();
 }
@@ -1540,8 +1611,8 @@ static cudaError_t win_dispatch(bool zero, const BlkLev* bl, const Tile* tiles, 
   static_assert(D + 3 <= NS, "a plane is read until two phases after its own");
   if (ntiles <= 0) return cudaSuccess;
   constexpr size_t SM = VecCfg<TPR, 1, TY, NS, D>::SMEM;
-  if (zero) k_rbgs_win<TPR, TY, NS, D, true><<<ntiles, TPR * (TY + 2), SM, st>>>(bl, tiles, zc, maps, rmaps, dst, err);
-  else k_rbgs_win<TPR, TY, NS, D, false><<<ntiles, TPR * (TY + 2), SM, st>>>(bl, tiles, zc, maps, rmaps, dst, err);
+  if (zero) pdl_launch(k_rbgs_win<TPR, TY, NS, D, true>, ntiles, TPR * (TY + 2), SM, st, bl, tiles, zc, maps, rmaps, dst, err);
+  else pdl_launch(k_rbgs_win<TPR, TY, NS, D, false>, ntiles, TPR * (TY + 2), SM, st, bl, tiles, zc, maps, rmaps, dst, err);
   return cudaGetLastError();
 }
 
@@ -1661,8 +1732,8 @@ cudaError_t launch_fill(const uint32_t* dsts, const uint32_t* srcs, int64_t n, T
                         bool zero_old, cudaStream_t st) {
   if (n <= 0) return cudaSuccess;
   int g = grid_for(n, 256);
-  if (zero_old) k_fill<T, true><<<g, 256, 0, st>>>(dsts, srcs, n, out, cur, old);
-  else k_fill<T, false><<<g, 256, 0, st>>>(dsts, srcs, n, out, cur, old);
+  if (zero_old) pdl_launch(k_fill<T, true>, g, 256, 0, st, dsts, srcs, n, out, cur, old);
+  else pdl_launch(k_fill<T, false>, g, 256, 0, st, dsts, srcs, n, out, cur, old);
   return cudaGetLastError();
 }
 
@@ -1677,9 +1748,9 @@ cudaError_t launch_restrict(bool var, bool zero_phi, const BlkLev* fine, const B
                             cudaStream_t st) {
   if (rt.nrows <= 0) return cudaSuccess;
   const int g = row_grid(rt.nrows);
-  if (zero_phi) k_restrict<T, false, true><<<g, 256, 0, st>>>(fine, coarse, rt.start, rt.nb, rt.nrows, phi, rhs, rhs_c, fx, fy, fz);
-  else if (var) k_restrict<T, true, false><<<g, 256, 0, st>>>(fine, coarse, rt.start, rt.nb, rt.nrows, phi, rhs, rhs_c, fx, fy, fz);
-  else k_restrict<T, false, false><<<g, 256, 0, st>>>(fine, coarse, rt.start, rt.nb, rt.nrows, phi, rhs, rhs_c, fx, fy, fz);
+  if (zero_phi) pdl_launch(k_restrict<T, false, true>, g, 256, 0, st, fine, coarse, rt.start, rt.nb, rt.nrows, phi, rhs, rhs_c, fx, fy, fz);
+  else if (var) pdl_launch(k_restrict<T, true, false>, g, 256, 0, st, fine, coarse, rt.start, rt.nb, rt.nrows, phi, rhs, rhs_c, fx, fy, fz);
+  else pdl_launch(k_restrict<T, false, false>, g, 256, 0, st, fine, coarse, rt.start, rt.nb, rt.nrows, phi, rhs, rhs_c, fx, fy, fz);
   return cudaGetLastError();
 }
 
@@ -1694,6 +1765,8 @@ template <typename T, bool ZERO_OLD>
 __global__ void __launch_bounds__(256) k_prolong_vec(const BlkLev* __restrict__ fine, const BlkLev* __restrict__ coarse,
                                                      const Tile* __restrict__ tiles, const T* __restrict__ phi_c,
                                                      const T* __restrict__ old, T* __restrict__ out) {
+  pdl_trigger();
+  pdl_wait();
   constexpr int VEC = 16 / (int)sizeof(T);
   constexpr int NC = VEC / 2 + 2;  // coarse columns a group reads
   using V = typename std::conditional<sizeof(T) == 4, float4, double2>::type;
@@ -1812,8 +1885,8 @@ template <typename T>
 cudaError_t launch_prolong_vec(bool zero_old, const BlkLev* fine, const BlkLev* coarse, const Tile* tiles, int ntiles,
                                const T* phi_c, const T* old, T* out, cudaStream_t st) {
   if (ntiles <= 0) return cudaSuccess;
-  if (zero_old) k_prolong_vec<T, true><<<ntiles, 256, 0, st>>>(fine, coarse, tiles, phi_c, old, out);
-  else k_prolong_vec<T, false><<<ntiles, 256, 0, st>>>(fine, coarse, tiles, phi_c, old, out);
+  if (zero_old) pdl_launch(k_prolong_vec<T, true>, ntiles, 256, 0, st, fine, coarse, tiles, phi_c, old, out);
+  else pdl_launch(k_prolong_vec<T, false>, ntiles, 256, 0, st, fine, coarse, tiles, phi_c, old, out);
   return cudaGetLastError();
 }
 template cudaError_t launch_prolong_vec<double>(bool, const BlkLev*, const BlkLev*, const Tile*, int, const double*,
@@ -1826,8 +1899,8 @@ cudaError_t launch_prolong(bool zero_old, const BlkLev* fine, const BlkLev* coar
                            const T* old, T* out, cudaStream_t st) {
   if (rt.nrows <= 0) return cudaSuccess;
   const int g = row_grid(rt.nrows);
-  if (zero_old) k_prolong_pairs<T, true><<<g, 256, 0, st>>>(fine, coarse, rt.start, rt.nb, rt.nrows, phi_c, old, out);
-  else k_prolong_pairs<T, false><<<g, 256, 0, st>>>(fine, coarse, rt.start, rt.nb, rt.nrows, phi_c, old, out);
+  if (zero_old) pdl_launch(k_prolong_pairs<T, true>, g, 256, 0, st, fine, coarse, rt.start, rt.nb, rt.nrows, phi_c, old, out);
+  else pdl_launch(k_prolong_pairs<T, false>, g, 256, 0, st, fine, coarse, rt.start, rt.nb, rt.nrows, phi_c, old, out);
   return cudaGetLastError();
 }
 
@@ -1849,6 +1922,8 @@ __global__ void __launch_bounds__(256) k_defect_vec(const BlkLev* __restrict__ b
                                                     const TE* __restrict__ e, double* __restrict__ p_next,
                                                     const double* __restrict__ bvec, TR* __restrict__ rhs_out,
                                                     double mean_b, double rscale, double* __restrict__ partials) {
+  pdl_trigger();
+  pdl_wait();
   using E2 = typename std::conditional<sizeof(TE) == 4, float2, double2>::type;
   using R2 = typename std::conditional<sizeof(TR) == 4, float2, double2>::type;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -1916,8 +1991,8 @@ cudaError_t launch_defect_vec(const BlkLev* bl, const Tile* tiles, int ntiles, c
                               double* partials, int grid, cudaStream_t st) {
   if (ntiles <= 0) return cudaSuccess;
   grid = ntiles;  // one tile per CTA (partials holds one quadruple per tile)
-  if (e) k_defect_vec<TE, TR, true><<<grid, 256, 0, st>>>(bl, tiles, ntiles, p, e, p_next, b, rhs_out, mean_b, rscale, partials);
-  else k_defect_vec<TE, TR, false><<<grid, 256, 0, st>>>(bl, tiles, ntiles, p, e, p_next, b, rhs_out, mean_b, rscale, partials);
+  if (e) pdl_launch(k_defect_vec<TE, TR, true>, grid, 256, 0, st, bl, tiles, ntiles, p, e, p_next, b, rhs_out, mean_b, rscale, partials);
+  else pdl_launch(k_defect_vec<TE, TR, false>, grid, 256, 0, st, bl, tiles, ntiles, p, e, p_next, b, rhs_out, mean_b, rscale, partials);
   return cudaGetLastError();
 }
 template cudaError_t launch_defect_vec<double, double>(const BlkLev*, const Tile*, int, const double*, const double*,
@@ -1934,11 +2009,11 @@ cudaError_t launch_defect(bool var, const BlkLev* bl, RowTab rt, const double* p
   if (rt.nrows <= 0) return cudaSuccess;
   const int g = defect_grid(rt.nrows);
   if (e) {
-    if (var) k_defect<TE, TR, true, true><<<g, 256, 0, st>>>(bl, rt.start, rt.nb, rt.nrows, p, e, p_next, b, rhs_out, mean_b, rscale, fx, fy, fz, partials);
-    else k_defect<TE, TR, true, false><<<g, 256, 0, st>>>(bl, rt.start, rt.nb, rt.nrows, p, e, p_next, b, rhs_out, mean_b, rscale, fx, fy, fz, partials);
+    if (var) pdl_launch(k_defect<TE, TR, true, true>, g, 256, 0, st, bl, rt.start, rt.nb, rt.nrows, p, e, p_next, b, rhs_out, mean_b, rscale, fx, fy, fz, partials);
+    else pdl_launch(k_defect<TE, TR, true, false>, g, 256, 0, st, bl, rt.start, rt.nb, rt.nrows, p, e, p_next, b, rhs_out, mean_b, rscale, fx, fy, fz, partials);
   } else {
-    if (var) k_defect<TE, TR, false, true><<<g, 256, 0, st>>>(bl, rt.start, rt.nb, rt.nrows, p, e, p_next, b, rhs_out, mean_b, rscale, fx, fy, fz, partials);
-    else k_defect<TE, TR, false, false><<<g, 256, 0, st>>>(bl, rt.start, rt.nb, rt.nrows, p, e, p_next, b, rhs_out, mean_b, rscale, fx, fy, fz, partials);
+    if (var) pdl_launch(k_defect<TE, TR, false, true>, g, 256, 0, st, bl, rt.start, rt.nb, rt.nrows, p, e, p_next, b, rhs_out, mean_b, rscale, fx, fy, fz, partials);
+    else pdl_launch(k_defect<TE, TR, false, false>, g, 256, 0, st, bl, rt.start, rt.nb, rt.nrows, p, e, p_next, b, rhs_out, mean_b, rscale, fx, fy, fz, partials);
   }
   return cudaGetLastError();
 }
@@ -1980,6 +2055,8 @@ __global__ void __launch_bounds__(TPR* TYC) k_restrict_tma(const BlkLev* __restr
                                                           T* __restrict__ rhs_c, const T* __restrict__ fx,
                                                           const T* __restrict__ fy, const T* __restrict__ fz,
                                                           int* err) {
+  pdl_trigger();
+  pdl_wait();
   using C = RTmaCfg<T, TPR, CPX, TYC, NS>;
   static_assert(D + 2 <= NS, "a fine plane is read until the phase after its own");
   using P2 = typename std::conditional<sizeof(T) == 4, float2, double2>::type;
@@ -2123,9 +2200,9 @@ static cudaError_t rtile_dispatch(bool var, bool zero, const BlkLev* fine, const
                                   const T* fz, cudaStream_t st) {
   if (ntiles <= 0) return cudaSuccess;
   constexpr size_t SM = rtile_smem<T, TPR, CPX, TYC>();
-  if (zero) k_restrict_tile<T, false, true, TPR, CPX, TYC><<<ntiles, TPR * TYC, SM, st>>>(fine, coarse, tiles, zc, phi, rhs, rhs_c, fx, fy, fz);
-  else if (var) k_restrict_tile<T, true, false, TPR, CPX, TYC><<<ntiles, TPR * TYC, SM, st>>>(fine, coarse, tiles, zc, phi, rhs, rhs_c, fx, fy, fz);
-  else k_restrict_tile<T, false, false, TPR, CPX, TYC><<<ntiles, TPR * TYC, SM, st>>>(fine, coarse, tiles, zc, phi, rhs, rhs_c, fx, fy, fz);
+  if (zero) pdl_launch(k_restrict_tile<T, false, true, TPR, CPX, TYC>, ntiles, TPR * TYC, SM, st, fine, coarse, tiles, zc, phi, rhs, rhs_c, fx, fy, fz);
+  else if (var) pdl_launch(k_restrict_tile<T, true, false, TPR, CPX, TYC>, ntiles, TPR * TYC, SM, st, fine, coarse, tiles, zc, phi, rhs, rhs_c, fx, fy, fz);
+  else pdl_launch(k_restrict_tile<T, false, false, TPR, CPX, TYC>, ntiles, TPR * TYC, SM, st, fine, coarse, tiles, zc, phi, rhs, rhs_c, fx, fy, fz);
   return cudaGetLastError();
 }
 
@@ -2157,11 +2234,11 @@ static cudaError_t rtma_dispatch(bool var, bool zero, const BlkLev* fine, const 
   constexpr size_t SM = RTmaCfg<T, TPR, CPX, TYC, NS>::SMEM;
   constexpr int NT = TPR * TYC;
   if (var) {
-    if (zero) k_restrict_tma<T, TPR, CPX, TYC, NS, D, true, true><<<ntiles, NT, SM, st>>>(fine, coarse, tiles, zc, pmaps, rmaps, rhs_c, fx, fy, fz, err);
-    else k_restrict_tma<T, TPR, CPX, TYC, NS, D, true, false><<<ntiles, NT, SM, st>>>(fine, coarse, tiles, zc, pmaps, rmaps, rhs_c, fx, fy, fz, err);
+    if (zero) pdl_launch(k_restrict_tma<T, TPR, CPX, TYC, NS, D, true, true>, ntiles, NT, SM, st, fine, coarse, tiles, zc, pmaps, rmaps, rhs_c, fx, fy, fz, err);
+    else pdl_launch(k_restrict_tma<T, TPR, CPX, TYC, NS, D, true, false>, ntiles, NT, SM, st, fine, coarse, tiles, zc, pmaps, rmaps, rhs_c, fx, fy, fz, err);
   } else {
-    if (zero) k_restrict_tma<T, TPR, CPX, TYC, NS, D, false, true><<<ntiles, NT, SM, st>>>(fine, coarse, tiles, zc, pmaps, rmaps, rhs_c, fx, fy, fz, err);
-    else k_restrict_tma<T, TPR, CPX, TYC, NS, D, false, false><<<ntiles, NT, SM, st>>>(fine, coarse, tiles, zc, pmaps, rmaps, rhs_c, fx, fy, fz, err);
+    if (zero) pdl_launch(k_restrict_tma<T, TPR, CPX, TYC, NS, D, false, true>, ntiles, NT, SM, st, fine, coarse, tiles, zc, pmaps, rmaps, rhs_c, fx, fy, fz, err);
+    else pdl_launch(k_restrict_tma<T, TPR, CPX, TYC, NS, D, false, false>, ntiles, NT, SM, st, fine, coarse, tiles, zc, pmaps, rmaps, rhs_c, fx, fy, fz, err);
   }
   return cudaGetLastError();
 }
@@ -2222,6 +2299,8 @@ template cudaError_t launch_restrict_tile<float>(int, bool, bool, const BlkLev*,
 // the padded device layout.
 __global__ void k_stage_scatter(const double* __restrict__ stg, int tx, int ty, int pl, int g0, int ex, int ey,
                                 int ez, double* __restrict__ dev, int sx, long long sxy) {
+  pdl_trigger();
+  pdl_wait();
   const long long n = (long long)ex * ey * ez;
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
     const int x = (int)(e % ex), y = (int)((e / ex) % ey), z = (int)(e / ((long long)ex * ey));
@@ -2232,6 +2311,8 @@ __global__ void k_stage_scatter(const double* __restrict__ stg, int tx, int ty, 
 
 __global__ void k_stage_gather(double* __restrict__ stg, int tx, int ty, int pl, int g0, int ex, int ey, int ez,
                                const double* __restrict__ dev, int sx, long long sxy) {
+  pdl_trigger();
+  pdl_wait();
   const long long n = (long long)ex * ey * ez;
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
     const int x = (int)(e % ex), y = (int)((e / ex) % ey), z = (int)(e / ((long long)ex * ey));
@@ -2245,47 +2326,47 @@ cudaError_t launch_stage(bool to_device, double* stg, int tx, int ty, int pl, in
   const long long n = (long long)ex * ey * ez;
   if (n <= 0) return cudaSuccess;
   const int grid = (int)std::min<long long>((n + 255) / 256, 148LL * 16);
-  if (to_device) k_stage_scatter<<<grid, 256, 0, st>>>(stg, tx, ty, pl, g0, ex, ey, ez, dev, sx, sxy);
-  else k_stage_gather<<<grid, 256, 0, st>>>(stg, tx, ty, pl, g0, ex, ey, ez, dev, sx, sxy);
+  if (to_device) pdl_launch(k_stage_scatter, grid, 256, 0, st, stg, tx, ty, pl, g0, ex, ey, ez, dev, sx, sxy);
+  else pdl_launch(k_stage_gather, grid, 256, 0, st, stg, tx, ty, pl, g0, ex, ey, ez, dev, sx, sxy);
   return cudaGetLastError();
 }
 
 cudaError_t launch_reduce4(const double* partials, int n, double* out, cudaStream_t st) {
-  k_reduce4<<<1, 1024, 0, st>>>(partials, n, out);
+  pdl_launch(k_reduce4, 1, 1024, 0, st, partials, n, out);
   return cudaGetLastError();
 }
 
 cudaError_t launch_sum_interior(const BlkLev* bl, CellTab ct, const double* a, double* partials, cudaStream_t st) {
   if (ct.ncta <= 0) return cudaSuccess;
-  k_sum_interior<<<ct.ncta, 256, 0, st>>>(bl, ct.cta_start, ct.nb, a, partials);
+  pdl_launch(k_sum_interior, ct.ncta, 256, 0, st, bl, ct.cta_start, ct.nb, a, partials);
   return cudaGetLastError();
 }
 
 cudaError_t launch_shift(double* a, int64_t n, const double* s, double scale, cudaStream_t st) {
-  k_shift<<<grid_for(n, 256), 256, 0, st>>>(a, n, s, scale);
+  pdl_launch(k_shift, grid_for(n, 256), 256, 0, st, a, n, s, scale);
   return cudaGetLastError();
 }
 
 cudaError_t launch_convert_d2f(const double* a, float* b, int64_t n, cudaStream_t st) {
-  k_d2f<<<grid_for(n, 256), 256, 0, st>>>(a, b, n);
+  pdl_launch(k_d2f, grid_for(n, 256), 256, 0, st, a, b, n);
   return cudaGetLastError();
 }
 cudaError_t launch_convert_f2d(const float* a, double* b, int64_t n, cudaStream_t st) {
-  k_f2d<<<grid_for(n, 256), 256, 0, st>>>(a, b, n);
+  pdl_launch(k_f2d, grid_for(n, 256), 256, 0, st, a, b, n);
   return cudaGetLastError();
 }
 
 cudaError_t launch_dens_restrict(const BlkLev* fine, const BlkLev* coarse, CellTab ct, const double* df, double* dc,
                                  cudaStream_t st) {
   if (ct.ncta <= 0) return cudaSuccess;
-  k_dens_restrict<<<ct.ncta, 256, 0, st>>>(fine, coarse, ct.cta_start, ct.nb, df, dc);
+  pdl_launch(k_dens_restrict, ct.ncta, 256, 0, st, fine, coarse, ct.cta_start, ct.nb, df, dc);
   return cudaGetLastError();
 }
 
 cudaError_t launch_face_coef(const BlkLev* bl, CellTab ct, const double* dens, const double* h3, double* fx,
                              double* fy, double* fz, cudaStream_t st) {
   if (ct.ncta <= 0) return cudaSuccess;
-  k_face_coef<<<ct.ncta, 256, 0, st>>>(bl, ct.cta_start, ct.nb, dens, h3, fx, fy, fz);
+  pdl_launch(k_face_coef, ct.ncta, 256, 0, st, bl, ct.cta_start, ct.nb, dens, h3, fx, fy, fz);
   return cudaGetLastError();
 }
 
