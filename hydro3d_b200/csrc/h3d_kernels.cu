@@ -579,6 +579,8 @@ __global__ void __launch_bounds__(TPR*(TY + 2)) k_rbgs_tma2(const BlkLev* __rest
       red(z);
     }
     if (z - 2 >= zs && z - 2 <= ze) black_store(z - 2);
+    // this phase's shared-memory writes are ordered before the TMA that reuses their slot
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
     __syncthreads();
     if (leader && z + D + 1 <= zhi + 1) issue(z + D + 1);
   }
@@ -758,6 +760,8 @@ __global__ void __launch_bounds__(TPR*(TY + 2)) k_rbgs_vec(const BlkLev* __restr
       if (red) *reinterpret_cast<float4*>(pslot(sr) + prow + x0) = ir.c;
       if (blk) *reinterpret_cast<float4*>(Drow + (long long)zb * sxy + x0) = ib.c;
     }
+    // this phase's shared-memory writes are ordered before the TMA that reuses their slot
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
     __syncthreads();
     if (leader && z + D + 1 <= zhi + 1) issue(z + D + 1);
     s0 = wrap(s0 + 1);
@@ -1570,6 +1574,8 @@ __global__ void __launch_bounds__(TPR*(TY + 2)) k_rbgs_win(const BlkLev* __restr
       colour(m2, m3, m1, ub, db, hb, bl, br, zb, (y + zb + 1) & 1);
       *reinterpret_cast<float4*>(Drow + (long long)zb * sxy) = m2;
     }
+    // this phase's shared-memory writes are ordered before the TMA that reuses their slot
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
     __syncthreads();
     if (leader && z + D + 1 <= zhi + 1) issue(z + D + 1);
     m3 = m2;
@@ -1726,6 +1732,76 @@ cudaError_t launch_rbgs(int variant, bool var, bool zero_src, const BlkLev* bl, 
     default: return cudaErrorInvalidValue;
   }
 }
+
+// ---------------------------------------------------------------------------
+// Several sweeps of a small level (mgrelax with `sweeps` iterations) in one
+// CTA, in place: per sweep the red cells (x+y+z odd), a barrier, the black
+// cells, a barrier, then the ghost fill from the level's sweep table (every
+// entry reads an interior cell, so the gather is order-free in place), a
+// barrier.  Same cell values as the out-of-place sweep + fill kernels: the
+// FP64 update keeps the reference's operand order and IEEE division.
+// zero: the iterate is known zero; it is cleared (ghosts included) first.
+// start[b]: first flat interior index of block b (start[nb] = all cells).
+template <typename T, bool VAR>
+__global__ void __launch_bounds__(1024) k_relax_small(const BlkLev* __restrict__ bls, const int* __restrict__ start,
+                                                      int nb, T* __restrict__ phi, const T* __restrict__ rhs,
+                                                      const T* __restrict__ fx, const T* __restrict__ fy,
+                                                      const T* __restrict__ fz, const uint32_t* __restrict__ fdst,
+                                                      const uint32_t* __restrict__ fsrc, int nfill, int sweeps,
+                                                      int zero, long long nelems) {
+  __shared__ BlkLev sb[kSmallLevelBlocks];
+  __shared__ int ss[kSmallLevelBlocks + 1];
+  for (int b = threadIdx.x; b < nb; b += blockDim.x) sb[b] = bls[b];
+  for (int b = threadIdx.x; b <= nb; b += blockDim.x) ss[b] = start[b];
+  __syncthreads();
+  const int ncell = ss[nb];
+  if (zero) {
+    for (long long q = threadIdx.x; q < nelems; q += blockDim.x) phi[q] = T(0);
+    __syncthreads();
+  }
+  for (int it = 0; it < sweeps; ++it) {
+    for (int colour = 1; colour >= 0; --colour) {  // red (x+y+z odd) first
+      for (int c = threadIdx.x; c < ncell; c += blockDim.x) {
+        int b = 0;
+        while (b + 1 < nb && ss[b + 1] <= c) ++b;
+        const BlkLev& B = sb[b];
+        const int local = c - ss[b];
+        const int x = 1 + local % B.nx, y = 1 + (local / B.nx) % B.ny, z = 1 + local / (B.nx * B.ny);
+        if (((x + y + z) & 1) != colour) continue;
+        const long long i = B.off + (long long)z * B.sxy + (long long)y * B.sx + x;
+        const Coef<T> cf = cell_coef<T, VAR>(B, x, y, z, i - B.off, VAR ? fx + B.off : nullptr,
+                                             VAR ? fy + B.off : nullptr, VAR ? fz + B.off : nullptr);
+        const T ap = coef_ap(cf);
+        const T v = gs_div(rhs[i] - (cf.aw * phi[i - 1] + cf.ae * phi[i + 1] + cf.as * phi[i - B.sx] +
+                                     cf.an * phi[i + B.sx] + cf.ab * phi[i - B.sxy] + cf.at * phi[i + B.sxy]),
+                           ap);
+        phi[i] = v;
+      }
+      __syncthreads();
+    }
+    for (int q = threadIdx.x; q < nfill; q += blockDim.x) phi[fdst[q]] = phi[fsrc[q] & kIdxMask];
+    __syncthreads();
+  }
+}
+
+template <typename T>
+cudaError_t launch_relax_small(bool var, const BlkLev* bl, const int* start, int nb, T* phi, const T* rhs,
+                               const T* fx, const T* fy, const T* fz, const uint32_t* fdst, const uint32_t* fsrc,
+                               int nfill, int sweeps, bool zero, long long nelems, cudaStream_t st) {
+  if (var)
+    pdl_launch(k_relax_small<T, true>, 1, 1024, 0, st, bl, start, nb, phi, rhs, fx, fy, fz, fdst, fsrc, nfill, sweeps,
+               (int)zero, nelems);
+  else
+    pdl_launch(k_relax_small<T, false>, 1, 1024, 0, st, bl, start, nb, phi, rhs, fx, fy, fz, fdst, fsrc, nfill,
+               sweeps, (int)zero, nelems);
+  return cudaGetLastError();
+}
+template cudaError_t launch_relax_small<double>(bool, const BlkLev*, const int*, int, double*, const double*,
+                                                const double*, const double*, const double*, const uint32_t*,
+                                                const uint32_t*, int, int, bool, long long, cudaStream_t);
+template cudaError_t launch_relax_small<float>(bool, const BlkLev*, const int*, int, float*, const float*,
+                                               const float*, const float*, const float*, const uint32_t*,
+                                               const uint32_t*, int, int, bool, long long, cudaStream_t);
 
 template <typename T>
 cudaError_t launch_fill(const uint32_t* dsts, const uint32_t* srcs, int64_t n, T* out, const T* cur, const T* old,

@@ -83,6 +83,16 @@ cudaError_t launch_rbgs(int variant, bool var, bool zero_src, const BlkLev* bl, 
                         const T* rhs, const T* fx, const T* fy,
                         const T* fz, cudaStream_t st);
 
+constexpr int kSmallLevelBlocks = 64;  // block descriptors the fused small-level kernel caches
+// `sweeps` red-black sweeps of a small level, each followed by its ghost fill,
+// in place in one CTA (see k_relax_small).  start: flat interior index of
+// each block's first cell (nb+1 entries); the fill table must read interior
+// cells only.
+template <typename T>
+cudaError_t launch_relax_small(bool var, const BlkLev* bl, const int* start, int nb, T* phi, const T* rhs,
+                               const T* fx, const T* fy, const T* fz, const uint32_t* fdst, const uint32_t* fsrc,
+                               int nfill, int sweeps, bool zero, long long nelems, cudaStream_t st);
+
 // Ghost gather: out[dst[e]] = (src[e] & old) ? old[src] : cur[src].
 template <typename T>
 cudaError_t launch_fill(const uint32_t* dsts, const uint32_t* srcs, int64_t n, T* out, const T* cur,

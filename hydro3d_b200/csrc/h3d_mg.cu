@@ -31,6 +31,9 @@ void h3d::set_call_error(const std::string& msg) { g_create_error = msg; }
 
 namespace {
 
+// Levels with at most this many interior cells relax in one single-CTA launch.
+constexpr int64_t kSmallLevelCells = 2048;
+
 struct Halo {
   uint32_t* d_dst = nullptr;
   uint32_t* d_src = nullptr;
@@ -50,7 +53,7 @@ struct Level {
   int* d_rows_int = nullptr;  // interior rows
   int nrows_int = 0;
   Tile* d_tiles = nullptr;
-  int ntiles = 0;
+  int ntiles = 0, tiles_cap = 0;
   int variant = 0, zc = 1;
   double* phi64[2] = {nullptr, nullptr};
   double* rhs64 = nullptr;
@@ -63,12 +66,15 @@ struct Level {
   CUtensorMap* d_maps = nullptr;  // [ty index][0,1: iterate buffer, 2: rhs][block] tensor maps
   CUtensorMap* d_rmaps = nullptr;  // as the fine level of a restriction: [tyc index][0,1: iterate, 2: rhs][block]
   Tile* d_rtiles = nullptr;       // restriction tiles (this level as the coarse level)
+  int rtiles_cap = 0;
   Tile* d_ptiles = nullptr;       // prolongation / defect tiles (kProlongRows rows of one plane, ghosts included)
   int nptiles = 0;
   bool pvec32 = false, pvec64 = false;  // every block's nx a multiple of 4 (FP32) / 2 (FP64) cells
   int nrtiles = 0, rvariant = 0, rzc = 1;
   bool tma_ok = false;
   bool f32 = false, var = false;  // iterate precision of the level's smoother; variable coefficients
+  int* d_cstart = nullptr;  // small levels: flat interior index of each block's first cell (fused relaxation)
+  bool small = false;       // relaxation runs as one fused single-CTA kernel
   int cur64 = 0, cur32 = 0;
   bool zero64 = false, zero32 = false;
   double sweep_bytes = 0;       // algorithmic bytes of one sweep (FP64 or FP32 by mode)
@@ -146,7 +152,12 @@ int dalloc(h3d_mg* h, T** p, size_t n) {
   *p = nullptr;
   if (n == 0) return H3D_OK;
   CU(cudaMalloc((void**)p, n * sizeof(T)));
+  // The zero fill must be complete before the caller fills the array: uploads
+  // with cudaMemcpy run on the legacy stream, which is not ordered after the
+  // solver's non-blocking stream (a late zero fill once wiped freshly
+  // uploaded tile lists, and the sweeps then indexed plane -1 of their ring).
   CU(cudaMemsetAsync(*p, 0, n * sizeof(T), h->st));
+  CU(cudaStreamSynchronize(h->st));
   return H3D_OK;
 }
 
@@ -203,6 +214,22 @@ bool variant_fits(const Level& Lv, int variant) {
   return true;
 }
 
+// Copies a tile list to its device array, growing the array only when the
+// list outgrows it (the autotuners rebuild tile lists many times).
+int upload_tiles(h3d_mg* h, Tile** d, int* cap, const std::vector<Tile>& t) {
+  if ((int)t.size() > *cap) {
+    CU(cudaDeviceSynchronize());
+    dfree(*d);
+    *d = nullptr;
+    *cap = 0;
+    TRY(dalloc(h, d, t.size()));
+    *cap = (int)t.size();
+  }
+  CU(cudaMemcpyAsync(*d, t.data(), t.size() * sizeof(Tile), cudaMemcpyHostToDevice, h->st));
+  CU(cudaStreamSynchronize(h->st));
+  return H3D_OK;
+}
+
 int build_tiles(h3d_mg* h, Level& Lv, int variant, int zc) {
   TileShape s = tile_shape(variant);
   std::vector<Tile> t;
@@ -212,15 +239,13 @@ int build_tiles(h3d_mg* h, Level& Lv, int variant, int zc) {
       for (int y0 = 1; y0 <= B.ny; y0 += s.ty)
         for (int x0 = 1; x0 <= B.nx; x0 += s.tx) t.push_back(Tile{(int)b, x0, y0, z0});
   }
-  dfree(Lv.d_tiles);
-  Lv.d_tiles = nullptr;
-  TRY(dalloc(h, &Lv.d_tiles, t.size()));
-  CU(cudaMemcpy(Lv.d_tiles, t.data(), t.size() * sizeof(Tile), cudaMemcpyHostToDevice));
+  TRY(upload_tiles(h, &Lv.d_tiles, &Lv.tiles_cap, t));
   Lv.ntiles = (int)t.size();
   Lv.variant = variant;
   Lv.zc = zc;
   return H3D_OK;
 }
+
 
 // Tiles of (TY rows x all x) x zc planes over every block of geometry G.
 std::vector<Tile> row_tiles(const LevelGeom& G, int ty, int zc) {
@@ -256,8 +281,7 @@ int build_restrict_tiles(h3d_mg* h, Level& C) {
   RestrictShape r = restrict_shape(v);
   int zc = pick_zc(C.geom, r.tyc);
   std::vector<Tile> t = row_tiles(C.geom, r.tyc, zc);
-  TRY(dalloc(h, &C.d_rtiles, t.size()));
-  CU(cudaMemcpy(C.d_rtiles, t.data(), t.size() * sizeof(Tile), cudaMemcpyHostToDevice));
+  TRY(upload_tiles(h, &C.d_rtiles, &C.rtiles_cap, t));
   C.nrtiles = (int)t.size();
   C.rvariant = v;
   C.rzc = zc;
@@ -395,6 +419,24 @@ struct Exec {
   }
 
   int relax(int g, int it) {
+    Level& V = L(g);
+    if (it > 0 && V.small && g > 1) {  // all sweeps and fills of this visit in one launch
+      const int nb = (int)V.geom.bl.size();
+      if (mixed_level(g)) {
+        CU(launch_relax_small<float>(h->var, V.d_bl, V.d_cstart, nb, V.phi32[V.cur32], V.rhs32, V.fx32, V.fy32,
+                                     V.fz32, V.sweep.d_dst, V.sweep.d_src, (int)V.sweep.n, it, V.zero32,
+                                     V.geom.n_elems, h->st));
+        V.zero32 = false;
+      } else {
+        CU(launch_relax_small<double>(h->var, V.d_bl, V.d_cstart, nb, V.phi64[V.cur64], V.rhs64, V.fx64, V.fy64,
+                                      V.fz64, V.sweep.d_dst, V.sweep.d_src, (int)V.sweep.n, it, V.zero64,
+                                      V.geom.n_elems, h->st));
+        V.zero64 = false;
+      }
+      TRY(chk("relax small", g));
+      h->kernels += 1;
+      return H3D_OK;
+    }
     for (int q = 0; q < it; ++q) TRY(sweep(g));
     return H3D_OK;
   }
@@ -866,7 +908,7 @@ int flush_l2(h3d_mg* h) {
 int autotune_level(h3d_mg* h, int g) {
   Level& V = h->lev[g];
   int best_v = V.variant, best_z = V.zc;
-  if (V.geom.n_interior < 64) return H3D_OK;  // a handful of cells: heuristic
+  if (V.geom.n_interior < 64 || (V.small && g > 1)) return H3D_OK;  // tiny or fused levels: no sweep kernels
   int nzm = 0, nxm = 0, nym = 0;
   for (const auto& B : V.geom.bl) { nzm = std::max(nzm, B.nz); nxm = std::max(nxm, B.nx); nym = std::max(nym, B.ny); }
   cudaEvent_t a, b;
@@ -881,14 +923,18 @@ int autotune_level(h3d_mg* h, int g) {
     for (int zc : {1, 2, 4, 8, 16, 32, 64, 128, 256}) {
       if (zc > nzm || (zc < 8 && V.geom.n_interior >= (1 << 20))) continue;
       TRY(build_tiles(h, V, v, zc));
-      float tot = 1e30f;  // fastest of the timed repetitions (robust to interference)
-      for (int rep = 0; rep < 6; ++rep) {
+      // a cycle runs sweeps from a non-zero and from the zero iterate: fastest
+      // repetition of each, weighted by how often a solve runs them (level 1
+      // of a mixed solve: 5 to 1 with two inner cycles; otherwise 2 to 1)
+      float tn = 1e30f, tz = 1e30f;
+      for (int rep = 0; rep < 12; ++rep) {
+        const bool zero = rep >= 6;
         TRY(flush_l2(h));
         CU(cudaEventRecord(a, h->st));
-        if (f32) CU(launch_rbgs<float>(v, h->var, false, V.d_bl, V.d_tiles, V.ntiles, zc, sweep_maps(V, V.cur32),
+        if (f32) CU(launch_rbgs<float>(v, h->var, zero, V.d_bl, V.d_tiles, V.ntiles, zc, sweep_maps(V, V.cur32),
                                        rhs_maps(V), h->d_err, V.phi32[V.cur32],
                                        V.phi32[1 - V.cur32], V.rhs32, V.fx32, V.fy32, V.fz32, h->st));
-        else CU(launch_rbgs<double>(v, h->var, false, V.d_bl, V.d_tiles, V.ntiles, zc, sweep_maps(V, V.cur64),
+        else CU(launch_rbgs<double>(v, h->var, zero, V.d_bl, V.d_tiles, V.ntiles, zc, sweep_maps(V, V.cur64),
                                     rhs_maps(V), h->d_err, V.phi64[V.cur64],
                                     V.phi64[1 - V.cur64], V.rhs64, V.fx64, V.fy64, V.fz64, h->st));
         CU(cudaEventRecord(b, h->st));
@@ -904,8 +950,9 @@ int autotune_level(h3d_mg* h, int g) {
         }
         float t;
         CU(cudaEventElapsedTime(&t, a, b));
-        if (rep > 0) tot = std::min(tot, t);
+        if (rep % 6 > 0) (zero ? tz : tn) = std::min(zero ? tz : tn, t);
       }
+      const float tot = tn * ((g == 1 && h->mixed) ? 5.f : 2.f) + tz;
       if (tot < best) { best = tot; best_v = v; best_z = zc; }
     }
   }
@@ -935,10 +982,7 @@ int autotune_restrict(h3d_mg* h, int gc) {
     for (int zc : {1, 2, 4, 8, 16, 32, 64}) {
       if (zc > nzm) continue;
       std::vector<Tile> t = row_tiles(C.geom, r.tyc, zc);
-      dfree(C.d_rtiles);
-      C.d_rtiles = nullptr;
-      TRY(dalloc(h, &C.d_rtiles, t.size()));
-      CU(cudaMemcpy(C.d_rtiles, t.data(), t.size() * sizeof(Tile), cudaMemcpyHostToDevice));
+      TRY(upload_tiles(h, &C.d_rtiles, &C.rtiles_cap, t));
       C.nrtiles = (int)t.size();
       float tot = 1e30f;  // fastest of the timed repetitions
       for (int rep = 0; rep < 6; ++rep) {
@@ -974,10 +1018,7 @@ int autotune_restrict(h3d_mg* h, int gc) {
   cudaEventDestroy(b);
   RestrictShape r = restrict_shape(best_v);
   std::vector<Tile> t = row_tiles(C.geom, r.tyc, best_z);
-  dfree(C.d_rtiles);
-  C.d_rtiles = nullptr;
-  TRY(dalloc(h, &C.d_rtiles, t.size()));
-  CU(cudaMemcpy(C.d_rtiles, t.data(), t.size() * sizeof(Tile), cudaMemcpyHostToDevice));
+  TRY(upload_tiles(h, &C.d_rtiles, &C.rtiles_cap, t));
   C.nrtiles = (int)t.size();
   C.rvariant = best_v;
   C.rzc = best_z;
@@ -1099,7 +1140,7 @@ int h3d_mg_destroy(h3d_mg* h) {
     void* ps[] = {V.d_bl, V.d_cta_all, V.d_cta_int, V.d_rows_all, V.d_rows_int, V.d_tiles, V.phi64[0], V.phi64[1], V.rhs64, V.phi32[0],
                   V.phi32[1], V.rhs32, V.fx64, V.fy64, V.fz64, V.fx32, V.fy32, V.fz32, V.dens,
                   V.sweep.d_dst, V.sweep.d_src, V.faces.d_dst, V.faces.d_src, V.exch.d_dst, V.exch.d_src,
-                  V.bound.d_dst, V.bound.d_src, V.d_maps, V.d_rmaps, V.d_rtiles, V.d_ptiles};
+                  V.bound.d_dst, V.bound.d_src, V.d_maps, V.d_rmaps, V.d_rtiles, V.d_ptiles, V.d_cstart};
     for (void* p : ps) dfree(p);
   }
   dfree(h->p64[0]);
@@ -1212,6 +1253,19 @@ int h3d_mg_create(h3d_mg** out, const h3d_mg_desc* desc) {
     std::string err;
     if ((rc = build_halo_table(h->blocks, g, kHaloSweep, true, d, s, &err)) != H3D_OK) return bail(fail(h, rc, err));
     if ((rc = upload_halo(h, V.sweep, d, s)) != H3D_OK) return bail(rc);
+    // small levels relax in one fused launch when their fill reads interior cells only
+    if (g > 1 && V.geom.n_interior <= kSmallLevelCells && V.geom.bl.size() <= (size_t)kSmallLevelBlocks) {
+      bool old = false;
+      for (uint32_t v : s) old = old || (v & kOldFlag);
+      if (!old) {
+        std::vector<int> cs(1, 0);
+        for (const auto& B : V.geom.bl) cs.push_back(cs.back() + B.nx * B.ny * B.nz);
+        if ((rc = dalloc(h, &V.d_cstart, cs.size())) != H3D_OK) return bail(rc);
+        if (cudaMemcpy(V.d_cstart, cs.data(), cs.size() * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess)
+          return bail(fail(h, H3D_ERR_CUDA, "small-level table"));
+        V.small = true;
+      }
+    }
     if (g == 1) {
       if ((rc = build_halo_table(h->blocks, g, kHaloFaces, true, d, s, &err)) != H3D_OK) return bail(fail(h, rc, err));
       if ((rc = upload_halo(h, V.faces, d, s)) != H3D_OK) return bail(rc);
@@ -1708,10 +1762,7 @@ int h3d_mg_set_restriction(h3d_mg* h, int32_t g, int32_t variant, int32_t zchunk
     return fail(h, H3D_ERR_ARG, "restriction variant does not fit this level");
   CU(cudaSetDevice(h->device));
   std::vector<Tile> t = row_tiles(C.geom, r.tyc, zchunk);
-  dfree(C.d_rtiles);
-  C.d_rtiles = nullptr;
-  TRY(dalloc(h, &C.d_rtiles, t.size()));
-  CU(cudaMemcpy(C.d_rtiles, t.data(), t.size() * sizeof(Tile), cudaMemcpyHostToDevice));
+  TRY(upload_tiles(h, &C.d_rtiles, &C.rtiles_cap, t));
   C.nrtiles = (int)t.size();
   C.rvariant = variant;
   C.rzc = zchunk;
