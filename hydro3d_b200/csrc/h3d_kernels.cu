@@ -403,6 +403,13 @@ __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
 
+// First 128-byte boundary of the dynamic shared memory, by pointer arithmetic
+// on the shared array itself so that accesses through it stay shared-memory
+// instructions (a round trip through an integer would make them generic).
+__device__ __forceinline__ unsigned char* smem_base128(unsigned char* raw) {
+  return raw + ((128u - (smem_u32(raw) & 127u)) & 127u);
+}
+
 // Bounded wait on an mbarrier phase: gives up after ~2^26 SM clocks (tens of
 // ms; a plane copy takes microseconds), records the failure in *err and makes
 // every later wait of this thread return at once, so a failed copy can never
@@ -473,7 +480,7 @@ __global__ void __launch_bounds__(TPR*(TY + 2)) k_rbgs_tma2(const BlkLev* __rest
   using C = Tma2Cfg<T, TPR, CP, TY, D>;
   constexpr int NS = C::NS;
   extern __shared__ unsigned char smem_raw[];
-  unsigned char* base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
+  unsigned char* base = smem_base128(smem_raw);
   uint64_t* bars = reinterpret_cast<uint64_t*>(base + NS * C::SLOT);
 
   const Tile t = tiles[blockIdx.x];
@@ -621,7 +628,7 @@ __global__ void __launch_bounds__(TPR*(TY + 2)) k_rbgs_vec(const BlkLev* __restr
   using C = VecCfg<TPR, GPT, TY, NS, D>;
   static_assert(D + 4 <= NS, "a plane is read until three phases after its own");
   extern __shared__ unsigned char smem_raw[];
-  unsigned char* base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
+  unsigned char* base = smem_base128(smem_raw);
   uint64_t* bars = reinterpret_cast<uint64_t*>(base + NS * C::SLOT);
 
   const Tile t = tiles[blockIdx.x];
@@ -1283,6 +1290,9 @@ static const TileShape kShapes[] = {
     {128, 16, 576, true, 32, 1, 3, 29}, {128, 8, 320, true, 32, 1, 3, 9},           // 42, 43
     {64, 8, 160, true, 16, 1, 3, 10},   {64, 16, 288, true, 16, 1, 3, 11},          // 44, 45
     {32, 16, 144, true, 8, 1, 3, 12},   {16, 16, 72, true, 4, 1, 3, 13},            // 46, 47
+    // register-window sweeps with two groups per lane
+    {128, 16, 288, true, 16, 2, 3, 29}, {128, 8, 160, true, 16, 2, 3, 9},           // 48, 49
+    {64, 16, 144, true, 8, 2, 3, 11},                                               // 50
 };
 #ifdef H3D_BOUNDS_CHECK
 // Debug builds only: first recorded out-of-bounds access {kernel id + 1, block, index, limit}.
@@ -1389,18 +1399,45 @@ static cudaError_t tma2_dispatch(bool var, const BlkLev* bl, const Tile* tiles, 
   X(27, 32, 2, 8, 2)       \
   X(28, 8, 1, 16, 2)
 
+// One cell of the seven-point update: (rhs - off-diagonal sum) x diagonal reciprocal.
+__device__ __forceinline__ float win_upd(float w, float e, float s, float n, float b, float t, float rv, float aw,
+                                         float ae, float as, float an, float ab, float at, float iv) {
+  const float sum = fmaf(at, t, fmaf(ab, b, fmaf(an, n, fmaf(as, s, fmaf(ae, e, aw * w)))));
+  return (rv - sum) * iv;
+}
+
+// The two cells of one colour of a group of four (positions 0, 2 when q1 is
+// false, else 1, 3).  aw0 / iv0 belong to the first cell of the group, ae3 /
+// iv3 to the last, iv12 to the middle two.
+__device__ __forceinline__ void win_colour(float4& c, const float4& bz, const float4& tz, const float4& u,
+                                           const float4& dn, const float4& rh, float l, float r, bool q1, float aw0,
+                                           float ae3, float ax, float as, float an, float ab, float at, float iv0,
+                                           float iv12, float iv3) {
+  if (!q1) {
+    c.x = win_upd(l, c.y, u.x, dn.x, bz.x, tz.x, rh.x, aw0, ax, as, an, ab, at, iv0);
+    c.z = win_upd(c.y, c.w, u.z, dn.z, bz.z, tz.z, rh.z, ax, ax, as, an, ab, at, iv12);
+  } else {
+    c.y = win_upd(c.x, c.z, u.y, dn.y, bz.y, tz.y, rh.y, ax, ax, as, an, ab, at, iv12);
+    c.w = win_upd(c.z, r, u.w, dn.w, bz.w, tz.w, rh.w, ax, ae3, as, an, ab, at, iv3);
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Register-window TMA sweep (k_rbgs_win), FP32 with constant coefficients.
 //
-// Same phases, staging and results as k_rbgs_vec (GPT = 1), but a thread keeps
-// its own group of planes z-3 .. z+1 in registers for the whole z march, so a
-// phase reads from shared memory only the group of the new plane z+1, the
-// rows y-1 and y+1 at planes z (red) and z-2 (black) and the right-hand side;
-// the cells left and right of the group come from the neighbouring lanes by
-// warp shuffles (a row is TPR consecutive lanes), the ghost columns from
-// shared memory.  A plane is last read two phases after its own, so the ring
-// needs D+3 slots.
-template <int TPR, int TY, int NS, int D, bool ZERO>
+// Same phases, staging and results as k_rbgs_vec, but a thread keeps its own
+// GPT groups of four cells (x0 = 1 + 4g, g = j + k*TPR) of planes z-3 .. z+1
+// in registers for the whole z march, so a phase reads from shared memory
+// only the groups of the new plane z+1, the rows y-1 and y+1 at planes z
+// (red) and z-2 (black) and the right-hand side; the cells left and right of
+// a group come from the neighbouring lanes by warp shuffles (a row is TPR
+// consecutive lanes), the ghost columns from shared memory.  A plane is last
+// read two phases after its own, so the ring needs D+3 slots.  ZERO: the
+// source iterate is identically zero (first sweep of a cycle): only the
+// right-hand side is staged, red cells are rhs times the diagonal reciprocal,
+// and black cells read the red values of neighbours in the block (zero
+// outside it).  GPT = 2 halves the per-plane overhead per cell.
+template <int TPR, int GPT, int TY, int NS, int D, bool ZERO>
 __global__ void __launch_bounds__(TPR*(TY + 2)) k_rbgs_win(const BlkLev* __restrict__ bls,
                                                           const Tile* __restrict__ tiles, int zc,
                                                           const CUtensorMap* __restrict__ maps,
@@ -1408,10 +1445,13 @@ __global__ void __launch_bounds__(TPR*(TY + 2)) k_rbgs_win(const BlkLev* __restr
                                                           float* __restrict__ dst, int* err) {
   pdl_trigger();
   pdl_wait();
-  using C = VecCfg<TPR, 1, TY, NS, D>;
+  using C = VecCfg<TPR, GPT, TY, NS, D>;
   static_assert(TPR <= 32 && (TPR & (TPR - 1)) == 0, "a row is a power-of-two lane segment of one warp");
+  static_assert(GPT == 1 || GPT == 2, "one or two groups per lane");
+  constexpr int R = TY + 2;         // rows of a tile with its two halo rows
+  constexpr int RE = (R + 1) / 2;   // rows of even index within the tile
   extern __shared__ unsigned char smem_raw[];
-  unsigned char* base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
+  unsigned char* base = smem_base128(smem_raw);
   uint64_t* bars = reinterpret_cast<uint64_t*>(base + NS * C::SLOT);
 
   const Tile t = tiles[blockIdx.x];
@@ -1419,22 +1459,30 @@ __global__ void __launch_bounds__(TPR*(TY + 2)) k_rbgs_win(const BlkLev* __restr
   const CUtensorMap* map = maps + t.b;
   const CUtensorMap* rmap = rmaps + t.b;
   const int nx = B.nx, ny = B.ny, nz = B.nz;
-  const long long sx = B.sx, sxy = B.sxy;
+  const long long sxy = B.sxy;
   const int y0 = t.y0, zs = t.z0;
   const int ze = min(zs + zc - 1, nz);
   const int zlo = max(zs - 1, 1), zhi = min(ze + 1, nz);
   const int BX = (nx + 2 + kXOff + 3) & ~3;  // smem row pitch == TMA box width
   const uint32_t tx_bytes = (uint32_t)(BX * ((ZERO ? 0 : TY + 4) + TY + 2) * 4);
-  const int tr = threadIdx.x / TPR, j = threadIdx.x % TPR;
+  // Lane segments hold rows of equal parity back to back (even rows first),
+  // so a warp that holds several rows updates cells of one colour in a phase.
+  const int seg = threadIdx.x / TPR, j = threadIdx.x % TPR;
+  const int tr = TPR == 32 ? seg : (seg < RE ? 2 * seg : 2 * (seg - RE) + 1);
   const int y = y0 - 1 + tr;
-  const int x0 = 1 + 4 * j;
-  const bool gin = x0 <= nx;
-  const bool yin = gin && y >= 1 && y <= ny;
-  const bool yown = yin && tr >= 1 && tr <= TY;
-  const bool lft = j == 0, rgt = x0 + 3 == nx;  // groups next to the ghost columns
-  const int pc = (tr + 1) * BX + kXOff + x0;    // own group in an iterate slot
-  const int rcol = tr * BX + kXOff + x0;        // own group in a right-hand-side slot
-  float* __restrict__ Drow = dst + B.off + (long long)y * sx + x0;
+  const bool yrow = y >= 1 && y <= ny;
+  int x0[GPT], pc[GPT], rcol[GPT];
+  bool gin[GPT], lft[GPT], rgt[GPT];
+#pragma unroll
+  for (int k = 0; k < GPT; ++k) {
+    x0[k] = 1 + 4 * (j + k * TPR);
+    gin[k] = x0[k] <= nx;
+    lft[k] = x0[k] == 1;
+    rgt[k] = x0[k] + 3 == nx;  // groups next to the ghost columns
+    pc[k] = (tr + 1) * BX + kXOff + x0[k];  // own group in an iterate slot
+    rcol[k] = tr * BX + kXOff + x0[k];      // own group in a right-hand-side slot
+  }
+  float* __restrict__ Drow = dst + B.off + (long long)y * B.sx;
   const bool leader = threadIdx.x == 0;
   bool bad = false;
 
@@ -1443,21 +1491,30 @@ __global__ void __launch_bounds__(TPR*(TY + 2)) k_rbgs_win(const BlkLev* __restr
   const float ax = (float)B.ax, ay = (float)B.ay, az = (float)B.az;
   const float as = (y == 1 && (ph & 4)) ? 0.f : ay;
   const float an = (y == ny && (ph & 8)) ? 0.f : ay;
-  const float aw0 = (x0 == 1 && (ph & 1)) ? 0.f : ax;
-  const float ae3 = (rgt && (ph & 2)) ? 0.f : ax;
-  // diagonal reciprocals of the three kinds of cells of a group, on interior
-  // planes [0], the bottom wall plane [1], the top wall plane [2] and a plane
-  // that is both [3] (nz = 1); no division inside the z march
-  auto rcp3 = [&](float ab, float at, float& i0, float& i3, float& i12) {
-    i0 = 1.f / (-(aw0 + ax + as + an + ab + at));
-    i3 = 1.f / (-(ax + ae3 + as + an + ab + at));
-    i12 = 1.f / (-(ax + ax + as + an + ab + at));
-  };
-  float inv0, inv3, inv12, inv0b, inv3b, inv12b, inv0t, inv3t, inv12t, inv0bt, inv3bt, inv12bt;
-  rcp3(az, az, inv0, inv3, inv12);
-  rcp3(0.f, az, inv0b, inv3b, inv12b);
-  rcp3(az, 0.f, inv0t, inv3t, inv12t);
-  rcp3(0.f, 0.f, inv0bt, inv3bt, inv12bt);
+  float aw0[GPT], ae3[GPT];
+#pragma unroll
+  for (int k = 0; k < GPT; ++k) {
+    aw0[k] = (lft[k] && (ph & 1)) ? 0.f : ax;
+    ae3[k] = (rgt[k] && (ph & 2)) ? 0.f : ax;
+  }
+  // diagonal reciprocals of the three kinds of cells of a group on interior
+  // planes, the bottom wall plane (b), the top wall plane (t) and a plane that
+  // is both (bt, nz = 1): no division inside the z march
+  auto rcp = [&](float aw, float ae, float ab, float at) { return 1.f / (-(aw + ae + as + an + ab + at)); };
+  float i0[GPT], i0b[GPT], i0t[GPT], i0bt[GPT], i3[GPT], i3b[GPT], i3t[GPT], i3bt[GPT];
+#pragma unroll
+  for (int k = 0; k < GPT; ++k) {
+    i0[k] = rcp(aw0[k], ax, az, az);
+    i0b[k] = rcp(aw0[k], ax, 0.f, az);
+    i0t[k] = rcp(aw0[k], ax, az, 0.f);
+    i0bt[k] = rcp(aw0[k], ax, 0.f, 0.f);
+    i3[k] = rcp(ax, ae3[k], az, az);
+    i3b[k] = rcp(ax, ae3[k], 0.f, az);
+    i3t[k] = rcp(ax, ae3[k], az, 0.f);
+    i3bt[k] = rcp(ax, ae3[k], 0.f, 0.f);
+  }
+  const float i12 = rcp(ax, ax, az, az), i12b = rcp(ax, ax, 0.f, az), i12t = rcp(ax, ax, az, 0.f),
+              i12bt = rcp(ax, ax, 0.f, 0.f);
 
   if (leader) {
     for (int q = 0; q < NS; ++q)
@@ -1469,7 +1526,7 @@ __global__ void __launch_bounds__(TPR*(TY + 2)) k_rbgs_win(const BlkLev* __restr
   auto pslot = [&](int s) -> float* { return reinterpret_cast<float*>(base + s * C::SLOT); };
   auto rslot = [&](int s) -> const float* { return reinterpret_cast<const float*>(base + s * C::SLOT + C::PSLOT); };
   auto issue = [&](int z) {  // leader only
-    const int sl = z % NS;
+    const int sl = (int)((unsigned)z % (unsigned)NS);
     const uint32_t bar = smem_u32(bars + sl);
     asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(tx_bytes) : "memory");
@@ -1485,106 +1542,140 @@ __global__ void __launch_bounds__(TPR*(TY + 2)) k_rbgs_win(const BlkLev* __restr
         "l"(reinterpret_cast<uint64_t>(rmap)), "r"(0), "r"(y0 - 1), "r"(z), "r"(bar)
         : "memory");
   };
-  auto wait_plane = [&](int z) {
-    const uint32_t parity = (uint32_t)(((z - zlo + 1) / NS) & 1);
-    mbar_wait(smem_u32(bars + z % NS), parity, err, bad);
+  // plane z sits in slot sl; it is the ((z - zlo + 1) / NS)-th use of that slot
+  auto wait_plane = [&](int sl, int z) {
+    const uint32_t parity = ((unsigned)(z - zlo + 1) / (unsigned)NS) & 1u;
+    mbar_wait(smem_u32(bars + sl), parity, err, bad);
   };
   auto wrap = [](int i) { return i < 0 ? i + NS : (i >= NS ? i - NS : i); };
-  auto upd = [](float w, float e, float s, float n, float b, float tt, float rv, float aw, float ae, float as_,
-                float an_, float ab, float at, float iv) -> float {
-    const float sum = fmaf(at, tt, fmaf(ab, b, fmaf(an_, n, fmaf(as_, s, fmaf(ae, e, aw * w)))));
-    return (rv - sum) * iv;
-  };
-  // Cells of colour q (positions q, q+2) of the own group c in plane z, with
+  // Cells of colour q1 (positions q1, q1+2) of group k (c) in plane z, with
   // the group below (bz) and above (tz), rows y-1 (u) and y+1 (dn), rhs rh,
-  // and the cells left (l) and right (r) of the group.
-  auto colour = [&](float4& c, const float4& bz, const float4& tz, const float4& u, const float4& dn,
-                    const float4& rh, float l, float r, int z, int q) {
-    const bool wlo = z == 1 && (ph & 16), whi = z == nz && (ph & 32);
-    const float ab = wlo ? 0.f : az, at = whi ? 0.f : az;
-    // wall planes change the diagonal
-    const float i0 = wlo ? (whi ? inv0bt : inv0b) : (whi ? inv0t : inv0);
-    const float i3 = wlo ? (whi ? inv3bt : inv3b) : (whi ? inv3t : inv3);
-    const float i12 = wlo ? (whi ? inv12bt : inv12b) : (whi ? inv12t : inv12);
-    if (q == 0) {
-      c.x = upd(l, c.y, u.x, dn.x, bz.x, tz.x, rh.x, aw0, ax, as, an, ab, at, i0);
-      c.z = upd(c.y, c.w, u.z, dn.z, bz.z, tz.z, rh.z, ax, ax, as, an, ab, at, i12);
-    } else {
-      c.y = upd(c.x, c.z, u.y, dn.y, bz.y, tz.y, rh.y, ax, ax, as, an, ab, at, i12);
-      c.w = upd(c.z, r, u.w, dn.w, bz.w, tz.w, rh.w, ax, ae3, as, an, ab, at, i3);
-    }
-  };
+  // and the cells left (l) and right (r) of the group.  Planes off the walls
+  // (all but at most two) take the branch with the interior coefficients; the
+  // branch is uniform over the CTA.
+#define H3D_WIN_COLOUR(c, bz, tz, u, dn, rh, l, r, zz, q1, k)                                                    \
+  do {                                                                                                           \
+    const bool wlo_ = (zz) == 1 && (ph & 16), whi_ = (zz) == nz && (ph & 32);                                    \
+    if (!(wlo_ || whi_)) {                                                                                       \
+      win_colour(c, bz, tz, u, dn, rh, l, r, q1, aw0[k], ae3[k], ax, as, an, az, az, i0[k], i12, i3[k]);          \
+    } else {                                                                                                     \
+      win_colour(c, bz, tz, u, dn, rh, l, r, q1, aw0[k], ae3[k], ax, as, an, wlo_ ? 0.f : az, whi_ ? 0.f : az,   \
+                 wlo_ ? (whi_ ? i0bt[k] : i0b[k]) : (whi_ ? i0t[k] : i0[k]),                                     \
+                 wlo_ ? (whi_ ? i12bt : i12b) : (whi_ ? i12t : i12),                                             \
+                 wlo_ ? (whi_ ? i3bt[k] : i3b[k]) : (whi_ ? i3t[k] : i3[k]));                                    \
+    }                                                                                                            \
+  } while (0)
   auto ld4 = [](const float* p) { return *reinterpret_cast<const float4*>(p); };
   // lanes of this warp that exist (the last warp of a CTA can be partial)
+  constexpr bool kWholeWarps = (TPR * R) % 32 == 0;
   const int wlanes = min(32, (int)blockDim.x - (int)(threadIdx.x & ~31u));
-  const unsigned FULL = wlanes == 32 ? 0xffffffffu : ((1u << wlanes) - 1u);
+  const unsigned FULL = kWholeWarps ? 0xffffffffu : (wlanes == 32 ? 0xffffffffu : ((1u << wlanes) - 1u));
+  // Cells left (.w of the group before) and right (.x of the group after) of
+  // every group k, from the neighbouring lanes of the row (ghost columns and
+  // a zero source outside the row are handled by the caller).
+  auto sides = [&](const float4 (&g)[GPT], float (&l)[GPT], float (&r)[GPT]) {
+#pragma unroll
+    for (int k = 0; k < GPT; ++k) {
+      l[k] = __shfl_up_sync(FULL, g[k].w, 1, TPR);
+      r[k] = __shfl_down_sync(FULL, g[k].x, 1, TPR);
+    }
+    if (GPT == 2) {  // across the two halves of the row: group TPR-1 <-> group TPR
+      const float lw = __shfl_sync(FULL, g[0].w, TPR - 1, TPR);
+      const float rx = __shfl_sync(FULL, g[GPT - 1].x, 0, TPR);
+      if (j == 0) l[GPT - 1] = lw;
+      if (j == TPR - 1) r[0] = rx;
+    }
+  };
 
   if (leader)
     for (int q = zlo - 1; q <= min(zlo + D, zhi + 1); ++q) issue(q);
-  wait_plane(zlo - 1);
-  wait_plane(zlo);
-  int s0 = zlo % NS;  // slot of plane z
-  // own group of planes z-3 .. z+1 (planes below z hold their red updates)
+  int s0 = (int)((unsigned)zlo % (unsigned)NS);  // slot of plane z
+  wait_plane(wrap(s0 - 1), zlo - 1);
+  wait_plane(s0, zlo);
+  // own groups of planes z-3 .. z+1 (planes below z hold their red updates)
   const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f);
-  float4 m3 = zero4, m2 = zero4, p1 = zero4;
-  float4 m1 = ZERO ? zero4 : ld4(pslot(wrap(s0 - 1)) + pc), c0 = ZERO ? zero4 : ld4(pslot(s0) + pc);
-  for (int z = zlo; z <= ze + 2; ++z) {
+  float4 m3[GPT], m2[GPT], m1[GPT], c0[GPT], p1[GPT];
+#pragma unroll
+  for (int k = 0; k < GPT; ++k) {
+    m3[k] = zero4;
+    m2[k] = zero4;
+    p1[k] = zero4;
+    m1[k] = ZERO ? zero4 : ld4(pslot(wrap(s0 - 1)) + pc[k]);
+    c0[k] = ZERO ? zero4 : ld4(pslot(s0) + pc[k]);
+  }
+  long long dz = (long long)(zlo - 2) * sxy;  // offset of plane z-2 in the block
+  for (int z = zlo; z <= ze + 2; ++z, dz += sxy) {
     const int zb = z - 2;
-    const bool red = z <= zhi && yin;              // red cells of plane z
-    const bool blk = zb >= zs && zb <= ze && yown;  // black cells of plane z-2
+    const bool red = z <= zhi && yrow;                                // red cells of plane z
+    const bool blk = zb >= zs && zb <= ze && yrow && tr >= 1 && tr <= TY;  // black cells of plane z-2
+    const bool q1 = (y + z) & 1;  // red cells of plane z at positions 1, 3 of the groups
+    float* Pz = pslot(s0);
+    const float* Rz = rslot(s0);
     const int sb = wrap(s0 - 2);
+    const float* Pb = pslot(sb);
+    const float* Rb = rslot(sb);
     if (z <= zhi) {
-      wait_plane(z + 1);
-      p1 = ZERO ? zero4 : ld4(pslot(wrap(s0 + 1)) + pc);
-    }
-    // neighbours across the group's ends: lanes of the same row, ghost columns at the row ends
-    float rl = __shfl_up_sync(FULL, c0.w, 1, TPR), rr = __shfl_down_sync(FULL, c0.x, 1, TPR);
-    float bl = __shfl_up_sync(FULL, m2.w, 1, TPR), br = __shfl_down_sync(FULL, m2.x, 1, TPR);
-    float4 ur = zero4, dr = zero4, hr, ub = zero4, db = zero4, hb;
-    if (red) {
-      const float* P = pslot(s0);
-      hr = ld4(rslot(s0) + rcol);
+      const int sp = wrap(s0 + 1);
+      wait_plane(sp, z + 1);
       if (!ZERO) {
-        ur = ld4(P + pc - BX);
-        dr = ld4(P + pc + BX);
-        if (lft) rl = P[pc - 1];
-        if (rgt) rr = P[pc + 4];
+#pragma unroll
+        for (int k = 0; k < GPT; ++k) p1[k] = ld4(pslot(sp) + pc[k]);
       }
     }
-    if (blk) {
-      const float* P = pslot(sb);
-      hb = ld4(rslot(sb) + rcol);
-      if (!ZERO) {
-        ub = ld4(P + pc - BX);
-        db = ld4(P + pc + BX);
-        if (lft) bl = P[pc - 1];
-        if (rgt) br = P[pc + 4];
-      } else {  // red neighbours inside the block; the zero source outside it
-        if (y > 1) ub = ld4(P + pc - BX);
-        if (y < ny) db = ld4(P + pc + BX);
-        if (lft) bl = 0.f;
-        if (rgt) br = 0.f;
+    float rl[GPT], rr[GPT], bl[GPT], br[GPT];
+    sides(c0, rl, rr);
+    sides(m2, bl, br);
+#pragma unroll
+    for (int k = 0; k < GPT; ++k) {
+      if (red && gin[k]) {
+        const float4 h = ld4(Rz + rcol[k]);
+        float4 u = zero4, dn = zero4;
+        if (!ZERO) {
+          u = ld4(Pz + pc[k] - BX);
+          dn = ld4(Pz + pc[k] + BX);
+          if (lft[k]) rl[k] = Pz[pc[k] - 1];
+          if (rgt[k]) rr[k] = Pz[pc[k] + 4];
+        }
+        H3D_WIN_COLOUR(c0[k], m1[k], p1[k], u, dn, h, rl[k], rr[k], z, q1, k);
+        *reinterpret_cast<float4*>(Pz + pc[k]) = c0[k];
       }
     }
-    if (red) {
-      colour(c0, m1, p1, ur, dr, hr, rl, rr, z, (y + z) & 1);
-      *reinterpret_cast<float4*>(pslot(s0) + pc) = c0;
-    }
-    if (blk) {
-      colour(m2, m3, m1, ub, db, hb, bl, br, zb, (y + zb + 1) & 1);
-      *reinterpret_cast<float4*>(Drow + (long long)zb * sxy) = m2;
+#pragma unroll
+    for (int k = 0; k < GPT; ++k) {
+      if (blk && gin[k]) {
+        const float4 h = ld4(Rb + rcol[k]);
+        float4 u = zero4, dn = zero4;
+        if (!ZERO) {
+          u = ld4(Pb + pc[k] - BX);
+          dn = ld4(Pb + pc[k] + BX);
+          if (lft[k]) bl[k] = Pb[pc[k] - 1];
+          if (rgt[k]) br[k] = Pb[pc[k] + 4];
+        } else {  // red neighbours inside the block; the zero source outside it
+          if (y > 1) u = ld4(Pb + pc[k] - BX);
+          if (y < ny) dn = ld4(Pb + pc[k] + BX);
+          if (lft[k]) bl[k] = 0.f;
+          if (rgt[k]) br[k] = 0.f;
+        }
+        H3D_WIN_COLOUR(m2[k], m3[k], m1[k], u, dn, h, bl[k], br[k], zb, !q1, k);
+        *reinterpret_cast<float4*>(Drow + dz + x0[k]) = m2[k];
+      }
     }
     // this phase's shared-memory writes are ordered before the TMA that reuses their slot
     asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
     __syncthreads();
     if (leader && z + D + 1 <= zhi + 1) issue(z + D + 1);
-    m3 = m2;
-    m2 = m1;
-    m1 = c0;
-    c0 = p1;
+#pragma unroll
+    for (int k = 0; k < GPT; ++k) {
+      m3[k] = m2[k];
+      m2[k] = m1[k];
+      m1[k] = c0[k];
+      c0[k] = p1[k];
+    }
     s0 = wrap(s0 + 1);
   }
 }
+
+#undef H3D_WIN_COLOUR
 
 template <int TPR, int GPT, int TY, int NS, int D>
 static cudaError_t vec_attr() {
@@ -1601,38 +1692,46 @@ static cudaError_t vec_dispatch(const BlkLev* bl, const Tile* tiles, int ntiles,
   return cudaGetLastError();
 }
 
-template <int TPR, int TY, int NS, int D>
+template <int TPR, int GPT, int TY, int NS, int D>
 static cudaError_t win_attr() {
-  cudaError_t e = cudaFuncSetAttribute(k_rbgs_win<TPR, TY, NS, D, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)VecCfg<TPR, 1, TY, NS, D>::SMEM);
+  cudaError_t e = cudaFuncSetAttribute(k_rbgs_win<TPR, GPT, TY, NS, D, false>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)VecCfg<TPR, GPT, TY, NS, D>::SMEM);
   if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(k_rbgs_win<TPR, TY, NS, D, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)VecCfg<TPR, 1, TY, NS, D>::SMEM);
+  return cudaFuncSetAttribute(k_rbgs_win<TPR, GPT, TY, NS, D, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)VecCfg<TPR, GPT, TY, NS, D>::SMEM);
 }
 
-template <int TPR, int TY, int NS, int D>
+template <int TPR, int GPT, int TY, int NS, int D>
 static cudaError_t win_dispatch(bool zero, const BlkLev* bl, const Tile* tiles, int ntiles, int zc,
                                 const CUtensorMap* maps, const CUtensorMap* rmaps, int* err, float* dst,
                                 cudaStream_t st) {
   static_assert(D + 3 <= NS, "a plane is read until two phases after its own");
   if (ntiles <= 0) return cudaSuccess;
-  constexpr size_t SM = VecCfg<TPR, 1, TY, NS, D>::SMEM;
-  if (zero) pdl_launch(k_rbgs_win<TPR, TY, NS, D, true>, ntiles, TPR * (TY + 2), SM, st, bl, tiles, zc, maps, rmaps, dst, err);
-  else pdl_launch(k_rbgs_win<TPR, TY, NS, D, false>, ntiles, TPR * (TY + 2), SM, st, bl, tiles, zc, maps, rmaps, dst, err);
+  constexpr size_t SM = VecCfg<TPR, GPT, TY, NS, D>::SMEM;
+  if (zero)
+    pdl_launch(k_rbgs_win<TPR, GPT, TY, NS, D, true>, ntiles, TPR * (TY + 2), SM, st, bl, tiles, zc, maps, rmaps, dst,
+               err);
+  else
+    pdl_launch(k_rbgs_win<TPR, GPT, TY, NS, D, false>, ntiles, TPR * (TY + 2), SM, st, bl, tiles, zc, maps, rmaps,
+               dst, err);
   return cudaGetLastError();
 }
 
 constexpr int kFirstWinShape = 40;
-// (variant, lanes per row, rows, ring slots, prefetch depth)
-#define H3D_WIN_SHAPES(X) \
-  X(40, 32, 4, 8, 5)      \
-  X(41, 32, 8, 8, 4)      \
-  X(42, 32, 16, 8, 4)     \
-  X(43, 32, 8, 8, 5)      \
-  X(44, 16, 8, 8, 5)      \
-  X(45, 16, 16, 8, 4)     \
-  X(46, 8, 16, 8, 5)      \
-  X(47, 4, 16, 8, 5)
+// (variant, lanes per row, groups of four cells per lane, rows, ring slots, prefetch depth)
+#define H3D_WIN_SHAPES(X)     \
+  X(40, 32, 1, 4, 8, 5)       \
+  X(41, 32, 1, 8, 8, 4)       \
+  X(42, 32, 1, 16, 8, 4)      \
+  X(43, 32, 1, 8, 8, 5)       \
+  X(44, 16, 1, 8, 8, 5)       \
+  X(45, 16, 1, 16, 8, 4)      \
+  X(46, 8, 1, 16, 8, 5)       \
+  X(47, 4, 1, 16, 8, 5)       \
+  X(48, 16, 2, 16, 8, 4)      \
+  X(49, 16, 2, 8, 8, 4)       \
+  X(50, 8, 2, 16, 8, 4)
 
 // (variant, threads per row, groups of four cells per thread, rows, ring slots, prefetch depth)
 #define H3D_VEC_SHAPES(X)  \
@@ -1677,8 +1776,8 @@ cudaError_t init_kernel_attributes() {
   if ((e = vec_attr<tpr, gpt, ty, ns, d>()) != cudaSuccess) return e;
   H3D_VEC_SHAPES(X)
 #undef X
-#define X(v, tpr, ty, ns, d) \
-  if ((e = win_attr<tpr, ty, ns, d>()) != cudaSuccess) return e;
+#define X(v, tpr, gpt, ty, ns, d) \
+  if ((e = win_attr<tpr, gpt, ty, ns, d>()) != cudaSuccess) return e;
   H3D_WIN_SHAPES(X)
 #undef X
   return e;
@@ -1705,8 +1804,8 @@ cudaError_t launch_rbgs(int variant, bool var, bool zero_src, const BlkLev* bl, 
       case v: return vec_dispatch<tpr, gpt, ty, ns, d>(bl, tiles, ntiles, zc, maps, rmaps, err, reinterpret_cast<float*>(dst), st);
       H3D_VEC_SHAPES(X)
 #undef X
-#define X(v, tpr, ty, ns, d) \
-      case v: return win_dispatch<tpr, ty, ns, d>(zero_src, bl, tiles, ntiles, zc, maps, rmaps, err, reinterpret_cast<float*>(dst), st);
+#define X(v, tpr, gpt, ty, ns, d) \
+      case v: return win_dispatch<tpr, gpt, ty, ns, d>(zero_src, bl, tiles, ntiles, zc, maps, rmaps, err, reinterpret_cast<float*>(dst), st);
       H3D_WIN_SHAPES(X)
 #undef X
       default: break;
@@ -2137,7 +2236,7 @@ __global__ void __launch_bounds__(TPR* TYC) k_restrict_tma(const BlkLev* __restr
   static_assert(D + 2 <= NS, "a fine plane is read until the phase after its own");
   using P2 = typename std::conditional<sizeof(T) == 4, float2, double2>::type;
   extern __shared__ unsigned char smem_raw[];
-  unsigned char* base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
+  unsigned char* base = smem_base128(smem_raw);
   uint64_t* bars = reinterpret_cast<uint64_t*>(base + NS * C::SLOT);
 
   const Tile t = tiles[blockIdx.x];

@@ -252,11 +252,15 @@ def test_mixed_precision_error_vs_fp64(oracle_mod, h3d):
 def test_every_smoother_variant(oracle_mod, h3d, precision):
     """Each smoother kernel variant (generic tiles, whole-row tiles, TMA-staged
     row tiles, single-barrier TMA row tiles) and several z-chunks give the
-    reference sweep, also with ragged row tiles (ny = 12): bit-exact in FP64,
-    within the FP32 tolerance in the mixed solver's FP32 levels."""
+    reference sweep, also with ragged row tiles (ny = 12) and rows longer
+    than one lane segment of the two-groups-per-lane sweeps (nx = 64, 96):
+    bit-exact in FP64, within the FP32 tolerance in the mixed solver's FP32
+    levels."""
     rng = np.random.default_rng(7)
     for layout, need in (((2, 2, 1), (32, 16, 16), [P, P, W, W, W, W], 3), 20), \
-                        (((2, 1, 1), (32, 12, 10), [W, W, P, P, W, W], 2), 10):
+                        (((2, 1, 1), (32, 12, 10), [W, W, P, P, W, W], 2), 10), \
+                        (((1, 1, 1), (96, 12, 8), [W, W, P, P, W, W], 2), 4), \
+                        (((2, 1, 1), (64, 8, 6), [P, P, W, W, W, W], 2), 6):
         blocks, s, orc = _pair(oracle_mod, h3d, layout, precision=precision)
         s.coeff(); orc.coeff()
         _, _, nvar = s.get_smoother(1)
