@@ -1760,6 +1760,8 @@ constexpr int kFirstWinShape = 40;
   X(18, 32, 4, 8)          \
   X(29, 32, 2, 16)
 
+cudaError_t defect_march_attributes();
+
 cudaError_t init_kernel_attributes() {
   cudaError_t e = cudaSuccess;
 #define X(v, tpr, cp, ty)                                                  \
@@ -1780,7 +1782,7 @@ cudaError_t init_kernel_attributes() {
   if ((e = win_attr<tpr, gpt, ty, ns, d>()) != cudaSuccess) return e;
   H3D_WIN_SHAPES(X)
 #undef X
-  return e;
+  return defect_march_attributes();
 }
 
 
@@ -1929,13 +1931,17 @@ cudaError_t launch_restrict(bool var, bool zero_phi, const BlkLev* fine, const B
   return cudaGetLastError();
 }
 
-// mgcorr + mgbound, tiled and vectorised: a CTA owns kProlongRows (32)
-// consecutive fine rows (ghost rows included) of one plane z of one block, a
-// warp every eighth row; a lane takes groups of VEC = 16/sizeof(T) interior cells (x0 = 1 +
-// VEC*g, a 16-byte aligned address in the padded layout: one vector load of
-// the old iterate and one vector store), lanes 0 and 1 the ghost columns.
-// Same interpolation, term order and mgbound source as k_prolong_pairs.
-// Needs nx a multiple of VEC.
+// mgcorr + mgbound, tiled and vectorised.  Fine rows 2k and 2k+1 (ghost
+// rows 0 and ny+1 included, also through their mgbound source) interpolate
+// from the same coarse rows k, k+1, and fine planes 2m, 2m+1 from the same
+// coarse planes m, m+1.  So a CTA owns the plane pair (2m, 2m+1) of one
+// block, a warp a row pair at a time (pairs w, w+8, ...), and a lane a group
+// of VEC = 16/sizeof(T) interior cells (x0 = 1 + VEC*g, a 16-byte aligned
+// address in the padded layout) of all four rows of the quad: one set of
+// coarse loads (2 x 2 coarse rows, VEC/2+2 columns) serves 4 VEC fine cells;
+// one vector load of the old iterate and one vector store per row.  Lanes 0
+// and 1 take the ghost columns.  Same interpolation, term order and mgbound
+// source as k_prolong_pairs.  Needs nx a multiple of VEC and ny, nz even.
 template <typename T, bool ZERO_OLD>
 __global__ void __launch_bounds__(256) k_prolong_vec(const BlkLev* __restrict__ fine, const BlkLev* __restrict__ coarse,
                                                      const Tile* __restrict__ tiles, const T* __restrict__ phi_c,
@@ -1949,110 +1955,129 @@ __global__ void __launch_bounds__(256) k_prolong_vec(const BlkLev* __restrict__ 
   const BlkLev F = fine[t.b];
   const BlkLev C = coarse[t.b];
   const int lane = threadIdx.x & 31;
-  const int z = t.z0;
   const int ph = F.phys;
-  for (int y = t.y0 + (threadIdx.x >> 5); y <= min(t.y0 + kProlongRows - 1, F.ny + 1); y += 8) {
-  int sy = y, sz = z;
-  if (y == 0 && (ph & 4)) sy = 1;
-  if (y == F.ny + 1 && (ph & 8)) sy = F.ny;
-  if (z == 0 && (ph & 16)) sz = 1;
-  if (z == F.nz + 1 && (ph & 32)) sz = F.nz;
-  const T wy0 = (sy & 1) ? T(1) : T(3), wy1 = (sy & 1) ? T(3) : T(1);
-  const T wz0 = (sz & 1) ? T(1) : T(3), wz1 = (sz & 1) ? T(3) : T(1);
-  const T w00 = wy0 * wz0, w10 = wy1 * wz0, w01 = wy0 * wz1, w11 = wy1 * wz1;  // [dj][dk]
-  const T* Pc = phi_c + C.off + (long long)(sz >> 1) * C.sxy + (long long)(sy >> 1) * C.sx;
+  // the two planes of the pair and their mgbound sources
+  int zq[2], szq[2];
+  T wz0[2], wz1[2];
+#pragma unroll
+  for (int iz = 0; iz < 2; ++iz) {
+    const int z = t.z0 + iz;
+    int sz = z;
+    if (z == 0 && (ph & 16)) sz = 1;
+    if (z == F.nz + 1 && (ph & 32)) sz = F.nz;
+    zq[iz] = z;
+    szq[iz] = sz;
+    wz0[iz] = (sz & 1) ? T(1) : T(3);
+    wz1[iz] = (sz & 1) ? T(3) : T(1);
+  }
   const long long cy = C.sx, cz = C.sxy;
-  const T* Orow = old + F.off + (long long)sz * F.sxy + (long long)sy * F.sx;
-  T* Out = out + F.off + (long long)z * F.sxy + (long long)y * F.sx;
-  // value of fine cell x whose mgbound source column is sx (pair index q = x >> 1)
-  auto interp = [&](const T* Q, int sx, T o) -> T {
-    const T wx0 = (sx & 1) ? T(1) : T(3), wx1 = (sx & 1) ? T(3) : T(1);
-    // term order (di,dj,dk): 000, 010, 001, 011, 100, 110, 101, 111 (mgsolver.for:838-892)
-    T s = (wx0 * w00) * Q[0];
-    s = s + (wx0 * w10) * Q[cy];
-    s = s + (wx0 * w01) * Q[cz];
-    s = s + (wx0 * w11) * Q[cy + cz];
-    s = s + (wx1 * w00) * Q[1];
-    s = s + (wx1 * w10) * Q[1 + cy];
-    s = s + (wx1 * w01) * Q[1 + cz];
-    s = s + (wx1 * w11) * Q[1 + cy + cz];
-    return o + s / T(64);
-  };
-  // the eight interpolation weights of odd (x0 = 1 + VEC*g + even m) and even
-  // fine columns, products of small integers, exact in either precision
-  T wo[8], we[8];
-  {
-    const T a[4] = {w00, w10, w01, w11};
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      wo[q] = T(1) * a[q];
-      wo[4 + q] = T(3) * a[q];
-      we[q] = T(3) * a[q];
-      we[4 + q] = T(1) * a[q];
-    }
-  }
-  const T* R00 = Pc;
-  const T* R10 = Pc + cy;
-  const T* R01 = Pc + cz;
-  const T* R11 = Pc + cy + cz;
   const int ng = F.nx / VEC;
-  for (int g = lane; g < ng; g += 32) {
-    const int x0 = 1 + VEC * g;
-    V ov;
-    if (ZERO_OLD) {
-      ov = V{};
-    } else {
-      ov = *reinterpret_cast<const V*>(Orow + x0);
-    }
-    T o[VEC], r[VEC];
-    *reinterpret_cast<V*>(o) = ov;
-    // the group's coarse values: columns (x0 >> 1) .. +NC-1 of the 2x2 coarse rows/planes
-    T cq[4][NC];
-    const int c0 = x0 >> 1;
+  for (int k = threadIdx.x >> 5; k <= F.ny / 2; k += 8) {
+    // rows 2k, 2k+1 and their sources
+    int yq[2], syq[2];
+    T wy0[2], wy1[2];
 #pragma unroll
-    for (int c = 0; c < NC; ++c) {
-      cq[0][c] = R00[c0 + c];
-      cq[1][c] = R10[c0 + c];
-      cq[2][c] = R01[c0 + c];
-      cq[3][c] = R11[c0 + c];
+    for (int iy = 0; iy < 2; ++iy) {
+      const int y = 2 * k + iy;
+      int sy = y;
+      if (y == 0 && (ph & 4)) sy = 1;
+      if (y == F.ny + 1 && (ph & 8)) sy = F.ny;
+      yq[iy] = y;
+      syq[iy] = sy;
+      wy0[iy] = (sy & 1) ? T(1) : T(3);
+      wy1[iy] = (sy & 1) ? T(3) : T(1);
     }
+    // coarse row k, plane m of the quad (the same for its four rows)
+    const T* Pc = phi_c + C.off + (long long)(szq[0] >> 1) * C.sxy + (long long)(syq[0] >> 1) * C.sx;
+    const T* R00 = Pc;
+    const T* R10 = Pc + cy;
+    const T* R01 = Pc + cz;
+    const T* R11 = Pc + cy + cz;
+    for (int g = lane; g < ng; g += 32) {
+      const int x0 = 1 + VEC * g;
+      T cq[4][NC];
+      const int c0 = x0 >> 1;
 #pragma unroll
-    for (int m = 0; m < VEC; ++m) {
-      const int kq = (m + 1) >> 1;  // (x >> 1) - (x0 >> 1) for x = x0 + m, x0 odd
-      const T* W = (m & 1) ? we : wo;  // x0 + m odd for even m
-      // term order (di,dj,dk): 000, 010, 001, 011, 100, 110, 101, 111 (mgsolver.for:838-892)
-      T s;
-      if (sizeof(T) == 8) {
-        s = W[0] * cq[0][kq];
-        s = s + W[1] * cq[1][kq];
-        s = s + W[2] * cq[2][kq];
-        s = s + W[3] * cq[3][kq];
-        s = s + W[4] * cq[0][kq + 1];
-        s = s + W[5] * cq[1][kq + 1];
-        s = s + W[6] * cq[2][kq + 1];
-        s = s + W[7] * cq[3][kq + 1];
-        r[m] = o[m] + s / T(64);
-      } else {  // FP32 inner solve: fused multiply-adds
-        s = W[0] * cq[0][kq];
-        s = fma(W[1], cq[1][kq], s);
-        s = fma(W[2], cq[2][kq], s);
-        s = fma(W[3], cq[3][kq], s);
-        s = fma(W[4], cq[0][kq + 1], s);
-        s = fma(W[5], cq[1][kq + 1], s);
-        s = fma(W[6], cq[2][kq + 1], s);
-        s = fma(W[7], cq[3][kq + 1], s);
-        r[m] = fma(s, T(1.0 / 64), o[m]);
+      for (int c = 0; c < NC; ++c) {
+        cq[0][c] = R00[c0 + c];
+        cq[1][c] = R10[c0 + c];
+        cq[2][c] = R01[c0 + c];
+        cq[3][c] = R11[c0 + c];
       }
+#pragma unroll
+      for (int iz = 0; iz < 2; ++iz)
+#pragma unroll
+        for (int iy = 0; iy < 2; ++iy) {
+          const T w00 = wy0[iy] * wz0[iz], w10 = wy1[iy] * wz0[iz], w01 = wy0[iy] * wz1[iz],
+                  w11 = wy1[iy] * wz1[iz];  // [dj][dk]
+          // the eight weights of odd (wo) and even (we) fine columns: products of small integers
+          const T wo[8] = {w00, w10, w01, w11, T(3) * w00, T(3) * w10, T(3) * w01, T(3) * w11};
+          const T we[8] = {T(3) * w00, T(3) * w10, T(3) * w01, T(3) * w11, w00, w10, w01, w11};
+          const long long ro = F.off + (long long)szq[iz] * F.sxy + (long long)syq[iy] * F.sx;
+          V ov;
+          if (ZERO_OLD) ov = V{};
+          else ov = *reinterpret_cast<const V*>(old + ro + x0);
+          T o[VEC], r[VEC];
+          *reinterpret_cast<V*>(o) = ov;
+#pragma unroll
+          for (int m = 0; m < VEC; ++m) {
+            const int kq = (m + 1) >> 1;  // (x >> 1) - (x0 >> 1) for x = x0 + m, x0 odd
+            const T* W = (m & 1) ? we : wo;  // x0 + m odd for even m
+            // term order (di,dj,dk): 000, 010, 001, 011, 100, 110, 101, 111 (mgsolver.for:838-892)
+            T sum;
+            if (sizeof(T) == 8) {
+              sum = W[0] * cq[0][kq];
+              sum = sum + W[1] * cq[1][kq];
+              sum = sum + W[2] * cq[2][kq];
+              sum = sum + W[3] * cq[3][kq];
+              sum = sum + W[4] * cq[0][kq + 1];
+              sum = sum + W[5] * cq[1][kq + 1];
+              sum = sum + W[6] * cq[2][kq + 1];
+              sum = sum + W[7] * cq[3][kq + 1];
+              r[m] = o[m] + sum / T(64);
+            } else {  // FP32 inner solve: fused multiply-adds
+              sum = W[0] * cq[0][kq];
+              sum = fma(W[1], cq[1][kq], sum);
+              sum = fma(W[2], cq[2][kq], sum);
+              sum = fma(W[3], cq[3][kq], sum);
+              sum = fma(W[4], cq[0][kq + 1], sum);
+              sum = fma(W[5], cq[1][kq + 1], sum);
+              sum = fma(W[6], cq[2][kq + 1], sum);
+              sum = fma(W[7], cq[3][kq + 1], sum);
+              r[m] = fma(sum, T(1.0 / 64), o[m]);
+            }
+          }
+          *reinterpret_cast<V*>(out + F.off + (long long)zq[iz] * F.sxy + (long long)yq[iy] * F.sx + x0) =
+              *reinterpret_cast<const V*>(r);
+        }
     }
-    *reinterpret_cast<V*>(Out + x0) = *reinterpret_cast<const V*>(r);
-  }
-  if (lane < 2) {  // ghost columns, evaluated at their mgbound source
-    const int x = lane ? F.nx + 1 : 0;
-    int sx = x;
-    if (x == 0 && (ph & 1)) sx = 1;
-    if (x == F.nx + 1 && (ph & 2)) sx = F.nx;
-    Out[x] = interp(Pc + (x >> 1), sx, ZERO_OLD ? T(0) : Orow[sx]);
-  }
+    if (lane < 2) {  // ghost columns, evaluated at their mgbound source
+      const int x = lane ? F.nx + 1 : 0;
+      int sx = x;
+      if (x == 0 && (ph & 1)) sx = 1;
+      if (x == F.nx + 1 && (ph & 2)) sx = F.nx;
+      const T wx0 = (sx & 1) ? T(1) : T(3), wx1 = (sx & 1) ? T(3) : T(1);
+      const T* Q = Pc + (x >> 1);
+#pragma unroll
+      for (int iz = 0; iz < 2; ++iz)
+#pragma unroll
+        for (int iy = 0; iy < 2; ++iy) {
+          const T w00 = wy0[iy] * wz0[iz], w10 = wy1[iy] * wz0[iz], w01 = wy0[iy] * wz1[iz],
+                  w11 = wy1[iy] * wz1[iz];
+          const long long ro = F.off + (long long)szq[iz] * F.sxy + (long long)syq[iy] * F.sx;
+          const T o = ZERO_OLD ? T(0) : old[ro + sx];
+          // term order (di,dj,dk): 000, 010, 001, 011, 100, 110, 101, 111 (mgsolver.for:838-892)
+          T sum = (wx0 * w00) * Q[0];
+          sum = sum + (wx0 * w10) * Q[cy];
+          sum = sum + (wx0 * w01) * Q[cz];
+          sum = sum + (wx0 * w11) * Q[cy + cz];
+          sum = sum + (wx1 * w00) * Q[1];
+          sum = sum + (wx1 * w10) * Q[1 + cy];
+          sum = sum + (wx1 * w01) * Q[1 + cz];
+          sum = sum + (wx1 * w11) * Q[1 + cy + cz];
+          out[F.off + (long long)zq[iz] * F.sxy + (long long)yq[iy] * F.sx + x] = o + sum / T(64);
+        }
+    }
   }
 }
 
@@ -2159,6 +2184,254 @@ __global__ void __launch_bounds__(256) k_defect_vec(const BlkLev* __restrict__ b
   }
   block_reduce4<256>(rr, bb, rm, rs, partials + 4 * (size_t)blockIdx.x);
 }
+
+// The same defect as a z march: a CTA owns kDefectRows rows of one block
+// over a chunk of planes, a warp a row (plus a warp for each halo row), a
+// lane GP pairs of cells (x0, x0+1), x0 = 1 + 2(lane + 32k), and the lanes
+// 0 and 1 the ghost columns x = 0 and x = nx + 1.  Every thread streams its
+// own cells of p, e and b into a private ring of kDefectRing planes in
+// shared memory with asynchronous copies (cp.async) issued kDefectRing
+// planes ahead, so DRAM sees the whole chunk in flight without registers
+// held for it; a thread reads back only what it copied itself (its own
+// wait_group orders it), so the ring needs no barrier.  p (+e) of planes
+// z-1 .. z+1 of its own cells stays in registers; the rows y-1, y+1 and the
+// cells left and right of a pair come from plane z staged in shared memory
+// (two buffers, one barrier a plane).  Cells written: p_next over the whole
+// padded block (ghost rows, columns and planes by the tiles and lanes that
+// hold them), rhs_out and the sums over the interior.  Same residual
+// arithmetic as k_defect; per-CTA partial sums in a fixed order.  Needs nx
+// even, nx <= 64 GP and constant coefficients.
+constexpr int kDefectRows = 8;
+constexpr int kDefectRing = 3;
+template <typename TE, int GP>
+struct DefectCfg {
+  static constexpr int R = kDefectRows + 2;  // rows with the two halo rows
+  static constexpr int RW = 64 * GP + 4;     // row: [pad, x = 0 .. nx + 1, pad...]; pairs 16-byte aligned
+  static constexpr size_t STAGE = 2ull * R * RW * sizeof(double);
+  static constexpr size_t RAWP = (size_t)kDefectRing * R * RW * sizeof(double);
+  static constexpr size_t RAWE = (size_t)kDefectRing * R * RW * sizeof(TE);
+  static constexpr size_t RAWB = (size_t)kDefectRing * kDefectRows * RW * sizeof(double);
+  static constexpr size_t SMEM = STAGE + RAWP + RAWE + RAWB + 128;  // + alignment of the dynamic base
+  static_assert(SMEM <= 232448, "defect ring exceeds shared memory");
+};
+
+__device__ __forceinline__ void cp_async16(void* sdst, const void* gsrc) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(smem_u32(sdst)), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void* sdst, const void* gsrc) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(smem_u32(sdst)), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async4(void* sdst, const void* gsrc) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(smem_u32(sdst)), "l"(gsrc) : "memory");
+}
+template <typename T>
+__device__ __forceinline__ void cp_async_pair(T* sdst, const T* gsrc) {  // two elements
+  if (sizeof(T) == 8) cp_async16(sdst, gsrc);
+  else cp_async8(sdst, gsrc);
+}
+template <typename T>
+__device__ __forceinline__ void cp_async_one(T* sdst, const T* gsrc) {
+  if (sizeof(T) == 8) cp_async8(sdst, gsrc);
+  else cp_async4(sdst, gsrc);
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+template <typename TE, typename TR, bool HAS_E, int GP>
+__global__ void __launch_bounds__(32 * (kDefectRows + 2)) k_defect_march(
+    const BlkLev* __restrict__ bls, const Tile* __restrict__ tiles, int zc, const double* __restrict__ p,
+    const TE* __restrict__ e, double* __restrict__ p_next, const double* __restrict__ bvec, TR* __restrict__ rhs_out,
+    double mean_b, double rscale, double* __restrict__ partials) {
+  pdl_trigger();
+  pdl_wait();
+  using C = DefectCfg<TE, GP>;
+  constexpr int R = C::R, RW = C::RW, NR = kDefectRing;
+  extern __shared__ unsigned char smem_raw[];
+  unsigned char* base = smem_base128(smem_raw);
+  double(*sm)[R][RW] = reinterpret_cast<double(*)[R][RW]>(base);
+  double(*rp)[R][RW] = reinterpret_cast<double(*)[R][RW]>(base + C::STAGE);
+  TE(*re)[R][RW] = reinterpret_cast<TE(*)[R][RW]>(base + C::STAGE + C::RAWP);
+  double(*rb)[kDefectRows][RW] = reinterpret_cast<double(*)[kDefectRows][RW]>(base + C::STAGE + C::RAWP + C::RAWE);
+  using R2 = typename std::conditional<sizeof(TR) == 4, float2, double2>::type;
+  using E2 = typename std::conditional<sizeof(TE) == 4, float2, double2>::type;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  double rr = 0, bb = 0, rm = 0, rs = 0;
+  const Tile t = tiles[blockIdx.x];
+  const BlkLev B = bls[t.b];
+  const int nx = B.nx, ny = B.ny, nz = B.nz;
+  const long long sx = B.sx, sxy = B.sxy;
+  const int zs = t.z0, ze = min(t.z0 + zc - 1, nz);
+  const int y = t.y0 - 1 + w;
+  const bool yin = y >= 0 && y <= ny + 1;                              // the row exists (ghost rows included)
+  const bool own = y >= t.y0 && y <= min(t.y0 + kDefectRows - 1, ny);  // interior rows of this tile
+  const bool wr = HAS_E && (own || (yin && (y == 0 || y == ny + 1)));  // rows whose p_next this tile writes
+  const long long row = B.off + (long long)y * sx;                     // cell (0, y, 0)
+  const int ng = nx >> 1;
+  bool gv[GP];
+#pragma unroll
+  for (int k = 0; k < GP; ++k) gv[k] = yin && lane + 32 * k < ng;
+  auto x0 = [&](int k) { return 1 + 2 * (lane + 32 * k); };
+  const bool gc = yin && lane < 2;  // lanes 0 and 1 hold the ghost columns x = 0 and x = nx + 1
+  const int gx = lane == 0 ? 0 : nx + 1;
+
+  // copy this thread's cells of plane z (p, e, and b on interior planes) into ring slot z - zs + 1 (mod NR)
+  auto issue = [&](int z) {
+    if (z <= ze + 1) {
+      const int sl = (z - zs + 1) % NR;
+      const long long rz = row + (long long)z * sxy;
+#pragma unroll
+      for (int k = 0; k < GP; ++k)
+        if (gv[k]) {
+          cp_async_pair(&rp[sl][w][1 + x0(k)], p + rz + x0(k));
+          if (HAS_E) cp_async_pair(&re[sl][w][1 + x0(k)], e + rz + x0(k));
+          if (own && z >= zs && z <= ze) cp_async_pair(&rb[sl][w - 1][1 + x0(k)], bvec + rz + x0(k));
+        }
+      if (gc) {
+        cp_async_one(&rp[sl][w][1 + gx], p + rz + gx);
+        if (HAS_E) cp_async_one(&re[sl][w][1 + gx], e + rz + gx);
+      }
+    }
+    cp_async_commit();  // one group per plane, empty ones included
+  };
+  // this thread's p (+ e) of planes z-1, z, z+1 and b of planes z, z+1
+  double2 P[3][GP], bz[GP], bz1[GP];
+  double G[3];
+  // plane z from its ring slot (the copies of the NR-1 later planes may still be in flight)
+  auto take = [&](double2 (&q)[GP], double& g, double2 (&bq)[GP], int z) {
+    cp_async_wait<NR - 1>();
+    const int sl = (z - zs + 1) % NR;
+#pragma unroll
+    for (int k = 0; k < GP; ++k)
+      if (gv[k]) {
+        double2 a = *reinterpret_cast<const double2*>(&rp[sl][w][1 + x0(k)]);
+        if (HAS_E) {
+          const E2 d = *reinterpret_cast<const E2*>(&re[sl][w][1 + x0(k)]);
+          a.x = a.x + (double)d.x;
+          a.y = a.y + (double)d.y;
+        }
+        q[k] = a;
+        if (own && z >= zs && z <= ze) bq[k] = *reinterpret_cast<const double2*>(&rb[sl][w - 1][1 + x0(k)]);
+      }
+    if (gc) g = HAS_E ? rp[sl][w][1 + gx] + (double)re[sl][w][1 + gx] : rp[sl][w][1 + gx];
+    issue(z + NR);  // the slot is free again (this thread read back only what it copied)
+  };
+  auto store_next = [&](const double2 (&q)[GP], double g, int z) {  // p_next = p + e of plane z
+    const long long rz = row + (long long)z * sxy;
+#pragma unroll
+    for (int k = 0; k < GP; ++k)
+      if (gv[k]) *reinterpret_cast<double2*>(p_next + rz + x0(k)) = q[k];
+    if (gc) p_next[rz + gx] = g;
+  };
+
+#pragma unroll
+  for (int q = 0; q < NR; ++q) issue(zs - 1 + q);
+  take(P[0], G[0], bz, zs - 1);
+  take(P[1], G[1], bz, zs);
+  if (wr && zs == 1) store_next(P[0], G[0], 0);  // ghost plane below
+  for (int z = zs; z <= ze; ++z) {
+    const int buf = z & 1;
+    const long long rz = row + (long long)z * sxy;
+    take(P[2], G[2], bz1, z + 1);
+    // stage plane z
+    if (yin) {
+#pragma unroll
+      for (int k = 0; k < GP; ++k)
+        if (gv[k]) *reinterpret_cast<double2*>(&sm[buf][w][1 + x0(k)]) = P[1][k];
+      if (gc) sm[buf][w][1 + gx] = G[1];
+    }
+    __syncthreads();
+    if (own) {
+#pragma unroll
+      for (int k = 0; k < GP; ++k) {
+        if (!gv[k]) continue;
+        const int xa = x0(k);
+        const double2 pc = P[1][k], bo = P[0][k], to = P[2][k], b2 = bz[k];
+        const double2 so = *reinterpret_cast<const double2*>(&sm[buf][w - 1][1 + xa]);
+        const double2 no = *reinterpret_cast<const double2*>(&sm[buf][w + 1][1 + xa]);
+        const double wv = sm[buf][w][xa], ev = sm[buf][w][xa + 3];
+        const long long i = rz + xa;
+        const Coef<double> c0 = cell_coef<double, false>(B, xa, y, z, i - B.off, nullptr, nullptr, nullptr);
+        const Coef<double> c1 = cell_coef<double, false>(B, xa + 1, y, z, i + 1 - B.off, nullptr, nullptr, nullptr);
+        const double ap0 = coef_ap(c0), ap1 = coef_ap(c1);
+        const double r0 = b2.x - (c0.aw * wv + c0.ae * pc.y + c0.as * so.x + c0.an * no.x + c0.ab * bo.x +
+                                  c0.at * to.x + ap0 * pc.x);
+        const double r1 = b2.y - (c1.aw * pc.x + c1.ae * ev + c1.as * so.y + c1.an * no.y + c1.ab * bo.y +
+                                  c1.at * to.y + ap1 * pc.y);
+        R2 ro;
+        ro.x = (TR)(r0 - mean_b);
+        ro.y = (TR)(r1 - mean_b);
+        *reinterpret_cast<R2*>(rhs_out + i) = ro;
+        rr += r0 * r0;
+        rr += r1 * r1;
+        bb += b2.x * b2.x;
+        bb += b2.y * b2.y;
+        rm = fmax(rm, fabs(r0) * rscale);
+        rm = fmax(rm, fabs(r1) * rscale);
+        rs += r0;
+        rs += r1;
+      }
+    }
+    if (wr) store_next(P[1], G[1], z);
+#pragma unroll
+    for (int k = 0; k < GP; ++k) {
+      P[0][k] = P[1][k];
+      P[1][k] = P[2][k];
+      bz[k] = bz1[k];
+    }
+    G[0] = G[1];
+    G[1] = G[2];
+  }
+  cp_async_wait<0>();  // nothing of this CTA's copies outlives it
+  if (wr && ze == nz) store_next(P[1], G[1], nz + 1);  // ghost plane above (now the middle plane)
+  block_reduce4<32 * (kDefectRows + 2)>(rr, bb, rm, rs, partials + 4 * (size_t)blockIdx.x);
+}
+
+template <typename TE, int GP>
+static cudaError_t defect_march_attr() {
+  return cudaFuncSetAttribute(k_defect_march<TE, TE, true, GP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)DefectCfg<TE, GP>::SMEM) != cudaSuccess
+             ? cudaGetLastError()
+             : cudaFuncSetAttribute(k_defect_march<TE, TE, false, GP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)DefectCfg<TE, GP>::SMEM);
+}
+cudaError_t defect_march_attributes() {
+  cudaError_t e;
+  if ((e = defect_march_attr<float, 1>()) || (e = defect_march_attr<float, 2>()) || (e = defect_march_attr<float, 4>()) ||
+      (e = defect_march_attr<double, 1>()) || (e = defect_march_attr<double, 2>()) ||
+      (e = defect_march_attr<double, 4>()))
+    return e;
+  return cudaSuccess;
+}
+
+template <typename TE, typename TR>
+cudaError_t launch_defect_march(int gp, const BlkLev* bl, const Tile* tiles, int ntiles, int zc, const double* p,
+                                const TE* e, double* p_next, const double* b, TR* rhs_out, double mean_b,
+                                double rscale, double* partials, cudaStream_t st) {
+  if (ntiles <= 0) return cudaSuccess;
+  constexpr int NT = 32 * (kDefectRows + 2);
+#define H3D_DM(G)                                                                                                    \
+  if (gp == G) {                                                                                                     \
+    constexpr size_t SM = DefectCfg<TE, G>::SMEM;                                                                    \
+    if (e) pdl_launch(k_defect_march<TE, TR, true, G>, ntiles, NT, SM, st, bl, tiles, zc, p, e, p_next, b, rhs_out, \
+                      mean_b, rscale, partials);                                                                     \
+    else pdl_launch(k_defect_march<TE, TR, false, G>, ntiles, NT, SM, st, bl, tiles, zc, p, e, p_next, b, rhs_out,  \
+                    mean_b, rscale, partials);                                                                       \
+    return cudaGetLastError();                                                                                       \
+  }
+  H3D_DM(1)
+  H3D_DM(2)
+  H3D_DM(4)
+#undef H3D_DM
+  return cudaErrorInvalidValue;
+}
+template cudaError_t launch_defect_march<double, double>(int, const BlkLev*, const Tile*, int, int, const double*,
+                                                         const double*, double*, const double*, double*, double,
+                                                         double, double*, cudaStream_t);
+template cudaError_t launch_defect_march<float, float>(int, const BlkLev*, const Tile*, int, int, const double*,
+                                                       const float*, double*, const double*, float*, double, double,
+                                                       double*, cudaStream_t);
+int defect_march_rows() { return kDefectRows; }
 
 template <typename TE, typename TR>
 cudaError_t launch_defect_vec(const BlkLev* bl, const Tile* tiles, int ntiles, const double* p, const TE* e,

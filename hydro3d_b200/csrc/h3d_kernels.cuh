@@ -110,9 +110,10 @@ cudaError_t launch_restrict(bool var, bool zero_phi, const BlkLev* fine, const B
 template <typename T>
 cudaError_t launch_prolong(bool zero_old, const BlkLev* fine, const BlkLev* coarse, RowTab rt,
                            const T* phi_c, const T* old, T* out, cudaStream_t st);
-// Same, tiled: tiles (b, 0, y0, z) of kProlongRows fine rows (ghost rows
-// included) of plane z; needs every block's nx to be a multiple of 16/sizeof(T).
-constexpr int kProlongRows = 32;
+// Same, tiled: tiles (b, 0, 0, 2m) of fine plane pairs (2m, 2m+1), ghost
+// planes included; needs every block's nx a multiple of 16/sizeof(T) and
+// ny, nz even.
+constexpr int kProlongRows = 32;  // rows of a tile of the tiled defect
 template <typename T>
 cudaError_t launch_prolong_vec(bool zero_old, const BlkLev* fine, const BlkLev* coarse, const Tile* tiles, int ntiles,
                                const T* phi_c, const T* old, T* out, cudaStream_t st);
@@ -123,6 +124,15 @@ template <typename TE, typename TR>
 cudaError_t launch_defect_vec(const BlkLev* bl, const Tile* tiles, int ntiles, const double* p, const TE* e,
                               double* p_next, const double* b, TR* rhs_out, double mean_b, double rscale,
                               double* partials, int grid, cudaStream_t st);
+
+// The same defect as a z march (constant coefficients, nx even, nx <= 64 gp):
+// tiles of defect_march_rows() interior rows of one block over zc planes from
+// z0, one CTA and partial sum each; gp = 1, 2 or 4 pairs of cells per lane.
+template <typename TE, typename TR>
+cudaError_t launch_defect_march(int gp, const BlkLev* bl, const Tile* tiles, int ntiles, int zc, const double* p,
+                                const TE* e, double* p_next, const double* b, TR* rhs_out, double mean_b,
+                                double rscale, double* partials, cudaStream_t st);
+int defect_march_rows();
 
 // Level-1 FP64 defect: pn = p + e (all cells, when e != null), r = b - A pn on
 // the interior, rhs_out = r - mean_b (as TR), per-CTA partial sums

@@ -67,9 +67,13 @@ struct Level {
   CUtensorMap* d_rmaps = nullptr;  // as the fine level of a restriction: [tyc index][0,1: iterate, 2: rhs][block]
   Tile* d_rtiles = nullptr;       // restriction tiles (this level as the coarse level)
   int rtiles_cap = 0;
-  Tile* d_ptiles = nullptr;       // prolongation / defect tiles (kProlongRows rows of one plane, ghosts included)
+  Tile* d_ptiles = nullptr;       // level 1: tiled-defect tiles (kProlongRows rows of one plane, ghosts included)
   int nptiles = 0;
-  bool pvec32 = false, pvec64 = false;  // every block's nx a multiple of 4 (FP32) / 2 (FP64) cells
+  Tile* d_qtiles = nullptr;       // prolongation tiles (plane pairs 2m, 2m+1 of a block, ghost planes included)
+  int nqtiles = 0;
+  Tile* d_dtiles = nullptr;       // level 1: z-march defect tiles (defect_march_rows() rows x dzc planes)
+  int ndtiles = 0, dzc = 1, dgp = 0;  // dgp: pairs per lane of the z-march defect (0: not usable)
+  bool pvec32 = false, pvec64 = false;  // every block's nx a multiple of 4 (FP32) / 2 (FP64) cells, ny and nz even
   int nrtiles = 0, rvariant = 0, rzc = 1;
   bool tma_ok = false;
   bool f32 = false, var = false;  // iterate precision of the level's smoother; variable coefficients
@@ -489,7 +493,7 @@ struct Exec {
         pc = C.phi32[C.cur32];
       }
       if (F.pvec32)
-        CU(launch_prolong_vec<float>(F.zero32, F.d_bl, C.d_bl, F.d_ptiles, F.nptiles, pc, F.phi32[F.cur32],
+        CU(launch_prolong_vec<float>(F.zero32, F.d_bl, C.d_bl, F.d_qtiles, F.nqtiles, pc, F.phi32[F.cur32],
                                      F.phi32[1 - F.cur32], h->st));
       else
         CU(launch_prolong<float>(F.zero32, F.d_bl, C.d_bl, ct, pc, F.phi32[F.cur32], F.phi32[1 - F.cur32], h->st));
@@ -499,7 +503,7 @@ struct Exec {
     } else {
       if (C.zero64) TRY(materialize_zero64(gf + 1));
       if (F.pvec64)
-        CU(launch_prolong_vec<double>(F.zero64, F.d_bl, C.d_bl, F.d_ptiles, F.nptiles, C.phi64[C.cur64],
+        CU(launch_prolong_vec<double>(F.zero64, F.d_bl, C.d_bl, F.d_qtiles, F.nqtiles, C.phi64[C.cur64],
                                       F.phi64[F.cur64], F.phi64[1 - F.cur64], h->st));
       else
         CU(launch_prolong<double>(F.zero64, F.d_bl, C.d_bl, ct, C.phi64[C.cur64], F.phi64[F.cur64],
@@ -576,16 +580,20 @@ struct Exec {
     const double* fz = h->var ? V.fz64 : nullptr;
     double* pin = h->p64[h->pc];
     double* pout = h->p64[1 - h->pc];
-    // the tiled kernel needs the level's 8-row tiles and constant coefficients
-    const bool tiled = V.d_ptiles && V.pvec64 && !h->var;
-    const int ngrid = tiled ? V.nptiles : defect_grid(ct.nrows);
+    // the z-march and tiled kernels need constant coefficients and nx even
+    const bool march = V.dgp > 0 && !h->var;
+    const bool tiled = !march && V.d_ptiles && V.pvec64 && !h->var;
+    const int ngrid = march ? V.ndtiles : tiled ? V.nptiles : defect_grid(ct.nrows);
     if (h->mixed) {
       const float* e = nullptr;
       if (with_e) {
         if (V.zero32) TRY(materialize_zero32(1));
         e = V.phi32[V.cur32];
       }
-      if (tiled)
+      if (march)
+        CU(launch_defect_march<float, float>(V.dgp, V.d_bl, V.d_dtiles, V.ndtiles, V.dzc, pin, e, pout, h->b64,
+                                             V.rhs32, h->mean_b, rscale, h->partials, h->st));
+      else if (tiled)
         CU(launch_defect_vec<float, float>(V.d_bl, V.d_ptiles, V.nptiles, pin, e, pout, h->b64, V.rhs32, h->mean_b,
                                            rscale, h->partials, ngrid, h->st));
       else
@@ -597,7 +605,10 @@ struct Exec {
         if (V.zero64) TRY(materialize_zero64(1));
         e = V.phi64[V.cur64];
       }
-      if (tiled)
+      if (march)
+        CU(launch_defect_march<double, double>(V.dgp, V.d_bl, V.d_dtiles, V.ndtiles, V.dzc, pin, e, pout, h->b64,
+                                               V.rhs64, h->mean_b, rscale, h->partials, h->st));
+      else if (tiled)
         CU(launch_defect_vec<double, double>(V.d_bl, V.d_ptiles, V.nptiles, pin, e, pout, h->b64, V.rhs64,
                                              h->mean_b, rscale, h->partials, ngrid, h->st));
       else
@@ -1140,7 +1151,7 @@ int h3d_mg_destroy(h3d_mg* h) {
     void* ps[] = {V.d_bl, V.d_cta_all, V.d_cta_int, V.d_rows_all, V.d_rows_int, V.d_tiles, V.phi64[0], V.phi64[1], V.rhs64, V.phi32[0],
                   V.phi32[1], V.rhs32, V.fx64, V.fy64, V.fz64, V.fx32, V.fy32, V.fz32, V.dens,
                   V.sweep.d_dst, V.sweep.d_src, V.faces.d_dst, V.faces.d_src, V.exch.d_dst, V.exch.d_src,
-                  V.bound.d_dst, V.bound.d_src, V.d_maps, V.d_rmaps, V.d_rtiles, V.d_ptiles, V.d_cstart};
+                  V.bound.d_dst, V.bound.d_src, V.d_maps, V.d_rmaps, V.d_rtiles, V.d_ptiles, V.d_qtiles, V.d_dtiles, V.d_cstart};
     for (void* p : ps) dfree(p);
   }
   dfree(h->p64[0]);
@@ -1272,20 +1283,57 @@ int h3d_mg_create(h3d_mg** out, const h3d_mg_desc* desc) {
     }
     V.f32 = f32_level(h, g);
     V.var = h->var;
-    if (g < h->L) {  // prolongation tiles: kProlongRows fine rows of one plane, ghost rows and planes included
-      std::vector<Tile> pt;
+    if (g < h->L) {
+      // prolongation tiles: plane pairs (2m, 2m+1) of a block, ghost planes included;
+      // level 1 also: row tiles of the tiled defect (kProlongRows rows of one plane)
+      std::vector<Tile> qt, pt;
       V.pvec32 = V.pvec64 = true;
       for (size_t b = 0; b < V.geom.bl.size(); ++b) {
         const BlkLev& B = V.geom.bl[b];
-        V.pvec32 = V.pvec32 && B.nx % 4 == 0;
-        V.pvec64 = V.pvec64 && B.nx % 2 == 0;
-        for (int z = 0; z <= B.nz + 1; ++z)
-          for (int y0 = 0; y0 <= B.ny + 1; y0 += kProlongRows) pt.push_back(Tile{(int)b, 0, y0, z});
+        const bool even = B.ny % 2 == 0 && B.nz % 2 == 0;
+        V.pvec32 = V.pvec32 && even && B.nx % 4 == 0;
+        V.pvec64 = V.pvec64 && even && B.nx % 2 == 0;
+        for (int z = 0; z <= B.nz; z += 2) qt.push_back(Tile{(int)b, 0, 0, z});
+        if (g == 1)
+          for (int z = 0; z <= B.nz + 1; ++z)
+            for (int y0 = 0; y0 <= B.ny + 1; y0 += kProlongRows) pt.push_back(Tile{(int)b, 0, y0, z});
       }
-      if ((rc = dalloc(h, &V.d_ptiles, pt.size())) != H3D_OK) return bail(rc);
-      if (cudaMemcpy(V.d_ptiles, pt.data(), pt.size() * sizeof(Tile), cudaMemcpyHostToDevice) != cudaSuccess)
+      if ((rc = dalloc(h, &V.d_qtiles, qt.size())) != H3D_OK) return bail(rc);
+      if (cudaMemcpy(V.d_qtiles, qt.data(), qt.size() * sizeof(Tile), cudaMemcpyHostToDevice) != cudaSuccess)
         return bail(fail(h, H3D_ERR_CUDA, "prolongation tiles"));
-      V.nptiles = (int)pt.size();
+      V.nqtiles = (int)qt.size();
+      if (!pt.empty()) {
+        if ((rc = dalloc(h, &V.d_ptiles, pt.size())) != H3D_OK) return bail(rc);
+        if (cudaMemcpy(V.d_ptiles, pt.data(), pt.size() * sizeof(Tile), cudaMemcpyHostToDevice) != cudaSuccess)
+          return bail(fail(h, H3D_ERR_CUDA, "defect tiles"));
+        V.nptiles = (int)pt.size();
+      }
+    }
+    if (g == 1 && !h->var) {  // z-march defect tiles: 8 rows of a block over a chunk of planes
+      int maxnx = 0, maxnz = 0, nyt = 0;
+      bool even = true;
+      for (const auto& B : V.geom.bl) {
+        maxnx = std::max(maxnx, B.nx);
+        maxnz = std::max(maxnz, B.nz);
+        even = even && B.nx % 2 == 0;
+        nyt += (B.ny + defect_march_rows() - 1) / defect_march_rows();
+      }
+      V.dgp = !even ? 0 : maxnx <= 64 ? 1 : maxnx <= 128 ? 2 : maxnx <= 256 ? 4 : 0;
+      if (V.dgp) {
+        // about six CTAs per SM in all, chunks of at least four planes
+        const int chunks = std::max(1, std::min((148 * 6 + nyt - 1) / nyt, maxnz / 4));
+        V.dzc = std::max(1, (maxnz + chunks - 1) / chunks);
+        std::vector<Tile> dt;
+        for (size_t b = 0; b < V.geom.bl.size(); ++b) {
+          const BlkLev& B = V.geom.bl[b];
+          for (int z0 = 1; z0 <= B.nz; z0 += V.dzc)
+            for (int y0 = 1; y0 <= B.ny; y0 += defect_march_rows()) dt.push_back(Tile{(int)b, 0, y0, z0});
+        }
+        if ((rc = dalloc(h, &V.d_dtiles, dt.size())) != H3D_OK) return bail(rc);
+        if (cudaMemcpy(V.d_dtiles, dt.data(), dt.size() * sizeof(Tile), cudaMemcpyHostToDevice) != cudaSuccess)
+          return bail(fail(h, H3D_ERR_CUDA, "defect tiles"));
+        V.ndtiles = (int)dt.size();
+      }
     }
     if ((rc = build_tensor_maps(h, g)) != H3D_OK) return bail(rc);
     if (g >= 2 && (rc = build_restrict_tiles(h, V)) != H3D_OK) return bail(rc);
@@ -1300,7 +1348,8 @@ int h3d_mg_create(h3d_mg** out, const h3d_mg_desc* desc) {
   const size_t n1 = (size_t)h->lev[1].geom.n_elems;
   if ((rc = dalloc(h, &h->p64[0], n1)) || (rc = dalloc(h, &h->p64[1], n1)) || (rc = dalloc(h, &h->b64, n1)))
     return bail(rc);
-  h->npartials = std::max(std::max(std::max(h->lev[1].ncta_all, h->lev[1].ncta_int), kDefectCtas), h->lev[1].nptiles);
+  h->npartials = std::max(std::max(std::max(h->lev[1].ncta_all, h->lev[1].ncta_int), kDefectCtas),
+                          std::max(h->lev[1].nptiles, h->lev[1].ndtiles));
   if ((rc = dalloc(h, &h->partials, 4 * (size_t)h->npartials)) || (rc = dalloc(h, &h->d_res, 4))) return bail(rc);
   if (cudaMallocHost((void**)&h->h_res, 4 * sizeof(double)) != cudaSuccess)
     return bail(fail(h, H3D_ERR_OOM, "pinned result buffer"));

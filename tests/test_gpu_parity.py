@@ -188,6 +188,30 @@ def test_newsolv_matches_oracle(oracle_mod, h3d, layout):
     s.close()
 
 
+def test_newsolv_wide_ragged_rows(oracle_mod, h3d):
+    """Twelve outer iterations of newsolv_mg on blocks of 96 x 12 x 8 cells
+    (rows of 48 cell pairs, row tiles of the defect that end inside a block,
+    several plane chunks per block) against the oracle: residual history
+    within 1e-9, iterate within 1e-10 (the two sum the norms in different
+    orders).  The elongated blocks converge slowly, so no convergence is
+    asked for."""
+    blocks = h3d.topology.block_grid((1, 2, 1), (96, 12, 8), [W, W, P, P, W, W], [1.0 / 32] * 3, 3, pl=2)
+    b, p = _host_problem(h3d, blocks, 16, 2)
+    s = h3d.MultigridSolver(blocks, 3)
+    info = s.newsolv_mg(p, b, tol=1e-30, maxcy=12, history=True)
+    orc = oracle_mod.Oracle(to_oracle_descs(oracle_mod, blocks), 3)
+    orc.coeff()
+    from tests.helpers import interior_of_host
+    ref = orc.solve([np.zeros((d.n[2] + 2, d.n[1] + 2, d.n[0] + 2)) for d in blocks],
+                    [interior_of_host(x, d) for x, d in zip(b, blocks)], tol=1e-30, maxcy=12)
+    assert info["cycles"] == ref["cycles"] == 12
+    np.testing.assert_allclose(info["history"], ref["history"], rtol=1e-9, atol=0)
+    got = [interior_of_host(x, d) for x, d in zip(p, blocks)]
+    want = [x[1:-1, 1:-1, 1:-1] for x in ref["p"]]
+    assert mean_removed_rel(got, want) <= 1e-10
+    s.close()
+
+
 def test_mgkcyc_host_fields(oracle_mod, h3d):
     blocks = h3d.topology.block_grid((2, 1, 1), (16, 16, 16), [W] * 6, [1.0 / 32] * 3, 3, pl=3)
     b, _ = _host_problem(h3d, blocks, 12, 3)
