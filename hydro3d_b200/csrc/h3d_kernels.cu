@@ -1293,6 +1293,9 @@ static const TileShape kShapes[] = {
     // register-window sweeps with two groups per lane
     {128, 16, 288, true, 16, 2, 3, 29}, {128, 8, 160, true, 16, 2, 3, 9},           // 48, 49
     {64, 16, 144, true, 8, 2, 3, 11},                                               // 50
+    // register-window sweeps with the z march unrolled over the window
+    {128, 8, 320, true, 32, 1, 3, 9},   {128, 16, 576, true, 32, 1, 3, 29},         // 51, 52
+    {128, 8, 320, true, 32, 1, 3, 9},                                               // 53
 };
 #ifdef H3D_BOUNDS_CHECK
 // Debug builds only: first recorded out-of-bounds access {kernel id + 1, block, index, limit}.
@@ -1437,7 +1440,7 @@ __device__ __forceinline__ void win_colour(float4& c, const float4& bz, const fl
 // right-hand side is staged, red cells are rhs times the diagonal reciprocal,
 // and black cells read the red values of neighbours in the block (zero
 // outside it).  GPT = 2 halves the per-plane overhead per cell.
-template <int TPR, int GPT, int TY, int NS, int D, bool ZERO>
+template <int TPR, int GPT, int TY, int NS, int D, bool ZERO, int U>
 __global__ void __launch_bounds__(TPR*(TY + 2)) k_rbgs_win(const BlkLev* __restrict__ bls,
                                                           const Tile* __restrict__ tiles, int zc,
                                                           const CUtensorMap* __restrict__ maps,
@@ -1604,6 +1607,7 @@ __global__ void __launch_bounds__(TPR*(TY + 2)) k_rbgs_win(const BlkLev* __restr
     c0[k] = ZERO ? zero4 : ld4(pslot(s0) + pc[k]);
   }
   long long dz = (long long)(zlo - 2) * sxy;  // offset of plane z-2 in the block
+#pragma unroll U
   for (int z = zlo; z <= ze + 2; ++z, dz += sxy) {
     const int zb = z - 2;
     const bool red = z <= zhi && yrow;                                // red cells of plane z
@@ -1692,17 +1696,17 @@ static cudaError_t vec_dispatch(const BlkLev* bl, const Tile* tiles, int ntiles,
   return cudaGetLastError();
 }
 
-template <int TPR, int GPT, int TY, int NS, int D>
+template <int TPR, int GPT, int TY, int NS, int D, int U>
 static cudaError_t win_attr() {
-  cudaError_t e = cudaFuncSetAttribute(k_rbgs_win<TPR, GPT, TY, NS, D, false>,
+  cudaError_t e = cudaFuncSetAttribute(k_rbgs_win<TPR, GPT, TY, NS, D, false, U>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)VecCfg<TPR, GPT, TY, NS, D>::SMEM);
   if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(k_rbgs_win<TPR, GPT, TY, NS, D, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  return cudaFuncSetAttribute(k_rbgs_win<TPR, GPT, TY, NS, D, true, U>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               (int)VecCfg<TPR, GPT, TY, NS, D>::SMEM);
 }
 
-template <int TPR, int GPT, int TY, int NS, int D>
+template <int TPR, int GPT, int TY, int NS, int D, int U>
 static cudaError_t win_dispatch(bool zero, const BlkLev* bl, const Tile* tiles, int ntiles, int zc,
                                 const CUtensorMap* maps, const CUtensorMap* rmaps, int* err, float* dst,
                                 cudaStream_t st) {
@@ -1710,28 +1714,32 @@ static cudaError_t win_dispatch(bool zero, const BlkLev* bl, const Tile* tiles, 
   if (ntiles <= 0) return cudaSuccess;
   constexpr size_t SM = VecCfg<TPR, GPT, TY, NS, D>::SMEM;
   if (zero)
-    pdl_launch(k_rbgs_win<TPR, GPT, TY, NS, D, true>, ntiles, TPR * (TY + 2), SM, st, bl, tiles, zc, maps, rmaps, dst,
-               err);
+    pdl_launch(k_rbgs_win<TPR, GPT, TY, NS, D, true, U>, ntiles, TPR * (TY + 2), SM, st, bl, tiles, zc, maps, rmaps,
+               dst, err);
   else
-    pdl_launch(k_rbgs_win<TPR, GPT, TY, NS, D, false>, ntiles, TPR * (TY + 2), SM, st, bl, tiles, zc, maps, rmaps,
+    pdl_launch(k_rbgs_win<TPR, GPT, TY, NS, D, false, U>, ntiles, TPR * (TY + 2), SM, st, bl, tiles, zc, maps, rmaps,
                dst, err);
   return cudaGetLastError();
 }
 
 constexpr int kFirstWinShape = 40;
-// (variant, lanes per row, groups of four cells per lane, rows, ring slots, prefetch depth)
+// (variant, lanes per row, groups of four cells per lane, rows, ring slots, prefetch depth,
+//  z-march unrolling: 5 = the length of the register window, so that it rotates without moves)
 #define H3D_WIN_SHAPES(X)     \
-  X(40, 32, 1, 4, 8, 5)       \
-  X(41, 32, 1, 8, 8, 4)       \
-  X(42, 32, 1, 16, 8, 4)      \
-  X(43, 32, 1, 8, 8, 5)       \
-  X(44, 16, 1, 8, 8, 5)       \
-  X(45, 16, 1, 16, 8, 4)      \
-  X(46, 8, 1, 16, 8, 5)       \
-  X(47, 4, 1, 16, 8, 5)       \
-  X(48, 16, 2, 16, 8, 4)      \
-  X(49, 16, 2, 8, 8, 4)       \
-  X(50, 8, 2, 16, 8, 4)
+  X(40, 32, 1, 4, 8, 5, 1)    \
+  X(41, 32, 1, 8, 8, 4, 1)    \
+  X(42, 32, 1, 16, 8, 4, 1)   \
+  X(43, 32, 1, 8, 8, 5, 1)    \
+  X(44, 16, 1, 8, 8, 5, 1)    \
+  X(45, 16, 1, 16, 8, 4, 1)   \
+  X(46, 8, 1, 16, 8, 5, 1)    \
+  X(47, 4, 1, 16, 8, 5, 1)    \
+  X(48, 16, 2, 16, 8, 4, 1)   \
+  X(49, 16, 2, 8, 8, 4, 1)    \
+  X(50, 8, 2, 16, 8, 4, 1)    \
+  X(51, 32, 1, 8, 8, 4, 5)    \
+  X(52, 32, 1, 16, 8, 4, 5)   \
+  X(53, 32, 1, 8, 8, 5, 5)
 
 // (variant, threads per row, groups of four cells per thread, rows, ring slots, prefetch depth)
 #define H3D_VEC_SHAPES(X)  \
@@ -1778,8 +1786,8 @@ cudaError_t init_kernel_attributes() {
   if ((e = vec_attr<tpr, gpt, ty, ns, d>()) != cudaSuccess) return e;
   H3D_VEC_SHAPES(X)
 #undef X
-#define X(v, tpr, gpt, ty, ns, d) \
-  if ((e = win_attr<tpr, gpt, ty, ns, d>()) != cudaSuccess) return e;
+#define X(v, tpr, gpt, ty, ns, d, u) \
+  if ((e = win_attr<tpr, gpt, ty, ns, d, u>()) != cudaSuccess) return e;
   H3D_WIN_SHAPES(X)
 #undef X
   return defect_march_attributes();
@@ -1806,8 +1814,8 @@ cudaError_t launch_rbgs(int variant, bool var, bool zero_src, const BlkLev* bl, 
       case v: return vec_dispatch<tpr, gpt, ty, ns, d>(bl, tiles, ntiles, zc, maps, rmaps, err, reinterpret_cast<float*>(dst), st);
       H3D_VEC_SHAPES(X)
 #undef X
-#define X(v, tpr, gpt, ty, ns, d) \
-      case v: return win_dispatch<tpr, gpt, ty, ns, d>(zero_src, bl, tiles, ntiles, zc, maps, rmaps, err, reinterpret_cast<float*>(dst), st);
+#define X(v, tpr, gpt, ty, ns, d, u) \
+      case v: return win_dispatch<tpr, gpt, ty, ns, d, u>(zero_src, bl, tiles, ntiles, zc, maps, rmaps, err, reinterpret_cast<float*>(dst), st);
       H3D_WIN_SHAPES(X)
 #undef X
       default: break;
