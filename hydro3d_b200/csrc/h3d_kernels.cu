@@ -20,19 +20,29 @@ namespace {
 // kernel lets the next one on the stream start launching at once
 // (griddepcontrol.launch_dependents) and waits for its predecessors to
 // complete (griddepcontrol.wait) before it touches data they write.  Both are
-// no-ops for a kernel launched without the attribute.  Off by default: on the
-// 33.5M-cell solve it measured 60.1 ms against 56.1 ms without (the early
-// launched grids hold SM resources the running ones need).
+// no-ops for a kernel launched without the attribute.  For every launch it
+// measured 60.1 ms against 56.1 ms without on the 33.5M-cell solve (the
+// early launched grids hold SM resources the running ones need).
 __device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory"); }
 __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
 
-static bool pdl_enabled() {
-  static const bool on = [] {
+// Launch policy (H3D_PDL): "1" every kernel, "0" none; by default only a
+// kernel of at most kPdlGrid CTAs that follows one of at most kPdlGrid CTAs
+// on the same host thread.  Such a predecessor runs in a single wave, so the
+// early-launched grid only takes SM slots that the predecessor leaves idle,
+// while the launch latency of the chains of small kernels of the coarse
+// levels is hidden.
+constexpr long long kPdlGrid = 2 * 148;
+static int pdl_mode() {
+  static const int m = [] {
     const char* v = std::getenv("H3D_PDL");
-    return v && v[0] == '1';
+    if (v && v[0] == '1') return 1;
+    if (v && v[0] == '0') return 0;
+    return 2;
   }();
-  return on;
+  return m;
 }
+static thread_local long long g_prev_grid = 1LL << 40;
 
 template <typename... KArgs, typename... Args>
 static cudaError_t pdl_launch(void (*k)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
@@ -46,7 +56,10 @@ static cudaError_t pdl_launch(void (*k)(KArgs...), dim3 grid, dim3 block, size_t
   at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
   at[0].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = at;
-  cfg.numAttrs = pdl_enabled() ? 1 : 0;
+  const long long n = (long long)grid.x * grid.y * grid.z;
+  const int mode = pdl_mode();
+  cfg.numAttrs = (mode == 1 || (mode == 2 && n <= kPdlGrid && g_prev_grid <= kPdlGrid)) ? 1 : 0;
+  g_prev_grid = n;
   return cudaLaunchKernelEx(&cfg, k, static_cast<KArgs>(args)...);
 }
 
@@ -780,13 +793,25 @@ template <typename T, bool ZERO_OLD>
 __global__ void k_fill(const uint32_t* __restrict__ dsts, const uint32_t* __restrict__ srcs, int64_t n,
                        T* __restrict__ out, const T* __restrict__ cur, const T* __restrict__ old) {
   pdl_trigger();
+  // the gather tables are written once at setup: fetch the first entry
+  // while the predecessor finishes
+  int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  uint32_t s = 0, d = 0;
+  if (e < n) {
+    s = __ldg(srcs + e);
+    d = __ldg(dsts + e);
+  }
   pdl_wait();
-  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
-    uint32_t s = __ldg(srcs + e);
+  for (; e < n; e += (int64_t)gridDim.x * blockDim.x) {
     T v;
     if (s & kOldFlag) v = ZERO_OLD ? T(0) : old[s & kIdxMask];
     else v = cur[s];
-    out[__ldg(dsts + e)] = v;
+    out[d] = v;
+    const int64_t en = e + (int64_t)gridDim.x * blockDim.x;
+    if (en < n) {
+      s = __ldg(srcs + en);
+      d = __ldg(dsts + en);
+    }
   }
 }
 
@@ -1295,7 +1320,9 @@ static const TileShape kShapes[] = {
     {64, 16, 144, true, 8, 2, 3, 11},                                               // 50
     // register-window sweeps with the z march unrolled over the window
     {128, 8, 320, true, 32, 1, 3, 9},   {128, 16, 576, true, 32, 1, 3, 29},         // 51, 52
-    {128, 8, 320, true, 32, 1, 3, 9},                                               // 53
+    {128, 8, 320, true, 32, 1, 3, 9},   {64, 8, 160, true, 16, 1, 3, 10},           // 53, 54
+    {64, 16, 288, true, 16, 1, 3, 11},  {32, 16, 144, true, 8, 1, 3, 12},           // 55, 56
+    {128, 8, 160, true, 16, 2, 3, 9},   {128, 4, 192, true, 32, 1, 3, 17},          // 57, 58
 };
 #ifdef H3D_BOUNDS_CHECK
 // Debug builds only: first recorded out-of-bounds access {kernel id + 1, block, index, limit}.
@@ -1447,7 +1474,6 @@ __global__ void __launch_bounds__(TPR*(TY + 2)) k_rbgs_win(const BlkLev* __restr
                                                           const CUtensorMap* __restrict__ rmaps,
                                                           float* __restrict__ dst, int* err) {
   pdl_trigger();
-  pdl_wait();
   using C = VecCfg<TPR, GPT, TY, NS, D>;
   static_assert(TPR <= 32 && (TPR & (TPR - 1)) == 0, "a row is a power-of-two lane segment of one warp");
   static_assert(GPT == 1 || GPT == 2, "one or two groups per lane");
@@ -1525,6 +1551,7 @@ __global__ void __launch_bounds__(TPR*(TY + 2)) k_rbgs_win(const BlkLev* __restr
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
   __syncthreads();
+  pdl_wait();  // everything above reads only setup data
 
   auto pslot = [&](int s) -> float* { return reinterpret_cast<float*>(base + s * C::SLOT); };
   auto rslot = [&](int s) -> const float* { return reinterpret_cast<const float*>(base + s * C::SLOT + C::PSLOT); };
@@ -1739,7 +1766,12 @@ constexpr int kFirstWinShape = 40;
   X(50, 8, 2, 16, 8, 4, 1)    \
   X(51, 32, 1, 8, 8, 4, 5)    \
   X(52, 32, 1, 16, 8, 4, 5)   \
-  X(53, 32, 1, 8, 8, 5, 5)
+  X(53, 32, 1, 8, 8, 5, 5)    \
+  X(54, 16, 1, 8, 8, 5, 5)    \
+  X(55, 16, 1, 16, 8, 4, 5)   \
+  X(56, 8, 1, 16, 8, 5, 5)    \
+  X(57, 16, 2, 8, 8, 4, 5)    \
+  X(58, 32, 1, 4, 8, 5, 5)
 
 // (variant, threads per row, groups of four cells per thread, rows, ring slots, prefetch depth)
 #define H3D_VEC_SHAPES(X)  \
@@ -1769,6 +1801,7 @@ constexpr int kFirstWinShape = 40;
   X(29, 32, 2, 16)
 
 cudaError_t defect_march_attributes();
+cudaError_t coarse_tail_attributes();
 
 cudaError_t init_kernel_attributes() {
   cudaError_t e = cudaSuccess;
@@ -1790,7 +1823,9 @@ cudaError_t init_kernel_attributes() {
   if ((e = win_attr<tpr, gpt, ty, ns, d, u>()) != cudaSuccess) return e;
   H3D_WIN_SHAPES(X)
 #undef X
-  return defect_march_attributes();
+  cudaError_t e2 = defect_march_attributes();
+  if (e2 != cudaSuccess) return e2;
+  return coarse_tail_attributes();
 }
 
 
@@ -1851,18 +1886,12 @@ cudaError_t launch_rbgs(int variant, bool var, bool zero_src, const BlkLev* bl, 
 // FP64 update keeps the reference's operand order and IEEE division.
 // zero: the iterate is known zero; it is cleared (ghosts included) first.
 // start[b]: first flat interior index of block b (start[nb] = all cells).
+// sb / ss: the block table and those starts, in shared memory.
 template <typename T, bool VAR>
-__global__ void __launch_bounds__(1024) k_relax_small(const BlkLev* __restrict__ bls, const int* __restrict__ start,
-                                                      int nb, T* __restrict__ phi, const T* __restrict__ rhs,
-                                                      const T* __restrict__ fx, const T* __restrict__ fy,
-                                                      const T* __restrict__ fz, const uint32_t* __restrict__ fdst,
-                                                      const uint32_t* __restrict__ fsrc, int nfill, int sweeps,
-                                                      int zero, long long nelems) {
-  __shared__ BlkLev sb[kSmallLevelBlocks];
-  __shared__ int ss[kSmallLevelBlocks + 1];
-  for (int b = threadIdx.x; b < nb; b += blockDim.x) sb[b] = bls[b];
-  for (int b = threadIdx.x; b <= nb; b += blockDim.x) ss[b] = start[b];
-  __syncthreads();
+__device__ void small_relax(const BlkLev* sb, const int* ss, int nb, T* __restrict__ phi, const T* __restrict__ rhs,
+                            const T* __restrict__ fx, const T* __restrict__ fy, const T* __restrict__ fz,
+                            const uint32_t* __restrict__ fdst, const uint32_t* __restrict__ fsrc, int nfill,
+                            int sweeps, int zero, long long nelems) {
   const int ncell = ss[nb];
   if (zero) {
     for (long long q = threadIdx.x; q < nelems; q += blockDim.x) phi[q] = T(0);
@@ -1891,6 +1920,300 @@ __global__ void __launch_bounds__(1024) k_relax_small(const BlkLev* __restrict__
     for (int q = threadIdx.x; q < nfill; q += blockDim.x) phi[fdst[q]] = phi[fsrc[q] & kIdxMask];
     __syncthreads();
   }
+}
+
+template <typename T, bool VAR>
+__global__ void __launch_bounds__(1024) k_relax_small(const BlkLev* __restrict__ bls, const int* __restrict__ start,
+                                                      int nb, T* __restrict__ phi, const T* __restrict__ rhs,
+                                                      const T* __restrict__ fx, const T* __restrict__ fy,
+                                                      const T* __restrict__ fz, const uint32_t* __restrict__ fdst,
+                                                      const uint32_t* __restrict__ fsrc, int nfill, int sweeps,
+                                                      int zero, long long nelems) {
+  pdl_trigger();
+  __shared__ BlkLev sb[kSmallLevelBlocks];
+  __shared__ int ss[kSmallLevelBlocks + 1];
+  // the block table and cell starts are written once at setup: read them
+  // while the predecessor finishes
+  for (int b = threadIdx.x; b < nb; b += blockDim.x) sb[b] = bls[b];
+  for (int b = threadIdx.x; b <= nb; b += blockDim.x) ss[b] = start[b];
+  pdl_wait();
+  __syncthreads();
+  small_relax<T, VAR>(sb, ss, nb, phi, rhs, fx, fy, fz, fdst, fsrc, nfill, sweeps, zero, nelems);
+}
+
+// The fused coarse tail keeps every tail level in shared memory, in a
+// compact layout: the iterate as the padded blocks back to back (block b at
+// cbl[b].off, pitches nx+2 and (nx+2)(ny+2)), the rhs as the interior cells
+// in natural order (block b from cbl[b].pad).  Cells come from per-level
+// tables built at setup, one 64-bit entry a cell: compact index (bits 0-23),
+// x, y, z (bits 24-31, 32-39, 40-47) and block (bits 48-53); interior
+// tables list the red cells (x+y+z odd) first.
+struct CellRef {
+  int i, x, y, z, b;
+};
+__device__ __forceinline__ CellRef cell_ref(unsigned long long e) {
+  CellRef c;
+  c.i = (int)(e & 0xffffffull);
+  c.x = (int)((e >> 24) & 0xff);
+  c.y = (int)((e >> 32) & 0xff);
+  c.z = (int)((e >> 40) & 0xff);
+  c.b = (int)((e >> 48) & 0x3f);
+  return c;
+}
+__device__ __forceinline__ int rhs_index(const BlkLev& B, int x, int y, int z) {
+  return B.pad + ((z - 1) * B.ny + (y - 1)) * B.nx + (x - 1);
+}
+__device__ __forceinline__ long long global_index(const BlkLev& G, int x, int y, int z) {
+  return G.off + (long long)z * G.sxy + (long long)y * G.sx + x;
+}
+
+// `sweeps` in-place red-black sweeps of a tail level, each followed by its
+// ghost fill; same cell arithmetic as small_relax.
+template <typename T>
+__device__ void tail_relax(const BlkLev* cb, const TailLevel& L, T* phi, const T* rhs, int sweeps) {
+  for (int it = 0; it < sweeps; ++it) {
+    for (int colour = 0; colour < 2; ++colour) {  // red (x+y+z odd) first
+      const int k0 = colour ? L.nred : 0, k1 = colour ? L.nint : L.nred;
+      for (int k = k0 + threadIdx.x; k < k1; k += blockDim.x) {
+        const CellRef c = cell_ref(__ldg(L.cells + k));
+        const BlkLev& B = cb[c.b];
+        const int i = c.i;
+        const Coef<T> cf = cell_coef<T, false>(B, c.x, c.y, c.z, i - B.off, nullptr, nullptr, nullptr);
+        const T ap = coef_ap(cf);
+        const T v = gs_div(rhs[rhs_index(B, c.x, c.y, c.z)] -
+                               (cf.aw * phi[i - 1] + cf.ae * phi[i + 1] + cf.as * phi[i - B.sx] +
+                                cf.an * phi[i + B.sx] + cf.ab * phi[i - B.sxy] + cf.at * phi[i + B.sxy]),
+                           ap);
+        phi[i] = v;
+      }
+      __syncthreads();
+    }
+    for (int q = threadIdx.x; q < L.nfill; q += blockDim.x) phi[__ldg(L.fdst + q)] = phi[__ldg(L.fsrc + q)];
+    __syncthreads();
+  }
+}
+
+// mgrestr into a tail level: the same residual sum over the eight children,
+// in the same order, as k_restrict; one thread a coarse cell.
+template <typename T>
+__device__ void tail_restrict(const BlkLev* fb, const BlkLev* cb, const TailLevel& Cl, const T* phi, const T* rhs,
+                              T* rhs_c, int zero_fine) {
+  for (int k = threadIdx.x; k < Cl.nint; k += blockDim.x) {
+    const CellRef cc = cell_ref(__ldg(Cl.cells + k));
+    const BlkLev& F = fb[cc.b];
+    const int X = cc.x, Y = cc.y, Z = cc.z;
+    const T* P = phi + F.off;
+    T sum = T(0);
+#pragma unroll
+    for (int dk = 0; dk < 2; ++dk)
+#pragma unroll
+      for (int dj = 0; dj < 2; ++dj)
+#pragma unroll
+        for (int di = 0; di < 2; ++di) {
+          const int x = 2 * X - 1 + di, y = 2 * Y - 1 + dj, z = 2 * Z - 1 + dk;
+          const int i = z * (int)F.sxy + y * F.sx + x;
+          const T rv = rhs[rhs_index(F, x, y, z)];
+          T r;
+          if (zero_fine) {
+            r = rv - T(0);
+          } else {
+            Coef<T> cf = cell_coef<T, false>(F, x, y, z, i, nullptr, nullptr, nullptr);
+            const T ap = coef_ap(cf);
+            r = rv - (cf.aw * P[i - 1] + cf.ae * P[i + 1] + cf.as * P[i - F.sx] + cf.an * P[i + F.sx] +
+                      cf.ab * P[i - F.sxy] + cf.at * P[i + F.sxy] + ap * P[i]);
+          }
+          sum = (di | dj | dk) ? sum + r : r;
+        }
+    rhs_c[rhs_index(cb[cc.b], X, Y, Z)] = T(0.125) * sum;
+  }
+  __syncthreads();
+}
+
+// mgcorr + mgbound of cell (x, y, z) (ghosts included) of block F: the value
+// k_prolong writes there, reading the old iterate from `old`.
+template <typename T>
+__device__ __forceinline__ T tail_prolong_value(const BlkLev& F, const BlkLev& C, const T* phi_c, const T* old, int x,
+                                                int y, int z, int zero_old) {
+  const int ph = F.phys;
+  int sx = x, sy = y, sz = z;
+  if (x == 0 && (ph & 1)) sx = 1;
+  if (x == F.nx + 1 && (ph & 2)) sx = F.nx;
+  if (y == 0 && (ph & 4)) sy = 1;
+  if (y == F.ny + 1 && (ph & 8)) sy = F.ny;
+  if (z == 0 && (ph & 16)) sz = 1;
+  if (z == F.nz + 1 && (ph & 32)) sz = F.nz;
+  const T wx0 = (sx & 1) ? T(1) : T(3), wx1 = (sx & 1) ? T(3) : T(1);
+  const T wy0 = (sy & 1) ? T(1) : T(3), wy1 = (sy & 1) ? T(3) : T(1);
+  const T wz0 = (sz & 1) ? T(1) : T(3), wz1 = (sz & 1) ? T(3) : T(1);
+  const int cy = C.sx, cz = (int)C.sxy;
+  const T* Q = phi_c + C.off + (sz >> 1) * cz + (sy >> 1) * cy + (sx >> 1);
+  // term order (di,dj,dk): 000, 010, 001, 011, 100, 110, 101, 111
+  T s = (wx0 * wy0 * wz0) * Q[0];
+  s = s + (wx0 * wy1 * wz0) * Q[cy];
+  s = s + (wx0 * wy0 * wz1) * Q[cz];
+  s = s + (wx0 * wy1 * wz1) * Q[cy + cz];
+  s = s + (wx1 * wy0 * wz0) * Q[1];
+  s = s + (wx1 * wy1 * wz0) * Q[1 + cy];
+  s = s + (wx1 * wy0 * wz1) * Q[1 + cz];
+  s = s + (wx1 * wy1 * wz1) * Q[1 + cy + cz];
+  const T o = zero_old ? T(0) : old[F.off + sz * (int)F.sxy + sy * F.sx + sx];
+  return o + s / T(64);
+}
+
+// mgcorr + mgbound into a tail level in place: the ghost cells read interior
+// and ghost cells of the old iterate, so their new values go to `scratch`
+// (one value a ghost-table entry) first; then the interior cells (each reads
+// only itself) update in place, then the ghosts are copied back.
+template <typename T>
+__device__ void tail_prolong(const BlkLev* fb, const BlkLev* cb, const TailLevel& F, const T* phi_c, T* phi,
+                             T* scratch, int zero_old) {
+  for (int k = threadIdx.x; k < F.nghost; k += blockDim.x) {
+    const CellRef c = cell_ref(__ldg(F.ghosts + k));
+    scratch[k] = tail_prolong_value(fb[c.b], cb[c.b], phi_c, phi, c.x, c.y, c.z, zero_old);
+  }
+  __syncthreads();
+  for (int k = threadIdx.x; k < F.nint; k += blockDim.x) {
+    const CellRef c = cell_ref(__ldg(F.cells + k));
+    phi[c.i] = tail_prolong_value(fb[c.b], cb[c.b], phi_c, phi, c.x, c.y, c.z, zero_old);
+  }
+  __syncthreads();
+  for (int k = threadIdx.x; k < F.nghost; k += blockDim.x) phi[(int)(__ldg(F.ghosts + k) & 0xffffffull)] = scratch[k];
+  __syncthreads();
+}
+
+// The rhs of a tail level from global memory (the restriction into the
+// first tail level ran outside); eight loads in flight a thread.
+template <typename T>
+__device__ void tail_load_rhs(const BlkLev* gb, const BlkLev* cb, const TailLevel& L, const T* __restrict__ g, T* rhs) {
+  constexpr int U = 8;
+  for (int k0 = threadIdx.x; k0 < L.nint; k0 += U * blockDim.x) {
+    T v[U];
+    int ri[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int k = k0 + u * blockDim.x;
+      ri[u] = -1;
+      if (k < L.nint) {
+        const CellRef c = cell_ref(__ldg(L.cells + k));
+        v[u] = g[global_index(gb[c.b], c.x, c.y, c.z)];
+        ri[u] = rhs_index(cb[c.b], c.x, c.y, c.z);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u)
+      if (ri[u] >= 0) rhs[ri[u]] = v[u];
+  }
+  __syncthreads();
+}
+
+// A tail level back to global memory: iterate (interior and ghost cells) and rhs.
+template <typename T>
+__device__ void tail_store(const BlkLev* gb, const BlkLev* cb, const TailLevel& L, const T* phi, const T* rhs,
+                           T* __restrict__ gphi, T* __restrict__ grhs) {
+  for (int k = threadIdx.x; k < L.nint + L.nghost; k += blockDim.x) {
+    const CellRef c = cell_ref(__ldg(k < L.nint ? L.cells + k : L.ghosts + (k - L.nint)));
+    const long long gi = global_index(gb[c.b], c.x, c.y, c.z);
+    gphi[gi] = phi[c.i];
+    if (k < L.nint) grhs[gi] = rhs[rhs_index(cb[c.b], c.x, c.y, c.z)];
+  }
+  __syncthreads();
+}
+
+// The coarse end of a V-cycle in one CTA, every level in shared memory: the
+// relaxations, restrictions, precision conversions and corrections of the
+// tail levels run as the ops of a program built on the host, in order, with
+// the CTA's barriers between them instead of kernel boundaries; one op loads
+// the first tail level's rhs, the last ones store every tail level.
+// curmask bit 2l (2l+1) selects the global FP32 (FP64) iterate buffer of
+// tail level l.
+__global__ void __launch_bounds__(1024) k_coarse_tail(const TailLevel* __restrict__ lv, const TailOp* __restrict__ ops,
+                                                      int nops, unsigned curmask) {
+  pdl_trigger();
+  __shared__ BlkLev fb[kSmallLevelBlocks], cb[kSmallLevelBlocks], gb[kSmallLevelBlocks];
+  extern __shared__ unsigned char smem_raw[];
+  unsigned char* arena = smem_base128(smem_raw);
+  pdl_wait();
+  for (int o = 0; o < nops; ++o) {
+    const TailOp op = ops[o];
+    const TailLevel& F = lv[op.fine];
+    const TailLevel& C = lv[op.coarse];
+    const int nb = F.nb;
+    __syncthreads();  // the previous op is done with the tables
+    for (int b = threadIdx.x; b < nb; b += blockDim.x) {
+      fb[b] = F.cbl[b];
+      cb[b] = C.cbl[b];
+      gb[b] = F.gbl[b];
+    }
+    __syncthreads();
+    auto at32 = [&](int off) { return reinterpret_cast<float*>(arena + off); };
+    auto at64 = [&](int off) { return reinterpret_cast<double*>(arena + off); };
+    switch (op.kind) {
+      case kTailLoadRhs:
+        if (op.f64) tail_load_rhs<double>(gb, fb, F, F.rhs64, at64(F.s_rhs64));
+        else tail_load_rhs<float>(gb, fb, F, F.rhs32, at32(F.s_rhs32));
+        break;
+      case kTailRelax:
+        if (op.f64) {
+          double* phi = at64(F.s_phi64);
+          if (op.zero) {
+            for (int q = threadIdx.x; q < F.npad; q += blockDim.x) phi[q] = 0.0;
+            __syncthreads();
+          }
+          tail_relax<double>(fb, F, phi, at64(F.s_rhs64), op.sweeps);
+        } else {
+          float* phi = at32(F.s_phi32);
+          if (op.zero) {
+            for (int q = threadIdx.x; q < F.npad; q += blockDim.x) phi[q] = 0.f;
+            __syncthreads();
+          }
+          tail_relax<float>(fb, F, phi, at32(F.s_rhs32), op.sweeps);
+        }
+        break;
+      case kTailRestrict:  // into the coarse rhs of the fine level's precision
+        if (op.f64) tail_restrict<double>(fb, cb, C, at64(F.s_phi64), at64(F.s_rhs64), at64(C.s_rhs64), op.zero);
+        else tail_restrict<float>(fb, cb, C, at32(F.s_phi32), at32(F.s_rhs32), at32(C.s_rhs32), op.zero);
+        break;
+      case kTailProlong:
+        if (op.f64)
+          tail_prolong<double>(fb, cb, F, at64(C.s_phi64), at64(F.s_phi64), at64(op.sweeps), op.zero);
+        else
+          tail_prolong<float>(fb, cb, F, at32(C.s_phi32), at32(F.s_phi32), at32(op.sweeps), op.zero);
+        break;
+      case kTailRhsF2D: {  // the coarsest rhs of a mixed solve to FP64
+        const float* a = at32(F.s_rhs32);
+        double* b = at64(F.s_rhs64);
+        for (int q = threadIdx.x; q < F.nint; q += blockDim.x) b[q] = (double)a[q];
+        __syncthreads();
+        break;
+      }
+      case kTailPhiD2F: {  // the coarsest iterate of a mixed solve to FP32
+        const double* a = at64(F.s_phi64);
+        float* b = at32(F.s_phi32);
+        for (int q = threadIdx.x; q < F.npad; q += blockDim.x) b[q] = (float)a[q];
+        __syncthreads();
+        break;
+      }
+      case kTailStore: {
+        const int c32 = (curmask >> (2 * op.fine)) & 1, c64 = (curmask >> (2 * op.fine + 1)) & 1;
+        if (F.s_phi32 >= 0) tail_store<float>(gb, fb, F, at32(F.s_phi32), at32(F.s_rhs32), F.phi32[c32], F.rhs32);
+        if (F.s_phi64 >= 0) tail_store<double>(gb, fb, F, at64(F.s_phi64), at64(F.s_rhs64), F.phi64[c64], F.rhs64);
+        break;
+      }
+      default:
+        break;
+    }
+  }
+}
+
+cudaError_t coarse_tail_attributes() {
+  return cudaFuncSetAttribute(k_coarse_tail, cudaFuncAttributeMaxDynamicSharedMemorySize, kTailSmemBytes);
+}
+
+cudaError_t launch_coarse_tail(const TailLevel* lv, const TailOp* ops, int nops, unsigned curmask, int smem_bytes,
+                               cudaStream_t st) {
+  if (nops <= 0) return cudaSuccess;
+  pdl_launch(k_coarse_tail, 1, 1024, (size_t)smem_bytes, st, lv, ops, nops, curmask);
+  return cudaGetLastError();
 }
 
 template <typename T>
@@ -1955,7 +2278,6 @@ __global__ void __launch_bounds__(256) k_prolong_vec(const BlkLev* __restrict__ 
                                                      const Tile* __restrict__ tiles, const T* __restrict__ phi_c,
                                                      const T* __restrict__ old, T* __restrict__ out) {
   pdl_trigger();
-  pdl_wait();
   constexpr int VEC = 16 / (int)sizeof(T);
   constexpr int NC = VEC / 2 + 2;  // coarse columns a group reads
   using V = typename std::conditional<sizeof(T) == 4, float4, double2>::type;
@@ -1980,6 +2302,7 @@ __global__ void __launch_bounds__(256) k_prolong_vec(const BlkLev* __restrict__ 
   }
   const long long cy = C.sx, cz = C.sxy;
   const int ng = F.nx / VEC;
+  pdl_wait();  // everything above reads only setup data
   for (int k = threadIdx.x >> 5; k <= F.ny / 2; k += 8) {
     // rows 2k, 2k+1 and their sources
     int yq[2], syq[2];
@@ -2252,7 +2575,6 @@ __global__ void __launch_bounds__(32 * (kDefectRows + 2)) k_defect_march(
     const TE* __restrict__ e, double* __restrict__ p_next, const double* __restrict__ bvec, TR* __restrict__ rhs_out,
     double mean_b, double rscale, double* __restrict__ partials) {
   pdl_trigger();
-  pdl_wait();
   using C = DefectCfg<TE, GP>;
   constexpr int R = C::R, RW = C::RW, NR = kDefectRing;
   extern __shared__ unsigned char smem_raw[];
@@ -2332,6 +2654,7 @@ __global__ void __launch_bounds__(32 * (kDefectRows + 2)) k_defect_march(
     if (gc) p_next[rz + gx] = g;
   };
 
+  pdl_wait();  // everything above reads only setup data
 #pragma unroll
   for (int q = 0; q < NR; ++q) issue(zs - 1 + q);
   take(P[0], G[0], bz, zs - 1);
@@ -2512,7 +2835,6 @@ __global__ void __launch_bounds__(TPR* TYC) k_restrict_tma(const BlkLev* __restr
                                                           const T* __restrict__ fy, const T* __restrict__ fz,
                                                           int* err) {
   pdl_trigger();
-  pdl_wait();
   using C = RTmaCfg<T, TPR, CPX, TYC, NS>;
   static_assert(D + 2 <= NS, "a fine plane is read until the phase after its own");
   using P2 = typename std::conditional<sizeof(T) == 4, float2, double2>::type;
@@ -2546,6 +2868,7 @@ __global__ void __launch_bounds__(TPR* TYC) k_restrict_tma(const BlkLev* __restr
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
   __syncthreads();
+  pdl_wait();  // everything above reads only setup data
 
   auto pslot = [&](int q) -> const T* { return reinterpret_cast<const T*>(base + (q % NS) * C::SLOT); };
   auto rslot = [&](int q) -> const T* { return reinterpret_cast<const T*>(base + (q % NS) * C::SLOT + C::PSLOT); };

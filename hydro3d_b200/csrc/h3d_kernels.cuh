@@ -88,6 +88,52 @@ constexpr int kSmallLevelBlocks = 64;  // block descriptors the fused small-leve
 // in place in one CTA (see k_relax_small).  start: flat interior index of
 // each block's first cell (nb+1 entries); the fill table must read interior
 // cells only.
+// The coarse end of a V-cycle in one CTA (k_coarse_tail), every tail level
+// in shared memory in a compact layout: per tail level its block tables
+// (global layout for loads and stores; compact layout with the rhs base of
+// each block in .pad), cell tables, compact fill table, global buffers and
+// the byte offsets of its arrays in the shared arena (-1: absent).
+struct TailLevel {
+  const BlkLev* gbl;
+  const BlkLev* cbl;
+  const unsigned long long* cells;   // interior cells, red (x+y+z odd) first
+  const unsigned long long* ghosts;  // ghost cells of the padded blocks
+  const uint32_t* fdst;              // sweep fill table, compact indices
+  const uint32_t* fsrc;
+  int nb, nint, nred, nghost, npad, nfill;
+  float* phi32[2];
+  float* rhs32;
+  double* phi64[2];
+  double* rhs64;
+  int s_phi32, s_rhs32, s_phi64, s_rhs64;
+};
+enum TailKind {
+  kTailRelax = 0,
+  kTailRestrict = 1,
+  kTailProlong = 2,
+  kTailRhsF2D = 3,
+  kTailPhiD2F = 4,
+  kTailLoadRhs = 5,
+  kTailStore = 6
+};
+struct TailOp {
+  int kind;
+  int f64;     // the op runs in FP64
+  int fine;    // relax / conversions / load / store: the level; restrict / prolong: the fine level
+  int coarse;  // restrict / prolong: the coarse level
+  int sweeps;  // relax: sweeps; prolong: arena offset of the ghost scratch
+  int zero;    // relax: zero the iterate first; restrict / prolong: the fine iterate is zero
+};
+constexpr int kTailMaxLevels = 16;  // curmask holds two bits a level
+constexpr int kTailSmemBytes = 212 * 1024;  // shared arena of the tail (+ 12 KB of block tables)
+// Cell entry of the tail tables: compact index (24 bits), x, y, z (8 bits each), block (6 bits).
+inline unsigned long long tail_cell(long long i, int x, int y, int z, int b) {
+  return (unsigned long long)i | ((unsigned long long)x << 24) | ((unsigned long long)y << 32) |
+         ((unsigned long long)z << 40) | ((unsigned long long)b << 48);
+}
+cudaError_t launch_coarse_tail(const TailLevel* lv, const TailOp* ops, int nops, unsigned curmask, int smem_bytes,
+                               cudaStream_t st);
+
 template <typename T>
 cudaError_t launch_relax_small(bool var, const BlkLev* bl, const int* start, int nb, T* phi, const T* rhs,
                                const T* fx, const T* fy, const T* fz, const uint32_t* fdst, const uint32_t* fsrc,

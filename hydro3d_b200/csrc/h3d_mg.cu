@@ -33,6 +33,7 @@ namespace {
 
 // Levels with at most this many interior cells relax in one single-CTA launch.
 constexpr int64_t kSmallLevelCells = 2048;
+constexpr int64_t kTailLevelCells = 2048;  // levels the fused coarse tail (one CTA) takes
 
 struct Halo {
   uint32_t* d_dst = nullptr;
@@ -77,8 +78,9 @@ struct Level {
   int nrtiles = 0, rvariant = 0, rzc = 1;
   bool tma_ok = false;
   bool f32 = false, var = false;  // iterate precision of the level's smoother; variable coefficients
-  int* d_cstart = nullptr;  // small levels: flat interior index of each block's first cell (fused relaxation)
+  int* d_cstart = nullptr;  // small / tail levels: flat interior index of each block's first cell
   bool small = false;       // relaxation runs as one fused single-CTA kernel
+  bool tailable = false;    // small enough for the fused coarse tail (has d_cstart)
   int cur64 = 0, cur32 = 0;
   bool zero64 = false, zero32 = false;
   double sweep_bytes = 0;       // algorithmic bytes of one sweep (FP64 or FP32 by mode)
@@ -127,6 +129,16 @@ struct h3d_mg {
   // contiguous host transfers; allocated on first use
   double* stage[2] = {nullptr, nullptr};
   std::vector<size_t> stage_off;
+  // fused coarse tail: levels tail_g..L in one single-CTA launch (tail_g = 0: none)
+  int tail_g = 0;
+  TailLevel* d_tail_lv = nullptr;
+  TailOp* d_tail_ops = nullptr;
+  unsigned long long* d_tail_cells = nullptr;  // cell tables of all tail levels
+  BlkLev* d_tail_cbl = nullptr;                // compact block tables of the tail levels
+  uint32_t* d_tail_fills = nullptr;            // compact sweep fill tables of the tail levels
+  int tail_nops = 0;
+  int tail_smem = 0;  // dynamic shared memory of the tail launch
+  std::vector<char> tail_zero32, tail_zero64;  // zero flags of the tail levels after the tail
 };
 
 namespace {
@@ -530,6 +542,26 @@ struct Exec {
   }
 
   // mgkcyc control flow (mgsolver.for:272-352) with kcycle = 1.
+  // the fused coarse tail (levels tail_g..L), entered right after the
+  // restriction into level tail_g
+  int tail() {
+    const int g0 = h->tail_g;
+    unsigned mask = 0;
+    for (int g = g0; g <= h->L; ++g) {
+      const Level& V = L(g);
+      mask |= (unsigned)(V.cur32 & 1) << (2 * (g - g0));
+      mask |= (unsigned)(V.cur64 & 1) << (2 * (g - g0) + 1);
+    }
+    CU(launch_coarse_tail(h->d_tail_lv, h->d_tail_ops, h->tail_nops, mask, h->tail_smem, h->st));
+    TRY(chk("coarse tail", g0));
+    for (int g = g0; g <= h->L; ++g) {
+      L(g).zero32 = h->tail_zero32[g - g0] != 0;
+      L(g).zero64 = h->tail_zero64[g - g0] != 0;
+    }
+    h->kernels += 1;
+    return H3D_OK;
+  }
+
   int vcycle() {
     const int Lv = h->L;
     const int irestr = h->desc.irestr, iproln = h->desc.iproln;
@@ -549,6 +581,13 @@ struct Exec {
     int g = 2, nrel = irestr;
     for (;;) {
       if (g == 1) break;
+      if (g == h->tail_g && kount[g] == 0) {  // levels g..L in one launch, up to g's post-relaxation
+        TRY(tail());
+        TRY(correct(g - 1));
+        g -= 1;
+        nrel = iproln;
+        continue;
+      }
       kount[g] += 1;
       TRY(relax_at(g, nrel, true));
       if (kount[g] == 2) {
@@ -1137,6 +1176,275 @@ int h3d_topology(int32_t nblocks, const int32_t* ext, const int32_t* bc, const d
   return H3D_OK;
 }
 
+// The fused coarse tail: the deepest run of levels g..L (g >= 2, at least two
+// levels, constant coefficients) whose arrays all fit the shared arena of one
+// CTA.  Its op program replays, from the moment the restriction into level g
+// has run, exactly what Exec::vcycle would launch for those levels
+// (relaxations with their zero-iterate flags, restrictions, the FP64
+// coarsest level's conversions, corrections), up to the post-relaxation of
+// level g; the correction into level g-1 stays outside.  The program starts
+// by loading level g's rhs and ends by storing every tail level.
+namespace {
+struct TailPlan {
+  std::vector<int> s_phi32, s_rhs32, s_phi64, s_rhs64;  // arena offsets per tail level
+  int scratch = 0, bytes = 0;
+};
+bool plan_tail(const h3d_mg* h, int g0, TailPlan* P) {
+  auto al = [](int v) { return (v + 15) & ~15; };
+  int at = 0, scratch = 0;
+  for (int q = g0; q <= h->L; ++q) {
+    const Level& V = h->lev[q];
+    int npad = 0, nint = (int)V.geom.n_interior;
+    for (const auto& B : V.geom.bl) npad += (B.nx + 2) * (B.ny + 2) * (B.nz + 2);
+    const bool f32 = f32_level(h, q), f64 = !f32 || (h->mixed && q == h->L);
+    const bool use32 = h->mixed;
+    int p32 = -1, r32 = -1, p64 = -1, r64 = -1;
+    if (use32) { p32 = at; at = al(at + npad * 4); r32 = at; at = al(at + nint * 4); }
+    if (f64) { p64 = at; at = al(at + npad * 8); r64 = at; at = al(at + nint * 8); }
+    P->s_phi32.push_back(p32);
+    P->s_rhs32.push_back(r32);
+    P->s_phi64.push_back(p64);
+    P->s_rhs64.push_back(r64);
+    if (q < h->L) scratch = std::max(scratch, (npad - nint) * (f32 ? 4 : 8));
+  }
+  P->scratch = at;
+  P->bytes = al(at + scratch) + 128;
+  return P->bytes <= kTailSmemBytes;
+}
+}  // namespace
+
+int build_tail(h3d_mg* h) {
+  const int Lv = h->L;
+  if (h->var) return H3D_OK;
+  int g0 = Lv + 1;
+  TailPlan plan;
+  for (int g = Lv; g >= 2; --g) {
+    TailPlan P;
+    if (!h->lev[g].tailable || !plan_tail(h, g, &P)) break;
+    g0 = g;
+    plan = P;
+  }
+  if (g0 > Lv - 1 || Lv - g0 + 1 > kTailMaxLevels) return H3D_OK;  // fewer than two tail levels
+  const int irestr = h->desc.irestr, iproln = h->desc.iproln, csw = h->desc.coarse_sweeps;
+  auto ti = [&](int g) { return g - g0; };
+  std::vector<char> z32(Lv + 2, 0), z64(Lv + 2, 0);
+  if (f32_level(h, g0)) z32[g0] = 1;
+  else z64[g0] = 1;
+  std::vector<TailOp> ops;
+  auto op = [&](int kind, bool f64, int fine, int coarse, int sweeps, int zero) {
+    ops.push_back(TailOp{kind, f64 ? 1 : 0, ti(fine), ti(coarse), sweeps, zero});
+  };
+  op(kTailLoadRhs, !f32_level(h, g0), g0, g0, 0, 0);
+  auto relax = [&](int g, int it) {
+    if (it <= 0) return;
+    const bool f32 = f32_level(h, g);
+    char& z = f32 ? z32[g] : z64[g];
+    op(kTailRelax, !f32, g, g, it, z);
+    z = 0;
+  };
+  auto relax_at = [&](int g, int it, bool first) {
+    if (g == Lv && Lv > 1 && csw > 0) {
+      if (first) relax(g, csw);
+      return;
+    }
+    relax(g, it);
+  };
+  auto restrict_to = [&](int gc) {
+    const bool f32 = f32_level(h, gc - 1);
+    op(kTailRestrict, !f32, gc - 1, gc, 0, f32 ? z32[gc - 1] : z64[gc - 1]);
+    if (f32) {
+      z32[gc] = 1;
+      if (!f32_level(h, gc)) {
+        op(kTailRhsF2D, true, gc, gc, 0, 0);
+        z64[gc] = 1;
+      }
+    } else {
+      z64[gc] = 1;
+    }
+  };
+  auto zero_fill = [&](int g, bool f64) { op(kTailRelax, f64, g, g, 0, 1); };
+  auto correct = [&](int gf) {
+    const int gc = gf + 1;
+    if (f32_level(h, gf)) {
+      if (f32_level(h, gc)) {
+        if (z32[gc]) { zero_fill(gc, false); z32[gc] = 0; }
+      } else {
+        if (z64[gc]) { zero_fill(gc, true); z64[gc] = 0; }
+        op(kTailPhiD2F, false, gc, gc, 0, 0);
+      }
+      op(kTailProlong, false, gf, gc, plan.scratch, z32[gf]);
+      z32[gf] = 0;
+    } else {
+      if (z64[gc]) { zero_fill(gc, true); z64[gc] = 0; }
+      op(kTailProlong, true, gf, gc, plan.scratch, z64[gf]);
+      z64[gf] = 0;
+    }
+  };
+  // the loop of Exec::vcycle from the first visit of level g0 on
+  std::vector<int> kount(Lv + 2, 0);
+  int g = g0, nrel = irestr;
+  for (;;) {
+    kount[g] += 1;
+    relax_at(g, nrel, true);
+    if (kount[g] == 2) {
+      if (g == g0) break;
+      correct(g - 1);
+      kount[g] = 0;
+      g -= 1;
+      nrel = iproln;
+    } else if (g < Lv) {
+      restrict_to(g + 1);
+      g += 1;
+      nrel = irestr;
+    } else {
+      relax_at(g, iproln, false);
+      correct(g - 1);
+      nrel = iproln;
+      g = Lv - 1;
+      if (g < g0) break;
+    }
+  }
+  for (int q = g0; q <= Lv; ++q) op(kTailStore, false, q, q, 0, 0);
+  // compact layouts, cell tables and fill tables
+  std::vector<unsigned long long> cells;
+  std::vector<uint32_t> fills;
+  std::vector<BlkLev> cbl;
+  struct At { size_t cells, ghosts, cbl, fdst, fsrc; int nint, nred, nghost, npad, nfill; };
+  std::vector<At> at;
+  for (int q = g0; q <= Lv; ++q) {
+    const Level& V = h->lev[q];
+    At a{};
+    a.cbl = cbl.size();
+    std::vector<long long> pbase, rbase;
+    long long pb = 0, rb = 0;
+    for (const auto& B : V.geom.bl) {
+      if (B.nx + 1 > 255 || B.ny + 1 > 255 || B.nz + 1 > 255) return H3D_OK;
+      BlkLev c = B;
+      c.off = pb;
+      c.sx = B.nx + 2;
+      c.sxy = (long long)(B.nx + 2) * (B.ny + 2);
+      c.pad = (int)rb;
+      cbl.push_back(c);
+      pbase.push_back(pb);
+      rbase.push_back(rb);
+      pb += c.sxy * (B.nz + 2);
+      rb += (long long)B.nx * B.ny * B.nz;
+    }
+    if (pb >= (1LL << 24)) return H3D_OK;
+    std::vector<unsigned long long> red, black, ghost;
+    for (size_t b = 0; b < V.geom.bl.size(); ++b) {
+      const BlkLev& B = V.geom.bl[b];
+      const BlkLev& c = cbl[a.cbl + b];
+      for (int z = 0; z <= B.nz + 1; ++z)
+        for (int y = 0; y <= B.ny + 1; ++y)
+          for (int x = 0; x <= B.nx + 1; ++x) {
+            const unsigned long long e = tail_cell(c.off + (long long)z * c.sxy + (long long)y * c.sx + x, x, y, z,
+                                                   (int)b);
+            const bool gh = x == 0 || y == 0 || z == 0 || x == B.nx + 1 || y == B.ny + 1 || z == B.nz + 1;
+            if (gh) ghost.push_back(e);
+            else if ((x + y + z) & 1) red.push_back(e);
+            else black.push_back(e);
+          }
+    }
+    a.cells = cells.size();
+    a.nred = (int)red.size();
+    a.nint = (int)(red.size() + black.size());
+    cells.insert(cells.end(), red.begin(), red.end());
+    cells.insert(cells.end(), black.begin(), black.end());
+    a.ghosts = cells.size();
+    a.nghost = (int)ghost.size();
+    cells.insert(cells.end(), ghost.begin(), ghost.end());
+    a.npad = (int)pb;
+    // the sweep fill table in compact indices
+    std::vector<uint32_t> d, sidx;
+    std::string err;
+    int rc = build_halo_table(h->blocks, q, kHaloSweep, true, d, sidx, &err);
+    if (rc != H3D_OK) return fail(h, rc, err);
+    auto compact = [&](uint32_t gi, long long* out) -> bool {
+      for (size_t b = 0; b < V.geom.bl.size(); ++b) {
+        const BlkLev& B = V.geom.bl[b];
+        const long long lo = B.off, hi = B.off + B.sxy * (B.nz + 2);
+        if ((long long)gi < lo || (long long)gi >= hi) continue;
+        const long long l = (long long)gi - lo;
+        const int z = (int)(l / B.sxy), y = (int)((l % B.sxy) / B.sx), x = (int)(l % B.sx);
+        if (x > B.nx + 1) return false;
+        const BlkLev& c = cbl[a.cbl + b];
+        *out = c.off + (long long)z * c.sxy + (long long)y * c.sx + x;
+        return true;
+      }
+      return false;
+    };
+    a.fdst = fills.size();
+    for (uint32_t v : d) {
+      long long ci;
+      if (!compact(v, &ci)) return H3D_OK;
+      fills.push_back((uint32_t)ci);
+    }
+    a.fsrc = fills.size();
+    for (uint32_t v : sidx) {
+      long long ci;
+      if ((v & kOldFlag) || !compact(v & kIdxMask, &ci)) return H3D_OK;
+      fills.push_back((uint32_t)ci);
+    }
+    a.nfill = (int)d.size();
+    at.push_back(a);
+  }
+  int rc;
+  BlkLev* d_cbl = nullptr;
+  uint32_t* d_fills = nullptr;
+  if ((rc = dalloc(h, &h->d_tail_cells, cells.size())) != H3D_OK || (rc = dalloc(h, &d_cbl, cbl.size())) != H3D_OK ||
+      (rc = dalloc(h, &d_fills, std::max<size_t>(fills.size(), 1))) != H3D_OK)
+    return rc;
+  h->d_tail_cbl = d_cbl;
+  h->d_tail_fills = d_fills;
+  if (cudaMemcpy(h->d_tail_cells, cells.data(), cells.size() * 8, cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(d_cbl, cbl.data(), cbl.size() * sizeof(BlkLev), cudaMemcpyHostToDevice) != cudaSuccess ||
+      (!fills.empty() &&
+       cudaMemcpy(d_fills, fills.data(), fills.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess))
+    return fail(h, H3D_ERR_CUDA, "coarse tail tables");
+  std::vector<TailLevel> lv;
+  for (int q = g0; q <= Lv; ++q) {
+    const Level& V = h->lev[q];
+    const At& a = at[q - g0];
+    const int k = q - g0;
+    TailLevel t{};
+    t.gbl = V.d_bl;
+    t.cbl = d_cbl + a.cbl;
+    t.cells = h->d_tail_cells + a.cells;
+    t.ghosts = h->d_tail_cells + a.ghosts;
+    t.fdst = d_fills + a.fdst;
+    t.fsrc = d_fills + a.fsrc;
+    t.nb = (int)V.geom.bl.size();
+    t.nint = a.nint;
+    t.nred = a.nred;
+    t.nghost = a.nghost;
+    t.npad = a.npad;
+    t.nfill = a.nfill;
+    t.phi32[0] = V.phi32[0];
+    t.phi32[1] = V.phi32[1];
+    t.rhs32 = V.rhs32;
+    t.phi64[0] = V.phi64[0];
+    t.phi64[1] = V.phi64[1];
+    t.rhs64 = V.rhs64;
+    t.s_phi32 = plan.s_phi32[k];
+    t.s_rhs32 = plan.s_rhs32[k];
+    t.s_phi64 = plan.s_phi64[k];
+    t.s_rhs64 = plan.s_rhs64[k];
+    lv.push_back(t);
+  }
+  if ((rc = dalloc(h, &h->d_tail_lv, lv.size())) != H3D_OK) return rc;
+  if ((rc = dalloc(h, &h->d_tail_ops, ops.size())) != H3D_OK) return rc;
+  if (cudaMemcpy(h->d_tail_lv, lv.data(), lv.size() * sizeof(TailLevel), cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(h->d_tail_ops, ops.data(), ops.size() * sizeof(TailOp), cudaMemcpyHostToDevice) != cudaSuccess)
+    return fail(h, H3D_ERR_CUDA, "coarse tail program");
+  h->tail_nops = (int)ops.size();
+  h->tail_smem = plan.bytes;
+  h->tail_zero32.assign(z32.begin() + g0, z32.begin() + Lv + 1);
+  h->tail_zero64.assign(z64.begin() + g0, z64.begin() + Lv + 1);
+  h->tail_g = g0;
+  return H3D_OK;
+}
+
 int h3d_mg_destroy(h3d_mg* h) {
   if (!h) return H3D_OK;
   cudaSetDevice(h->device);
@@ -1161,6 +1469,11 @@ int h3d_mg_destroy(h3d_mg* h) {
   dfree(h->d_res);
   dfree(h->d_h3);
   dfree(h->d_err);
+  dfree(h->d_tail_lv);
+  dfree(h->d_tail_ops);
+  dfree(h->d_tail_cells);
+  dfree(h->d_tail_cbl);
+  dfree(h->d_tail_fills);
   dfree(h->stage[0]);
   dfree(h->stage[1]);
   if (h->h_res) cudaFreeHost(h->h_res);
@@ -1264,8 +1577,9 @@ int h3d_mg_create(h3d_mg** out, const h3d_mg_desc* desc) {
     std::string err;
     if ((rc = build_halo_table(h->blocks, g, kHaloSweep, true, d, s, &err)) != H3D_OK) return bail(fail(h, rc, err));
     if ((rc = upload_halo(h, V.sweep, d, s)) != H3D_OK) return bail(rc);
-    // small levels relax in one fused launch when their fill reads interior cells only
-    if (g > 1 && V.geom.n_interior <= kSmallLevelCells && V.geom.bl.size() <= (size_t)kSmallLevelBlocks) {
+    // small levels relax in one fused launch when their fill reads interior cells only;
+    // slightly larger ones can still join the fused coarse tail
+    if (g > 1 && V.geom.n_interior <= kTailLevelCells && V.geom.bl.size() <= (size_t)kSmallLevelBlocks) {
       bool old = false;
       for (uint32_t v : s) old = old || (v & kOldFlag);
       if (!old) {
@@ -1274,7 +1588,8 @@ int h3d_mg_create(h3d_mg** out, const h3d_mg_desc* desc) {
         if ((rc = dalloc(h, &V.d_cstart, cs.size())) != H3D_OK) return bail(rc);
         if (cudaMemcpy(V.d_cstart, cs.data(), cs.size() * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess)
           return bail(fail(h, H3D_ERR_CUDA, "small-level table"));
-        V.small = true;
+        V.tailable = true;
+        V.small = V.geom.n_interior <= kSmallLevelCells;
       }
     }
     if (g == 1) {
@@ -1345,6 +1660,7 @@ int h3d_mg_create(h3d_mg** out, const h3d_mg_desc* desc) {
     V.sweep_bytes = (double)V.geom.n_interior * w * (3.0 + (h->var ? 3.0 : 0.0));
     V.sweep_bytes_zero = (double)V.geom.n_interior * w * (2.0 + (h->var ? 3.0 : 0.0));
   }
+  if ((rc = build_tail(h)) != H3D_OK) return bail(rc);
   const size_t n1 = (size_t)h->lev[1].geom.n_elems;
   if ((rc = dalloc(h, &h->p64[0], n1)) || (rc = dalloc(h, &h->p64[1], n1)) || (rc = dalloc(h, &h->b64, n1)))
     return bail(rc);
