@@ -10,6 +10,8 @@
 
 #include <type_traits>
 
+#include <cooperative_groups.h>
+
 #include "h3d_kernels.cuh"
 
 namespace h3d {
@@ -1967,28 +1969,35 @@ __device__ __forceinline__ long long global_index(const BlkLev& G, int x, int y,
   return G.off + (long long)z * G.sxy + (long long)y * G.sx + x;
 }
 
+// The red then the black cells of one in-place sweep of a tail level; same
+// cell arithmetic as small_relax.
+template <typename T>
+__device__ void tail_colours(const BlkLev* cb, const TailLevel& L, T* phi, const T* rhs) {
+  for (int colour = 0; colour < 2; ++colour) {  // red (x+y+z odd) first
+    const int k0 = colour ? L.nred : 0, k1 = colour ? L.nint : L.nred;
+    for (int k = k0 + threadIdx.x; k < k1; k += blockDim.x) {
+      const CellRef c = cell_ref(L.cells[k]);
+      const BlkLev& B = cb[c.b];
+      const int i = c.i;
+      const Coef<T> cf = cell_coef<T, false>(B, c.x, c.y, c.z, i - B.off, nullptr, nullptr, nullptr);
+      const T ap = coef_ap(cf);
+      const T v = gs_div(rhs[rhs_index(B, c.x, c.y, c.z)] -
+                             (cf.aw * phi[i - 1] + cf.ae * phi[i + 1] + cf.as * phi[i - B.sx] +
+                              cf.an * phi[i + B.sx] + cf.ab * phi[i - B.sxy] + cf.at * phi[i + B.sxy]),
+                         ap);
+      phi[i] = v;
+    }
+    __syncthreads();
+  }
+}
+
 // `sweeps` in-place red-black sweeps of a tail level, each followed by its
-// ghost fill; same cell arithmetic as small_relax.
+// ghost fill.
 template <typename T>
 __device__ void tail_relax(const BlkLev* cb, const TailLevel& L, T* phi, const T* rhs, int sweeps) {
   for (int it = 0; it < sweeps; ++it) {
-    for (int colour = 0; colour < 2; ++colour) {  // red (x+y+z odd) first
-      const int k0 = colour ? L.nred : 0, k1 = colour ? L.nint : L.nred;
-      for (int k = k0 + threadIdx.x; k < k1; k += blockDim.x) {
-        const CellRef c = cell_ref(__ldg(L.cells + k));
-        const BlkLev& B = cb[c.b];
-        const int i = c.i;
-        const Coef<T> cf = cell_coef<T, false>(B, c.x, c.y, c.z, i - B.off, nullptr, nullptr, nullptr);
-        const T ap = coef_ap(cf);
-        const T v = gs_div(rhs[rhs_index(B, c.x, c.y, c.z)] -
-                               (cf.aw * phi[i - 1] + cf.ae * phi[i + 1] + cf.as * phi[i - B.sx] +
-                                cf.an * phi[i + B.sx] + cf.ab * phi[i - B.sxy] + cf.at * phi[i + B.sxy]),
-                           ap);
-        phi[i] = v;
-      }
-      __syncthreads();
-    }
-    for (int q = threadIdx.x; q < L.nfill; q += blockDim.x) phi[__ldg(L.fdst + q)] = phi[__ldg(L.fsrc + q)];
+    tail_colours<T>(cb, L, phi, rhs);
+    for (int q = threadIdx.x; q < L.nfill; q += blockDim.x) phi[L.fdst[q]] = phi[L.fsrc[q]];
     __syncthreads();
   }
 }
@@ -1999,7 +2008,7 @@ template <typename T>
 __device__ void tail_restrict(const BlkLev* fb, const BlkLev* cb, const TailLevel& Cl, const T* phi, const T* rhs,
                               T* rhs_c, int zero_fine) {
   for (int k = threadIdx.x; k < Cl.nint; k += blockDim.x) {
-    const CellRef cc = cell_ref(__ldg(Cl.cells + k));
+    const CellRef cc = cell_ref(Cl.cells[k]);
     const BlkLev& F = fb[cc.b];
     const int X = cc.x, Y = cc.y, Z = cc.z;
     const T* P = phi + F.off;
@@ -2068,16 +2077,16 @@ template <typename T>
 __device__ void tail_prolong(const BlkLev* fb, const BlkLev* cb, const TailLevel& F, const T* phi_c, T* phi,
                              T* scratch, int zero_old) {
   for (int k = threadIdx.x; k < F.nghost; k += blockDim.x) {
-    const CellRef c = cell_ref(__ldg(F.ghosts + k));
+    const CellRef c = cell_ref(F.ghosts[k]);
     scratch[k] = tail_prolong_value(fb[c.b], cb[c.b], phi_c, phi, c.x, c.y, c.z, zero_old);
   }
   __syncthreads();
   for (int k = threadIdx.x; k < F.nint; k += blockDim.x) {
-    const CellRef c = cell_ref(__ldg(F.cells + k));
+    const CellRef c = cell_ref(F.cells[k]);
     phi[c.i] = tail_prolong_value(fb[c.b], cb[c.b], phi_c, phi, c.x, c.y, c.z, zero_old);
   }
   __syncthreads();
-  for (int k = threadIdx.x; k < F.nghost; k += blockDim.x) phi[(int)(__ldg(F.ghosts + k) & 0xffffffull)] = scratch[k];
+  for (int k = threadIdx.x; k < F.nghost; k += blockDim.x) phi[(int)(F.ghosts[k] & 0xffffffull)] = scratch[k];
   __syncthreads();
 }
 
@@ -2094,7 +2103,7 @@ __device__ void tail_load_rhs(const BlkLev* gb, const BlkLev* cb, const TailLeve
       const int k = k0 + u * blockDim.x;
       ri[u] = -1;
       if (k < L.nint) {
-        const CellRef c = cell_ref(__ldg(L.cells + k));
+        const CellRef c = cell_ref(L.cells[k]);
         v[u] = g[global_index(gb[c.b], c.x, c.y, c.z)];
         ri[u] = rhs_index(cb[c.b], c.x, c.y, c.z);
       }
@@ -2111,7 +2120,7 @@ template <typename T>
 __device__ void tail_store(const BlkLev* gb, const BlkLev* cb, const TailLevel& L, const T* phi, const T* rhs,
                            T* __restrict__ gphi, T* __restrict__ grhs) {
   for (int k = threadIdx.x; k < L.nint + L.nghost; k += blockDim.x) {
-    const CellRef c = cell_ref(__ldg(k < L.nint ? L.cells + k : L.ghosts + (k - L.nint)));
+    const CellRef c = cell_ref(k < L.nint ? L.cells[k] : L.ghosts[k - L.nint]);
     const long long gi = global_index(gb[c.b], c.x, c.y, c.z);
     gphi[gi] = phi[c.i];
     if (k < L.nint) grhs[gi] = rhs[rhs_index(cb[c.b], c.x, c.y, c.z)];
@@ -2205,8 +2214,178 @@ __global__ void __launch_bounds__(1024) k_coarse_tail(const TailLevel* __restric
   }
 }
 
+// The coarse end of a V-cycle as one thread-block cluster: CTA b holds block
+// b of every tail level in its shared memory (compact layout, every block of
+// a level the same size) and runs the same op program as k_coarse_tail on
+// it.  Restrictions, corrections and conversions only touch the CTA's own
+// block; after the colours of a sweep the cluster synchronises, every CTA
+// gathers its ghost cells from the other CTAs' shared memory (fdst: own
+// compact index; fsrc: source rank << 24 | its compact index), and the
+// cluster synchronises again before any interior changes.
+__global__ void __launch_bounds__(kClusterTailThreads) k_coarse_cluster(const TailLevel* __restrict__ lvg,
+                                                                        const TailOp* __restrict__ opsg, int nops,
+                                                                        int nlev, unsigned curmask) {
+  pdl_trigger();
+  namespace cg = cooperative_groups;
+  cg::cluster_group cl = cg::this_cluster();
+  const int b = (int)cl.block_rank();
+  __shared__ BlkLev fb[1], cb[1], gb[1];  // this block: fine / coarse compact layout, fine global layout
+  __shared__ TailLevel lv[kTailMaxLevels];
+  __shared__ TailOp ops[kClusterTailMaxOps];
+  extern __shared__ unsigned char smem_raw[];
+  unsigned char* arena = smem_base128(smem_raw);
+  // the program, the level records and this block's tables are setup data:
+  // stage them in shared memory (cell and ghost tables, this block's fill
+  // entries) while the predecessor finishes
+  for (int q = threadIdx.x; q < nops; q += blockDim.x) ops[q] = opsg[q];
+  if (threadIdx.x < nlev) lv[threadIdx.x] = lvg[threadIdx.x];
+  __syncthreads();
+  for (int l = 0; l < nlev; ++l) {
+    const TailLevel& G = lvg[l];
+    unsigned long long* cs = reinterpret_cast<unsigned long long*>(arena + lv[l].s_cells);
+    for (int k = threadIdx.x; k < G.nint + G.nghost; k += blockDim.x)
+      cs[k] = k < G.nint ? __ldg(G.cells + k) : __ldg(G.ghosts + (k - G.nint));
+    const int f0 = __ldg(G.fstart + b), f1 = __ldg(G.fstart + b + 1);
+    uint32_t* fd = reinterpret_cast<uint32_t*>(arena + lv[l].s_fill);
+    for (int k = threadIdx.x; k < f1 - f0; k += blockDim.x) {
+      fd[2 * k] = __ldg(G.fdst + f0 + k);
+      fd[2 * k + 1] = __ldg(G.fsrc + f0 + k);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      lv[l].cells = cs;
+      lv[l].ghosts = cs + G.nint;
+      lv[l].fdst = fd;
+      lv[l].nfill = f1 - f0;
+    }
+  }
+  __syncthreads();
+  pdl_wait();
+  auto compact = [](BlkLev B) {
+    B.off = 0;
+    B.sx = B.nx + 2;
+    B.sxy = (long long)(B.nx + 2) * (B.ny + 2);
+    B.pad = 0;
+    return B;
+  };
+  for (int o = 0; o < nops; ++o) {
+    const TailOp op = ops[o];
+    const TailLevel& F = lv[op.fine];
+    const TailLevel& C = lv[op.coarse];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      gb[0] = F.gbl[b];
+      fb[0] = compact(F.gbl[b]);
+      cb[0] = compact(C.gbl[b]);
+    }
+    __syncthreads();
+    auto at32 = [&](int off) { return reinterpret_cast<float*>(arena + off); };
+    auto at64 = [&](int off) { return reinterpret_cast<double*>(arena + off); };
+    switch (op.kind) {
+      case kTailLoadRhs:
+        if (op.f64) tail_load_rhs<double>(gb, fb, F, F.rhs64, at64(F.s_rhs64));
+        else tail_load_rhs<float>(gb, fb, F, F.rhs32, at32(F.s_rhs32));
+        break;
+      case kTailRelax: {
+        auto relax = [&](auto* phi, const auto* rhs) {
+          using T = typename std::remove_pointer<decltype(phi)>::type;
+          if (op.zero) {
+            for (int q = threadIdx.x; q < F.npad; q += blockDim.x) phi[q] = T(0);
+            __syncthreads();
+          }
+          for (int it = 0; it < op.sweeps; ++it) {
+            tail_colours<T>(fb, F, phi, rhs);
+            cl.sync();  // every block's sweep done
+            for (int q = threadIdx.x; q < F.nfill; q += blockDim.x) {  // (dst, src) pairs of this block
+              const uint32_t dsti = F.fdst[2 * q], src = F.fdst[2 * q + 1];
+              const T* remote = cl.map_shared_rank(phi, (int)(src >> 24));
+              phi[dsti] = remote[src & 0xffffffu];
+            }
+            cl.sync();  // every ghost gathered before any interior changes
+          }
+        };
+        if (op.f64) relax(at64(F.s_phi64), (const double*)at64(F.s_rhs64));
+        else relax(at32(F.s_phi32), (const float*)at32(F.s_rhs32));
+        break;
+      }
+      case kTailRestrict:
+        if (op.f64) tail_restrict<double>(fb, cb, C, at64(F.s_phi64), at64(F.s_rhs64), at64(C.s_rhs64), op.zero);
+        else tail_restrict<float>(fb, cb, C, at32(F.s_phi32), at32(F.s_rhs32), at32(C.s_rhs32), op.zero);
+        break;
+      case kTailProlong:
+        if (op.f64) tail_prolong<double>(fb, cb, F, at64(C.s_phi64), at64(F.s_phi64), at64(op.sweeps), op.zero);
+        else tail_prolong<float>(fb, cb, F, at32(C.s_phi32), at32(F.s_phi32), at32(op.sweeps), op.zero);
+        break;
+      case kTailRhsF2D: {
+        const float* x = at32(F.s_rhs32);
+        double* y = at64(F.s_rhs64);
+        for (int q = threadIdx.x; q < F.nint; q += blockDim.x) y[q] = (double)x[q];
+        __syncthreads();
+        break;
+      }
+      case kTailPhiD2F: {
+        const double* x = at64(F.s_phi64);
+        float* y = at32(F.s_phi32);
+        for (int q = threadIdx.x; q < F.npad; q += blockDim.x) y[q] = (float)x[q];
+        __syncthreads();
+        break;
+      }
+      case kTailStore: {
+        const int c32 = (curmask >> (2 * op.fine)) & 1, c64 = (curmask >> (2 * op.fine + 1)) & 1;
+        if (F.s_phi32 >= 0) tail_store<float>(gb, fb, F, at32(F.s_phi32), at32(F.s_rhs32), F.phi32[c32], F.rhs32);
+        if (F.s_phi64 >= 0) tail_store<double>(gb, fb, F, at64(F.s_phi64), at64(F.s_rhs64), F.phi64[c64], F.rhs64);
+        break;
+      }
+      default:
+        break;
+    }
+  }
+  cl.sync();  // no CTA leaves while another may still read its shared memory
+}
+
 cudaError_t coarse_tail_attributes() {
-  return cudaFuncSetAttribute(k_coarse_tail, cudaFuncAttributeMaxDynamicSharedMemorySize, kTailSmemBytes);
+  cudaError_t e = cudaFuncSetAttribute(k_coarse_tail, cudaFuncAttributeMaxDynamicSharedMemorySize, kTailSmemBytes);
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(k_coarse_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize, kTailSmemBytes);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(k_coarse_cluster, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+}
+
+static cudaError_t cluster_config(int nb, int smem_bytes, cudaStream_t st, cudaLaunchConfig_t* cfg,
+                                  cudaLaunchAttribute* at) {
+  *cfg = cudaLaunchConfig_t{};
+  cfg->gridDim = dim3(nb);
+  cfg->blockDim = dim3(kClusterTailThreads);
+  cfg->dynamicSmemBytes = (size_t)smem_bytes;
+  cfg->stream = st;
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = nb;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg->attrs = at;
+  cfg->numAttrs = 1;
+  return cudaSuccess;
+}
+
+int coarse_cluster_fits(int nb, int smem_bytes) {
+  cudaLaunchConfig_t cfg;
+  cudaLaunchAttribute at[1];
+  cluster_config(nb, smem_bytes, nullptr, &cfg, at);
+  int n = 0;
+  if (cudaOccupancyMaxActiveClusters(&n, k_coarse_cluster, &cfg) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return n;
+}
+
+cudaError_t launch_coarse_cluster(int nb, const TailLevel* lv, int nlev, const TailOp* ops, int nops,
+                                  unsigned curmask, int smem_bytes, cudaStream_t st) {
+  if (nops <= 0 || nops > kClusterTailMaxOps || nlev > kTailMaxLevels) return cudaErrorInvalidValue;
+  cudaLaunchConfig_t cfg;
+  cudaLaunchAttribute at[1];
+  cluster_config(nb, smem_bytes, st, &cfg, at);
+  return cudaLaunchKernelEx(&cfg, k_coarse_cluster, lv, ops, nops, nlev, curmask);
 }
 
 cudaError_t launch_coarse_tail(const TailLevel* lv, const TailOp* ops, int nops, unsigned curmask, int smem_bytes,

@@ -98,14 +98,16 @@ struct TailLevel {
   const BlkLev* cbl;
   const unsigned long long* cells;   // interior cells, red (x+y+z odd) first
   const unsigned long long* ghosts;  // ghost cells of the padded blocks
-  const uint32_t* fdst;              // sweep fill table, compact indices
-  const uint32_t* fsrc;
+  const uint32_t* fdst;              // sweep fill table, compact indices (cluster tail: own block)
+  const uint32_t* fsrc;              // (cluster tail: source rank << 24 | compact index in its block)
+  const int* fstart;                 // cluster tail: fill entries of block b are fstart[b] .. fstart[b+1]-1
   int nb, nint, nred, nghost, npad, nfill;
   float* phi32[2];
   float* rhs32;
   double* phi64[2];
   double* rhs64;
   int s_phi32, s_rhs32, s_phi64, s_rhs64;
+  int s_cells, s_fill;  // cluster tail: arena offsets of the staged cell tables and this block's fill pairs
 };
 enum TailKind {
   kTailRelax = 0,
@@ -133,6 +135,14 @@ inline unsigned long long tail_cell(long long i, int x, int y, int z, int b) {
 }
 cudaError_t launch_coarse_tail(const TailLevel* lv, const TailOp* ops, int nops, unsigned curmask, int smem_bytes,
                                cudaStream_t st);
+// The same program as one cluster of nb CTAs (nb <= 16), CTA b holding block b
+// of every tail level (all blocks of a level the same size).
+constexpr int kClusterTailThreads = 512;
+constexpr int kClusterTailMaxBlocks = 16;
+int coarse_cluster_fits(int nb, int smem_bytes);  // clusters that can be resident at once (0: none)
+constexpr int kClusterTailMaxOps = 160;
+cudaError_t launch_coarse_cluster(int nb, const TailLevel* lv, int nlev, const TailOp* ops, int nops,
+                                  unsigned curmask, int smem_bytes, cudaStream_t st);
 
 template <typename T>
 cudaError_t launch_relax_small(bool var, const BlkLev* bl, const int* start, int nb, T* phi, const T* rhs,

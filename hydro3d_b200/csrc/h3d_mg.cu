@@ -135,6 +135,9 @@ struct h3d_mg {
   TailOp* d_tail_ops = nullptr;
   unsigned long long* d_tail_cells = nullptr;  // cell tables of all tail levels
   BlkLev* d_tail_cbl = nullptr;                // compact block tables of the tail levels
+  int* d_tail_starts = nullptr;                // cluster tail: per-block fill ranges
+  int tail_cluster = 0;                        // cluster tail: CTAs of the cluster (0: single-CTA tail)
+  int tail_nlev = 0;
   uint32_t* d_tail_fills = nullptr;            // compact sweep fill tables of the tail levels
   int tail_nops = 0;
   int tail_smem = 0;  // dynamic shared memory of the tail launch
@@ -552,7 +555,11 @@ struct Exec {
       mask |= (unsigned)(V.cur32 & 1) << (2 * (g - g0));
       mask |= (unsigned)(V.cur64 & 1) << (2 * (g - g0) + 1);
     }
-    CU(launch_coarse_tail(h->d_tail_lv, h->d_tail_ops, h->tail_nops, mask, h->tail_smem, h->st));
+    if (h->tail_cluster)
+      CU(launch_coarse_cluster(h->tail_cluster, h->d_tail_lv, h->tail_nlev, h->d_tail_ops, h->tail_nops, mask,
+                               h->tail_smem, h->st));
+    else
+      CU(launch_coarse_tail(h->d_tail_lv, h->d_tail_ops, h->tail_nops, mask, h->tail_smem, h->st));
     TRY(chk("coarse tail", g0));
     for (int g = g0; g <= h->L; ++g) {
       L(g).zero32 = h->tail_zero32[g - g0] != 0;
@@ -1213,24 +1220,18 @@ bool plan_tail(const h3d_mg* h, int g0, TailPlan* P) {
 }
 }  // namespace
 
-int build_tail(h3d_mg* h) {
+// The op program of a tail from level g0 (see build_tail); z32 / z64 return
+// the zero flags of every level after it.
+void emit_tail_ops(const h3d_mg* h, int g0, int scratch, std::vector<TailOp>& ops, std::vector<char>& z32,
+                   std::vector<char>& z64) {
   const int Lv = h->L;
-  if (h->var) return H3D_OK;
-  int g0 = Lv + 1;
-  TailPlan plan;
-  for (int g = Lv; g >= 2; --g) {
-    TailPlan P;
-    if (!h->lev[g].tailable || !plan_tail(h, g, &P)) break;
-    g0 = g;
-    plan = P;
-  }
-  if (g0 > Lv - 1 || Lv - g0 + 1 > kTailMaxLevels) return H3D_OK;  // fewer than two tail levels
   const int irestr = h->desc.irestr, iproln = h->desc.iproln, csw = h->desc.coarse_sweeps;
   auto ti = [&](int g) { return g - g0; };
-  std::vector<char> z32(Lv + 2, 0), z64(Lv + 2, 0);
+  z32.assign(Lv + 2, 0);
+  z64.assign(Lv + 2, 0);
   if (f32_level(h, g0)) z32[g0] = 1;
   else z64[g0] = 1;
-  std::vector<TailOp> ops;
+  ops.clear();
   auto op = [&](int kind, bool f64, int fine, int coarse, int sweeps, int zero) {
     ops.push_back(TailOp{kind, f64 ? 1 : 0, ti(fine), ti(coarse), sweeps, zero});
   };
@@ -1272,11 +1273,11 @@ int build_tail(h3d_mg* h) {
         if (z64[gc]) { zero_fill(gc, true); z64[gc] = 0; }
         op(kTailPhiD2F, false, gc, gc, 0, 0);
       }
-      op(kTailProlong, false, gf, gc, plan.scratch, z32[gf]);
+      op(kTailProlong, false, gf, gc, scratch, z32[gf]);
       z32[gf] = 0;
     } else {
       if (z64[gc]) { zero_fill(gc, true); z64[gc] = 0; }
-      op(kTailProlong, true, gf, gc, plan.scratch, z64[gf]);
+      op(kTailProlong, true, gf, gc, scratch, z64[gf]);
       z64[gf] = 0;
     }
   };
@@ -1305,6 +1306,23 @@ int build_tail(h3d_mg* h) {
     }
   }
   for (int q = g0; q <= Lv; ++q) op(kTailStore, false, q, q, 0, 0);
+}
+
+int build_tail(h3d_mg* h) {
+  const int Lv = h->L;
+  if (h->var) return H3D_OK;
+  int g0 = Lv + 1;
+  TailPlan plan;
+  for (int g = Lv; g >= 2; --g) {
+    TailPlan P;
+    if (!h->lev[g].tailable || !plan_tail(h, g, &P)) break;
+    g0 = g;
+    plan = P;
+  }
+  if (g0 > Lv - 1 || Lv - g0 + 1 > kTailMaxLevels) return H3D_OK;  // fewer than two tail levels
+  std::vector<TailOp> ops;
+  std::vector<char> z32, z64;
+  emit_tail_ops(h, g0, plan.scratch, ops, z32, z64);
   // compact layouts, cell tables and fill tables
   std::vector<unsigned long long> cells;
   std::vector<uint32_t> fills;
@@ -1445,6 +1463,201 @@ int build_tail(h3d_mg* h) {
   return H3D_OK;
 }
 
+// The fused coarse tail as one cluster of CTAs, CTA b holding block b of
+// every tail level: the deepest run of levels g..L (g >= 2, at least two
+// levels) whose blocks are all the same size at each level and whose arrays,
+// one block of each level, fit one CTA's shared arena; nb <= 16 blocks;
+// constant coefficients; sweep fills that read interior cells only.
+int build_cluster_tail(h3d_mg* h) {
+  const int Lv = h->L;
+  const int nb = (int)h->blocks.size();
+  if (h->var || nb > kClusterTailMaxBlocks) return H3D_OK;
+  auto al = [](int v) { return (v + 15) & ~15; };
+  struct Lay { int npad, nint, s_phi32, s_rhs32, s_phi64, s_rhs64, s_cells, s_fill; };
+  std::vector<Lay> lay;
+  int g0 = Lv + 1, bytes = 0, scratch_at = 0;
+  for (int g = Lv; g >= 2; --g) {
+    const Level& V = h->lev[g];
+    const BlkLev& B0 = V.geom.bl[0];
+    bool same = true;
+    for (const auto& B : V.geom.bl) same = same && B.nx == B0.nx && B.ny == B0.ny && B.nz == B0.nz;
+    if (!same || B0.nx + 1 > 255 || B0.ny + 1 > 255 || B0.nz + 1 > 255) break;
+    // arena with levels g..L (one block each) plus the ghost scratch of the fine levels
+    std::vector<Lay> L2;
+    int at = 0, scratch = 0;
+    for (int q = g; q <= Lv; ++q) {
+      const BlkLev& Bq = h->lev[q].geom.bl[0];
+      Lay l{};
+      l.npad = (Bq.nx + 2) * (Bq.ny + 2) * (Bq.nz + 2);
+      l.nint = Bq.nx * Bq.ny * Bq.nz;
+      const bool f32 = f32_level(h, q), f64 = !f32 || (h->mixed && q == Lv);
+      l.s_phi32 = l.s_rhs32 = l.s_phi64 = l.s_rhs64 = -1;
+      if (h->mixed) { l.s_phi32 = at; at = al(at + l.npad * 4); l.s_rhs32 = at; at = al(at + l.nint * 4); }
+      if (f64) { l.s_phi64 = at; at = al(at + l.npad * 8); l.s_rhs64 = at; at = al(at + l.nint * 8); }
+      if (q < Lv) scratch = std::max(scratch, (l.npad - l.nint) * (f32 ? 4 : 8));
+      L2.push_back(l);
+    }
+    // staged tables: cell + ghost entries of every level, the largest per-block fill list
+    int tab = al(at + scratch);
+    for (int q = g; q <= Lv; ++q) {
+      const BlkLev& Bq = h->lev[q].geom.bl[0];
+      const int npad = (Bq.nx + 2) * (Bq.ny + 2) * (Bq.nz + 2);
+      L2[q - g].s_cells = tab;
+      tab = al(tab + npad * 8);
+      L2[q - g].s_fill = tab;
+      tab = al(tab + (npad - Bq.nx * Bq.ny * Bq.nz) * 8);  // (dst, src) pairs: a ghost is filled once at most
+    }
+    const int need = tab + 128;
+    if (need > kTailSmemBytes) break;
+    g0 = g;
+    lay = L2;
+    bytes = need;
+    scratch_at = at;
+  }
+  if (g0 > Lv - 1 || Lv - g0 + 1 > kTailMaxLevels) return H3D_OK;
+  if (coarse_cluster_fits(nb, bytes) < 1) return H3D_OK;
+  std::vector<TailOp> ops;
+  std::vector<char> z32, z64;
+  emit_tail_ops(h, g0, scratch_at, ops, z32, z64);
+  // per level: cell tables (block field 0) and per-block fill tables
+  std::vector<unsigned long long> cells;
+  std::vector<uint32_t> fills;
+  std::vector<int> starts;
+  struct At { size_t cells, ghosts, fdst, fsrc, fstart; int nred, nint, nghost; };
+  std::vector<At> at;
+  for (int q = g0; q <= Lv; ++q) {
+    const Level& V = h->lev[q];
+    const BlkLev& B = V.geom.bl[0];
+    const int sx = B.nx + 2, sxy = (B.nx + 2) * (B.ny + 2);
+    At a{};
+    std::vector<unsigned long long> red, black, ghost;
+    for (int z = 0; z <= B.nz + 1; ++z)
+      for (int y = 0; y <= B.ny + 1; ++y)
+        for (int x = 0; x <= B.nx + 1; ++x) {
+          const unsigned long long e = tail_cell((long long)z * sxy + (long long)y * sx + x, x, y, z, 0);
+          const bool gh = x == 0 || y == 0 || z == 0 || x == B.nx + 1 || y == B.ny + 1 || z == B.nz + 1;
+          if (gh) ghost.push_back(e);
+          else if ((x + y + z) & 1) red.push_back(e);
+          else black.push_back(e);
+        }
+    a.cells = cells.size();
+    a.nred = (int)red.size();
+    a.nint = (int)(red.size() + black.size());
+    cells.insert(cells.end(), red.begin(), red.end());
+    cells.insert(cells.end(), black.begin(), black.end());
+    a.ghosts = cells.size();
+    a.nghost = (int)ghost.size();
+    cells.insert(cells.end(), ghost.begin(), ghost.end());
+    std::vector<uint32_t> d, sidx;
+    std::string err;
+    int rc = build_halo_table(h->blocks, q, kHaloSweep, true, d, sidx, &err);
+    if (rc != H3D_OK) return fail(h, rc, err);
+    auto locate = [&](uint32_t gi, int* blk, uint32_t* ci) -> bool {
+      for (size_t b = 0; b < V.geom.bl.size(); ++b) {
+        const BlkLev& G = V.geom.bl[b];
+        const long long lo = G.off, hi = G.off + G.sxy * (G.nz + 2);
+        if ((long long)gi < lo || (long long)gi >= hi) continue;
+        const long long l = (long long)gi - lo;
+        const int z = (int)(l / G.sxy), y = (int)((l % G.sxy) / G.sx), x = (int)(l % G.sx);
+        if (x > G.nx + 1) return false;
+        *blk = (int)b;
+        *ci = (uint32_t)(z * sxy + y * sx + x);
+        return true;
+      }
+      return false;
+    };
+    std::vector<std::vector<std::pair<uint32_t, uint32_t>>> per(nb);
+    for (size_t e = 0; e < d.size(); ++e) {
+      int bd, bs;
+      uint32_t cd, cs;
+      if ((sidx[e] & kOldFlag) || !locate(d[e], &bd, &cd) || !locate(sidx[e] & kIdxMask, &bs, &cs)) return H3D_OK;
+      per[bd].push_back({cd, ((uint32_t)bs << 24) | cs});
+    }
+    a.fstart = starts.size();
+    a.fdst = fills.size();
+    std::vector<uint32_t> fd, fs;
+    int acc = 0;
+    for (int b = 0; b < nb; ++b) {
+      starts.push_back(acc);
+      for (auto& pr : per[b]) { fd.push_back(pr.first); fs.push_back(pr.second); }
+      acc += (int)per[b].size();
+    }
+    starts.push_back(acc);
+    fills.insert(fills.end(), fd.begin(), fd.end());
+    a.fsrc = fills.size();
+    fills.insert(fills.end(), fs.begin(), fs.end());
+    at.push_back(a);
+  }
+  int rc;
+  uint32_t* d_fills = nullptr;
+  int* d_starts = nullptr;
+  if ((rc = dalloc(h, &h->d_tail_cells, cells.size())) != H3D_OK ||
+      (rc = dalloc(h, &d_fills, std::max<size_t>(fills.size(), 1))) != H3D_OK ||
+      (rc = dalloc(h, &d_starts, starts.size())) != H3D_OK)
+    return rc;
+  h->d_tail_fills = d_fills;
+  h->d_tail_starts = d_starts;
+  if (cudaMemcpy(h->d_tail_cells, cells.data(), cells.size() * 8, cudaMemcpyHostToDevice) != cudaSuccess ||
+      (!fills.empty() && cudaMemcpy(d_fills, fills.data(), fills.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess) ||
+      cudaMemcpy(d_starts, starts.data(), starts.size() * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess)
+    return fail(h, H3D_ERR_CUDA, "cluster tail tables");
+  std::vector<TailLevel> lv;
+  for (int q = g0; q <= Lv; ++q) {
+    const Level& V = h->lev[q];
+    const At& a = at[q - g0];
+    const Lay& l = lay[q - g0];
+    TailLevel t{};
+    t.gbl = V.d_bl;
+    t.cbl = nullptr;
+    t.cells = h->d_tail_cells + a.cells;
+    t.ghosts = h->d_tail_cells + a.ghosts;
+    t.fdst = d_fills + a.fdst;
+    t.fsrc = d_fills + a.fsrc;
+    t.fstart = d_starts + a.fstart;
+    t.nb = nb;
+    t.nint = a.nint;
+    t.nred = a.nred;
+    t.nghost = a.nghost;
+    t.npad = l.npad;
+    t.nfill = 0;
+    t.phi32[0] = V.phi32[0];
+    t.phi32[1] = V.phi32[1];
+    t.rhs32 = V.rhs32;
+    t.phi64[0] = V.phi64[0];
+    t.phi64[1] = V.phi64[1];
+    t.rhs64 = V.rhs64;
+    t.s_phi32 = l.s_phi32;
+    t.s_rhs32 = l.s_rhs32;
+    t.s_phi64 = l.s_phi64;
+    t.s_rhs64 = l.s_rhs64;
+    t.s_cells = l.s_cells;
+    t.s_fill = l.s_fill;
+    lv.push_back(t);
+  }
+  // every block's fill list must fit its staged region
+  for (int q = g0; q <= Lv; ++q) {
+    const Lay& l = lay[q - g0];
+    const int cap = l.npad - l.nint;
+    const size_t f0 = at[q - g0].fstart;
+    for (int b = 0; b < nb; ++b)
+      if (starts[f0 + b + 1] - starts[f0 + b] > cap) return H3D_OK;
+  }
+  if ((int)ops.size() > kClusterTailMaxOps) return H3D_OK;
+  if ((rc = dalloc(h, &h->d_tail_lv, lv.size())) != H3D_OK) return rc;
+  if ((rc = dalloc(h, &h->d_tail_ops, ops.size())) != H3D_OK) return rc;
+  if (cudaMemcpy(h->d_tail_lv, lv.data(), lv.size() * sizeof(TailLevel), cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(h->d_tail_ops, ops.data(), ops.size() * sizeof(TailOp), cudaMemcpyHostToDevice) != cudaSuccess)
+    return fail(h, H3D_ERR_CUDA, "cluster tail program");
+  h->tail_nlev = Lv - g0 + 1;
+  h->tail_nops = (int)ops.size();
+  h->tail_smem = bytes;
+  h->tail_zero32.assign(z32.begin() + g0, z32.begin() + Lv + 1);
+  h->tail_zero64.assign(z64.begin() + g0, z64.begin() + Lv + 1);
+  h->tail_g = g0;
+  h->tail_cluster = nb;
+  return H3D_OK;
+}
+
 int h3d_mg_destroy(h3d_mg* h) {
   if (!h) return H3D_OK;
   cudaSetDevice(h->device);
@@ -1474,6 +1687,7 @@ int h3d_mg_destroy(h3d_mg* h) {
   dfree(h->d_tail_cells);
   dfree(h->d_tail_cbl);
   dfree(h->d_tail_fills);
+  dfree(h->d_tail_starts);
   dfree(h->stage[0]);
   dfree(h->stage[1]);
   if (h->h_res) cudaFreeHost(h->h_res);
@@ -1660,7 +1874,8 @@ int h3d_mg_create(h3d_mg** out, const h3d_mg_desc* desc) {
     V.sweep_bytes = (double)V.geom.n_interior * w * (3.0 + (h->var ? 3.0 : 0.0));
     V.sweep_bytes_zero = (double)V.geom.n_interior * w * (2.0 + (h->var ? 3.0 : 0.0));
   }
-  if ((rc = build_tail(h)) != H3D_OK) return bail(rc);
+  if ((rc = build_cluster_tail(h)) != H3D_OK) return bail(rc);
+  if (!h->tail_g && (rc = build_tail(h)) != H3D_OK) return bail(rc);
   const size_t n1 = (size_t)h->lev[1].geom.n_elems;
   if ((rc = dalloc(h, &h->p64[0], n1)) || (rc = dalloc(h, &h->p64[1], n1)) || (rc = dalloc(h, &h->b64, n1)))
     return bail(rc);
