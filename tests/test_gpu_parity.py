@@ -18,6 +18,8 @@ LAYOUTS = [
     ((2, 2, 2), (8, 16, 8), [P, P, W, W, W, W], 3),
     ((3, 2, 2), (16, 8, 8), [W, W, P, P, W, W], 2),
     ((2, 1, 3), (8, 8, 16), [P] * 6, 3),
+    # more blocks than one thread-block cluster holds: the single-CTA coarse tail
+    ((3, 3, 2), (8, 8, 8), [P, P, W, W, W, W], 3),
 ]
 FP32_RTOL = 2e-5
 
@@ -147,6 +149,29 @@ def test_fp32_kernels_close(oracle_mod, h3d):
     _rand_level(rng, s, orc, 1)
     s.mgrestr(2); orc.mgrestr(2)
     _assert_level(s, orc, 2, "rhs", exact=False)
+    s.close()
+
+
+@pytest.mark.parametrize("layout", [((4, 2, 2), (16, 16, 16), [P, P, W, W, W, W], 4),
+                                    ((3, 3, 2), (8, 8, 8), [W, W, P, P, W, W], 3)])
+def test_mixed_vcycle_coarse_tails(oracle_mod, h3d, layout):
+    """Mixed-precision V-cycles whose coarse levels run fused: 16 equal blocks
+    (one thread-block cluster) and 18 blocks (one CTA), against the FP64
+    oracle V-cycle; tolerance 1e-4 of the largest value.  Coarse levels are
+    read back too (the fused tail stores them)."""
+    blocks, s, orc = _pair(oracle_mod, h3d, layout, precision="mixed")
+    s.coeff(); orc.coeff()
+    rng = np.random.default_rng(31)
+    _rand_level(rng, s, orc, 1)
+    for _ in range(2):
+        s.vcycle(); orc.vcycle()
+        for ib in range(len(blocks)):
+            a, b = s.get_level(1, "phi", ib), orc.get_phi(1, ib)
+            np.testing.assert_allclose(a, b, rtol=0, atol=1e-4 * np.abs(b).max())
+    g = layout[3]
+    for ib in range(len(blocks)):
+        a, b = s.get_level(g - 1, "rhs", ib), orc.get_rhs(g - 1, ib)
+        np.testing.assert_allclose(a, b, rtol=0, atol=1e-4 * np.abs(b).max())
     s.close()
 
 
