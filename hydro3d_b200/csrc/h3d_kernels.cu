@@ -1474,7 +1474,8 @@ __global__ void __launch_bounds__(TPR*(TY + 2)) k_rbgs_win(const BlkLev* __restr
                                                           const Tile* __restrict__ tiles, int zc,
                                                           const CUtensorMap* __restrict__ maps,
                                                           const CUtensorMap* __restrict__ rmaps,
-                                                          float* __restrict__ dst, int* err) {
+                                                          float* __restrict__ dst, int* err,
+                                                          const long long* __restrict__ push) {
   pdl_trigger();
   using C = VecCfg<TPR, GPT, TY, NS, D>;
   static_assert(TPR <= 32 && (TPR & (TPR - 1)) == 0, "a row is a power-of-two lane segment of one warp");
@@ -1516,6 +1517,12 @@ __global__ void __launch_bounds__(TPR*(TY + 2)) k_rbgs_win(const BlkLev* __restr
   float* __restrict__ Drow = dst + B.off + (long long)y * B.sx;
   const bool leader = threadIdx.x == 0;
   bool bad = false;
+  // ghost pushes: face f (W, E, S, N, B, T) of this block is the source of a
+  // whole ghost face; its new values are also stored at their own address +
+  // pd[f] (kNoPush: none), so the fill after the sweep skips those faces
+  long long pd[6];
+#pragma unroll
+  for (int f = 0; f < 6; ++f) pd[f] = push ? __ldg(push + 6 * t.b + f) : kNoPush;
 
   // constant coefficients (mgsolver.for:186-205): walls zero the face term
   const int ph = B.phys;
@@ -1690,7 +1697,14 @@ __global__ void __launch_bounds__(TPR*(TY + 2)) k_rbgs_win(const BlkLev* __restr
           if (rgt[k]) br[k] = 0.f;
         }
         H3D_WIN_COLOUR(m2[k], m3[k], m1[k], u, dn, h, bl[k], br[k], zb, !q1, k);
-        *reinterpret_cast<float4*>(Drow + dz + x0[k]) = m2[k];
+        float* o = Drow + dz + x0[k];
+        *reinterpret_cast<float4*>(o) = m2[k];
+        if (lft[k] && pd[0] != kNoPush) o[pd[0]] = m2[k].x;
+        if (rgt[k] && pd[1] != kNoPush) o[3 + pd[1]] = m2[k].w;
+        if (y == 1 && pd[2] != kNoPush) *reinterpret_cast<float4*>(o + pd[2]) = m2[k];
+        if (y == ny && pd[3] != kNoPush) *reinterpret_cast<float4*>(o + pd[3]) = m2[k];
+        if (zb == 1 && pd[4] != kNoPush) *reinterpret_cast<float4*>(o + pd[4]) = m2[k];
+        if (zb == nz && pd[5] != kNoPush) *reinterpret_cast<float4*>(o + pd[5]) = m2[k];
       }
     }
     // this phase's shared-memory writes are ordered before the TMA that reuses their slot
@@ -1738,16 +1752,16 @@ static cudaError_t win_attr() {
 template <int TPR, int GPT, int TY, int NS, int D, int U>
 static cudaError_t win_dispatch(bool zero, const BlkLev* bl, const Tile* tiles, int ntiles, int zc,
                                 const CUtensorMap* maps, const CUtensorMap* rmaps, int* err, float* dst,
-                                cudaStream_t st) {
+                                const long long* push, cudaStream_t st) {
   static_assert(D + 3 <= NS, "a plane is read until two phases after its own");
   if (ntiles <= 0) return cudaSuccess;
   constexpr size_t SM = VecCfg<TPR, GPT, TY, NS, D>::SMEM;
   if (zero)
     pdl_launch(k_rbgs_win<TPR, GPT, TY, NS, D, true, U>, ntiles, TPR * (TY + 2), SM, st, bl, tiles, zc, maps, rmaps,
-               dst, err);
+               dst, err, push);
   else
     pdl_launch(k_rbgs_win<TPR, GPT, TY, NS, D, false, U>, ntiles, TPR * (TY + 2), SM, st, bl, tiles, zc, maps, rmaps,
-               dst, err);
+               dst, err, push);
   return cudaGetLastError();
 }
 
@@ -1832,10 +1846,16 @@ cudaError_t init_kernel_attributes() {
 
 
 
+bool rbgs_pushes(int variant, bool var, bool f32) {
+  return f32 && !var && variant >= kFirstWinShape && variant < num_tile_shapes();
+}
+
 template <typename T>
 cudaError_t launch_rbgs(int variant, bool var, bool zero_src, const BlkLev* bl, const Tile* tiles, int ntiles,
                         int zc, const CUtensorMap* maps, const CUtensorMap* rmaps, int* err, const T* src, T* dst,
-                        const T* rhs, const T* fx, const T* fy, const T* fz, cudaStream_t st) {
+                        const T* rhs, const T* fx, const T* fy, const T* fz, const long long* push, cudaStream_t st) {
+  // ghost pushes need the register-window sweep to run as asked
+  if (push && (!rbgs_pushes(variant, var, sizeof(T) == 4) || !maps || !rmaps)) return cudaErrorInvalidValue;
   if (variant >= 0 && variant < num_tile_shapes() && kShapes[variant].tma) {
     // nothing to stage from a zero source: the equivalent plain-load kernel zero-fills;
     // the vectorised sweep is FP32 with constant coefficients only
@@ -1852,7 +1872,7 @@ cudaError_t launch_rbgs(int variant, bool var, bool zero_src, const BlkLev* bl, 
       H3D_VEC_SHAPES(X)
 #undef X
 #define X(v, tpr, gpt, ty, ns, d, u) \
-      case v: return win_dispatch<tpr, gpt, ty, ns, d, u>(zero_src, bl, tiles, ntiles, zc, maps, rmaps, err, reinterpret_cast<float*>(dst), st);
+      case v: return win_dispatch<tpr, gpt, ty, ns, d, u>(zero_src, bl, tiles, ntiles, zc, maps, rmaps, err, reinterpret_cast<float*>(dst), push, st);
       H3D_WIN_SHAPES(X)
 #undef X
       default: break;
@@ -2453,7 +2473,7 @@ cudaError_t launch_restrict(bool var, bool zero_phi, const BlkLev* fine, const B
 // and 1 take the ghost columns.  Same interpolation, term order and mgbound
 // source as k_prolong_pairs.  Needs nx a multiple of VEC and ny, nz even.
 template <typename T, bool ZERO_OLD>
-__global__ void __launch_bounds__(256) k_prolong_vec(const BlkLev* __restrict__ fine, const BlkLev* __restrict__ coarse,
+__global__ void __launch_bounds__(256, 3) k_prolong_vec(const BlkLev* __restrict__ fine, const BlkLev* __restrict__ coarse,
                                                      const Tile* __restrict__ tiles, const T* __restrict__ phi_c,
                                                      const T* __restrict__ old, T* __restrict__ out) {
   pdl_trigger();
@@ -3331,10 +3351,10 @@ cudaError_t launch_face_coef(const BlkLev* bl, CellTab ct, const double* dens, c
 // explicit instantiations
 template cudaError_t launch_rbgs<double>(int, bool, bool, const BlkLev*, const Tile*, int, int, const CUtensorMap*,
                                          const CUtensorMap*, int*, const double*, double*, const double*, const double*, const double*,
-                                         const double*, cudaStream_t);
+                                         const double*, const long long*, cudaStream_t);
 template cudaError_t launch_rbgs<float>(int, bool, bool, const BlkLev*, const Tile*, int, int, const CUtensorMap*,
                                         const CUtensorMap*, int*, const float*, float*, const float*, const float*, const float*,
-                                        const float*, cudaStream_t);
+                                        const float*, const long long*, cudaStream_t);
 template cudaError_t launch_fill<double>(const uint32_t*, const uint32_t*, int64_t, double*, const double*,
                                          const double*, bool, cudaStream_t);
 template cudaError_t launch_fill<float>(const uint32_t*, const uint32_t*, int64_t, float*, const float*, const float*,

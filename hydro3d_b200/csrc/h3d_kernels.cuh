@@ -76,12 +76,17 @@ TileShape tile_shape(int variant);
 // maps: tensor maps of src for every block (TMA variants); rmaps: tensor maps
 // of rhs (variants that stage it); err: device flag set when a bounded wait
 // gives up.
+// push: per block, six element offsets (faces W, E, S, N, B, T; kNoPush: none)
+// from a face cell to the ghost cell it is the source of; the register-window
+// sweeps store their new face values there too (others reject a push table).
+constexpr long long kNoPush = (long long)(~0ull >> 1);
+bool rbgs_pushes(int variant, bool var, bool f32);
 template <typename T>
 cudaError_t launch_rbgs(int variant, bool var, bool zero_src, const BlkLev* bl, const Tile* tiles,
                         int ntiles, int zc, const CUtensorMap* maps, const CUtensorMap* rmaps, int* err,
                         const T* src, T* dst,
                         const T* rhs, const T* fx, const T* fy,
-                        const T* fz, cudaStream_t st);
+                        const T* fz, const long long* push, cudaStream_t st);
 
 constexpr int kSmallLevelBlocks = 64;  // block descriptors the fused small-level kernel caches
 // `sweeps` red-black sweeps of a small level, each followed by its ghost fill,

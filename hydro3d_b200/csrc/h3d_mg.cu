@@ -64,6 +64,9 @@ struct Level {
   float *fx32 = nullptr, *fy32 = nullptr, *fz32 = nullptr;
   double* dens = nullptr;
   Halo sweep, faces, exch, bound;
+  Halo sweep_push;              // the sweep fill without the faces the register-window sweeps push
+  long long* d_push = nullptr;  // per block, six ghost push offsets (kNoPush: none)
+  bool push_ok = false;
   CUtensorMap* d_maps = nullptr;  // [ty index][0,1: iterate buffer, 2: rhs][block] tensor maps
   CUtensorMap* d_rmaps = nullptr;  // as the fine level of a restriction: [tyc index][0,1: iterate, 2: rhs][block]
   Tile* d_rtiles = nullptr;       // restriction tiles (this level as the coarse level)
@@ -411,12 +414,14 @@ struct Exec {
     if (mixed_level(g)) {
       float* src = V.phi32[V.cur32];
       float* dst = V.phi32[1 - V.cur32];
+      const bool push = V.push_ok && rbgs_pushes(V.variant, h->var, true);
       CU(launch_rbgs<float>(V.variant, h->var, V.zero32, V.d_bl, V.d_tiles, V.ntiles, V.zc, sweep_maps(V, V.cur32),
                             rhs_maps(V), h->d_err, src, dst, V.rhs32,
-                            V.fx32, V.fy32, V.fz32, st));
+                            V.fx32, V.fy32, V.fz32, push ? V.d_push : nullptr, st));
       TRY(chk("sweep fp32", g));
       if (e1) CU(record(e1));
-      CU(launch_fill<float>(V.sweep.d_dst, V.sweep.d_src, V.sweep.n, dst, dst, src, V.zero32, st));
+      const Halo& fill = push ? V.sweep_push : V.sweep;
+      CU(launch_fill<float>(fill.d_dst, fill.d_src, fill.n, dst, dst, src, V.zero32, st));
       TRY(chk("fill fp32", g));
       V.cur32 = 1 - V.cur32;
       V.zero32 = false;
@@ -425,7 +430,7 @@ struct Exec {
       double* dst = V.phi64[1 - V.cur64];
       CU(launch_rbgs<double>(V.variant, h->var, V.zero64, V.d_bl, V.d_tiles, V.ntiles, V.zc, sweep_maps(V, V.cur64),
                              rhs_maps(V), h->d_err, src, dst, V.rhs64,
-                             V.fx64, V.fy64, V.fz64, st));
+                             V.fx64, V.fy64, V.fz64, nullptr, st));
       TRY(chk("sweep fp64", g));
       if (e1) CU(record(e1));
       CU(launch_fill<double>(V.sweep.d_dst, V.sweep.d_src, V.sweep.n, dst, dst, src, V.zero64, st));
@@ -988,12 +993,13 @@ int autotune_level(h3d_mg* h, int g) {
         const bool zero = rep >= 6;
         TRY(flush_l2(h));
         CU(cudaEventRecord(a, h->st));
+        const long long* push = (f32 && V.push_ok && rbgs_pushes(v, h->var, true)) ? V.d_push : nullptr;
         if (f32) CU(launch_rbgs<float>(v, h->var, zero, V.d_bl, V.d_tiles, V.ntiles, zc, sweep_maps(V, V.cur32),
                                        rhs_maps(V), h->d_err, V.phi32[V.cur32],
-                                       V.phi32[1 - V.cur32], V.rhs32, V.fx32, V.fy32, V.fz32, h->st));
+                                       V.phi32[1 - V.cur32], V.rhs32, V.fx32, V.fy32, V.fz32, push, h->st));
         else CU(launch_rbgs<double>(v, h->var, zero, V.d_bl, V.d_tiles, V.ntiles, zc, sweep_maps(V, V.cur64),
                                     rhs_maps(V), h->d_err, V.phi64[V.cur64],
-                                    V.phi64[1 - V.cur64], V.rhs64, V.fx64, V.fy64, V.fz64, h->st));
+                                    V.phi64[1 - V.cur64], V.rhs64, V.fx64, V.fy64, V.fz64, nullptr, h->st));
         CU(cudaEventRecord(b, h->st));
         {
           cudaError_t e = cudaEventSynchronize(b);
@@ -1180,6 +1186,93 @@ int h3d_topology(int32_t nblocks, const int32_t* ext, const int32_t* bc, const d
       }
     }
   }
+  return H3D_OK;
+}
+
+// Ghost pushes of a level: a whole face of ghost cells of block bd whose
+// sweep-fill sources are, cell for cell, the adjacent face of interior cells
+// of one block bs (same pitches) is written by bs's register-window sweep
+// (an element offset from each source cell to its ghost), and left out of
+// the fill table.  Faces with any other source pattern stay in the table.
+int build_push(h3d_mg* h, Level& V, const std::vector<uint32_t>& d, const std::vector<uint32_t>& s) {
+  const auto& G = V.geom;
+  const int nb = (int)G.bl.size();
+  auto locate = [&](uint32_t gi, int* b, int* x, int* y, int* z) -> bool {
+    for (int q = 0; q < nb; ++q) {
+      const BlkLev& B = G.bl[q];
+      const long long lo = B.off, hi = B.off + B.sxy * (B.nz + 2);
+      if ((long long)gi < lo || (long long)gi >= hi) continue;
+      const long long l = (long long)gi - lo;
+      *z = (int)(l / B.sxy);
+      *y = (int)((l % B.sxy) / B.sx);
+      *x = (int)(l % B.sx);
+      *b = q;
+      return *x <= B.nx + 1;
+    }
+    return false;
+  };
+  struct Face { int bs = -2, side = -1, cnt = 0; bool bad = false; };
+  std::vector<Face> face(nb * 6);
+  std::vector<int> efac(d.size(), -1);
+  for (size_t e = 0; e < d.size(); ++e) {
+    int bd, x, y, z;
+    if (!locate(d[e], &bd, &x, &y, &z)) continue;
+    const BlkLev& D = G.bl[bd];
+    const int out = (x == 0 || x == D.nx + 1) + (y == 0 || y == D.ny + 1) + (z == 0 || z == D.nz + 1);
+    if (out != 1) continue;
+    const int f = x == 0 ? 0 : x == D.nx + 1 ? 1 : y == 0 ? 2 : y == D.ny + 1 ? 3 : z == 0 ? 4 : 5;
+    Face& F = face[bd * 6 + f];
+    efac[e] = bd * 6 + f;
+    F.cnt++;
+    int bs, xs, ys, zs;
+    if ((s[e] & kOldFlag) || !locate(s[e] & kIdxMask, &bs, &xs, &ys, &zs)) { F.bad = true; continue; }
+    const BlkLev& S = G.bl[bs];
+    int side = -1;
+    if (f < 2) {
+      if (ys == y && zs == z && S.nx > 1) side = xs == 1 ? 0 : xs == S.nx ? 1 : -1;
+    } else if (f < 4) {
+      if (xs == x && zs == z && S.ny > 1) side = ys == 1 ? 2 : ys == S.ny ? 3 : -1;
+    } else {
+      if (xs == x && ys == y && S.nz > 1) side = zs == 1 ? 4 : zs == S.nz ? 5 : -1;
+    }
+    if (side < 0) { F.bad = true; continue; }
+    if (F.bs == -2) { F.bs = bs; F.side = side; }
+    else if (F.bs != bs || F.side != side) F.bad = true;
+  }
+  std::vector<long long> delta(nb * 6, kNoPush);
+  std::vector<char> pushed(nb * 6, 0);
+  for (int bd = 0; bd < nb; ++bd)
+    for (int f = 0; f < 6; ++f) {
+      const Face& F = face[bd * 6 + f];
+      const BlkLev& D = G.bl[bd];
+      const long long area = f < 2 ? (long long)D.ny * D.nz : f < 4 ? (long long)D.nx * D.nz : (long long)D.nx * D.ny;
+      if (F.bad || F.bs < 0 || F.cnt != area) continue;
+      const BlkLev& S = G.bl[F.bs];
+      if (S.sx != D.sx || S.sxy != D.sxy) continue;
+      long long& dl = delta[F.bs * 6 + F.side];
+      if (dl != kNoPush) continue;  // the source face already feeds another ghost face
+      const long long base = D.off - S.off;
+      const int g = (f & 1) ? (f < 2 ? D.nx + 1 : f < 4 ? D.ny + 1 : D.nz + 1) : 0;  // ghost coordinate
+      switch (F.side) {
+        case 0: dl = base + (g - 1); break;
+        case 1: dl = base + (g - S.nx); break;
+        case 2: dl = base + (long long)(g - 1) * D.sx; break;
+        case 3: dl = base + (long long)(g - S.ny) * D.sx; break;
+        case 4: dl = base + (long long)(g - 1) * D.sxy; break;
+        default: dl = base + (long long)(g - S.nz) * D.sxy; break;
+      }
+      pushed[bd * 6 + f] = 1;
+    }
+  std::vector<uint32_t> rd, rs;
+  for (size_t e = 0; e < d.size(); ++e)
+    if (efac[e] < 0 || !pushed[efac[e]]) {
+      rd.push_back(d[e]);
+      rs.push_back(s[e]);
+    }
+  TRY(dalloc(h, &V.d_push, delta.size()));
+  CU(cudaMemcpy(V.d_push, delta.data(), delta.size() * sizeof(long long), cudaMemcpyHostToDevice));
+  TRY(upload_halo(h, V.sweep_push, rd, rs));
+  V.push_ok = true;
   return H3D_OK;
 }
 
@@ -1672,7 +1765,7 @@ int h3d_mg_destroy(h3d_mg* h) {
     void* ps[] = {V.d_bl, V.d_cta_all, V.d_cta_int, V.d_rows_all, V.d_rows_int, V.d_tiles, V.phi64[0], V.phi64[1], V.rhs64, V.phi32[0],
                   V.phi32[1], V.rhs32, V.fx64, V.fy64, V.fz64, V.fx32, V.fy32, V.fz32, V.dens,
                   V.sweep.d_dst, V.sweep.d_src, V.faces.d_dst, V.faces.d_src, V.exch.d_dst, V.exch.d_src,
-                  V.bound.d_dst, V.bound.d_src, V.d_maps, V.d_rmaps, V.d_rtiles, V.d_ptiles, V.d_qtiles, V.d_dtiles, V.d_cstart};
+                  V.bound.d_dst, V.bound.d_src, V.sweep_push.d_dst, V.sweep_push.d_src, V.d_push, V.d_maps, V.d_rmaps, V.d_rtiles, V.d_ptiles, V.d_qtiles, V.d_dtiles, V.d_cstart};
     for (void* p : ps) dfree(p);
   }
   dfree(h->p64[0]);
@@ -1791,6 +1884,7 @@ int h3d_mg_create(h3d_mg** out, const h3d_mg_desc* desc) {
     std::string err;
     if ((rc = build_halo_table(h->blocks, g, kHaloSweep, true, d, s, &err)) != H3D_OK) return bail(fail(h, rc, err));
     if ((rc = upload_halo(h, V.sweep, d, s)) != H3D_OK) return bail(rc);
+    if (f32_level(h, g) && !h->var && (rc = build_push(h, V, d, s)) != H3D_OK) return bail(rc);
     // small levels relax in one fused launch when their fill reads interior cells only;
     // slightly larger ones can still join the fused coarse tail
     if (g > 1 && V.geom.n_interior <= kTailLevelCells && V.geom.bl.size() <= (size_t)kSmallLevelBlocks) {
