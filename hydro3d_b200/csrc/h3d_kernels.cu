@@ -1173,18 +1173,20 @@ __global__ void __launch_bounds__(1024) k_reduce4(const double* __restrict__ par
   block_reduce4<1024>(a0, a1, a2, a3, out);
 }
 
-__global__ void __launch_bounds__(256) k_sum_interior(const BlkLev* __restrict__ bls, const int* __restrict__ cta_start,
-                                                      int nb, const double* __restrict__ a,
+// Sum of a field over the interior cells: a warp a row at a time (grid-stride
+// over the level's interior rows), one partial sum per CTA in a fixed order.
+__global__ void __launch_bounds__(256) k_sum_interior(const BlkLev* __restrict__ bls, const int* __restrict__ row_start,
+                                                      int nb, int nrows, const double* __restrict__ a,
                                                       double* __restrict__ partials) {
   pdl_trigger();
   pdl_wait();
-  const int b = find_block(cta_start, nb, blockIdx.x);
-  const BlkLev B = bls[b];
-  const int local = (blockIdx.x - cta_start[b]) * blockDim.x + threadIdx.x;
+  const int lane = threadIdx.x & 31;
   double s = 0;
-  if (local < B.nx * B.ny * B.nz) {
-    const int x = local % B.nx + 1, y = (local / B.nx) % B.ny + 1, z = local / (B.nx * B.ny) + 1;
-    s = a[B.off + (long long)z * B.sxy + (long long)y * B.sx + x];
+  for (int rid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; rid < nrows; rid += (gridDim.x * blockDim.x) >> 5) {
+    const RowRef rr = row_of(bls, row_start, nb, rid, true);
+    const BlkLev& B = bls[rr.b];
+    const double* row = a + B.off + (long long)rr.z * B.sxy + (long long)rr.y * B.sx;
+    for (int x = 1 + lane; x <= B.nx; x += 32) s += row[x];
   }
   block_reduce4<256>(s, 0.0, 0.0, 0.0, partials + 4 * (size_t)blockIdx.x);
 }
@@ -3314,9 +3316,13 @@ cudaError_t launch_reduce4(const double* partials, int n, double* out, cudaStrea
   return cudaGetLastError();
 }
 
-cudaError_t launch_sum_interior(const BlkLev* bl, CellTab ct, const double* a, double* partials, cudaStream_t st) {
-  if (ct.ncta <= 0) return cudaSuccess;
-  pdl_launch(k_sum_interior, ct.ncta, 256, 0, st, bl, ct.cta_start, ct.nb, a, partials);
+cudaError_t launch_sum_interior(const BlkLev* bl, RowTab rt, const double* a, double* partials, int* nparts,
+                                cudaStream_t st) {
+  *nparts = 0;
+  if (rt.nrows <= 0) return cudaSuccess;
+  const int g = defect_grid(rt.nrows);
+  pdl_launch(k_sum_interior, g, 256, 0, st, bl, rt.start, rt.nb, rt.nrows, a, partials);
+  *nparts = g;
   return cudaGetLastError();
 }
 

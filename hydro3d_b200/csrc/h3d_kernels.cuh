@@ -207,7 +207,7 @@ cudaError_t launch_defect(bool var, const BlkLev* bl, RowTab rt, const double* p
 cudaError_t launch_reduce4(const double* partials, int n, double* out, cudaStream_t st);
 
 // Interior sum of a level-1 field (per-CTA partials, reduce with launch_reduce4).
-cudaError_t launch_sum_interior(const BlkLev* bl, CellTab ct, const double* a, double* partials,
+cudaError_t launch_sum_interior(const BlkLev* bl, RowTab rt, const double* a, double* partials, int* nparts,
                                 cudaStream_t st);
 // a -= s on every cell (incl. ghosts); s read from device memory.
 cudaError_t launch_shift(double* a, int64_t n, const double* s, double scale, cudaStream_t st);

@@ -2111,10 +2111,11 @@ int h3d_mg_solve_resident(h3d_mg* h, const h3d_solve_opts* opts, h3d_solve_info*
   if (h->mixed && is_all_neumann(h)) {
     // FP64 null-space handling: the compatible part of b has zero mean; the
     // FP32 cycles see the defect with the mean of b removed.
-    CellTab ct{V.d_cta_int, (int)V.geom.bl.size(), V.ncta_int};
-    CU(launch_sum_interior(V.d_bl, ct, h->b64, h->partials, h->st));
+    RowTab rt{V.d_rows_int, (int)V.geom.bl.size(), V.nrows_int};
+    int np = 0;
+    CU(launch_sum_interior(V.d_bl, rt, h->b64, h->partials, &np, h->st));
     TRY(ex.chk("sum b", 1));
-    CU(launch_reduce4(h->partials, ct.ncta, h->d_res, h->st));
+    CU(launch_reduce4(h->partials, np, h->d_res, h->st));
     TRY(ex.chk("reduce sum b", 1));
     CU(cudaMemcpyAsync(h->h_res, h->d_res, 4 * sizeof(double), cudaMemcpyDeviceToHost, h->st));
     CU(cudaStreamSynchronize(h->st));
@@ -2144,9 +2145,10 @@ int h3d_mg_solve_resident(h3d_mg* h, const h3d_solve_opts* opts, h3d_solve_info*
     if (opts->stop_rule == 1 && rinf < opts->tol && iter > 1) status = 0;  // newsolv_mg.for:57
   }
   if (opts->remove_mean) {
-    CellTab ct{V.d_cta_int, (int)V.geom.bl.size(), V.ncta_int};
-    CU(launch_sum_interior(V.d_bl, ct, h->p64[h->pc], h->partials, h->st));
-    CU(launch_reduce4(h->partials, ct.ncta, h->d_res, h->st));
+    RowTab rt{V.d_rows_int, (int)V.geom.bl.size(), V.nrows_int};
+    int np = 0;
+    CU(launch_sum_interior(V.d_bl, rt, h->p64[h->pc], h->partials, &np, h->st));
+    CU(launch_reduce4(h->partials, np, h->d_res, h->st));
     CU(launch_shift(h->p64[h->pc], V.geom.n_elems, h->d_res, 1.0 / (double)V.geom.n_interior, h->st));
     h->kernels += 3;
   }
