@@ -1525,6 +1525,17 @@ __global__ void __launch_bounds__(TPR*(TY + 2)) k_rbgs_win(const BlkLev* __restr
   long long pd[6];
 #pragma unroll
   for (int f = 0; f < 6; ++f) pd[f] = push ? __ldg(push + 6 * t.b + f) : kNoPush;
+  // which pushes this thread does: x faces at the row ends (every row), y faces
+  // on the block's first and last rows (loop invariant), z faces on the
+  // first and last planes (decided per plane, uniform over the CTA)
+  bool pxw[GPT], pxe[GPT];
+#pragma unroll
+  for (int k = 0; k < GPT; ++k) {
+    pxw[k] = lft[k] && pd[0] != kNoPush;
+    pxe[k] = rgt[k] && pd[1] != kNoPush;
+  }
+  const bool pys = y == 1 && pd[2] != kNoPush, pyn = y == ny && pd[3] != kNoPush;
+  const bool pzb = pd[4] != kNoPush, pzt = pd[5] != kNoPush;
 
   // constant coefficients (mgsolver.for:186-205): walls zero the face term
   const int ph = B.phys;
@@ -1701,12 +1712,15 @@ __global__ void __launch_bounds__(TPR*(TY + 2)) k_rbgs_win(const BlkLev* __restr
         H3D_WIN_COLOUR(m2[k], m3[k], m1[k], u, dn, h, bl[k], br[k], zb, !q1, k);
         float* o = Drow + dz + x0[k];
         *reinterpret_cast<float4*>(o) = m2[k];
-        if (lft[k] && pd[0] != kNoPush) o[pd[0]] = m2[k].x;
-        if (rgt[k] && pd[1] != kNoPush) o[3 + pd[1]] = m2[k].w;
-        if (y == 1 && pd[2] != kNoPush) *reinterpret_cast<float4*>(o + pd[2]) = m2[k];
-        if (y == ny && pd[3] != kNoPush) *reinterpret_cast<float4*>(o + pd[3]) = m2[k];
-        if (zb == 1 && pd[4] != kNoPush) *reinterpret_cast<float4*>(o + pd[4]) = m2[k];
-        if (zb == nz && pd[5] != kNoPush) *reinterpret_cast<float4*>(o + pd[5]) = m2[k];
+        if (pxw[k]) o[pd[0]] = m2[k].x;
+        if (pxe[k]) o[3 + pd[1]] = m2[k].w;
+        const bool pz = (zb == 1 && pzb) || (zb == nz && pzt);
+        if (__builtin_expect(pys || pyn || pz, 0)) {  // rare: two rows and two planes of a block
+          if (pys) *reinterpret_cast<float4*>(o + pd[2]) = m2[k];
+          if (pyn) *reinterpret_cast<float4*>(o + pd[3]) = m2[k];
+          if (zb == 1 && pzb) *reinterpret_cast<float4*>(o + pd[4]) = m2[k];
+          if (zb == nz && pzt) *reinterpret_cast<float4*>(o + pd[5]) = m2[k];
+        }
       }
     }
     // this phase's shared-memory writes are ordered before the TMA that reuses their slot
