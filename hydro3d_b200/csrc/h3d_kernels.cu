@@ -761,7 +761,11 @@ __global__ void __launch_bounds__(TPR*(TY + 2)) k_rbgs_vec(const BlkLev* __restr
   wait_plane(zlo - 1);
   wait_plane(zlo);
   int s0 = slot_of(zlo);  // slot of plane z
-  auto wrap = [](int i) { return i < 0 ? i + NS : (i >= NS ? i - NS : i); };
+  // ring slot of i in [-NS, 2 NS): a mask when the ring is a power of two
+  auto wrap = [](int i) {
+    if constexpr ((NS & (NS - 1)) == 0) return i & (NS - 1);
+    else return i < 0 ? i + NS : (i >= NS ? i - NS : i);
+  };
   for (int z = zlo; z <= ze + 2; ++z) {
     const bool red = z <= zhi && yin;                    // red cells of plane z
     const int zb = z - 2;
@@ -1599,7 +1603,11 @@ __global__ void __launch_bounds__(TPR*(TY + 2)) k_rbgs_win(const BlkLev* __restr
     const uint32_t parity = ((unsigned)(z - zlo + 1) / (unsigned)NS) & 1u;
     mbar_wait(smem_u32(bars + sl), parity, err, bad);
   };
-  auto wrap = [](int i) { return i < 0 ? i + NS : (i >= NS ? i - NS : i); };
+  // ring slot of i in [-NS, 2 NS): a mask when the ring is a power of two
+  auto wrap = [](int i) {
+    if constexpr ((NS & (NS - 1)) == 0) return i & (NS - 1);
+    else return i < 0 ? i + NS : (i >= NS ? i - NS : i);
+  };
   // Cells of colour q1 (positions q1, q1+2) of group k (c) in plane z, with
   // the group below (bz) and above (tz), rows y-1 (u) and y+1 (dn), rhs rh,
   // and the cells left (l) and right (r) of the group.  Planes off the walls
