@@ -73,3 +73,44 @@ def test_uneven_face_neighbours_rejected(h3d):
     ext = np.array([[0, 8, 0, 8, 0, 8], [8, 16, 0, 4, 0, 8]])
     blocks = h3d.topology.from_extents(ext, [W] * 6, [0.1] * 3, 2)
     assert blocks[0].nb_face[1] == -1 and blocks[1].nb_face[0] == -1
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_sweep_face_ghosts_are_pushable(h3d, case):
+    """The register-window sweeps write whole ghost faces themselves (ghost
+    pushes): a face qualifies when every one of its ghosts is filled from the
+    adjacent interior face of one block, cell for cell.  On these regular
+    layouts every face ghost does (walls from the block itself, neighbours and
+    periodic partners from the facing block), so only edges and corners are
+    left to the gather."""
+    nblk, n, bc, ngrid, g = case
+    blocks = h3d.topology.block_grid(nblk, n, bc, [1 / 16.0] * 3, ngrid)
+    s = 2 ** (g - 1)
+    dims = [(d.n[0] // s, d.n[1] // s, d.n[2] // s) for d in blocks]
+    starts = np.cumsum([0] + [(x + 2) * (y + 2) * (z + 2) for x, y, z in dims])
+
+    def locate(i):
+        b = int(np.searchsorted(starts, i, side="right") - 1)
+        nx, ny, _ = dims[b]
+        l = i - starts[b]
+        return b, l % (nx + 2), (l // (nx + 2)) % (ny + 2), l // ((nx + 2) * (ny + 2))
+
+    dst, src = h3d.halo_table(blocks, g, 0)
+    faces = {}
+    for d, sv in zip(dst, src):
+        b, x, y, z = locate(int(d))
+        nx, ny, nz = dims[b]
+        out = [x in (0, nx + 1), y in (0, ny + 1), z in (0, nz + 1)]
+        if sum(out) != 1:
+            continue
+        axis = out.index(True)
+        side = int((x, y, z)[axis] != 0)
+        bs, xs, ys, zs = locate(int(sv) & 0x7FFFFFFF)
+        src_c, dst_c = [xs, ys, zs], [x, y, z]
+        others = [a for a in range(3) if a != axis]
+        assert all(src_c[a] == dst_c[a] for a in others)
+        assert src_c[axis] in (1, dims[bs][axis])
+        faces.setdefault((b, axis, side), set()).add((bs, src_c[axis]))
+    for key, srcs in faces.items():
+        assert len(srcs) == 1, key
+    assert len(faces) == 6 * len(blocks)
