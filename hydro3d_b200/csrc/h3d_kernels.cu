@@ -2880,10 +2880,22 @@ __global__ void __launch_bounds__(32 * (kDefectRows + 2)) k_defect_march(
   pdl_wait();  // everything above reads only setup data
 #pragma unroll
   for (int q = 0; q < NR; ++q) issue(zs - 1 + q);
+  // face coefficients (mgsolver.for:186-205): walls zero the face term; a pair
+  // (x0, x0+1) starts at an odd x, so only x0 can be the west wall cell and
+  // only x0+1 the east one (nx is even)
+  const double cax = B.ax, cay = B.ay, caz = B.az;
+  const double cas = (y == 1 && (B.phys & 4)) ? 0.0 : cay, can = (y == ny && (B.phys & 8)) ? 0.0 : cay;
+  double aw0[GP], ae1[GP];
+#pragma unroll
+  for (int k = 0; k < GP; ++k) {
+    aw0[k] = (x0(k) == 1 && (B.phys & 1)) ? 0.0 : cax;
+    ae1[k] = (x0(k) + 1 == nx && (B.phys & 2)) ? 0.0 : cax;
+  }
   take(P[0], G[0], bz, zs - 1);
   take(P[1], G[1], bz, zs);
   if (wr && zs == 1) store_next(P[0], G[0], 0);  // ghost plane below
   for (int z = zs; z <= ze; ++z) {
+    const double cab = (z == 1 && (B.phys & 16)) ? 0.0 : caz, cat = (z == nz && (B.phys & 32)) ? 0.0 : caz;
     const int buf = z & 1;
     const long long rz = row + (long long)z * sxy;
     take(P[2], G[2], bz1, z + 1);
@@ -2905,8 +2917,9 @@ __global__ void __launch_bounds__(32 * (kDefectRows + 2)) k_defect_march(
         const double2 no = *reinterpret_cast<const double2*>(&sm[buf][w + 1][1 + xa]);
         const double wv = sm[buf][w][xa], ev = sm[buf][w][xa + 3];
         const long long i = rz + xa;
-        const Coef<double> c0 = cell_coef<double, false>(B, xa, y, z, i - B.off, nullptr, nullptr, nullptr);
-        const Coef<double> c1 = cell_coef<double, false>(B, xa + 1, y, z, i + 1 - B.off, nullptr, nullptr, nullptr);
+        // the coefficients of cell_coef, from the thread's x and y faces and the plane's z faces
+        const Coef<double> c0{aw0[k], cax, cas, can, cab, cat};
+        const Coef<double> c1{cax, ae1[k], cas, can, cab, cat};
         const double ap0 = coef_ap(c0), ap1 = coef_ap(c1);
         const double r0 = b2.x - (c0.aw * wv + c0.ae * pc.y + c0.as * so.x + c0.an * no.x + c0.ab * bo.x +
                                   c0.at * to.x + ap0 * pc.x);
