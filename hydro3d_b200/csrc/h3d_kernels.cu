@@ -1331,6 +1331,8 @@ static const TileShape kShapes[] = {
     {128, 8, 320, true, 32, 1, 3, 9},   {64, 8, 160, true, 16, 1, 3, 10},           // 53, 54
     {64, 16, 288, true, 16, 1, 3, 11},  {32, 16, 144, true, 8, 1, 3, 12},           // 55, 56
     {128, 8, 160, true, 16, 2, 3, 9},   {128, 4, 192, true, 32, 1, 3, 17},          // 57, 58
+    // 15-row tiles: nine a 128-row block, so 16 such blocks give 144 CTAs, one per SM on 148 SMs
+    {128, 15, 544, true, 32, 1, 3, -1}, {128, 15, 544, true, 32, 1, 3, -1},         // 59, 60
 };
 #ifdef H3D_BOUNDS_CHECK
 // Debug builds only: first recorded out-of-bounds access {kernel id + 1, block, index, limit}.
@@ -1339,7 +1341,7 @@ extern "C" int h3d_debug_bounds(unsigned long long* out) {
   return 0;
 }
 #endif
-int tma_ty_index(int ty) { return ty == 4 ? 0 : ty == 8 ? 1 : ty == 16 ? 2 : ty == 32 ? 3 : -1; }
+int tma_ty_index(int ty) { return ty == 4 ? 0 : ty == 8 ? 1 : ty == 16 ? 2 : ty == 32 ? 3 : ty == 15 ? 4 : -1; }
 int num_tile_shapes() { return (int)(sizeof(kShapes) / sizeof(kShapes[0])); }
 TileShape tile_shape(int v) { return kShapes[v]; }
 
@@ -1811,7 +1813,9 @@ constexpr int kFirstWinShape = 40;
   X(55, 16, 1, 16, 8, 4, 5)   \
   X(56, 8, 1, 16, 8, 5, 5)    \
   X(57, 16, 2, 8, 8, 4, 5)    \
-  X(58, 32, 1, 4, 8, 5, 5)
+  X(58, 32, 1, 4, 8, 5, 5)    \
+  X(59, 32, 1, 15, 8, 4, 5)   \
+  X(60, 32, 1, 15, 8, 5, 5)
 
 // (variant, threads per row, groups of four cells per thread, rows, ring slots, prefetch depth)
 #define H3D_VEC_SHAPES(X)  \

@@ -35,8 +35,8 @@ struct TileShape {
   int alt;   // for TMA shapes: the equivalent row shape (used for zero sources)
 };
 // TMA box heights (TY+4) are one of these; tensor maps are built per height.
-constexpr int kNumTmaTy = 4;
-int tma_ty_index(int ty);  // 0,1,2,3 for TY = 4, 8, 16, 32; -1 otherwise
+constexpr int kNumTmaTy = 5;
+int tma_ty_index(int ty);  // 0,1,2,3,4 for TY = 4, 8, 16, 32, 15; -1 otherwise
 constexpr int kDefectCtas = 148 * 4;  // CTAs (and partial sums) of the defect kernel
 int defect_grid(int nrows);
 // Sets the dynamic shared-memory limits of the row-tile smoothers (call once

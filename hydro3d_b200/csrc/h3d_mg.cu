@@ -894,7 +894,7 @@ int build_tensor_maps(h3d_mg* h, int g) {
   if (!enc) return H3D_OK;
   const size_t nb = V.geom.bl.size();
   std::vector<CUtensorMap> maps((size_t)kNumTmaTy * 3 * nb);
-  const int tys[kNumTmaTy] = {4, 8, 16, 32};
+  const int tys[kNumTmaTy] = {4, 8, 16, 32, 15};
   for (int ti = 0; ti < kNumTmaTy; ++ti)
     for (int buf = 0; buf < 3; ++buf)
       for (size_t b = 0; b < nb; ++b) {
