@@ -47,6 +47,24 @@ def dist_env():
     return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
 
 
+def max_over_ranks(x, world):
+    """The largest x over all ranks (device-timed milliseconds: the slowest
+    replica sets the job time); x itself on one rank."""
+    if world <= 1:
+        return float(x)
+    import torch
+    import torch.distributed as tdist
+    t = torch.tensor([float(x)], dtype=torch.float64)
+    tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_ms_per_solve(total_ms_max, steps, world):
+    """Whole-job time per solve of N replicas that each ran `steps` solves:
+    the slowest replica's total over all solves of the job."""
+    return total_ms_max / (steps * world)
+
+
 def load_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -296,14 +314,8 @@ def main():
     clk = clocks.stop()
     ms_fp64, infos_fp64 = timed_solves(fp64, prob, max(1, min(args.steps, 3)), args.warmup, barrier=barrier)
 
-    total_ms = sum(ms_mixed)
-    if dist:
-        import torch
-        import torch.distributed as tdist
-        t = torch.tensor([total_ms], dtype=torch.float64)
-        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
-        total_ms = float(t.item())
-    value = total_ms / (args.steps * world)
+    total_ms = max_over_ranks(sum(ms_mixed), world)
+    value = job_ms_per_solve(total_ms, args.steps, world)
 
     # solution error of the mixed solve against the FP64 solve (same inputs)
     from hydro3d_b200 import host_field
