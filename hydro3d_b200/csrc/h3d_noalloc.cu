@@ -1,12 +1,14 @@
 // Residual norms of one block with no device allocation.
 //
-// Some hosts of this solver cannot allocate device memory themselves: a
-// Fortran time loop that runs inside a CUDA graph it captured, code running
-// under a memory pool whose budget is already committed, or an embedding
-// that forbids cudaMalloc after start-up.  h3d_residual_noalloc() serves
-// them: it evaluates r = b - A p for one block from device arrays the caller
-// already owns, and keeps its per-row partial sums in a fixed array in this
-// library's own device memory, so the call allocates and frees nothing.
+// Some hosts of this solver cannot allocate device memory themselves: code
+// running under a memory pool whose budget was committed at start-up, or an
+// embedding (a Fortran time loop under a host framework that owns the device
+// heap) that forbids cudaMalloc after initialisation.  h3d_residual_noalloc()
+// serves them: it evaluates r = b - A p for one block from device arrays the
+// caller already owns, and keeps its per-row partial sums in a fixed array in
+// this library's own device memory, so the call allocates and frees nothing.
+// It copies its four results to host memory and synchronises the stream it
+// was given before it returns.
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -26,6 +28,11 @@ static __device__ __align__(256) double g_noalloc_scratch[4 * kNoAllocMaxRows + 
 constexpr int kMaxDevices = 64;
 std::mutex g_mu;
 double* g_scratch_ptr[kMaxDevices] = {nullptr};
+int g_sm_count[kMaxDevices] = {0};
+
+// max(a, |r|) that keeps a NaN once one is seen (fmax would drop it, and a
+// non-finite residual would then read as a finite max|r|).
+__device__ __forceinline__ double nan_max(double a, double v) { return (v != v || v > a) ? v : a; }
 
 // r = b - A p for the interior cells of one row; same operand order as the
 // solver's defect (mgsolver.for:707-714).  One warp per row, fixed lane order.
@@ -49,14 +56,14 @@ __global__ void __launch_bounds__(256) k_resid_rows(const double* __restrict__ p
                              ab * p[i - B.sxy] + at * p[i + B.sxy] + ap * p[i]);
       rr += r * r;
       bb += bv * bv;
-      rm = fmax(rm, fabs(r) * B.dv);
+      rm = nan_max(rm, fabs(r) * B.dv);
       rs += r;
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
       rr += __shfl_xor_sync(0xffffffffu, rr, o);
       bb += __shfl_xor_sync(0xffffffffu, bb, o);
-      rm = fmax(rm, __shfl_xor_sync(0xffffffffu, rm, o));
+      rm = nan_max(rm, __shfl_xor_sync(0xffffffffu, rm, o));
       rs += __shfl_xor_sync(0xffffffffu, rs, o);
     }
     if (lane == 0) {
@@ -75,7 +82,7 @@ __global__ void __launch_bounds__(256) k_resid_reduce(double* __restrict__ scrat
   for (int q = threadIdx.x; q < nrows; q += 256) {
     a0 += scratch[4 * (size_t)q];
     a1 += scratch[4 * (size_t)q + 1];
-    a2 = fmax(a2, scratch[4 * (size_t)q + 2]);
+    a2 = nan_max(a2, scratch[4 * (size_t)q + 2]);
     a3 += scratch[4 * (size_t)q + 3];
   }
   sh[0][threadIdx.x] = a0; sh[1][threadIdx.x] = a1; sh[2][threadIdx.x] = a2; sh[3][threadIdx.x] = a3;
@@ -84,7 +91,7 @@ __global__ void __launch_bounds__(256) k_resid_reduce(double* __restrict__ scrat
     if (threadIdx.x < s) {
       sh[0][threadIdx.x] += sh[0][threadIdx.x + s];
       sh[1][threadIdx.x] += sh[1][threadIdx.x + s];
-      sh[2][threadIdx.x] = fmax(sh[2][threadIdx.x], sh[2][threadIdx.x + s]);
+      sh[2][threadIdx.x] = nan_max(sh[2][threadIdx.x], sh[2][threadIdx.x + s]);
       sh[3][threadIdx.x] += sh[3][threadIdx.x + s];
     }
     __syncthreads();
@@ -93,9 +100,10 @@ __global__ void __launch_bounds__(256) k_resid_reduce(double* __restrict__ scrat
     for (int k = 0; k < 4; ++k) scratch[4 * (size_t)nrows + k] = sh[k][0];
 }
 
-// Device address of the scratch array on the current device (set-up, once
-// per device; the array's host-side name is only a stand-in for it).
-int scratch_of_current_device(double** out) {
+// Device address of the scratch array on the current device and that
+// device's multiprocessor count (set-up, once per device; the array's
+// host-side name is only a stand-in for its address).
+int scratch_of_current_device(double** out, int* sms) {
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
     h3d::set_call_error("h3d_residual_noalloc: no current CUDA device");
@@ -109,9 +117,17 @@ int scratch_of_current_device(double** out) {
       h3d::set_call_error(std::string("h3d_residual_noalloc: cudaGetSymbolAddress: ") + cudaGetErrorString(e));
       return H3D_ERR_CUDA;
     }
+    int nsm = 0;
+    e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess || nsm < 1) {
+      h3d::set_call_error(std::string("h3d_residual_noalloc: cudaDeviceGetAttribute: ") + cudaGetErrorString(e));
+      return H3D_ERR_CUDA;
+    }
+    g_sm_count[dev] = nsm;
     g_scratch_ptr[dev] = ptr;
   }
   *out = g_scratch_ptr[dev];
+  *sms = g_sm_count[dev];
   return H3D_OK;
 }
 
@@ -129,7 +145,8 @@ extern "C" int h3d_residual_noalloc(const double* p, const double* b, int32_t nx
     return H3D_ERR_ARG;
   }
   double* scratch = nullptr;
-  int rc = scratch_of_current_device(&scratch);
+  int sms = 0;
+  int rc = scratch_of_current_device(&scratch, &sms);
   if (rc != H3D_OK) return rc;
   h3d::BlkLev B{};
   B.nx = nx; B.ny = ny; B.nz = nz;
@@ -144,7 +161,7 @@ extern "C" int h3d_residual_noalloc(const double* p, const double* b, int32_t nx
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   const int nrows = ny * nz;
   int grid = (nrows + 7) / 8;
-  if (grid > 148 * 8) grid = 148 * 8;
+  if (grid > sms * 8) grid = sms * 8;
   k_resid_rows<<<grid, 256, 0, st>>>(p, b, B, scratch);
   k_resid_reduce<<<1, 256, 0, st>>>(scratch, nrows);
   cudaError_t e = cudaGetLastError();

@@ -178,19 +178,21 @@ int h3d_halo_table(int32_t nblocks, const h3d_block_desc* blocks, int32_t g,
                    int64_t* n);
 
 /* Residual norms of one block without allocating device memory.  For hosts
- * that cannot call cudaMalloc (a time loop running inside a CUDA graph it
- * captured, a committed memory pool, an embedding that forbids allocation
- * after start-up).  No counterpart in the reference.
+ * that cannot call cudaMalloc: code running under a memory pool whose budget
+ * was committed at start-up, or an embedding that forbids device allocation
+ * after initialisation.  No counterpart in the reference.
  *   p: device array (nz+2, ny+2, nx+2), x fastest, one ghost layer; b: device
  *   array of the same shape (interior read); h = dx, dy, dz; phys_mask bit f
  *   (W,E,S,N,B,T) = wall face (zero coefficient); out (host) receives
- *   {sum r^2, sum b^2, max|r|*dx*dy*dz, sum r} of r = b - A p; stream may be 0.
+ *   {sum r^2, sum b^2, max|r|*dx*dy*dz, sum r} of r = b - A p (a NaN in r
+ *   shows in every entry); stream may be 0.
  * Its per-row partial sums live in a fixed 2 MiB device array inside this
  * library (held by every GPU that loads it until exit), so ny*nz must not
  * exceed 65536 (H3D_ERR_ARG otherwise).  The first call on a device looks up
- * that array's device address; make it before any stream capture.  Calls that
- * overlap on the GPU share the array and race; the call synchronizes its
- * stream before returning. */
+ * that array's device address and the device's multiprocessor count.  Calls
+ * that overlap on the GPU share the array and race.  The call copies its
+ * result into `out` on `stream` and synchronises that stream before it
+ * returns. */
 int h3d_residual_noalloc(const double* p, const double* b, int32_t nx, int32_t ny, int32_t nz,
                          const double* h, int32_t phys_mask, double* out, void* stream);
 

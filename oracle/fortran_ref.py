@@ -45,7 +45,9 @@ from typing import Dict, List, Optional, Tuple
 
 import numpy as np
 
-REF_SRC = os.environ.get("H3D_REFERENCE_SRC", "/root/reference/src_v70")
+# Directory holding the reference's src_v70 Fortran files.  There is no
+# default: the translator runs only where H3D_REFERENCE_SRC names that tree.
+REF_SRC = os.environ.get("H3D_REFERENCE_SRC", "")
 
 # ---------------------------------------------------------------------------
 # Run-time support used by the generated code

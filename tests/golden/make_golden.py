@@ -25,6 +25,10 @@ from oracle import oracle as O  # noqa: E402
 
 W, P = 4, 5
 
+# The reference's Fortran sources: H3D_REFERENCE_SRC if set, else the
+# read-only mount of the reference tree this script was written against.
+REF_SRC = F.REF_SRC or "/root/reference/src_v70"
+
 
 def grid(nb, n):
     ext = []
@@ -48,7 +52,7 @@ CASES = {
 H = (1.0 / 32, 1.0 / 32, 1.0 / 32)
 
 
-def run_case(name, src_dir=F.REF_SRC):
+def run_case(name, src_dir=REF_SRC):
     ext, bc, ngrd, itr, pl_ex, lsm, seed = CASES[name]
     descs = O.topology(ext, bc, H, ngrd)
     R = F.Reference(list(descs), ngrd, mg_itrsch=itr, pl_ex=pl_ex, lsm=lsm, src_dir=src_dir)

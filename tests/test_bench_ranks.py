@@ -38,7 +38,12 @@ def test_two_rank_job_time_is_the_slowest_rank():
             p.start()
         for p in procs:
             p.join(120)
-            assert p.exitcode == 0
+        codes = [p.exitcode for p in procs]
+        for p in procs:  # a rank stuck in a collective must not outlive the test
+            if p.is_alive():
+                p.terminate()
+                p.join(10)
+        assert codes == [0, 0], codes
         res = dict(out)
     assert sorted(res) == [0, 1]
     for rank, (r, w, local, got, per) in res.items():

@@ -79,19 +79,23 @@ def test_cuda_matches_reference(h3d, name):
     s.close()
 
 
+def _make_golden():
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("make_golden", os.path.join(GOLDEN, "make_golden.py"))
+    mg = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mg)
+    return mg
+
+
 def _reference_tree():
-    from oracle import fortran_ref as F
-    return F.REF_SRC if os.path.isfile(os.path.join(F.REF_SRC, "mgsolver.for")) else None
+    src = _make_golden().REF_SRC
+    return src if os.path.isfile(os.path.join(src, "mgsolver.for")) else None
 
 
 @pytest.mark.skipif(_reference_tree() is None, reason="reference source tree not present")
 @pytest.mark.parametrize("name", ["walls_2x1x1", "lsm_periodic_x_2x1x2", "periodic_x_2x2x2"])
 def test_fixture_regenerates(oracle_mod, name):
-    import importlib.util
-    spec = importlib.util.spec_from_file_location("make_golden", os.path.join(GOLDEN, "make_golden.py"))
-    mg = importlib.util.module_from_spec(spec)
-    spec.loader.exec_module(mg)
-    fresh = mg.run_case(name)
+    fresh = _make_golden().run_case(name)
     old = _load(name)
     assert sorted(fresh) == sorted(old)
     for k in old:

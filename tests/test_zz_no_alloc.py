@@ -16,12 +16,13 @@ W, P = 4, 5
 RTOL = 1e-12
 
 
-def _call(lib, p_dev, b_dev, n, h, phys):
+def _call(lib, p_dev, b_dev, n, h, phys, stream=None):
     import torch
     out = (C.c_double * 4)()
     hh = (C.c_double * 3)(*h)
+    st = C.c_void_p(stream.cuda_stream) if stream is not None else None
     rc = lib.h3d_residual_noalloc(C.c_void_p(p_dev.data_ptr()), C.c_void_p(b_dev.data_ptr()),
-                                  n[0], n[1], n[2], hh, phys, out, None)
+                                  n[0], n[1], n[2], hh, phys, out, st)
     assert rc == 0, lib.h3d_mg_last_error(None)
     torch.cuda.synchronize()
     return np.array(out[:])
@@ -91,3 +92,44 @@ def test_noalloc_rejects_oversize(h3d):
                                   8, 257, 256, hh, 63, out, None)
     assert rc == h3d._lib.H3D_ERR_ARG
     assert b"65536" in lib.h3d_mg_last_error(None)
+
+
+def test_noalloc_at_row_limit_on_a_stream(h3d):
+    """ny*nz = 65536 rows exactly: the final quadruple lands in the last four
+    doubles of the fixed device array.  Called on a caller-owned stream, twice,
+    against a numpy evaluation of r = b - A p."""
+    import torch
+    n = (4, 256, 256)
+    h = (0.5, 0.25, 0.125)
+    phys = 63
+    rng = np.random.default_rng(91)
+    shape = (n[2] + 2, n[1] + 2, n[0] + 2)
+    p = rng.standard_normal(shape)
+    b = rng.standard_normal(shape)
+    lib = h3d.lib()
+    p_dev = torch.from_numpy(p).cuda()
+    b_dev = torch.from_numpy(b).cuda()
+    st = torch.cuda.Stream()
+    first = _call(lib, p_dev, b_dev, n, h, phys, stream=st)
+    second = _call(lib, p_dev, b_dev, n, h, phys, stream=st)
+    assert np.array_equal(first, second)
+    r = _numpy_residual(p, b, n, h, phys)
+    bi = b[1:-1, 1:-1, 1:-1]
+    assert abs(first[0] - (r * r).sum()) <= 1e-12 * (r * r).sum()
+    assert abs(first[1] - (bi * bi).sum()) <= 1e-12 * (bi * bi).sum()
+    assert abs(first[2] - np.abs(r).max() * h[0] * h[1] * h[2]) <= 1e-12 * np.abs(r).max()
+    assert abs(first[3] - r.sum()) <= 1e-10 * np.abs(r).sum()
+
+
+def test_noalloc_reports_nan(h3d):
+    """A NaN in b shows in every entry of the result, max|r|*dV included."""
+    import torch
+    n = (16, 8, 8)
+    rng = np.random.default_rng(5)
+    shape = (n[2] + 2, n[1] + 2, n[0] + 2)
+    p = rng.standard_normal(shape)
+    b = rng.standard_normal(shape)
+    b[4, 3, 7] = np.nan
+    lib = h3d.lib()
+    out = _call(lib, torch.from_numpy(p).cuda(), torch.from_numpy(b).cuda(), n, (1.0, 1.0, 1.0), 63)
+    assert np.all(np.isnan(out)), out
