@@ -15,7 +15,8 @@ With N > 1 (torchrun) every rank solves its own replica (the path does not
 shard across GPUs in this build); the value is the whole job's ms per solve
 (max-over-ranks device time / (N*K)).  `--impl reference` times the CPU
 implementation of the same path (the oracle restatement of the reference
-Fortran, OpenMP over all host cores) on a bounded sample.
+Fortran, OpenMP over all host cores): every timed step one complete
+converged solve.
 """
 from __future__ import annotations
 
@@ -127,9 +128,80 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def make_problem(cfg):
+def oracle_resolve(ext, bc, h, ngrid):
+    """Block neighbours found by the oracle's read_infodom restatement (the
+    CPU arms build their blocks without the CUDA library)."""
+    from oracle import oracle as O
+    return O.topology(ext, bc, h, ngrid)
+
+
+def make_problem(cfg, resolve=None, prev_solve=None):
+    """The workload of configuration `cfg`.  Configuration 2 starts from the
+    converged pressure of its independent previous-seed problem:
+    `prev_solve(problem)` solves that problem to 1e-8 (untimed set-up) and
+    returns its block host fields."""
     from hydro3d_b200 import synth
-    return synth.CONFIGS[cfg]()
+    if cfg != 2:
+        return synth.CONFIGS[cfg](resolve=resolve)
+    prev = synth.config2(seed=1017, resolve=resolve)
+    fields = prev_solve(prev)
+    return synth.config2(p0=synth.gather(fields, prev.blocks), resolve=resolve)
+
+
+def gpu_prev_solve(prob):
+    s = build_solver_dev(prob, "fp64", int(os.environ.get("LOCAL_RANK", 0)))
+    info = s.solve_resident(tol=TOL, maxcy=400)
+    if not info["converged"]:
+        raise RuntimeError("previous-seed solve did not converge")
+    from hydro3d_b200 import host_field
+    out = [host_field(d) for d in prob.blocks]
+    for ib in range(len(prob.blocks)):
+        s.download("p", ib, out[ib])
+    s.close()
+    return out
+
+
+class OracleSolver:
+    """The oracle (C restatement of the reference multigrid, OpenMP over the
+    planes of each block) set up on one workload."""
+
+    def __init__(self, prob, threads):
+        from oracle import oracle as O
+        import ctypes as C
+        from hydro3d_b200 import interior, with_ghost
+        od = (O.BlockDesc * len(prob.blocks))()
+        C.memmove(od, (type(prob.blocks[0]) * len(prob.blocks))(*prob.blocks), C.sizeof(od))
+        self.orc = O.Oracle(list(od), prob.ngrid, 3, 2, 1, lsm=prob.var_coef, threads=threads)
+        if prob.var_coef:
+            for ib, (d, x) in enumerate(zip(prob.blocks, prob.dens)):
+                self.orc.set_density(ib, np.ascontiguousarray(interior(x, d)))
+        self.orc.coeff()
+        self.b = [np.ascontiguousarray(interior(x, d)) for x, d in zip(prob.b, prob.blocks)]
+        self.p0 = [np.ascontiguousarray(with_ghost(x, d)) for x, d in zip(prob.p0, prob.blocks)]
+
+    def solve(self, maxcy=400, tol=TOL):
+        """One defect-correction solve from p0; returns (ms, result)."""
+        t0 = time.perf_counter()
+        res = self.orc.solve(self.p0, self.b, tol=tol, maxcy=maxcy)
+        return (time.perf_counter() - t0) * 1e3, res
+
+    def close(self):
+        self.orc.close()
+
+
+def oracle_prev_solve(threads):
+    def solve(prob):
+        from hydro3d_b200 import host_field, interior
+        o = OracleSolver(prob, threads)
+        _, res = o.solve()
+        o.close()
+        if res["status"] != 0:
+            raise RuntimeError("previous-seed oracle solve did not converge")
+        out = [host_field(d) for d in prob.blocks]
+        for x, d, pr in zip(out, prob.blocks, res["p"]):
+            interior(x, d)[...] = pr[1:-1, 1:-1, 1:-1]
+        return out
+    return solve
 
 
 def build_solver(prob, precision, use_graph=True):
@@ -201,59 +273,72 @@ def mean_removed_error(a_list, b_list, blocks):
     return float(np.linalg.norm(a - b) / np.linalg.norm(b))
 
 
-def cpu_port_sample(prob, fp64_cycles, threads, sample_cycles=2):
-    """Oracle (C restatement of the reference MG, OpenMP) on the full workload:
-    time `sample_cycles` defect-correction V-cycles, project to the cycle count
-    of the identical FP64 algorithm."""
-    from oracle import oracle as O
-    import ctypes as C
-    od = (O.BlockDesc * len(prob.blocks))()
-    C.memmove(od, (type(prob.blocks[0]) * len(prob.blocks))(*prob.blocks), C.sizeof(od))
-    orc = O.Oracle(list(od), prob.ngrid, 3, 2, 1, lsm=prob.var_coef, threads=threads)
-    if prob.var_coef:
-        from hydro3d_b200 import interior
-        for ib, (d, x) in enumerate(zip(prob.blocks, prob.dens)):
-            orc.set_density(ib, np.ascontiguousarray(interior(x, d)))
-    orc.coeff()
-    from hydro3d_b200 import interior, with_ghost
-    b = [np.ascontiguousarray(interior(x, d)) for x, d in zip(prob.b, prob.blocks)]
-    p = [np.ascontiguousarray(with_ghost(x, d)) for x, d in zip(prob.p0, prob.blocks)]
-    t0 = time.perf_counter()
-    res = orc.solve(p, b, tol=0.0, maxcy=sample_cycles)
-    dt = time.perf_counter() - t0
-    orc.close()
-    per_cycle = dt / max(res["cycles"], 1)
-    return per_cycle * 1e3 * fp64_cycles, per_cycle, res
+def cpu_full_solve(prob, threads):
+    """One complete FP64 solve of the workload by the oracle to 1e-8 (the
+    reference algorithm, measured, not projected)."""
+    o = OracleSolver(prob, threads)
+    ms, res = o.solve()
+    o.close()
+    if res["status"] != 0:
+        raise RuntimeError(f"oracle solve did not converge ({res['cycles']} cycles)")
+    return ms, res
 
 
 def run_reference(args):
+    """The reference's CPU algorithm (the oracle: a C restatement of the
+    reference multigrid, no Fortran toolchain exists to build the reference
+    itself) on the box's host cores.  Every timed step is one complete
+    converged FP64 solve of the workload; every warm-up step one V-cycle.
+    Neither the problem set-up nor the solve loads the CUDA library."""
     rank, world, _ = dist_env()
     if rank != 0:
         return
-    prob = make_problem(args.config)
     threads = os.cpu_count() or 1
     from oracle import oracle as O
     O.lib()
-    # cycle count of the reference algorithm on this workload (FP64, to 1e-8)
-    cyc = args.ref_cycles
-    vals = []
+    prob = make_problem(args.config, resolve=oracle_resolve, prev_solve=oracle_prev_solve(threads))
+    o = OracleSolver(prob, threads)
     for _ in range(args.warmup):
-        cpu_port_sample(prob, cyc, threads, sample_cycles=1)
+        o.solve(maxcy=1, tol=0.0)
+    ms, cycles = [], []
     for _ in range(args.steps):
-        v, per_cycle, _ = cpu_port_sample(prob, cyc, threads, sample_cycles=args.ref_sample_cycles)
-        vals.append(v)
-    value = statistics.median(vals)
+        t, res = o.solve()
+        if res["status"] != 0:
+            raise RuntimeError(f"oracle solve did not converge ({res['cycles']} cycles)")
+        ms.append(t)
+        cycles.append(res["cycles"])
+    o.close()
+    value = sum(ms) / len(ms)
     line = {
         "impl": "reference", "metric": "poisson_solve_ms_to_1e-8", "value": round(value, 3), "unit": "ms",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(value, 3),
         "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOADS[args.config], "solver": "reference V(2,1) RBGS, FP64"},
+        "config": config_of(args.config, prob),
+        "cycles": cycles[-1], "relres": res["relres"],
         "cpu_baseline": {"value": round(value, 3), "unit": "ms", "cores": threads, "kind": "port",
-                         "sample": f"{args.ref_sample_cycles} FP64 V-cycles per step on the full workload, "
-                                   f"scaled to the {cyc} cycles the identical FP64 algorithm needs to 1e-8"},
+                         "sample": f"{args.steps} complete FP64 solves of the full workload to 1e-8 "
+                                   f"({cycles[-1]} V(2,1) cycles each, measured); warm-up steps one V-cycle"},
         "e2e": {"value": round(value, 3), "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+def config_of(cfg, prob):
+    return {"workload": WORKLOADS[cfg], "tol": TOL, "cells": prob.cells,
+            "l2": "inputs larger than L2 (one level-1 FP64 field is %.0f MB)" % (prob.cells * 8 / 1e6)
+            if prob.cells * 8 > 126e6 else "inputs smaller than L2 (no flush between solves)"}
+
+
+def mcell_updates(prob, cycles):
+    """Cell updates of `cycles` V(2,1) cycles: three sweeps of every level
+    (two before and one after the coarse correction; the coarsest level
+    irestr + iproln sweeps)."""
+    per = 0
+    for d in prob.blocks:
+        for g in range(1, prob.ngrid + 1):
+            s = 2 ** (g - 1)
+            per += (d.n[0] // s) * (d.n[1] // s) * (d.n[2] // s) * 3
+    return per * cycles
 
 
 def main():
@@ -263,8 +348,6 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--config", type=int, default=3)
-    ap.add_argument("--ref-cycles", type=int, default=int(os.environ.get("H3D_REF_CYCLES", "0")) or 0)
-    ap.add_argument("--ref-sample-cycles", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--ncu-region", action="store_true",
@@ -274,8 +357,6 @@ def main():
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
-        if args.ref_cycles <= 0:
-            args.ref_cycles = REF_CYCLES.get(args.config, 30)
         return run_reference(args)
 
     rank, world, local = dist_env()
@@ -289,7 +370,7 @@ def main():
     import hydro3d_b200  # noqa: F401  (loads libh3dmg.so; raises if missing)
     os.environ.setdefault("CUDA_DEVICE_ORDER", "PCI_BUS_ID")
     device = local
-    prob = make_problem(args.config)
+    prob = make_problem(args.config, prev_solve=gpu_prev_solve)
     peak, peak_kind = load_peaks()
     if args.ncu_region:
         import torch
@@ -334,7 +415,7 @@ def main():
     bytes_launch = sm_bytes / max(sm_n, 1)
     avg_launch_ms = sm_ms / max(sm_n, 1)
     achieved = sm_bytes / (sm_ms * 1e-3) / 1e9 if sm_n else None
-    traffic = read_profile_traffic()
+    traffic = read_profile_traffic(args.config, mixed.get_smoother(1)[0])
 
     e2e = None
     if not args.no_e2e:
@@ -345,10 +426,10 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
-        v, per_cycle, _ = cpu_port_sample(prob, infos_fp64[-1]["cycles"], threads, sample_cycles=2)
+        v, res = cpu_full_solve(prob, threads)
         cpu = {"value": round(v, 1), "unit": "ms", "cores": threads, "kind": "port",
-               "sample": f"2 FP64 V-cycles of the oracle on the full workload ({per_cycle * 1e3:.0f} ms/cycle), "
-                         f"scaled to the {infos_fp64[-1]['cycles']} cycles the FP64 algorithm needs"}
+               "sample": f"one complete FP64 solve of the full workload to 1e-8 by the oracle "
+                         f"({res['cycles']} V(2,1) cycles, measured)", "cycles": res["cycles"]}
 
     if rank == 0:
         fp64_ms = statistics.median(ms_fp64)
@@ -357,15 +438,13 @@ def main():
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(value, 3),
             "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
             "data": "synthetic (seeded; no dataset)",
-            "config": {"workload": WORKLOADS[args.config], "precision": "FP32 V(2,1) RBGS inside FP64 refinement",
-                       "inner_cycles": 2, "tol": TOL, "cells": prob.cells,
-                       "l2": "inputs larger than L2 (one level-1 FP64 field is %.0f MB)" % (prob.cells * 8 / 1e6),
-                       "parallelism": "replicas" if world > 1 else "single GPU"},
+            "config": dict(config_of(args.config, prob), precision="FP32 V(2,1) RBGS inside FP64 refinement",
+                           inner_cycles=2, parallelism="replicas" if world > 1 else "single GPU"),
             "fp64_ms": round(fp64_ms, 3), "speedup_vs_fp64": round(fp64_ms / (total_ms / (args.steps * world) * world), 3)
             if world == 1 else None,
             "cycles_mixed": info["cycles"], "outer_mixed": info["outer"], "cycles_fp64": infos_fp64[-1]["cycles"],
             "relres_mixed": info["relres"], "relres_fp64": infos_fp64[-1]["relres"], "error_vs_fp64": err,
-            "mcell_updates_per_s": None,
+            "mcell_updates_per_s": round(mcell_updates(prob, info["cycles"]) / (value * 1e-3) / 1e6, 1),
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1) if achieved else None, "peak": peak,
                          "unit": "GB/s", "frac": round(achieved / peak, 4) if achieved else None,
                          "traffic": traffic, "kernel": "level-1 FP32 smoother (autotuned variant %d)" % mixed.get_smoother(1)[0],
@@ -383,24 +462,24 @@ def main():
         tdist.destroy_process_group()
 
 
-# FP64 V-cycle counts to 1e-8 of the reference algorithm per workload (the
-# GPU FP64 path reproduces the reference arithmetic bit for bit, so its count
-# is the reference's count); used to scale the reference arm's bounded sample.
-REF_CYCLES = {1: 45, 2: 30, 3: 54, 4: 60, 5: 60}
-
-
-def read_profile_traffic():
-    """DRAM bytes per smoother launch from the committed ncu summary, if any."""
+def read_profile_traffic(cfg, variant):
+    """DRAM bytes (read + write) per level-1 smoother launch from the committed
+    ncu summary of this workload, when that capture is of the variant the
+    autotuner chose in this run; None otherwise."""
     p = os.path.join(ROOT, "profiles", "k_rbgs_win_fp32_config3.md")
-    if not os.path.exists(p):
+    if cfg != 3 or not os.path.exists(p):
         return None
+    vals = {}
     for ln in open(p):
-        if ln.startswith("traffic_bytes_per_launch"):
-            try:
-                return float(ln.split("=")[1])
-            except ValueError:
-                return None
-    return None
+        if "=" in ln and ln.split("=")[0].strip() in ("traffic_bytes_per_launch", "smoother_variant"):
+            k, v = ln.split("=", 1)
+            vals[k.strip()] = v.strip()
+    try:
+        if int(vals.get("smoother_variant", -1)) != variant:
+            return None
+        return float(vals["traffic_bytes_per_launch"])
+    except (KeyError, ValueError):
+        return None
 
 
 def build_solver_dev(prob, precision, device):

@@ -6,6 +6,9 @@ divergence of a seeded velocity field, computed the way calmas does it
 by the cell volume), with boundary-normal wall velocities zero so the
 all-Neumann problems are compatible.  Seeds: numpy PCG64, 1000 + config
 index (and +17 for the "previous solve" field of configuration 2).
+
+Every generator takes `resolve`, passed on to topology.from_extents: None
+finds block neighbours with the library, a callable finds them without it.
 """
 from __future__ import annotations
 
@@ -77,11 +80,24 @@ def _split(global_field, blocks):
     return out
 
 
-def config1(seed: int = 1001, n: int = 64, ngrid: int = 4) -> Problem:
+def gather(fields, blocks):
+    """Inverse of the scatter into blocks: the global (NZ, NY, NX) cell field
+    of block host fields placed at their origins."""
+    NX = max(d.origin[0] + d.n[0] for d in blocks)
+    NY = max(d.origin[1] + d.n[1] for d in blocks)
+    NZ = max(d.origin[2] + d.n[2] for d in blocks)
+    g = np.zeros((NZ, NY, NX))
+    for a, d in zip(fields, blocks):
+        o = d.origin
+        g[o[2]:o[2] + d.n[2], o[1]:o[1] + d.n[1], o[0]:o[0] + d.n[0]] = interior(a, d)
+    return g
+
+
+def config1(seed: int = 1001, n: int = 64, ngrid: int = 4, resolve=None) -> Problem:
     """Single block n^3, h = 1/n, walls on all faces, zero initial guess."""
     rng = np.random.Generator(np.random.PCG64(seed))
     h = (1.0 / n,) * 3
-    blocks = topology.block_grid((1, 1, 1), (n, n, n), [WALL] * 6, h, ngrid)
+    blocks = topology.block_grid((1, 1, 1), (n, n, n), [WALL] * 6, h, ngrid, resolve=resolve)
     b = divergence(*_uniform_velocity(rng, (n, n, n)), h)
     return Problem("config1", blocks, ngrid, _split(b, blocks), [host_field(d) for d in blocks],
                    meta=dict(seed=seed))
@@ -97,7 +113,8 @@ def _config2_rhs(seed, N, h):
     return b
 
 
-def config2(seed: int = 1002, nb: int = 2, n: int = 96, ngrid: int = 6, p0: Optional[np.ndarray] = None) -> Problem:
+def config2(seed: int = 1002, nb: int = 2, n: int = 96, ngrid: int = 6, p0: Optional[np.ndarray] = None,
+            resolve=None) -> Problem:
     """(nb*n)^3 as nb^3 blocks of n^3; periodic in x, walls in y and z.
 
     b = div u of a U(-1,1) velocity (periodic in x) plus sin(2 pi x)cos(2 pi y)
@@ -108,7 +125,7 @@ def config2(seed: int = 1002, nb: int = 2, n: int = 96, ngrid: int = 6, p0: Opti
     N = nb * n
     h = (1.0 / N,) * 3
     bc = [PER, PER, WALL, WALL, WALL, WALL]
-    blocks = topology.block_grid((nb, nb, nb), (n, n, n), bc, h, ngrid)
+    blocks = topology.block_grid((nb, nb, nb), (n, n, n), bc, h, ngrid, resolve=resolve)
     b = _config2_rhs(seed, N, h)
     pinit = [host_field(d) for d in blocks]
     if p0 is not None:
@@ -140,13 +157,13 @@ def spectral_velocity(rng, shape, box, kmin=1.0, kmax=64.0):
     return f
 
 
-def config3(seed: int = 1003, nblk=(4, 2, 2), n: int = 128, ngrid: int = 7) -> Problem:
+def config3(seed: int = 1003, nblk=(4, 2, 2), n: int = 128, ngrid: int = 7, resolve=None) -> Problem:
     """512x256x256 cells as 4x2x2 blocks of 128^3, all walls, spectral velocity."""
     rng = np.random.Generator(np.random.PCG64(seed))
     NX, NY, NZ = nblk[0] * n, nblk[1] * n, nblk[2] * n
     hh = 1.0 / max(NY, NZ)
     h = (hh, hh, hh)
-    blocks = topology.block_grid(nblk, (n, n, n), [WALL] * 6, h, ngrid)
+    blocks = topology.block_grid(nblk, (n, n, n), [WALL] * 6, h, ngrid, resolve=resolve)
     box = (NZ * hh, NY * hh, NX * hh)
     comps = []
     for _ in range(3):
@@ -161,12 +178,13 @@ def config3(seed: int = 1003, nblk=(4, 2, 2), n: int = 128, ngrid: int = 7) -> P
                    meta=dict(seed=seed))
 
 
-def config4(seed: int = 1004, nblocks: int = 27, ngrid: int = 4, choices=(32, 48, 64, 96, 128)) -> Problem:
+def config4(seed: int = 1004, nblocks: int = 27, ngrid: int = 4, choices=(32, 48, 64, 96, 128),
+            resolve=None) -> Problem:
     """27 independent wall-bounded blocks of seeded uneven sizes, h = 1/64."""
     rng = np.random.Generator(np.random.PCG64(seed))
     sizes = [tuple(int(v) for v in rng.choice(choices, size=3)) for _ in range(nblocks)]
     h = (1.0 / 64,) * 3
-    blocks = topology.independent_blocks(sizes, h, ngrid)
+    blocks = topology.independent_blocks(sizes, h, ngrid, resolve=resolve)
     bs = []
     for d in blocks:
         n = (d.n[0], d.n[1], d.n[2])
@@ -184,14 +202,15 @@ def heaviside(phi, eps):
     return Hs
 
 
-def config5(seed: int = 1005, n: int = 256, ngrid: int = 8, rho_l: float = 1000.0, rho_g: float = 1.0) -> Problem:
+def config5(seed: int = 1005, n: int = 256, ngrid: int = 8, rho_l: float = 1000.0, rho_g: float = 1.0,
+            resolve=None) -> Problem:
     """Two-phase variable-coefficient problem: single block n^3, density from a
     seeded sphere level set (heavy fluid outside), L_LSM coefficients."""
     rng = np.random.Generator(np.random.PCG64(seed))
     hh = 1.0 / n
     h = (hh, hh, hh)
     c = rng.uniform(0.3, 0.7, 3)
-    blocks = topology.block_grid((1, 1, 1), (n, n, n), [WALL] * 6, h, ngrid)
+    blocks = topology.block_grid((1, 1, 1), (n, n, n), [WALL] * 6, h, ngrid, resolve=resolve)
     xc = (np.arange(n) + 0.5) * hh
     phi = np.sqrt((xc[None, None, :] - c[0]) ** 2 + (xc[None, :, None] - c[1]) ** 2 +
                   (xc[:, None, None] - c[2]) ** 2) - 0.2

@@ -16,10 +16,45 @@ WALL = 4       # any bc code other than 5 is a zero-gradient wall for p
 PERIODIC = 5   # control.cin periodic code
 
 
-def from_extents(ext: np.ndarray, bc: Sequence[int], h: Sequence[float], ngrid: int, pl: int = 1):
-    """Descriptors for blocks with integer extents ext[b] = (xs, xe, ys, ye, zs, ze)."""
+def grid_extents(nblk: Sequence[int], n: Sequence[int]) -> np.ndarray:
+    """Extents of a regular nblk[0] x nblk[1] x nblk[2] arrangement of equal
+    blocks of n cells, numbered x fastest (the reference's type-2 infodom
+    layout, alloc_dom.for:466-477)."""
+    ext = []
+    for k in range(nblk[2]):
+        for j in range(nblk[1]):
+            for i in range(nblk[0]):
+                ext.append((i * n[0], (i + 1) * n[0], j * n[1], (j + 1) * n[1], k * n[2], (k + 1) * n[2]))
+    return np.array(ext, dtype=np.int32)
+
+
+def gap_extents(sizes: Sequence[Sequence[int]]) -> np.ndarray:
+    """Extents of blocks laid out along x with a one-cell gap between
+    neighbours, so no two blocks share a face, edge or corner."""
+    ext = []
+    x = 0
+    for s in sizes:
+        ext.append((x, x + s[0], 0, s[1], 0, s[2]))
+        x += s[0] + 1
+    return np.array(ext, dtype=np.int32)
+
+
+def from_extents(ext: np.ndarray, bc: Sequence[int], h: Sequence[float], ngrid: int, pl: int = 1,
+                 resolve=None):
+    """Descriptors for blocks with integer extents ext[b] = (xs, xe, ys, ye, zs, ze).
+
+    Neighbours are found by the library's h3d_topology; `resolve(ext, bc, h,
+    ngrid)`, if given, is called instead and must return descriptors with the
+    h3d_block_desc layout."""
     ext = np.ascontiguousarray(ext, dtype=np.int32).reshape(-1, 6)
     nb = ext.shape[0]
+    if resolve is not None:
+        out = resolve(ext, bc, h, ngrid)
+        for d in out:
+            d.pl = pl
+            for a in range(3):
+                d.ttc[a] = d.n[a] + 2 * pl
+        return list(out)
     bcv = np.ascontiguousarray(bc, dtype=np.int32)
     hv = np.ascontiguousarray(h, dtype=np.float64)
     out = (_lib.BlockDesc * nb)()
@@ -35,24 +70,13 @@ def from_extents(ext: np.ndarray, bc: Sequence[int], h: Sequence[float], ngrid: 
 
 
 def block_grid(nblk: Sequence[int], n: Sequence[int], bc: Sequence[int], h: Sequence[float], ngrid: int,
-               pl: int = 1):
-    """A regular nblk[0] x nblk[1] x nblk[2] arrangement of equal blocks of n cells.
-
-    Blocks are numbered x fastest (as the reference's type-2 infodom layout,
-    alloc_dom.for:466-477)."""
-    ext = []
-    for k in range(nblk[2]):
-        for j in range(nblk[1]):
-            for i in range(nblk[0]):
-                ext.append((i * n[0], (i + 1) * n[0], j * n[1], (j + 1) * n[1], k * n[2], (k + 1) * n[2]))
-    return from_extents(np.array(ext), bc, h, ngrid, pl)
+               pl: int = 1, resolve=None):
+    """A regular nblk[0] x nblk[1] x nblk[2] arrangement of equal blocks of n
+    cells, numbered x fastest (alloc_dom.for:466-477)."""
+    return from_extents(grid_extents(nblk, n), bc, h, ngrid, pl, resolve)
 
 
-def independent_blocks(sizes: Sequence[Sequence[int]], h: Sequence[float], ngrid: int, pl: int = 1):
+def independent_blocks(sizes: Sequence[Sequence[int]], h: Sequence[float], ngrid: int, pl: int = 1,
+                       resolve=None):
     """Blocks that do not touch (each an isolated all-wall Poisson problem)."""
-    ext = []
-    x = 0
-    for s in sizes:
-        ext.append((x, x + s[0], 0, s[1], 0, s[2]))
-        x += s[0] + 1  # a one-cell gap: no face, edge or corner contact
-    return from_extents(np.array(ext), [WALL] * 6, h, ngrid, pl)
+    return from_extents(gap_extents(sizes), [WALL] * 6, h, ngrid, pl, resolve)

@@ -272,9 +272,10 @@ void or_put_phi(or_mg* m, int g, int ib, const double* a) {
   int ni, nj, nk;
   lev_dims(d, g, &ni, &nj, &nk);
   int64_t nij = (int64_t)ni * nj, nijk = d->faz[g] - (int64_t)ni * nj * nk;
+#pragma omp parallel for num_threads(g_threads) schedule(static) if (g_threads > 1)
   for (int k = 1; k <= nk; ++k)
-    for (int j = 1; j <= nj; ++j)
-      for (int i = 1; i <= ni; ++i)
+    for (int i = 1; i <= ni; ++i)
+      for (int j = 1; j <= nj; ++j)
         d->cof[PHI(i, j, k)] = a[((int64_t)(k - 1) * nj + (j - 1)) * ni + (i - 1)];
 }
 
@@ -283,6 +284,7 @@ void or_get_phi(const or_mg* m, int g, int ib, double* a) {
   int ni, nj, nk;
   lev_dims(d, g, &ni, &nj, &nk);
   int64_t nij = (int64_t)ni * nj, nijk = d->faz[g] - (int64_t)ni * nj * nk;
+#pragma omp parallel for num_threads(g_threads) schedule(static) if (g_threads > 1)
   for (int k = 1; k <= nk; ++k)
     for (int j = 1; j <= nj; ++j)
       for (int i = 1; i <= ni; ++i)
@@ -298,6 +300,7 @@ void or_get_coef(const or_mg* m, int g, int ib, int s, double* a) {
   int ni, nj, nk;
   lev_dims(d, g, &ni, &nj, &nk);
   int64_t incr = (int64_t)(ni - 2) * (nj - 2) * (nk - 2);
+#pragma omp parallel for num_threads(g_threads) schedule(static) if (g_threads > 1)
   for (int k = 2; k <= nk - 1; ++k)
     for (int j = 2; j <= nj - 1; ++j)
       for (int i = 2; i <= ni - 1; ++i)
@@ -310,9 +313,10 @@ void or_put_rhs(or_mg* m, int g, int ib, const double* a) {
   int ni, nj, nk;
   lev_dims(d, g, &ni, &nj, &nk);
   int64_t incr = (int64_t)(ni - 2) * (nj - 2) * (nk - 2);
+#pragma omp parallel for num_threads(g_threads) schedule(static) if (g_threads > 1)
   for (int k = 2; k <= nk - 1; ++k)
-    for (int j = 2; j <= nj - 1; ++j)
-      for (int i = 2; i <= ni - 1; ++i)
+    for (int i = 2; i <= ni - 1; ++i)
+      for (int j = 2; j <= nj - 1; ++j)
         d->cof[cofidx(d, g, ni, nj, i, j, k) + 7 * incr] =
             a[((int64_t)(k - 2) * (nj - 2) + (j - 2)) * (ni - 2) + (i - 2)];
 }
@@ -599,6 +603,10 @@ void or_exchbc_mgpp(or_mg* m, int g) { /* exchangepp.for:2837-3454 */
 
 /* ---------------------------------------------------------------- mgrelax */
 static void relax_block_rbgs(or_dom* d, int g, int colour) {
+  /* One colour pass of mgsolver.for:553-578 / :580-605.  Cells of one colour
+   * do not read each other, so the pass is evaluated plane by plane in
+   * storage order (j fastest, every second j); each cell's arithmetic is the
+   * reference's. */
   int ni, nj, nk;
   lev_dims(d, g, &ni, &nj, &nk);
   int64_t nij = (int64_t)ni * nj, nijk = d->faz[g] - (int64_t)ni * nj * nk;
@@ -607,9 +615,8 @@ static void relax_block_rbgs(or_dom* d, int g, int colour) {
   int64_t faz = d->faz[g];
 #pragma omp parallel for num_threads(g_threads) schedule(static) if (g_threads > 1)
   for (int k = 2; k <= nk - 1; ++k)
-    for (int j = 2; j <= nj - 1; ++j)
-      for (int i = 2; i <= ni - 1; ++i) {
-        if ((i + j + k) % 2 != colour) continue;
+    for (int i = 2; i <= ni - 1; ++i)
+      for (int j = 2 + ((i + 2 + k + colour) & 1); j <= nj - 1; j += 2) {
         int64_t ijkphi = PHI(i, j, k);
         int64_t w = faz + (k - 2) * nij2 + (int64_t)(i - 2) * (nj - 2) + (j - 1);
         c[ijkphi] = (c[w + 7 * incr] -
@@ -739,8 +746,8 @@ void or_mgrestr(or_mg* m, int glevel) { /* mgsolver.for:623-766 */
     int64_t incr_c = nijc2 * (nkc - 2);
     {
       int64_t base = d->faz[glevel] - (int64_t)nic * njc * nkc;
-      for (int64_t q = 1; q <= (int64_t)nic * njc * nkc; ++q) d->cof[base + q] = 0.0; /* :655-662 */
-      for (int64_t q = 0; q < incr_c; ++q) d->cof[d->faz[glevel] + 1 + q + 7 * incr_c] = 0.0; /* :664-672 */
+      memset(d->cof + base + 1, 0, sizeof(double) * (size_t)nic * njc * nkc);       /* :655-662 */
+      memset(d->cof + d->faz[glevel] + 1 + 7 * incr_c, 0, sizeof(double) * (size_t)incr_c); /* :664-672 */
     }
     int nif, njf, nkf;
     int clamp = glevel > d->ngrid;
@@ -772,6 +779,7 @@ void or_mgrestr(or_mg* m, int glevel) { /* mgsolver.for:623-766 */
                            c[w + 6 * incr_f] * c[p]);
         }
     double* cw = d->cof;
+#pragma omp parallel for num_threads(g_threads) schedule(static) if (g_threads > 1)
     for (int k = 2; k <= nkc - 1; ++k)
       for (int i = 2; i <= nic - 1; ++i)
         for (int j = 2; j <= njc - 1; ++j) {
@@ -916,9 +924,12 @@ double or_residual(or_mg* m, double* const* p, const double* const* b,
     int64_t nij2 = (int64_t)(ni - 2) * (nj - 2), incr = nij2 * (nk - 2);
     const double* c = d->cof;
     double dv = d->d.h[0] * d->d.h[1] * d->d.h[2];
-    double brr = 0.0, bbb = 0.0, bmax = 0.0;
-#pragma omp parallel for num_threads(g_threads) schedule(static) reduction(+ : brr, bbb) reduction(max : bmax) if (g_threads > 1)
-    for (int k = 2; k <= nk - 1; ++k)
+    /* per-plane partial sums, added in plane order: the result does not
+     * depend on the thread count */
+    double* part = (double*)calloc((size_t)3 * nk, sizeof(double));
+#pragma omp parallel for num_threads(g_threads) schedule(static) if (g_threads > 1)
+    for (int k = 2; k <= nk - 1; ++k) {
+      double brr = 0.0, bbb = 0.0, bmax = 0.0;
       for (int j = 2; j <= nj - 1; ++j)
         for (int i = 2; i <= ni - 1; ++i) {
           int64_t ph = PHI(i, j, k);
@@ -932,11 +943,18 @@ double or_residual(or_mg* m, double* const* p, const double* const* b,
           brr += rv * rv;
           bbb += bv * bv;
           double a = fabs(rv) * dv;
-          if (a > bmax) bmax = a;
+          if (!(a <= bmax)) bmax = a; /* keeps a NaN */
         }
-    rr += brr;
-    bb += bbb;
-    if (bmax > rmax) rmax = bmax;
+      part[3 * k - 3] = brr;
+      part[3 * k - 2] = bbb;
+      part[3 * k - 1] = bmax;
+    }
+    for (int k = 2; k <= nk - 1; ++k) {
+      rr += part[3 * k - 3];
+      bb += part[3 * k - 2];
+      if (!(part[3 * k - 1] <= rmax)) rmax = part[3 * k - 1];
+    }
+    free(part);
   }
   if (bnorm2) *bnorm2 = bb;
   if (rinf) *rinf = rmax;
