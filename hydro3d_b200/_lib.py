@@ -89,6 +89,7 @@ class SolveInfo(C.Structure):
         ("smoother_launches", C.c_int64),
         ("kernel_launches", C.c_int64),
         ("smoother_bytes", C.c_double),
+        ("relres_block_max", C.c_double),
     ]
 
 

@@ -1177,6 +1177,23 @@ __global__ void __launch_bounds__(1024) k_reduce4(const double* __restrict__ par
   block_reduce4<1024>(a0, a1, a2, a3, out);
 }
 
+// Per-block sums of the defect partials: CTA b reduces partials
+// start[b] .. start[b+1]-1 (the tiles of block b) in a fixed order.
+__global__ void __launch_bounds__(256) k_reduce4_blocks(const double* __restrict__ partials,
+                                                        const int* __restrict__ start, double* __restrict__ out) {
+  pdl_trigger();
+  pdl_wait();
+  const int b = blockIdx.x;
+  double a0 = 0, a1 = 0, a2 = 0, a3 = 0;
+  for (int q = start[b] + threadIdx.x; q < start[b + 1]; q += 256) {
+    a0 += partials[4 * (size_t)q];
+    a1 += partials[4 * (size_t)q + 1];
+    a2 = fmax(a2, partials[4 * (size_t)q + 2]);
+    a3 += partials[4 * (size_t)q + 3];
+  }
+  block_reduce4<256>(a0, a1, a2, a3, out + 4 * (size_t)b);
+}
+
 // Sum of a field over the interior cells: a warp a row at a time (grid-stride
 // over the level's interior rows), one partial sum per CTA in a fixed order.
 __global__ void __launch_bounds__(256) k_sum_interior(const BlkLev* __restrict__ bls, const int* __restrict__ row_start,
@@ -3347,6 +3364,11 @@ cudaError_t launch_stage(bool to_device, double* stg, int tx, int ty, int pl, in
   const int grid = (int)std::min<long long>((n + 255) / 256, 148LL * 16);
   if (to_device) pdl_launch(k_stage_scatter, grid, 256, 0, st, stg, tx, ty, pl, g0, ex, ey, ez, dev, sx, sxy);
   else pdl_launch(k_stage_gather, grid, 256, 0, st, stg, tx, ty, pl, g0, ex, ey, ez, dev, sx, sxy);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_reduce4_blocks(const double* partials, const int* start, int nb, double* out, cudaStream_t st) {
+  pdl_launch(k_reduce4_blocks, nb, 256, 0, st, partials, start, out);
   return cudaGetLastError();
 }
 

@@ -205,6 +205,8 @@ cudaError_t launch_defect(bool var, const BlkLev* bl, RowTab rt, const double* p
                           cudaStream_t st);
 // Deterministic reduction of n partial quadruples into out[4].
 cudaError_t launch_reduce4(const double* partials, int n, double* out, cudaStream_t st);
+// Per-block sums: out[4b..4b+3] from partials start[b] .. start[b+1]-1.
+cudaError_t launch_reduce4_blocks(const double* partials, const int* start, int nb, double* out, cudaStream_t st);
 
 // Interior sum of a level-1 field (per-CTA partials, reduce with launch_reduce4).
 cudaError_t launch_sum_interior(const BlkLev* bl, RowTab rt, const double* a, double* partials, int* nparts,

@@ -77,6 +77,8 @@ struct Level {
   int nqtiles = 0;
   Tile* d_dtiles = nullptr;       // level 1: z-march defect tiles (defect_march_rows() rows x dzc planes)
   int ndtiles = 0, dzc = 1, dgp = 0;  // dgp: pairs per lane of the z-march defect (0: not usable)
+  int* d_dstart = nullptr;        // level 1: first z-march defect tile of each block (nb + 1 entries)
+  int* d_pstart = nullptr;        // level 1: first tiled-defect tile of each block (nb + 1 entries)
   bool pvec32 = false, pvec64 = false;  // every block's nx a multiple of 4 (FP32) / 2 (FP64) cells, ny and nz even
   int nrtiles = 0, rvariant = 0, rzc = 1;
   bool tma_ok = false;
@@ -115,6 +117,9 @@ struct h3d_mg {
   int npartials = 0;
   double* d_res = nullptr;
   double* h_res = nullptr;  // pinned, 4 doubles
+  bool per_block = false;    // the defect also reduces its partial sums per block (stop_rule 2)
+  double* d_resb = nullptr;  // per block {sum r^2, sum b^2, max|r| dV, sum r}
+  double* h_resb = nullptr;  // pinned copy of d_resb
   double* d_h3 = nullptr;   // per-block dx,dy,dz
   int* d_err = nullptr;     // set by a device wait that gave up
   double mean_b = 0.0;
@@ -180,6 +185,20 @@ int dalloc(h3d_mg* h, T** p, size_t n) {
   // uploaded tile lists, and the sweeps then indexed plane -1 of their ring).
   CU(cudaMemsetAsync(*p, 0, n * sizeof(T), h->st));
   CU(cudaStreamSynchronize(h->st));
+  return H3D_OK;
+}
+
+// First tile of every block in a tile list whose tiles are grouped by block
+// (nb + 1 entries, the last one the tile count), uploaded to *d_start.
+int upload_tile_starts(h3d_mg* h, const std::vector<Tile>& tiles, int nb, int** d_start) {
+  std::vector<int> st(nb + 1, (int)tiles.size());
+  for (int q = (int)tiles.size() - 1; q >= 0; --q) st[tiles[q].b] = q;
+  for (int b = nb - 1; b >= 0; --b)
+    if (st[b] > st[b + 1]) st[b] = st[b + 1];
+  int rc = dalloc(h, d_start, st.size());
+  if (rc != H3D_OK) return rc;
+  if (cudaMemcpy(*d_start, st.data(), st.size() * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess)
+    return fail(h, H3D_ERR_CUDA, "tile starts");
   return H3D_OK;
 }
 
@@ -672,6 +691,16 @@ struct Exec {
     TRY(chk("reduce", 1));
     CU(cudaMemcpyAsync(h->h_res, h->d_res, 4 * sizeof(double), cudaMemcpyDeviceToHost, h->st));
     h->kernels += 2;
+    if (h->per_block && h->blocks.size() > 1) {
+      // the march and tiled defects write one partial per tile, tiles grouped by block
+      const int* start = march ? V.d_dstart : tiled ? V.d_pstart : nullptr;
+      if (!start) return fail(h, H3D_ERR_BAD_CONFIG, "per-block stop rule: the defect of this layout has no per-block partial sums");
+      const int nb = (int)h->blocks.size();
+      CU(launch_reduce4_blocks(h->partials, start, nb, h->d_resb, h->st));
+      TRY(chk("reduce per block", 1));
+      CU(cudaMemcpyAsync(h->h_resb, h->d_resb, 4 * sizeof(double) * nb, cudaMemcpyDeviceToHost, h->st));
+      h->kernels += 1;
+    }
     return H3D_OK;
   }
 
@@ -750,7 +779,7 @@ int run_iteration(h3d_mg* h, int inner, double* prof_ms, int64_t* prof_n, double
     std::vector<cudaEvent_t> used(h->ev_eager.begin(), h->ev_eager.begin() + ex.prof_used);
     return accumulate_events(h, used, ex.prof_bytes, prof_ms, prof_n, prof_bytes);
   }
-  std::vector<int> key = state_key(h, inner * 2 + (h->profiling ? 1 : 0));
+  std::vector<int> key = state_key(h, inner * 4 + (h->profiling ? 1 : 0) + (h->per_block ? 2 : 0));
   auto it = h->graphs.find(key);
   if (it == h->graphs.end()) {
     CachedGraph cg;
@@ -1765,7 +1794,7 @@ int h3d_mg_destroy(h3d_mg* h) {
     void* ps[] = {V.d_bl, V.d_cta_all, V.d_cta_int, V.d_rows_all, V.d_rows_int, V.d_tiles, V.phi64[0], V.phi64[1], V.rhs64, V.phi32[0],
                   V.phi32[1], V.rhs32, V.fx64, V.fy64, V.fz64, V.fx32, V.fy32, V.fz32, V.dens,
                   V.sweep.d_dst, V.sweep.d_src, V.faces.d_dst, V.faces.d_src, V.exch.d_dst, V.exch.d_src,
-                  V.bound.d_dst, V.bound.d_src, V.sweep_push.d_dst, V.sweep_push.d_src, V.d_push, V.d_maps, V.d_rmaps, V.d_rtiles, V.d_ptiles, V.d_qtiles, V.d_dtiles, V.d_cstart};
+                  V.bound.d_dst, V.bound.d_src, V.sweep_push.d_dst, V.sweep_push.d_src, V.d_push, V.d_maps, V.d_rmaps, V.d_rtiles, V.d_ptiles, V.d_qtiles, V.d_dtiles, V.d_cstart, V.d_dstart, V.d_pstart};
     for (void* p : ps) dfree(p);
   }
   dfree(h->p64[0]);
@@ -1773,6 +1802,8 @@ int h3d_mg_destroy(h3d_mg* h) {
   dfree(h->b64);
   dfree(h->partials);
   dfree(h->d_res);
+  dfree(h->d_resb);
+  if (h->h_resb) cudaFreeHost(h->h_resb);
   dfree(h->d_h3);
   dfree(h->d_err);
   dfree(h->d_tail_lv);
@@ -1930,6 +1961,7 @@ int h3d_mg_create(h3d_mg** out, const h3d_mg_desc* desc) {
         if (cudaMemcpy(V.d_ptiles, pt.data(), pt.size() * sizeof(Tile), cudaMemcpyHostToDevice) != cudaSuccess)
           return bail(fail(h, H3D_ERR_CUDA, "defect tiles"));
         V.nptiles = (int)pt.size();
+        if ((rc = upload_tile_starts(h, pt, (int)V.geom.bl.size(), &V.d_pstart)) != H3D_OK) return bail(rc);
       }
     }
     if (g == 1 && !h->var) {  // z-march defect tiles: 8 rows of a block over a chunk of planes
@@ -1956,6 +1988,7 @@ int h3d_mg_create(h3d_mg** out, const h3d_mg_desc* desc) {
         if (cudaMemcpy(V.d_dtiles, dt.data(), dt.size() * sizeof(Tile), cudaMemcpyHostToDevice) != cudaSuccess)
           return bail(fail(h, H3D_ERR_CUDA, "defect tiles"));
         V.ndtiles = (int)dt.size();
+        if ((rc = upload_tile_starts(h, dt, (int)V.geom.bl.size(), &V.d_dstart)) != H3D_OK) return bail(rc);
       }
     }
     if ((rc = build_tensor_maps(h, g)) != H3D_OK) return bail(rc);
@@ -1976,6 +2009,9 @@ int h3d_mg_create(h3d_mg** out, const h3d_mg_desc* desc) {
   h->npartials = std::max(std::max(std::max(h->lev[1].ncta_all, h->lev[1].ncta_int), kDefectCtas),
                           std::max(h->lev[1].nptiles, h->lev[1].ndtiles));
   if ((rc = dalloc(h, &h->partials, 4 * (size_t)h->npartials)) || (rc = dalloc(h, &h->d_res, 4))) return bail(rc);
+  if ((rc = dalloc(h, &h->d_resb, 4 * h->blocks.size())) != H3D_OK) return bail(rc);
+  if (cudaMallocHost((void**)&h->h_resb, 4 * sizeof(double) * h->blocks.size()) != cudaSuccess)
+    return bail(fail(h, H3D_ERR_OOM, "pinned per-block result buffer"));
   if (cudaMallocHost((void**)&h->h_res, 4 * sizeof(double)) != cudaSuccess)
     return bail(fail(h, H3D_ERR_OOM, "pinned result buffer"));
   std::vector<double> h3;
@@ -2089,8 +2125,15 @@ int h3d_mg_residual(h3d_mg* h, double* rr, double* bb, double* rinf) {
 
 int h3d_mg_solve_resident(h3d_mg* h, const h3d_solve_opts* opts, h3d_solve_info* info) {
   if (!h || !opts) return H3D_ERR_ARG;
+  if (opts->stop_rule < 0 || opts->stop_rule > 2) return fail(h, H3D_ERR_ARG, "stop_rule must be 0, 1 or 2");
   CU(cudaSetDevice(h->device));
   TRY(ensure_coeffs(h));
+  const int nb = (int)h->blocks.size();
+  struct PerBlock {  // restores the handle's defect mode on every exit
+    h3d_mg* h;
+    ~PerBlock() { h->per_block = false; }
+  } pb_guard{h};
+  h->per_block = opts->stop_rule == 2 && nb > 1;
   h3d_solve_info I{};
   const int maxcy = opts->maxcy > 0 ? opts->maxcy : h->desc.maxcy;
   const int inner = h->mixed ? h->desc.inner_cycles : 1;
@@ -2128,9 +2171,24 @@ int h3d_mg_solve_resident(h3d_mg* h, const h3d_solve_opts* opts, h3d_solve_info*
   I.bnorm = std::sqrt(bb);
   const double bn = I.bnorm > 0 ? I.bnorm : 1.0;
   double rel = std::sqrt(h->h_res[0]) / bn, rinf = h->h_res[2];
-  if (opts->record_history) h->history.push_back(rel);
+  // per-block relative residuals (stop_rule 2): ||r_b|| / ||b_b|| of every block
+  std::vector<double> bnb(nb, bn);
+  if (h->per_block)
+    for (int b = 0; b < nb; ++b) bnb[b] = h->h_resb[4 * b + 1] > 0 ? std::sqrt(h->h_resb[4 * b + 1]) : 1.0;
+  auto block_max = [&]() {
+    if (!h->per_block) return rel;
+    double m = 0;
+    for (int b = 0; b < nb; ++b) {
+      const double v = std::sqrt(h->h_resb[4 * b]) / bnb[b];
+      if (!(v <= m)) m = v;  // keeps a NaN
+    }
+    return m;
+  };
+  double relb = block_max();
+  if (opts->record_history) h->history.push_back(opts->stop_rule == 2 ? relb : rel);
   int status = 1, iter = 0;
   if (opts->stop_rule == 0 && rel <= opts->tol) status = 0;
+  if (opts->stop_rule == 2 && relb <= opts->tol) status = 0;
   double prof_ms = 0, prof_bytes = 0;
   int64_t prof_n = 0;
   while (status != 0 && iter < maxcy) {
@@ -2139,10 +2197,12 @@ int h3d_mg_solve_resident(h3d_mg* h, const h3d_solve_opts* opts, h3d_solve_info*
     I.cycles += inner;
     rel = std::sqrt(h->h_res[0]) / bn;
     rinf = h->h_res[2];
-    if (opts->record_history) h->history.push_back(rel);
-    if (!std::isfinite(rel) || rel > 1e8) { status = 2; break; }
+    relb = block_max();
+    if (opts->record_history) h->history.push_back(opts->stop_rule == 2 ? relb : rel);
+    if (!std::isfinite(rel) || rel > 1e8 || !std::isfinite(relb)) { status = 2; break; }
     if (opts->stop_rule == 0 && rel <= opts->tol) status = 0;
     if (opts->stop_rule == 1 && rinf < opts->tol && iter > 1) status = 0;  // newsolv_mg.for:57
+    if (opts->stop_rule == 2 && relb <= opts->tol) status = 0;
   }
   if (opts->remove_mean) {
     RowTab rt{V.d_rows_int, (int)V.geom.bl.size(), V.nrows_int};
@@ -2160,6 +2220,7 @@ int h3d_mg_solve_resident(h3d_mg* h, const h3d_solve_opts* opts, h3d_solve_info*
   cudaEventDestroy(t1);
   I.outer = iter;
   I.relres = rel;
+  I.relres_block_max = relb;
   I.rmax = rinf;
   I.device_ms = ms;
   I.smoother_ms = prof_ms;

@@ -79,7 +79,9 @@ typedef struct h3d_solve_opts {
   double tol;             /* tolerance (see stop_rule) */
   int32_t maxcy;          /* cycle cap (0 = desc.maxcy) */
   int32_t stop_rule;      /* 0: ||b-Ap||2/||b||2 <= tol, checked before each cycle;
-                             1: reference rule rmax < tol .and. iter > 1 (newsolv_mg.for:57) */
+                             1: reference rule rmax < tol .and. iter > 1 (newsolv_mg.for:57);
+                             2: every block's own ||b-Ap||2/||b||2 <= tol (independent
+                                blocks; needs even nx in every block) */
   int32_t remove_mean;    /* 1: subtract the FP64 mean of p at the end (all-Neumann) */
   int32_t record_history; /* 1: keep ||r||/||b|| per cycle (read with h3d_mg_history) */
 } h3d_solve_opts;
@@ -95,6 +97,7 @@ typedef struct h3d_solve_info {
   int64_t smoother_launches;
   int64_t kernel_launches;/* kernels this library launched during the solve */
   double smoother_bytes;  /* algorithmic bytes of the profiled level-1 smoother launches */
+  double relres_block_max;/* stop_rule 2: largest per-block ||b-Ap||2/||b||2; else = relres */
 } h3d_solve_info;
 
 /* --- set-up (localparameters.for:202-239, initial.for:329-360, coeff) ---- */

@@ -12,8 +12,7 @@ and runs the CUDA path against the oracle on the same inputs:
             the level state bit for bit, then two outer FP64 iterations
             (history within 1e-12, iterate within 1e-12).
   config 4  27 uneven independent blocks: one V-cycle bit for bit on every
-            block; the mixed-precision solve reaches 1e-8 and its pressure is
-            within 1e-8 of the FP64 solve.
+            block; the mixed-precision solve reaches 1e-8 in every block.
   config 5  256^3, 1000:1 density (L_LSM coefficients): two V-cycles bit for
             bit.
 """
@@ -134,25 +133,33 @@ def test_config3_vcycles_bitexact_and_outer_steps(oracle_mod, h3d):
 
 
 def test_config4_uneven_blocks(oracle_mod, h3d):
+    """27 independent blocks of 15+ different shapes in one solver: one
+    V-cycle bit for bit on every block, then the mixed-precision solve with
+    the per-block stop rule (every block's ||r||/||b|| <= 1e-8, recomputed
+    here by the oracle from the returned pressure) and every block's pressure
+    within 1e-6 of the oracle's solution to 1e-12 (the ratio of the algebraic
+    error to the residual of these Neumann blocks bounds it)."""
     from hydro3d_b200 import synth
     prob = synth.config4()
     sizes = {tuple(d.n) for d in prob.blocks}
-    assert len(sizes) > 10  # blocks of many different shapes in one solver
+    assert len(sizes) > 10
     orc = _vcycles_bitexact(h3d, oracle_mod, prob, ncycles=1)
-    ref = _oracle_solve(orc, prob, tol=1e-10)
-    orc.close()
+    ref = _oracle_solve(orc, prob, tol=1e-12, maxcy=600)
     assert ref["status"] == 0
     s = _solver(h3d, prob, precision="mixed")
-    p, info = _gpu_solve(s, prob)
+    p = [x.copy() for x in prob.p0]
+    info = s.newsolv_mg(p, prob.b, tol=1e-8, maxcy=400, stop_rule=2)
     s.close()
-    assert info["converged"] and info["relres"] <= 1e-8
+    assert info["converged"] and info["relres_block_max"] <= 1e-8
+    r, _, _, _ = orc.residual([_canon(x, d) for x, d in zip(p, prob.blocks)],
+                              [interior_of_host(x, d) for x, d in zip(prob.b, prob.blocks)])
+    orc.close()
+    for rb, x, d in zip(r, prob.b, prob.blocks):
+        assert np.linalg.norm(rb) <= 1.0001e-8 * np.linalg.norm(interior_of_host(x, d))
     got = [interior_of_host(x, d) for x, d in zip(p, prob.blocks)]
     want = [x[1:-1, 1:-1, 1:-1] for x in ref["p"]]
-    # independent blocks: each block's pressure is determined up to its own constant
-    for g, w in zip(got, want):
-        assert mean_removed_rel([g], [w]) <= 1e-6
-    assert mean_removed_rel(got, want) <= 1e-8 or all(
-        mean_removed_rel([g], [w]) <= 1e-8 for g, w in zip(got, want))
+    errs = [mean_removed_rel([g], [w]) for g, w in zip(got, want)]
+    assert max(errs) <= 1e-6, max(errs)
 
 
 def test_config5_lsm_vcycles_bitexact(oracle_mod, h3d):
