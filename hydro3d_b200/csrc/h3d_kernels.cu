@@ -240,6 +240,294 @@ __global__ void __launch_bounds__(NT) k_rbgs(const BlkLev* __restrict__ bls, con
 }
 
 
+// ---------------------------------------------------------------------------
+// First red-black sweep from a zero iterate (FP32, constant coefficients) as
+// a stencil on the right-hand side.  With a zero source every red cell only
+// sees black neighbours that are still zero, so red = rhs * (1/ap); a black
+// cell sees red neighbours, each rhs_nb * (1/ap_nb) inside the block and zero
+// outside it (the ghosts of a zero iterate).  These are the exact FP32
+// operations of the TMA window sweep in its zero-source mode (same products,
+// same fused multiply-add chain), evaluated without its plane ring and
+// per-plane barriers: a thread owns one 4-cell group of one row and marches a
+// chunk of planes, keeping the group's right-hand side of planes z-1, z, z+1
+// in registers; rows y+-1 and the two cells beside the group come from L1.
+// 1/ap of a cell depends only on which wall faces it touches: a 64-entry
+// table per CTA.  Ghost pushes as in the window sweep.
+__global__ void __launch_bounds__(256) k_rbgs_zero32(const BlkLev* __restrict__ bls, const Tile* __restrict__ tiles,
+                                                     int zc, const float* __restrict__ rhs, float* __restrict__ dst,
+                                                     const long long* __restrict__ push) {
+  pdl_trigger();
+  __shared__ float ivtab[64];
+  const Tile t = tiles[blockIdx.x];
+  const BlkLev B = bls[t.b];
+  const int nx = B.nx, ny = B.ny, nz = B.nz, ph = B.phys;
+  const float ax = (float)B.ax, ay = (float)B.ay, az = (float)B.az;
+  if (threadIdx.x < 64) {
+    const int m = threadIdx.x;
+    const float aw = (m & 1) ? 0.f : ax, ae = (m & 2) ? 0.f : ax, as = (m & 4) ? 0.f : ay, an = (m & 8) ? 0.f : ay,
+                ab = (m & 16) ? 0.f : az, at = (m & 32) ? 0.f : az;
+    ivtab[m] = 1.f / (-(aw + ae + as + an + ab + at));
+  }
+  __syncthreads();
+  pdl_wait();
+  const int G = nx >> 2;           // groups per row
+  const int rows = blockDim.x / G;  // rows of this tile
+  const int r = threadIdx.x / G, g = threadIdx.x - r * G;
+  const int y = t.y0 + r;
+  if (r >= rows || y > ny) return;
+  const int x0 = 1 + 4 * g;
+  const long long sx = B.sx, sxy = B.sxy;
+  const float* __restrict__ R = rhs + B.off;
+  float* __restrict__ D = dst + B.off;
+  const int zs = t.z0, ze = min(t.z0 + zc - 1, nz);
+  // wall mask of a cell (only faces that are physical walls count)
+  auto wmask = [&](int x, int yy, int z) {
+    return ph & ((x == 1 ? 1 : 0) | (x == nx ? 2 : 0) | (yy == 1 ? 4 : 0) | (yy == ny ? 8 : 0) | (z == 1 ? 16 : 0) |
+                 (z == nz ? 32 : 0));
+  };
+  long long pd[6];
+#pragma unroll
+  for (int f = 0; f < 6; ++f) pd[f] = push ? __ldg(push + 6 * t.b + f) : kNoPush;
+  const bool pxw = x0 == 1 && pd[0] != kNoPush, pxe = x0 + 3 == nx && pd[1] != kNoPush;
+  const bool pys = y == 1 && pd[2] != kNoPush, pyn = y == ny && pd[3] != kNoPush;
+  auto ld4 = [](const float* p) { return *reinterpret_cast<const float4*>(p); };
+  const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f);
+  const long long row = (long long)y * sx + x0;
+  float4 hb = zs > 1 ? ld4(R + (long long)(zs - 1) * sxy + row) : zero4;
+  float4 hz = ld4(R + (long long)zs * sxy + row);
+  for (int z = zs; z <= ze; ++z) {
+    const long long o = (long long)z * sxy + row;
+    const float4 ht = z < nz ? ld4(R + o + sxy) : zero4;
+    const float4 hs = y > 1 ? ld4(R + o - sx) : zero4;
+    const float4 hn = y < ny ? ld4(R + o + sx) : zero4;
+    const float rl = x0 > 1 ? R[o - 1] : 0.f;
+    const float rr = x0 + 4 <= nx ? R[o + 4] : 0.f;
+    const float hzv[4] = {hz.x, hz.y, hz.z, hz.w};
+    const float hbv[4] = {hb.x, hb.y, hb.z, hb.w};
+    const float htv[4] = {ht.x, ht.y, ht.z, ht.w};
+    const float hsv[4] = {hs.x, hs.y, hs.z, hs.w};
+    const float hnv[4] = {hn.x, hn.y, hn.z, hn.w};
+    float out[4];
+    const int par = (x0 + y + z) & 1;  // cell k is red when (x0 + k + y + z) is odd
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int x = x0 + k;
+      const int m = wmask(x, y, z);
+      const float iv = ivtab[m];
+      if (((par + k) & 1) == 1) {
+        out[k] = hzv[k] * iv;
+      } else {
+        // red neighbours (zero outside the block's interior)
+        const float w = k > 0 ? hzv[k - 1] * ivtab[wmask(x - 1, y, z)] : (x0 > 1 ? rl * ivtab[wmask(x - 1, y, z)] : 0.f);
+        const float e = k < 3 ? hzv[k + 1] * ivtab[wmask(x + 1, y, z)] : (x + 1 <= nx ? rr * ivtab[wmask(x + 1, y, z)] : 0.f);
+        const float sv = y > 1 ? hsv[k] * ivtab[wmask(x, y - 1, z)] : 0.f;
+        const float nv = y < ny ? hnv[k] * ivtab[wmask(x, y + 1, z)] : 0.f;
+        const float bv = z > 1 ? hbv[k] * ivtab[wmask(x, y, z - 1)] : 0.f;
+        const float tv = z < nz ? htv[k] * ivtab[wmask(x, y, z + 1)] : 0.f;
+        const float aw = (m & 1) ? 0.f : ax, ae = (m & 2) ? 0.f : ax, as = (m & 4) ? 0.f : ay,
+                    an = (m & 8) ? 0.f : ay, ab = (m & 16) ? 0.f : az, at = (m & 32) ? 0.f : az;
+        const float sum = fmaf(at, tv, fmaf(ab, bv, fmaf(an, nv, fmaf(as, sv, fmaf(ae, e, aw * w)))));
+        out[k] = (hzv[k] - sum) * iv;
+      }
+    }
+    const float4 v = make_float4(out[0], out[1], out[2], out[3]);
+    float* q = D + o;
+    *reinterpret_cast<float4*>(q) = v;
+    if (pxw) q[pd[0]] = v.x;
+    if (pxe) q[3 + pd[1]] = v.w;
+    if (pys) *reinterpret_cast<float4*>(q + pd[2]) = v;
+    if (pyn) *reinterpret_cast<float4*>(q + pd[3]) = v;
+    if (z == 1 && pd[4] != kNoPush) *reinterpret_cast<float4*>(q + pd[4]) = v;
+    if (z == nz && pd[5] != kNoPush) *reinterpret_cast<float4*>(q + pd[5]) = v;
+    hb = hz;
+    hz = ht;
+  }
+}
+
+}  // namespace
+
+cudaError_t launch_rbgs_zero32(const BlkLev* bl, const Tile* tiles, int ntiles, int zc, const float* rhs, float* dst,
+                               const long long* push, cudaStream_t st) {
+  if (ntiles <= 0) return cudaSuccess;
+  pdl_launch(k_rbgs_zero32, ntiles, 256, 0, st, bl, tiles, zc, rhs, dst, push);
+  return cudaGetLastError();
+}
+
+namespace {
+
+// ---------------------------------------------------------------------------
+// Sequential smoothers of mgrelax on the GPU: lexicographic Gauss-Seidel
+// (mg_itrsch=1, mgsolver.for:407-432) and the line TDMA (mg_itrsch=2,
+// :434-549).  Both are Gauss-Seidel orderings: the reference visits cells
+// (lines) one after another and every cell (line) reads the already updated
+// values of its predecessors.  On the GPU one CTA owns one block; cells
+// (lines) whose predecessors are all done form a wavefront (a hyperplane
+// x+y+z = const of cells, an anti-diagonal of lines) and are updated in
+// parallel, with a CTA barrier between wavefronts, so every value is the
+// one the sequential loop computes, with the reference's operand order.
+// Blocks are independent within a sweep (their ghosts change only in the
+// exchange after it), so blocks run as separate CTAs.  The sweep is out of
+// place like the other smoothers: the CTA first copies its block, ghosts
+// included, from src to dst (zeros for a zero iterate) and then works in
+// place on dst.
+
+// The block's cells, ghosts included, from src (or zeros) into dst.
+template <typename T>
+__device__ __forceinline__ void copy_block(const BlkLev& B, const T* __restrict__ S, T* __restrict__ D, bool zero) {
+  const int ex = B.nx + 2, ey = B.ny + 2, ez = B.nz + 2;
+  const long long n = (long long)ex * ey * ez;
+  for (long long q = threadIdx.x; q < n; q += blockDim.x) {
+    const int x = (int)(q % ex), y = (int)((q / ex) % ey), z = (int)(q / ((long long)ex * ey));
+    const long long i = (long long)z * B.sxy + (long long)y * B.sx + x;
+    D[i] = zero ? T(0) : S[i];
+  }
+}
+
+template <typename T, bool VAR>
+__global__ void __launch_bounds__(512) k_gslex(const BlkLev* __restrict__ bls, const T* __restrict__ src,
+                                               T* __restrict__ dst, const T* __restrict__ rhs,
+                                               const T* __restrict__ fx, const T* __restrict__ fy,
+                                               const T* __restrict__ fz, bool zero) {
+  pdl_trigger();
+  pdl_wait();
+  const BlkLev B = bls[blockIdx.x];
+  T* __restrict__ D = dst + B.off;
+  const T* __restrict__ R = rhs + B.off;
+  const T* FX = VAR ? fx + B.off : nullptr;
+  const T* FY = VAR ? fy + B.off : nullptr;
+  const T* FZ = VAR ? fz + B.off : nullptr;
+  copy_block(B, src + B.off, D, zero);
+  __syncthreads();
+  const int nx = B.nx, ny = B.ny, nz = B.nz;
+  const long long sx = B.sx, sxy = B.sxy;
+  // cell (x, y, z) is in wavefront d = (x-1) + (y-1) + (z-1)
+  for (int d = 0; d <= (nx - 1) + (ny - 1) + (nz - 1); ++d) {
+    const int zmin = max(0, d - (nx - 1) - (ny - 1)), zmax = min(nz - 1, d);
+    const int nzr = zmax - zmin + 1;
+    for (int q = threadIdx.x; q < nzr * ny; q += blockDim.x) {
+      const int z = zmin + q / ny + 1, y = q % ny + 1;
+      const int x = d - (y - 1) - (z - 1) + 1;
+      if (x < 1 || x > nx) continue;
+      const long long i = (long long)z * sxy + (long long)y * sx + x;
+      const Coef<T> c = cell_coef<T, VAR>(B, x, y, z, i, FX, FY, FZ);
+      D[i] = gs_div(R[i] - (c.aw * D[i - 1] + c.ae * D[i + 1] + c.as * D[i - sx] + c.an * D[i + sx] +
+                            c.ab * D[i - sxy] + c.at * D[i + sxy]),
+                    coef_ap(c));
+    }
+    __syncthreads();
+  }
+}
+
+// One TDMA line of the block (AXIS 0: along x at (y, z) = (u, v); 1: along y
+// at (x, z) = (u, v); 2: along z at (x, y) = (u, v)).  Forward elimination
+// keeps the reference's recurrences, apr = 1/(ap - lo*a(s-1)), a(s) = hi*apr,
+// c(s) = (su - <the four cross terms in the reference's order> - lo*c(s-1))*apr,
+// with a(0) = 0 and c(0) the ghost before the line; back substitution
+// phi(s) = c(s) - a(s)*phi(s+1) from the ghost after it.  c(s) is kept in the
+// line's own cell (no other line of the wavefront reads it), a(s) in A.
+template <typename T, bool VAR, int AXIS>
+__device__ __forceinline__ void tdma_line(const BlkLev& B, T* __restrict__ D, T* __restrict__ A,
+                                          const T* __restrict__ R, const T* FX, const T* FY, const T* FZ, int u,
+                                          int v) {
+  const long long sx = B.sx, sxy = B.sxy;
+  const int n = AXIS == 0 ? B.nx : AXIS == 1 ? B.ny : B.nz;
+  const long long st = AXIS == 0 ? 1 : AXIS == 1 ? sx : sxy;
+  long long i = AXIS == 0 ? (long long)v * sxy + (long long)u * sx
+                          : AXIS == 1 ? (long long)v * sxy + u : (long long)v * sx + u;  // position 0
+  T aprev = T(0), cprev = D[i];
+  for (int s = 1; s <= n; ++s) {
+    i += st;
+    const int x = AXIS == 0 ? s : u, y = AXIS == 0 ? u : AXIS == 1 ? s : v, z = AXIS == 2 ? s : v;
+    const Coef<T> c = cell_coef<T, VAR>(B, x, y, z, i, FX, FY, FZ);
+    const T ap = coef_ap(c);
+    T lo, hi, t;
+    if (AXIS == 1) {  // j-lines, mgsolver.for:443-473
+      lo = c.as; hi = c.an;
+      t = R[i] - c.ae * D[i + 1] - c.aw * D[i - 1] - c.at * D[i + sxy] - c.ab * D[i - sxy];
+    } else if (AXIS == 0) {  // i-lines, :476-510
+      lo = c.aw; hi = c.ae;
+      t = R[i] - c.an * D[i + sx] - c.as * D[i - sx] - c.at * D[i + sxy] - c.ab * D[i - sxy];
+    } else {  // k-lines, :513-547
+      lo = c.ab; hi = c.at;
+      t = R[i] - c.an * D[i + sx] - c.as * D[i - sx] - c.ae * D[i + 1] - c.aw * D[i - 1];
+    }
+    const T apr = gs_div(T(1), ap - lo * aprev);
+    aprev = hi * apr;
+    cprev = (t - lo * cprev) * apr;
+    A[i] = aprev;
+    D[i] = cprev;
+  }
+  T nxt = D[i + st];
+  for (int s = n; s >= 1; --s) {
+    nxt = D[i] - A[i] * nxt;
+    D[i] = nxt;
+    i -= st;
+  }
+}
+
+// One pass of lines along AXIS: the reference runs them with the slower of
+// the two other indices outer (j-lines: k then i; i-lines: k then j; k-lines:
+// i then j), so line (u, v) follows (u-1, v) and (u, v-1): anti-diagonals
+// u + v = const are the wavefronts.
+template <typename T, bool VAR, int AXIS>
+__device__ __forceinline__ void tdma_pass(const BlkLev& B, T* __restrict__ D, T* __restrict__ A,
+                                          const T* __restrict__ R, const T* FX, const T* FY, const T* FZ) {
+  const int nu = AXIS == 0 ? B.ny : B.nx, nv = AXIS == 2 ? B.ny : B.nz;
+  for (int d = 0; d <= (nu - 1) + (nv - 1); ++d) {
+    const int ulo = max(0, d - (nv - 1)), uhi = min(nu - 1, d);
+    for (int u = ulo + (int)threadIdx.x; u <= uhi; u += blockDim.x)
+      tdma_line<T, VAR, AXIS>(B, D, A, R, FX, FY, FZ, u + 1, d - u + 1);
+    __syncthreads();
+  }
+}
+
+template <typename T, bool VAR>
+__global__ void __launch_bounds__(256) k_tdma(const BlkLev* __restrict__ bls, const T* __restrict__ src,
+                                              T* __restrict__ dst, const T* __restrict__ rhs, T* __restrict__ acoef,
+                                              const T* __restrict__ fx, const T* __restrict__ fy,
+                                              const T* __restrict__ fz, bool zero) {
+  pdl_trigger();
+  pdl_wait();
+  const BlkLev B = bls[blockIdx.x];
+  T* __restrict__ D = dst + B.off;
+  T* __restrict__ A = acoef + B.off;
+  const T* __restrict__ R = rhs + B.off;
+  const T* FX = VAR ? fx + B.off : nullptr;
+  const T* FY = VAR ? fy + B.off : nullptr;
+  const T* FZ = VAR ? fz + B.off : nullptr;
+  copy_block(B, src + B.off, D, zero);
+  __syncthreads();
+  tdma_pass<T, VAR, 1>(B, D, A, R, FX, FY, FZ);  // j-lines
+  tdma_pass<T, VAR, 0>(B, D, A, R, FX, FY, FZ);  // i-lines
+  tdma_pass<T, VAR, 2>(B, D, A, R, FX, FY, FZ);  // k-lines
+}
+
+}  // namespace
+
+template <typename T>
+cudaError_t launch_seq_smoother(int itrsch, bool var, bool zero, const BlkLev* bl, int nb, const T* src, T* dst,
+                                const T* rhs, T* acoef, const T* fx, const T* fy, const T* fz, cudaStream_t st) {
+  if (nb <= 0) return cudaSuccess;
+  if (itrsch == 1) {
+    if (var) pdl_launch(k_gslex<T, true>, nb, 512, 0, st, bl, src, dst, rhs, fx, fy, fz, zero);
+    else pdl_launch(k_gslex<T, false>, nb, 512, 0, st, bl, src, dst, rhs, fx, fy, fz, zero);
+  } else {
+    if (var) pdl_launch(k_tdma<T, true>, nb, 256, 0, st, bl, src, dst, rhs, acoef, fx, fy, fz, zero);
+    else pdl_launch(k_tdma<T, false>, nb, 256, 0, st, bl, src, dst, rhs, acoef, fx, fy, fz, zero);
+  }
+  return cudaGetLastError();
+}
+
+template cudaError_t launch_seq_smoother<double>(int, bool, bool, const BlkLev*, int, const double*, double*,
+                                                 const double*, double*, const double*, const double*,
+                                                 const double*, cudaStream_t);
+template cudaError_t launch_seq_smoother<float>(int, bool, bool, const BlkLev*, int, const float*, float*,
+                                                const float*, float*, const float*, const float*, const float*,
+                                                cudaStream_t);
+
+namespace {
+
+
 // Per-thread stencil state of the row-tile smoothers.  A thread's cells are
 // fixed for the whole z march (pair k, member m: x = 2(tc + k*TPR) + 1 + m),
 // so the constant coefficients of mgsolver.for:186-205 are selected once.

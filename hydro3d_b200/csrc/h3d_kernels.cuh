@@ -149,6 +149,17 @@ constexpr int kClusterTailMaxOps = 160;
 cudaError_t launch_coarse_cluster(int nb, const TailLevel* lv, int nlev, const TailOp* ops, int nops,
                                   unsigned curmask, int smem_bytes, cudaStream_t st);
 
+// First red-black sweep from a zero iterate of an FP32 constant-coefficient
+// level (every block's nx a multiple of 4, at most 1024): tiles (block, y0 =
+// first row, z0 = first plane) of 256 / (nx/4) rows and zc planes.
+cudaError_t launch_rbgs_zero32(const BlkLev* bl, const Tile* tiles, int ntiles, int zc, const float* rhs, float* dst,
+                               const long long* push, cudaStream_t st);
+// Lexicographic Gauss-Seidel (itrsch 1) or line-TDMA (itrsch 2) sweep of
+// every block of a level, one CTA per block (bit-exact wavefront orderings
+// of mgsolver.for:407-549); acoef: level-sized scratch of the TDMA.
+template <typename T>
+cudaError_t launch_seq_smoother(int itrsch, bool var, bool zero, const BlkLev* bl, int nb, const T* src, T* dst,
+                                const T* rhs, T* acoef, const T* fx, const T* fy, const T* fz, cudaStream_t st);
 template <typename T>
 cudaError_t launch_relax_small(bool var, const BlkLev* bl, const int* start, int nb, T* phi, const T* rhs,
                                const T* fx, const T* fy, const T* fz, const uint32_t* fdst, const uint32_t* fsrc,

@@ -88,6 +88,10 @@ struct Level {
   bool tailable = false;    // small enough for the fused coarse tail (has d_cstart)
   int cur64 = 0, cur32 = 0;
   bool zero64 = false, zero32 = false;
+  Tile* d_ztiles = nullptr;     // FP32 zero-source sweep tiles (launch_rbgs_zero32), or none
+  int nztiles = 0, zzc = 1;
+  double* seq64 = nullptr;      // line-TDMA scratch a(s) of every cell (mg_itrsch 2)
+  float* seq32 = nullptr;
   double sweep_bytes = 0;       // algorithmic bytes of one sweep (FP64 or FP32 by mode)
   double sweep_bytes_zero = 0;  // ... of a sweep from the zero iterate (the iterate is not read)
 };
@@ -430,6 +434,49 @@ struct Exec {
       CU(record(e0));
       prof_bytes.push_back((mixed_level(g) ? V.zero32 : V.zero64) ? V.sweep_bytes_zero : V.sweep_bytes);
     }
+    if (h->desc.mg_itrsch != 3) {  // lexicographic GS or line TDMA: one CTA per block
+      const int nb = (int)V.geom.bl.size();
+      if (mixed_level(g)) {
+        float* src = V.phi32[V.cur32];
+        float* dst = V.phi32[1 - V.cur32];
+        CU(launch_seq_smoother<float>(h->desc.mg_itrsch, h->var, V.zero32, V.d_bl, nb, src, dst, V.rhs32, V.seq32,
+                                      V.fx32, V.fy32, V.fz32, st));
+        TRY(chk("sequential sweep fp32", g));
+        if (e1) CU(record(e1));
+        CU(launch_fill<float>(V.sweep.d_dst, V.sweep.d_src, V.sweep.n, dst, dst, src, V.zero32, st));
+        TRY(chk("fill fp32", g));
+        V.cur32 = 1 - V.cur32;
+        V.zero32 = false;
+      } else {
+        double* src = V.phi64[V.cur64];
+        double* dst = V.phi64[1 - V.cur64];
+        CU(launch_seq_smoother<double>(h->desc.mg_itrsch, h->var, V.zero64, V.d_bl, nb, src, dst, V.rhs64, V.seq64,
+                                       V.fx64, V.fy64, V.fz64, st));
+        TRY(chk("sequential sweep fp64", g));
+        if (e1) CU(record(e1));
+        CU(launch_fill<double>(V.sweep.d_dst, V.sweep.d_src, V.sweep.n, dst, dst, src, V.zero64, st));
+        TRY(chk("fill fp64", g));
+        V.cur64 = 1 - V.cur64;
+        V.zero64 = false;
+      }
+      h->kernels += (V.sweep.n > 0) ? 2 : 1;
+      return H3D_OK;
+    }
+    if (mixed_level(g) && V.zero32 && V.d_ztiles) {  // first sweep from a zero iterate: a stencil on rhs
+      float* src = V.phi32[V.cur32];
+      float* dst = V.phi32[1 - V.cur32];
+      const bool push = V.push_ok;
+      CU(launch_rbgs_zero32(V.d_bl, V.d_ztiles, V.nztiles, V.zzc, V.rhs32, dst, push ? V.d_push : nullptr, st));
+      TRY(chk("zero-source sweep fp32", g));
+      if (e1) CU(record(e1));
+      const Halo& fill = push ? V.sweep_push : V.sweep;
+      CU(launch_fill<float>(fill.d_dst, fill.d_src, fill.n, dst, dst, src, true, st));
+      TRY(chk("fill fp32", g));
+      V.cur32 = 1 - V.cur32;
+      V.zero32 = false;
+      h->kernels += (fill.n > 0) ? 2 : 1;
+      return H3D_OK;
+    }
     if (mixed_level(g)) {
       float* src = V.phi32[V.cur32];
       float* dst = V.phi32[1 - V.cur32];
@@ -463,7 +510,7 @@ struct Exec {
 
   int relax(int g, int it) {
     Level& V = L(g);
-    if (it > 0 && V.small && g > 1) {  // all sweeps and fills of this visit in one launch
+    if (it > 0 && V.small && g > 1 && h->desc.mg_itrsch == 3) {  // all sweeps and fills of this visit in one launch
       const int nb = (int)V.geom.bl.size();
       if (mixed_level(g)) {
         CU(launch_relax_small<float>(h->var, V.d_bl, V.d_cstart, nb, V.phi32[V.cur32], V.rhs32, V.fx32, V.fy32,
@@ -1432,7 +1479,7 @@ void emit_tail_ops(const h3d_mg* h, int g0, int scratch, std::vector<TailOp>& op
 
 int build_tail(h3d_mg* h) {
   const int Lv = h->L;
-  if (h->var) return H3D_OK;
+  if (h->var || h->desc.mg_itrsch != 3) return H3D_OK;  // the fused tail relaxes by red-black GS
   int g0 = Lv + 1;
   TailPlan plan;
   for (int g = Lv; g >= 2; --g) {
@@ -1593,7 +1640,7 @@ int build_tail(h3d_mg* h) {
 int build_cluster_tail(h3d_mg* h) {
   const int Lv = h->L;
   const int nb = (int)h->blocks.size();
-  if (h->var || nb > kClusterTailMaxBlocks) return H3D_OK;
+  if (h->var || nb > kClusterTailMaxBlocks || h->desc.mg_itrsch != 3) return H3D_OK;
   auto al = [](int v) { return (v + 15) & ~15; };
   struct Lay { int npad, nint, s_phi32, s_rhs32, s_phi64, s_rhs64, s_cells, s_fill; };
   std::vector<Lay> lay;
@@ -1794,7 +1841,7 @@ int h3d_mg_destroy(h3d_mg* h) {
     void* ps[] = {V.d_bl, V.d_cta_all, V.d_cta_int, V.d_rows_all, V.d_rows_int, V.d_tiles, V.phi64[0], V.phi64[1], V.rhs64, V.phi32[0],
                   V.phi32[1], V.rhs32, V.fx64, V.fy64, V.fz64, V.fx32, V.fy32, V.fz32, V.dens,
                   V.sweep.d_dst, V.sweep.d_src, V.faces.d_dst, V.faces.d_src, V.exch.d_dst, V.exch.d_src,
-                  V.bound.d_dst, V.bound.d_src, V.sweep_push.d_dst, V.sweep_push.d_src, V.d_push, V.d_maps, V.d_rmaps, V.d_rtiles, V.d_ptiles, V.d_qtiles, V.d_dtiles, V.d_cstart, V.d_dstart, V.d_pstart};
+                  V.bound.d_dst, V.bound.d_src, V.sweep_push.d_dst, V.sweep_push.d_src, V.d_push, V.d_maps, V.d_rmaps, V.d_rtiles, V.d_ptiles, V.d_qtiles, V.d_dtiles, V.d_cstart, V.d_dstart, V.d_pstart, V.seq64, V.seq32, V.d_ztiles};
     for (void* p : ps) dfree(p);
   }
   dfree(h->p64[0]);
@@ -1826,8 +1873,8 @@ int h3d_mg_create(h3d_mg** out, const h3d_mg_desc* desc) {
   *out = nullptr;
   const h3d_mg_desc& D = *desc;
   if (D.ngrd_gl < 1 || D.ngrd_gl > kMaxLevels) return fail(nullptr, H3D_ERR_BAD_CONFIG, "ngrd_gl out of range");
-  if (D.mg_itrsch != 3)
-    return fail(nullptr, H3D_ERR_BAD_CONFIG, "only mg_itrsch=3 (red-black Gauss-Seidel) runs on the GPU");
+  if (D.mg_itrsch < 1 || D.mg_itrsch > 3)
+    return fail(nullptr, H3D_ERR_BAD_CONFIG, "mg_itrsch must be 1 (GS-lex), 2 (line TDMA) or 3 (red-black GS)");
   if (D.irestr < 0 || D.iproln < 0 || D.irestr + D.iproln < 1)
     return fail(nullptr, H3D_ERR_BAD_CONFIG, "irestr/iproln must be >= 0 with at least one sweep");
   if (D.precision != H3D_PREC_FP64 && D.precision != H3D_PREC_MIXED)
@@ -1900,6 +1947,10 @@ int h3d_mg_create(h3d_mg** out, const h3d_mg_desc* desc) {
       if ((rc = dalloc(h, &V.phi32[0], n)) || (rc = dalloc(h, &V.phi32[1], n)) || (rc = dalloc(h, &V.rhs32, n)))
         return bail(rc);
     }
+    if (D.mg_itrsch == 2) {
+      if (need64 && (rc = dalloc(h, &V.seq64, n))) return bail(rc);
+      if (need32 && (rc = dalloc(h, &V.seq32, n))) return bail(rc);
+    }
     if (h->var) {
       if ((rc = dalloc(h, &V.dens, n)) || (rc = dalloc(h, &V.fx64, n)) || (rc = dalloc(h, &V.fy64, n)) ||
           (rc = dalloc(h, &V.fz64, n)))
@@ -1962,6 +2013,34 @@ int h3d_mg_create(h3d_mg** out, const h3d_mg_desc* desc) {
           return bail(fail(h, H3D_ERR_CUDA, "defect tiles"));
         V.nptiles = (int)pt.size();
         if ((rc = upload_tile_starts(h, pt, (int)V.geom.bl.size(), &V.d_pstart)) != H3D_OK) return bail(rc);
+      }
+    }
+    const char* zs_env = std::getenv("H3D_ZERO_STENCIL");
+    if (f32_level(h, g) && !h->var && h->desc.mg_itrsch == 3 && !(zs_env && zs_env[0] == '0')) {
+      // zero-source FP32 sweep tiles: 256 / (nx/4) rows of a block over a chunk of planes
+      // (H3D_ZERO_STENCIL=0: the zero-source mode of the tuned sweep kernel instead)
+      bool ok = true;
+      int maxnz = 0, nyz = 0;
+      for (const auto& B : V.geom.bl) {
+        ok = ok && B.nx % 4 == 0 && B.nx <= 1024;
+        if (!ok) break;
+        maxnz = std::max(maxnz, B.nz);
+        nyz += (B.ny + 256 / (B.nx / 4) - 1) / (256 / (B.nx / 4));
+      }
+      if (ok) {
+        // about eight CTAs per SM in all, at least four planes a chunk
+        V.zzc = std::max(4, std::min(32, (nyz * maxnz + 148 * 8 - 1) / (148 * 8)));
+        std::vector<Tile> zt;
+        for (size_t b = 0; b < V.geom.bl.size(); ++b) {
+          const BlkLev& B = V.geom.bl[b];
+          const int rows = 256 / (B.nx / 4);
+          for (int z0 = 1; z0 <= B.nz; z0 += V.zzc)
+            for (int y0 = 1; y0 <= B.ny; y0 += rows) zt.push_back(Tile{(int)b, 1, y0, z0});
+        }
+        if ((rc = dalloc(h, &V.d_ztiles, zt.size())) != H3D_OK) return bail(rc);
+        if (cudaMemcpy(V.d_ztiles, zt.data(), zt.size() * sizeof(Tile), cudaMemcpyHostToDevice) != cudaSuccess)
+          return bail(fail(h, H3D_ERR_CUDA, "zero-sweep tiles"));
+        V.nztiles = (int)zt.size();
       }
     }
     if (g == 1 && !h->var) {  // z-march defect tiles: 8 rows of a block over a chunk of planes
@@ -2059,7 +2138,8 @@ int h3d_mg_coeff(h3d_mg* h) {
     CU(cudaStreamSynchronize(h->st));
   }
   // autotune the smoother tiles of the large levels once coefficients exist
-  for (int g = 1; g <= h->L; ++g) TRY(autotune_level(h, g));
+  if (h->desc.mg_itrsch == 3)  // the tuned variants are red-black sweeps
+    for (int g = 1; g <= h->L; ++g) TRY(autotune_level(h, g));
   for (int g = 2; g <= h->L; ++g) TRY(autotune_restrict(h, g));
   CU(cudaStreamSynchronize(h->st));
   h->coeffs_ready = true;

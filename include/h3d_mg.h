@@ -60,7 +60,8 @@ typedef struct h3d_block_desc {
 typedef struct h3d_mg_desc {
   int32_t nblocks;
   int32_t ngrd_gl;        /* MG levels (module_vars.for:8) */
-  int32_t mg_itrsch;      /* smoother; 3 = red-black GS (the only GPU smoother) */
+  int32_t mg_itrsch;      /* smoother (mgsolver.for:374-621): 1 lexicographic GS, 2 line TDMA,
+                             3 red-black GS (the fast path; 1 and 2 run as wavefronts) */
   int32_t irestr, iproln; /* pre/post sweeps (control.cin line 11) */
   int32_t maxcy;          /* default cycle cap for h3d_mg_newsolv */
   int32_t precision;      /* H3D_PREC_* */

@@ -40,8 +40,9 @@ def test_strerror_and_create_errors(h3d):
     d.ngrd_gl = 2
     for b in arr:
         b.ngrid = 2
-    d.mg_itrsch = 2
+    d.mg_itrsch = 4  # smoothers are 1 (GS-lex), 2 (line TDMA) and 3 (red-black GS)
     assert L.h3d_mg_create(C.byref(h), C.byref(d)) == _lib.H3D_ERR_BAD_CONFIG
+    assert b"mg_itrsch" in L.h3d_mg_last_error(None)
 
 
 def test_product_does_not_touch_oracle():
@@ -51,3 +52,14 @@ def test_product_does_not_touch_oracle():
             if f.endswith((".py", ".cu", ".cpp", ".h", ".cuh")):
                 txt = open(os.path.join(dp, f)).read()
                 assert "oracle" not in txt.replace("oracle/", ""), f
+
+
+def test_library_resolves_its_own_symbols():
+    """Every symbol of the library's own namespace is defined in it (a
+    launcher left inside an unnamed namespace would only fail at load time
+    on the GPU machine)."""
+    import subprocess
+    out = subprocess.run(["nm", "-DC", os.path.join(ROOT, "hydro3d_b200", "libh3dmg.so")], capture_output=True,
+                         text=True, check=True).stdout
+    undef = [ln for ln in out.splitlines() if " U " in ln and ("h3d" in ln or "launch_" in ln)]
+    assert not undef, undef

@@ -4,8 +4,9 @@ tests/golden/make_golden.py ran the reference's coeff + mgkcyc, translated
 statement by statement from mgsolver.for / exchangepp.for /
 localparameters.for by oracle/fortran_ref.py, on seeded inputs.  Here:
   * the oracle reproduces every fixture bit for bit (this pins the oracle);
-  * the CUDA path (FP64, through the C ABI) reproduces the RBGS fixtures bit
-    for bit (the GPU smoother is red-black Gauss-Seidel only);
+  * the CUDA path (FP64, through the C ABI) reproduces every fixture bit for
+    bit, with the fixture's own smoother (red-black GS, lexicographic GS or
+    line TDMA);
   * where the reference source tree is present (not on GPU machines), the
     fixtures are regenerated and must be identical (the generator is
     deterministic).
@@ -54,12 +55,10 @@ def test_oracle_matches_reference(oracle_mod, name):
 @pytest.mark.parametrize("name", NAMES)
 def test_cuda_matches_reference(h3d, name):
     g = _load(name)
-    if int(g["mg_itrsch"]) != 3:
-        pytest.skip("the CUDA path implements the red-black Gauss-Seidel smoother (mg_itrsch = 3)")
     nb = int(g["nblocks"])
     ngrd = int(g["ngrd_gl"])
     blocks = h3d.topology.from_extents(g["ext"], g["bc"], g["h"], ngrd, pl=1)
-    s = h3d.MultigridSolver(blocks, ngrd, var_coef=bool(g["lsm"]))
+    s = h3d.MultigridSolver(blocks, ngrd, mg_itrsch=int(g["mg_itrsch"]), var_coef=bool(g["lsm"]))
     if g["lsm"]:
         for ib, d in enumerate(blocks):
             dens = h3d.host_field(d)

@@ -136,9 +136,12 @@ def test_config4_uneven_blocks(oracle_mod, h3d):
     """27 independent blocks of 15+ different shapes in one solver: one
     V-cycle bit for bit on every block, then the mixed-precision solve with
     the per-block stop rule (every block's ||r||/||b|| <= 1e-8, recomputed
-    here by the oracle from the returned pressure) and every block's pressure
-    within 1e-6 of the oracle's solution to 1e-12 (the ratio of the algebraic
-    error to the residual of these Neumann blocks bounds it)."""
+    here by the oracle from the returned pressure), and every block's error
+    against the oracle's solution to 1e-12 within the bound the residual
+    sets: ||e|| <= ||r|| / lambda_min, lambda_min = (4/h^2) sin^2(pi/(2 n))
+    the smallest non-zero eigenvalue of the block's Neumann operator (n its
+    longest axis).  Long thin blocks make that bound large: a residual of
+    1e-8 allows errors near 1e-4 there."""
     from hydro3d_b200 import synth
     prob = synth.config4()
     sizes = {tuple(d.n) for d in prob.blocks}
@@ -156,10 +159,13 @@ def test_config4_uneven_blocks(oracle_mod, h3d):
     orc.close()
     for rb, x, d in zip(r, prob.b, prob.blocks):
         assert np.linalg.norm(rb) <= 1.0001e-8 * np.linalg.norm(interior_of_host(x, d))
-    got = [interior_of_host(x, d) for x, d in zip(p, prob.blocks)]
-    want = [x[1:-1, 1:-1, 1:-1] for x in ref["p"]]
-    errs = [mean_removed_rel([g], [w]) for g, w in zip(got, want)]
-    assert max(errs) <= 1e-6, max(errs)
+    for rb, x, d, w in zip(r, p, prob.blocks, ref["p"]):
+        g = interior_of_host(x, d)
+        w = w[1:-1, 1:-1, 1:-1]
+        e = (g - g.mean()) - (w - w.mean())
+        hh = d.h[0]
+        lam = 4.0 / (hh * hh) * np.sin(np.pi / (2 * max(d.n))) ** 2
+        assert np.linalg.norm(e) <= 1.01 * np.linalg.norm(rb) / lam + 1e-12 * np.linalg.norm(w), tuple(d.n)
 
 
 def test_config5_lsm_vcycles_bitexact(oracle_mod, h3d):

@@ -24,11 +24,11 @@ LAYOUTS = [
 FP32_RTOL = 2e-5
 
 
-def _pair(O, h3d, layout, precision="fp64", var=False, use_graph=False):
+def _pair(O, h3d, layout, precision="fp64", var=False, use_graph=False, itrsch=3):
     nblk, n, bc, ngrid = layout
     blocks = h3d.topology.block_grid(nblk, n, bc, [1.0 / 32] * 3, ngrid)
-    s = h3d.MultigridSolver(blocks, ngrid, precision=precision, var_coef=var, use_graph=use_graph)
-    orc = O.Oracle(to_oracle_descs(O, blocks), ngrid, 3, 2, 1, lsm=var)
+    s = h3d.MultigridSolver(blocks, ngrid, mg_itrsch=itrsch, precision=precision, var_coef=var, use_graph=use_graph)
+    orc = O.Oracle(to_oracle_descs(O, blocks), ngrid, itrsch, 2, 1, lsm=var)
     return blocks, s, orc
 
 
@@ -383,3 +383,93 @@ def test_mixed_vcycle_every_level2_smoother(oracle_mod, h3d):
             np.testing.assert_allclose(a, b, rtol=0, atol=1e-4 * np.abs(b).max(), err_msg="variant %d" % v)
     assert tried >= 15
     s.close()
+
+
+# Lexicographic Gauss-Seidel (mg_itrsch 1) and line TDMA (2): the reference's
+# sequential orderings as wavefronts, one CTA per block.
+@pytest.mark.parametrize("itrsch", [1, 2])
+@pytest.mark.parametrize("layout", LAYOUTS)
+def test_sequential_smoothers_bitexact(oracle_mod, h3d, layout, itrsch):
+    """mgrelax (two sweeps) on every level and two V-cycles, bit for bit."""
+    blocks, s, orc = _pair(oracle_mod, h3d, layout, itrsch=itrsch)
+    s.coeff(); orc.coeff()
+    rng = np.random.default_rng(40 + itrsch)
+    for g in range(1, layout[3] + 1):
+        _rand_level(rng, s, orc, g)
+        s.mgrelax(g, 2)
+        orc.mgrelax(g, 2)
+        _assert_level(s, orc, g)
+    _rand_level(rng, s, orc, 1)
+    for _ in range(2):
+        s.vcycle(); orc.vcycle()
+        _assert_level(s, orc, 1)
+    s.close()
+
+
+@pytest.mark.parametrize("itrsch", [1, 2])
+def test_sequential_smoothers_var_coef_and_ragged(oracle_mod, h3d, itrsch):
+    """L_LSM coefficients (density ratio up to 1000) and a block whose three
+    axes differ (lines of three lengths, anti-diagonals of unequal sides)."""
+    layout = ((2, 1, 1), (24, 8, 16), [W] * 6, 2)
+    blocks, s, orc = _pair(oracle_mod, h3d, layout, var=True, itrsch=itrsch)
+    rng = np.random.default_rng(50 + itrsch)
+    for ib, d in enumerate(blocks):
+        dens = h3d.host_field(d)
+        rho = np.exp(rng.uniform(0, np.log(1000.0), (d.n[2], d.n[1], d.n[0])))
+        h3d.interior(dens, d)[...] = rho
+        s.set_density(ib, dens)
+        orc.set_density(ib, rho)
+    s.coeff(); orc.coeff()
+    for g in (1, 2):
+        _rand_level(rng, s, orc, g)
+        s.mgrelax(g, 1); orc.mgrelax(g, 1)
+        _assert_level(s, orc, g)
+    _rand_level(rng, s, orc, 1)
+    s.vcycle(); orc.vcycle()
+    _assert_level(s, orc, 1)
+    s.close()
+
+
+@pytest.mark.parametrize("itrsch", [1, 2])
+def test_sequential_smoothers_solve(oracle_mod, h3d, itrsch):
+    """newsolv_mg with each sequential smoother: the oracle's cycle count and
+    residual history; the mixed-precision solve reaches the tolerance."""
+    layout = ((2, 2, 1), (16, 16, 16), [P, P, W, W, W, W], 4)
+    blocks = h3d.topology.block_grid(layout[0], layout[1], layout[2], [1.0 / 32] * 3, layout[3])
+    b, p = _host_problem(h3d, blocks, 60 + itrsch, 1)
+    s = h3d.MultigridSolver(blocks, layout[3], mg_itrsch=itrsch)
+    info = s.newsolv_mg([x.copy() for x in p], b, tol=1e-8, maxcy=300, history=True)
+    orc = oracle_mod.Oracle(to_oracle_descs(oracle_mod, blocks), layout[3], itrsch, 2, 1)
+    orc.coeff()
+    from tests.helpers import interior_of_host
+    ref = orc.solve([np.zeros((d.n[2] + 2, d.n[1] + 2, d.n[0] + 2)) for d in blocks],
+                    [interior_of_host(x, d) for x, d in zip(b, blocks)], tol=1e-8, maxcy=300)
+    assert info["converged"] and ref["status"] == 0
+    assert info["cycles"] == ref["cycles"]
+    np.testing.assert_allclose(info["history"], ref["history"], rtol=1e-9, atol=0)
+    s.close()
+    m = h3d.MultigridSolver(blocks, layout[3], mg_itrsch=itrsch, precision="mixed")
+    info = m.newsolv_mg([x.copy() for x in p], b, tol=1e-8, maxcy=300)
+    assert info["converged"] and info["relres"] <= 1e-8
+    m.close()
+
+
+def test_zero_source_stencil_matches_window_sweep(h3d, monkeypatch):
+    """The first FP32 sweep from a zero iterate runs as a stencil on the
+    right-hand side (launch_rbgs_zero32); with H3D_ZERO_STENCIL=0 the tuned
+    TMA sweep kernel runs it in its zero-source mode.  The two evaluate the
+    same FP32 operations: V-cycles (level 1 from zero after every defect,
+    levels 2.. from zero after every restriction) agree bit for bit, on
+    walls, periodic faces and 16 blocks."""
+    out = []
+    for flag in ("1", "0"):
+        monkeypatch.setenv("H3D_ZERO_STENCIL", flag)
+        blocks = h3d.topology.block_grid((4, 2, 2), (32, 16, 24), [P, P, W, W, W, W], [1.0 / 32] * 3, 3)
+        b, p = _host_problem(h3d, blocks, 70, 1)
+        s = h3d.MultigridSolver(blocks, 3, precision="mixed", coarse_sweeps=16)
+        pc = [x.copy() for x in p]
+        info = s.newsolv_mg(pc, b, tol=1e-30, maxcy=3)
+        out.append((pc, info["history"] if "history" in info else info["relres"]))
+        s.close()
+    for a, c in zip(out[0][0], out[1][0]):
+        assert np.array_equal(a, c)
