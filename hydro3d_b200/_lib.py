@@ -26,6 +26,8 @@ PREC_FP64 = 0
 PREC_MIXED = 1
 FIELD_P = 0
 FIELD_B = 1
+FIELD_U, FIELD_V, FIELD_W = 2, 3, 4
+FIELD_USTAR, FIELD_VSTAR, FIELD_WSTAR = 5, 6, 7
 
 
 class BlockDesc(C.Structure):
@@ -63,6 +65,7 @@ class MGDesc(C.Structure):
         ("coarse_sweeps", C.c_int32),
         ("inner_cycles", C.c_int32),
         ("use_graph", C.c_int32),
+        ("coarse_op", C.c_int32),
         ("blocks", C.POINTER(BlockDesc)),
     ]
 
@@ -102,6 +105,8 @@ EXPORTS = [
     "h3d_mg_set_profiling", "h3d_mg_smoother_bytes", "h3d_mg_set_smoother", "h3d_mg_get_smoother",
     "h3d_mg_set_restriction", "h3d_mg_get_restriction", "h3d_topology", "h3d_halo_table",
     "h3d_mg_strerror", "h3d_mg_last_error", "h3d_residual_noalloc",
+    "h3d_mg_calvel", "h3d_mg_calmas", "h3d_mg_pbound", "h3d_mg_project_resident", "h3d_mg_project",
+    "h3d_mg_set_wait_limit", "h3d_mg_wait_probe",
 ]
 
 _lib = None
@@ -156,6 +161,14 @@ def lib():
         "h3d_topology": (i32, [i32, C.POINTER(C.c_int32), C.POINTER(C.c_int32), pd, i32, C.POINTER(BlockDesc)]),
         "h3d_halo_table": (i32, [i32, C.POINTER(BlockDesc), i32, i32, pu32, pu32, i64, C.POINTER(i64)]),
         "h3d_residual_noalloc": (i32, [C.c_void_p, C.c_void_p, i32, i32, i32, pd, i32, pd, C.c_void_p]),
+        "h3d_mg_set_wait_limit": (i32, [vp, i64]),
+        "h3d_mg_wait_probe": (i32, [vp]),
+        "h3d_mg_calvel": (i32, [vp, dbl, dbl]),
+        "h3d_mg_calmas": (i32, [vp, dbl, pd, pd]),
+        "h3d_mg_pbound": (i32, [vp]),
+        "h3d_mg_project_resident": (i32, [vp, dbl, dbl, C.POINTER(SolveOpts), C.POINTER(SolveInfo)]),
+        "h3d_mg_project": (i32, [vp, ppd, ppd, ppd, ppd, ppd, ppd, ppd, dbl, dbl, C.POINTER(SolveOpts),
+                                 C.POINTER(SolveInfo)]),
         "h3d_mg_strerror": (C.c_char_p, [C.c_int]),
         "h3d_mg_last_error": (C.c_char_p, [vp]),
     }

@@ -253,7 +253,7 @@ __global__ void __launch_bounds__(NT) k_rbgs(const BlkLev* __restrict__ bls, con
 // in registers; rows y+-1 and the two cells beside the group come from L1.
 // 1/ap of a cell depends only on which wall faces it touches: a 64-entry
 // table per CTA.  Ghost pushes as in the window sweep.
-__global__ void __launch_bounds__(256) k_rbgs_zero32(const BlkLev* __restrict__ bls, const Tile* __restrict__ tiles,
+__global__ void __launch_bounds__(256, 3) k_rbgs_zero32(const BlkLev* __restrict__ bls, const Tile* __restrict__ tiles,
                                                      int zc, const float* __restrict__ rhs, float* __restrict__ dst,
                                                      const long long* __restrict__ push) {
   pdl_trigger();
@@ -293,15 +293,39 @@ __global__ void __launch_bounds__(256) k_rbgs_zero32(const BlkLev* __restrict__ 
   auto ld4 = [](const float* p) { return *reinterpret_cast<const float4*>(p); };
   const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f);
   const long long row = (long long)y * sx + x0;
+  // Rows y+-1 inside the block and off the walls make the mask of every cell
+  // and neighbour a function of x alone (the fast path below; uniform across
+  // a warp, which is one row when nx = 128).  Of the x positions x0-1 ..
+  // x0+4 only x0 and x0+3 can be wall cells (nx is a multiple of 4) and only
+  // x0-1 and x0+4 can lie outside the block (their zero-iterate value is 0).
+  const bool fy = y >= 3 && y <= ny - 2;
+  const float iv0 = ivtab[0];
+  const float iv_0 = ivtab[x0 == 1 ? (ph & 1) : 0], iv_3 = ivtab[x0 + 3 == nx ? (ph & 2) : 0];
+  const float ivw = x0 > 1 ? iv0 : 0.f, ive = x0 + 4 <= nx ? iv0 : 0.f;
+  const float aw0 = (x0 == 1 && (ph & 1)) ? 0.f : ax, ae3 = (x0 + 3 == nx && (ph & 2)) ? 0.f : ax;
+  // plane z of the own row and rows y+-1 and the cells beside the group, one
+  // plane ahead of their use
+  auto load_plane = [&](int z, float4& hs_, float4& hn_, float& rl_, float& rr_) {
+    const long long o = (long long)z * sxy + row;
+    hs_ = y > 1 ? ld4(R + o - sx) : zero4;
+    hn_ = y < ny ? ld4(R + o + sx) : zero4;
+    rl_ = x0 > 1 ? R[o - 1] : 0.f;
+    rr_ = x0 + 4 <= nx ? R[o + 4] : 0.f;
+  };
   float4 hb = zs > 1 ? ld4(R + (long long)(zs - 1) * sxy + row) : zero4;
   float4 hz = ld4(R + (long long)zs * sxy + row);
+  float4 ht = zs < nz ? ld4(R + (long long)(zs + 1) * sxy + row) : zero4;
+  float4 hs, hn;
+  float rl, rr;
+  load_plane(zs, hs, hn, rl, rr);
   for (int z = zs; z <= ze; ++z) {
     const long long o = (long long)z * sxy + row;
-    const float4 ht = z < nz ? ld4(R + o + sxy) : zero4;
-    const float4 hs = y > 1 ? ld4(R + o - sx) : zero4;
-    const float4 hn = y < ny ? ld4(R + o + sx) : zero4;
-    const float rl = x0 > 1 ? R[o - 1] : 0.f;
-    const float rr = x0 + 4 <= nx ? R[o + 4] : 0.f;
+    float4 ht2 = zero4, hs2 = zero4, hn2 = zero4;
+    float rl2 = 0.f, rr2 = 0.f;
+    if (z < ze) {
+      if (z + 1 < nz) ht2 = ld4(R + o + 2 * sxy);
+      load_plane(z + 1, hs2, hn2, rl2, rr2);
+    }
     const float hzv[4] = {hz.x, hz.y, hz.z, hz.w};
     const float hbv[4] = {hb.x, hb.y, hb.z, hb.w};
     const float htv[4] = {ht.x, ht.y, ht.z, ht.w};
@@ -309,25 +333,44 @@ __global__ void __launch_bounds__(256) k_rbgs_zero32(const BlkLev* __restrict__ 
     const float hnv[4] = {hn.x, hn.y, hn.z, hn.w};
     float out[4];
     const int par = (x0 + y + z) & 1;  // cell k is red when (x0 + k + y + z) is odd
+    if (fy && z >= 3 && z <= nz - 2) {
+      // the general update below with every mask a function of x: the same
+      // products and the same fused chain
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      const int x = x0 + k;
-      const int m = wmask(x, y, z);
-      const float iv = ivtab[m];
-      if (((par + k) & 1) == 1) {
-        out[k] = hzv[k] * iv;
-      } else {
-        // red neighbours (zero outside the block's interior)
-        const float w = k > 0 ? hzv[k - 1] * ivtab[wmask(x - 1, y, z)] : (x0 > 1 ? rl * ivtab[wmask(x - 1, y, z)] : 0.f);
-        const float e = k < 3 ? hzv[k + 1] * ivtab[wmask(x + 1, y, z)] : (x + 1 <= nx ? rr * ivtab[wmask(x + 1, y, z)] : 0.f);
-        const float sv = y > 1 ? hsv[k] * ivtab[wmask(x, y - 1, z)] : 0.f;
-        const float nv = y < ny ? hnv[k] * ivtab[wmask(x, y + 1, z)] : 0.f;
-        const float bv = z > 1 ? hbv[k] * ivtab[wmask(x, y, z - 1)] : 0.f;
-        const float tv = z < nz ? htv[k] * ivtab[wmask(x, y, z + 1)] : 0.f;
-        const float aw = (m & 1) ? 0.f : ax, ae = (m & 2) ? 0.f : ax, as = (m & 4) ? 0.f : ay,
-                    an = (m & 8) ? 0.f : ay, ab = (m & 16) ? 0.f : az, at = (m & 32) ? 0.f : az;
-        const float sum = fmaf(at, tv, fmaf(ab, bv, fmaf(an, nv, fmaf(as, sv, fmaf(ae, e, aw * w)))));
-        out[k] = (hzv[k] - sum) * iv;
+      for (int k = 0; k < 4; ++k) {
+        const float ivk = k == 0 ? iv_0 : (k == 3 ? iv_3 : iv0);
+        if (((par + k) & 1) == 1) {
+          out[k] = hzv[k] * ivk;
+        } else {
+          const float w = k > 0 ? hzv[k - 1] * (k == 1 ? iv_0 : iv0) : rl * ivw;
+          const float e = k < 3 ? hzv[k + 1] * (k == 2 ? iv_3 : iv0) : rr * ive;
+          const float aw = k == 0 ? aw0 : ax, ae = k == 3 ? ae3 : ax;
+          const float sum = fmaf(az, htv[k] * ivk, fmaf(az, hbv[k] * ivk, fmaf(ay, hnv[k] * ivk,
+                            fmaf(ay, hsv[k] * ivk, fmaf(ae, e, aw * w)))));
+          out[k] = (hzv[k] - sum) * ivk;
+        }
+      }
+    } else {
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const int x = x0 + k;
+        const int m = wmask(x, y, z);
+        const float iv = ivtab[m];
+        if (((par + k) & 1) == 1) {
+          out[k] = hzv[k] * iv;
+        } else {
+          // red neighbours (zero outside the block's interior)
+          const float w = k > 0 ? hzv[k - 1] * ivtab[wmask(x - 1, y, z)] : (x0 > 1 ? rl * ivtab[wmask(x - 1, y, z)] : 0.f);
+          const float e = k < 3 ? hzv[k + 1] * ivtab[wmask(x + 1, y, z)] : (x + 1 <= nx ? rr * ivtab[wmask(x + 1, y, z)] : 0.f);
+          const float sv = y > 1 ? hsv[k] * ivtab[wmask(x, y - 1, z)] : 0.f;
+          const float nv = y < ny ? hnv[k] * ivtab[wmask(x, y + 1, z)] : 0.f;
+          const float bv = z > 1 ? hbv[k] * ivtab[wmask(x, y, z - 1)] : 0.f;
+          const float tv = z < nz ? htv[k] * ivtab[wmask(x, y, z + 1)] : 0.f;
+          const float aw = (m & 1) ? 0.f : ax, ae = (m & 2) ? 0.f : ax, as = (m & 4) ? 0.f : ay,
+                      an = (m & 8) ? 0.f : ay, ab = (m & 16) ? 0.f : az, at = (m & 32) ? 0.f : az;
+          const float sum = fmaf(at, tv, fmaf(ab, bv, fmaf(an, nv, fmaf(as, sv, fmaf(ae, e, aw * w)))));
+          out[k] = (hzv[k] - sum) * iv;
+        }
       }
     }
     const float4 v = make_float4(out[0], out[1], out[2], out[3]);
@@ -341,6 +384,11 @@ __global__ void __launch_bounds__(256) k_rbgs_zero32(const BlkLev* __restrict__ 
     if (z == nz && pd[5] != kNoPush) *reinterpret_cast<float4*>(q + pd[5]) = v;
     hb = hz;
     hz = ht;
+    ht = ht2;
+    hs = hs2;
+    hn = hn2;
+    rl = rl2;
+    rr = rr2;
   }
 }
 
@@ -713,10 +761,17 @@ __device__ __forceinline__ unsigned char* smem_base128(unsigned char* raw) {
   return raw + ((128u - (smem_u32(raw) & 127u)) & 127u);
 }
 
-// Bounded wait on an mbarrier phase: gives up after ~2^26 SM clocks (tens of
-// ms; a plane copy takes microseconds), records the failure in *err and makes
-// every later wait of this thread return at once, so a failed copy can never
-// hang the kernel.
+// Bounded wait on an mbarrier phase: gives up after g_wait_clocks SM clocks
+// (default 2^26, tens of ms; a plane copy takes microseconds; set at run time
+// by set_wait_clocks), records the failure in *err and makes every later
+// wait of this thread return at once, so a failed copy can never hang the
+// kernel.  A thread whose wait gave up issues no further copies, and before
+// its CTA exits the issuing thread waits (drain_ring, a fixed limit of its
+// own) for the copies it already issued, so none lands after the CTA's shared
+// memory is released.
+__device__ long long g_wait_clocks = 1LL << 26;
+constexpr long long kDrainClocks = 1LL << 31;
+
 __device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
   uint32_t done;
   asm volatile(
@@ -729,13 +784,31 @@ __device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
 
 __device__ __forceinline__ void mbar_wait(uint32_t bar, uint32_t parity, int* err, bool& bad) {
   if (bad || mbar_try(bar, parity)) return;
+  const long long lim = g_wait_clocks;
   const long long t0 = clock64();
   for (;;) {
     if (mbar_try(bar, parity)) return;
-    if (clock64() - t0 > (1LL << 26)) {
+    if (clock64() - t0 > lim) {
       bad = true;
       atomicExch(err, 1);
       return;
+    }
+  }
+}
+
+// The copies of a ring whose planes first .. last went through slots
+// q % ns (the (q - first) / ns -th use of the slot): waits for the last copy
+// into every slot.
+__device__ __forceinline__ void drain_ring(const uint64_t* bars, int ns, int first, int last, int* err) {
+  for (int q = max(first, last - ns + 1); q <= last; ++q) {
+    const uint32_t bar = smem_u32(bars + (unsigned)q % (unsigned)ns);
+    const uint32_t parity = ((unsigned)(q - first) / (unsigned)ns) & 1u;
+    const long long t0 = clock64();
+    while (!mbar_try(bar, parity)) {
+      if (clock64() - t0 > kDrainClocks) {
+        atomicExch(err, 2);
+        break;
+      }
     }
   }
 }
@@ -820,7 +893,9 @@ __global__ void __launch_bounds__(TPR*(TY + 2)) k_rbgs_tma2(const BlkLev* __rest
 
   auto pslot = [&](int z) -> T* { return reinterpret_cast<T*>(base + (z % NS) * C::SLOT); };
   auto rslot = [&](int z) -> const T* { return reinterpret_cast<const T*>(base + (z % NS) * C::SLOT + C::PSLOT); };
+  int last_q = -1;  // last plane issued (leader)
   auto issue = [&](int z) {  // leader only
+    last_q = z;
     const uint32_t bar = smem_u32(bars + (z % NS));
     asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(tx_bytes) : "memory");
@@ -892,8 +967,9 @@ __global__ void __launch_bounds__(TPR*(TY + 2)) k_rbgs_tma2(const BlkLev* __rest
     // this phase's shared-memory writes are ordered before the TMA that reuses their slot
     asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
     __syncthreads();
-    if (leader && z + D + 1 <= zhi + 1) issue(z + D + 1);
+    if (leader && !bad && z + D + 1 <= zhi + 1) issue(z + D + 1);
   }
+  if (leader && bad) drain_ring(bars, NS, zlo - 1, last_q, err);
 }
 
 // ---------------------------------------------------------------------------
@@ -981,7 +1057,9 @@ __global__ void __launch_bounds__(TPR*(TY + 2)) k_rbgs_vec(const BlkLev* __restr
   auto slot_of = [&](int z) { return z % NS; };
   auto pslot = [&](int s) -> float* { return reinterpret_cast<float*>(base + s * C::SLOT); };
   auto rslot = [&](int s) -> const float* { return reinterpret_cast<const float*>(base + s * C::SLOT + C::PSLOT); };
+  int last_q = -1;  // last plane issued (leader)
   auto issue = [&](int z) {  // leader only
+    last_q = z;
     const int sl = slot_of(z);
     const uint32_t bar = smem_u32(bars + sl);
     asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
@@ -1077,9 +1155,10 @@ __global__ void __launch_bounds__(TPR*(TY + 2)) k_rbgs_vec(const BlkLev* __restr
     // this phase's shared-memory writes are ordered before the TMA that reuses their slot
     asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
     __syncthreads();
-    if (leader && z + D + 1 <= zhi + 1) issue(z + D + 1);
+    if (leader && !bad && z + D + 1 <= zhi + 1) issue(z + D + 1);
     s0 = wrap(s0 + 1);
   }
+  if (leader && bad) drain_ring(bars, NS, zlo - 1, last_q, err);
 }
 
 // ---------------------------------------------------------------------------
@@ -1888,7 +1967,9 @@ __global__ void __launch_bounds__(TPR*(TY + 2)) k_rbgs_win(const BlkLev* __restr
 
   auto pslot = [&](int s) -> float* { return reinterpret_cast<float*>(base + s * C::SLOT); };
   auto rslot = [&](int s) -> const float* { return reinterpret_cast<const float*>(base + s * C::SLOT + C::PSLOT); };
+  int last_q = -1;  // last plane issued (leader)
   auto issue = [&](int z) {  // leader only
+    last_q = z;
     const int sl = (int)((unsigned)z % (unsigned)NS);
     const uint32_t bar = smem_u32(bars + sl);
     asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
@@ -2041,7 +2122,7 @@ __global__ void __launch_bounds__(TPR*(TY + 2)) k_rbgs_win(const BlkLev* __restr
     // this phase's shared-memory writes are ordered before the TMA that reuses their slot
     asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
     __syncthreads();
-    if (leader && z + D + 1 <= zhi + 1) issue(z + D + 1);
+    if (leader && !bad && z + D + 1 <= zhi + 1) issue(z + D + 1);
 #pragma unroll
     for (int k = 0; k < GPT; ++k) {
       m3[k] = m2[k];
@@ -2051,6 +2132,7 @@ __global__ void __launch_bounds__(TPR*(TY + 2)) k_rbgs_win(const BlkLev* __restr
     }
     s0 = wrap(s0 + 1);
   }
+  if (leader && bad) drain_ring(bars, NS, zlo - 1, last_q, err);
 }
 
 #undef H3D_WIN_COLOUR
@@ -3417,7 +3499,9 @@ __global__ void __launch_bounds__(TPR* TYC) k_restrict_tma(const BlkLev* __restr
 
   auto pslot = [&](int q) -> const T* { return reinterpret_cast<const T*>(base + (q % NS) * C::SLOT); };
   auto rslot = [&](int q) -> const T* { return reinterpret_cast<const T*>(base + (q % NS) * C::SLOT + C::PSLOT); };
+  int last_q = -1;  // last plane issued (leader)
   auto issue = [&](int q) {  // leader only
+    last_q = q;
     const uint32_t bar = smem_u32(bars + q % NS);
     asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(tx_bytes) : "memory");
@@ -3491,8 +3575,9 @@ __global__ void __launch_bounds__(TPR* TYC) k_restrict_tma(const BlkLev* __restr
       }
     }
     __syncthreads();
-    if (leader && zf + D + 1 <= zfb + 1) issue(zf + D + 1);
+    if (leader && !bad && zf + D + 1 <= zfb + 1) issue(zf + D + 1);
   }
+  if (leader && bad) drain_ring(bars, NS, zfa - 1, last_q, err);
 }
 
 // ---- tile restriction ------------------------------------------------------
@@ -3688,6 +3773,251 @@ cudaError_t launch_convert_f2d(const float* a, double* b, int64_t n, cudaStream_
   pdl_launch(k_f2d, grid_for(n, 256), 256, 0, st, a, b, n);
   return cudaGetLastError();
 }
+
+namespace {
+
+// ---------------------------------------------------------------------------
+// Face-sum coarse coefficients (L_LSM, coarse_op = 1; not a reference
+// routine).  The coefficient of a coarse face is the sum of the four fine
+// face coefficients that tile it, times 1/16: 1/2 for the two half cells in
+// series along the face normal (the conductance of the coarse face in the
+// finite-volume form) and 1/8 for the 8-cell average the restriction makes
+// of the residual (mgsolver.for:748-752), which leaves the rhs on the fine
+// cell-volume scale.  With a uniform density it equals 4^-(g-1) times the
+// reference's fine-spacing coefficient; across a 1000:1 density jump it keeps
+// the conductance of every light-fluid path, which averaging the density
+// (mgsolver.for:78-105) does not.  Sum order fixed: ((f00 + f10) + f01) + f11.
+__global__ void __launch_bounds__(256) k_face_coef_sum(const BlkLev* __restrict__ fine,
+                                                       const BlkLev* __restrict__ coarse,
+                                                       const int* __restrict__ cta_start, int nb,
+                                                       const double* __restrict__ ffx, const double* __restrict__ ffy,
+                                                       const double* __restrict__ ffz, double* __restrict__ cfx,
+                                                       double* __restrict__ cfy, double* __restrict__ cfz) {
+  pdl_trigger();
+  pdl_wait();
+  const int b = find_block(cta_start, nb, blockIdx.x);
+  const BlkLev C = coarse[b];
+  const BlkLev F = fine[b];
+  const int local = (blockIdx.x - cta_start[b]) * blockDim.x + threadIdx.x;
+  const int mx = C.nx + 2, my = C.ny + 2, mz = C.nz + 2;
+  if (local >= mx * my * mz) return;
+  const int x = local % mx, y = (local / mx) % my, z = local / (mx * my);
+  const long long ic = C.off + (long long)z * C.sxy + (long long)y * C.sx + x;
+  const bool iny = y >= 1 && y <= C.ny, inz = z >= 1 && z <= C.nz, inx = x >= 1 && x <= C.nx;
+  auto fi = [&](int fx_, int fy_, int fz_) { return F.off + (long long)fz_ * F.sxy + (long long)fy_ * F.sx + fx_; };
+  if (x <= C.nx && iny && inz) {  // coarse face X = fine face 2X, fine rows 2Y-1..2Y, planes 2Z-1..2Z
+    const int X = 2 * x, Y = 2 * y - 1, Z = 2 * z - 1;
+    cfx[ic] = (((ffx[fi(X, Y, Z)] + ffx[fi(X, Y + 1, Z)]) + ffx[fi(X, Y, Z + 1)]) + ffx[fi(X, Y + 1, Z + 1)]) * 0.0625;
+  }
+  if (y <= C.ny && inx && inz) {
+    const int X = 2 * x - 1, Y = 2 * y, Z = 2 * z - 1;
+    cfy[ic] = (((ffy[fi(X, Y, Z)] + ffy[fi(X + 1, Y, Z)]) + ffy[fi(X, Y, Z + 1)]) + ffy[fi(X + 1, Y, Z + 1)]) * 0.0625;
+  }
+  if (z <= C.nz && inx && iny) {
+    const int X = 2 * x - 1, Y = 2 * y - 1, Z = 2 * z;
+    cfz[ic] = (((ffz[fi(X, Y, Z)] + ffz[fi(X + 1, Y, Z)]) + ffz[fi(X, Y + 1, Z)]) + ffz[fi(X + 1, Y + 1, Z)]) * 0.0625;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// The projection (press.for:2-144).  Face velocities live in the level-1
+// layout of the cell they belong to: u at (x,y,z) is the east face of cell
+// (x,y,z) (u(i) of the reference, i = x + isp - 1), x = 0 the block's west
+// face; v north faces, w top faces.
+
+// calvel (press.for:77-144): u = ustar - dt*alfapr*(p(i+1)-p(i))/dx on the
+// faces the reference updates (x = 1..nx, or 1..nx-1 when the east face is a
+// physical wall: ieu = iep - 1, localparameters.for:186-192; v and w alike),
+// divided by the face density 0.5*(dens(i)+dens(i+1)) for L_LSM.  Operand
+// order as written there (dtal = dt*alfapr, then *(dp), /dx, /face density).
+// One warp per interior row.
+template <bool LSM>
+__global__ void __launch_bounds__(256) k_calvel(const BlkLev* __restrict__ bls, const int* __restrict__ row_start,
+                                                int nb, int nrows, const double* __restrict__ h3,
+                                                const double* __restrict__ p, const double* __restrict__ dens,
+                                                const double* __restrict__ us, const double* __restrict__ vs,
+                                                const double* __restrict__ ws, double* __restrict__ u,
+                                                double* __restrict__ v, double* __restrict__ w, double dtal) {
+  pdl_trigger();
+  pdl_wait();
+  const int lane = threadIdx.x & 31;
+  for (int rid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; rid < nrows; rid += (gridDim.x * blockDim.x) >> 5) {
+    const RowRef ref = row_of(bls, row_start, nb, rid, true);
+    const BlkLev B = bls[ref.b];
+    const int y = ref.y, z = ref.z;
+    const double dx = h3[3 * ref.b], dy = h3[3 * ref.b + 1], dz = h3[3 * ref.b + 2];
+    const int nxu = B.nx - ((B.phys & 2) ? 1 : 0);
+    const bool vrow = y <= B.ny - ((B.phys & 8) ? 1 : 0);
+    const bool wrow = z <= B.nz - ((B.phys & 32) ? 1 : 0);
+    const long long rowg = B.off + (long long)z * B.sxy + (long long)y * B.sx;
+    for (int x = 1 + lane; x <= B.nx; x += 32) {
+      const long long i = rowg + x;
+      const double pc = p[i];
+      if (x <= nxu) {
+        double t = dtal * (p[i + 1] - pc) / dx;
+        if (LSM) t = t / (0.5 * (dens[i] + dens[i + 1]));
+        u[i] = us[i] - t;
+      }
+      if (vrow) {
+        double t = dtal * (p[i + B.sx] - pc) / dy;
+        if (LSM) t = t / (0.5 * (dens[i] + dens[i + B.sx]));
+        v[i] = vs[i] - t;
+      }
+      if (wrow) {
+        double t = dtal * (p[i + B.sxy] - pc) / dz;
+        if (LSM) t = t / (0.5 * (dens[i] + dens[i + B.sxy]));
+        w[i] = ws[i] - t;
+      }
+    }
+  }
+}
+
+// exchange(1..3) after calvel: one gather table (face ghosts of the interior
+// rows, physical walls excluded) applied to the three components.
+__global__ void __launch_bounds__(256) k_gather3(const uint32_t* __restrict__ dst, const uint32_t* __restrict__ src,
+                                                 int64_t n, double* __restrict__ a0, double* __restrict__ a1,
+                                                 double* __restrict__ a2) {
+  pdl_trigger();
+  pdl_wait();
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+    const uint32_t d = dst[e], s = src[e];
+    a0[d] = a0[s];
+    a1[d] = a1[s];
+    a2[d] = a2[s];
+  }
+}
+
+// calmas (press.for:40-62): fact = (u(i)-u(i-1))/dx + (v(j)-v(j-1))/dy +
+// (w(k)-w(k-1))/dz; su = fact/dt, or sup = fact*dx*dy*dz/dt for L_LSM;
+// rmax = max |fact*dx*dy*dz|.  su goes to bout (FP64) and to the level-1
+// right-hand side rhs_out (as TR); per-CTA partials {sum su^2, 0, rmax,
+// sum su}.
+template <bool LSM, typename TR>
+__global__ void __launch_bounds__(256) k_calmas(const BlkLev* __restrict__ bls, const int* __restrict__ row_start,
+                                                int nb, int nrows, const double* __restrict__ h3,
+                                                const double* __restrict__ u, const double* __restrict__ v,
+                                                const double* __restrict__ w, double dt, double* __restrict__ bout,
+                                                TR* __restrict__ rhs_out, double* __restrict__ partials) {
+  pdl_trigger();
+  pdl_wait();
+  const int lane = threadIdx.x & 31;
+  double ss = 0, rm = 0, rs = 0;
+  for (int rid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; rid < nrows; rid += (gridDim.x * blockDim.x) >> 5) {
+    const RowRef ref = row_of(bls, row_start, nb, rid, true);
+    const BlkLev B = bls[ref.b];
+    const double dx = h3[3 * ref.b], dy = h3[3 * ref.b + 1], dz = h3[3 * ref.b + 2];
+    const long long rowg = B.off + (long long)ref.z * B.sxy + (long long)ref.y * B.sx;
+    for (int x = 1 + lane; x <= B.nx; x += 32) {
+      const long long i = rowg + x;
+      const double fact = (u[i] - u[i - 1]) / dx + (v[i] - v[i - B.sx]) / dy + (w[i] - w[i - B.sxy]) / dz;
+      const double s = LSM ? fact * dx * dy * dz / dt : fact / dt;
+      bout[i] = s;
+      rhs_out[i] = (TR)s;
+      ss += s * s;
+      rs += s;
+      const double a = fabs(fact * dx * dy * dz);
+      if (!(a <= rm)) rm = a;  // keeps a NaN
+    }
+  }
+  block_reduce4<256>(ss, 0.0, rm, rs, partials + 4 * (size_t)blockIdx.x);
+}
+
+// p = p + (pp - ppref) over the block and its ghost layer (newsolv_mg.for:
+// 39-49, ppref = 0): one warp per row of every row.
+template <typename TE>
+__global__ void __launch_bounds__(256) k_padd(const BlkLev* __restrict__ bls, const int* __restrict__ row_start,
+                                              int nb, int nrows, double* __restrict__ p, const TE* __restrict__ e) {
+  pdl_trigger();
+  pdl_wait();
+  const int lane = threadIdx.x & 31;
+  for (int rid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; rid < nrows; rid += (gridDim.x * blockDim.x) >> 5) {
+    const RowRef ref = row_of(bls, row_start, nb, rid, false);
+    const BlkLev B = bls[ref.b];
+    const long long rowg = B.off + (long long)ref.z * B.sxy + (long long)ref.y * B.sx;
+    for (int x = lane; x <= B.nx + 1; x += 32) {
+      const long long i = rowg + x;
+      p[i] = p[i] + ((double)e[i] - 0.0);
+    }
+  }
+}
+
+}  // namespace
+
+// The failure path of the bounded waits, made to run out: one warp waits
+// (mbar_wait, the sweeps' own routine and limit) on an mbarrier that expects
+// one arrival and receives none, so the wait gives up after g_wait_clocks,
+// sets *err and the kernel returns.  No copy is issued.
+__global__ void k_wait_probe(int* err) {
+  __shared__ uint64_t bar;
+  if (threadIdx.x == 0)
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&bar)) : "memory");
+  __syncthreads();
+  bool bad = false;
+  mbar_wait(smem_u32(&bar), 0u, err, bad);
+  __syncthreads();
+}
+
+cudaError_t launch_wait_probe(int* err, cudaStream_t st) {
+  k_wait_probe<<<1, 32, 0, st>>>(err);
+  return cudaGetLastError();
+}
+
+cudaError_t set_wait_clocks(long long clocks) {
+  const long long c = clocks > 0 ? clocks : (1LL << 26);
+  return cudaMemcpyToSymbol(g_wait_clocks, &c, sizeof(c));
+}
+
+cudaError_t launch_face_coef_sum(const BlkLev* fine, const BlkLev* coarse, CellTab ct, const double* ffx,
+                                 const double* ffy, const double* ffz, double* cfx, double* cfy, double* cfz,
+                                 cudaStream_t st) {
+  if (ct.ncta <= 0) return cudaSuccess;
+  pdl_launch(k_face_coef_sum, ct.ncta, 256, 0, st, fine, coarse, ct.cta_start, ct.nb, ffx, ffy, ffz, cfx, cfy, cfz);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_calvel(bool lsm, const BlkLev* bl, RowTab rt, const double* h3, const double* p,
+                          const double* dens, const double* us, const double* vs, const double* ws, double* u,
+                          double* v, double* w, double dtal, cudaStream_t st) {
+  if (rt.nrows <= 0) return cudaSuccess;
+  const int g = defect_grid(rt.nrows);
+  if (lsm) pdl_launch(k_calvel<true>, g, 256, 0, st, bl, rt.start, rt.nb, rt.nrows, h3, p, dens, us, vs, ws, u, v, w, dtal);
+  else pdl_launch(k_calvel<false>, g, 256, 0, st, bl, rt.start, rt.nb, rt.nrows, h3, p, dens, us, vs, ws, u, v, w, dtal);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_gather3(const uint32_t* dst, const uint32_t* src, int64_t n, double* a0, double* a1, double* a2,
+                           cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  pdl_launch(k_gather3, grid_for(n, 256), 256, 0, st, dst, src, n, a0, a1, a2);
+  return cudaGetLastError();
+}
+
+template <typename TR>
+cudaError_t launch_calmas(bool lsm, const BlkLev* bl, RowTab rt, const double* h3, const double* u, const double* v,
+                          const double* w, double dt, double* bout, TR* rhs_out, double* partials, int* nparts,
+                          cudaStream_t st) {
+  *nparts = 0;
+  if (rt.nrows <= 0) return cudaSuccess;
+  const int g = defect_grid(rt.nrows);
+  if (lsm) pdl_launch(k_calmas<true, TR>, g, 256, 0, st, bl, rt.start, rt.nb, rt.nrows, h3, u, v, w, dt, bout, rhs_out, partials);
+  else pdl_launch(k_calmas<false, TR>, g, 256, 0, st, bl, rt.start, rt.nb, rt.nrows, h3, u, v, w, dt, bout, rhs_out, partials);
+  *nparts = g;
+  return cudaGetLastError();
+}
+template cudaError_t launch_calmas<double>(bool, const BlkLev*, RowTab, const double*, const double*, const double*,
+                                           const double*, double, double*, double*, double*, int*, cudaStream_t);
+template cudaError_t launch_calmas<float>(bool, const BlkLev*, RowTab, const double*, const double*, const double*,
+                                          const double*, double, double*, float*, double*, int*, cudaStream_t);
+
+template <typename TE>
+cudaError_t launch_padd(const BlkLev* bl, RowTab rt, double* p, const TE* e, cudaStream_t st) {
+  if (rt.nrows <= 0) return cudaSuccess;
+  pdl_launch(k_padd<TE>, defect_grid(rt.nrows), 256, 0, st, bl, rt.start, rt.nb, rt.nrows, p, e);
+  return cudaGetLastError();
+}
+template cudaError_t launch_padd<double>(const BlkLev*, RowTab, double*, const double*, cudaStream_t);
+template cudaError_t launch_padd<float>(const BlkLev*, RowTab, double*, const float*, cudaStream_t);
+
 
 cudaError_t launch_dens_restrict(const BlkLev* fine, const BlkLev* coarse, CellTab ct, const double* df, double* dc,
                                  cudaStream_t st) {

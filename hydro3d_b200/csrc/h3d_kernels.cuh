@@ -236,4 +236,35 @@ cudaError_t launch_dens_restrict(const BlkLev* fine, const BlkLev* coarse, CellT
 cudaError_t launch_face_coef(const BlkLev* bl, CellTab ct, const double* dens, const double* h3 /*per block dx,dy,dz*/,
                              double* fx, double* fy, double* fz, cudaStream_t st);
 
+// Limit of every bounded mbarrier wait on the current device, in SM clocks
+// (<= 0: the default 2^26).
+cudaError_t set_wait_clocks(long long clocks);
+// One bounded wait on an mbarrier nothing arrives at (sets *err when it gives up).
+cudaError_t launch_wait_probe(int* err, cudaStream_t st);
+
+// Face-sum coarse coefficients of level g from those of level g-1 (L_LSM,
+// coarse_op 1): a coarse face = (sum of its four fine faces) / 16.
+cudaError_t launch_face_coef_sum(const BlkLev* fine, const BlkLev* coarse, CellTab ct, const double* ffx,
+                                 const double* ffy, const double* ffz, double* cfx, double* cfy, double* cfz,
+                                 cudaStream_t st);
+
+// The projection on level 1 (press.for:2-144, newsolv_mg.for:39-49).
+// calvel: u, v, w from ustar, vstar, wstar and p (dtal = dt*alfapr; dens read
+// for L_LSM only).
+cudaError_t launch_calvel(bool lsm, const BlkLev* bl, RowTab interior_rows, const double* h3, const double* p,
+                          const double* dens, const double* us, const double* vs, const double* ws, double* u,
+                          double* v, double* w, double dtal, cudaStream_t st);
+// a_c[dst[e]] = a_c[src[e]] for the three arrays (velocity face ghosts).
+cudaError_t launch_gather3(const uint32_t* dst, const uint32_t* src, int64_t n, double* a0, double* a1, double* a2,
+                           cudaStream_t st);
+// calmas: su into bout (FP64) and rhs_out (TR); partials {sum su^2, 0, rmax,
+// sum su} per CTA (*nparts of them, reduce with launch_reduce4).
+template <typename TR>
+cudaError_t launch_calmas(bool lsm, const BlkLev* bl, RowTab interior_rows, const double* h3, const double* u,
+                          const double* v, const double* w, double dt, double* bout, TR* rhs_out, double* partials,
+                          int* nparts, cudaStream_t st);
+// p += e on every cell of every row (ghost layer included).
+template <typename TE>
+cudaError_t launch_padd(const BlkLev* bl, RowTab all_rows, double* p, const TE* e, cudaStream_t st);
+
 }  // namespace h3d

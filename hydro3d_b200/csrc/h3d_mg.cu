@@ -154,6 +154,17 @@ struct h3d_mg {
   int tail_nops = 0;
   int tail_smem = 0;  // dynamic shared memory of the tail launch
   std::vector<char> tail_zero32, tail_zero64;  // zero flags of the tail levels after the tail
+  // the projection (allocated on first use): face velocities u, v, w and
+  // ustar, vstar, wstar in the level-1 layout, and the gather table of their
+  // face ghosts (exchange(1..3) after calvel)
+  double* vel[3] = {nullptr, nullptr, nullptr};
+  double* vstar[3] = {nullptr, nullptr, nullptr};
+  uint32_t* d_vdst = nullptr;
+  uint32_t* d_vsrc = nullptr;
+  int64_t nvfill = 0;
+  bool proj = false;        // outer iterations end with p += pp, calvel, calmas
+  double proj_dtal = 0.0;   // dt*alfapr
+  double proj_dt = 1.0;
 };
 
 namespace {
@@ -752,13 +763,63 @@ struct Exec {
   }
 
   // One outer iteration: V-cycle(s) on the current defect, then p += e and
-  // the new defect.
+  // the new defect (the projection: p += e, exchange(4) + pbound, calvel,
+  // calmas).
   int iteration(int inner) {
     Level& V = L(1);
     if (h->mixed) V.zero32 = true;
     else V.zero64 = true;
     for (int q = 0; q < inner; ++q) TRY(vcycle());
+    if (h->proj) {
+      TRY(proj_update());
+      return vel_defect();
+    }
     return defect(true);
+  }
+
+  // newsolv_mg.for:39-52: p = p + (pp - ppref) over the block and its ghost
+  // layer, then exchange(4) + pbound (the face ghosts of the interior rows).
+  int proj_update() {
+    Level& V = L(1);
+    RowTab ra{V.d_rows_all, (int)V.geom.bl.size(), V.nrows_all};
+    double* p = h->p64[h->pc];
+    if (h->mixed) {
+      if (V.zero32) TRY(materialize_zero32(1));
+      CU(launch_padd<float>(V.d_bl, ra, p, V.phi32[V.cur32], h->st));
+    } else {
+      if (V.zero64) TRY(materialize_zero64(1));
+      CU(launch_padd<double>(V.d_bl, ra, p, V.phi64[V.cur64], h->st));
+    }
+    TRY(chk("p update", 1));
+    CU(launch_fill<double>(V.faces.d_dst, V.faces.d_src, V.faces.n, p, p, p, false, h->st));
+    TRY(chk("pressure halo", 1));
+    h->kernels += 2;
+    return H3D_OK;
+  }
+
+  // calvel with its exchange(1..3), then calmas into the level-1 right-hand
+  // side and the FP64 su (newsolv_mg.for:54-55); the sums reach h_res.
+  int vel_defect() {
+    Level& V = L(1);
+    RowTab ri{V.d_rows_int, (int)V.geom.bl.size(), V.nrows_int};
+    CU(launch_calvel(h->var, V.d_bl, ri, h->d_h3, h->p64[h->pc], V.dens, h->vstar[0], h->vstar[1], h->vstar[2],
+                     h->vel[0], h->vel[1], h->vel[2], h->proj_dtal, h->st));
+    TRY(chk("calvel", 1));
+    CU(launch_gather3(h->d_vdst, h->d_vsrc, h->nvfill, h->vel[0], h->vel[1], h->vel[2], h->st));
+    TRY(chk("velocity exchange", 1));
+    int np = 0;
+    if (h->mixed)
+      CU(launch_calmas<float>(h->var, V.d_bl, ri, h->d_h3, h->vel[0], h->vel[1], h->vel[2], h->proj_dt, h->b64,
+                              V.rhs32, h->partials, &np, h->st));
+    else
+      CU(launch_calmas<double>(h->var, V.d_bl, ri, h->d_h3, h->vel[0], h->vel[1], h->vel[2], h->proj_dt, h->b64,
+                               V.rhs64, h->partials, &np, h->st));
+    TRY(chk("calmas", 1));
+    CU(launch_reduce4(h->partials, np, h->d_res, h->st));
+    TRY(chk("reduce", 1));
+    CU(cudaMemcpyAsync(h->h_res, h->d_res, 4 * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+    h->kernels += (h->nvfill > 0) ? 4 : 3;
+    return H3D_OK;
   }
 };
 
@@ -826,7 +887,8 @@ int run_iteration(h3d_mg* h, int inner, double* prof_ms, int64_t* prof_n, double
     std::vector<cudaEvent_t> used(h->ev_eager.begin(), h->ev_eager.begin() + ex.prof_used);
     return accumulate_events(h, used, ex.prof_bytes, prof_ms, prof_n, prof_bytes);
   }
-  std::vector<int> key = state_key(h, inner * 4 + (h->profiling ? 1 : 0) + (h->per_block ? 2 : 0));
+  std::vector<int> key =
+      state_key(h, inner * 8 + (h->profiling ? 1 : 0) + (h->per_block ? 2 : 0) + (h->proj ? 4 : 0));
   auto it = h->graphs.find(key);
   if (it == h->graphs.end()) {
     CachedGraph cg;
@@ -1861,6 +1923,12 @@ int h3d_mg_destroy(h3d_mg* h) {
   dfree(h->d_tail_starts);
   dfree(h->stage[0]);
   dfree(h->stage[1]);
+  for (int c = 0; c < 3; ++c) {
+    dfree(h->vel[c]);
+    dfree(h->vstar[c]);
+  }
+  dfree(h->d_vdst);
+  dfree(h->d_vsrc);
   if (h->h_res) cudaFreeHost(h->h_res);
   if (h->st) cudaStreamDestroy(h->st);
   delete h;
@@ -1879,6 +1947,7 @@ int h3d_mg_create(h3d_mg** out, const h3d_mg_desc* desc) {
     return fail(nullptr, H3D_ERR_BAD_CONFIG, "irestr/iproln must be >= 0 with at least one sweep");
   if (D.precision != H3D_PREC_FP64 && D.precision != H3D_PREC_MIXED)
     return fail(nullptr, H3D_ERR_BAD_CONFIG, "unknown precision");
+  if (D.coarse_op < 0 || D.coarse_op > 1) return fail(nullptr, H3D_ERR_BAD_CONFIG, "coarse_op must be 0 or 1");
   for (int b = 0; b < D.nblocks; ++b) {
     const h3d_block_desc& d = D.blocks[b];
     if (d.ngrid != D.ngrd_gl) return fail(nullptr, H3D_ERR_BAD_CONFIG, "every block needs ngrid == ngrd_gl");
@@ -2110,7 +2179,7 @@ int h3d_mg_set_density(h3d_mg* h, int32_t ib, const double* dens) {
   if (!h->var) return fail(h, H3D_ERR_ARG, "handle was created with var_coef = 0");
   TRY(check_block_host_dims(h, h->blocks[ib]));
   CU(cudaSetDevice(h->device));
-  TRY(copy_field_3d(h, true, h->lev[1].dens, h->lev[1].geom.bl[ib], const_cast<double*>(dens), h->blocks[ib], false));
+  TRY(copy_field_3d(h, true, h->lev[1].dens, h->lev[1].geom.bl[ib], const_cast<double*>(dens), h->blocks[ib], true));
   CU(cudaStreamSynchronize(h->st));
   h->coeffs_ready = false;
   return H3D_OK;
@@ -2122,13 +2191,16 @@ int h3d_mg_coeff(h3d_mg* h) {
   if (h->var) {
     for (int g = 1; g <= h->L; ++g) {
       Level& V = h->lev[g];
+      CellTab ca{V.d_cta_all, (int)V.geom.bl.size(), V.ncta_all};
       if (g > 1) {
         Level& F = h->lev[g - 1];
         CellTab ct{V.d_cta_int, (int)V.geom.bl.size(), V.ncta_int};
         CU(launch_dens_restrict(F.d_bl, V.d_bl, ct, F.dens, V.dens, h->st));
+        if (h->desc.coarse_op == 1)
+          CU(launch_face_coef_sum(F.d_bl, V.d_bl, ca, F.fx64, F.fy64, F.fz64, V.fx64, V.fy64, V.fz64, h->st));
       }
-      CellTab ca{V.d_cta_all, (int)V.geom.bl.size(), V.ncta_all};
-      CU(launch_face_coef(V.d_bl, ca, V.dens, h->d_h3, V.fx64, V.fy64, V.fz64, h->st));
+      if (g == 1 || h->desc.coarse_op == 0)
+        CU(launch_face_coef(V.d_bl, ca, V.dens, h->d_h3, V.fx64, V.fy64, V.fz64, h->st));
       if (h->mixed) {
         CU(launch_convert_d2f(V.fx64, V.fx32, V.geom.n_elems, h->st));
         CU(launch_convert_d2f(V.fy64, V.fy32, V.geom.n_elems, h->st));
@@ -2146,6 +2218,9 @@ int h3d_mg_coeff(h3d_mg* h) {
   return H3D_OK;
 }
 
+static int ensure_velocity(h3d_mg* h);
+static double* velocity_field(h3d_mg* h, int field);
+
 static int ensure_coeffs(h3d_mg* h) {
   if (!h->coeffs_ready) return h3d_mg_coeff(h);
   return H3D_OK;
@@ -2158,7 +2233,11 @@ int h3d_mg_upload(h3d_mg* h, int32_t field, int32_t ib, const double* host) {
   const BlkLev& B = h->lev[1].geom.bl[ib];
   if (field == H3D_FIELD_P) TRY(copy_field_3d(h, true, h->p64[h->pc], B, const_cast<double*>(host), h->blocks[ib], true));
   else if (field == H3D_FIELD_B) TRY(copy_field_3d(h, true, h->b64, B, const_cast<double*>(host), h->blocks[ib], false));
-  else return H3D_ERR_ARG;
+  else if (field >= H3D_FIELD_U && field <= H3D_FIELD_WSTAR) {
+    TRY(ensure_velocity(h));
+    TRY(copy_field_3d(h, true, velocity_field(h, field), B, const_cast<double*>(host), h->blocks[ib], true));
+  } else
+    return H3D_ERR_ARG;
   return H3D_OK;
 }
 
@@ -2169,7 +2248,11 @@ int h3d_mg_download(h3d_mg* h, int32_t field, int32_t ib, double* host) {
   const BlkLev& B = h->lev[1].geom.bl[ib];
   if (field == H3D_FIELD_P) TRY(copy_field_3d(h, false, h->p64[h->pc], B, host, h->blocks[ib], true));
   else if (field == H3D_FIELD_B) TRY(copy_field_3d(h, false, h->b64, B, host, h->blocks[ib], false));
-  else return H3D_ERR_ARG;
+  else if (field >= H3D_FIELD_U && field <= H3D_FIELD_WSTAR) {
+    TRY(ensure_velocity(h));
+    TRY(copy_field_3d(h, false, velocity_field(h, field), B, host, h->blocks[ib], true));
+  } else
+    return H3D_ERR_ARG;
   CU(cudaStreamSynchronize(h->st));
   return H3D_OK;
 }
@@ -2336,6 +2419,238 @@ int h3d_mg_history(h3d_mg* h, double* out, int32_t cap, int32_t* n) {
     for (int q = 0; q < k; ++q) out[q] = h->history[q];
   *n = (int)h->history.size();
   return H3D_OK;
+}
+
+// ---------------------------------------------------------- the projection
+// Face ghosts of the velocity components after calvel (exchange(1..3) at
+// equal resolution: exchange_bc.for then exchange.for:302-1650, ghost layer
+// 0 on the interior rows): a low-side ghost takes the source block's last
+// interior plane, a high-side ghost its first; the source is the face
+// neighbour, else (bc = 5) the block itself when it has no neighbour on
+// either side of that axis, else its periodic partner.  Physical walls keep
+// their values.  Every entry reads an interior cell, so the order is free.
+static int build_vel_table(h3d_mg* h) {
+  const LevelGeom& G = h->lev[1].geom;
+  std::vector<uint32_t> dst, src;
+  const int nb = (int)h->blocks.size();
+  for (int b = 0; b < nb; ++b) {
+    const h3d_block_desc& d = h->blocks[b];
+    const BlkLev& B = G.bl[b];
+    for (int f = 0; f < 6; ++f) {
+      if (B.phys & (1 << f)) continue;
+      int sb = -1;
+      if (d.nb_face[f] >= 0) sb = d.nb_face[f];
+      else if (d.bc[f] == 5) sb = d.nb_face[f ^ 1] < 0 ? b : d.nb_periodic[f];
+      if (sb < 0) continue;
+      const BlkLev& S = G.bl[sb];
+      const int ax = f / 2, hi = f & 1;
+      const int nB[3] = {B.nx, B.ny, B.nz}, nS[3] = {S.nx, S.ny, S.nz};
+      for (int a = 0; a < 3; ++a)
+        if (a != ax && nB[a] != nS[a]) return fail(h, H3D_ERR_BAD_CONFIG, "velocity exchange: face extents differ");
+      const int ta = (ax + 1) % 3, tb = (ax + 2) % 3;
+      for (int q = 1; q <= nB[tb]; ++q)
+        for (int r = 1; r <= nB[ta]; ++r) {
+          int cd[3], cs[3];
+          cd[ta] = cs[ta] = r;
+          cd[tb] = cs[tb] = q;
+          cd[ax] = hi ? nB[ax] + 1 : 0;
+          cs[ax] = hi ? 1 : nS[ax];
+          dst.push_back((uint32_t)(B.off + (long long)cd[2] * B.sxy + (long long)cd[1] * B.sx + cd[0]));
+          src.push_back((uint32_t)(S.off + (long long)cs[2] * S.sxy + (long long)cs[1] * S.sx + cs[0]));
+        }
+    }
+  }
+  h->nvfill = (int64_t)dst.size();
+  if (h->nvfill == 0) return H3D_OK;
+  TRY(dalloc(h, &h->d_vdst, dst.size()));
+  TRY(dalloc(h, &h->d_vsrc, src.size()));
+  CU(cudaMemcpyAsync(h->d_vdst, dst.data(), dst.size() * 4, cudaMemcpyHostToDevice, h->st));
+  CU(cudaMemcpyAsync(h->d_vsrc, src.data(), src.size() * 4, cudaMemcpyHostToDevice, h->st));
+  CU(cudaStreamSynchronize(h->st));
+  return H3D_OK;
+}
+
+static int ensure_velocity(h3d_mg* h) {
+  if (h->vel[0]) return H3D_OK;
+  const size_t n = (size_t)h->lev[1].geom.n_elems;
+  for (int c = 0; c < 3; ++c) {
+    TRY(dalloc(h, &h->vel[c], n));
+    TRY(dalloc(h, &h->vstar[c], n));
+  }
+  return build_vel_table(h);
+}
+
+static double* velocity_field(h3d_mg* h, int field) {
+  if (field >= H3D_FIELD_U && field <= H3D_FIELD_W) return h->vel[field - H3D_FIELD_U];
+  if (field >= H3D_FIELD_USTAR && field <= H3D_FIELD_WSTAR) return h->vstar[field - H3D_FIELD_USTAR];
+  return nullptr;
+}
+
+// Cached graphs of projection iterations hold dt*alfapr and dt as kernel
+// arguments: drop them when either changes.
+static void set_projection_scalars(h3d_mg* h, double dt, double alfapr) {
+  const double dtal = dt * alfapr;
+  if (dtal == h->proj_dtal && dt == h->proj_dt) return;
+  for (auto it = h->graphs.begin(); it != h->graphs.end();) {
+    if (it->first[0] & 4) {
+      if (it->second.exec) cudaGraphExecDestroy(it->second.exec);
+      for (auto e : it->second.events) cudaEventDestroy(e);
+      it = h->graphs.erase(it);
+    } else {
+      ++it;
+    }
+  }
+  h->proj_dtal = dtal;
+  h->proj_dt = dt;
+}
+
+int h3d_mg_calvel(h3d_mg* h, double dt, double alfapr) {
+  if (!h) return H3D_ERR_ARG;
+  CU(cudaSetDevice(h->device));
+  TRY(ensure_velocity(h));
+  set_projection_scalars(h, dt, alfapr);
+  Level& V = h->lev[1];
+  RowTab ri{V.d_rows_int, (int)V.geom.bl.size(), V.nrows_int};
+  CU(launch_calvel(h->var, V.d_bl, ri, h->d_h3, h->p64[h->pc], V.dens, h->vstar[0], h->vstar[1], h->vstar[2],
+                   h->vel[0], h->vel[1], h->vel[2], h->proj_dtal, h->st));
+  CU(launch_gather3(h->d_vdst, h->d_vsrc, h->nvfill, h->vel[0], h->vel[1], h->vel[2], h->st));
+  CU(cudaStreamSynchronize(h->st));
+  return check_device_error(h);
+}
+
+int h3d_mg_calmas(h3d_mg* h, double dt, double* rmax, double* su2) {
+  if (!h) return H3D_ERR_ARG;
+  if (!(dt > 0)) return fail(h, H3D_ERR_ARG, "dt must be positive");
+  CU(cudaSetDevice(h->device));
+  TRY(ensure_velocity(h));
+  Level& V = h->lev[1];
+  RowTab ri{V.d_rows_int, (int)V.geom.bl.size(), V.nrows_int};
+  int np = 0;
+  if (h->mixed)
+    CU(launch_calmas<float>(h->var, V.d_bl, ri, h->d_h3, h->vel[0], h->vel[1], h->vel[2], dt, h->b64, V.rhs32,
+                            h->partials, &np, h->st));
+  else
+    CU(launch_calmas<double>(h->var, V.d_bl, ri, h->d_h3, h->vel[0], h->vel[1], h->vel[2], dt, h->b64, V.rhs64,
+                             h->partials, &np, h->st));
+  CU(launch_reduce4(h->partials, np, h->d_res, h->st));
+  CU(cudaMemcpyAsync(h->h_res, h->d_res, 4 * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+  CU(cudaStreamSynchronize(h->st));
+  if (su2) *su2 = h->h_res[0];
+  if (rmax) *rmax = h->h_res[2];
+  return H3D_OK;
+}
+
+int h3d_mg_pbound(h3d_mg* h) {
+  if (!h) return H3D_ERR_ARG;
+  CU(cudaSetDevice(h->device));
+  Level& V = h->lev[1];
+  double* p = h->p64[h->pc];
+  CU(launch_fill<double>(V.faces.d_dst, V.faces.d_src, V.faces.n, p, p, p, false, h->st));
+  CU(cudaStreamSynchronize(h->st));
+  return H3D_OK;
+}
+
+int h3d_mg_project_resident(h3d_mg* h, double dt, double alfapr, const h3d_solve_opts* opts,
+                            h3d_solve_info* info) {
+  if (!h || !opts) return H3D_ERR_ARG;
+  if (opts->stop_rule != 0 && opts->stop_rule != 1)
+    return fail(h, H3D_ERR_ARG, "the projection stops on rule 0 or 1");
+  if (!(dt > 0)) return fail(h, H3D_ERR_ARG, "dt must be positive");
+  CU(cudaSetDevice(h->device));
+  TRY(ensure_coeffs(h));
+  TRY(ensure_velocity(h));
+  struct ProjGuard {  // restores the handle's defect mode on every exit
+    h3d_mg* h;
+    ~ProjGuard() { h->proj = false; }
+  } guard{h};
+  set_projection_scalars(h, dt, alfapr);
+  h->proj = true;
+  h->per_block = false;
+  h3d_solve_info I{};
+  const int maxcy = opts->maxcy > 0 ? opts->maxcy : h->desc.maxcy;
+  const int inner = h->mixed ? h->desc.inner_cycles : 1;
+  h->history.clear();
+  cudaEvent_t t0, t1;
+  CU(cudaEventCreate(&t0));
+  CU(cudaEventCreate(&t1));
+  int64_t k0 = h->kernels;
+  CU(cudaEventRecord(t0, h->st));
+  Exec ex{h};
+  TRY(ex.vel_defect());  // calvel, calmas on the given p (newsolv_mg.for:16-17)
+  CU(cudaStreamSynchronize(h->st));
+  I.bnorm = std::sqrt(h->h_res[0]);
+  const double bn = I.bnorm > 0 ? I.bnorm : 1.0;
+  double rel = std::sqrt(h->h_res[0]) / bn, rmax = h->h_res[2];
+  if (opts->record_history) h->history.push_back(opts->stop_rule == 1 ? rmax : rel);
+  int status = 1, iter = 0;
+  if (opts->stop_rule == 0 && rel <= opts->tol) status = 0;
+  double prof_ms = 0, prof_bytes = 0;
+  int64_t prof_n = 0;
+  while (status != 0 && iter < maxcy) {
+    TRY(run_iteration(h, inner, &prof_ms, &prof_n, &prof_bytes));
+    iter += 1;
+    I.cycles += inner;
+    rel = std::sqrt(h->h_res[0]) / bn;
+    rmax = h->h_res[2];
+    if (opts->record_history) h->history.push_back(opts->stop_rule == 1 ? rmax : rel);
+    if (!std::isfinite(rel) || !std::isfinite(rmax) || rel > 1e8) { status = 2; break; }
+    if (opts->stop_rule == 0 && rel <= opts->tol) status = 0;
+    if (opts->stop_rule == 1 && rmax < opts->tol && iter > 1) status = 0;  // newsolv_mg.for:57
+  }
+  if (status != 2 && rmax > 10.0) status = 2;  // 'BIG RMAX!! STOP', newsolv_mg.for:65-75
+  CU(cudaEventRecord(t1, h->st));
+  CU(cudaEventSynchronize(t1));
+  float ms = 0;
+  CU(cudaEventElapsedTime(&ms, t0, t1));
+  cudaEventDestroy(t0);
+  cudaEventDestroy(t1);
+  I.outer = iter;
+  I.relres = rel;
+  I.relres_block_max = rel;
+  I.rmax = rmax;
+  I.device_ms = ms;
+  I.smoother_ms = prof_ms;
+  I.smoother_launches = prof_n;
+  I.smoother_bytes = prof_bytes;
+  I.kernel_launches = h->kernels - k0;
+  if (info) *info = I;
+  TRY(check_device_error(h));
+  if (status == 2) return fail(h, H3D_ERR_DIVERGED, "divergence not finite or rmax above 10");
+  if (status != 0) return fail(h, H3D_ERR_NOT_CONVERGED, "not converged within maxcy cycles");
+  return H3D_OK;
+}
+
+int h3d_mg_project(h3d_mg* h, double* const* p, double* const* u, double* const* v, double* const* w,
+                   const double* const* ustar, const double* const* vstar, const double* const* wstar,
+                   double dt, double alfapr, const h3d_solve_opts* opts, h3d_solve_info* info) {
+  if (!h || !p || !u || !v || !w || !ustar || !vstar || !wstar || !opts) return H3D_ERR_ARG;
+  CU(cudaSetDevice(h->device));
+  TRY(ensure_velocity(h));
+  const int nb = (int)h->blocks.size();
+  for (int ib = 0; ib < nb; ++ib) {
+    const h3d_block_desc& d = h->blocks[ib];
+    TRY(check_block_host_dims(h, d));
+    const BlkLev& B = h->lev[1].geom.bl[ib];
+    TRY(copy_field_3d(h, true, h->p64[h->pc], B, p[ib], d, true));
+    TRY(copy_field_3d(h, true, h->vel[0], B, u[ib], d, true));
+    TRY(copy_field_3d(h, true, h->vel[1], B, v[ib], d, true));
+    TRY(copy_field_3d(h, true, h->vel[2], B, w[ib], d, true));
+    TRY(copy_field_3d(h, true, h->vstar[0], B, const_cast<double*>(ustar[ib]), d, true));
+    TRY(copy_field_3d(h, true, h->vstar[1], B, const_cast<double*>(vstar[ib]), d, true));
+    TRY(copy_field_3d(h, true, h->vstar[2], B, const_cast<double*>(wstar[ib]), d, true));
+  }
+  int rc = h3d_mg_project_resident(h, dt, alfapr, opts, info);
+  if (rc != H3D_OK && rc != H3D_ERR_NOT_CONVERGED) return rc;
+  for (int ib = 0; ib < nb; ++ib) {
+    const h3d_block_desc& d = h->blocks[ib];
+    const BlkLev& B = h->lev[1].geom.bl[ib];
+    TRY(copy_field_3d(h, false, h->p64[h->pc], B, p[ib], d, true));
+    TRY(copy_field_3d(h, false, h->vel[0], B, u[ib], d, true));
+    TRY(copy_field_3d(h, false, h->vel[1], B, v[ib], d, true));
+    TRY(copy_field_3d(h, false, h->vel[2], B, w[ib], d, true));
+  }
+  CU(cudaStreamSynchronize(h->st));
+  return rc;
 }
 
 // ---------------------------------------------------------- level hooks
@@ -2541,6 +2856,22 @@ int h3d_mg_sync(h3d_mg* h) {
   CU(cudaSetDevice(h->device));
   CU(cudaStreamSynchronize(h->st));
   return H3D_OK;
+}
+
+int h3d_mg_set_wait_limit(h3d_mg* h, int64_t clocks) {
+  if (!h) return H3D_ERR_ARG;
+  CU(cudaSetDevice(h->device));
+  CU(cudaStreamSynchronize(h->st));
+  CU(set_wait_clocks((long long)clocks));
+  return H3D_OK;
+}
+
+int h3d_mg_wait_probe(h3d_mg* h) {
+  if (!h) return H3D_ERR_ARG;
+  CU(cudaSetDevice(h->device));
+  CU(launch_wait_probe(h->d_err, h->st));
+  CU(cudaStreamSynchronize(h->st));
+  return check_device_error(h);
 }
 
 int h3d_mg_set_profiling(h3d_mg* h, int32_t on) {

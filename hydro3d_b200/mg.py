@@ -6,6 +6,10 @@ and their argument meaning:
     coeff()                        mgsolver.for:2-224
     mgkcyc(pp, su)                 mgsolver.for:226-372   (one V-cycle)
     newsolv_mg(p, b, ...)          newsolv_mg.for:2-93    (outer defect correction)
+    project(p, u, v, w, ustar, vstar, wstar, dt, ...)
+                                   newsolv_mg.for:2-93 with calvel/calmas (press.for:2-144)
+    calvel(dt, alfapr) / calmas(dt) / pbound()
+                                   press.for:2-207 on the resident fields
     mgrelax(g, it) / mgrestr(g) / mgcorr(g) / mgbound(g) / exchangepp(g)
                                    mgsolver.for:374-997, exchangepp.for:2-2835
 
@@ -55,7 +59,7 @@ class MultigridSolver:
 
     def __init__(self, blocks: Sequence, ngrd_gl: int, mg_itrsch: int = 3, irestr: int = 2, iproln: int = 1,
                  maxcy: int = 30, precision: str = "fp64", var_coef: bool = False, device: int = 0,
-                 coarse_sweeps: int = 0, inner_cycles: int = 0, use_graph: bool = True):
+                 coarse_sweeps: int = 0, inner_cycles: int = 0, use_graph: bool = True, coarse_op: int = 0):
         self.L = _lib.lib()
         self.blocks = list(blocks)
         self._arr = (_lib.BlockDesc * len(self.blocks))(*self.blocks)
@@ -72,6 +76,7 @@ class MultigridSolver:
         desc.coarse_sweeps = coarse_sweeps
         desc.inner_cycles = inner_cycles
         desc.use_graph = int(bool(use_graph))
+        desc.coarse_op = coarse_op
         desc.blocks = self._arr
         self.ngrd = ngrd_gl
         self.precision = precision
@@ -128,7 +133,7 @@ class MultigridSolver:
         o.record_history = int(bool(history))
         return o
 
-    def _info(self, rc, info, history):
+    def _info(self, rc, info, history, raise_diverged=True):
         out = {k: getattr(info, k) for k, _ in _lib.SolveInfo._fields_}
         out["converged"] = rc == _lib.H3D_OK
         out["status"] = rc
@@ -138,7 +143,7 @@ class MultigridSolver:
             buf = np.zeros(n.value)
             self.L.h3d_mg_history(self._h, _dp(buf), n.value, C.byref(n))
             out["history"] = buf
-        if rc not in (_lib.H3D_OK, _lib.H3D_ERR_NOT_CONVERGED):
+        if rc not in (_lib.H3D_OK, _lib.H3D_ERR_NOT_CONVERGED) and (raise_diverged or rc != _lib.H3D_ERR_DIVERGED):
             self._check(rc, "solve")
         return out
 
@@ -153,14 +158,51 @@ class MultigridSolver:
         rc = self.L.h3d_mg_newsolv(self._h, _ptrs(p), _ptrs(b), C.byref(opts), C.byref(info))
         return self._info(rc, info, history)
 
+    def project(self, p: List[np.ndarray], u: List[np.ndarray], v: List[np.ndarray], w: List[np.ndarray],
+                ustar: List[np.ndarray], vstar: List[np.ndarray], wstar: List[np.ndarray], dt: float,
+                alfapr: float = 1.0, tol: float = 1e-8, maxcy: int = 0, stop_rule: int = 0,
+                history: bool = False) -> dict:
+        """newsolv_mg with the velocities: p, u, v, w host fields in/out,
+        ustar, vstar, wstar host fields in.  stop_rule 1 is the reference's
+        rmax < tol (after at least two cycles); 0 is ||su|| <= tol ||su_0||."""
+        for a in list(p) + list(u) + list(v) + list(w) + list(ustar) + list(vstar) + list(wstar):
+            assert a.dtype == np.float64 and a.flags.c_contiguous
+        opts = self._opts(tol, maxcy, stop_rule, False, history)
+        info = _lib.SolveInfo()
+        rc = self.L.h3d_mg_project(self._h, _ptrs(p), _ptrs(u), _ptrs(v), _ptrs(w), _ptrs(ustar), _ptrs(vstar),
+                                   _ptrs(wstar), dt, alfapr, C.byref(opts), C.byref(info))
+        return self._info(rc, info, history)
+
+    def project_resident(self, dt: float, alfapr: float = 1.0, tol: float = 1e-8, maxcy: int = 0,
+                         stop_rule: int = 0, history: bool = False) -> dict:
+        opts = self._opts(tol, maxcy, stop_rule, False, history)
+        info = _lib.SolveInfo()
+        rc = self.L.h3d_mg_project_resident(self._h, dt, alfapr, C.byref(opts), C.byref(info))
+        return self._info(rc, info, history)
+
+    def calvel(self, dt: float, alfapr: float = 1.0):
+        self._check(self.L.h3d_mg_calvel(self._h, dt, alfapr), "h3d_mg_calvel")
+
+    def calmas(self, dt: float):
+        """(rmax, sum su^2); su lands in the resident field 'b'."""
+        rmax, s2 = C.c_double(), C.c_double()
+        self._check(self.L.h3d_mg_calmas(self._h, dt, C.byref(rmax), C.byref(s2)), "h3d_mg_calmas")
+        return rmax.value, s2.value
+
+    def pbound(self):
+        self._check(self.L.h3d_mg_pbound(self._h), "h3d_mg_pbound")
+
     # resident operation --------------------------------------------------
+    FIELDS = {"p": _lib.FIELD_P, "b": _lib.FIELD_B, "u": _lib.FIELD_U, "v": _lib.FIELD_V, "w": _lib.FIELD_W,
+              "ustar": _lib.FIELD_USTAR, "vstar": _lib.FIELD_VSTAR, "wstar": _lib.FIELD_WSTAR}
+
     def upload(self, field: str, ib: int, host: np.ndarray):
-        f = {"p": _lib.FIELD_P, "b": _lib.FIELD_B}[field]
+        f = self.FIELDS[field]
         host = np.ascontiguousarray(host, dtype=np.float64)
         self._check(self.L.h3d_mg_upload(self._h, f, ib, _dp(host)), "h3d_mg_upload")
 
     def download(self, field: str, ib: int, host: np.ndarray):
-        f = {"p": _lib.FIELD_P, "b": _lib.FIELD_B}[field]
+        f = self.FIELDS[field]
         assert host.dtype == np.float64 and host.flags.c_contiguous
         self._check(self.L.h3d_mg_download(self._h, f, ib, _dp(host)), "h3d_mg_download")
 
@@ -169,16 +211,27 @@ class MultigridSolver:
         self._check(self.L.h3d_mg_zero_field(self._h, f), "h3d_mg_zero_field")
 
     def solve_resident(self, tol: float = 1e-8, maxcy: int = 0, stop_rule: int = 0, remove_mean: bool = False,
-                       history: bool = False) -> dict:
+                       history: bool = False, raise_diverged: bool = True) -> dict:
+        """Solve with p and b resident.  A diverged solve raises unless
+        raise_diverged is False (then info["status"] is H3D_ERR_DIVERGED)."""
         opts = self._opts(tol, maxcy, stop_rule, remove_mean, history)
         info = _lib.SolveInfo()
         rc = self.L.h3d_mg_solve_resident(self._h, C.byref(opts), C.byref(info))
-        return self._info(rc, info, history)
+        return self._info(rc, info, history, raise_diverged)
 
     def residual(self):
         rr, bb, ri = C.c_double(), C.c_double(), C.c_double()
         self._check(self.L.h3d_mg_residual(self._h, C.byref(rr), C.byref(bb), C.byref(ri)), "h3d_mg_residual")
         return rr.value, bb.value, ri.value
+
+    def set_wait_limit(self, clocks: int):
+        """Limit of the bounded device waits on this GPU (<= 0: the default)."""
+        self._check(self.L.h3d_mg_set_wait_limit(self._h, int(clocks)), "h3d_mg_set_wait_limit")
+
+    def wait_probe(self) -> int:
+        """One bounded device wait that cannot complete: the status code
+        (H3D_ERR_TIMEOUT once the limit has run out)."""
+        return self.L.h3d_mg_wait_probe(self._h)
 
     def set_profiling(self, on: bool):
         self._check(self.L.h3d_mg_set_profiling(self._h, int(bool(on))), "h3d_mg_set_profiling")

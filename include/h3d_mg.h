@@ -70,6 +70,10 @@ typedef struct h3d_mg_desc {
   int32_t coarse_sweeps;  /* sweeps at the coarsest level; 0 = irestr+iproln (reference) */
   int32_t inner_cycles;   /* MIXED: FP32 V-cycles per FP64 refinement step (0 = 2) */
   int32_t use_graph;      /* 1: capture each V-cycle as a CUDA graph */
+  int32_t coarse_op;      /* L_LSM coarse levels: 0 = coeff's coefficients from the averaged
+                             density (mgsolver.for:78-184, the reference); 1 = face-sum
+                             coarsening (each coarse face = sum of its four fine faces / 16),
+                             which keeps converging at 1000:1 density ratios */
   const h3d_block_desc* blocks;
 } h3d_mg_desc;
 
@@ -105,7 +109,8 @@ typedef struct h3d_solve_info {
 int h3d_mg_create(h3d_mg** out, const h3d_mg_desc* desc);
 int h3d_mg_destroy(h3d_mg* h);
 /* Density of block ib as a host field (ttc dims, pl ghosts); L_LSM only.
- * Replaces the dom(ib)%dens read in coeff (mgsolver.for:82). */
+ * Replaces the dom(ib)%dens read in coeff (mgsolver.for:82); the first ghost
+ * layer is kept for calvel's face densities (press.for:92-94). */
 int h3d_mg_set_density(h3d_mg* h, int32_t ib, const double* dens);
 /* coeff (mgsolver.for:2-224): per-level coefficients on the device. */
 int h3d_mg_coeff(h3d_mg* h);
@@ -122,6 +127,16 @@ int h3d_mg_newsolv(h3d_mg* h, double* const* p, const double* const* b,
 /* --- device-resident operation ------------------------------------------ */
 #define H3D_FIELD_P 0     /* level-1 pressure, FP64, canonical with ghosts */
 #define H3D_FIELD_B 1     /* level-1 right-hand side, FP64, canonical interior */
+/* Face velocities of the projection, FP64, canonical with the ghost layer:
+ * entry (x,y,z) of U is the east face of cell (x,y,z) (x = 0: the block's
+ * west face), V north faces, W top faces; the host arrays are the reference's
+ * dom(ib)%u, v, w (module_multidata.for:52) and ustar, vstar, wstar (:64-65). */
+#define H3D_FIELD_U 2
+#define H3D_FIELD_V 3
+#define H3D_FIELD_W 4
+#define H3D_FIELD_USTAR 5
+#define H3D_FIELD_VSTAR 6
+#define H3D_FIELD_WSTAR 7
 /* Copy block ib of a resident field from/to a host field (ttc dims, pl ghosts). */
 int h3d_mg_upload(h3d_mg* h, int32_t field, int32_t ib, const double* host);
 int h3d_mg_download(h3d_mg* h, int32_t field, int32_t ib, double* host);
@@ -135,6 +150,40 @@ int h3d_mg_residual(h3d_mg* h, double* rr, double* bb, double* rinf);
 /* Relative residual history of the last solve (n <= cap entries written). */
 int h3d_mg_history(h3d_mg* h, double* out, int32_t cap, int32_t* n);
 
+/* --- the projection on resident fields (press.for, newsolv_mg.for) ------ */
+/* calvel (press.for:77-144) with its exchange(1..3): U, V, W from USTAR,
+ * VSTAR, WSTAR and the resident pressure, on the faces the reference updates
+ * (every interior face but the last one before a physical wall,
+ * localparameters.for:186-192), divided by the face density for L_LSM (the
+ * density of h3d_mg_set_density, ghost layer included); then the face ghosts
+ * of the interior rows from the neighbouring or periodic block.  Faces on
+ * physical walls keep their values (the boundary condition). */
+int h3d_mg_calvel(h3d_mg* h, double dt, double alfapr);
+/* calmas (press.for:2-75, second-order branch): su = div u / dt (L_LSM:
+ * sup = div u * dx*dy*dz / dt) into H3D_FIELD_B and the level-1 right-hand
+ * side; *rmax = max |div u * dx*dy*dz| (:61-63), *su2 = sum su^2 (either may
+ * be NULL). */
+int h3d_mg_calmas(h3d_mg* h, double dt, double* rmax, double* su2);
+/* exchange(4) + pbound (press.for:146-207) on the resident pressure: every
+ * face ghost of the interior rows from the neighbour, periodic partner or
+ * (physical wall) the adjacent interior cell. */
+int h3d_mg_pbound(h3d_mg* h);
+/* newsolv_mg (newsolv_mg.for:2-93) with the velocities: calvel, calmas, then
+ * per iteration mgkcyc on pp = 0 with rhs su (MIXED: FP32 V-cycles), p = p +
+ * pp over the block and its ghost layer, exchange(4) + pbound, calvel,
+ * calmas.  stop_rule 1: the reference's rmax < tol .and. iter > 1 (:57);
+ * stop_rule 0: ||su||2 <= tol * ||su||2 of the first calmas (info->bnorm);
+ * stop_rule 2 is rejected.  info->rmax and info->relres report the last
+ * calmas.  Reads P, U, V, W, USTAR, VSTAR, WSTAR; writes P, U, V, W, B.
+ * Edge and corner ghosts of P keep p + pp (calvel does not read them). */
+int h3d_mg_project_resident(h3d_mg* h, double dt, double alfapr, const h3d_solve_opts* opts,
+                            h3d_solve_info* info);
+/* The same from host fields (ttc dims, pl ghosts; the first ghost layer is
+ * read and written): p, u, v, w in/out, ustar, vstar, wstar in. */
+int h3d_mg_project(h3d_mg* h, double* const* p, double* const* u, double* const* v, double* const* w,
+                   const double* const* ustar, const double* const* vstar, const double* const* wstar,
+                   double dt, double alfapr, const h3d_solve_opts* opts, h3d_solve_info* info);
+
 /* --- reference subroutines on the resident level state ----------------- */
 /* Canonical level arrays of block ib at level g; field 0 = phi, 1 = rhs. */
 int h3d_mg_put_level(h3d_mg* h, int32_t g, int32_t field, int32_t ib, const double* a);
@@ -146,6 +195,22 @@ int h3d_mg_mgbound(h3d_mg* h, int32_t g);               /* mgsolver.for:912-997 
 int h3d_mg_exchangepp(h3d_mg* h, int32_t g);            /* exchangepp.for:2-2835 */
 int h3d_mg_vcycle(h3d_mg* h);                           /* mgkcyc body on level state */
 int h3d_mg_sync(h3d_mg* h);
+
+/* --- failure detection --------------------------------------------------- */
+/* Limit, in SM clocks, of every bounded device wait (the mbarrier waits of the
+ * TMA-staged kernels) on this handle's GPU; <= 0 restores the default 2^26
+ * (tens of milliseconds, where a plane copy takes microseconds).  A wait that
+ * runs out makes the call return H3D_ERR_TIMEOUT; the kernel finishes (after
+ * the copies it issued have landed) and the handle stays usable.  The limit
+ * lives in the library's device memory: it applies to every handle on that
+ * GPU.  No counterpart in the reference (its waits are MPI_WAIT). */
+int h3d_mg_set_wait_limit(h3d_mg* h, int64_t clocks);
+/* Runs one bounded wait that cannot complete (an mbarrier nothing arrives
+ * at) with the current limit: returns H3D_ERR_TIMEOUT once the limit has run
+ * out, the way a sweep whose plane copy never lands would, and the handle
+ * stays usable.  For checking the failure path; no counterpart in the
+ * reference. */
+int h3d_mg_wait_probe(h3d_mg* h);
 
 /* --- profiling ----------------------------------------------------------- */
 /* 1: bracket every level-1 smoother launch with CUDA events on the solve

@@ -19,7 +19,9 @@ semantics:
   * set-up: localparameters.for (pl, isp..kep, ttc, rdv, nwork/cof sizing,
     ngg/ngc/nge);
   * the solver: mgsolver.for (coeff, mgkcyc, mgrelax, mgrestr, mgcorr,
-    mgbound) and exchangepp.for (exchangepp, exchbc_mgpp).
+    mgbound) and exchangepp.for (exchangepp, exchbc_mgpp);
+  * the projection: press.for (calmas, calvel, pbound), exchange.for
+    (exchange, exchange_smlvl) and exchange_bc.for (exchange_bc).
 Fortran semantics kept: default REAL and real literals are 8-byte (the
 reference's -real-size 64); integer division truncates toward zero; integer
 MOD takes the dividend's sign; assignment of a real to an integer truncates;
@@ -943,6 +945,33 @@ class UnitTranslator:
                 self.emit("pass")
             self.ind -= 1
             return i + 1
+        m = re.match(r"^select\s*case\s*\((.*)\)$", t)
+        if m:  # SELECT CASE with scalar case values (no ranges)
+            self.tmp += 1
+            sv = "_sel%d" % self.tmp
+            self.emit("%s = %s" % (sv, self.ex(parse_expr(m.group(1)))[0]))
+            j, first = i + 1, True
+            while True:
+                tj = stmts[j][2]
+                if re.match(r"^end\s*select$", tj):
+                    if first:
+                        self.emit("pass")
+                    return j + 1
+                mc = re.match(r"^case\s*\((.*)\)$", tj)
+                if mc:
+                    vals = _split_top(mc.group(1))
+                    if any(":" in v for v in vals):
+                        raise FortranError("case ranges are not supported")
+                    cond = " or ".join("%s == %s" % (sv, self.ex(parse_expr(v))[0]) for v in vals)
+                    self.emit(("if %s:" if first else "elif %s:") % cond)
+                elif re.match(r"^case\s+default$", tj):
+                    self.emit("else:" if not first else "if True:")
+                else:
+                    raise FortranError("statement before the first case")
+                first = False
+                self.ind += 1
+                j = self.block(stmts, j + 1, [r"^case\b", r"^end\s*select$"])
+                self.ind -= 1
         m = re.match(r"^go\s*to\s*(\d+)$", t)
         if m:
             if self.depth:
@@ -1028,6 +1057,9 @@ SOLVER_UNITS = {
     "mgsolver.for": ["coeff", "mgkcyc", "mgrelax", "mgrestr", "mgcorr", "mgbound"],
     "exchangepp.for": ["exchangepp", "exchbc_mgpp"],
     "localparameters.for": ["localparameters"],
+    "press.for": ["calmas", "calvel", "pbound"],
+    "exchange.for": ["exchange", "exchange_smlvl"],
+    "exchange_bc.for": ["exchange_bc"],
 }
 MODULE_FILES = ["module_vars.for", "module_multidata.for", "module_mpi.for"]
 MPI_CONSTANTS = {"mpi_comm_world": 0, "mpi_double_precision": 1, "mpi_integer": 2, "mpi_max": 3,
@@ -1129,9 +1161,10 @@ class Reference:
         for ib in range(1, nb + 1):
             o = M.v_dom.g(ib)
             tti, ttj, ttk = o.c_ttc_i, o.c_ttc_j, o.c_ttc_k
-            for f in ("pp", "su", "sup", "dens", "p"):
-                setattr(o, "c_" + f, FArray("r", [(1, tti), (1, ttj), (1, ttk)]))
+            for f in ("pp", "su", "sup", "dens", "p", "u", "v", "w", "ustar", "vstar", "wstar"):
+                setattr(o, "c_" + f, FArray("r", [(1, tti), (1, ttj), (1, ttk)]))  # initial.for:146-160
             o.c_faz = FArray("i", [(1, ngrd_gl)])                       # initial.for:250
+            o.c_stfcinf = FArray("r", [(1, 6), (1, M.v_pl), (1, M.v_ngg)])  # initial.for:183
             for f in ("sendb_m1", "sendb_p1", "recvb_m1", "recvb_p1", "sendb_m2", "sendb_p2",
                       "recvb_m2", "recvb_p2", "sendb_m3", "sendb_p3", "recvb_m3", "recvb_p3"):
                 setattr(o, "c_" + f, FArray("r", [(1, M.v_ngg)]))          # initial.for:252-257

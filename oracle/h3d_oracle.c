@@ -308,6 +308,36 @@ void or_get_coef(const or_mg* m, int g, int ib, int s, double* a) {
             d->cof[cofidx(d, g, ni, nj, i, j, k) + s * incr];
 }
 
+/* Multiplies the seven coefficient slots (aw..ap) of level g by s.  Not a
+ * reference routine: it models the product's consistent coarse-level
+ * scaling of the L_LSM coefficients (s = 4^-(g-1)), under which the coarse
+ * correction of the FV-integrated operator is the consistent one instead of
+ * 4^-(g-1) of it (coeff uses the fine dx, dy, dz on every level,
+ * mgsolver.for:130-184). */
+void or_scale_level_coef(or_mg* m, int g, double s) {
+  for (int ib = 0; ib < m->nbp; ++ib) {
+    or_dom* d = &m->dom[ib];
+    int ni, nj, nk;
+    lev_dims(d, g, &ni, &nj, &nk);
+    int64_t incr = (int64_t)(ni - 2) * (nj - 2) * (nk - 2);
+    for (int64_t q = 0; q < 7 * incr; ++q) d->cof[d->faz[g] + 1 + q] *= s;
+  }
+}
+
+/* Overwrites coefficient slot s of level g (interior, x fastest).  Not a
+ * reference routine: lets tests model the product's coarse operators. */
+void or_set_coef(or_mg* m, int g, int ib, int s, const double* a) {
+  or_dom* d = &m->dom[ib];
+  int ni, nj, nk;
+  lev_dims(d, g, &ni, &nj, &nk);
+  int64_t incr = (int64_t)(ni - 2) * (nj - 2) * (nk - 2);
+  for (int k = 2; k <= nk - 1; ++k)
+    for (int j = 2; j <= nj - 1; ++j)
+      for (int i = 2; i <= ni - 1; ++i)
+        d->cof[cofidx(d, g, ni, nj, i, j, k) + s * incr] =
+            a[((int64_t)(k - 2) * (nj - 2) + (j - 2)) * (ni - 2) + (i - 2)];
+}
+
 void or_put_rhs(or_mg* m, int g, int ib, const double* a) {
   or_dom* d = &m->dom[ib];
   int ni, nj, nk;
@@ -1010,6 +1040,213 @@ int or_solve(or_mg* m, double* const* p, const double* const* b, double tol,
   free(pp);
   return status;
 }
+
+/* ------------------------------------------------------------- projection */
+/* Canonical index of cell (x, y, z) of a level-1 block array (nz+2, ny+2,
+ * nx+2), x fastest, one ghost layer. */
+#define CAN(x, y, z) ((((int64_t)(z)) * (ny + 2) + (y)) * (nx + 2) + (x))
+
+void or_calvel(or_mg* m, double* const* u, double* const* v, double* const* w,
+               const double* const* us, const double* const* vs, const double* const* ws,
+               const double* const* p, const double* const* dens, double dt, double alfapr) {
+  /* press.for:77-144.  Update ranges isu..ieu etc. (localparameters.for:
+   * 106-133, 186-192): every interior face except the last one of an axis
+   * that ends in a physical wall (no neighbour, bc /= 5). */
+  for (int ib = 0; ib < m->nbp; ++ib) {
+    const or_dom* d = &m->dom[ib];
+    const int nx = d->d.n[0], ny = d->d.n[1], nz = d->d.n[2];
+    const double dx = d->d.h[0], dy = d->d.h[1], dz = d->d.h[2];
+    const int ieu = nx - ((d->d.nb_face[1] < 0 && d->d.bc[1] != 5) ? 1 : 0);
+    const int jev = ny - ((d->d.nb_face[3] < 0 && d->d.bc[3] != 5) ? 1 : 0);
+    const int kew = nz - ((d->d.nb_face[5] < 0 && d->d.bc[5] != 5) ? 1 : 0);
+    const double* P = p[ib];
+    const double* D = m->lsm ? dens[ib] : NULL;
+    for (int k = 1; k <= nz; ++k) /* :88-101 */
+      for (int i = 1; i <= ieu; ++i)
+        for (int j = 1; j <= ny; ++j) {
+          int64_t q = CAN(i, j, k);
+          if (m->lsm)
+            u[ib][q] = (us[ib][q] - dt * alfapr * (P[q + 1] - P[q]) / dx / (0.5 * (D[q] + D[q + 1])));
+          else
+            u[ib][q] = (us[ib][q] - dt * alfapr * (P[q + 1] - P[q]) / dx);
+        }
+    const int64_t sx = nx + 2, sxy = (int64_t)(nx + 2) * (ny + 2);
+    for (int k = 1; k <= nz; ++k) /* :104-118 */
+      for (int i = 1; i <= nx; ++i)
+        for (int j = 1; j <= jev; ++j) {
+          int64_t q = CAN(i, j, k);
+          if (m->lsm)
+            v[ib][q] = (vs[ib][q] - dt * alfapr * (P[q + sx] - P[q]) / dy / (0.5 * (D[q] + D[q + sx])));
+          else
+            v[ib][q] = (vs[ib][q] - dt * alfapr * (P[q + sx] - P[q]) / dy);
+        }
+    for (int k = 1; k <= kew; ++k) /* :120-134 */
+      for (int i = 1; i <= nx; ++i)
+        for (int j = 1; j <= ny; ++j) {
+          int64_t q = CAN(i, j, k);
+          if (m->lsm)
+            w[ib][q] = (ws[ib][q] - dt * alfapr * (P[q + sxy] - P[q]) / dz / (0.5 * (D[q] + D[q + sxy])));
+          else
+            w[ib][q] = (ws[ib][q] - dt * alfapr * (P[q + sxy] - P[q]) / dz);
+        }
+  }
+}
+
+/* The source of the face ghosts of face f (0..5 = W,E,S,N,B,T) of block ib
+ * in the velocity exchanges: the neighbour (exchange_smlvl), the periodic
+ * partner or the block itself (exchange_bc), or -1 for a physical wall. */
+static int vel_face_source(const or_mg* m, int ib, int f) {
+  const or_block_desc* d = &m->dom[ib].d;
+  if (d->nb_face[f] >= 0) return d->nb_face[f];
+  if (d->bc[f] != 5) return -1;
+  if (d->nb_face[f ^ 1] < 0) return ib; /* single block along the axis: own wrap */
+  return d->nb_periodic[f];
+}
+
+void or_vel_exchange(or_mg* m, double* const* fld) {
+  /* exchange(1..3) as calvel ends (press.for:140-142), equal resolution:
+   * exchange_bc (exchange_bc.for:17-...) then exchange_smlvl (exchange.for:
+   * 302-1650).  Face ghost layer 0 on the interior rows (the rows the
+   * unpack loops kspr..kepr, jspr..jepr cover, exchange.for:1560-1640):
+   * a low-side ghost (x = 0) takes the source's last interior plane
+   * (ie - ly with ie = its iep, x = nx), a high-side ghost (x = nx+1) the
+   * source's first (is + ly, x = 1).  Physical walls keep their values.
+   * Every written cell reads an interior cell, so the order is free. */
+  for (int ib = 0; ib < m->nbp; ++ib) {
+    const or_dom* d = &m->dom[ib];
+    const int nx = d->d.n[0], ny = d->d.n[1], nz = d->d.n[2];
+    for (int f = 0; f < 6; ++f) {
+      const int s = vel_face_source(m, ib, f);
+      if (s < 0) continue;
+      const or_dom* S = &m->dom[s];
+      const int sx_ = S->d.n[0], sy_ = S->d.n[1], sz_ = S->d.n[2];
+      const int ax = f / 2, hi = f & 1;
+      const double* src = fld[s];
+      double* dst = fld[ib];
+      for (int k = 1; k <= (ax == 2 ? 1 : nz); ++k)
+        for (int j = 1; j <= (ax == 1 ? 1 : ny); ++j)
+          for (int i = 1; i <= (ax == 0 ? 1 : nx); ++i) {
+            int x = i, y = j, z = k, xs = i, ys = j, zs = k;
+            if (ax == 0) { x = hi ? nx + 1 : 0; xs = hi ? 1 : sx_; }
+            if (ax == 1) { y = hi ? ny + 1 : 0; ys = hi ? 1 : sy_; }
+            if (ax == 2) { z = hi ? nz + 1 : 0; zs = hi ? 1 : sz_; }
+            int64_t qs = (((int64_t)zs) * (sy_ + 2) + ys) * (sx_ + 2) + xs;
+            dst[CAN(x, y, z)] = src[qs];
+          }
+    }
+  }
+}
+
+double or_calmas(or_mg* m, const double* const* u, const double* const* v, const double* const* w,
+                 double dt, double* const* su, double* rmax) {
+  /* press.for:2-75, second-order branch (:40-62): fact = div u; su = fact/dt
+   * (L_LSM: sup = fact*dx*dy*dz/dt); rmax = max |fact*dx*dy*dz|.  Returns
+   * the sum of su^2 (per-plane partial sums added in plane order). */
+  double ss = 0.0, rm = 0.0;
+  for (int ib = 0; ib < m->nbp; ++ib) {
+    const or_dom* d = &m->dom[ib];
+    const int nx = d->d.n[0], ny = d->d.n[1], nz = d->d.n[2];
+    const double dx = d->d.h[0], dy = d->d.h[1], dz = d->d.h[2];
+    const int64_t sx = nx + 2, sxy = (int64_t)(nx + 2) * (ny + 2);
+    double* part = (double*)calloc((size_t)2 * nz, sizeof(double));
+#pragma omp parallel for num_threads(g_threads) schedule(static) if (g_threads > 1)
+    for (int k = 1; k <= nz; ++k) {
+      double s2 = 0.0, mx = 0.0;
+      for (int i = 1; i <= nx; ++i)
+        for (int j = 1; j <= ny; ++j) {
+          int64_t q = CAN(i, j, k);
+          double fact = ((u[ib][q] - u[ib][q - 1]) / dx + (v[ib][q] - v[ib][q - sx]) / dy +
+                         (w[ib][q] - w[ib][q - sxy]) / dz);
+          double r = m->lsm ? fact * dx * dy * dz / dt : fact / dt;
+          su[ib][((int64_t)(k - 1) * ny + (j - 1)) * nx + (i - 1)] = r;
+          s2 += r * r;
+          double fact1 = fact * dx * dy * dz;
+          double a = fabs(fact1);
+          if (!(a <= mx)) mx = a; /* keeps a NaN */
+        }
+      part[2 * k - 2] = s2;
+      part[2 * k - 1] = mx;
+    }
+    for (int k = 1; k <= nz; ++k) {
+      ss += part[2 * k - 2];
+      if (!(part[2 * k - 1] <= rm)) rm = part[2 * k - 1];
+    }
+    free(part);
+  }
+  if (rmax) *rmax = rm;
+  return ss;
+}
+
+int or_project(or_mg* m, double* const* p, double* const* u, double* const* v, double* const* w,
+               const double* const* us, const double* const* vs, const double* const* ws,
+               const double* const* dens, double dt, double alfapr, double tol, int maxcy,
+               int stop_rule, int* cycles, double* relres, double* rmax_out, double* history) {
+  /* newsolv_mg.for:2-93 with the velocities: calvel, calmas, then per
+   * iteration mgkcyc on pp = 0 with rhs su (sup for L_LSM), p = p + (pp -
+   * ppref) over the block and its ghost layer, exchange(4) + pbound, calvel,
+   * calmas.  stop_rule 1: rmax < tol .and. iter > 1 (:57); stop_rule 0:
+   * ||su||2 <= tol * ||su||2 of the first calmas.  history (may be NULL)
+   * receives maxcy+1 entries (rmax for rule 1, the relative norm for 0). */
+  int nb = m->nbp;
+  double** su = (double**)calloc((size_t)nb, sizeof(double*));
+  double** pp = (double**)calloc((size_t)nb, sizeof(double*));
+  for (int ib = 0; ib < nb; ++ib) {
+    const or_dom* d = &m->dom[ib];
+    size_t ni = (size_t)d->d.n[0], nj = (size_t)d->d.n[1], nk = (size_t)d->d.n[2];
+    su[ib] = (double*)calloc(ni * nj * nk, sizeof(double));
+    pp[ib] = (double*)calloc((ni + 2) * (nj + 2) * (nk + 2), sizeof(double));
+  }
+  double rmax;
+  or_calvel(m, u, v, w, us, vs, ws, (const double* const*)p, dens, dt, alfapr); /* :16-17 */
+  or_vel_exchange(m, u);
+  or_vel_exchange(m, v);
+  or_vel_exchange(m, w);
+  double s0 = sqrt(or_calmas(m, (const double* const*)u, (const double* const*)v, (const double* const*)w, dt,
+                             su, &rmax));
+  double bn = s0 > 0 ? s0 : 1.0, rel = s0 / bn;
+  if (history) history[0] = stop_rule == 1 ? rmax : rel;
+  int iter = 0, status = 1;
+  if (stop_rule == 0 && rel <= tol) status = 0;
+  while (status != 0 && iter < maxcy) {
+    for (int ib = 0; ib < nb; ++ib) {
+      const or_dom* d = &m->dom[ib];
+      size_t n = (size_t)(d->d.n[0] + 2) * (d->d.n[1] + 2) * (d->d.n[2] + 2);
+      memset(pp[ib], 0, n * sizeof(double)); /* :20-22, :45 */
+    }
+    or_mgkcyc(m, pp, (const double* const*)su); /* :26 */
+    ++iter;
+    for (int ib = 0; ib < nb; ++ib) { /* :39-49, ppref = 0 */
+      const or_dom* d = &m->dom[ib];
+      size_t n = (size_t)(d->d.n[0] + 2) * (d->d.n[1] + 2) * (d->d.n[2] + 2);
+      for (size_t q = 0; q < n; ++q) p[ib][q] = (p[ib][q] + (pp[ib][q] - 0.0));
+    }
+    /* exchange(4) + pbound (:51-52): the level-1 exchangepp gives every face
+     * ghost the value they give (or_residual); edge and corner ghosts are
+     * not read by calvel */
+    for (int ib = 0; ib < nb; ++ib) or_put_phi(m, 1, ib, p[ib]);
+    or_exchangepp(m, 1);
+    for (int ib = 0; ib < nb; ++ib) or_get_phi(m, 1, ib, p[ib]);
+    or_calvel(m, u, v, w, us, vs, ws, (const double* const*)p, dens, dt, alfapr); /* :54 */
+    or_vel_exchange(m, u);
+    or_vel_exchange(m, v);
+    or_vel_exchange(m, w);
+    double s = sqrt(or_calmas(m, (const double* const*)u, (const double* const*)v, (const double* const*)w, dt,
+                              su, &rmax)); /* :55 */
+    rel = s / bn;
+    if (history) history[iter] = stop_rule == 1 ? rmax : rel;
+    if (stop_rule == 0 && rel <= tol) status = 0;
+    if (stop_rule == 1 && rmax < tol && iter > 1) status = 0; /* :57 */
+    if (!isfinite(rel)) { status = 2; break; }
+  }
+  if (cycles) *cycles = iter;
+  if (relres) *relres = rel;
+  if (rmax_out) *rmax_out = rmax;
+  for (int ib = 0; ib < nb; ++ib) { free(su[ib]); free(pp[ib]); }
+  free(su);
+  free(pp);
+  return status;
+}
+#undef CAN
 
 /* --------------------------------------------------------------- topology */
 int or_topology(int nblocks, const int32_t* ext, const int32_t* bc,

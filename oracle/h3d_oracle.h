@@ -11,7 +11,8 @@
  * toolchain is in the image).  The oracle is pinned by (a) golden fixtures
  * made by running the reference's own Fortran source (coeff, mgkcyc,
  * mgrelax, mgrestr, mgcorr, mgbound, exchangepp, exchbc_mgpp,
- * localparameters) through the statement-by-statement translator in
+ * localparameters; calvel, calmas, pbound, exchange, exchange_smlvl,
+ * exchange_bc) through the statement-by-statement translator in
  * oracle/fortran_ref.py (tests/golden/make_golden.py; the oracle reproduces
  * every fixture bit for bit, tests/test_golden.py), and (b) algebraic
  * properties (manufactured Neumann cosine modes, null space, symmetry).
@@ -68,6 +69,12 @@ void or_get_rhs(const or_mg* m, int g, int ib, double* a);
 /* Coefficient slot s (0 aw,1 ae,2 as,3 an,4 ab,5 at,6 ap) interior-only. */
 void or_get_coef(const or_mg* m, int g, int ib, int s, double* a);
 
+/* Scales the coefficient slots aw..ap of level g by s (not a reference
+ * routine: models the product's consistent L_LSM coarse scaling). */
+void or_scale_level_coef(or_mg* m, int g, double s);
+/* Overwrites coefficient slot s of level g, block ib (interior, x fastest). */
+void or_set_coef(or_mg* m, int g, int ib, int s, const double* a);
+
 /* Reference subroutines on the resident state. */
 void or_mgrelax(or_mg* m, int g, int it);   /* mgsolver.for:374-621 */
 void or_mgrestr(or_mg* m, int g);           /* mgsolver.for:623-766 */
@@ -94,6 +101,27 @@ double or_residual(or_mg* m, double* const* p, const double* const* b,
 int or_solve(or_mg* m, double* const* p, const double* const* b, double tol,
              int maxcy, int stop_rule, int* cycles, double* relres,
              double* history);
+
+/* The projection (press.for:2-144, newsolv_mg.for:2-93).  Face velocities
+ * use the canonical level-1 layout of the cell they belong to: u(x,y,z) is
+ * the east face of cell (x,y,z), x = 0 the block's west face (a ghost), and
+ * likewise v (north faces) and w (top faces).  dens (L_LSM only) is the
+ * level-1 density, canonical with its face ghosts as the host's exchange
+ * left them. */
+void or_calvel(or_mg* m, double* const* u, double* const* v, double* const* w,
+               const double* const* us, const double* const* vs, const double* const* ws,
+               const double* const* p, const double* const* dens, double dt, double alfapr);
+/* exchange(1..3) of one velocity component: face ghosts, interior rows. */
+void or_vel_exchange(or_mg* m, double* const* fld);
+/* calmas: su (interior, (nz,ny,nx)) and rmax; returns sum su^2. */
+double or_calmas(or_mg* m, const double* const* u, const double* const* v, const double* const* w,
+                 double dt, double* const* su, double* rmax);
+/* newsolv_mg with the velocities.  Returns 0 converged, 1 not converged,
+ * 2 diverged. */
+int or_project(or_mg* m, double* const* p, double* const* u, double* const* v, double* const* w,
+               const double* const* us, const double* const* vs, const double* const* ws,
+               const double* const* dens, double dt, double alfapr, double tol, int maxcy,
+               int stop_rule, int* cycles, double* relres, double* rmax, double* history);
 
 /* Block topology from integer extents: read_infodom neighbour discovery
  * (alloc_dom.for:524-1200).  ext is nblocks x 6 (x0,x1,y0,y1,z0,z1) in global

@@ -72,11 +72,20 @@ def lib():
         for nm in ("or_mgrestr", "or_mgcorr", "or_mgbound", "or_exchangepp", "or_exchbc_mgpp"):
             getattr(L, nm).argtypes = [vp, i32]
         L.or_vcycle.argtypes = [vp]
+        L.or_scale_level_coef.argtypes = [vp, i32, dbl]
+        L.or_set_coef.argtypes = [vp, i32, i32, i32, pd]
         L.or_mgkcyc.argtypes = [vp, ppd, ppd]
         L.or_residual.argtypes = [vp, ppd, ppd, ppd, pd, pd]
         L.or_residual.restype = dbl
         L.or_solve.argtypes = [vp, ppd, ppd, dbl, i32, i32, C.POINTER(C.c_int), pd, pd]
         L.or_solve.restype = i32
+        L.or_calvel.argtypes = [vp, ppd, ppd, ppd, ppd, ppd, ppd, ppd, ppd, dbl, dbl]
+        L.or_vel_exchange.argtypes = [vp, ppd]
+        L.or_calmas.argtypes = [vp, ppd, ppd, ppd, dbl, ppd, pd]
+        L.or_calmas.restype = dbl
+        L.or_project.argtypes = [vp, ppd, ppd, ppd, ppd, ppd, ppd, ppd, ppd, dbl, dbl, dbl, i32, i32,
+                                 C.POINTER(C.c_int), pd, pd, pd]
+        L.or_project.restype = i32
         L.or_topology.argtypes = [i32, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(BlockDesc)]
         L.or_topology.restype = i32
         L.or_set_threads.argtypes = [i32]
@@ -177,6 +186,13 @@ class Oracle:
         lib().or_get_coef(self._h, g, ib, s, _dp(a))
         return a
 
+    def set_coef(self, g, ib, s, a):
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        lib().or_set_coef(self._h, g, ib, s, _dp(a))
+
+    def scale_level_coef(self, g, s):
+        lib().or_scale_level_coef(self._h, g, s)
+
     def mgrelax(self, g, it):
         lib().or_mgrelax(self._h, g, it)
 
@@ -219,4 +235,45 @@ class Oracle:
         st = lib().or_solve(self._h, _ptrs(p), _ptrs(b), tol, maxcy, stop_rule,
                             C.byref(cyc), C.byref(rel), _dp(hist))
         return dict(p=p, status=st, cycles=cyc.value, relres=rel.value,
+                    history=hist[: cyc.value + 1])
+
+    # projection (press.for:2-144, newsolv_mg.for:2-93) ----------------------
+    def _dens_ptrs(self, dens):
+        if dens is None:
+            return None, _ptrs([np.zeros(1)] * self.nb)
+        d = [np.ascontiguousarray(a, dtype=np.float64) for a in dens]
+        return d, _ptrs(d)
+
+    def calvel(self, u, v, w, us, vs, ws, p, dt, alfapr=1.0, dens=None):
+        """calvel followed by its exchange(1..3); u, v, w (canonical face
+        arrays) are updated in place and returned."""
+        u, v, w = ([np.ascontiguousarray(a, dtype=np.float64).copy() for a in f] for f in (u, v, w))
+        us, vs, ws, p = ([np.ascontiguousarray(a, dtype=np.float64) for a in f] for f in (us, vs, ws, p))
+        keep, dp = self._dens_ptrs(dens)
+        lib().or_calvel(self._h, _ptrs(u), _ptrs(v), _ptrs(w), _ptrs(us), _ptrs(vs), _ptrs(ws), _ptrs(p), dp,
+                        dt, alfapr)
+        for f in (u, v, w):
+            lib().or_vel_exchange(self._h, _ptrs(f))
+        return u, v, w
+
+    def calmas(self, u, v, w, dt):
+        """(su per block (nz, ny, nx), sum su^2, rmax)."""
+        u, v, w = ([np.ascontiguousarray(a, dtype=np.float64) for a in f] for f in (u, v, w))
+        su = [np.empty(self.dims(1, ib)) for ib in range(self.nb)]
+        rmax = C.c_double()
+        ss = lib().or_calmas(self._h, _ptrs(u), _ptrs(v), _ptrs(w), dt, _ptrs(su), C.byref(rmax))
+        return su, ss, rmax.value
+
+    def project(self, p, u, v, w, us, vs, ws, dt, alfapr=1.0, dens=None, tol=1e-8, maxcy=200, stop_rule=0):
+        p, u, v, w = ([np.ascontiguousarray(a, dtype=np.float64).copy() for a in f] for f in (p, u, v, w))
+        us, vs, ws = ([np.ascontiguousarray(a, dtype=np.float64) for a in f] for f in (us, vs, ws))
+        keep, dp = self._dens_ptrs(dens)
+        cyc = C.c_int()
+        rel = C.c_double()
+        rmax = C.c_double()
+        hist = np.zeros(maxcy + 1)
+        st = lib().or_project(self._h, _ptrs(p), _ptrs(u), _ptrs(v), _ptrs(w), _ptrs(us), _ptrs(vs), _ptrs(ws), dp,
+                              dt, alfapr, tol, maxcy, stop_rule, C.byref(cyc), C.byref(rel), C.byref(rmax),
+                              _dp(hist))
+        return dict(p=p, u=u, v=v, w=w, status=st, cycles=cyc.value, relres=rel.value, rmax=rmax.value,
                     history=hist[: cyc.value + 1])

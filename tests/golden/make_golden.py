@@ -1,4 +1,4 @@
-"""Write the golden mgkcyc fixtures of tests/golden/ from the reference's own Fortran.
+"""Write the golden fixtures of tests/golden/ from the reference's own Fortran.
 
     python tests/golden/make_golden.py        (needs the reference source tree)
 
@@ -11,6 +11,10 @@ the multigrid path must never read, are filled with NaN in the reference run.
 
 Stored per block (x fastest, one ghost layer): pp_in, pp_out (nz+2, ny+2,
 nx+2), su (nz, ny, nx) and, for L_LSM cases, dens (nz, ny, nx).
+
+The project_*.npz fixtures run the reference's calvel, calmas, mgkcyc,
+exchange(4) and pbound (press.for, exchange.for, exchange_bc.for) in the
+order of newsolv_mg's loop; see run_projection_case.
 """
 import os
 import sys
@@ -91,11 +95,98 @@ def run_case(name, src_dir=REF_SRC):
     return out
 
 
+# The projection (newsolv_mg with the velocities): name -> (layout, bc, ngrd_gl, lsm, seed)
+PROJ_CASES = {
+    "walls_2x1x1": (grid((2, 1, 1), (8, 8, 8)), [W] * 6, 3, False, 201),
+    "periodic_x_2x2x1": (grid((2, 2, 1), (8, 8, 8)), [P, P, W, W, W, W], 3, False, 202),
+    "periodic_all_1x2x2": (grid((1, 2, 2), (8, 8, 8)), [P] * 6, 3, False, 203),
+    "lsm_periodic_y_2x2x1": (grid((2, 2, 1), (8, 8, 8)), [W, W, P, P, W, W], 3, True, 204),
+}
+DT, ALFAPR, NITER = 0.5, 0.9, 2
+
+
+def run_projection_case(name, src_dir=REF_SRC):
+    """The reference's own calvel (with its exchange(1..3)), calmas, mgkcyc,
+    exchange(4) and pbound in newsolv_mg's order (newsolv_mg.for:16-55),
+    NITER iterations from seeded p, u, v, w, ustar, vstar, wstar (wall faces
+    of u, v, w zero), pl = 1 so the host arrays are the canonical ones.
+    Stored per block: the inputs, and after the loop p, u, v, w, su (sup for
+    L_LSM) and the rmax after the first calmas and after every iteration."""
+    ext, bc, ngrd, lsm, seed = PROJ_CASES[name]
+    descs = O.topology(ext, bc, H, ngrd)
+    R = F.Reference(list(descs), ngrd, pl_ex=0, lsm=lsm, src_dir=src_dir)
+    M = R.M
+    M.v_rdivmax = 1        # alloc_dom.for: the largest rdiv (no refinement)
+    M.v_differencing = 1   # second-order branch of calmas (press.for:40-58)
+    M.v_dt = DT
+    M.v_alfapr = ALFAPR
+    assert R.pl == 1
+    rng = np.random.default_rng(seed)
+    out = {"ext": ext, "bc": np.array(bc, np.int32), "h": np.array(H), "ngrd_gl": ngrd, "lsm": int(lsm),
+           "nblocks": len(descs), "dt": DT, "alfapr": ALFAPR, "niter": NITER}
+    for ib, d in enumerate(descs):
+        nx, ny, nz = d.n
+        shp = (nz + 2, ny + 2, nx + 2)
+        for k in ("p", "ustar", "vstar", "wstar"):
+            a = rng.uniform(-1.0, 1.0, shp)
+            R.put_field(k, ib, a)
+            out["%s_in_%d" % (k, ib)] = a
+        for ax, k in enumerate(("u", "v", "w")):
+            a = rng.uniform(-1.0, 1.0, shp)
+            lo = d.nb_face[2 * ax] < 0 and d.bc[2 * ax] != 5
+            hi = d.nb_face[2 * ax + 1] < 0 and d.bc[2 * ax + 1] != 5
+            sl = [slice(None)] * 3
+            if lo:
+                sl[2 - ax] = 0
+                a[tuple(sl)] = 0.0
+            if hi:
+                sl[2 - ax] = d.n[ax]
+                a[tuple(sl)] = 0.0
+            R.put_field(k, ib, a)
+            out["%s_in_%d" % (k, ib)] = a
+        if lsm:
+            dens = rng.uniform(1.0, 4.0, shp)
+            R.put_field("dens", ib, dens)
+            out["dens_%d" % ib] = dens
+        R.put_field("pp", ib, np.zeros(shp))
+    R.call("coeff")
+    rmax = []
+    R.call("calvel")
+    R.call("calmas")
+    rmax.append(M.v_rmax)
+    for _ in range(NITER):
+        R.call("mgkcyc")
+        for ib in range(len(descs)):  # newsolv_mg.for:39-49 (ppref = 0)
+            p = R.get_field("p", ib)
+            pp = R.get_field("pp", ib)
+            R.put_field("p", ib, p + (pp - 0.0))
+            R.put_field("pp", ib, np.zeros_like(pp))
+        R.call("exchange", 4)
+        R.call("pbound")
+        R.call("calvel")
+        R.call("calmas")
+        rmax.append(M.v_rmax)
+    out["rmax"] = np.array(rmax)
+    for ib in range(len(descs)):
+        for k in ("p", "u", "v", "w"):
+            out["%s_out_%d" % (k, ib)] = R.get_field(k, ib)
+        s = R.get_field("sup" if lsm else "su", ib)
+        out["su_out_%d" % ib] = s[1:-1, 1:-1, 1:-1].copy()
+        for k in ("p_out", "u_out", "su_out"):
+            if not np.isfinite(out["%s_%d" % (k, ib)]).all():
+                raise RuntimeError("%s: the reference produced non-finite values" % name)
+    return out
+
+
 def main():
     for name in CASES:
         data = run_case(name)
         np.savez_compressed(os.path.join(HERE, "mgkcyc_%s.npz" % name), **data)
         print("wrote", name)
+    for name in PROJ_CASES:
+        data = run_projection_case(name)
+        np.savez_compressed(os.path.join(HERE, "project_%s.npz" % name), **data)
+        print("wrote project", name)
 
 
 if __name__ == "__main__":

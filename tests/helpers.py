@@ -30,3 +30,47 @@ def mean_removed_rel(a, b):
     a = a - a.mean()
     b = b - b.mean()
     return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def projection_fields(blocks, seed, lsm=False, dens_hi=1000.0):
+    """Seeded canonical per-block inputs of the projection (newsolv_mg with
+    velocities): p, u, v, w, ustar, vstar, wstar (and a density for L_LSM),
+    each (nz+2, ny+2, nx+2), x fastest.
+
+    Everything is random (ghosts included) except the velocity faces on
+    physical walls, which are zero, so the pressure equation is compatible
+    (the density, L_LSM only, is uniform in [1, dens_hi]):
+    u at x = 0 of a block whose west face is a wall and at x = nx when the east
+    face is, and likewise v and w."""
+    rng = np.random.default_rng(seed)
+    out = {k: [] for k in ("p", "u", "v", "w", "us", "vs", "ws", "dens")}
+    for d in blocks:
+        shp = (d.n[2] + 2, d.n[1] + 2, d.n[0] + 2)
+        for k in ("p", "us", "vs", "ws"):
+            out[k].append(rng.uniform(-1.0, 1.0, shp))
+        for ax, k in enumerate(("u", "v", "w")):
+            a = rng.uniform(-1.0, 1.0, shp)
+            lo = d.nb_face[2 * ax] < 0 and d.bc[2 * ax] != 5
+            hi = d.nb_face[2 * ax + 1] < 0 and d.bc[2 * ax + 1] != 5
+            idx_lo = [slice(None)] * 3
+            idx_hi = [slice(None)] * 3
+            idx_lo[2 - ax] = 0
+            idx_hi[2 - ax] = d.n[ax]
+            if lo:
+                a[tuple(idx_lo)] = 0.0
+            if hi:
+                a[tuple(idx_hi)] = 0.0
+            out[k].append(a)
+        out["dens"].append(rng.uniform(1.0, dens_hi, shp) if lsm else np.ones(shp))
+    return out
+
+
+def to_host(blocks, canon):
+    """Canonical per-block arrays -> host fields (ttc dims, pl ghosts)."""
+    res = []
+    for a, d in zip(canon, blocks):
+        h = np.zeros((d.ttc[2], d.ttc[1], d.ttc[0]))
+        p = d.pl
+        h[p - 1:p + d.n[2] + 1, p - 1:p + d.n[1] + 1, p - 1:p + d.n[0] + 1] = a
+        res.append(h)
+    return res

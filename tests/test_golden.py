@@ -99,3 +99,91 @@ def test_fixture_regenerates(oracle_mod, name):
     assert sorted(fresh) == sorted(old)
     for k in old:
         assert np.array_equal(np.asarray(fresh[k]), old[k]), k
+
+
+# -- the projection: calvel, calmas, exchange(1..4), pbound in newsolv_mg's loop
+PFILES = sorted(glob.glob(os.path.join(GOLDEN, "project_*.npz")))
+PNAMES = [os.path.basename(f)[len("project_"):-len(".npz")] for f in PFILES]
+
+
+def _pload(name):
+    with np.load(os.path.join(GOLDEN, "project_%s.npz" % name)) as z:
+        return {k: z[k] for k in z.files}
+
+
+def _face_mask(shape):
+    """Interior cells and face ghosts: what the projection defines (the
+    reference's exchanges also write edge and corner ghosts, which neither
+    calvel nor calmas reads)."""
+    g = [(np.arange(n) == 0) | (np.arange(n) == n - 1) for n in shape]
+    return (g[0][:, None, None].astype(int) + g[1][None, :, None] + g[2][None, None, :]) <= 1
+
+
+def test_projection_fixtures_present():
+    assert len(PNAMES) >= 4
+
+
+@pytest.mark.parametrize("name", PNAMES)
+def test_oracle_projection_matches_reference(oracle_mod, name):
+    g = _pload(name)
+    O = oracle_mod
+    nb, lsm = int(g["nblocks"]), bool(g["lsm"])
+    descs = O.topology(g["ext"], g["bc"], g["h"], int(g["ngrd_gl"]))
+    orc = O.Oracle(list(descs), int(g["ngrd_gl"]), 3, 2, 1, lsm=lsm)
+    dens = [g["dens_%d" % ib] for ib in range(nb)] if lsm else None
+    if lsm:
+        for ib in range(nb):
+            orc.set_density(ib, dens[ib][1:-1, 1:-1, 1:-1])
+    orc.coeff()
+    f = {k: [g["%s_in_%d" % (k, ib)] for ib in range(nb)] for k in ("p", "u", "v", "w", "ustar", "vstar", "wstar")}
+    res = orc.project(f["p"], f["u"], f["v"], f["w"], f["ustar"], f["vstar"], f["wstar"], float(g["dt"]),
+                      float(g["alfapr"]), dens=dens, tol=0.0, maxcy=int(g["niter"]), stop_rule=1)
+    assert res["cycles"] == int(g["niter"])
+    assert np.array_equal(res["history"], g["rmax"]), (res["history"], g["rmax"])
+    su, _, _ = orc.calmas(res["u"], res["v"], res["w"], float(g["dt"]))
+    for ib in range(nb):
+        m = _face_mask(res["p"][ib].shape)
+        for k in ("p", "u", "v", "w"):
+            got, want = res[k][ib], g["%s_out_%d" % (k, ib)]
+            assert np.array_equal(got[m], want[m]), (name, k, ib, float(np.abs(got[m] - want[m]).max()))
+        assert np.array_equal(su[ib], g["su_out_%d" % ib])
+    orc.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", PNAMES)
+def test_cuda_projection_matches_reference(h3d, name):
+    g = _pload(name)
+    nb, lsm = int(g["nblocks"]), bool(g["lsm"])
+    ngrd = int(g["ngrd_gl"])
+    blocks = h3d.topology.from_extents(g["ext"], g["bc"], g["h"], ngrd, pl=1)
+    s = h3d.MultigridSolver(blocks, ngrd, var_coef=lsm)
+    if lsm:
+        for ib in range(nb):
+            s.set_density(ib, np.ascontiguousarray(g["dens_%d" % ib]))
+    s.coeff()
+    f = {k: [np.ascontiguousarray(g["%s_in_%d" % (k, ib)]) for ib in range(nb)]
+         for k in ("p", "u", "v", "w", "ustar", "vstar", "wstar")}
+    info = s.project(f["p"], f["u"], f["v"], f["w"], f["ustar"], f["vstar"], f["wstar"], float(g["dt"]),
+                     float(g["alfapr"]), tol=0.0, maxcy=int(g["niter"]), stop_rule=1, history=True)
+    assert info["outer"] == int(g["niter"]) and not info["converged"]
+    assert np.array_equal(info["history"], g["rmax"])
+    for ib, d in enumerate(blocks):
+        m = _face_mask(f["p"][ib].shape)
+        for k in ("p", "u", "v", "w"):
+            got, want = f[k][ib], g["%s_out_%d" % (k, ib)]
+            assert np.array_equal(got[m], want[m]), (name, k, ib, float(np.abs(got[m] - want[m]).max()))
+        b = h3d.host_field(d)
+        s.download("b", ib, b)
+        assert np.array_equal(h3d.interior(b, d), g["su_out_%d" % ib])
+    s.close()
+
+
+@pytest.mark.skipif(_reference_tree() is None, reason="reference source tree not present")
+@pytest.mark.parametrize("name", ["walls_2x1x1", "lsm_periodic_y_2x2x1"])
+def test_projection_fixture_regenerates(oracle_mod, name):
+    fresh = _make_golden().run_projection_case(name)
+    old = _pload(name)
+    assert sorted(fresh) == sorted(old)
+    for k in old:
+        assert np.array_equal(np.asarray(fresh[k]), old[k]), k

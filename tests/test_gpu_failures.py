@@ -70,3 +70,29 @@ def test_incompatible_rhs_reports_not_converged(h3d):
     info = s.newsolv_mg([x.copy() for x in p], off, tol=1e-8, maxcy=20)
     assert info["status"] == h3d._lib.H3D_ERR_NOT_CONVERGED
     s.close()
+
+
+def test_bounded_device_wait_reports_timeout(h3d):
+    """A device wait on an mbarrier that nothing arrives at (the sweeps' own
+    bounded-wait routine) gives up after the limit set at run time (2^20
+    clocks, about half a millisecond), the host reads H3D_ERR_TIMEOUT, and
+    the same handle then solves the problem.  No copy is in flight and
+    nothing faults: the wait simply runs out."""
+    import time
+    blocks, b, p = _problem(h3d)
+    s = h3d.MultigridSolver(blocks, 3, use_graph=False)
+    s.coeff()
+    s.set_wait_limit(1 << 20)
+    try:
+        t0 = time.perf_counter()
+        assert s.wait_probe() == h3d._lib.H3D_ERR_TIMEOUT
+        assert time.perf_counter() - t0 < 5.0
+        # a solve under the short limit still completes (its copies land in microseconds)
+        info = s.newsolv_mg([x.copy() for x in p], b, tol=1e-8, maxcy=200)
+        assert info["converged"]
+    finally:
+        s.set_wait_limit(0)
+    assert s.wait_probe() == h3d._lib.H3D_ERR_TIMEOUT  # the default limit runs out too (tens of ms)
+    info = s.newsolv_mg([x.copy() for x in p], b, tol=1e-8, maxcy=200)
+    assert info["converged"] and info["relres"] <= 1e-8
+    s.close()
