@@ -452,7 +452,7 @@ def main():
     info = infos_mixed[-1]
     sm_ms = sum(i["smoother_ms"] for i in infos_prof)
     sm_n = sum(i["smoother_launches"] for i in infos_prof)
-    sm_bytes = sum(i["smoother_bytes"] for i in infos_prof)  # sweeps from a zero iterate move 8 B/cell, others 12
+    sm_bytes = sum(i["smoother_bytes"] for i in infos_prof)  # full sweeps: 12 B a cell (iterate, rhs, new iterate)
     bytes_launch = sm_bytes / max(sm_n, 1)
     avg_launch_ms = sm_ms / max(sm_n, 1)
     achieved = sm_bytes / (sm_ms * 1e-3) / 1e9 if sm_n else None
@@ -499,7 +499,8 @@ def main():
             "mcell_updates_per_s": round(mcell_updates(prob, info["cycles"]) / (value * 1e-3) / 1e6, 1),
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1) if achieved else None, "peak": peak,
                          "unit": "GB/s", "frac": round(achieved / peak, 4) if achieved else None,
-                         "traffic": traffic, "kernel": "level-1 FP32 smoother (autotuned variant %d)" % mixed.get_smoother(1)[0],
+                         "traffic": traffic, "kernel": "level-1 FP32 full red-black sweep (autotuned variant %d)"
+                         % mixed.get_smoother(1)[0],
                          "bytes_per_launch": bytes_launch, "avg_launch_ms": round(avg_launch_ms, 5),
                          "peak_source": peak_kind},
             "cpu_baseline": cpu, "e2e": e2e,

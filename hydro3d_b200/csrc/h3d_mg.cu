@@ -439,11 +439,14 @@ struct Exec {
     Level& V = L(g);
     cudaStream_t st = h->st;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
-    if (prof && g == 1 && prof_used + 2 <= prof->size()) {
+    // profiling brackets the full level-1 sweeps (3 words a cell); the first
+    // sweep from a zero iterate is another kernel with other bytes
+    const bool from_zero = mixed_level(g) ? V.zero32 : V.zero64;
+    if (prof && g == 1 && !from_zero && prof_used + 2 <= prof->size()) {
       e0 = (*prof)[prof_used++];
       e1 = (*prof)[prof_used++];
       CU(record(e0));
-      prof_bytes.push_back((mixed_level(g) ? V.zero32 : V.zero64) ? V.sweep_bytes_zero : V.sweep_bytes);
+      prof_bytes.push_back(V.sweep_bytes);
     }
     if (h->desc.mg_itrsch != 3) {  // lexicographic GS or line TDMA: one CTA per block
       const int nb = (int)V.geom.bl.size();

@@ -98,7 +98,8 @@ typedef struct h3d_solve_info {
   double rmax;            /* final max|b-Ap| * dV (calmas measure, press.for:61-63) */
   double bnorm;           /* ||b||2 */
   double device_ms;       /* device time of the solve, CUDA events on the solve stream */
-  double smoother_ms;     /* device time in level-1 smoother launches (profiling on) */
+  double smoother_ms;     /* device time in the full level-1 sweeps (profiling on; the first
+                             sweep from a zero iterate is not included) */
   int64_t smoother_launches;
   int64_t kernel_launches;/* kernels this library launched during the solve */
   double smoother_bytes;  /* algorithmic bytes of the profiled level-1 smoother launches */
@@ -213,8 +214,9 @@ int h3d_mg_set_wait_limit(h3d_mg* h, int64_t clocks);
 int h3d_mg_wait_probe(h3d_mg* h);
 
 /* --- profiling ----------------------------------------------------------- */
-/* 1: bracket every level-1 smoother launch with CUDA events on the solve
- * stream and add its duration to h3d_solve_info.smoother_ms. */
+/* 1: bracket every full level-1 sweep (not the first one from a zero
+ * iterate) with CUDA events on the solve stream and add its duration to
+ * h3d_solve_info.smoother_ms. */
 int h3d_mg_set_profiling(h3d_mg* h, int32_t on);
 /* Smoother kernel variant and z-chunk of level g (the autotuner's choice is
  * the default; H3D_ERR_ARG if the variant cannot run this level).  *nvariants

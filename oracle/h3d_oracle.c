@@ -1248,6 +1248,177 @@ int or_project(or_mg* m, double* const* p, double* const* u, double* const* v, d
 }
 #undef CAN
 
+/* -------------------------------------------------------------------- SIP */
+/* Stone's strongly implicit procedure on the pressure correction
+ * (sipsol.for:2-205, ifi = 44) with the coefficients pressure_1sweep builds
+ * (press.for:407-438: 1/dx^2, 1/dy^2, 1/dz^2, zero on the faces of physical
+ * walls, ap = -(aw+ae+as+an+ab+at)).  pp is canonical with the ghost layer
+ * (in/out), su interior.  The LU factors are rebuilt on every call, as the
+ * reference does.  resab (may be NULL) receives sum |res| of every sweep;
+ * returns the sweep count the reference leaves in nsweep. */
+#define SIPC(x, y, z) ((((int64_t)(z)) * (ny + 2) + (y)) * (nx + 2) + (x))
+typedef struct {
+  double aw, ae, as, an, ab, at, ap;
+} sip_coef;
+
+static sip_coef sip_cell_coef(const or_block_desc* d, int x, int y, int z) {
+  sip_coef c;
+  const double dx = d->h[0], dy = d->h[1], dz = d->h[2];
+  c.aw = 1.0 / (dx * dx);
+  c.ae = 1.0 / (dx * dx);
+  c.an = 1.0 / (dy * dy);
+  c.as = 1.0 / (dy * dy);
+  c.at = 1.0 / (dz * dz);
+  c.ab = 1.0 / (dz * dz);
+  if (d->nb_face[0] < 0 && d->bc[0] != 5 && x == 1) c.aw = 0.0;
+  if (d->nb_face[1] < 0 && d->bc[1] != 5 && x == d->n[0]) c.ae = 0.0;
+  if (d->nb_face[2] < 0 && d->bc[2] != 5 && y == 1) c.as = 0.0;
+  if (d->nb_face[3] < 0 && d->bc[3] != 5 && y == d->n[1]) c.an = 0.0;
+  if (d->nb_face[4] < 0 && d->bc[4] != 5 && z == 1) c.ab = 0.0;
+  if (d->nb_face[5] < 0 && d->bc[5] != 5 && z == d->n[2]) c.at = 0.0;
+  c.ap = -1.0 * (c.aw + c.ae + c.as + c.an + c.ab + c.at);
+  return c;
+}
+
+int or_sipsol(or_mg* m, double* const* pp, const double* const* su, int nswp, double* resab_hist) {
+  const double alfa = 0.92, small = 1e-20;
+  const int nb = m->nbp;
+  double** L = (double**)calloc((size_t)nb * 8, sizeof(double*));
+  for (int ib = 0; ib < nb; ++ib) {
+    const or_block_desc* d = &m->dom[ib].d;
+    const size_t n = (size_t)(d->n[0] + 2) * (d->n[1] + 2) * (d->n[2] + 2);
+    for (int q = 0; q < 8; ++q) L[8 * ib + q] = (double*)calloc(n, sizeof(double));
+  }
+  /* LU coefficients, sipsol.for:77-105 (loop order k, i, j) */
+  for (int ib = 0; ib < nb; ++ib) {
+    const or_block_desc* d = &m->dom[ib].d;
+    const int nx = d->n[0], ny = d->n[1], nz = d->n[2];
+    const int64_t sj = nx + 2, sk = (int64_t)(nx + 2) * (ny + 2);
+    double *lb = L[8 * ib], *lw = L[8 * ib + 1], *ls = L[8 * ib + 2], *lpr = L[8 * ib + 3];
+    double *un = L[8 * ib + 4], *ue = L[8 * ib + 5], *ut = L[8 * ib + 6];
+    for (int k = 1; k <= nz; ++k)
+      for (int i = 1; i <= nx; ++i)
+        for (int j = 1; j <= ny; ++j) {
+          const int64_t q = SIPC(i, j, k);
+          const sip_coef c = sip_cell_coef(d, i, j, k);
+          /* ijk-nij = k-1, ijk-nj = i-1, ijk-1 = j-1 (the reference's j-fastest index) */
+          lb[q] = c.ab / (1. + alfa * (un[q - sk] + ue[q - sk]));
+          lw[q] = c.aw / (1. + alfa * (un[q - 1] + ut[q - 1]));
+          ls[q] = c.as / (1. + alfa * (ue[q - sj] + ut[q - sj]));
+          const double p1 = alfa * (lb[q] * un[q - sk] + lw[q] * un[q - 1]);
+          const double p2 = alfa * (lb[q] * ue[q - sk] + ls[q] * ue[q - sj]);
+          const double p3 = alfa * (lw[q] * ut[q - 1] + ls[q] * ut[q - sj]);
+          lpr[q] = 1. / (c.ap + p1 + p2 + p3 - lb[q] * ut[q - sk] - lw[q] * ue[q - 1] - ls[q] * un[q - sj] + small);
+          un[q] = (c.an - p1) * lpr[q];
+          ue[q] = (c.ae - p2) * lpr[q];
+          ut[q] = (c.at - p3) * lpr[q];
+        }
+  }
+  double relast = 0.0, res1 = 0.0;
+  int nsweep;
+  for (nsweep = 1; nsweep <= nswp; ++nsweep) { /* :110-196 */
+    double resab = 0.0;
+    for (int ib = 0; ib < nb; ++ib) {
+      const or_block_desc* d = &m->dom[ib].d;
+      const int nx = d->n[0], ny = d->n[1], nz = d->n[2];
+      const int64_t sj = nx + 2, sk = (int64_t)(nx + 2) * (ny + 2);
+      double *lb = L[8 * ib], *lw = L[8 * ib + 1], *ls = L[8 * ib + 2], *lpr = L[8 * ib + 3];
+      double *un = L[8 * ib + 4], *ue = L[8 * ib + 5], *ut = L[8 * ib + 6], *res = L[8 * ib + 7];
+      double* fi = pp[ib];
+      for (int k = 1; k <= nz; ++k) /* residual, :146-157 */
+        for (int i = 1; i <= nx; ++i)
+          for (int j = 1; j <= ny; ++j) {
+            const int64_t q = SIPC(i, j, k);
+            const sip_coef c = sip_cell_coef(d, i, j, k);
+            const double s = su[ib][((int64_t)(k - 1) * ny + (j - 1)) * nx + (i - 1)];
+            res[q] = (s - c.ap * fi[q] - c.an * fi[q + sj] - c.as * fi[q - sj] - c.ae * fi[q + 1] - c.aw * fi[q - 1] -
+                      c.ab * fi[q - sk] - c.at * fi[q + sk]);
+            resab = resab + fabs(res[q]);
+          }
+      for (int k = 1; k <= nz; ++k) /* forward substitution, :159-167 */
+        for (int i = 1; i <= nx; ++i)
+          for (int j = 1; j <= ny; ++j) {
+            const int64_t q = SIPC(i, j, k);
+            res[q] = (res[q] - lb[q] * res[q - sk] - lw[q] * res[q - 1] - ls[q] * res[q - sj]) * lpr[q];
+          }
+      for (int k = nz; k >= 1; --k) /* backward substitution and correction, :169-178 */
+        for (int i = nx; i >= 1; --i)
+          for (int j = ny; j >= 1; --j) {
+            const int64_t q = SIPC(i, j, k);
+            res[q] = res[q] - un[q] * res[q + sj] - ue[q] * res[q + 1] - ut[q] * res[q + sk];
+            fi[q] = fi[q] + res[q];
+          }
+    }
+    if (resab_hist) resab_hist[nsweep - 1] = resab;
+    if (nsweep == 1) res1 = resab;
+    const double rsm = resab / (res1 + small);
+    or_vel_exchange(m, pp); /* exchange(44): face ghosts, walls untouched */
+    const double reldif = fabs(rsm - relast); /* :187-192 */
+    relast = rsm;
+    if (rsm <= 0.001) break;
+    if (reldif <= 0.00001) break;
+  }
+  if (nsweep > nswp) nsweep = nswp; /* :194 (the DO variable one past the end, minus one) */
+  for (int q = 0; q < nb * 8; ++q) free(L[q]);
+  free(L);
+  return nsweep;
+}
+#undef SIPC
+
+int or_pressure_1sweep(or_mg* m, double* const* p, double* const* u, double* const* v, double* const* w,
+                       const double* const* us, const double* const* vs, const double* const* ws, double dt,
+                       double alfapr, double eps, int niter, int nswp, int* iters, int* nsweeps, double* rmax_hist) {
+  /* press.for:382-519 without the boundary updates after the loop: calvel,
+   * then iterate calmas (stop on rmax < eps .and. iter > 1), sipsol(44) on
+   * pp = 0, p = p + (pp - ppref), exchange(4) + pbound, calvel, at most niter
+   * times.  rmax_hist (may be NULL) receives the rmax of every calmas (niter
+   * entries at most).  Returns the last rmax. */
+  const int nb = m->nbp;
+  double** su = (double**)calloc((size_t)nb, sizeof(double*));
+  double** pp = (double**)calloc((size_t)nb, sizeof(double*));
+  for (int ib = 0; ib < nb; ++ib) {
+    const or_dom* d = &m->dom[ib];
+    size_t ni = (size_t)d->d.n[0], nj = (size_t)d->d.n[1], nk = (size_t)d->d.n[2];
+    su[ib] = (double*)calloc(ni * nj * nk, sizeof(double));
+    pp[ib] = (double*)calloc((ni + 2) * (nj + 2) * (nk + 2), sizeof(double));
+  }
+  double rmax = 0.0;
+  int iter = 0, total = 0;
+  or_calvel(m, u, v, w, us, vs, ws, (const double* const*)p, NULL, dt, alfapr);
+  or_vel_exchange(m, u);
+  or_vel_exchange(m, v);
+  or_vel_exchange(m, w);
+  for (;;) {
+    iter = iter + 1;
+    or_calmas(m, (const double* const*)u, (const double* const*)v, (const double* const*)w, dt, su, &rmax);
+    if (rmax_hist) rmax_hist[iter - 1] = rmax;
+    if (rmax < eps && iter > 1) break;
+    total += or_sipsol(m, pp, (const double* const*)su, nswp, NULL);
+    for (int ib = 0; ib < nb; ++ib) {
+      const or_dom* d = &m->dom[ib];
+      size_t n = (size_t)(d->d.n[0] + 2) * (d->d.n[1] + 2) * (d->d.n[2] + 2);
+      for (size_t q = 0; q < n; ++q) {
+        p[ib][q] = (p[ib][q] + (pp[ib][q] - 0.0));
+        pp[ib][q] = 0.0;
+      }
+    }
+    for (int ib = 0; ib < nb; ++ib) or_put_phi(m, 1, ib, p[ib]);
+    or_exchangepp(m, 1);
+    for (int ib = 0; ib < nb; ++ib) or_get_phi(m, 1, ib, p[ib]);
+    or_calvel(m, u, v, w, us, vs, ws, (const double* const*)p, NULL, dt, alfapr);
+    or_vel_exchange(m, u);
+    or_vel_exchange(m, v);
+    or_vel_exchange(m, w);
+    if (!(iter < niter)) break;
+  }
+  if (iters) *iters = iter;
+  if (nsweeps) *nsweeps = total;
+  for (int ib = 0; ib < nb; ++ib) { free(su[ib]); free(pp[ib]); }
+  free(su);
+  free(pp);
+  return 0;
+}
+
 /* --------------------------------------------------------------- topology */
 int or_topology(int nblocks, const int32_t* ext, const int32_t* bc,
                 or_block_desc* out) {

@@ -123,6 +123,19 @@ int or_project(or_mg* m, double* const* p, double* const* u, double* const* v, d
                const double* const* dens, double dt, double alfapr, double tol, int maxcy,
                int stop_rule, int* cycles, double* relres, double* rmax, double* history);
 
+/* Stone's SIP (sipsol.for:2-205, ifi = 44) on pp (canonical with ghosts,
+ * in/out) with rhs su (interior) and pressure_1sweep's coefficients; at most
+ * nswp sweeps; resab (may be NULL) receives sum |res| per sweep.  Returns the
+ * reference's nsweep. */
+int or_sipsol(or_mg* m, double* const* pp, const double* const* su, int nswp, double* resab);
+/* pressure_1sweep (press.for:382-519) without its closing boundu/v/w: the
+ * SIP pressure loop over the velocities.  rmax_hist (may be NULL, niter
+ * entries) gets the rmax of every calmas. */
+int or_pressure_1sweep(or_mg* m, double* const* p, double* const* u, double* const* v, double* const* w,
+                       const double* const* us, const double* const* vs, const double* const* ws, double dt,
+                       double alfapr, double eps, int niter, int nswp, int* iters, int* nsweeps,
+                       double* rmax_hist);
+
 /* Block topology from integer extents: read_infodom neighbour discovery
  * (alloc_dom.for:524-1200).  ext is nblocks x 6 (x0,x1,y0,y1,z0,z1) in global
  * cell units; bc[6] global codes.  Fills nb_face/nb_corner/nb_edge/
