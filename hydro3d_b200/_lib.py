@@ -28,6 +28,7 @@ FIELD_P = 0
 FIELD_B = 1
 FIELD_U, FIELD_V, FIELD_W = 2, 3, 4
 FIELD_USTAR, FIELD_VSTAR, FIELD_WSTAR = 5, 6, 7
+FIELD_PP = 8
 
 
 class BlockDesc(C.Structure):
@@ -106,7 +107,7 @@ EXPORTS = [
     "h3d_mg_set_restriction", "h3d_mg_get_restriction", "h3d_topology", "h3d_halo_table",
     "h3d_mg_strerror", "h3d_mg_last_error", "h3d_residual_noalloc",
     "h3d_mg_calvel", "h3d_mg_calmas", "h3d_mg_pbound", "h3d_mg_project_resident", "h3d_mg_project",
-    "h3d_mg_set_wait_limit", "h3d_mg_wait_probe",
+    "h3d_mg_set_wait_limit", "h3d_mg_wait_probe", "h3d_mg_sipsol", "h3d_mg_pressure_1sweep",
 ]
 
 _lib = None
@@ -163,6 +164,8 @@ def lib():
         "h3d_residual_noalloc": (i32, [C.c_void_p, C.c_void_p, i32, i32, i32, pd, i32, pd, C.c_void_p]),
         "h3d_mg_set_wait_limit": (i32, [vp, i64]),
         "h3d_mg_wait_probe": (i32, [vp]),
+        "h3d_mg_sipsol": (i32, [vp, i32, C.POINTER(i32), pd]),
+        "h3d_mg_pressure_1sweep": (i32, [vp, dbl, dbl, dbl, i32, i32, C.POINTER(SolveInfo)]),
         "h3d_mg_calvel": (i32, [vp, dbl, dbl]),
         "h3d_mg_calmas": (i32, [vp, dbl, pd, pd]),
         "h3d_mg_pbound": (i32, [vp]),

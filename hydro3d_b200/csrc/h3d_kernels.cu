@@ -3943,6 +3943,153 @@ __global__ void __launch_bounds__(256) k_padd(const BlkLev* __restrict__ bls, co
 
 }  // namespace
 
+namespace {
+
+// ---------------------------------------------------------------------------
+// Stone's strongly implicit procedure (sipsol.for:2-205, ifi = 44), the
+// reference's alternative pressure solver, on the level-1 layout with the
+// constant coefficients pressure_1sweep builds (press.for:407-438: the same
+// values as coeff's level 1).  The LU factors and both substitutions are
+// recurrences over the predecessors (x-1, y-1, z-1) (successors for the
+// backward pass), so hyperplanes x+y+z = const are the wavefronts: one CTA
+// per block sweeps them in order with a CTA barrier between, every value the
+// one the reference's k, i, j loops compute, in its operand order.  Factor
+// and residual arrays are zero outside the interior (never written there),
+// as the reference's are.
+struct SipLU {
+  double *lb, *lw, *ls, *lpr, *un, *ue, *ut, *res;
+};
+
+// Calls f(x, y, z, i) for every interior cell of hyperplane x+y+z = d + 3,
+// spread over the CTA's threads.
+template <typename F>
+__device__ __forceinline__ void sip_plane(const BlkLev& B, int d, F&& f) {
+  const int nx = B.nx, ny = B.ny, nz = B.nz;
+  const int zmin = max(0, d - (nx - 1) - (ny - 1)), zmax = min(nz - 1, d);
+  const int nzr = zmax - zmin + 1;
+  for (int q = threadIdx.x; q < nzr * ny; q += blockDim.x) {
+    const int z = zmin + q / ny + 1, y = q % ny + 1;
+    const int x = d - (y - 1) - (z - 1) + 1;
+    if (x < 1 || x > nx) continue;
+    f(x, y, z, (long long)z * B.sxy + (long long)y * B.sx + x);
+  }
+}
+
+__global__ void __launch_bounds__(512) k_sip_factor(const BlkLev* __restrict__ bls, SipLU lu) {
+  pdl_trigger();
+  pdl_wait();
+  const BlkLev B = bls[blockIdx.x];
+  const double alfa = 0.92, small = 1e-20;  // sipsol.for:32-33
+  double *lb = lu.lb + B.off, *lw = lu.lw + B.off, *ls = lu.ls + B.off, *lpr = lu.lpr + B.off;
+  double *un = lu.un + B.off, *ue = lu.ue + B.off, *ut = lu.ut + B.off;
+  const long long sj = B.sx, sk = B.sxy;
+  for (int d = 0; d <= (B.nx - 1) + (B.ny - 1) + (B.nz - 1); ++d) {  // sipsol.for:77-105
+    sip_plane(B, d, [&](int x, int y, int z, long long q) {
+      const Coef<double> c = cell_coef<double, false>(B, x, y, z, q, nullptr, nullptr, nullptr);
+      const double ap = coef_ap(c);
+      lb[q] = c.ab / (1. + alfa * (un[q - sk] + ue[q - sk]));
+      lw[q] = c.aw / (1. + alfa * (un[q - 1] + ut[q - 1]));
+      ls[q] = c.as / (1. + alfa * (ue[q - sj] + ut[q - sj]));
+      const double p1 = alfa * (lb[q] * un[q - sk] + lw[q] * un[q - 1]);
+      const double p2 = alfa * (lb[q] * ue[q - sk] + ls[q] * ue[q - sj]);
+      const double p3 = alfa * (lw[q] * ut[q - 1] + ls[q] * ut[q - sj]);
+      lpr[q] = 1. / (ap + p1 + p2 + p3 - lb[q] * ut[q - sk] - lw[q] * ue[q - 1] - ls[q] * un[q - sj] + small);
+      un[q] = (c.an - p1) * lpr[q];
+      ue[q] = (c.ae - p2) * lpr[q];
+      ut[q] = (c.at - p3) * lpr[q];
+    });
+    __syncthreads();
+  }
+}
+
+// One SIP sweep of every block (sipsol.for:144-179): residual, forward and
+// backward substitution, fi += correction; the block's sum |res| into
+// partials[4 * block] (the other three entries zero).
+__global__ void __launch_bounds__(512) k_sip_sweep(const BlkLev* __restrict__ bls, SipLU lu, double* __restrict__ fi_all,
+                                                   const double* __restrict__ su_all, double* __restrict__ partials) {
+  pdl_trigger();
+  pdl_wait();
+  __shared__ double red[16];
+  const BlkLev B = bls[blockIdx.x];
+  const double *lb = lu.lb + B.off, *lw = lu.lw + B.off, *ls = lu.ls + B.off, *lpr = lu.lpr + B.off;
+  const double *un = lu.un + B.off, *ue = lu.ue + B.off, *ut = lu.ut + B.off;
+  double* res = lu.res + B.off;
+  double* fi = fi_all + B.off;
+  const double* su = su_all + B.off;
+  const long long sj = B.sx, sk = B.sxy;
+  const int nx = B.nx, ny = B.ny, nz = B.nz;
+  double acc = 0.0;
+  const long long ncell = (long long)nx * ny * nz;
+  for (long long c0 = threadIdx.x; c0 < ncell; c0 += blockDim.x) {  // residual, :146-157
+    const int x = (int)(c0 % nx) + 1, y = (int)((c0 / nx) % ny) + 1, z = (int)(c0 / ((long long)nx * ny)) + 1;
+    const long long q = (long long)z * sk + (long long)y * sj + x;
+    const Coef<double> c = cell_coef<double, false>(B, x, y, z, q, nullptr, nullptr, nullptr);
+    const double r = (su[q] - coef_ap(c) * fi[q] - c.an * fi[q + sj] - c.as * fi[q - sj] - c.ae * fi[q + 1] -
+                      c.aw * fi[q - 1] - c.ab * fi[q - sk] - c.at * fi[q + sk]);
+    res[q] = r;
+    acc += fabs(r);
+  }
+  __syncthreads();
+  const int dmax = (nx - 1) + (ny - 1) + (nz - 1);
+  for (int d = 0; d <= dmax; ++d) {  // forward substitution, :159-167
+    sip_plane(B, d, [&](int, int, int, long long q) {
+      res[q] = (res[q] - lb[q] * res[q - sk] - lw[q] * res[q - 1] - ls[q] * res[q - sj]) * lpr[q];
+    });
+    __syncthreads();
+  }
+  for (int d = dmax; d >= 0; --d) {  // backward substitution and correction, :169-178
+    sip_plane(B, d, [&](int, int, int, long long q) {
+      res[q] = res[q] - un[q] * res[q + sj] - ue[q] * res[q + 1] - ut[q] * res[q + sk];
+      fi[q] = fi[q] + res[q];
+    });
+    __syncthreads();
+  }
+  // block sum of |res| in a fixed order (warp shuffles, then warps in order)
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[w];
+    partials[4 * blockIdx.x] = s;
+    partials[4 * blockIdx.x + 1] = 0.0;
+    partials[4 * blockIdx.x + 2] = 0.0;
+    partials[4 * blockIdx.x + 3] = 0.0;
+  }
+}
+
+__global__ void __launch_bounds__(256) k_gather1(const uint32_t* __restrict__ dst, const uint32_t* __restrict__ src,
+                                                 int64_t n, double* __restrict__ a) {
+  pdl_trigger();
+  pdl_wait();
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x)
+    a[dst[e]] = a[src[e]];
+}
+
+}  // namespace
+
+cudaError_t launch_sip_factor(const BlkLev* bl, int nb, SipArrays a, cudaStream_t st) {
+  if (nb <= 0) return cudaSuccess;
+  SipLU lu{a.lb, a.lw, a.ls, a.lpr, a.un, a.ue, a.ut, a.res};
+  pdl_launch(k_sip_factor, nb, 512, 0, st, bl, lu);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_sip_sweep(const BlkLev* bl, int nb, SipArrays a, double* fi, const double* su, double* partials,
+                             cudaStream_t st) {
+  if (nb <= 0) return cudaSuccess;
+  SipLU lu{a.lb, a.lw, a.ls, a.lpr, a.un, a.ue, a.ut, a.res};
+  pdl_launch(k_sip_sweep, nb, 512, 0, st, bl, lu, fi, su, partials);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_gather1(const uint32_t* dst, const uint32_t* src, int64_t n, double* a, cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  pdl_launch(k_gather1, grid_for(n, 256), 256, 0, st, dst, src, n, a);
+  return cudaGetLastError();
+}
+
+
 // The failure path of the bounded waits, made to run out: one warp waits
 // (mbar_wait, the sweeps' own routine and limit) on an mbarrier that expects
 // one arrival and receives none, so the wait gives up after g_wait_clocks,

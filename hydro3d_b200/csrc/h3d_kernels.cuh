@@ -248,6 +248,18 @@ cudaError_t launch_face_coef_sum(const BlkLev* fine, const BlkLev* coarse, CellT
                                  const double* ffy, const double* ffz, double* cfx, double* cfy, double* cfz,
                                  cudaStream_t st);
 
+// Stone's SIP (sipsol.for) on level 1: factor arrays and the residual
+// (level-1 layout, zero outside the interior).
+struct SipArrays {
+  double *lb, *lw, *ls, *lpr, *un, *ue, *ut, *res;
+};
+cudaError_t launch_sip_factor(const BlkLev* bl, int nb, SipArrays a, cudaStream_t st);
+// One sweep of every block on fi with rhs su; partials[4b] = sum |res| of block b.
+cudaError_t launch_sip_sweep(const BlkLev* bl, int nb, SipArrays a, double* fi, const double* su, double* partials,
+                             cudaStream_t st);
+// a[dst[e]] = a[src[e]].
+cudaError_t launch_gather1(const uint32_t* dst, const uint32_t* src, int64_t n, double* a, cudaStream_t st);
+
 // The projection on level 1 (press.for:2-144, newsolv_mg.for:39-49).
 // calvel: u, v, w from ustar, vstar, wstar and p (dtal = dt*alfapr; dens read
 // for L_LSM only).

@@ -162,6 +162,8 @@ struct h3d_mg {
   uint32_t* d_vdst = nullptr;
   uint32_t* d_vsrc = nullptr;
   int64_t nvfill = 0;
+  double* sip[8] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};  // SIP factors, res
+  double* sip_pp = nullptr;  // the SIP pressure correction (level-1 layout)
   bool proj = false;        // outer iterations end with p += pp, calvel, calmas
   double proj_dtal = 0.0;   // dt*alfapr
   double proj_dt = 1.0;
@@ -1932,6 +1934,8 @@ int h3d_mg_destroy(h3d_mg* h) {
   }
   dfree(h->d_vdst);
   dfree(h->d_vsrc);
+  for (int q = 0; q < 8; ++q) dfree(h->sip[q]);
+  dfree(h->sip_pp);
   if (h->h_res) cudaFreeHost(h->h_res);
   if (h->st) cudaStreamDestroy(h->st);
   delete h;
@@ -2222,6 +2226,7 @@ int h3d_mg_coeff(h3d_mg* h) {
 }
 
 static int ensure_velocity(h3d_mg* h);
+static int ensure_sip(h3d_mg* h);
 static double* velocity_field(h3d_mg* h, int field);
 
 static int ensure_coeffs(h3d_mg* h) {
@@ -2239,6 +2244,9 @@ int h3d_mg_upload(h3d_mg* h, int32_t field, int32_t ib, const double* host) {
   else if (field >= H3D_FIELD_U && field <= H3D_FIELD_WSTAR) {
     TRY(ensure_velocity(h));
     TRY(copy_field_3d(h, true, velocity_field(h, field), B, const_cast<double*>(host), h->blocks[ib], true));
+  } else if (field == H3D_FIELD_PP) {
+    TRY(ensure_sip(h));
+    TRY(copy_field_3d(h, true, h->sip_pp, B, const_cast<double*>(host), h->blocks[ib], true));
   } else
     return H3D_ERR_ARG;
   return H3D_OK;
@@ -2254,6 +2262,9 @@ int h3d_mg_download(h3d_mg* h, int32_t field, int32_t ib, double* host) {
   else if (field >= H3D_FIELD_U && field <= H3D_FIELD_WSTAR) {
     TRY(ensure_velocity(h));
     TRY(copy_field_3d(h, false, velocity_field(h, field), B, host, h->blocks[ib], true));
+  } else if (field == H3D_FIELD_PP) {
+    TRY(ensure_sip(h));
+    TRY(copy_field_3d(h, false, h->sip_pp, B, host, h->blocks[ib], true));
   } else
     return H3D_ERR_ARG;
   CU(cudaStreamSynchronize(h->st));
@@ -2473,6 +2484,11 @@ static int build_vel_table(h3d_mg* h) {
   return H3D_OK;
 }
 
+static int ensure_face_table(h3d_mg* h) {
+  if (h->d_vdst) return H3D_OK;  // (a layout without block faces rebuilds an empty table)
+  return build_vel_table(h);
+}
+
 static int ensure_velocity(h3d_mg* h) {
   if (h->vel[0]) return H3D_OK;
   const size_t n = (size_t)h->lev[1].geom.n_elems;
@@ -2480,13 +2496,129 @@ static int ensure_velocity(h3d_mg* h) {
     TRY(dalloc(h, &h->vel[c], n));
     TRY(dalloc(h, &h->vstar[c], n));
   }
-  return build_vel_table(h);
+  return ensure_face_table(h);
 }
 
 static double* velocity_field(h3d_mg* h, int field) {
   if (field >= H3D_FIELD_U && field <= H3D_FIELD_W) return h->vel[field - H3D_FIELD_U];
   if (field >= H3D_FIELD_USTAR && field <= H3D_FIELD_WSTAR) return h->vstar[field - H3D_FIELD_USTAR];
+  if (field == H3D_FIELD_PP) return h->sip_pp;
   return nullptr;
+}
+
+// ---------------------------------------------------------------- SIP
+static int ensure_sip(h3d_mg* h) {
+  if (h->var) return fail(h, H3D_ERR_BAD_CONFIG, "SIP: constant coefficients only (press.for:407-438)");
+  if ((int)h->blocks.size() > h->npartials) return fail(h, H3D_ERR_BAD_CONFIG, "SIP: too many blocks");
+  if (h->sip_pp) return H3D_OK;
+  TRY(ensure_face_table(h));
+  const size_t n = (size_t)h->lev[1].geom.n_elems;
+  for (int q = 0; q < 8; ++q) TRY(dalloc(h, &h->sip[q], n));
+  TRY(dalloc(h, &h->sip_pp, n));
+  return H3D_OK;
+}
+
+// sipsol(44) (sipsol.for:2-205) on the resident correction with the resident
+// right-hand side (H3D_FIELD_B): factors, then at most nswp sweeps, each
+// followed by exchange(44) (face ghosts; walls untouched) and the stop test
+// on sum |res| relative to the first sweep (<= 0.001, or changing by at most
+// 0.00001).  *nsweep gets the reference's sweep count.
+static int sip_run(h3d_mg* h, int nswp, int* nsweep, double* resab_last) {
+  Level& V = h->lev[1];
+  const int nb = (int)V.geom.bl.size();
+  SipArrays a{h->sip[0], h->sip[1], h->sip[2], h->sip[3], h->sip[4], h->sip[5], h->sip[6], h->sip[7]};
+  CU(launch_sip_factor(V.d_bl, nb, a, h->st));
+  h->kernels += 1;
+  const double small = 1e-20;
+  double relast = 0.0, res1 = 0.0, resab = 0.0;
+  int ns;
+  for (ns = 1; ns <= nswp; ++ns) {
+    CU(launch_sip_sweep(V.d_bl, nb, a, h->sip_pp, h->b64, h->partials, h->st));
+    CU(launch_gather1(h->d_vdst, h->d_vsrc, h->nvfill, h->sip_pp, h->st));
+    CU(launch_reduce4(h->partials, nb, h->d_res, h->st));
+    CU(cudaMemcpyAsync(h->h_res, h->d_res, 4 * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+    CU(cudaStreamSynchronize(h->st));
+    h->kernels += 3;
+    resab = h->h_res[0];
+    if (!std::isfinite(resab)) return fail(h, H3D_ERR_DIVERGED, "SIP residual is not finite");
+    if (ns == 1) res1 = resab;
+    const double rsm = resab / (res1 + small);
+    const double reldif = std::fabs(rsm - relast);
+    relast = rsm;
+    if (rsm <= 0.001) break;
+    if (reldif <= 0.00001) break;
+  }
+  if (ns > nswp) ns = nswp;
+  if (nsweep) *nsweep = ns;
+  if (resab_last) *resab_last = resab;
+  return H3D_OK;
+}
+
+int h3d_mg_sipsol(h3d_mg* h, int32_t nswp, int32_t* nsweep, double* resab) {
+  if (!h || nswp < 1) return H3D_ERR_ARG;
+  CU(cudaSetDevice(h->device));
+  TRY(ensure_sip(h));
+  int ns = 0;
+  TRY(sip_run(h, nswp, &ns, resab));
+  if (nsweep) *nsweep = ns;
+  return H3D_OK;
+}
+
+int h3d_mg_pressure_1sweep(h3d_mg* h, double dt, double alfapr, double eps, int32_t niter, int32_t nswp,
+                           h3d_solve_info* info) {
+  if (!h || niter < 1 || nswp < 1) return H3D_ERR_ARG;
+  if (!(dt > 0)) return fail(h, H3D_ERR_ARG, "dt must be positive");
+  CU(cudaSetDevice(h->device));
+  TRY(ensure_sip(h));
+  TRY(ensure_velocity(h));
+  Level& V = h->lev[1];
+  RowTab ra{V.d_rows_all, (int)V.geom.bl.size(), V.nrows_all};
+  h3d_solve_info I{};
+  h->history.clear();
+  cudaEvent_t t0, t1;
+  CU(cudaEventCreate(&t0));
+  CU(cudaEventCreate(&t1));
+  const int64_t k0 = h->kernels;
+  CU(cudaEventRecord(t0, h->st));
+  const size_t bytes = (size_t)V.geom.n_elems * sizeof(double);
+  CU(cudaMemsetAsync(h->sip_pp, 0, bytes, h->st));  // press.for:402
+  TRY(h3d_mg_calvel(h, dt, alfapr));               // :439
+  int iter = 0, total = 0;
+  double rmax = 0.0, su2 = 0.0;
+  for (;;) {  // :441-472
+    iter += 1;
+    TRY(h3d_mg_calmas(h, dt, &rmax, &su2));
+    h->history.push_back(rmax);
+    if (!std::isfinite(rmax)) break;
+    if (rmax < eps && iter > 1) break;
+    int ns = 0;
+    TRY(sip_run(h, nswp, &ns, nullptr));
+    total += ns;
+    double* p = h->p64[h->pc];
+    CU(launch_padd<double>(V.d_bl, ra, p, h->sip_pp, h->st));  // p = p + (pp - ppref), ppref = 0
+    CU(cudaMemsetAsync(h->sip_pp, 0, bytes, h->st));
+    CU(launch_fill<double>(V.faces.d_dst, V.faces.d_src, V.faces.n, p, p, p, false, h->st));  // exchange(4), pbound
+    h->kernels += 2;
+    TRY(h3d_mg_calvel(h, dt, alfapr));
+    if (!(iter < niter)) break;
+  }
+  CU(cudaEventRecord(t1, h->st));
+  CU(cudaEventSynchronize(t1));
+  float ms = 0;
+  CU(cudaEventElapsedTime(&ms, t0, t1));
+  cudaEventDestroy(t0);
+  cudaEventDestroy(t1);
+  I.outer = iter;
+  I.cycles = total;
+  I.rmax = rmax;
+  I.relres = std::sqrt(su2);
+  I.relres_block_max = I.relres;
+  I.device_ms = ms;
+  I.kernel_launches = h->kernels - k0;
+  if (info) *info = I;
+  TRY(check_device_error(h));
+  if (!std::isfinite(rmax) || rmax > 10.0) return fail(h, H3D_ERR_DIVERGED, "rmax not finite or above 10");
+  return H3D_OK;
 }
 
 // Cached graphs of projection iterations hold dt*alfapr and dt as kernel

@@ -10,6 +10,8 @@ and their argument meaning:
                                    newsolv_mg.for:2-93 with calvel/calmas (press.for:2-144)
     calvel(dt, alfapr) / calmas(dt) / pbound()
                                    press.for:2-207 on the resident fields
+    sipsol(nswp) / pressure_1sweep(dt, ...)
+                                   sipsol.for:2-205, press.for:382-519 (the SIP path)
     mgrelax(g, it) / mgrestr(g) / mgcorr(g) / mgbound(g) / exchangepp(g)
                                    mgsolver.for:374-997, exchangepp.for:2-2835
 
@@ -180,6 +182,20 @@ class MultigridSolver:
         rc = self.L.h3d_mg_project_resident(self._h, dt, alfapr, C.byref(opts), C.byref(info))
         return self._info(rc, info, history)
 
+    def sipsol(self, nswp: int):
+        """sipsol(44) on the resident 'pp' with rhs 'b': (nsweep, last sum |res|)."""
+        ns, ra = C.c_int32(), C.c_double()
+        self._check(self.L.h3d_mg_sipsol(self._h, nswp, C.byref(ns), C.byref(ra)), "h3d_mg_sipsol")
+        return ns.value, ra.value
+
+    def pressure_1sweep(self, dt: float, alfapr: float = 1.0, eps: float = 1e-8, niter: int = 10,
+                        nswp: int = 50) -> dict:
+        """The SIP pressure loop (press.for:382-519) on the resident fields;
+        history = rmax of every calmas."""
+        info = _lib.SolveInfo()
+        rc = self.L.h3d_mg_pressure_1sweep(self._h, dt, alfapr, eps, niter, nswp, C.byref(info))
+        return self._info(rc, info, True)
+
     def calvel(self, dt: float, alfapr: float = 1.0):
         self._check(self.L.h3d_mg_calvel(self._h, dt, alfapr), "h3d_mg_calvel")
 
@@ -194,7 +210,7 @@ class MultigridSolver:
 
     # resident operation --------------------------------------------------
     FIELDS = {"p": _lib.FIELD_P, "b": _lib.FIELD_B, "u": _lib.FIELD_U, "v": _lib.FIELD_V, "w": _lib.FIELD_W,
-              "ustar": _lib.FIELD_USTAR, "vstar": _lib.FIELD_VSTAR, "wstar": _lib.FIELD_WSTAR}
+              "ustar": _lib.FIELD_USTAR, "vstar": _lib.FIELD_VSTAR, "wstar": _lib.FIELD_WSTAR, "pp": _lib.FIELD_PP}
 
     def upload(self, field: str, ib: int, host: np.ndarray):
         f = self.FIELDS[field]

@@ -138,6 +138,8 @@ int h3d_mg_newsolv(h3d_mg* h, double* const* p, const double* const* b,
 #define H3D_FIELD_USTAR 5
 #define H3D_FIELD_VSTAR 6
 #define H3D_FIELD_WSTAR 7
+/* The SIP pressure correction pp (sipsol.for), FP64, canonical with ghosts. */
+#define H3D_FIELD_PP 8
 /* Copy block ib of a resident field from/to a host field (ttc dims, pl ghosts). */
 int h3d_mg_upload(h3d_mg* h, int32_t field, int32_t ib, const double* host);
 int h3d_mg_download(h3d_mg* h, int32_t field, int32_t ib, double* host);
@@ -184,6 +186,28 @@ int h3d_mg_project_resident(h3d_mg* h, double dt, double alfapr, const h3d_solve
 int h3d_mg_project(h3d_mg* h, double* const* p, double* const* u, double* const* v, double* const* w,
                    const double* const* ustar, const double* const* vstar, const double* const* wstar,
                    double dt, double alfapr, const h3d_solve_opts* opts, h3d_solve_info* info);
+
+/* --- the SIP pressure path (solver = 1: press.for:382-519, sipsol.for) --- */
+/* sipsol(44) (sipsol.for:2-205): Stone's strongly implicit procedure on the
+ * resident correction H3D_FIELD_PP with right-hand side H3D_FIELD_B and the
+ * coefficients pressure_1sweep builds (press.for:407-438); LU factors
+ * rebuilt on every call as the reference does; at most nswp sweeps, each
+ * followed by exchange(44) (face ghosts from neighbours and periodic
+ * partners), stopping when sum |res| falls to 0.001 of the first sweep's or
+ * changes by at most 0.00001 of it.  *nsweep receives the reference's
+ * nsweep, *resab the last sum |res|.  The recurrences run as wavefronts
+ * (hyperplanes x+y+z = const), one CTA per block.  Constant coefficients
+ * only (H3D_ERR_BAD_CONFIG for L_LSM handles). */
+int h3d_mg_sipsol(h3d_mg* h, int32_t nswp, int32_t* nsweep, double* resab);
+/* pressure_1sweep (press.for:382-519) on the resident fields, without the
+ * boundu/v/w that follow it: pp = 0, calvel, then at most niter times
+ * calmas (stop when rmax < eps after the first), sipsol(44), p = p + pp over
+ * the block and its ghost layer, pp = 0, exchange(4) + pbound, calvel.
+ * info->outer = iterations, info->cycles = SIP sweeps in all, info->rmax the
+ * last calmas's, info->relres = ||su||2 of the last calmas; the rmax history
+ * is read with h3d_mg_history.  rmax above 10 gives H3D_ERR_DIVERGED. */
+int h3d_mg_pressure_1sweep(h3d_mg* h, double dt, double alfapr, double eps, int32_t niter, int32_t nswp,
+                           h3d_solve_info* info);
 
 /* --- reference subroutines on the resident level state ----------------- */
 /* Canonical level arrays of block ib at level g; field 0 = phi, 1 = rhs. */

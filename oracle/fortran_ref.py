@@ -21,7 +21,8 @@ semantics:
   * the solver: mgsolver.for (coeff, mgkcyc, mgrelax, mgrestr, mgcorr,
     mgbound) and exchangepp.for (exchangepp, exchbc_mgpp);
   * the projection: press.for (calmas, calvel, pbound), exchange.for
-    (exchange, exchange_smlvl) and exchange_bc.for (exchange_bc).
+    (exchange, exchange_smlvl) and exchange_bc.for (exchange_bc);
+  * the SIP solver: sipsol.for (sipsol).
 Fortran semantics kept: default REAL and real literals are 8-byte (the
 reference's -real-size 64); integer division truncates toward zero; integer
 MOD takes the dividend's sign; assignment of a real to an integer truncates;
@@ -910,7 +911,27 @@ class UnitTranslator:
             j = self.block(stmts, i + 1, [r"^end\s*do$"])
             self.depth -= 1
             self.ind -= 1
-            self.emit("%s = %s + %s * (%s)" % (vcode, a0, n, s))
+            post = "%s = %s + %s * (%s)" % (vcode, a0, n, s)
+            if self.in_dispatch:
+                # a GOTO out of the loop leaves the DO variable as it is (no
+                # final increment) and continues at the label
+                self.emit("else:")
+                self.ind += 1
+                self.emit(post)
+                self.ind -= 1
+                if self.depth:
+                    self.emit("if _brk:")
+                    self.ind += 1
+                    self.emit("break")
+                    self.ind -= 1
+                else:
+                    self.emit("if _brk:")
+                    self.ind += 1
+                    self.emit("_brk = False")
+                    self.emit("continue")
+                    self.ind -= 1
+            else:
+                self.emit(post)
             return j + 1
         if re.match(r"^do\s+\d", t):
             raise FortranError("unsupported do form")
@@ -974,10 +995,12 @@ class UnitTranslator:
                 self.ind -= 1
         m = re.match(r"^go\s*to\s*(\d+)$", t)
         if m:
-            if self.depth:
-                raise FortranError("goto inside a DO loop")
             self.emit("_lab = %s" % m.group(1))
-            self.emit("continue")
+            if self.depth:  # out of the enclosing DO loops, then to the label
+                self.emit("_brk = True")
+                self.emit("break")
+            else:
+                self.emit("continue")
             return i + 1
         if re.match(r"^call\s", t):
             self.call(t)
@@ -1027,6 +1050,7 @@ class UnitTranslator:
                 self.emit("v_%s = FArray(%r, [%s])" % (name, sym.kind, ", ".join(bounds)))
         if gotos:
             self.emit("_lab = 0")
+            self.emit("_brk = False")
             self.emit("while True:")
             self.ind += 1
             self.emit("if _lab == 0:")
@@ -1060,6 +1084,7 @@ SOLVER_UNITS = {
     "press.for": ["calmas", "calvel", "pbound"],
     "exchange.for": ["exchange", "exchange_smlvl"],
     "exchange_bc.for": ["exchange_bc"],
+    "sipsol.for": ["sipsol"],
 }
 MODULE_FILES = ["module_vars.for", "module_multidata.for", "module_mpi.for"]
 MPI_CONSTANTS = {"mpi_comm_world": 0, "mpi_double_precision": 1, "mpi_integer": 2, "mpi_max": 3,
@@ -1161,8 +1186,9 @@ class Reference:
         for ib in range(1, nb + 1):
             o = M.v_dom.g(ib)
             tti, ttj, ttk = o.c_ttc_i, o.c_ttc_j, o.c_ttc_k
-            for f in ("pp", "su", "sup", "dens", "p", "u", "v", "w", "ustar", "vstar", "wstar"):
-                setattr(o, "c_" + f, FArray("r", [(1, tti), (1, ttj), (1, ttk)]))  # initial.for:146-160
+            for f in ("pp", "su", "sup", "dens", "p", "u", "v", "w", "ustar", "vstar", "wstar",
+                      "ap", "ae", "aw", "an", "as", "at", "ab"):
+                setattr(o, "c_" + f, FArray("r", [(1, tti), (1, ttj), (1, ttk)]))  # initial.for:146-163
             o.c_faz = FArray("i", [(1, ngrd_gl)])                       # initial.for:250
             o.c_stfcinf = FArray("r", [(1, 6), (1, M.v_pl), (1, M.v_ngg)])  # initial.for:183
             for f in ("sendb_m1", "sendb_p1", "recvb_m1", "recvb_p1", "sendb_m2", "sendb_p2",

@@ -86,6 +86,11 @@ def lib():
         L.or_project.argtypes = [vp, ppd, ppd, ppd, ppd, ppd, ppd, ppd, ppd, dbl, dbl, dbl, i32, i32,
                                  C.POINTER(C.c_int), pd, pd, pd]
         L.or_project.restype = i32
+        L.or_sipsol.argtypes = [vp, ppd, ppd, i32, pd]
+        L.or_sipsol.restype = i32
+        L.or_pressure_1sweep.argtypes = [vp, ppd, ppd, ppd, ppd, ppd, ppd, ppd, dbl, dbl, dbl, i32, i32,
+                                         C.POINTER(C.c_int), C.POINTER(C.c_int), pd]
+        L.or_pressure_1sweep.restype = i32
         L.or_topology.argtypes = [i32, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(BlockDesc)]
         L.or_topology.restype = i32
         L.or_set_threads.argtypes = [i32]
@@ -277,3 +282,21 @@ class Oracle:
                               _dp(hist))
         return dict(p=p, u=u, v=v, w=w, status=st, cycles=cyc.value, relres=rel.value, rmax=rmax.value,
                     history=hist[: cyc.value + 1])
+
+    # SIP (sipsol.for:2-205, press.for:382-519) -----------------------------
+    def sipsol(self, pp, su, nswp):
+        """pp canonical (in/out copy returned), su interior: (pp, nsweep, sum|res| per sweep)."""
+        pp = [np.ascontiguousarray(a, dtype=np.float64).copy() for a in pp]
+        su = [np.ascontiguousarray(a, dtype=np.float64) for a in su]
+        hist = np.zeros(nswp)
+        ns = lib().or_sipsol(self._h, _ptrs(pp), _ptrs(su), nswp, _dp(hist))
+        return pp, ns, hist[:ns]
+
+    def pressure_1sweep(self, p, u, v, w, us, vs, ws, dt, alfapr=1.0, eps=1e-8, niter=10, nswp=50):
+        p, u, v, w = ([np.ascontiguousarray(a, dtype=np.float64).copy() for a in f] for f in (p, u, v, w))
+        us, vs, ws = ([np.ascontiguousarray(a, dtype=np.float64) for a in f] for f in (us, vs, ws))
+        it, ns = C.c_int(), C.c_int()
+        hist = np.zeros(niter)
+        lib().or_pressure_1sweep(self._h, _ptrs(p), _ptrs(u), _ptrs(v), _ptrs(w), _ptrs(us), _ptrs(vs), _ptrs(ws),
+                                 dt, alfapr, eps, niter, nswp, C.byref(it), C.byref(ns), _dp(hist))
+        return dict(p=p, u=u, v=v, w=w, iters=it.value, nsweeps=ns.value, history=hist[:it.value])

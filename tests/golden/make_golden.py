@@ -14,7 +14,9 @@ nx+2), su (nz, ny, nx) and, for L_LSM cases, dens (nz, ny, nx).
 
 The project_*.npz fixtures run the reference's calvel, calmas, mgkcyc,
 exchange(4) and pbound (press.for, exchange.for, exchange_bc.for) in the
-order of newsolv_mg's loop; see run_projection_case.
+order of newsolv_mg's loop; see run_projection_case.  The sip_*.npz fixtures
+run the SIP pressure path (sipsol.for and press.for's pressure_1sweep loop);
+see run_sip_case.
 """
 import os
 import sys
@@ -178,6 +180,113 @@ def run_projection_case(name, src_dir=REF_SRC):
     return out
 
 
+# The SIP pressure path (solver = 1): name -> (layout, bc, nswp, seed)
+SIP_CASES = {
+    "walls_2x1x1": (grid((2, 1, 1), (8, 8, 8)), [W] * 6, 6, 301),
+    "periodic_x_2x2x1": (grid((2, 2, 1), (8, 8, 8)), [P, P, W, W, W, W], 60, 302),
+    "periodic_all_1x2x2": (grid((1, 2, 2), (8, 8, 8)), [P] * 6, 60, 303),
+}
+SIP_NITER = 2
+
+
+def run_sip_case(name, src_dir=REF_SRC):
+    """The reference's pressure_1sweep loop (press.for:439-472) from its own
+    calvel, calmas, sipsol(44), exchange(4) and pbound, SIP_NITER iterations
+    of at most nswp sweeps, with the coefficients pressure_1sweep builds
+    (press.for:407-438, restated below in its loop order and operand order).
+    Stored per block: the inputs, p, u, v, w and pp after the loop, the rmax
+    of every calmas and the sweep count of every sipsol."""
+    ext, bc, nswp, seed = SIP_CASES[name]
+    descs = O.topology(ext, bc, H, 2)
+    R = F.Reference(list(descs), 2, pl_ex=0, lsm=False, src_dir=src_dir)
+    M = R.M
+    M.v_rdivmax = 1
+    M.v_differencing = 1
+    M.v_dt = DT
+    M.v_alfapr = ALFAPR
+    M.v_nswp = F.FArray("i", [(1, 4)])
+    M.v_nswp.fill(nswp)
+    rng = np.random.default_rng(seed)
+    out = {"ext": ext, "bc": np.array(bc, np.int32), "h": np.array(H), "nblocks": len(descs), "dt": DT,
+           "alfapr": ALFAPR, "nswp": nswp, "niter": SIP_NITER}
+    for ib, d in enumerate(descs):
+        nx, ny, nz = d.n
+        shp = (nz + 2, ny + 2, nx + 2)
+        for k in ("p", "ustar", "vstar", "wstar"):
+            a = rng.uniform(-1.0, 1.0, shp)
+            R.put_field(k, ib, a)
+            out["%s_in_%d" % (k, ib)] = a
+        for ax, k in enumerate(("u", "v", "w")):
+            a = rng.uniform(-1.0, 1.0, shp)
+            sl = [slice(None)] * 3
+            if d.nb_face[2 * ax] < 0 and d.bc[2 * ax] != 5:
+                sl[2 - ax] = 0
+                a[tuple(sl)] = 0.0
+            if d.nb_face[2 * ax + 1] < 0 and d.bc[2 * ax + 1] != 5:
+                sl[2 - ax] = d.n[ax]
+                a[tuple(sl)] = 0.0
+            R.put_field(k, ib, a)
+            out["%s_in_%d" % (k, ib)] = a
+        # press.for:401-438: ap, pp, su zeroed, then the coefficients
+        o = R.dom(ib)
+        dx, dy, dz = o.c_dx, o.c_dy, o.c_dz
+        co = {k: np.zeros(shp) for k in ("aw", "ae", "an", "as", "at", "ab", "ap")}
+        for k in range(1, nz + 1):
+            for i in range(1, nx + 1):
+                for j in range(1, ny + 1):
+                    co["aw"][k, j, i] = 1.0 / (dx * dx)
+                    co["ae"][k, j, i] = 1.0 / (dx * dx)
+                    co["an"][k, j, i] = 1.0 / (dy * dy)
+                    co["as"][k, j, i] = 1.0 / (dy * dy)
+                    co["at"][k, j, i] = 1.0 / (dz * dz)
+                    co["ab"][k, j, i] = 1.0 / (dz * dz)
+                    if d.nb_face[0] < 0 and d.bc[0] != 5:
+                        co["aw"][k, j, 1] = 0.0
+                    if d.nb_face[1] < 0 and d.bc[1] != 5:
+                        co["ae"][k, j, nx] = 0.0
+                    if d.nb_face[2] < 0 and d.bc[2] != 5:
+                        co["as"][k, 1, i] = 0.0
+                    if d.nb_face[3] < 0 and d.bc[3] != 5:
+                        co["an"][k, ny, i] = 0.0
+                    if d.nb_face[4] < 0 and d.bc[4] != 5:
+                        co["ab"][1, j, i] = 0.0
+                    if d.nb_face[5] < 0 and d.bc[5] != 5:
+                        co["at"][nz, j, i] = 0.0
+                    co["ap"][k, j, i] = -1.0 * (co["aw"][k, j, i] + co["ae"][k, j, i] + co["as"][k, j, i] +
+                                                co["an"][k, j, i] + co["ab"][k, j, i] + co["at"][k, j, i])
+        for k2, a in co.items():
+            R.put_field(k2, ib, a)
+        R.put_field("pp", ib, np.zeros(shp))
+        R.put_field("su", ib, np.zeros(shp))
+    rmax, sweeps = [], []
+    R.call("calvel")
+    it = 0
+    while True:  # press.for:441-472
+        it += 1
+        R.call("calmas")
+        rmax.append(M.v_rmax)
+        R.call("sipsol", 44)
+        sweeps.append(M.v_nsweep)
+        for ib in range(len(descs)):
+            p = R.get_field("p", ib)
+            pp = R.get_field("pp", ib)
+            R.put_field("p", ib, p + (pp - 0.0))
+            R.put_field("pp", ib, np.zeros_like(pp))
+        R.call("exchange", 4)
+        R.call("pbound")
+        R.call("calvel")
+        if not it < SIP_NITER:
+            break
+    out["rmax"] = np.array(rmax)
+    out["nsweep"] = np.array(sweeps)
+    for ib in range(len(descs)):
+        for k in ("p", "u", "v", "w"):
+            out["%s_out_%d" % (k, ib)] = R.get_field(k, ib)
+        if not np.isfinite(out["p_out_%d" % ib]).all():
+            raise RuntimeError("%s: the reference produced non-finite values" % name)
+    return out
+
+
 def main():
     for name in CASES:
         data = run_case(name)
@@ -187,6 +296,10 @@ def main():
         data = run_projection_case(name)
         np.savez_compressed(os.path.join(HERE, "project_%s.npz" % name), **data)
         print("wrote project", name)
+    for name in SIP_CASES:
+        data = run_sip_case(name)
+        np.savez_compressed(os.path.join(HERE, "sip_%s.npz" % name), **data)
+        print("wrote sip", name)
 
 
 if __name__ == "__main__":

@@ -187,3 +187,72 @@ def test_projection_fixture_regenerates(oracle_mod, name):
     assert sorted(fresh) == sorted(old)
     for k in old:
         assert np.array_equal(np.asarray(fresh[k]), old[k]), k
+
+
+# -- the SIP pressure path (sipsol.for, pressure_1sweep's loop)
+SFILES = sorted(glob.glob(os.path.join(GOLDEN, "sip_*.npz")))
+SNAMES = [os.path.basename(f)[len("sip_"):-len(".npz")] for f in SFILES]
+
+
+def _sload(name):
+    with np.load(os.path.join(GOLDEN, "sip_%s.npz" % name)) as z:
+        return {k: z[k] for k in z.files}
+
+
+def test_sip_fixtures_present():
+    assert len(SNAMES) >= 3
+
+
+@pytest.mark.parametrize("name", SNAMES)
+def test_oracle_sip_matches_reference(oracle_mod, name):
+    g = _sload(name)
+    O = oracle_mod
+    nb = int(g["nblocks"])
+    descs = O.topology(g["ext"], g["bc"], g["h"], 2)
+    orc = O.Oracle(list(descs), 2, 3, 2, 1)
+    orc.coeff()
+    f = {k: [g["%s_in_%d" % (k, ib)] for ib in range(nb)] for k in ("p", "u", "v", "w", "ustar", "vstar", "wstar")}
+    res = orc.pressure_1sweep(f["p"], f["u"], f["v"], f["w"], f["ustar"], f["vstar"], f["wstar"], float(g["dt"]),
+                              float(g["alfapr"]), eps=0.0, niter=int(g["niter"]), nswp=int(g["nswp"]))
+    assert res["iters"] == int(g["niter"])
+    assert np.array_equal(res["history"], g["rmax"])
+    assert res["nsweeps"] == int(np.sum(g["nsweep"]))
+    for ib in range(nb):
+        m = _face_mask(res["p"][ib].shape)
+        for k in ("p", "u", "v", "w"):
+            got, want = res[k][ib], g["%s_out_%d" % (k, ib)]
+            assert np.array_equal(got[m], want[m]), (name, k, ib, float(np.abs(got[m] - want[m]).max()))
+    orc.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", SNAMES)
+def test_cuda_sip_matches_reference(h3d, name):
+    g = _sload(name)
+    nb = int(g["nblocks"])
+    blocks = h3d.topology.from_extents(g["ext"], g["bc"], g["h"], 2, pl=1)
+    s = h3d.MultigridSolver(blocks, 2)
+    for k in ("p", "u", "v", "w", "ustar", "vstar", "wstar"):
+        for ib in range(nb):
+            s.upload(k, ib, np.ascontiguousarray(g["%s_in_%d" % (k, ib)]))
+    info = s.pressure_1sweep(float(g["dt"]), float(g["alfapr"]), eps=0.0, niter=int(g["niter"]),
+                             nswp=int(g["nswp"]))
+    assert info["outer"] == int(g["niter"]) and info["cycles"] == int(np.sum(g["nsweep"]))
+    assert np.array_equal(info["history"], g["rmax"])
+    for ib, d in enumerate(blocks):
+        for k in ("p", "u", "v", "w"):
+            host = h3d.host_field(d)
+            s.download(k, ib, host)
+            want = g["%s_out_%d" % (k, ib)]
+            m = _face_mask(want.shape)
+            assert np.array_equal(host[m], want[m]), (name, k, ib, float(np.abs(host[m] - want[m]).max()))
+    s.close()
+
+
+@pytest.mark.skipif(_reference_tree() is None, reason="reference source tree not present")
+def test_sip_fixture_regenerates(oracle_mod):
+    fresh = _make_golden().run_sip_case("periodic_x_2x2x1")
+    old = _sload("periodic_x_2x2x1")
+    assert sorted(fresh) == sorted(old)
+    for k in old:
+        assert np.array_equal(np.asarray(fresh[k]), old[k]), k
