@@ -35,10 +35,12 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 TOL = 1e-8
-# FP32 V-cycles per FP64 refinement step of the mixed solver (measured on
-# configuration 3: 2 -> 6 refinement steps, 9.9 ms; 3 -> 4 steps, 9.3 ms;
-# 4 -> 3 steps, 9.0 ms, all 12 V-cycles and the same 1.5e-9 error).
-INNER = 4
+# FP32 V-cycles per FP64 refinement step of the mixed solver, per workload
+# (measured: on configuration 3, 2 -> 6 refinement steps, 9.9 ms; 3 -> 4
+# steps, 9.3 ms; 4 -> 3 steps, 9.0 ms, all 12 V-cycles and the same 1.5e-9
+# error; on configurations 2 and 4, 4 overshoots the tolerance by a cycle or
+# two, 2 does not).
+INNER = {1: 2, 2: 2, 3: 4, 4: 2, 5: 2}
 # Sweeps of the FP64 coarsest level in the mixed solver: enough to converge
 # that level (on the configuration-3 hierarchy 16 leave 14 V-cycles, 32 and 64
 # both 12), so the V-cycle contracts every mode at the rate of its finer
@@ -480,7 +482,8 @@ def main():
             "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
             "data": "synthetic (seeded; no dataset)",
             "config": dict(config_of(args.config, prob), precision="FP32 V(2,1) RBGS inside FP64 refinement",
-                           inner_cycles=INNER, coarse="FP64 coarsest level, %d RBGS sweeps" % COARSE_SWEEPS
+                           inner_cycles=INNER.get(args.config, 2),
+                           coarse="FP64 coarsest level, %d RBGS sweeps" % COARSE_SWEEPS
                            + ("; coarse coefficients by face sums" if prob.var_coef else ""),
                            parallelism="replicas" if world > 1 else "single GPU"),
             "fp64_ms": round(fp64_ms, 3), "speedup_vs_fp64": round(fp64_ms / (total_ms / (args.steps * world) * world), 3)
@@ -535,6 +538,11 @@ def read_profile_traffic(cfg, variant):
         return None
 
 
+def prob_config(prob):
+    """Configuration number of a workload built by synth (config1 .. config5)."""
+    return int(prob.name[-1]) if prob.name.startswith("config") else 0
+
+
 def build_solver_dev(prob, precision, device, coarse_sweeps=None, coarse_op=None):
     """A solver on `device` with the workload's b and p0 resident.  The mixed
     solver converges its FP64 coarsest level (COARSE_SWEEPS sweeps) and, for
@@ -548,7 +556,7 @@ def build_solver_dev(prob, precision, device, coarse_sweeps=None, coarse_op=None
         coarse_op = 1 if (precision == "mixed" and prob.var_coef) else 0
     s = MultigridSolver(prob.blocks, prob.ngrid, precision=precision, var_coef=prob.var_coef, maxcy=400,
                         device=device, coarse_sweeps=coarse_sweeps, coarse_op=coarse_op,
-                        inner_cycles=INNER if precision == "mixed" else 0)
+                        inner_cycles=INNER.get(prob_config(prob), 2) if precision == "mixed" else 0)
     if prob.var_coef:
         for ib, d in enumerate(prob.dens):
             s.set_density(ib, d)

@@ -2359,6 +2359,47 @@ __device__ void small_relax(const BlkLev* sb, const int* ss, int nb, T* __restri
   }
 }
 
+// All sweeps of one relaxation visit of a level whose ghost fill stays inside
+// every block (independent blocks, a single block, periodic wraps onto
+// itself): one CTA per block, in place, the cell arithmetic of small_relax;
+// fill entries of block b are fstart[b] .. fstart[b+1]-1 (sources in block b).
+template <typename T, bool VAR>
+__global__ void __launch_bounds__(1024) k_relax_blocks(const BlkLev* __restrict__ bls, const int* __restrict__ fstart,
+                                                       T* __restrict__ phi, const T* __restrict__ rhs,
+                                                       const T* __restrict__ fx, const T* __restrict__ fy,
+                                                       const T* __restrict__ fz, const uint32_t* __restrict__ fdst,
+                                                       const uint32_t* __restrict__ fsrc, int sweeps, int zero) {
+  pdl_trigger();
+  const BlkLev B = bls[blockIdx.x];
+  const int f0 = fstart[blockIdx.x], f1 = fstart[blockIdx.x + 1];
+  pdl_wait();
+  if (zero) {
+    const long long n = (long long)(B.nz + 2) * B.sxy;
+    for (long long q = threadIdx.x; q < n; q += blockDim.x) phi[B.off + q] = T(0);
+    __syncthreads();
+  }
+  const int ncell = B.nx * B.ny * B.nz;
+  for (int it = 0; it < sweeps; ++it) {
+    for (int colour = 1; colour >= 0; --colour) {  // red (x+y+z odd) first
+      for (int c = threadIdx.x; c < ncell; c += blockDim.x) {
+        const int x = 1 + c % B.nx, y = 1 + (c / B.nx) % B.ny, z = 1 + c / (B.nx * B.ny);
+        if (((x + y + z) & 1) != colour) continue;
+        const long long i = B.off + (long long)z * B.sxy + (long long)y * B.sx + x;
+        const Coef<T> cf = cell_coef<T, VAR>(B, x, y, z, i - B.off, VAR ? fx + B.off : nullptr,
+                                             VAR ? fy + B.off : nullptr, VAR ? fz + B.off : nullptr);
+        const T ap = coef_ap(cf);
+        const T v = gs_div(rhs[i] - (cf.aw * phi[i - 1] + cf.ae * phi[i + 1] + cf.as * phi[i - B.sx] +
+                                     cf.an * phi[i + B.sx] + cf.ab * phi[i - B.sxy] + cf.at * phi[i + B.sxy]),
+                           ap);
+        phi[i] = v;
+      }
+      __syncthreads();
+    }
+    for (int q = f0 + threadIdx.x; q < f1; q += blockDim.x) phi[fdst[q]] = phi[fsrc[q] & kIdxMask];
+    __syncthreads();
+  }
+}
+
 template <typename T, bool VAR>
 __global__ void __launch_bounds__(1024) k_relax_small(const BlkLev* __restrict__ bls, const int* __restrict__ start,
                                                       int nb, T* __restrict__ phi, const T* __restrict__ rhs,
@@ -2842,6 +2883,25 @@ cudaError_t launch_relax_small(bool var, const BlkLev* bl, const int* start, int
                sweeps, (int)zero, nelems);
   return cudaGetLastError();
 }
+template <typename T>
+cudaError_t launch_relax_blocks(bool var, const BlkLev* bl, int nb, const int* fstart, T* phi, const T* rhs,
+                                const T* fx, const T* fy, const T* fz, const uint32_t* fdst, const uint32_t* fsrc,
+                                int sweeps, bool zero, cudaStream_t st) {
+  if (nb <= 0) return cudaSuccess;
+  if (var)
+    pdl_launch(k_relax_blocks<T, true>, nb, 1024, 0, st, bl, fstart, phi, rhs, fx, fy, fz, fdst, fsrc, sweeps,
+               (int)zero);
+  else
+    pdl_launch(k_relax_blocks<T, false>, nb, 1024, 0, st, bl, fstart, phi, rhs, fx, fy, fz, fdst, fsrc, sweeps,
+               (int)zero);
+  return cudaGetLastError();
+}
+template cudaError_t launch_relax_blocks<double>(bool, const BlkLev*, int, const int*, double*, const double*,
+                                                 const double*, const double*, const double*, const uint32_t*,
+                                                 const uint32_t*, int, bool, cudaStream_t);
+template cudaError_t launch_relax_blocks<float>(bool, const BlkLev*, int, const int*, float*, const float*,
+                                                const float*, const float*, const float*, const uint32_t*,
+                                                const uint32_t*, int, bool, cudaStream_t);
 template cudaError_t launch_relax_small<double>(bool, const BlkLev*, const int*, int, double*, const double*,
                                                 const double*, const double*, const double*, const uint32_t*,
                                                 const uint32_t*, int, int, bool, long long, cudaStream_t);

@@ -248,6 +248,14 @@ cudaError_t launch_face_coef_sum(const BlkLev* fine, const BlkLev* coarse, CellT
                                  const double* ffy, const double* ffz, double* cfx, double* cfy, double* cfz,
                                  cudaStream_t st);
 
+// `sweeps` in-place red-black sweeps of a level whose ghost fill is
+// block-local, one CTA per block; fstart: fill entries of each block (the
+// table sorted by block, nb + 1 entries).
+template <typename T>
+cudaError_t launch_relax_blocks(bool var, const BlkLev* bl, int nb, const int* fstart, T* phi, const T* rhs,
+                                const T* fx, const T* fy, const T* fz, const uint32_t* fdst, const uint32_t* fsrc,
+                                int sweeps, bool zero, cudaStream_t st);
+
 // Stone's SIP (sipsol.for) on level 1: factor arrays and the residual
 // (level-1 layout, zero outside the interior).
 struct SipArrays {

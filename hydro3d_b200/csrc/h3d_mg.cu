@@ -33,6 +33,9 @@ namespace {
 
 // Levels with at most this many interior cells relax in one single-CTA launch.
 constexpr int64_t kSmallLevelCells = 2048;
+// Largest block relaxed by one CTA per visit (a 32^3 block in one CTA is slower
+// than the tiled sweep kernels; 16^3 is four cells a thread and colour)
+constexpr int64_t kBlockLocalCells = 4096;
 constexpr int64_t kTailLevelCells = 2048;  // levels the fused coarse tail (one CTA) takes
 
 struct Halo {
@@ -85,6 +88,9 @@ struct Level {
   bool f32 = false, var = false;  // iterate precision of the level's smoother; variable coefficients
   int* d_cstart = nullptr;  // small / tail levels: flat interior index of each block's first cell
   bool small = false;       // relaxation runs as one fused single-CTA kernel
+  bool blocal = false;      // the sweep fill stays inside every block: a visit is one launch, a CTA per block
+  Halo lfill;               // that fill, sorted by block
+  int* d_lfstart = nullptr; // its per-block entry ranges (nb + 1)
   bool tailable = false;    // small enough for the fused coarse tail (has d_cstart)
   int cur64 = 0, cur32 = 0;
   bool zero64 = false, zero32 = false;
@@ -540,6 +546,21 @@ struct Exec {
         V.zero64 = false;
       }
       TRY(chk("relax small", g));
+      h->kernels += 1;
+      return H3D_OK;
+    }
+    if (it > 0 && V.blocal && g > 1 && h->desc.mg_itrsch == 3) {  // a visit in one launch, a CTA per block
+      const int nb = (int)V.geom.bl.size();
+      if (mixed_level(g)) {
+        CU(launch_relax_blocks<float>(h->var, V.d_bl, nb, V.d_lfstart, V.phi32[V.cur32], V.rhs32, V.fx32, V.fy32,
+                                      V.fz32, V.lfill.d_dst, V.lfill.d_src, it, V.zero32, h->st));
+        V.zero32 = false;
+      } else {
+        CU(launch_relax_blocks<double>(h->var, V.d_bl, nb, V.d_lfstart, V.phi64[V.cur64], V.rhs64, V.fx64, V.fy64,
+                                       V.fz64, V.lfill.d_dst, V.lfill.d_src, it, V.zero64, h->st));
+        V.zero64 = false;
+      }
+      TRY(chk("relax blocks", g));
       h->kernels += 1;
       return H3D_OK;
     }
@@ -1908,7 +1929,7 @@ int h3d_mg_destroy(h3d_mg* h) {
     void* ps[] = {V.d_bl, V.d_cta_all, V.d_cta_int, V.d_rows_all, V.d_rows_int, V.d_tiles, V.phi64[0], V.phi64[1], V.rhs64, V.phi32[0],
                   V.phi32[1], V.rhs32, V.fx64, V.fy64, V.fz64, V.fx32, V.fy32, V.fz32, V.dens,
                   V.sweep.d_dst, V.sweep.d_src, V.faces.d_dst, V.faces.d_src, V.exch.d_dst, V.exch.d_src,
-                  V.bound.d_dst, V.bound.d_src, V.sweep_push.d_dst, V.sweep_push.d_src, V.d_push, V.d_maps, V.d_rmaps, V.d_rtiles, V.d_ptiles, V.d_qtiles, V.d_dtiles, V.d_cstart, V.d_dstart, V.d_pstart, V.seq64, V.seq32, V.d_ztiles};
+                  V.bound.d_dst, V.bound.d_src, V.sweep_push.d_dst, V.sweep_push.d_src, V.d_push, V.d_maps, V.d_rmaps, V.d_rtiles, V.d_ptiles, V.d_qtiles, V.d_dtiles, V.d_cstart, V.d_dstart, V.d_pstart, V.seq64, V.seq32, V.d_ztiles, V.lfill.d_dst, V.lfill.d_src, V.d_lfstart};
     for (void* p : ps) dfree(p);
   }
   dfree(h->p64[0]);
@@ -2056,6 +2077,40 @@ int h3d_mg_create(h3d_mg** out, const h3d_mg_desc* desc) {
           return bail(fail(h, H3D_ERR_CUDA, "small-level table"));
         V.tailable = true;
         V.small = V.geom.n_interior <= kSmallLevelCells;
+      }
+    }
+    // levels whose fill stays inside every block and whose blocks are small
+    // enough for one CTA each relax a whole visit in one launch
+    if (g > 1 && !V.small) {
+      int64_t maxc = 0;
+      std::vector<int> owner(V.geom.bl.size());
+      for (const auto& B : V.geom.bl) maxc = std::max<int64_t>(maxc, (int64_t)B.nx * B.ny * B.nz);
+      auto block_of = [&](uint32_t idx) {
+        for (size_t b = 0; b < V.geom.bl.size(); ++b) {
+          const BlkLev& B = V.geom.bl[b];
+          if ((long long)idx >= B.off && (long long)idx < B.off + (long long)(B.nz + 2) * B.sxy) return (int)b;
+        }
+        return -1;
+      };
+      bool local = maxc <= kBlockLocalCells;
+      std::vector<std::vector<std::pair<uint32_t, uint32_t>>> per(V.geom.bl.size());
+      for (size_t e = 0; local && e < d.size(); ++e) {
+        const int bd = block_of(d[e]), bs = block_of(s[e] & kIdxMask);
+        if (bd < 0 || bd != bs || (s[e] & kOldFlag)) local = false;  // in place: interior sources only
+        else per[bd].push_back({d[e], s[e]});
+      }
+      if (local) {
+        std::vector<uint32_t> ld, ls;
+        std::vector<int> st(1, 0);
+        for (const auto& v : per) {
+          for (const auto& pr : v) { ld.push_back(pr.first); ls.push_back(pr.second); }
+          st.push_back((int)ld.size());
+        }
+        if ((rc = upload_halo(h, V.lfill, ld, ls)) != H3D_OK) return bail(rc);
+        if ((rc = dalloc(h, &V.d_lfstart, st.size())) != H3D_OK) return bail(rc);
+        if (cudaMemcpy(V.d_lfstart, st.data(), st.size() * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess)
+          return bail(fail(h, H3D_ERR_CUDA, "block-local fill table"));
+        V.blocal = true;
       }
     }
     if (g == 1) {
