@@ -139,6 +139,17 @@ extern "C" int h3d_residual_noalloc(const double* p, const double* b, int32_t nx
     h3d::set_call_error("h3d_residual_noalloc: null pointer or empty block");
     return H3D_ERR_ARG;
   }
+  {
+    // it copies to host memory and synchronises the stream: neither may be
+    // captured into a graph, so a capturing stream is refused before any work
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaError_t e = cudaStreamIsCapturing(static_cast<cudaStream_t>(stream), &cs);
+    if (e != cudaSuccess || cs != cudaStreamCaptureStatusNone) {
+      h3d::set_call_error("h3d_residual_noalloc: the stream is being captured into a CUDA graph; this call copies "
+                          "its result to host memory and synchronises the stream, so it cannot be captured");
+      return H3D_ERR_ARG;
+    }
+  }
   if ((long long)ny * nz > kNoAllocMaxRows) {
     h3d::set_call_error("h3d_residual_noalloc: block has ny*nz = " + std::to_string((long long)ny * nz) +
                         " rows; the allocation-free residual handles at most " + std::to_string(kNoAllocMaxRows));

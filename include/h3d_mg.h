@@ -287,7 +287,8 @@ int h3d_halo_table(int32_t nblocks, const h3d_block_desc* blocks, int32_t g,
  * that array's device address and the device's multiprocessor count.  Calls
  * that overlap on the GPU share the array and race.  The call copies its
  * result into `out` on `stream` and synchronises that stream before it
- * returns. */
+ * returns, so it cannot run on a stream that is being captured into a CUDA
+ * graph: it then returns H3D_ERR_ARG without doing anything. */
 int h3d_residual_noalloc(const double* p, const double* b, int32_t nx, int32_t ny, int32_t nz,
                          const double* h, int32_t phys_mask, double* out, void* stream);
 

@@ -133,3 +133,29 @@ def test_noalloc_reports_nan(h3d):
     lib = h3d.lib()
     out = _call(lib, torch.from_numpy(p).cuda(), torch.from_numpy(b).cuda(), n, (1.0, 1.0, 1.0), 63)
     assert np.all(np.isnan(out)), out
+
+
+def test_noalloc_refuses_a_capturing_stream(h3d):
+    """The call copies its result to host memory and synchronises its stream,
+    which a stream under graph capture does not allow: it must return
+    H3D_ERR_ARG at once, before any work, and leave the capture intact."""
+    import torch
+    n = (8, 8, 8)
+    lib = h3d._lib.lib()
+    p = torch.zeros((n[2] + 2, n[1] + 2, n[0] + 2), dtype=torch.float64, device="cuda")
+    b = torch.zeros_like(p)
+    _call(lib, p, b, n, (0.1, 0.1, 0.1), 63)  # first call on the device: set-up outside any capture
+    s = torch.cuda.Stream()
+    g = torch.cuda.CUDAGraph()
+    out = (C.c_double * 4)()
+    hh = (C.c_double * 3)(0.1, 0.1, 0.1)
+    with torch.cuda.graph(g, stream=s):
+        rc = lib.h3d_residual_noalloc(C.c_void_p(p.data_ptr()), C.c_void_p(b.data_ptr()), n[0], n[1], n[2], hh, 63,
+                                      out, C.c_void_p(s.cuda_stream))
+        p.add_(1.0)  # the capture itself stays valid
+    assert rc == h3d._lib.H3D_ERR_ARG
+    assert b"captured" in lib.h3d_mg_last_error(None)
+    g.replay()
+    torch.cuda.synchronize()
+    assert float(p[1, 1, 1]) == 1.0
+    del g
