@@ -80,3 +80,25 @@ def independent_blocks(sizes: Sequence[Sequence[int]], h: Sequence[float], ngrid
                        resolve=None):
     """Blocks that do not touch (each an isolated all-wall Poisson problem)."""
     return from_extents(gap_extents(sizes), [WALL] * 6, h, ngrid, pl, resolve)
+
+
+def refine(descs, rdiv: Sequence[int], ngrid_input: int):
+    """Local mesh refinement of a layout (LMR = 2, localparameters.for:24-59,
+    102-104, 247-249): block b keeps its physical extent and gets rdiv[b]
+    times the cells per axis, spacing h / rdiv[b] and ngrid_input +
+    log2(rdiv[b]) levels.  `descs` are the unrefined descriptors (ngrid and h
+    of the coarse layout); they are changed in place and returned.  Face,
+    edge and corner neighbours may differ by a factor of 2 in rdiv."""
+    for d, r in zip(descs, rdiv):
+        r = int(r)
+        lg = r.bit_length() - 1
+        if r < 1 or (1 << lg) != r:
+            raise ValueError("rdiv must be a power of 2")
+        for a in range(3):
+            d.n[a] = d.n[a] * r
+            d.h[a] = d.h[a] / r
+            d.origin[a] = d.origin[a] * r
+            d.ttc[a] = d.n[a] + 2 * d.pl
+        d.rdiv = r
+        d.ngrid = int(ngrid_input) + lg
+    return descs

@@ -1137,10 +1137,13 @@ class Reference:
         M.v_rdiv = FArray("i", [(0, nb - 1)])
         M.v_myrank = 0
         M.v_nprocs = 1
-        # control.cin settings the path reads
-        M.v_lmr = 1
+        rdivs = [int(getattr(d, "rdiv", 1) or 1) for d in blocks]
+        lmr = any(r > 1 for r in rdivs)
+        ngrid_input = ngrd_gl - (max(rdivs).bit_length() - 1)
+        # control.cin settings the path reads (LMR = 2: local mesh refinement)
+        M.v_lmr = 2 if lmr else 1
         M.v_pl_ex = pl_ex
-        M.v_ngrid_input = ngrd_gl
+        M.v_ngrid_input = ngrid_input
         M.v_solver = 2
         M.v_mg_itrsch = mg_itrsch
         M.v_irestr = irestr
@@ -1148,24 +1151,29 @@ class Reference:
         M.v_l_lsm = bool(lsm)
         M.v_l_lsmbase = False
         M.v_periodic = any(int(c) == 5 for d in blocks for c in d.bc)
-        M.v_g_dx, M.v_g_dy, M.v_g_dz = (float(x) for x in blocks[0].h)
+        # g_dx: the unrefined spacing; a block of ratio rdiv has g_dx / rdiv
+        # (localparameters.for:247-249) and its origin in its own cells
+        M.v_g_dx, M.v_g_dy, M.v_g_dz = (float(x) * rdivs[0] for x in blocks[0].h)
         for ib, d in enumerate(blocks, 1):
             o = Obj(T)
             M.v_dom.s(o, ib)
             M.v_dom_id.s(ib - 1, ib)
             M.v_dom_ad.s(0, ib - 1)
             M.v_dom_indid.s(ib, ib - 1)
-            M.v_rdiv.s(1, ib - 1)
-            if tuple(float(x) for x in d.h) != (M.v_g_dx, M.v_g_dy, M.v_g_dz):
-                raise FortranError("blocks with different spacings need rdiv > 1")
-            o.c_ngrid = int(d.ngrid)
+            r = rdivs[ib - 1]
+            M.v_rdiv.s(r, ib - 1)
+            if tuple(float(x) * r for x in d.h) != (M.v_g_dx, M.v_g_dy, M.v_g_dz):
+                raise FortranError("block spacings are not g_dx / rdiv")
+            o.c_ngrid = ngrid_input  # localparameters.for:44-47 adds log2(rdiv)
             # alloc_dom.for:read_infodom extents (xsl..zel) and neighbours
-            o.c_xsl = d.origin[0] * M.v_g_dx
-            o.c_xel = (d.origin[0] + d.n[0]) * M.v_g_dx
-            o.c_ysl = d.origin[1] * M.v_g_dy
-            o.c_yel = (d.origin[1] + d.n[1]) * M.v_g_dy
-            o.c_zsl = d.origin[2] * M.v_g_dz
-            o.c_zel = (d.origin[2] + d.n[2]) * M.v_g_dz
+            if any(d.origin[a] % r or d.n[a] % r for a in range(3)):
+                raise FortranError("refined block not aligned with the unrefined grid")
+            o.c_xsl = (d.origin[0] // r) * M.v_g_dx
+            o.c_xel = ((d.origin[0] + d.n[0]) // r) * M.v_g_dx
+            o.c_ysl = (d.origin[1] // r) * M.v_g_dy
+            o.c_yel = ((d.origin[1] + d.n[1]) // r) * M.v_g_dy
+            o.c_zsl = (d.origin[2] // r) * M.v_g_dz
+            o.c_zel = ((d.origin[2] + d.n[2]) // r) * M.v_g_dz
             for name, v in zip(("iprev", "inext", "jprev", "jnext", "kprev", "knext"), d.nb_face):
                 setattr(o, "c_" + name, int(v))
             for name, v in zip(("corprev1", "corprev2", "corprev3", "corprev4",
@@ -1182,6 +1190,10 @@ class Reference:
         self.ns["localparameters"]()
         if M.v_ngrd_gl != ngrd_gl:
             raise FortranError("ngrd_gl changed by localparameters")
+        for ib, d in enumerate(blocks, 1):
+            if M.v_dom.g(ib).c_ngrid != int(d.ngrid):
+                raise FortranError("block %d: localparameters gives ngrid %d, the descriptor %d"
+                                   % (ib - 1, M.v_dom.g(ib).c_ngrid, int(d.ngrid)))
         # initial.for:140-290 allocations of the arrays the solver touches
         for ib in range(1, nb + 1):
             o = M.v_dom.g(ib)

@@ -3,8 +3,10 @@
  *
  * A restatement in C of the reference multigrid path of Hydro3D v7.0:
  *   coeff, mgkcyc, mgrelax, mgrestr, mgcorr, mgbound   (src_v70/mgsolver.for)
- *   exchangepp, exchbc_mgpp (same-rank, equal-resolution branches)
+ *   exchangepp, exchbc_mgpp (same-rank branches, incl. the local mesh
+ *   refinement ones between blocks of refinement ratio 1:2)
  *                                                      (src_v70/exchangepp.for)
+ *   rdv(ib,g) and per-block level counts of LMR       (src_v70/localparameters.for:24-59)
  *   newsolv_mg outer loop                              (src_v70/newsolv_mg.for)
  *   read_infodom neighbour discovery                   (src_v70/alloc_dom.for)
  * All arithmetic is IEEE FP64 evaluated left to right in the reference's
@@ -48,8 +50,11 @@ struct or_mg {
   int nbp, ngrd_gl, mg_itrsch, irestr, iproln, lsm, periodic;
   int ngg;                      /* longest line / largest plane */
   int err;
+  int lmr;                      /* some blocks have rdiv > 1 */
+  int* rdv;                     /* rdv(ib, g) at rdv[ib * (MAXLEV + 1) + g] */
   or_dom* dom;
 };
+#define RDV(m, ib, g) ((m)->rdv[(ib) * (MAXLEV + 1) + (g)])
 
 static int g_threads = 1;
 void or_set_threads(int n) { g_threads = n > 0 ? n : 1; }
@@ -78,13 +83,38 @@ or_mg* or_create(int nblocks, const or_block_desc* blocks, int ngrd_gl,
   m->iproln = iproln;
   m->lsm = lsm;
   m->dom = (or_dom*)calloc((size_t)nblocks, sizeof(or_dom));
+  m->rdv = (int*)calloc((size_t)nblocks * (MAXLEV + 1), sizeof(int));
   if (ngrd_gl < 1 || ngrd_gl > MAXLEV) m->err = 1;
+  /* localparameters.for:28-59: ngrd_gl = ngrid_input + log2(max rdiv); a block
+   * of ratio rdiv has ngrid_input + log2(rdiv) levels; rdv(ib, g) is rdiv up to
+   * level ngrid_input, halves on each further level of the block, and is 1
+   * beyond the block's last level. */
+  int maxlog = 0;
+  for (int ib = 0; ib < nblocks; ++ib) {
+    int r = blocks[ib].rdiv, lg = 0;
+    while ((1 << lg) < r) ++lg;
+    if (r < 1 || (1 << lg) != r) m->err = 1;
+    if (lg > maxlog) maxlog = lg;
+    if (r > 1) m->lmr = 1;
+  }
+  int ngrid_input = ngrd_gl - maxlog;
+  if (ngrid_input < 1) m->err = 1;
   int nmax = 0;
   for (int ib = 0; ib < nblocks; ++ib) {
     or_dom* d = &m->dom[ib];
     d->d = blocks[ib];
     d->ngrid = blocks[ib].ngrid;
-    if (d->ngrid != ngrd_gl || blocks[ib].rdiv != 1) m->err = 1;
+    int lg = 0;
+    while ((1 << lg) < blocks[ib].rdiv) ++lg;
+    if (d->ngrid != ngrid_input + lg) m->err = 1;
+    if (m->err) continue;
+    for (int g = 1; g <= ngrd_gl; ++g) {
+      int v;
+      if (g > d->ngrid) v = 1;
+      else if (g <= ngrid_input) v = blocks[ib].rdiv;
+      else v = RDV(m, ib, g - 1) / 2;
+      RDV(m, ib, g) = v;
+    }
     for (int a = 0; a < 6; ++a)
       if (d->d.bc[a] == 5) m->periodic = 1; /* alloc_dom.for:1224-1231 */
     /* divisibility check, localparameters.for:204-209 */
@@ -150,6 +180,7 @@ void or_destroy(or_mg* m) {
     }
   }
   free(m->dom);
+  free(m->rdv);
   free(m);
 }
 
@@ -424,116 +455,231 @@ static int edge_len(int e, int ni, int nj, int nk) {
   return ax == 0 ? ni : (ax == 1 ? nj : nk);
 }
 
+/* Level view of one block for the exchange: dims incl. ghosts and the phi
+ * slab offsets of mgsolver.for:412. */
+typedef struct {
+  int n[3];            /* ni, nj, nk */
+  int64_t nij, nj, nijk;
+  double* fi;
+} lview;
+
+static lview lview_of(or_mg* m, int ib, int g) {
+  or_dom* d = &m->dom[ib];
+  lview v;
+  lev_dims(d, g, &v.n[0], &v.n[1], &v.n[2]);
+  v.nj = v.n[1];
+  v.nij = (int64_t)v.n[0] * v.n[1];
+  v.nijk = d->faz[g] - v.nij * v.n[2];
+  v.fi = d->cof;
+  return v;
+}
+
+static int64_t lcell(const lview* v, int i, int j, int k) {
+  return (int64_t)(k - 1) * v->nij + (int64_t)(i - 1) * v->nj + j + v->nijk;
+}
+
+/* A face plane of sync direction a (0: i, 1: j, 2: k) is addressed as
+ * (c, u, w): c along the direction, (u, w) in the plane with u fastest in the
+ * receive buffer, (w - 1) * ns1 + u: (j, k) for a = 0, (i, k) for a = 1,
+ * (j, i) for a = 2 (exchangepp.for:69-122). */
+static int64_t fcell(const lview* v, int a, int c, int u, int w) {
+  if (a == 0) return lcell(v, c, u, w);
+  if (a == 1) return lcell(v, u, c, w);
+  return lcell(v, w, u, c);
+}
+static int fns1(const lview* v, int a) { return a == 1 ? v->n[0] : v->n[1]; }
+static int fns2(const lview* v, int a) { return a == 2 ? v->n[0] : v->n[2]; }
+
+/* Pack of sender sb's face plane for the receiver's buffer rb (prev: the
+ * sender's first interior planes go to its previous neighbour).  Equal
+ * resolution: the full plane (exchangepp.for:155-162); sender finer: the 8-cell
+ * average of its two first planes on the receiver's coarse plane interior
+ * (:164-174); sender coarser: 2 x its first plane on the four fine cells of
+ * each coarse cell (:176-189). */
+static void face_pack(const lview* s, int a, int prev, int cmp, double* rb) {
+  const double* fi = s->fi;
+  int ns1 = fns1(s, a), ns2 = fns2(s, a), na = s->n[a];
+  if (cmp == 0) {
+    int c = prev ? 2 : na - 1;
+    for (int w = 1; w <= ns2; ++w)
+      for (int u = 1; u <= ns1; ++u) rb[(w - 1) * ns1 + u] = fi[fcell(s, a, c, u, w)];
+  } else if (cmp > 0) {
+    int nsc1 = (ns1 - 2) / 2 + 2, nsc2 = (ns2 - 2) / 2 + 2;
+    int c0 = prev ? 2 : na - 2;
+    for (int w = 2; w <= nsc2 - 1; ++w)
+      for (int u = 2; u <= nsc1 - 1; ++u) {
+        int u0 = 2 * u - 2, w0 = 2 * w - 2;
+        rb[(w - 1) * nsc1 + u] =
+            0.125 * (fi[fcell(s, a, c0, u0, w0)] + fi[fcell(s, a, c0, u0 + 1, w0)] +
+                     fi[fcell(s, a, c0, u0, w0 + 1)] + fi[fcell(s, a, c0, u0 + 1, w0 + 1)] +
+                     fi[fcell(s, a, c0 + 1, u0, w0)] + fi[fcell(s, a, c0 + 1, u0 + 1, w0)] +
+                     fi[fcell(s, a, c0 + 1, u0, w0 + 1)] + fi[fcell(s, a, c0 + 1, u0 + 1, w0 + 1)]);
+      }
+  } else {
+    int nsr1 = 2 * (ns1 - 2) + 2;
+    int c = prev ? 2 : na - 1;
+    for (int w = 2; w <= ns2 - 1; ++w)
+      for (int u = 2; u <= ns1 - 1; ++u) {
+        double val = 2.0 * fi[fcell(s, a, c, u, w)];
+        rb[(2 * w - 3) * nsr1 + 2 * u - 2] = val;
+        rb[(2 * w - 3) * nsr1 + 2 * u - 1] = val;
+        rb[(2 * w - 2) * nsr1 + 2 * u - 2] = val;
+        rb[(2 * w - 2) * nsr1 + 2 * u - 1] = val;
+      }
+  }
+}
+
+/* Unpack into the receiver's ghost plane (prev: c = 1, next: c = n).  Equal:
+ * the full plane (exchangepp.for:2106-2113); receiver finer: (r + 3 f1 - f2)/4
+ * from the received value and its first two interior planes, over the full
+ * plane (:2115-2123); receiver coarser: the plane's interior rows (:2125-2131). */
+static void face_unpack(lview* r, int a, int prev, int cmp, const double* rb) {
+  double* fi = r->fi;
+  int ns1 = fns1(r, a), ns2 = fns2(r, a), na = r->n[a];
+  int cg = prev ? 1 : na, c1 = prev ? 2 : na - 1, c2 = prev ? 3 : na - 2;
+  if (cmp == 0) {
+    for (int w = 1; w <= ns2; ++w)
+      for (int u = 1; u <= ns1; ++u) fi[fcell(r, a, cg, u, w)] = rb[(w - 1) * ns1 + u];
+  } else if (cmp > 0) {
+    for (int w = 1; w <= ns2; ++w)
+      for (int u = 1; u <= ns1; ++u)
+        fi[fcell(r, a, cg, u, w)] =
+            (rb[(w - 1) * ns1 + u] + 3.0 * fi[fcell(r, a, c1, u, w)] - fi[fcell(r, a, c2, u, w)]) / 4.0;
+  } else {
+    for (int w = 2; w <= ns2 - 1; ++w)
+      for (int u = 2; u <= ns1 - 1; ++u) fi[fcell(r, a, cg, u, w)] = rb[(w - 1) * ns1 + u];
+  }
+}
+
+/* Corner/edge sender cells: per axis (i, j, k) the code P2 ("2") or PN1
+ * ("n-1"), or RUN for an edge's running index. */
+static int lmr_pos(int code, int n, int run) { return code == RUN ? run : (code == P2 ? 2 : n - 1); }
+
+/* The 8-cell average of a finer sender at a corner or edge: the 2x2x2 cells
+ * from base (i0,j0,k0), summed with j, then i, then k as the fastest bit
+ * (exchangepp.for:447-451, 653-659), divided by 8. */
+static double avg8_jik(const lview* s, int i0, int j0, int k0) {
+  const double* fi = s->fi;
+  int64_t ll = lcell(s, i0, j0, k0), nj = s->nj, nij = s->nij;
+  return (fi[ll] + fi[ll + 1] + fi[ll + nj] + fi[ll + 1 + nj] + fi[ll + nij] + fi[ll + 1 + nij] +
+          fi[ll + nj + nij] + fi[ll + 1 + nj + nij]) / 8.0;
+}
+
+/* Trilinear value of a coarser sender at a fine corner/edge cell: 27, 9, 3, 1
+ * weights of the cell and its neighbours toward the receiver (steps sj, si,
+ * sk of +-1), in the j, i, k bit order, divided by 64 (exchangepp.for:452-458). */
+static double interp64_jik(const lview* s, int i0, int j0, int k0, int si, int sj, int sk) {
+  const double* fi = s->fi;
+  int64_t ll = lcell(s, i0, j0, k0);
+  int64_t dj = sj, di = (int64_t)si * s->nj, dk = (int64_t)sk * s->nij;
+  return (27.0 * fi[ll] + 9.0 * fi[ll + dj] + 9.0 * fi[ll + di] + 3.0 * fi[ll + di + dj] + 9.0 * fi[ll + dk] +
+          3.0 * fi[ll + dj + dk] + 3.0 * fi[ll + di + dk] + 1.0 * fi[ll + di + dj + dk]) / 64.0;
+}
+
+static int sgn_out(int code) { return code == P2 ? -1 : 1; }
+
+/* A corner value for the receiver (exchangepp.for:441-640, 1400-1600). */
+static double corner_pack(const lview* s, const int* code, int cmp) {
+  if (cmp == 0) return s->fi[lcell(s, lmr_pos(code[0], s->n[0], 0), lmr_pos(code[1], s->n[1], 0),
+                                   lmr_pos(code[2], s->n[2], 0))];
+  if (cmp > 0) {
+    int b[3];
+    for (int a = 0; a < 3; ++a) b[a] = code[a] == P2 ? 2 : s->n[a] - 2;
+    return avg8_jik(s, b[0], b[1], b[2]);
+  }
+  return interp64_jik(s, lmr_pos(code[0], s->n[0], 0), lmr_pos(code[1], s->n[1], 0),
+                      lmr_pos(code[2], s->n[2], 0), sgn_out(code[0]), sgn_out(code[1]), sgn_out(code[2]));
+}
+
+/* An edge line for the receiver's buffer buf (exchangepp.for:646-1100,
+ * 1604-2056): equal, nn = 2..len-1; sender finer, the averages of the fine
+ * pairs 2nn-2, 2nn-1 on nn = 2..lenc-1; sender coarser, two fine values
+ * 2nn-2 (running step -1) and 2nn-1 (+1) from each coarse cell. */
+static void edge_pack(const lview* s, const int* code, int ax, int cmp, double* buf) {
+  int len = s->n[ax];
+  if (cmp == 0) {
+    for (int nn = 2; nn <= len - 1; ++nn)
+      buf[nn] = s->fi[lcell(s, lmr_pos(code[0], s->n[0], nn), lmr_pos(code[1], s->n[1], nn),
+                            lmr_pos(code[2], s->n[2], nn))];
+  } else if (cmp > 0) {
+    int lenc = (len - 2) / 2 + 2;
+    for (int nn = 2; nn <= lenc - 1; ++nn) {
+      int b[3];
+      for (int a = 0; a < 3; ++a) b[a] = code[a] == RUN ? 2 * nn - 2 : (code[a] == P2 ? 2 : s->n[a] - 2);
+      buf[nn] = avg8_jik(s, b[0], b[1], b[2]);
+    }
+  } else {
+    for (int nn = 2; nn <= len - 1; ++nn)
+      for (int h = 0; h < 2; ++h) {
+        int sg[3];
+        for (int a = 0; a < 3; ++a) sg[a] = code[a] == RUN ? (h ? 1 : -1) : sgn_out(code[a]);
+        buf[2 * nn - 2 + h] = interp64_jik(s, lmr_pos(code[0], s->n[0], nn), lmr_pos(code[1], s->n[1], nn),
+                                           lmr_pos(code[2], s->n[2], nn), sg[0], sg[1], sg[2]);
+      }
+  }
+}
+
+static int rdv_cmp(const or_mg* m, int a, int b, int g) {
+  int ra = RDV(m, a, g), rb = RDV(m, b, g);
+  return ra == rb ? 0 : (ra > rb ? 1 : -1);
+}
+
 void or_exchangepp(or_mg* m, int g) { /* exchangepp.for:2-2835 */
+  if (m->lmr)
+    /* The reference reads receive-buffer entries no sender of this call wrote
+     * (the ghost rows of a plane a coarser neighbour sends); they hold what an
+     * earlier exchange left there.  Here they read as zero. */
+    for (int ib = 0; ib < m->nbp; ++ib) {
+      memset(m->dom[ib].recvb_m1, 0, sizeof(double) * ((size_t)m->ngg + 1));
+      memset(m->dom[ib].recvb_p1, 0, sizeof(double) * ((size_t)m->ngg + 1));
+    }
   for (int sync_dir = 1; sync_dir <= 3; ++sync_dir) {
-    /* pack loop, exchangepp.for:48-2063 (same-rank, equal-resolution) */
+    const int a = sync_dir - 1;
+    /* pack loop, exchangepp.for:48-2063 (same-rank branches) */
     for (int ib = 0; ib < m->nbp; ++ib) {
       or_dom* d = &m->dom[ib];
-      int ni, nj, nk;
-      lev_dims(d, g, &ni, &nj, &nk);
-      int64_t nij = (int64_t)ni * nj, nijk = d->faz[g] - (int64_t)ni * nj * nk;
-      const double* fi = d->cof;
-      int cprev = d->d.nb_face[2 * (sync_dir - 1)];
-      int cnext = d->d.nb_face[2 * (sync_dir - 1) + 1];
-      if (cprev >= 0) { /* :149-271 */
-        double* rb = m->dom[cprev].recvb_p1;
-        if (sync_dir == 1) {
-          for (int k = 1; k <= nk; ++k)
-            for (int j = 1; j <= nj; ++j) rb[(k - 1) * nj + j] = fi[PHI(2, j, k)];
-        } else if (sync_dir == 2) {
-          for (int k = 1; k <= nk; ++k)
-            for (int i = 1; i <= ni; ++i) rb[(k - 1) * ni + i] = fi[PHI(i, 2, k)];
-        } else {
-          for (int i = 1; i <= ni; ++i)
-            for (int j = 1; j <= nj; ++j) rb[(i - 1) * nj + j] = fi[PHI(i, j, 2)];
-        }
-      }
+      lview s = lview_of(m, ib, g);
+      int cprev = d->d.nb_face[2 * a];
+      int cnext = d->d.nb_face[2 * a + 1];
+      if (cprev >= 0) face_pack(&s, a, 1, rdv_cmp(m, ib, cprev, g), m->dom[cprev].recvb_p1); /* :149-430 */
       if (sync_dir == 3) { /* prev corners and edges, :435-1100 */
         for (int c = 0; c < 4; ++c) {
           int nbr = d->d.nb_corner[c];
           if (nbr < 0) continue;
-          m->dom[nbr].rc_p[c + 1] =
-              fi[PHI(pos(corprev_src[c][0], ni, 0), pos(corprev_src[c][1], nj, 0),
-                     pos(corprev_src[c][2], nk, 0))];
+          m->dom[nbr].rc_p[c + 1] = corner_pack(&s, corprev_src[c], rdv_cmp(m, ib, nbr, g));
         }
         for (int e = 0; e < 6; ++e) {
           int nbr = d->d.nb_edge[e];
           if (nbr < 0) continue;
-          int len = edge_len(e, ni, nj, nk);
-          for (int nn = 2; nn <= len - 1; ++nn)
-            m->dom[nbr].re_p[e + 1][nn] =
-                fi[PHI(pos(edgprev_src[e][0], ni, nn), pos(edgprev_src[e][1], nj, nn),
-                       pos(edgprev_src[e][2], nk, nn))];
+          edge_pack(&s, edgprev_src[e], edg_axis[e], rdv_cmp(m, ib, nbr, g), m->dom[nbr].re_p[e + 1]);
         }
       }
-      if (cnext >= 0) { /* :1107-1393 */
-        double* rb = m->dom[cnext].recvb_m1;
-        if (sync_dir == 1) {
-          for (int k = 1; k <= nk; ++k)
-            for (int j = 1; j <= nj; ++j) rb[(k - 1) * nj + j] = fi[PHI(ni - 1, j, k)];
-        } else if (sync_dir == 2) {
-          for (int k = 1; k <= nk; ++k)
-            for (int i = 1; i <= ni; ++i) rb[(k - 1) * ni + i] = fi[PHI(i, nj - 1, k)];
-        } else {
-          for (int i = 1; i <= ni; ++i)
-            for (int j = 1; j <= nj; ++j) rb[(i - 1) * nj + j] = fi[PHI(i, j, nk - 1)];
-        }
-      }
+      if (cnext >= 0) face_pack(&s, a, 0, rdv_cmp(m, ib, cnext, g), m->dom[cnext].recvb_m1); /* :1107-1393 */
       if (sync_dir == 3) { /* next corners and edges, :1394-2060 */
         for (int c = 0; c < 4; ++c) {
           int nbr = d->d.nb_corner[4 + c];
           if (nbr < 0) continue;
-          m->dom[nbr].rc_m[c + 1] =
-              fi[PHI(pos(cornext_src[c][0], ni, 0), pos(cornext_src[c][1], nj, 0),
-                     pos(cornext_src[c][2], nk, 0))];
+          m->dom[nbr].rc_m[c + 1] = corner_pack(&s, cornext_src[c], rdv_cmp(m, ib, nbr, g));
         }
         for (int e = 0; e < 6; ++e) {
           int nbr = d->d.nb_edge[6 + e];
           if (nbr < 0) continue;
-          int len = edge_len(e, ni, nj, nk);
-          for (int nn = 2; nn <= len - 1; ++nn)
-            m->dom[nbr].re_m[e + 1][nn] =
-                fi[PHI(pos(edgnext_src[e][0], ni, nn), pos(edgnext_src[e][1], nj, nn),
-                       pos(edgnext_src[e][2], nk, nn))];
+          edge_pack(&s, edgnext_src[e], edg_axis[e], rdv_cmp(m, ib, nbr, g), m->dom[nbr].re_m[e + 1]);
         }
       }
     }
     /* unpack loop, exchangepp.for:2066-2826 */
     for (int ib = 0; ib < m->nbp; ++ib) {
       or_dom* d = &m->dom[ib];
-      int ni, nj, nk;
-      lev_dims(d, g, &ni, &nj, &nk);
-      int64_t nij = (int64_t)ni * nj, nijk = d->faz[g] - (int64_t)ni * nj * nk;
-      double* fi = d->cof;
-      int cprev = d->d.nb_face[2 * (sync_dir - 1)];
-      int cnext = d->d.nb_face[2 * (sync_dir - 1) + 1];
-      if (cprev >= 0) { /* :2101-2196 */
-        const double* rb = d->recvb_m1;
-        if (sync_dir == 1) {
-          for (int k = 1; k <= nk; ++k)
-            for (int j = 1; j <= nj; ++j) fi[PHI(1, j, k)] = rb[(k - 1) * nj + j];
-        } else if (sync_dir == 2) {
-          for (int k = 1; k <= nk; ++k)
-            for (int i = 1; i <= ni; ++i) fi[PHI(i, 1, k)] = rb[(k - 1) * ni + i];
-        } else {
-          for (int i = 1; i <= ni; ++i)
-            for (int j = 1; j <= nj; ++j) fi[PHI(i, j, 1)] = rb[(i - 1) * nj + j];
-        }
-      }
-      if (cnext >= 0) { /* :2306-2402 */
-        const double* rb = d->recvb_p1;
-        if (sync_dir == 1) {
-          for (int k = 1; k <= nk; ++k)
-            for (int j = 1; j <= nj; ++j) fi[PHI(ni, j, k)] = rb[(k - 1) * nj + j];
-        } else if (sync_dir == 2) {
-          for (int k = 1; k <= nk; ++k)
-            for (int i = 1; i <= ni; ++i) fi[PHI(i, nj, k)] = rb[(k - 1) * ni + i];
-        } else {
-          for (int i = 1; i <= ni; ++i)
-            for (int j = 1; j <= nj; ++j) fi[PHI(i, j, nk)] = rb[(i - 1) * nj + j];
-        }
-      }
-      if (sync_dir == 3) { /* :2511-2826 */
+      lview r = lview_of(m, ib, g);
+      int64_t nij = r.nij, nj = r.nj, nijk = r.nijk;
+      double* fi = r.fi;
+      int ni = r.n[0], nk = r.n[2];
+      int cprev = d->d.nb_face[2 * a];
+      int cnext = d->d.nb_face[2 * a + 1];
+      if (cprev >= 0) face_unpack(&r, a, 1, rdv_cmp(m, ib, cprev, g), d->recvb_m1); /* :2101-2302 */
+      if (cnext >= 0) face_unpack(&r, a, 0, rdv_cmp(m, ib, cnext, g), d->recvb_p1); /* :2306-2505 */
+      if (sync_dir == 3) { /* :2511-2826, plain copies at every resolution */
         for (int c = 0; c < 4; ++c)
           if (d->d.nb_corner[c] >= 0)
             fi[PHI(pos(corprev_dst[c][0], ni, 0), pos(corprev_dst[c][1], nj, 0),

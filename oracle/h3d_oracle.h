@@ -43,7 +43,7 @@ typedef struct {
   int32_t nb_edge[12];    /* edgprev1..6 edgnext1..6                          */
   int32_t nb_periodic[6]; /* per_ip per_in per_jp per_jn per_kp per_kn        */
   int32_t bc[6];          /* bc_west bc_east bc_south bc_north bc_bottom bc_top */
-  int32_t rdiv;           /* refinement ratio (only 1 is supported)           */
+  int32_t rdiv;           /* local mesh refinement ratio (a power of 2; LMR)   */
   int32_t origin[3];      /* global cell index of the first interior cell     */
 } or_block_desc;
 

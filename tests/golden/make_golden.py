@@ -28,6 +28,7 @@ sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
 
 from oracle import fortran_ref as F  # noqa: E402
 from oracle import oracle as O  # noqa: E402
+from hydro3d_b200.topology import refine  # noqa: E402
 
 W, P = 4, 5
 
@@ -55,17 +56,40 @@ CASES = {
     "lexgs_2x2x1": (grid((2, 2, 1), (8, 8, 8)), [W, W, P, P, W, W], 3, 1, 0, False, 106),
     "tdma_2x2x1": (grid((2, 2, 1), (8, 8, 8)), [W] * 6, 3, 2, 0, False, 107),
 }
+# Local mesh refinement (LMR = 2): the layout above is the unrefined one and its
+# ngrd_gl is ngrid_input; block b gets rdiv[b] (hydro3d_b200.topology.refine).
+# Periodic partners keep equal ratios (exchbc_mgpp has no refinement branch).
+LMR_CASES = {
+    "lmr_walls_2x1x1": (grid((2, 1, 1), (8, 8, 8)), [W] * 6, 3, 3, 0, False, 111, [1, 2]),
+    "lmr_corners_2x2x2": (grid((2, 2, 2), (8, 8, 8)), [W] * 6, 3, 3, 0, False, 112, [2, 1, 1, 1, 1, 1, 1, 1]),
+    "lmr_periodic_x_1x2x2": (grid((1, 2, 2), (8, 8, 8)), [P, P, W, W, W, W], 2, 3, 0, False, 113, [1, 2, 2, 1]),
+    "lmr_ratio4_2x2x1": (grid((2, 2, 1), (4, 4, 4)), [W, W, W, W, P, P], 2, 3, 0, False, 114, [2, 2, 2, 4]),
+    "lmr_tdma_2x2x1": (grid((2, 2, 1), (8, 8, 8)), [W] * 6, 3, 2, 0, False, 115, [1, 2, 2, 1]),
+}
+CASES.update(LMR_CASES)
 H = (1.0 / 32, 1.0 / 32, 1.0 / 32)
 
 
+def lmr_descs(ext, bc, h, ngrid_input, rdiv):
+    """The unrefined layout's descriptors, refined by rdiv, and ngrd_gl."""
+    descs = refine(list(O.topology(ext, bc, h, ngrid_input)), rdiv, ngrid_input)
+    return descs, ngrid_input + max(int(r).bit_length() - 1 for r in rdiv)
+
+
 def run_case(name, src_dir=REF_SRC):
-    ext, bc, ngrd, itr, pl_ex, lsm, seed = CASES[name]
-    descs = O.topology(ext, bc, H, ngrd)
+    ext, bc, ngrd, itr, pl_ex, lsm, seed = CASES[name][:7]
+    rdiv = CASES[name][7] if len(CASES[name]) > 7 else None
+    if rdiv is None:
+        descs = O.topology(ext, bc, H, ngrd)
+    else:
+        descs, ngrd = lmr_descs(ext, bc, H, ngrd, rdiv)
     R = F.Reference(list(descs), ngrd, mg_itrsch=itr, pl_ex=pl_ex, lsm=lsm, src_dir=src_dir)
     pl = R.pl
     rng = np.random.default_rng(seed)
     out = {"ext": ext, "bc": np.array(bc, np.int32), "h": np.array(H), "ngrd_gl": ngrd, "mg_itrsch": itr,
            "pl": pl, "lsm": int(lsm), "nblocks": len(descs)}
+    if rdiv is not None:
+        out["rdiv"] = np.array(rdiv, np.int32)
     for ib, d in enumerate(descs):
         nx, ny, nz = d.n
         shp = (nz + 2 * pl, ny + 2 * pl, nx + 2 * pl)
@@ -287,20 +311,27 @@ def run_sip_case(name, src_dir=REF_SRC):
     return out
 
 
-def main():
+def main(prefix=""):
+    """Write every fixture whose name starts with prefix (all by default)."""
     for name in CASES:
+        if not name.startswith(prefix):
+            continue
         data = run_case(name)
         np.savez_compressed(os.path.join(HERE, "mgkcyc_%s.npz" % name), **data)
         print("wrote", name)
     for name in PROJ_CASES:
+        if not ("project_" + name).startswith(prefix):
+            continue
         data = run_projection_case(name)
         np.savez_compressed(os.path.join(HERE, "project_%s.npz" % name), **data)
         print("wrote project", name)
     for name in SIP_CASES:
+        if not ("sip_" + name).startswith(prefix):
+            continue
         data = run_sip_case(name)
         np.savez_compressed(os.path.join(HERE, "sip_%s.npz" % name), **data)
         print("wrote sip", name)
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1] if len(sys.argv) > 1 else "")

@@ -30,14 +30,27 @@ def _load(name):
 
 
 def test_fixtures_present():
-    assert len(NAMES) >= 7
+    assert len(NAMES) >= 12
+    assert sum(n.startswith("lmr_") for n in NAMES) >= 5
+
+
+def _layout(g, topo):
+    """Descriptors of a fixture's layout: topo(ext, bc, h, ngrid) builds the
+    unrefined blocks; LMR fixtures then refine them by their rdiv."""
+    ngrd = int(g["ngrd_gl"])
+    if "rdiv" not in g:
+        return list(topo(g["ext"], g["bc"], g["h"], ngrd))
+    from hydro3d_b200.topology import refine
+    rdiv = [int(r) for r in g["rdiv"]]
+    ngi = ngrd - (max(rdiv).bit_length() - 1)
+    return refine(list(topo(g["ext"], g["bc"], g["h"], ngi)), rdiv, ngi)
 
 
 @pytest.mark.parametrize("name", NAMES)
 def test_oracle_matches_reference(oracle_mod, name):
     g = _load(name)
     O = oracle_mod
-    descs = O.topology(g["ext"], g["bc"], g["h"], int(g["ngrd_gl"]))
+    descs = _layout(g, O.topology)
     nb = int(g["nblocks"])
     orc = O.Oracle(list(descs), int(g["ngrd_gl"]), int(g["mg_itrsch"]), 2, 1, lsm=bool(g["lsm"]))
     if g["lsm"]:
@@ -57,7 +70,7 @@ def test_cuda_matches_reference(h3d, name):
     g = _load(name)
     nb = int(g["nblocks"])
     ngrd = int(g["ngrd_gl"])
-    blocks = h3d.topology.from_extents(g["ext"], g["bc"], g["h"], ngrd, pl=1)
+    blocks = _layout(g, lambda e, b, h, n: h3d.topology.from_extents(e, b, h, n, pl=1))
     s = h3d.MultigridSolver(blocks, ngrd, mg_itrsch=int(g["mg_itrsch"]), var_coef=bool(g["lsm"]))
     if g["lsm"]:
         for ib, d in enumerate(blocks):
@@ -92,7 +105,7 @@ def _reference_tree():
 
 
 @pytest.mark.skipif(_reference_tree() is None, reason="reference source tree not present")
-@pytest.mark.parametrize("name", ["walls_2x1x1", "lsm_periodic_x_2x1x2", "periodic_x_2x2x2"])
+@pytest.mark.parametrize("name", ["walls_2x1x1", "lsm_periodic_x_2x1x2", "periodic_x_2x2x2", "lmr_corners_2x2x2"])
 def test_fixture_regenerates(oracle_mod, name):
     fresh = _make_golden().run_case(name)
     old = _load(name)
