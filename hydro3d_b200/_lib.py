@@ -104,7 +104,7 @@ EXPORTS = [
     "h3d_mg_history", "h3d_mg_put_level", "h3d_mg_get_level", "h3d_mg_mgrelax", "h3d_mg_mgrestr",
     "h3d_mg_mgcorr", "h3d_mg_mgbound", "h3d_mg_exchangepp", "h3d_mg_vcycle", "h3d_mg_sync",
     "h3d_mg_set_profiling", "h3d_mg_smoother_bytes", "h3d_mg_set_smoother", "h3d_mg_get_smoother",
-    "h3d_mg_set_restriction", "h3d_mg_get_restriction", "h3d_topology", "h3d_halo_table",
+    "h3d_mg_set_restriction", "h3d_mg_get_restriction", "h3d_topology", "h3d_halo_table", "h3d_halo_expr",
     "h3d_mg_strerror", "h3d_mg_last_error", "h3d_residual_noalloc",
     "h3d_mg_calvel", "h3d_mg_calmas", "h3d_mg_pbound", "h3d_mg_project_resident", "h3d_mg_project",
     "h3d_mg_set_wait_limit", "h3d_mg_wait_probe", "h3d_mg_sipsol", "h3d_mg_pressure_1sweep",
@@ -161,6 +161,8 @@ def lib():
         "h3d_mg_get_restriction": (i32, [vp, i32, C.POINTER(i32), C.POINTER(i32), C.POINTER(i32)]),
         "h3d_topology": (i32, [i32, C.POINTER(C.c_int32), C.POINTER(C.c_int32), pd, i32, C.POINTER(BlockDesc)]),
         "h3d_halo_table": (i32, [i32, C.POINTER(BlockDesc), i32, i32, pu32, pu32, i64, C.POINTER(i64)]),
+        "h3d_halo_expr": (i32, [i32, C.POINTER(BlockDesc), i32, i32, pu32, i64, C.POINTER(i64), pu32, pu32, i64,
+                                C.POINTER(i64)]),
         "h3d_residual_noalloc": (i32, [C.c_void_p, C.c_void_p, i32, i32, i32, pd, i32, pd, C.c_void_p]),
         "h3d_mg_set_wait_limit": (i32, [vp, i64]),
         "h3d_mg_wait_probe": (i32, [vp]),

@@ -3720,6 +3720,7 @@ cudaError_t launch_restrict_tile(int variant, bool var, bool zero_phi, const Blk
                                  const Tile* tiles, int ntiles, int zc, const T* phi, const T* rhs, T* rhs_c,
                                  const T* fx, const T* fy, const T* fz, const CUtensorMap* pmaps,
                                  const CUtensorMap* rmaps, int* err, cudaStream_t st) {
+  if (ntiles <= 0) return cudaSuccess;
   switch (variant) {
 #define X(v, tpr, cpx, tyc) \
     case v: return rtile_dispatch<T, tpr, cpx, tyc>(var, zero_phi, fine, coarse, tiles, ntiles, zc, phi, rhs, rhs_c, fx, fy, fz, st);
@@ -4267,5 +4268,167 @@ template cudaError_t launch_defect<double, double>(bool, const BlkLev*, RowTab, 
 template cudaError_t launch_defect<float, float>(bool, const BlkLev*, RowTab, const double*, const float*, double*,
                                                  const double*, float*, double, double, const double*, const double*,
                                                  const double*, double*, cudaStream_t);
+
+// ---------------------------------------------------------------------------
+// Local mesh refinement (LMR).
+//
+// Expression fill: the level's exchange sequence, resolved on the host into
+// nodes (exchangepp.for LMR branches: 8-cell averages :164-174, injection 2x
+// :176-189, the finer receiver's extrapolation :2115-2123, corner and edge
+// averages and trilinear values :447-458) evaluated here in the reference's
+// operation order.
+template <typename T>
+__device__ __forceinline__ T xref(uint32_t r, const T* __restrict__ cur, const T* __restrict__ old, bool zero_old,
+                                  const T* __restrict__ sc) {
+  const uint32_t i = r & 0x3fffffffu;
+  switch (r >> 30) {
+    case 0: return cur[i];
+    case 1: return sc[i];
+    case 2: return zero_old ? T(0) : old[i];
+    default: return T(0);
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_expr_nodes(const uint32_t* __restrict__ nodes, long long begin, long long end,
+                                                    const T* __restrict__ cur, const T* __restrict__ old,
+                                                    bool zero_old, T* __restrict__ sc) {
+  const long long k = begin + (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= end) return;
+  const uint32_t* w = nodes + 9 * k;
+  auto a = [&](int q) { return xref<T>(w[1 + q], cur, old, zero_old, sc); };
+  T v;
+  switch (w[0]) {
+    case 1: {  // 0.125 * (sum of eight), left to right
+      T s = a(0);
+#pragma unroll
+      for (int q = 1; q < 8; ++q) s = s + a(q);
+      v = s * T(0.125);
+      break;
+    }
+    case 2: v = T(2) * a(0); break;
+    case 3: v = ((a(0) + T(3) * a(1)) - a(2)) * T(0.25); break;  // (r + 3 f1 - f2) / 4
+    case 4: {  // (27, 9, 9, 3, 9, 3, 3, 1) / 64, left to right
+      T s = T(27) * a(0);
+      s = s + T(9) * a(1);
+      s = s + T(9) * a(2);
+      s = s + T(3) * a(3);
+      s = s + T(9) * a(4);
+      s = s + T(3) * a(5);
+      s = s + T(3) * a(6);
+      s = s + a(7);
+      v = s * T(1.0 / 64);
+      break;
+    }
+    default: v = a(0); break;
+  }
+  sc[k] = v;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_expr_write(const uint32_t* __restrict__ dst, const uint32_t* __restrict__ src,
+                                                    long long n, T* out, const T* cur, const T* __restrict__ sc) {
+  const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= n) return;
+  out[dst[e]] = xref<T>(src[e], cur, cur, true, sc);  // writes never read pre-fill values
+}
+
+template <typename T>
+cudaError_t launch_expr_fill(const uint32_t* nodes, const int64_t* depth_start, int ndepth, const uint32_t* dst,
+                             const uint32_t* src, int64_t nw, T* out, const T* cur, const T* old, bool zero_old,
+                             T* scratch, cudaStream_t st) {
+  for (int d = 0; d < ndepth; ++d) {
+    const long long b = depth_start[d], e = depth_start[d + 1];
+    if (e <= b) continue;
+    k_expr_nodes<T><<<(unsigned)((e - b + 255) / 256), 256, 0, st>>>(nodes, b, e, cur, old, zero_old, scratch);
+  }
+  if (nw > 0) k_expr_write<T><<<(unsigned)((nw + 255) / 256), 256, 0, st>>>(dst, src, nw, out, cur, scratch);
+  return cudaGetLastError();
+}
+template cudaError_t launch_expr_fill<double>(const uint32_t*, const int64_t*, int, const uint32_t*, const uint32_t*,
+                                              int64_t, double*, const double*, const double*, bool, double*,
+                                              cudaStream_t);
+template cudaError_t launch_expr_fill<float>(const uint32_t*, const int64_t*, int, const uint32_t*, const uint32_t*,
+                                             int64_t, float*, const float*, const float*, bool, float*,
+                                             cudaStream_t);
+
+// Blocks past their last level: restriction and correction between levels of
+// the same size.  Grid (cells / 256, listed blocks); a thread per cell.
+template <typename T, bool ZERO>
+__global__ void __launch_bounds__(256) k_restrict_same(const BlkLev* __restrict__ fine,
+                                                       const BlkLev* __restrict__ coarse, const int* __restrict__ blist,
+                                                       const T* __restrict__ phi, const T* __restrict__ rhs,
+                                                       T* __restrict__ rhs_c) {
+  const int b = blist[blockIdx.y];
+  const BlkLev F = fine[b];
+  const BlkLev Cc = coarse[b];
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= F.nx * F.ny * F.nz) return;
+  const int x = 1 + q % F.nx, y = 1 + (q / F.nx) % F.ny, z = 1 + q / (F.nx * F.ny);
+  const long long i = F.off + (long long)z * F.sxy + (long long)y * F.sx + x;
+  T r = rhs[i];
+  if (!ZERO) {
+    const Coef<T> c = cell_coef<T, false>(F, x, y, z, i, nullptr, nullptr, nullptr);
+    const T ap = coef_ap(c);
+    // resf = su - (aw pW + ae pE + as pS + an pN + ab pB + at pT + ap pP), mgsolver.for:706-713
+    r = r - (c.aw * phi[i - 1] + c.ae * phi[i + 1] + c.as * phi[i - F.sx] + c.an * phi[i + F.sx] +
+             c.ab * phi[i - F.sxy] + c.at * phi[i + F.sxy] + ap * phi[i]);
+  }
+  rhs_c[Cc.off + (long long)z * Cc.sxy + (long long)y * Cc.sx + x] = r;
+}
+
+template <typename T>
+cudaError_t launch_restrict_same(bool zero_phi, const BlkLev* fine, const BlkLev* coarse, const int* blist, int nbl,
+                                 int max_cells, const T* phi, const T* rhs, T* rhs_c, cudaStream_t st) {
+  if (nbl <= 0 || max_cells <= 0) return cudaSuccess;
+  dim3 g((unsigned)((max_cells + 255) / 256), (unsigned)nbl);
+  if (zero_phi) k_restrict_same<T, true><<<g, 256, 0, st>>>(fine, coarse, blist, phi, rhs, rhs_c);
+  else k_restrict_same<T, false><<<g, 256, 0, st>>>(fine, coarse, blist, phi, rhs, rhs_c);
+  return cudaGetLastError();
+}
+template cudaError_t launch_restrict_same<double>(bool, const BlkLev*, const BlkLev*, const int*, int, int,
+                                                  const double*, const double*, double*, cudaStream_t);
+template cudaError_t launch_restrict_same<float>(bool, const BlkLev*, const BlkLev*, const int*, int, int,
+                                                 const float*, const float*, float*, cudaStream_t);
+
+template <typename T, bool ZERO_OLD>
+__global__ void __launch_bounds__(256) k_prolong_same(const BlkLev* __restrict__ fine,
+                                                      const BlkLev* __restrict__ coarse, const int* __restrict__ blist,
+                                                      const T* __restrict__ phi_c, const T* __restrict__ old,
+                                                      T* __restrict__ out) {
+  const int b = blist[blockIdx.y];
+  const BlkLev F = fine[b];
+  const BlkLev Cc = coarse[b];
+  const int mx = F.nx + 2, my = F.ny + 2;
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= mx * my * (F.nz + 2)) return;
+  const int x = q % mx, y = (q / mx) % my, z = q / (mx * my);
+  // mgbound after the correction: a wall ghost takes its neighbour's corrected value
+  const int ph = F.phys;
+  int sx = x, sy = y, sz = z;
+  if (x == 0 && (ph & 1)) sx = 1;
+  if (x == F.nx + 1 && (ph & 2)) sx = F.nx;
+  if (y == 0 && (ph & 4)) sy = 1;
+  if (y == F.ny + 1 && (ph & 8)) sy = F.ny;
+  if (z == 0 && (ph & 16)) sz = 1;
+  if (z == F.nz + 1 && (ph & 32)) sz = F.nz;
+  const T o = ZERO_OLD ? T(0) : old[F.off + (long long)sz * F.sxy + (long long)sy * F.sx + sx];
+  out[F.off + (long long)z * F.sxy + (long long)y * F.sx + x] =
+      o + phi_c[Cc.off + (long long)sz * Cc.sxy + (long long)sy * Cc.sx + sx];
+}
+
+template <typename T>
+cudaError_t launch_prolong_same(bool zero_old, const BlkLev* fine, const BlkLev* coarse, const int* blist, int nbl,
+                                int max_cells, const T* phi_c, const T* old, T* out, cudaStream_t st) {
+  if (nbl <= 0 || max_cells <= 0) return cudaSuccess;
+  dim3 g((unsigned)((max_cells + 255) / 256), (unsigned)nbl);
+  if (zero_old) k_prolong_same<T, true><<<g, 256, 0, st>>>(fine, coarse, blist, phi_c, old, out);
+  else k_prolong_same<T, false><<<g, 256, 0, st>>>(fine, coarse, blist, phi_c, old, out);
+  return cudaGetLastError();
+}
+template cudaError_t launch_prolong_same<double>(bool, const BlkLev*, const BlkLev*, const int*, int, int,
+                                                 const double*, const double*, double*, cudaStream_t);
+template cudaError_t launch_prolong_same<float>(bool, const BlkLev*, const BlkLev*, const int*, int, int,
+                                                const float*, const float*, float*, cudaStream_t);
 
 }  // namespace h3d

@@ -287,4 +287,24 @@ cudaError_t launch_calmas(bool lsm, const BlkLev* bl, RowTab interior_rows, cons
 template <typename TE>
 cudaError_t launch_padd(const BlkLev* bl, RowTab all_rows, double* p, const TE* e, cudaStream_t st);
 
+// Local mesh refinement.  Expression fill of a level (see ExprTable): one
+// launch per node depth (depth_start: host array of ndepth + 1 offsets), then
+// the ghost writes out[dst[e]] = ref(src[e]).  cur: current values (may be
+// out), old: pre-fill values (zero_old: all zero), scratch: node values.
+template <typename T>
+cudaError_t launch_expr_fill(const uint32_t* nodes, const int64_t* depth_start, int ndepth, const uint32_t* dst,
+                             const uint32_t* src, int64_t nw, T* out, const T* cur, const T* old, bool zero_old,
+                             T* scratch, cudaStream_t st);
+// mgrestr for the listed blocks past their last level (glevel > ngrid,
+// mgsolver.for:724-737): the coarse rhs is the fine residual, cell for cell.
+template <typename T>
+cudaError_t launch_restrict_same(bool zero_phi, const BlkLev* fine, const BlkLev* coarse, const int* blist, int nbl,
+                                 int max_cells, const T* phi, const T* rhs, T* rhs_c, cudaStream_t st);
+// mgcorr for the listed blocks whose coarser level is the same size
+// (glevel >= ngrid, mgsolver.for:812-824): out = old + coarse on every cell,
+// with the following mgbound fused (ghosts of wall faces read their source).
+template <typename T>
+cudaError_t launch_prolong_same(bool zero_old, const BlkLev* fine, const BlkLev* coarse, const int* blist, int nbl,
+                                int max_cells, const T* phi_c, const T* old, T* out, cudaStream_t st);
+
 }  // namespace h3d

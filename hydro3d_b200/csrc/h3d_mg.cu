@@ -45,6 +45,16 @@ struct Halo {
   bool built = false;
 };
 
+// An expression fill on the device (see ExprTable).
+struct XFill {
+  uint32_t* d_nodes = nullptr;
+  uint32_t* d_dst = nullptr;
+  uint32_t* d_src = nullptr;
+  int64_t nw = 0, nnodes = 0;
+  std::vector<int64_t> ds;  // node ranges by depth (host)
+  bool built = false;
+};
+
 struct Level {
   LevelGeom geom;
   BlkLev* d_bl = nullptr;
@@ -98,6 +108,17 @@ struct Level {
   int nztiles = 0, zzc = 1;
   double* seq64 = nullptr;      // line-TDMA scratch a(s) of every cell (mg_itrsch 2)
   float* seq32 = nullptr;
+  // local mesh refinement
+  bool expr = false;            // the level's fills are expression tables (neighbours of different rdv)
+  XFill xs, xe;                 // sweep fill (mgbound + exchangepp), exchangepp alone (built on first use)
+  double* xscratch = nullptr;   // node values of the expression fills (FP64 or FP32)
+  int64_t xscratch_n = 0;
+  int* d_rsame = nullptr;       // blocks past their last level here (restriction into this level is a copy)
+  int nrsame = 0, rsame_cells = 0;
+  int* d_psame = nullptr;       // blocks whose next coarser level has this level's size (correction is an add)
+  int npsame = 0, psame_cells = 0;
+  int* d_prows = nullptr;       // prolongation rows of the other blocks (ghost rows included)
+  int nprows = 0;
   double sweep_bytes = 0;       // algorithmic bytes of one sweep (FP64 or FP32 by mode)
   double sweep_bytes_zero = 0;  // ... of a sweep from the zero iterate (the iterate is not read)
 };
@@ -149,6 +170,7 @@ struct h3d_mg {
   std::vector<size_t> stage_off;
   // fused coarse tail: levels tail_g..L in one single-CTA launch (tail_g = 0: none)
   int tail_g = 0;
+  bool lmr = false;  // blocks of different refinement ratio or level count (LMR = 2)
   TailLevel* d_tail_lv = nullptr;
   TailOp* d_tail_ops = nullptr;
   unsigned long long* d_tail_cells = nullptr;  // cell tables of all tail levels
@@ -239,6 +261,66 @@ int upload_halo(h3d_mg* h, Halo& H, const std::vector<uint32_t>& d, const std::v
   return H3D_OK;
 }
 
+// Builds and uploads the expression form of level g's fill of `kind`.
+int upload_xfill(h3d_mg* h, int g, int kind, XFill& X) {
+  ExprTable T;
+  std::string err;
+  const int rc = build_expr_table(h->blocks, g, kind, true, T, &err);
+  if (rc != H3D_OK) return fail(h, rc, err);
+  Level& V = h->lev[g];
+  X.nw = (int64_t)T.dst.size();
+  X.nnodes = (int64_t)T.nodes.size() / 9;
+  X.ds = T.depth_start;
+  if (!T.nodes.empty()) {
+    TRY(dalloc(h, &X.d_nodes, T.nodes.size()));
+    CU(cudaMemcpy(X.d_nodes, T.nodes.data(), T.nodes.size() * 4, cudaMemcpyHostToDevice));
+  }
+  if (X.nw > 0) {
+    TRY(dalloc(h, &X.d_dst, T.dst.size()));
+    TRY(dalloc(h, &X.d_src, T.src.size()));
+    CU(cudaMemcpy(X.d_dst, T.dst.data(), T.dst.size() * 4, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(X.d_src, T.src.data(), T.src.size() * 4, cudaMemcpyHostToDevice));
+  }
+  if (X.nnodes > V.xscratch_n) {
+    CU(cudaDeviceSynchronize());
+    dfree(V.xscratch);
+    V.xscratch = nullptr;
+    TRY(dalloc(h, &V.xscratch, (size_t)X.nnodes));
+    V.xscratch_n = X.nnodes;
+  }
+  X.built = true;
+  return H3D_OK;
+}
+
+// Runs an expression fill: out's ghosts from cur (current values) and old
+// (pre-fill values, zero when zero_old).
+template <typename T>
+cudaError_t run_xfill(const Level& V, const XFill& X, T* out, const T* cur, const T* old, bool zero_old,
+                      cudaStream_t st) {
+  return launch_expr_fill<T>(X.d_nodes, X.ds.data(), (int)X.ds.size() - 1, X.d_dst, X.d_src, X.nw, out, cur, old,
+                             zero_old, reinterpret_cast<T*>(V.xscratch), st);
+}
+
+// Uploads a list of block ids; *cells = the largest listed block's cell count
+// (interior, or with the ghost layer).
+int upload_block_list(h3d_mg* h, const LevelGeom& G, const std::vector<char>& sel, bool ghosts, int** d, int* n,
+                      int* cells) {
+  std::vector<int> ids;
+  long long mc = 0;
+  for (size_t b = 0; b < G.bl.size(); ++b)
+    if (sel[b]) {
+      ids.push_back((int)b);
+      const BlkLev& B = G.bl[b];
+      mc = std::max(mc, ghosts ? (long long)(B.nx + 2) * (B.ny + 2) * (B.nz + 2) : (long long)B.nx * B.ny * B.nz);
+    }
+  *n = (int)ids.size();
+  *cells = (int)mc;
+  if (ids.empty()) return H3D_OK;
+  TRY(dalloc(h, d, ids.size()));
+  CU(cudaMemcpy(*d, ids.data(), ids.size() * sizeof(int), cudaMemcpyHostToDevice));
+  return H3D_OK;
+}
+
 int build_cta_table(h3d_mg* h, const LevelGeom& G, bool interior, int** d_tab, int* ncta) {
   std::vector<int> start(G.bl.size() + 1, 0);
   for (size_t b = 0; b < G.bl.size(); ++b) {
@@ -311,11 +393,12 @@ int build_tiles(h3d_mg* h, Level& Lv, int variant, int zc) {
 }
 
 
-// Tiles of (TY rows x all x) x zc planes over every block of geometry G.
+// Restriction tiles of (TY rows x all x) x zc planes over every block of the
+// coarse geometry G (blocks past their last level restrict by a copy instead).
 std::vector<Tile> row_tiles(const LevelGeom& G, int ty, int zc) {
   std::vector<Tile> t;
   for (size_t b = 0; b < G.bl.size(); ++b)
-    for (int z0 = 1; z0 <= G.bl[b].nz; z0 += zc)
+    for (int z0 = 1; !G.clamped[b] && z0 <= G.bl[b].nz; z0 += zc)
       for (int y0 = 1; y0 <= G.bl[b].ny; y0 += ty) t.push_back(Tile{(int)b, 1, y0, z0});
   return t;
 }
@@ -414,6 +497,17 @@ const CUtensorMap* rhs_maps(const Level& V) {
 // FP32; the coarsest level (the coarse solve) stays FP64.
 bool f32_level(const h3d_mg* h, int g) { return h->mixed && !(g == h->L && h->L > 1); }
 
+// The level-1 pressure halo before an FP64 defect: exchange(4) + pbound
+// (newsolv_mg.for:51-52), i.e. the face ghosts of the sweep fill; with local
+// mesh refinement the sweep's expression fill, in place.
+int pressure_halo(h3d_mg* h) {
+  Level& V = h->lev[1];
+  double* p = h->p64[h->pc];
+  if (V.expr) CU(run_xfill<double>(V, V.xs, p, p, p, false, h->st));
+  else CU(launch_fill<double>(V.faces.d_dst, V.faces.d_src, V.faces.n, p, p, p, false, h->st));
+  return H3D_OK;
+}
+
 struct Exec {
   h3d_mg* h;
   std::vector<cudaEvent_t>* prof = nullptr;  // pre-created events for level-1 sweeps
@@ -443,6 +537,22 @@ struct Exec {
     return cudaEventRecord(e, h->st);
   }
 
+  // The fill after a sweep: the dst iterate's ghosts from its interior and
+  // the src iterate's ghosts (zero: src is the zero iterate).  Returns the
+  // number of kernels it launched.
+  template <typename T>
+  int sweep_fill(const Level& V, const Halo& H, T* dst, const T* src, bool zero, int64_t* nk) {
+    if (V.expr) {
+      CU(run_xfill<T>(V, V.xs, dst, dst, src, zero, h->st));
+      for (size_t d = 0; d + 1 < V.xs.ds.size(); ++d) *nk += V.xs.ds[d + 1] > V.xs.ds[d];
+      *nk += V.xs.nw > 0;
+    } else {
+      CU(launch_fill<T>(H.d_dst, H.d_src, H.n, dst, dst, src, zero, h->st));
+      *nk += H.n > 0;
+    }
+    return H3D_OK;
+  }
+
   int sweep(int g) {
     Level& V = L(g);
     cudaStream_t st = h->st;
@@ -465,7 +575,7 @@ struct Exec {
                                       V.fx32, V.fy32, V.fz32, st));
         TRY(chk("sequential sweep fp32", g));
         if (e1) CU(record(e1));
-        CU(launch_fill<float>(V.sweep.d_dst, V.sweep.d_src, V.sweep.n, dst, dst, src, V.zero32, st));
+        TRY(sweep_fill<float>(V, V.sweep, dst, src, V.zero32, &h->kernels));
         TRY(chk("fill fp32", g));
         V.cur32 = 1 - V.cur32;
         V.zero32 = false;
@@ -476,12 +586,12 @@ struct Exec {
                                        V.fx64, V.fy64, V.fz64, st));
         TRY(chk("sequential sweep fp64", g));
         if (e1) CU(record(e1));
-        CU(launch_fill<double>(V.sweep.d_dst, V.sweep.d_src, V.sweep.n, dst, dst, src, V.zero64, st));
+        TRY(sweep_fill<double>(V, V.sweep, dst, src, V.zero64, &h->kernels));
         TRY(chk("fill fp64", g));
         V.cur64 = 1 - V.cur64;
         V.zero64 = false;
       }
-      h->kernels += (V.sweep.n > 0) ? 2 : 1;
+      h->kernels += 1;
       return H3D_OK;
     }
     if (mixed_level(g) && V.zero32 && V.d_ztiles) {  // first sweep from a zero iterate: a stencil on rhs
@@ -492,11 +602,11 @@ struct Exec {
       TRY(chk("zero-source sweep fp32", g));
       if (e1) CU(record(e1));
       const Halo& fill = push ? V.sweep_push : V.sweep;
-      CU(launch_fill<float>(fill.d_dst, fill.d_src, fill.n, dst, dst, src, true, st));
+      TRY(sweep_fill<float>(V, fill, dst, src, true, &h->kernels));
       TRY(chk("fill fp32", g));
       V.cur32 = 1 - V.cur32;
       V.zero32 = false;
-      h->kernels += (fill.n > 0) ? 2 : 1;
+      h->kernels += 1;
       return H3D_OK;
     }
     if (mixed_level(g)) {
@@ -509,7 +619,7 @@ struct Exec {
       TRY(chk("sweep fp32", g));
       if (e1) CU(record(e1));
       const Halo& fill = push ? V.sweep_push : V.sweep;
-      CU(launch_fill<float>(fill.d_dst, fill.d_src, fill.n, dst, dst, src, V.zero32, st));
+      TRY(sweep_fill<float>(V, fill, dst, src, V.zero32, &h->kernels));
       TRY(chk("fill fp32", g));
       V.cur32 = 1 - V.cur32;
       V.zero32 = false;
@@ -521,12 +631,12 @@ struct Exec {
                              V.fx64, V.fy64, V.fz64, nullptr, st));
       TRY(chk("sweep fp64", g));
       if (e1) CU(record(e1));
-      CU(launch_fill<double>(V.sweep.d_dst, V.sweep.d_src, V.sweep.n, dst, dst, src, V.zero64, st));
+      TRY(sweep_fill<double>(V, V.sweep, dst, src, V.zero64, &h->kernels));
       TRY(chk("fill fp64", g));
       V.cur64 = 1 - V.cur64;
       V.zero64 = false;
     }
-    h->kernels += (V.sweep.n > 0) ? 2 : 1;
+    h->kernels += 1;
     return H3D_OK;
   }
 
@@ -579,6 +689,11 @@ struct Exec {
                                      restrict_maps(F, C.rvariant, F.cur32, false),
                                      restrict_maps(F, C.rvariant, 0, true), h->d_err, h->st));
       TRY(chk("restrict fp32", gc));
+      if (C.nrsame > 0) {
+        CU(launch_restrict_same<float>(F.zero32, F.d_bl, C.d_bl, C.d_rsame, C.nrsame, C.rsame_cells,
+                                       F.phi32[F.cur32], F.rhs32, C.rhs32, h->st));
+        h->kernels += 1;
+      }
       C.zero32 = true;
       if (!mixed_level(gc)) {  // coarsest level solved in FP64
         CU(launch_convert_f2d(C.rhs32, C.rhs64, C.geom.n_elems, h->st));
@@ -592,6 +707,11 @@ struct Exec {
                                       restrict_maps(F, C.rvariant, F.cur64, false),
                                       restrict_maps(F, C.rvariant, 0, true), h->d_err, h->st));
       TRY(chk("restrict fp64", gc));
+      if (C.nrsame > 0) {
+        CU(launch_restrict_same<double>(F.zero64, F.d_bl, C.d_bl, C.d_rsame, C.nrsame, C.rsame_cells,
+                                        F.phi64[F.cur64], F.rhs64, C.rhs64, h->st));
+        h->kernels += 1;
+      }
       C.zero64 = true;
     }
     h->kernels += 1;
@@ -602,7 +722,7 @@ struct Exec {
   int correct(int gf) {
     Level& F = L(gf);
     Level& C = L(gf + 1);
-    RowTab ct{F.d_rows_all, (int)F.geom.bl.size(), F.nrows_all};
+    RowTab ct{F.d_prows ? F.d_prows : F.d_rows_all, (int)F.geom.bl.size(), F.d_prows ? F.nprows : F.nrows_all};
     if (mixed_level(gf)) {
       const float* pc;
       if (mixed_level(gf + 1)) {
@@ -620,6 +740,11 @@ struct Exec {
                                      F.phi32[1 - F.cur32], h->st));
       else
         CU(launch_prolong<float>(F.zero32, F.d_bl, C.d_bl, ct, pc, F.phi32[F.cur32], F.phi32[1 - F.cur32], h->st));
+      if (F.npsame > 0) {
+        CU(launch_prolong_same<float>(F.zero32, F.d_bl, C.d_bl, F.d_psame, F.npsame, F.psame_cells, pc,
+                                      F.phi32[F.cur32], F.phi32[1 - F.cur32], h->st));
+        h->kernels += 1;
+      }
       TRY(chk("prolong fp32", gf));
       F.cur32 = 1 - F.cur32;
       F.zero32 = false;
@@ -631,6 +756,11 @@ struct Exec {
       else
         CU(launch_prolong<double>(F.zero64, F.d_bl, C.d_bl, ct, C.phi64[C.cur64], F.phi64[F.cur64],
                                   F.phi64[1 - F.cur64], h->st));
+      if (F.npsame > 0) {
+        CU(launch_prolong_same<double>(F.zero64, F.d_bl, C.d_bl, F.d_psame, F.npsame, F.psame_cells,
+                                       C.phi64[C.cur64], F.phi64[F.cur64], F.phi64[1 - F.cur64], h->st));
+        h->kernels += 1;
+      }
       TRY(chk("prolong fp64", gf));
       F.cur64 = 1 - F.cur64;
       F.zero64 = false;
@@ -799,6 +929,25 @@ struct Exec {
     if (h->proj) {
       TRY(proj_update());
       return vel_defect();
+    }
+    if (h->lmr) {
+      // p += e, then the pressure halo of p itself (exchange(4) + pbound,
+      // newsolv_mg.for:39-52): with refinement the ghosts are averages and
+      // extrapolations, so the ghosts of p + e are not those of p plus e's
+      RowTab ra{V.d_rows_all, (int)V.geom.bl.size(), V.nrows_all};
+      double* p = h->p64[h->pc];
+      if (h->mixed) {
+        if (V.zero32) TRY(materialize_zero32(1));
+        CU(launch_padd<float>(V.d_bl, ra, p, V.phi32[V.cur32], h->st));
+      } else {
+        if (V.zero64) TRY(materialize_zero64(1));
+        CU(launch_padd<double>(V.d_bl, ra, p, V.phi64[V.cur64], h->st));
+      }
+      TRY(chk("p update", 1));
+      TRY(pressure_halo(h));
+      TRY(chk("pressure halo", 1));
+      h->kernels += 2;
+      return defect(false);
     }
     return defect(true);
   }
@@ -1567,7 +1716,7 @@ void emit_tail_ops(const h3d_mg* h, int g0, int scratch, std::vector<TailOp>& op
 
 int build_tail(h3d_mg* h) {
   const int Lv = h->L;
-  if (h->var || h->desc.mg_itrsch != 3) return H3D_OK;  // the fused tail relaxes by red-black GS
+  if (h->var || h->lmr || h->desc.mg_itrsch != 3) return H3D_OK;  // the fused tail relaxes by red-black GS
   int g0 = Lv + 1;
   TailPlan plan;
   for (int g = Lv; g >= 2; --g) {
@@ -1728,7 +1877,9 @@ int build_tail(h3d_mg* h) {
 int build_cluster_tail(h3d_mg* h) {
   const int Lv = h->L;
   const int nb = (int)h->blocks.size();
-  if (h->var || nb > kClusterTailMaxBlocks || h->desc.mg_itrsch != 3) return H3D_OK;
+  // (the fused tails restrict and correct between levels of equal-resolution
+  // blocks only: none with local mesh refinement)
+  if (h->var || h->lmr || nb > kClusterTailMaxBlocks || h->desc.mg_itrsch != 3) return H3D_OK;
   auto al = [](int v) { return (v + 15) & ~15; };
   struct Lay { int npad, nint, s_phi32, s_rhs32, s_phi64, s_rhs64, s_cells, s_fill; };
   std::vector<Lay> lay;
@@ -1929,7 +2080,9 @@ int h3d_mg_destroy(h3d_mg* h) {
     void* ps[] = {V.d_bl, V.d_cta_all, V.d_cta_int, V.d_rows_all, V.d_rows_int, V.d_tiles, V.phi64[0], V.phi64[1], V.rhs64, V.phi32[0],
                   V.phi32[1], V.rhs32, V.fx64, V.fy64, V.fz64, V.fx32, V.fy32, V.fz32, V.dens,
                   V.sweep.d_dst, V.sweep.d_src, V.faces.d_dst, V.faces.d_src, V.exch.d_dst, V.exch.d_src,
-                  V.bound.d_dst, V.bound.d_src, V.sweep_push.d_dst, V.sweep_push.d_src, V.d_push, V.d_maps, V.d_rmaps, V.d_rtiles, V.d_ptiles, V.d_qtiles, V.d_dtiles, V.d_cstart, V.d_dstart, V.d_pstart, V.seq64, V.seq32, V.d_ztiles, V.lfill.d_dst, V.lfill.d_src, V.d_lfstart};
+                  V.bound.d_dst, V.bound.d_src, V.sweep_push.d_dst, V.sweep_push.d_src, V.d_push, V.d_maps, V.d_rmaps, V.d_rtiles, V.d_ptiles, V.d_qtiles, V.d_dtiles, V.d_cstart, V.d_dstart, V.d_pstart, V.seq64, V.seq32, V.d_ztiles, V.lfill.d_dst, V.lfill.d_src, V.d_lfstart,
+                  V.xs.d_nodes, V.xs.d_dst, V.xs.d_src, V.xe.d_nodes, V.xe.d_dst, V.xe.d_src, V.xscratch, V.d_rsame,
+                  V.d_psame, V.d_prows};
     for (void* p : ps) dfree(p);
   }
   dfree(h->p64[0]);
@@ -1976,10 +2129,27 @@ int h3d_mg_create(h3d_mg** out, const h3d_mg_desc* desc) {
   if (D.precision != H3D_PREC_FP64 && D.precision != H3D_PREC_MIXED)
     return fail(nullptr, H3D_ERR_BAD_CONFIG, "unknown precision");
   if (D.coarse_op < 0 || D.coarse_op > 1) return fail(nullptr, H3D_ERR_BAD_CONFIG, "coarse_op must be 0 or 1");
+  // local mesh refinement (localparameters.for:28-59): ngrd_gl = ngrid_input +
+  // log2(max rdiv), a block of ratio rdiv has ngrid_input + log2(rdiv) levels
+  int maxlog = 0;
+  bool lmr = false;
+  for (int b = 0; b < D.nblocks; ++b) {
+    const int r = D.blocks[b].rdiv;
+    int lg = 0;
+    while ((1 << lg) < r) ++lg;
+    if (r < 1 || (1 << lg) != r) return fail(nullptr, H3D_ERR_BAD_CONFIG, "rdiv must be a power of 2");
+    maxlog = std::max(maxlog, lg);
+  }
+  const int ngrid_input = D.ngrd_gl - maxlog;
+  if (ngrid_input < 1) return fail(nullptr, H3D_ERR_BAD_CONFIG, "ngrd_gl smaller than log2(max rdiv) + 1");
   for (int b = 0; b < D.nblocks; ++b) {
     const h3d_block_desc& d = D.blocks[b];
-    if (d.ngrid != D.ngrd_gl) return fail(nullptr, H3D_ERR_BAD_CONFIG, "every block needs ngrid == ngrd_gl");
-    if (d.rdiv != 1) return fail(nullptr, H3D_ERR_BAD_CONFIG, "local mesh refinement (rdiv > 1) is not supported");
+    int lg = 0;
+    while ((1 << lg) < d.rdiv) ++lg;
+    if (d.ngrid != ngrid_input + lg)
+      return fail(nullptr, H3D_ERR_BAD_CONFIG,
+                  "every block needs ngrid == ngrd_gl - log2(max rdiv) + log2(rdiv) (ngrd_gl without refinement)");
+    if (d.ngrid != D.ngrd_gl) lmr = true;
     int pow2 = 1 << (d.ngrid - 1);
     for (int a = 0; a < 3; ++a)
       if (d.n[a] <= 0 || d.n[a] % pow2 != 0)  // localparameters.for:204-209
@@ -1988,7 +2158,23 @@ int h3d_mg_create(h3d_mg** out, const h3d_mg_desc* desc) {
       if (d.nb_face[f] >= D.nblocks || d.nb_periodic[f] >= D.nblocks)
         return fail(nullptr, H3D_ERR_BAD_CONFIG, "neighbour id out of range");
     }
+    for (int e = 0; e < 12; ++e)
+      if (d.nb_edge[e] >= D.nblocks) return fail(nullptr, H3D_ERR_BAD_CONFIG, "neighbour id out of range");
+    for (int c = 0; c < 8; ++c)
+      if (d.nb_corner[c] >= D.nblocks) return fail(nullptr, H3D_ERR_BAD_CONFIG, "neighbour id out of range");
   }
+  {
+    std::vector<h3d_block_desc> bl(D.blocks, D.blocks + D.nblocks);
+    for (int g = 1; g <= D.ngrd_gl && !lmr; ++g) lmr = level_is_lmr(bl, g);
+    for (int b = 0; b < D.nblocks; ++b)
+      for (int f = 0; f < 6; ++f) {
+        const int t = D.blocks[b].nb_periodic[f];
+        if (t >= 0 && D.blocks[t].rdiv != D.blocks[b].rdiv)  // exchbc_mgpp copies equal planes only
+          return fail(nullptr, H3D_ERR_BAD_CONFIG, "periodic partners need equal rdiv");
+      }
+  }
+  if (lmr && D.var_coef)
+    return fail(nullptr, H3D_ERR_BAD_CONFIG, "local mesh refinement with L_LSM coefficients is not supported");
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= D.device || D.device < 0)
     return fail(nullptr, H3D_ERR_NO_DEVICE, "no CUDA device");
@@ -2011,6 +2197,7 @@ int h3d_mg_create(h3d_mg** out, const h3d_mg_desc* desc) {
   }
   h->mixed = D.precision == H3D_PREC_MIXED;
   h->var = D.var_coef != 0;
+  h->lmr = lmr;
   int rc = H3D_OK;
   auto bail = [&](int r) {
     g_create_error = h->last_error;
@@ -2061,12 +2248,37 @@ int h3d_mg_create(h3d_mg** out, const h3d_mg_desc* desc) {
     }
     std::vector<uint32_t> d, s;
     std::string err;
-    if ((rc = build_halo_table(h->blocks, g, kHaloSweep, true, d, s, &err)) != H3D_OK) return bail(fail(h, rc, err));
-    if ((rc = upload_halo(h, V.sweep, d, s)) != H3D_OK) return bail(rc);
-    if (f32_level(h, g) && !h->var && (rc = build_push(h, V, d, s)) != H3D_OK) return bail(rc);
+    V.expr = h->lmr && level_is_lmr(h->blocks, g);
+    if (V.expr) {  // neighbours of different rdv: the fill has arithmetic
+      if ((rc = upload_xfill(h, g, kHaloSweep, V.xs)) != H3D_OK) return bail(rc);
+    } else {
+      if ((rc = build_halo_table(h->blocks, g, kHaloSweep, true, d, s, &err)) != H3D_OK)
+        return bail(fail(h, rc, err));
+      if ((rc = upload_halo(h, V.sweep, d, s)) != H3D_OK) return bail(rc);
+    }
+    if (!V.expr && f32_level(h, g) && !h->var && (rc = build_push(h, V, d, s)) != H3D_OK) return bail(rc);
+    if (h->lmr) {  // blocks past their last level restrict by a copy and correct by an add
+      if (g >= 2 && (rc = upload_block_list(h, V.geom, V.geom.clamped, false, &V.d_rsame, &V.nrsame,
+                                            &V.rsame_cells)) != H3D_OK)
+        return bail(rc);
+      if (g < h->L) {
+        if ((rc = upload_block_list(h, V.geom, V.geom.same_next, true, &V.d_psame, &V.npsame, &V.psame_cells)) !=
+            H3D_OK)
+          return bail(rc);
+        std::vector<int> start(V.geom.bl.size() + 1, 0);
+        for (size_t b = 0; b < V.geom.bl.size(); ++b)
+          start[b + 1] = start[b] + (V.geom.same_next[b] ? 0 : (V.geom.bl[b].ny + 2) * (V.geom.bl[b].nz + 2));
+        V.nprows = start.back();
+        if ((rc = dalloc(h, &V.d_prows, start.size())) != H3D_OK) return bail(rc);
+        if (cudaMemcpy(V.d_prows, start.data(), start.size() * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess)
+          return bail(fail(h, H3D_ERR_CUDA, "prolongation rows"));
+      }
+    }
     // small levels relax in one fused launch when their fill reads interior cells only;
-    // slightly larger ones can still join the fused coarse tail
-    if (g > 1 && V.geom.n_interior <= kTailLevelCells && V.geom.bl.size() <= (size_t)kSmallLevelBlocks) {
+    // slightly larger ones can still join the fused coarse tail (which has no
+    // level-count clamp: not with local mesh refinement)
+    if (!V.expr && g > 1 && V.geom.n_interior <= kTailLevelCells &&
+        V.geom.bl.size() <= (size_t)kSmallLevelBlocks) {
       bool old = false;
       for (uint32_t v : s) old = old || (v & kOldFlag);
       if (!old) {
@@ -2075,13 +2287,13 @@ int h3d_mg_create(h3d_mg** out, const h3d_mg_desc* desc) {
         if ((rc = dalloc(h, &V.d_cstart, cs.size())) != H3D_OK) return bail(rc);
         if (cudaMemcpy(V.d_cstart, cs.data(), cs.size() * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess)
           return bail(fail(h, H3D_ERR_CUDA, "small-level table"));
-        V.tailable = true;
+        V.tailable = !h->lmr;
         V.small = V.geom.n_interior <= kSmallLevelCells;
       }
     }
     // levels whose fill stays inside every block and whose blocks are small
     // enough for one CTA each relax a whole visit in one launch
-    if (g > 1 && !V.small) {
+    if (!V.expr && g > 1 && !V.small) {
       int64_t maxc = 0;
       std::vector<int> owner(V.geom.bl.size());
       for (const auto& B : V.geom.bl) maxc = std::max<int64_t>(maxc, (int64_t)B.nx * B.ny * B.nz);
@@ -2113,7 +2325,7 @@ int h3d_mg_create(h3d_mg** out, const h3d_mg_desc* desc) {
         V.blocal = true;
       }
     }
-    if (g == 1) {
+    if (g == 1 && !V.expr) {  // (with refinement the pressure halo is the sweep's expression fill)
       if ((rc = build_halo_table(h->blocks, g, kHaloFaces, true, d, s, &err)) != H3D_OK) return bail(fail(h, rc, err));
       if ((rc = upload_halo(h, V.faces, d, s)) != H3D_OK) return bail(rc);
     }
@@ -2127,9 +2339,11 @@ int h3d_mg_create(h3d_mg** out, const h3d_mg_desc* desc) {
       for (size_t b = 0; b < V.geom.bl.size(); ++b) {
         const BlkLev& B = V.geom.bl[b];
         const bool even = B.ny % 2 == 0 && B.nz % 2 == 0;
-        V.pvec32 = V.pvec32 && even && B.nx % 4 == 0;
-        V.pvec64 = V.pvec64 && even && B.nx % 2 == 0;
-        for (int z = 0; z <= B.nz; z += 2) qt.push_back(Tile{(int)b, 0, 0, z});
+        if (!V.geom.same_next[b]) {  // (blocks whose coarser level is the same size correct by an add)
+          V.pvec32 = V.pvec32 && even && B.nx % 4 == 0;
+          V.pvec64 = V.pvec64 && even && B.nx % 2 == 0;
+          for (int z = 0; z <= B.nz; z += 2) qt.push_back(Tile{(int)b, 0, 0, z});
+        }
         if (g == 1)
           for (int z = 0; z <= B.nz + 1; ++z)
             for (int y0 = 0; y0 <= B.ny + 1; y0 += kProlongRows) pt.push_back(Tile{(int)b, 0, y0, z});
@@ -2339,9 +2553,7 @@ int h3d_mg_residual(h3d_mg* h, double* rr, double* bb, double* rinf) {
   if (!h) return H3D_ERR_ARG;
   CU(cudaSetDevice(h->device));
   TRY(ensure_coeffs(h));
-  Level& V = h->lev[1];
-  CU(launch_fill<double>(V.faces.d_dst, V.faces.d_src, V.faces.n, h->p64[h->pc], h->p64[h->pc], h->p64[h->pc],
-                         false, h->st));
+  TRY(pressure_halo(h));
   Exec ex{h};
   double save = h->mean_b;
   h->mean_b = 0.0;
@@ -2377,13 +2589,12 @@ int h3d_mg_solve_resident(h3d_mg* h, const h3d_solve_opts* opts, h3d_solve_info*
   CU(cudaEventRecord(t0, h->st));
   Level& V = h->lev[1];
   // pressure halo (exchange(4) + pbound, newsolv_mg.for:51-52)
-  CU(launch_fill<double>(V.faces.d_dst, V.faces.d_src, V.faces.n, h->p64[h->pc], h->p64[h->pc], h->p64[h->pc],
-                         false, h->st));
+  TRY(pressure_halo(h));
   h->kernels += 1;
   Exec ex{h};
   TRY(ex.chk("pressure halo", 1));
   h->mean_b = 0.0;
-  if (h->mixed && is_all_neumann(h)) {
+  if (h->mixed && is_all_neumann(h) && !h->lmr) {  // (with refinement the operator's left null vector is not constant)
     // FP64 null-space handling: the compatible part of b has zero mean; the
     // FP32 cycles see the defect with the mean of b removed.
     RowTab rt{V.d_rows_int, (int)V.geom.bl.size(), V.nrows_int};
@@ -2545,6 +2756,8 @@ static int ensure_face_table(h3d_mg* h) {
 }
 
 static int ensure_velocity(h3d_mg* h) {
+  if (h->lmr)
+    return fail(h, H3D_ERR_BAD_CONFIG, "the projection loop with local mesh refinement is not supported");
   if (h->vel[0]) return H3D_OK;
   const size_t n = (size_t)h->lev[1].geom.n_elems;
   for (int c = 0; c < 3; ++c) {
@@ -2564,6 +2777,7 @@ static double* velocity_field(h3d_mg* h, int field) {
 // ---------------------------------------------------------------- SIP
 static int ensure_sip(h3d_mg* h) {
   if (h->var) return fail(h, H3D_ERR_BAD_CONFIG, "SIP: constant coefficients only (press.for:407-438)");
+  if (h->lmr) return fail(h, H3D_ERR_BAD_CONFIG, "SIP with local mesh refinement is not supported");
   if ((int)h->blocks.size() > h->npartials) return fail(h, H3D_ERR_BAD_CONFIG, "SIP: too many blocks");
   if (h->sip_pp) return H3D_OK;
   TRY(ensure_face_table(h));
@@ -2732,6 +2946,7 @@ int h3d_mg_calmas(h3d_mg* h, double dt, double* rmax, double* su2) {
 
 int h3d_mg_pbound(h3d_mg* h) {
   if (!h) return H3D_ERR_ARG;
+  if (h->lmr) return fail(h, H3D_ERR_BAD_CONFIG, "pbound with local mesh refinement is not supported");
   CU(cudaSetDevice(h->device));
   Level& V = h->lev[1];
   double* p = h->p64[h->pc];
@@ -2960,6 +3175,28 @@ int h3d_mg_mgcorr(h3d_mg* h, int32_t g) {
 static int apply_table_hook(h3d_mg* h, int g, int kind) {
   CU(cudaSetDevice(h->device));
   Level& V = h->lev[g];
+  if (V.expr && kind == kHaloExchange) {  // exchangepp between blocks of different rdv
+    if (!V.xe.built) TRY(upload_xfill(h, g, kHaloExchange, V.xe));
+    Exec ex{h};
+    const size_t n = (size_t)V.geom.n_elems;
+    if (f32_level(h, g)) {
+      if (V.zero32) TRY(ex.materialize_zero32(g));
+      float* cur = V.phi32[V.cur32];
+      float* nxt = V.phi32[1 - V.cur32];
+      CU(cudaMemcpyAsync(nxt, cur, n * 4, cudaMemcpyDeviceToDevice, h->st));
+      CU(run_xfill<float>(V, V.xe, nxt, cur, cur, false, h->st));
+      V.cur32 = 1 - V.cur32;
+    } else {
+      if (V.zero64) TRY(ex.materialize_zero64(g));
+      double* cur = V.phi64[V.cur64];
+      double* nxt = V.phi64[1 - V.cur64];
+      CU(cudaMemcpyAsync(nxt, cur, n * 8, cudaMemcpyDeviceToDevice, h->st));
+      CU(run_xfill<double>(V, V.xe, nxt, cur, cur, false, h->st));
+      V.cur64 = 1 - V.cur64;
+    }
+    CU(cudaStreamSynchronize(h->st));
+    return H3D_OK;
+  }
   Halo* H = kind == kHaloExchange ? &V.exch : &V.bound;
   if (!H->built) {
     std::vector<uint32_t> d, s;

@@ -321,6 +321,24 @@ class MultigridSolver:
         self._check(self.L.h3d_mg_vcycle(self._h), "h3d_mg_vcycle")
 
 
+def halo_expr(blocks: Sequence, g: int, kind: int):
+    """Expression form of level g's fill (host-only; see h3d_halo_expr):
+    returns nodes (n, 9) uint32, dst, src."""
+    L = _lib.lib()
+    arr = (_lib.BlockDesc * len(blocks))(*blocks)
+    n = C.c_int64()
+    nn = C.c_int64()
+    check(L.h3d_halo_expr(len(blocks), arr, g, kind, None, 0, C.byref(nn), None, None, 0, C.byref(n)), None,
+          "h3d_halo_expr")
+    nodes = np.zeros((nn.value, 9), dtype=np.uint32)
+    dst = np.zeros(n.value, dtype=np.uint32)
+    src = np.zeros(n.value, dtype=np.uint32)
+    pu = C.POINTER(C.c_uint32)
+    check(L.h3d_halo_expr(len(blocks), arr, g, kind, nodes.ctypes.data_as(pu), nn.value, C.byref(nn),
+                          dst.ctypes.data_as(pu), src.ctypes.data_as(pu), n.value, C.byref(n)), None, "h3d_halo_expr")
+    return nodes, dst, src
+
+
 def halo_table(blocks: Sequence, g: int, kind: int):
     """Ghost gather table of level g (host-only; see h3d_halo_table)."""
     L = _lib.lib()

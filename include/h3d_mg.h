@@ -50,7 +50,9 @@ typedef struct h3d_block_desc {
   int32_t nb_edge[12];    /* edgprev1..6, edgnext1..6 */
   int32_t nb_periodic[6]; /* per_ip per_in per_jp per_jn per_kp per_kn */
   int32_t bc[6];          /* bc_west bc_east bc_south bc_north bc_bottom bc_top; 5 = periodic */
-  int32_t rdiv;           /* local mesh refinement ratio; only 1 is supported */
+  int32_t rdiv;           /* local mesh refinement ratio rdiv (a power of 2, LMR = 2;
+                             localparameters.for:24-59): n and h are the refined block's,
+                             ngrid = ngrid_input + log2(rdiv) */
   int32_t origin[3];      /* global index of the first interior cell (informational) */
 } h3d_block_desc;
 
@@ -271,6 +273,20 @@ int h3d_topology(int32_t nblocks, const int32_t* ext, const int32_t* bc,
 int h3d_halo_table(int32_t nblocks, const h3d_block_desc* blocks, int32_t g,
                    int32_t kind, uint32_t* dst, uint32_t* src, int64_t cap,
                    int64_t* n);
+/* Expression form of the same fill (kinds 0, 1, 2), which levels with local
+ * mesh refinement use: exchangepp between blocks of different rdv averages,
+ * injects, extrapolates and interpolates (exchangepp.for:164-189, 447-458,
+ * 2115-2123).  A reference r is, by bits 31..30: 00 the current value of cell
+ * r, 10 the pre-fill value of cell r & 0x3fffffff, 01 node r & 0x3fffffff,
+ * 11 zero (a receive-buffer entry this exchange never wrote).  Node k is
+ * nodes[9k..9k+8] = op, operands: 0 copy a0; 1 (a0+...+a7)*0.125; 2 2*a0;
+ * 3 ((a0 + 3*a1) - a2)/4; 4 (27a0+9a1+9a2+3a3+9a4+3a5+3a6+1a7)/64, sums left
+ * to right.  Nodes only read nodes of lower index.  Write e: dst[e] <- src[e]
+ * (a current cell, a node or zero).  nodes == NULL or dst == NULL skips that
+ * output; *nnodes and *n are always returned. */
+int h3d_halo_expr(int32_t nblocks, const h3d_block_desc* blocks, int32_t g,
+                  int32_t kind, uint32_t* nodes, int64_t node_cap, int64_t* nnodes,
+                  uint32_t* dst, uint32_t* src, int64_t cap, int64_t* n);
 
 /* Residual norms of one block without allocating device memory.  For hosts
  * that cannot call cudaMalloc: code running under a memory pool whose budget

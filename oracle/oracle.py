@@ -156,7 +156,7 @@ class Oracle:
     # shapes --------------------------------------------------------------
     def dims(self, g, ib):
         n = self.descs[ib].n
-        s = 2 ** (g - 1)
+        s = 2 ** (min(g, self.descs[ib].ngrid) - 1)  # level clamp, mgsolver.for:392-400
         return (n[2] // s, n[1] // s, n[0] // s)
 
     # reference routines -------------------------------------------------

@@ -74,3 +74,61 @@ def to_host(blocks, canon):
         h[p - 1:p + d.n[2] + 1, p - 1:p + d.n[1] + 1, p - 1:p + d.n[0] + 1] = a
         res.append(h)
     return res
+
+
+def apply_expr(nodes, dst, src, flat):
+    """Applies an expression fill (h3d_halo_expr) to the concatenated
+    canonical arrays `flat` in place, in FP64 with the operation order the
+    table states.  Pre-fill values are those of `flat` on entry."""
+    flat = np.asarray(flat)
+    old = flat.copy()
+    vals = np.zeros(len(nodes))
+
+    def ref(r):
+        r = np.asarray(r, dtype=np.uint32)
+        tag = r >> np.uint32(30)
+        idx = (r & np.uint32(0x3FFFFFFF)).astype(np.int64)
+        out = np.zeros(r.shape)
+        m = tag == 0
+        out[m] = flat[idx[m]]
+        m = tag == 1
+        out[m] = vals[idx[m]]
+        m = tag == 2
+        out[m] = old[idx[m]]
+        return out
+
+    if len(nodes):
+        op = nodes[:, 0]
+        # operands name lower-index nodes only: evaluate until nothing changes
+        # (one pass per depth)
+        depth = np.zeros(len(nodes), dtype=np.int64)
+        for k in range(len(nodes)):
+            for q in range(1, 9):
+                r = int(nodes[k, q])
+                if r >> 30 == 1:
+                    depth[k] = max(depth[k], depth[r & 0x3FFFFFFF] + 1)
+        for d in range(int(depth.max()) + 1):
+            sel = np.nonzero(depth == d)[0]
+            a = [ref(nodes[sel, q]) for q in range(1, 9)]
+            o = op[sel]
+            v = np.zeros(len(sel))
+            m = o == 0
+            v[m] = a[0][m]
+            m = o == 1
+            s = a[0][m]
+            for q in range(1, 8):
+                s = s + a[q][m]
+            v[m] = s * 0.125
+            m = o == 2
+            v[m] = 2.0 * a[0][m]
+            m = o == 3
+            v[m] = ((a[0][m] + 3.0 * a[1][m]) - a[2][m]) / 4.0
+            m = o == 4
+            w = (27.0, 9.0, 9.0, 3.0, 9.0, 3.0, 3.0, 1.0)
+            s = w[0] * a[0][m]
+            for q in range(1, 8):
+                s = s + w[q] * a[q][m]
+            v[m] = s / 64.0
+            vals[sel] = v
+    flat[np.asarray(dst, dtype=np.int64)] = ref(src)
+    return flat
