@@ -40,7 +40,7 @@ TOL = 1e-8
 # steps, 9.3 ms; 4 -> 3 steps, 9.0 ms, all 12 V-cycles and the same 1.5e-9
 # error; on configurations 2 and 4, 4 overshoots the tolerance by a cycle or
 # two, 2 does not).
-INNER = {1: 2, 2: 2, 3: 4, 4: 2, 5: 2}
+INNER = {1: 2, 2: 2, 3: 4, 4: 2, 5: 2, 6: 2}
 # Sweeps of the FP64 coarsest level in the mixed solver: enough to converge
 # that level (on the configuration-3 hierarchy 16 leave 14 V-cycles, 32 and 64
 # both 12), so the V-cycle contracts every mode at the rate of its finer
@@ -57,6 +57,8 @@ WORKLOADS = {
     3: "config3: 512x256x256 (33.5M cells) as 4x2x2 blocks of 128^3, all-Neumann, k^-5/3 spectral rhs, 7 levels",
     4: "config4: 27 independent all-Neumann blocks, axes from {32,48,64,96,128}, 4 levels",
     5: "config5: 256^3 two-phase 1000:1 density (L_LSM coefficients), 8 levels",
+    6: "config6 (local mesh refinement): 4x2x2 blocks of 64^3 at h=1/128, the 8 blocks of x index 1-2 refined "
+       "to 128^3 at h=1/256 (18.9M cells), walls, 7 levels, rhs = A p of a seeded smooth pressure",
 }
 
 
@@ -151,14 +153,19 @@ def oracle_resolve(ext, bc, h, ngrid):
     return O.topology(ext, bc, h, ngrid)
 
 
-def make_problem(cfg, resolve=None, prev_solve=None):
+def make_problem(cfg, resolve=None, prev_solve=None, residual_of=None):
     """The workload of configuration `cfg`.  Configuration 2 starts from the
     converged pressure of its independent previous-seed problem:
     `prev_solve(problem)` solves that problem to 1e-8 (untimed set-up) and
-    returns its block host fields."""
+    returns its block host fields.  Configuration 6's right-hand side is
+    A p_exact by the arm's own operator: `residual_of(problem)` returns the
+    function synth.manufacture calls."""
     from hydro3d_b200 import synth
     if cfg != 2:
-        return synth.CONFIGS[cfg](resolve=resolve)
+        prob = synth.CONFIGS[cfg](resolve=resolve)
+        if prob.b is None:
+            synth.manufacture(prob, residual_of(prob))
+        return prob
     prev = synth.config2(seed=1017, resolve=resolve)
     fields = prev_solve(prev)
     return synth.config2(p0=synth.gather(fields, prev.blocks), resolve=resolve)
@@ -168,6 +175,37 @@ def stop_rule(prob):
     """Independent blocks (configuration 4) are each solved to the tolerance:
     the per-block rule; otherwise the global relative residual."""
     return 2 if prob.name == "config4" else 0
+
+
+def gpu_residual_of(prob):
+    """b - A p with b = 0 on the GPU (the FP64 defect into the level-1 rhs)."""
+    def residual(pex):
+        from hydro3d_b200 import MultigridSolver, host_field
+        s = MultigridSolver(prob.blocks, prob.ngrid, device=int(os.environ.get("LOCAL_RANK", 0)))
+        s.coeff()
+        s.zero_field("b")
+        for ib in range(len(prob.blocks)):
+            s.upload("p", ib, pex[ib])
+        s.residual()
+        out = [s.get_level(1, "rhs", ib) for ib in range(len(prob.blocks))]
+        s.close()
+        return out
+    return residual
+
+
+def oracle_residual_of(threads):
+    """b - A p with b = 0 by the oracle (its level-1 exchangepp ghost fill)."""
+    def make(prob):
+        def residual(pex):
+            from hydro3d_b200 import with_ghost
+            o = OracleSolver(prob, threads, need_b=False)
+            p = [np.ascontiguousarray(with_ghost(x, d)) for x, d in zip(pex, prob.blocks)]
+            zeros = [np.zeros((d.n[2], d.n[1], d.n[0])) for d in prob.blocks]
+            r, _, _, _ = o.orc.residual(p, zeros)
+            o.close()
+            return r
+        return residual
+    return make
 
 
 def gpu_prev_solve(prob):
@@ -187,7 +225,7 @@ class OracleSolver:
     """The oracle (C restatement of the reference multigrid, OpenMP over the
     planes of each block) set up on one workload."""
 
-    def __init__(self, prob, threads):
+    def __init__(self, prob, threads, need_b=True):
         from oracle import oracle as O
         import ctypes as C
         from hydro3d_b200 import interior, with_ghost
@@ -198,6 +236,8 @@ class OracleSolver:
             for ib, (d, x) in enumerate(zip(prob.blocks, prob.dens)):
                 self.orc.set_density(ib, np.ascontiguousarray(interior(x, d)))
         self.orc.coeff()
+        if not need_b:
+            return
         self.b = [np.ascontiguousarray(interior(x, d)) for x, d in zip(prob.b, prob.blocks)]
         self.p0 = [np.ascontiguousarray(with_ghost(x, d)) for x, d in zip(prob.p0, prob.blocks)]
 
@@ -313,7 +353,8 @@ def run_reference(args):
     threads = os.cpu_count() or 1
     from oracle import oracle as O
     O.lib()
-    prob = make_problem(args.config, resolve=oracle_resolve, prev_solve=oracle_prev_solve(threads))
+    prob = make_problem(args.config, resolve=oracle_resolve, prev_solve=oracle_prev_solve(threads),
+                        residual_of=oracle_residual_of(threads))
     o = OracleSolver(prob, threads)
     for _ in range(args.warmup):
         o.solve(maxcy=1, tol=0.0)
@@ -353,7 +394,7 @@ def mcell_updates(prob, cycles):
     per = 0
     for d in prob.blocks:
         for g in range(1, prob.ngrid + 1):
-            s = 2 ** (g - 1)
+            s = 2 ** (min(g, d.ngrid) - 1)  # level clamp of a block past its last level
             per += (d.n[0] // s) * (d.n[1] // s) * (d.n[2] // s) * 3
     return per * cycles
 
@@ -387,7 +428,7 @@ def main():
     import hydro3d_b200  # noqa: F401  (loads libh3dmg.so; raises if missing)
     os.environ.setdefault("CUDA_DEVICE_ORDER", "PCI_BUS_ID")
     device = local
-    prob = make_problem(args.config, prev_solve=gpu_prev_solve)
+    prob = make_problem(args.config, prev_solve=gpu_prev_solve, residual_of=gpu_residual_of)
     peak, peak_kind = load_peaks()
     if args.ncu_region:
         import torch

@@ -1368,7 +1368,7 @@ __global__ void __launch_bounds__(256) k_defect(const BlkLev* __restrict__ bls, 
         rhs_out[i] = (TR)(r - mean_b);
         rr += r * r;
         bb += bv * bv;
-        rm = fmax(rm, fabs(r) * rscale);
+        rm = fmax(rm, fabs(r) * (rscale < 0.0 ? B.dv : rscale));
         rs += r;
       }
     }
@@ -3135,6 +3135,7 @@ __global__ void __launch_bounds__(256) k_defect_vec(const BlkLev* __restrict__ b
   double rr = 0, bb = 0, rm = 0, rs = 0;
   const Tile t = tiles[blockIdx.x];
   const BlkLev B = bls[t.b];
+  const double rsc = rscale < 0.0 ? B.dv : rscale;  // rmax measure: |r| times the block's cell volume
   const int z = t.z0;
   for (int y = t.y0 + w; y <= min(t.y0 + kProlongRows - 1, B.ny + 1); y += 8) {
     const bool row_in = y >= 1 && y <= B.ny && z >= 1 && z <= B.nz;
@@ -3177,8 +3178,8 @@ __global__ void __launch_bounds__(256) k_defect_vec(const BlkLev* __restrict__ b
       rr += r1 * r1;
       bb += bv.x * bv.x;
       bb += bv.y * bv.y;
-      rm = fmax(rm, fabs(r0) * rscale);
-      rm = fmax(rm, fabs(r1) * rscale);
+      rm = fmax(rm, fabs(r0) * rsc);
+      rm = fmax(rm, fabs(r1) * rsc);
       rs += r0;
       rs += r1;
     }
@@ -3263,6 +3264,7 @@ __global__ void __launch_bounds__(32 * (kDefectRows + 2)) k_defect_march(
   double rr = 0, bb = 0, rm = 0, rs = 0;
   const Tile t = tiles[blockIdx.x];
   const BlkLev B = bls[t.b];
+  const double rsc = rscale < 0.0 ? B.dv : rscale;  // rmax measure: |r| times the block's cell volume
   const int nx = B.nx, ny = B.ny, nz = B.nz;
   const long long sx = B.sx, sxy = B.sxy;
   const int zs = t.z0, ze = min(t.z0 + zc - 1, nz);
@@ -3384,8 +3386,8 @@ __global__ void __launch_bounds__(32 * (kDefectRows + 2)) k_defect_march(
         rr += r1 * r1;
         bb += b2.x * b2.x;
         bb += b2.y * b2.y;
-        rm = fmax(rm, fabs(r0) * rscale);
-        rm = fmax(rm, fabs(r1) * rscale);
+        rm = fmax(rm, fabs(r0) * rsc);
+        rm = fmax(rm, fabs(r1) * rsc);
         rs += r0;
         rs += r1;
       }

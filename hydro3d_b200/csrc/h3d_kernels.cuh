@@ -208,7 +208,8 @@ int defect_march_rows();
 
 // Level-1 FP64 defect: pn = p + e (all cells, when e != null), r = b - A pn on
 // the interior, rhs_out = r - mean_b (as TR), per-CTA partial sums
-// {sum r^2, sum b^2, max |r|*rscale, sum r} into partials[4*cta].
+// {sum r^2, sum b^2, max |r|*rscale, sum r} into partials[4*cta]; rscale < 0
+// stands for each block's own cell volume dv.
 template <typename TE, typename TR>
 cudaError_t launch_defect(bool var, const BlkLev* bl, RowTab rt, const double* p, const TE* e,
                           double* p_next, const double* b, TR* rhs_out, double mean_b, double rscale,

@@ -858,7 +858,9 @@ struct Exec {
   int defect(bool with_e) {
     Level& V = L(1);
     RowTab ct{V.d_rows_all, (int)V.geom.bl.size(), V.nrows_all};
-    double rscale = h->var ? 1.0 : V.geom.bl[0].dv;
+    // rmax = max |r| dV (press.for:61-63): sup already carries dV (L_LSM);
+    // otherwise each block's own cell volume (-1), which differs with refinement
+    double rscale = h->var ? 1.0 : -1.0;
     const double* fx = h->var ? V.fx64 : nullptr;
     const double* fy = h->var ? V.fy64 : nullptr;
     const double* fz = h->var ? V.fz64 : nullptr;

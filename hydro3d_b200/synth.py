@@ -1,4 +1,5 @@
-"""Seeded synthetic pressure-Poisson workloads (the five benchmark configurations).
+"""Seeded synthetic pressure-Poisson workloads (the five benchmark configurations
+and a local-mesh-refinement one).
 
 No public dataset is involved: every right-hand side is the discrete
 divergence of a seeded velocity field, computed the way calmas does it
@@ -222,4 +223,69 @@ def config5(seed: int = 1005, n: int = 256, ngrid: int = 8, rho_l: float = 1000.
                    var_coef=True, meta=dict(seed=seed, centre=c.tolist()))
 
 
-CONFIGS = {1: config1, 2: config2, 3: config3, 4: config4, 5: config5}
+def smooth_pressure(rng, nmodes: int = 24, kmax: float = 4.0):
+    """A seeded smooth pressure: nmodes cosines cos(2 pi k.x + phase) with
+    integer wave vectors 1 <= |k| <= kmax and amplitude |k|^(-5/3); returns
+    p(x, y, z) for cell-centre coordinate arrays."""
+    ks, amps, phases = [], [], []
+    while len(ks) < nmodes:
+        k = rng.integers(-int(kmax), int(kmax) + 1, 3)
+        kn = float(np.sqrt((k * k).sum()))
+        if 1.0 <= kn <= kmax:
+            ks.append(k.astype(np.float64))
+            amps.append(kn ** (-5.0 / 3.0))
+            phases.append(rng.uniform(0.0, 2.0 * np.pi))
+
+    def p(x, y, z):
+        out = np.zeros(np.broadcast(x, y, z).shape)
+        for k, a, ph in zip(ks, amps, phases):
+            out += a * np.cos(2.0 * np.pi * (k[0] * x + k[1] * y + k[2] * z) + ph)
+        return out
+    return p
+
+
+def config6(seed: int = 1006, nblk=(4, 2, 2), n: int = 64, ngrid_input: int = 6, refined=(1, 2),
+            resolve=None) -> Problem:
+    """Local mesh refinement (LMR = 2): 4x2x2 blocks of n^3 unrefined cells
+    (h = 1/(2n)), those of x index in `refined` refined by 2 (2n cells a side
+    at h/2): 8 x 64^3 + 8 x 128^3 = 18.9M cells, walls, 7 levels.
+
+    The operator with refinement is not symmetric and its left null vector is
+    not constant, so a divergence right-hand side is not compatible.  The
+    right-hand side is b = A p of the seeded smooth pressure meta["p_exact"]
+    (host fields), made by each solver's own operator: `b` is None until
+    `manufacture` fills it."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    hh = 1.0 / (nblk[1] * n)
+    blocks = topology.block_grid(nblk, (n, n, n), [WALL] * 6, (hh,) * 3, ngrid_input, resolve=resolve)
+    rdiv = [2 if (b % nblk[0]) in refined else 1 for b in range(len(blocks))]
+    topology.refine(blocks, rdiv, ngrid_input)
+    pf = smooth_pressure(rng)
+    pex = []
+    for d in blocks:
+        a = host_field(d)
+        x = (d.origin[0] + np.arange(d.n[0]) + 0.5) * d.h[0]
+        y = (d.origin[1] + np.arange(d.n[1]) + 0.5) * d.h[1]
+        z = (d.origin[2] + np.arange(d.n[2]) + 0.5) * d.h[2]
+        interior(a, d)[...] = pf(x[None, None, :], y[None, :, None], z[:, None, None])
+        pex.append(a)
+    return Problem("config6", blocks, ngrid_input + 1, None, [host_field(d) for d in blocks],
+                   meta=dict(seed=seed, rdiv=rdiv, p_exact=pex))
+
+
+def manufacture(prob: Problem, residual_of):
+    """Fills prob.b = A p_exact for a manufactured workload; residual_of(p)
+    returns the interior residual b - A p of b = 0 per block (canonical
+    (nz, ny, nx) arrays)."""
+    if prob.b is not None:
+        return prob
+    r = residual_of(prob.meta["p_exact"])
+    prob.b = []
+    for d, x in zip(prob.blocks, r):
+        a = host_field(d)
+        interior(a, d)[...] = -x
+        prob.b.append(a)
+    return prob
+
+
+CONFIGS = {1: config1, 2: config2, 3: config3, 4: config4, 5: config5, 6: config6}
