@@ -67,6 +67,7 @@ class MGDesc(C.Structure):
         ("inner_cycles", C.c_int32),
         ("use_graph", C.c_int32),
         ("coarse_op", C.c_int32),
+        ("coarse_direct", C.c_int32),
         ("blocks", C.POINTER(BlockDesc)),
     ]
 

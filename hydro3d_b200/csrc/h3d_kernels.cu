@@ -2784,6 +2784,39 @@ __global__ void __launch_bounds__(kClusterTailThreads) k_coarse_cluster(const Ta
         else relax(at32(F.s_phi32), (const float*)at32(F.s_rhs32));
         break;
       }
+      case kTailDense: {  // x = P b over the cells of every block (FP64), then the sweep fill
+        double* phi = at64(F.s_phi64);
+        const double* rhs = at64(F.s_rhs64);
+        if (op.zero) {
+          for (int q = threadIdx.x; q < F.npad; q += blockDim.x) phi[q] = 0.0;
+        }
+        cl.sync();  // every block's rhs is complete
+        const int nper = F.nint, n = F.dense_n;
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+        const BlkLev& B = fb[0];
+        for (int i = warp; i < nper; i += nwarp) {  // a warp per row of this block; lanes split the columns
+          const double* Pr = F.dense + (long long)(b * nper + i) * n;
+          double s = 0.0;
+          for (int j = lane; j < n; j += 32) {
+            const double* r = cl.map_shared_rank(rhs, j / nper);
+            s += __ldg(Pr + j) * r[j % nper];
+          }
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+          if (lane == 0) {
+            const int x = i % B.nx + 1, y = (i / B.nx) % B.ny + 1, z = i / (B.nx * B.ny) + 1;
+            phi[(long long)z * B.sxy + (long long)y * B.sx + x] = s;
+          }
+        }
+        cl.sync();  // every block's interior is written
+        for (int q = threadIdx.x; q < F.nfill; q += blockDim.x) {
+          const uint32_t dsti = F.fdst[2 * q], src = F.fdst[2 * q + 1];
+          const double* remote = cl.map_shared_rank(phi, (int)(src >> 24));
+          phi[dsti] = remote[src & 0xffffffu];
+        }
+        cl.sync();  // every ghost gathered before any interior changes
+        break;
+      }
       case kTailRestrict:
         if (op.f64) tail_restrict<double>(fb, cb, C, at64(F.s_phi64), at64(F.s_rhs64), at64(C.s_rhs64), op.zero);
         else tail_restrict<float>(fb, cb, C, at32(F.s_phi32), at32(F.s_rhs32), at32(C.s_rhs32), op.zero);

@@ -113,6 +113,8 @@ struct TailLevel {
   double* rhs64;
   int s_phi32, s_rhs32, s_phi64, s_rhs64;
   int s_cells, s_fill;  // cluster tail: arena offsets of the staged cell tables and this block's fill pairs
+  const double* dense;  // coarsest level solved directly: its pseudo-inverse, dense_n x dense_n, row-major
+  int dense_n;
 };
 enum TailKind {
   kTailRelax = 0,
@@ -121,8 +123,10 @@ enum TailKind {
   kTailRhsF2D = 3,
   kTailPhiD2F = 4,
   kTailLoadRhs = 5,
-  kTailStore = 6
+  kTailStore = 6,
+  kTailDense = 7  // cluster tail: phi = P rhs on the coarsest level (FP64), then its fill
 };
+constexpr int kDenseMaxCells = 512;  // largest coarsest level solved by its pseudo-inverse
 struct TailOp {
   int kind;
   int f64;     // the op runs in FP64

@@ -61,7 +61,8 @@ class MultigridSolver:
 
     def __init__(self, blocks: Sequence, ngrd_gl: int, mg_itrsch: int = 3, irestr: int = 2, iproln: int = 1,
                  maxcy: int = 30, precision: str = "fp64", var_coef: bool = False, device: int = 0,
-                 coarse_sweeps: int = 0, inner_cycles: int = 0, use_graph: bool = True, coarse_op: int = 0):
+                 coarse_sweeps: int = 0, inner_cycles: int = 0, use_graph: bool = True, coarse_op: int = 0,
+                 coarse_direct: bool = False):
         self.L = _lib.lib()
         self.blocks = list(blocks)
         self._arr = (_lib.BlockDesc * len(self.blocks))(*self.blocks)
@@ -79,6 +80,7 @@ class MultigridSolver:
         desc.inner_cycles = inner_cycles
         desc.use_graph = int(bool(use_graph))
         desc.coarse_op = coarse_op
+        desc.coarse_direct = int(bool(coarse_direct))
         desc.blocks = self._arr
         self.ngrd = ngrd_gl
         self.precision = precision

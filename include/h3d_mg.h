@@ -76,6 +76,9 @@ typedef struct h3d_mg_desc {
                              density (mgsolver.for:78-184, the reference); 1 = face-sum
                              coarsening (each coarse face = sum of its four fine faces / 16),
                              which keeps converging at 1000:1 density ratios */
+  int32_t coarse_direct;  /* 1: with coarse_sweeps > 0, solve a small coarsest level (at most
+                             512 cells, constant coefficients, symmetric) directly by its
+                             pseudo-inverse instead of the sweeps; 0: the sweeps */
   const h3d_block_desc* blocks;
 } h3d_mg_desc;
 
