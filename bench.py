@@ -35,12 +35,14 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 TOL = 1e-8
-# FP32 V-cycles per FP64 refinement step of the mixed solver, per workload
-# (measured: on configuration 3, 2 -> 6 refinement steps, 9.9 ms; 3 -> 4
-# steps, 9.3 ms; 4 -> 3 steps, 9.0 ms, all 12 V-cycles and the same 1.5e-9
-# error; on configurations 2 and 4, 4 overshoots the tolerance by a cycle or
-# two, 2 does not).
-INNER = {1: 2, 2: 2, 3: 4, 4: 2, 5: 2, 6: 2}
+# The mixed solver's cycle per workload: (pre-sweeps, post-sweeps, FP32
+# V-cycles per FP64 refinement step), the fastest measured shape whose solution
+# stays within the error of the V(2,1) one.  Configuration 3: V(2,1) x 4 8.61
+# ms, 12 cycles, error 1.4e-9 (V(2,2) x 3 and V(1,3) x 3 take 7.86 ms in 9
+# cycles but stop at 4-7e-9 with errors of 1.1-1.3e-8); configuration 6
+# (refinement): V(2,2) x 3 13.3 ms, 12 cycles, against V(2,1) x 4 20.6 ms, 24
+# cycles; configuration 4: V(1,2) x 3 12.7 against 13.2 ms.
+MIXED_CYCLE = {1: (2, 1, 4), 2: (2, 1, 2), 3: (2, 1, 4), 4: (1, 2, 3), 5: (2, 1, 4), 6: (2, 2, 3)}
 # Sweeps of the FP64 coarsest level in the mixed solver: enough to converge
 # that level (on the configuration-3 hierarchy 16 leave 14 V-cycles, 32 and 64
 # both 12), so the V-cycle contracts every mode at the rate of its finer
@@ -401,15 +403,14 @@ def config_of(cfg, prob):
             if prob.cells * 8 > 126e6 else "inputs smaller than L2 (no flush between solves)"}
 
 
-def mcell_updates(prob, cycles):
-    """Cell updates of `cycles` V(2,1) cycles: three sweeps of every level
-    (two before and one after the coarse correction; the coarsest level
-    irestr + iproln sweeps)."""
+def mcell_updates(prob, cycles, sweeps=3):
+    """Cell updates of `cycles` V-cycles of `sweeps` sweeps a level (V(2,1):
+    two before and one after the coarse correction)."""
     per = 0
     for d in prob.blocks:
         for g in range(1, prob.ngrid + 1):
             s = 2 ** (min(g, d.ngrid) - 1)  # level clamp of a block past its last level
-            per += (d.n[0] // s) * (d.n[1] // s) * (d.n[2] // s) * 3
+            per += (d.n[0] // s) * (d.n[1] // s) * (d.n[2] // s) * sweeps
     return per * cycles
 
 
@@ -463,7 +464,7 @@ def main():
     # the FP64 solution to EXACT_TOL (FP64 V-cycles with the converged
     # coarsest level): what "error against the FP64 solution" is measured on
     exact = build_solver_dev(prob, "fp64", device, coarse_sweeps=COARSE_SWEEPS,
-                             coarse_op=1 if prob.var_coef else 0)
+                             coarse_op=1 if prob.var_coef else 0, same_cycle=True)
     # the FP64 counterpart of the mixed solver (the same V-cycle in FP64) to
     # the benchmark tolerance, then to EXACT_TOL
     ms_fp64c, infos_fp64c = timed_solves(exact, prob, max(1, min(args.steps, 3)), 1, barrier=barrier)
@@ -544,9 +545,11 @@ def main():
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(value, 3),
             "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
             "data": "synthetic (seeded; no dataset)",
-            "config": dict(config_of(args.config, prob), precision="FP32 V(2,1) RBGS inside FP64 refinement",
-                           inner_cycles=INNER.get(args.config, 2),
-                           coarse="FP64 coarsest level, %d RBGS sweeps" % COARSE_SWEEPS
+            "config": dict(config_of(args.config, prob),
+                           precision="FP32 V(%d,%d) RBGS inside FP64 refinement" % MIXED_CYCLE[args.config][:2],
+                           inner_cycles=MIXED_CYCLE[args.config][2],
+                           coarse="FP64 coarsest level: solved by its pseudo-inverse when it has at most "
+                                  "%d cells, else %d RBGS sweeps" % (8 * COARSE_SWEEPS, COARSE_SWEEPS)
                            + ("; coarse coefficients by face sums" if prob.var_coef else ""),
                            parallelism="replicas" if world > 1 else "single GPU"),
             "fp64_ms": round(fp64_ms, 3), "speedup_vs_fp64": round(fp64_ms / (total_ms / (args.steps * world) * world), 3)
@@ -562,7 +565,8 @@ def main():
             "error_note": f"relative L2 (means removed) against the FP64 solution solved to {EXACT_TOL}; "
                           f"the plain FP64 solve to {TOL} is {err_plain:.2e} from it",
             "error_plain_fp64": err_plain,
-            "mcell_updates_per_s": round(mcell_updates(prob, info["cycles"]) / (value * 1e-3) / 1e6, 1),
+            "mcell_updates_per_s": round(mcell_updates(prob, info["cycles"], sum(MIXED_CYCLE[args.config][:2]))
+                                         / (value * 1e-3) / 1e6, 1),
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1) if achieved else None, "peak": peak,
                          "unit": "GB/s", "frac": round(achieved / peak, 4) if achieved else None,
                          "traffic": traffic, "kernel": "level-1 FP32 full red-black sweep (autotuned variant %d)"
@@ -606,21 +610,26 @@ def prob_config(prob):
     return int(prob.name[-1]) if prob.name.startswith("config") else 0
 
 
-def build_solver_dev(prob, precision, device, coarse_sweeps=None, coarse_op=None):
+def build_solver_dev(prob, precision, device, coarse_sweeps=None, coarse_op=None, same_cycle=None):
     """A solver on `device` with the workload's b and p0 resident.  The mixed
-    solver converges its FP64 coarsest level (COARSE_SWEEPS sweeps) and, for
-    variable coefficients, builds its coarse levels by face sums; the FP64
-    solver keeps the reference's irestr + iproln sweeps and coarse
-    coefficients unless told otherwise."""
+    solver runs the workload's cycle (MIXED_CYCLE), converges its FP64
+    coarsest level (directly or by COARSE_SWEEPS sweeps) and, for variable
+    coefficients, builds its coarse levels by face sums; the FP64 solver keeps
+    the reference's V(2,1), 3 coarsest sweeps and coarse coefficients unless
+    told otherwise (same_cycle: the mixed solver's cycle shape and coarse
+    solve, in FP64)."""
     from hydro3d_b200 import MultigridSolver
+    mixed = precision == "mixed"
+    same = mixed if same_cycle is None else same_cycle
     if coarse_sweeps is None:
-        coarse_sweeps = COARSE_SWEEPS if precision == "mixed" else 0
+        coarse_sweeps = COARSE_SWEEPS if mixed else 0
     if coarse_op is None:
-        coarse_op = 1 if (precision == "mixed" and prob.var_coef) else 0
+        coarse_op = 1 if (mixed and prob.var_coef) else 0
+    ir, ip, inner = MIXED_CYCLE[prob_config(prob)]
     s = MultigridSolver(prob.blocks, prob.ngrid, precision=precision, var_coef=prob.var_coef, maxcy=400,
                         device=device, coarse_sweeps=coarse_sweeps, coarse_op=coarse_op,
-                        coarse_direct=COARSE_DIRECT and precision == "mixed",
-                        inner_cycles=INNER.get(prob_config(prob), 2) if precision == "mixed" else 0)
+                        coarse_direct=COARSE_DIRECT and same,
+                        irestr=ir if same else 2, iproln=ip if same else 1, inner_cycles=inner if mixed else 0)
     if prob.var_coef:
         for ib, d in enumerate(prob.dens):
             s.set_density(ib, d)
