@@ -348,11 +348,13 @@ def mean_removed_error(a_list, b_list, blocks, per_block=False):
 
 def cpu_full_solve(prob, threads):
     """One complete FP64 solve of the workload by the oracle to 1e-8 (the
-    reference algorithm, measured, not projected)."""
+    reference algorithm, measured, not projected).  On the variable-density
+    workload the reference's coarse operator diverges: the solve stops at
+    FP64_CAP cycles and the result says so (res["status"] != 0)."""
     o = OracleSolver(prob, threads)
-    ms, res = o.solve()
+    ms, res = o.solve(maxcy=FP64_CAP if prob.var_coef else 400)
     o.close()
-    if res["status"] != 0:
+    if res["status"] != 0 and not prob.var_coef:
         raise RuntimeError(f"oracle solve did not converge ({res['cycles']} cycles)")
     return ms, res
 
@@ -534,9 +536,12 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         v, res = cpu_full_solve(prob, threads)
+        what = ("one complete FP64 solve of the full workload to 1e-8 by the oracle" if res["status"] == 0 else
+                "the oracle's FP64 solve of the full workload stopped unconverged (the reference algorithm "
+                f"diverges here, relres {res['relres']:.3g})")
         cpu = {"value": round(v, 1), "unit": "ms", "cores": threads, "kind": "port",
-               "sample": f"one complete FP64 solve of the full workload to 1e-8 by the oracle "
-                         f"({res['cycles']} V(2,1) cycles, measured)", "cycles": res["cycles"]}
+               "sample": f"{what} ({res['cycles']} V(2,1) cycles, measured)", "cycles": res["cycles"],
+               "converged": res["status"] == 0}
 
     if rank == 0:
         fp64_ms = statistics.median(ms_fp64)
