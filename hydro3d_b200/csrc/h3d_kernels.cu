@@ -2705,8 +2705,8 @@ __global__ void __launch_bounds__(kClusterTailThreads) k_coarse_cluster(const Ta
   namespace cg = cooperative_groups;
   cg::cluster_group cl = cg::this_cluster();
   const int b = (int)cl.block_rank();
-  __shared__ BlkLev fb[1], cb[1], gb[1];  // this block: fine / coarse compact layout, fine global layout
   __shared__ TailLevel lv[kTailMaxLevels];
+  __shared__ BlkLev gtab[kTailMaxLevels], ctab[kTailMaxLevels];  // this block per level: global / compact layout
   __shared__ TailOp ops[kClusterTailMaxOps];
   extern __shared__ unsigned char smem_raw[];
   unsigned char* arena = smem_base128(smem_raw);
@@ -2744,17 +2744,21 @@ __global__ void __launch_bounds__(kClusterTailThreads) k_coarse_cluster(const Ta
     B.pad = 0;
     return B;
   };
+  if (threadIdx.x < nlev) {
+    const BlkLev G = lvg[threadIdx.x].gbl[b];
+    gtab[threadIdx.x] = G;
+    ctab[threadIdx.x] = compact(G);
+  }
+  __syncthreads();
   for (int o = 0; o < nops; ++o) {
     const TailOp op = ops[o];
     const TailLevel& F = lv[op.fine];
     const TailLevel& C = lv[op.coarse];
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      gb[0] = F.gbl[b];
-      fb[0] = compact(F.gbl[b]);
-      cb[0] = compact(C.gbl[b]);
-    }
-    __syncthreads();
+    // this block's tables at the op's levels (staged once; every op ends with
+    // a barrier of the CTA or the cluster)
+    const BlkLev* gb = gtab + op.fine;
+    const BlkLev* fb = ctab + op.fine;
+    const BlkLev* cb = ctab + op.coarse;
     auto at32 = [&](int off) { return reinterpret_cast<float*>(arena + off); };
     auto at64 = [&](int off) { return reinterpret_cast<double*>(arena + off); };
     switch (op.kind) {
