@@ -37,12 +37,14 @@ sys.path.insert(0, ROOT)
 TOL = 1e-8
 # The mixed solver's cycle per workload: (pre-sweeps, post-sweeps, FP32
 # V-cycles per FP64 refinement step), the fastest measured shape whose solution
-# stays within the error of the V(2,1) one.  Configuration 3: V(2,1) x 4 8.61
-# ms, 12 cycles, error 1.4e-9 (V(2,2) x 3 and V(1,3) x 3 take 7.86 ms in 9
-# cycles but stop at 4-7e-9 with errors of 1.1-1.3e-8); configuration 6
-# (refinement): V(2,2) x 3 13.3 ms, 12 cycles, against V(2,1) x 4 20.6 ms, 24
-# cycles; configuration 4: V(1,2) x 3 12.7 against 13.2 ms.
-MIXED_CYCLE = {1: (2, 1, 4), 2: (2, 1, 2), 3: (2, 1, 4), 4: (1, 2, 3), 5: (2, 1, 4), 6: (2, 2, 3)}
+# stays within the error of the V(2,1) x 4 one.  Configuration 3: V(2,1) x 4
+# 8.5 ms, 12 cycles, error 1.4e-9 (V(2,1) x 6 8.3 ms and V(2,2) x 5 8.2 ms stop
+# after two refinement steps with errors of 2.0-2.6e-8; V(2,2) x 3 7.9 ms,
+# 1.3e-8); configuration 6 (refinement): V(2,2) x 6 12.3 ms, 12 cycles,
+# against V(2,1) x 4 20.6 ms, 24 cycles; configuration 2: V(2,1) x 5 2.8 ms
+# against x 2 3.1 ms; 4: V(1,2) x 6 12.2 against V(2,1) x 2 13.2 ms; 5: V(2,1)
+# x 8 34.0 against x 4 36.0 ms.
+MIXED_CYCLE = {1: (2, 1, 4), 2: (2, 1, 5), 3: (2, 1, 4), 4: (1, 2, 6), 5: (2, 1, 8), 6: (2, 2, 6)}
 # Sweeps of the FP64 coarsest level in the mixed solver: enough to converge
 # that level (on the configuration-3 hierarchy 16 leave 14 V-cycles, 32 and 64
 # both 12), so the V-cycle contracts every mode at the rate of its finer
