@@ -106,6 +106,7 @@ struct Level {
   int cur64 = 0, cur32 = 0;
   bool zero64 = false, zero32 = false;
   Tile* d_ztiles = nullptr;     // FP32 zero-source sweep tiles (launch_rbgs_zero32), or none
+  bool use_z32 = true;          // the zero-source kernel beat the tuned sweep's zero mode (autotuner)
   int nztiles = 0, zzc = 1;
   double* seq64 = nullptr;      // line-TDMA scratch a(s) of every cell (mg_itrsch 2)
   float* seq32 = nullptr;
@@ -597,7 +598,7 @@ struct Exec {
       h->kernels += 1;
       return H3D_OK;
     }
-    if (mixed_level(g) && V.zero32 && V.d_ztiles) {  // first sweep from a zero iterate: a stencil on rhs
+    if (mixed_level(g) && V.zero32 && V.d_ztiles && V.use_z32) {  // first sweep from a zero iterate: a stencil on rhs
       float* src = V.phi32[V.cur32];
       float* dst = V.phi32[1 - V.cur32];
       const bool push = V.push_ok;
@@ -1294,7 +1295,7 @@ int autotune_level(h3d_mg* h, int g) {
   cudaEvent_t a, b;
   CU(cudaEventCreate(&a));
   CU(cudaEventCreate(&b));
-  float best = 1e30f;
+  float best = 1e30f, best_tz = 1e30f;
   const bool f32 = f32_level(h, g);
   for (int v = 0; v < num_tile_shapes(); ++v) {
     TileShape s = tile_shape(v);
@@ -1334,12 +1335,30 @@ int autotune_level(h3d_mg* h, int g) {
         if (rep % 6 > 0) (zero ? tz : tn) = std::min(zero ? tz : tn, t);
       }
       const float tot = tn * ((g == 1 && h->mixed) ? 5.f : 2.f) + tz;
-      if (tot < best) { best = tot; best_v = v; best_z = zc; }
+      if (tot < best) { best = tot; best_v = v; best_z = zc; best_tz = tz; }
     }
+  }
+  TRY(build_tiles(h, V, best_v, best_z));
+  // the first sweep from a zero iterate: the zero-source stencil kernel or the
+  // chosen sweep's zero mode, whichever is faster on this level
+  if (f32 && !h->var && V.d_ztiles && V.nztiles > 0) {
+    const long long* push = (V.push_ok && rbgs_pushes(V.variant, h->var, true)) ? V.d_push : nullptr;
+    float tz32 = 1e30f;
+    for (int rep = 0; rep < 6; ++rep) {
+      TRY(flush_l2(h));
+      CU(cudaEventRecord(a, h->st));
+      CU(launch_rbgs_zero32(V.d_bl, V.d_ztiles, V.nztiles, V.zzc, V.rhs32, V.phi32[1 - V.cur32], push, h->st));
+      CU(cudaEventRecord(b, h->st));
+      CU(cudaEventSynchronize(b));
+      float t;
+      CU(cudaEventElapsedTime(&t, a, b));
+      if (rep > 0) tz32 = std::min(tz32, t);
+    }
+    V.use_z32 = tz32 < best_tz;
   }
   cudaEventDestroy(a);
   cudaEventDestroy(b);
-  return build_tiles(h, V, best_v, best_z);
+  return H3D_OK;
 }
 
 // Times every restriction variant and coarse z-chunk that fits the level
