@@ -3014,7 +3014,8 @@ __global__ void __launch_bounds__(256, 3) k_prolong_vec(const BlkLev* __restrict
   const long long cy = C.sx, cz = C.sxy;
   const int ng = F.nx / VEC;
   pdl_wait();  // everything above reads only setup data
-  for (int k = threadIdx.x >> 5; k <= F.ny / 2; k += 8) {
+#pragma unroll 2
+  for (int k = threadIdx.x >> 5; k <= F.ny / 2; k += 8) {  // two row pairs in flight a warp
     // rows 2k, 2k+1 and their sources
     int yq[2], syq[2];
     T wy0[2], wy1[2];
