@@ -79,6 +79,8 @@ struct Level {
   double* dens = nullptr;
   Halo sweep, faces, exch, bound;
   Halo sweep_push;              // the sweep fill without the faces the register-window sweeps push
+  Halo live, live_push;         // the parts of sweep / sweep_push that the next sweep or restriction reads
+  bool live_ok = false;         // live fills may stand in for the full fill (FP32 RBGS levels)
   long long* d_push = nullptr;  // per block, six ghost push offsets (kNoPush: none)
   bool push_ok = false;
   CUtensorMap* d_maps = nullptr;  // [ty index][0,1: iterate buffer, 2: rhs][block] tensor maps
@@ -557,7 +559,9 @@ struct Exec {
     return H3D_OK;
   }
 
-  int sweep(int g) {
+  // partial: the next reader of this level is a sweep or a restriction of
+  // it, so the fill may leave out the ghosts those never read (live tables)
+  int sweep(int g, bool partial = false) {
     Level& V = L(g);
     cudaStream_t st = h->st;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -605,7 +609,7 @@ struct Exec {
       CU(launch_rbgs_zero32(V.d_bl, V.d_ztiles, V.nztiles, V.zzc, V.rhs32, dst, push ? V.d_push : nullptr, st));
       TRY(chk("zero-source sweep fp32", g));
       if (e1) CU(record(e1));
-      const Halo& fill = push ? V.sweep_push : V.sweep;
+      const Halo& fill = partial && V.live_ok ? (push ? V.live_push : V.live) : (push ? V.sweep_push : V.sweep);
       TRY(sweep_fill<float>(V, fill, dst, src, true, &h->kernels));
       TRY(chk("fill fp32", g));
       V.cur32 = 1 - V.cur32;
@@ -622,7 +626,7 @@ struct Exec {
                             V.fx32, V.fy32, V.fz32, push ? V.d_push : nullptr, st));
       TRY(chk("sweep fp32", g));
       if (e1) CU(record(e1));
-      const Halo& fill = push ? V.sweep_push : V.sweep;
+      const Halo& fill = partial && V.live_ok ? (push ? V.live_push : V.live) : (push ? V.sweep_push : V.sweep);
       TRY(sweep_fill<float>(V, fill, dst, src, V.zero32, &h->kernels));
       TRY(chk("fill fp32", g));
       V.cur32 = 1 - V.cur32;
@@ -644,7 +648,9 @@ struct Exec {
     return H3D_OK;
   }
 
-  int relax(int g, int it) {
+  // live_next: the visit's next reader of level g is a restriction from it or
+  // another sweep of it (they read the live ghosts only)
+  int relax(int g, int it, bool live_next = false) {
     Level& V = L(g);
     if (it > 0 && V.small && g > 1 && h->desc.mg_itrsch == 3) {  // all sweeps and fills of this visit in one launch
       const int nb = (int)V.geom.bl.size();
@@ -678,7 +684,7 @@ struct Exec {
       h->kernels += 1;
       return H3D_OK;
     }
-    for (int q = 0; q < it; ++q) TRY(sweep(g));
+    for (int q = 0; q < it; ++q) TRY(sweep(g, live_next || q + 1 < it));
     return H3D_OK;
   }
 
@@ -811,20 +817,22 @@ struct Exec {
     return H3D_OK;
   }
 
-  int vcycle() {
+  // more: another V-cycle follows on the same level-1 iterate (its first reader
+  // is a sweep), so the last level-1 sweep may leave out the unread ghosts
+  int vcycle(bool more = false) {
     const int Lv = h->L;
     const int irestr = h->desc.irestr, iproln = h->desc.iproln;
     const int csw = h->desc.coarse_sweeps;
-    auto relax_at = [&](int g, int it, bool coarsest_first) -> int {
+    auto relax_at = [&](int g, int it, bool coarsest_first, bool live_next) -> int {
       if (g == Lv && Lv > 1 && csw > 0) return coarsest_first ? relax(g, csw) : H3D_OK;
-      return relax(g, it);
+      return relax(g, it, live_next);
     };
     if (Lv == 1) {
       if (csw > 0) return relax(1, csw);
       TRY(relax(1, irestr));
       return relax(1, iproln);
     }
-    TRY(relax(1, irestr));
+    TRY(relax(1, irestr, true));
     TRY(restrict_to(2));
     int kount[kMaxLevels + 2] = {0};
     int g = 2, nrel = irestr;
@@ -838,7 +846,7 @@ struct Exec {
         continue;
       }
       kount[g] += 1;
-      TRY(relax_at(g, nrel, true));
+      TRY(relax_at(g, nrel, true, kount[g] != 2 && g < Lv));
       if (kount[g] == 2) {
         TRY(correct(g - 1));
         kount[g] = 0;
@@ -849,13 +857,13 @@ struct Exec {
         g += 1;
         nrel = irestr;
       } else {
-        TRY(relax_at(g, iproln, false));
+        TRY(relax_at(g, iproln, false, false));
         TRY(correct(g - 1));
         nrel = iproln;
         g = Lv - 1;
       }
     }
-    return relax(1, iproln);
+    return relax(1, iproln, more);
   }
 
   // FP64 defect on the resident p/b: e = level-1 iterate (or none).
@@ -931,7 +939,7 @@ struct Exec {
     Level& V = L(1);
     if (h->mixed) V.zero32 = true;
     else V.zero64 = true;
-    for (int q = 0; q < inner; ++q) TRY(vcycle());
+    for (int q = 0; q < inner; ++q) TRY(vcycle(q + 1 < inner));
     if (h->proj) {
       TRY(proj_update());
       return vel_defect();
@@ -1526,6 +1534,58 @@ int h3d_topology(int32_t nblocks, const int32_t* ext, const int32_t* bc, const d
   return H3D_OK;
 }
 
+// The live part of a sweep fill: face ghosts of faces that are not physical
+// walls.  A sweep and the residual of a restriction read a cell's six face
+// neighbours only, with a zero coefficient across a wall (mgsolver.for:186-205),
+// so edge, corner and wall ghosts written after a sweep whose next reader is
+// one of those are never read.  Prolongation from the level and the outer
+// defect read the whole ghost shell: the last sweep before them keeps the full
+// fill.  Returns false (no live tables) unless every source is a current
+// interior cell, so that one full fill after any number of live ones leaves
+// the same ghost shell as full fills throughout.
+bool live_entries(const LevelGeom& G, const std::vector<uint32_t>& d, const std::vector<uint32_t>& s,
+                  std::vector<uint32_t>* ld, std::vector<uint32_t>* ls) {
+  const int nb = (int)G.bl.size();
+  auto locate = [&](uint32_t gi, int* b, int* x, int* y, int* z) -> bool {
+    for (int q = 0; q < nb; ++q) {
+      const BlkLev& B = G.bl[q];
+      const long long lo = B.off, hi = B.off + B.sxy * (B.nz + 2);
+      if ((long long)gi < lo || (long long)gi >= hi) continue;
+      const long long l = (long long)gi - lo;
+      *z = (int)(l / B.sxy);
+      *y = (int)((l % B.sxy) / B.sx);
+      *x = (int)(l % B.sx);
+      *b = q;
+      return *x <= B.nx + 1;
+    }
+    return false;
+  };
+  ld->clear();
+  ls->clear();
+  for (size_t e = 0; e < d.size(); ++e) {
+    int bs, xs, ys, zs, bd, x, y, z;
+    if ((s[e] & kOldFlag) || !locate(s[e] & kIdxMask, &bs, &xs, &ys, &zs)) return false;
+    const BlkLev& S = G.bl[bs];
+    if (xs < 1 || xs > S.nx || ys < 1 || ys > S.ny || zs < 1 || zs > S.nz) return false;
+    if (!locate(d[e], &bd, &x, &y, &z)) return false;
+    const BlkLev& D = G.bl[bd];
+    const bool ox = x == 0 || x == D.nx + 1, oy = y == 0 || y == D.ny + 1, oz = z == 0 || z == D.nz + 1;
+    if (ox + oy + oz != 1) continue;  // interior (none in a sweep fill), edge or corner ghost
+    const int f = ox ? (x == 0 ? 0 : 1) : oy ? (y == 0 ? 2 : 3) : (z == 0 ? 4 : 5);
+    if (D.phys & (1 << f)) continue;  // a wall: zero coefficient
+    ld->push_back(d[e]);
+    ls->push_back(s[e]);
+  }
+  return true;
+}
+
+int build_live(h3d_mg* h, Level& V, const std::vector<uint32_t>& d, const std::vector<uint32_t>& s) {
+  std::vector<uint32_t> ld, ls;
+  V.live_ok = live_entries(V.geom, d, s, &ld, &ls);
+  if (V.live_ok) TRY(upload_halo(h, V.live, ld, ls));
+  return H3D_OK;
+}
+
 // Ghost pushes of a level: a whole face of ghost cells of block bd whose
 // sweep-fill sources are, cell for cell, the adjacent face of interior cells
 // of one block bs (same pitches) is written by bs's register-window sweep
@@ -1609,6 +1669,11 @@ int build_push(h3d_mg* h, Level& V, const std::vector<uint32_t>& d, const std::v
   TRY(dalloc(h, &V.d_push, delta.size()));
   CU(cudaMemcpy(V.d_push, delta.data(), delta.size() * sizeof(long long), cudaMemcpyHostToDevice));
   TRY(upload_halo(h, V.sweep_push, rd, rs));
+  if (V.live_ok) {  // the live part of the pushed fill (a subset of a valid table)
+    std::vector<uint32_t> ld, ls;
+    if (!live_entries(V.geom, rd, rs, &ld, &ls)) return fail(h, H3D_ERR_INTERNAL, "live push table");
+    TRY(upload_halo(h, V.live_push, ld, ls));
+  }
   V.push_ok = true;
   return H3D_OK;
 }
@@ -2236,7 +2301,7 @@ int h3d_mg_destroy(h3d_mg* h) {
     void* ps[] = {V.d_bl, V.d_cta_all, V.d_cta_int, V.d_rows_all, V.d_rows_int, V.d_tiles, V.phi64[0], V.phi64[1], V.rhs64, V.phi32[0],
                   V.phi32[1], V.rhs32, V.fx64, V.fy64, V.fz64, V.fx32, V.fy32, V.fz32, V.dens,
                   V.sweep.d_dst, V.sweep.d_src, V.faces.d_dst, V.faces.d_src, V.exch.d_dst, V.exch.d_src,
-                  V.bound.d_dst, V.bound.d_src, V.sweep_push.d_dst, V.sweep_push.d_src, V.d_push, V.d_maps, V.d_rmaps, V.d_rtiles, V.d_ptiles, V.d_qtiles, V.d_dtiles, V.d_cstart, V.d_dstart, V.d_pstart, V.seq64, V.seq32, V.d_ztiles, V.lfill.d_dst, V.lfill.d_src, V.d_lfstart,
+                  V.bound.d_dst, V.bound.d_src, V.sweep_push.d_dst, V.sweep_push.d_src, V.live.d_dst, V.live.d_src, V.live_push.d_dst, V.live_push.d_src, V.d_push, V.d_maps, V.d_rmaps, V.d_rtiles, V.d_ptiles, V.d_qtiles, V.d_dtiles, V.d_cstart, V.d_dstart, V.d_pstart, V.seq64, V.seq32, V.d_ztiles, V.lfill.d_dst, V.lfill.d_src, V.d_lfstart,
                   V.xs.d_nodes, V.xs.d_dst, V.xs.d_src, V.xe.d_nodes, V.xe.d_dst, V.xe.d_src, V.xscratch, V.d_rsame,
                   V.d_psame, V.d_prows};
     for (void* p : ps) dfree(p);
@@ -2413,6 +2478,7 @@ int h3d_mg_create(h3d_mg** out, const h3d_mg_desc* desc) {
         return bail(fail(h, rc, err));
       if ((rc = upload_halo(h, V.sweep, d, s)) != H3D_OK) return bail(rc);
     }
+    if (!V.expr && f32_level(h, g) && (rc = build_live(h, V, d, s)) != H3D_OK) return bail(rc);
     if (!V.expr && f32_level(h, g) && !h->var && (rc = build_push(h, V, d, s)) != H3D_OK) return bail(rc);
     if (h->lmr) {  // blocks past their last level restrict by a copy and correct by an add
       if (g >= 2 && (rc = upload_block_list(h, V.geom, V.geom.clamped, false, &V.d_rsame, &V.nrsame,
