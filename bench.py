@@ -36,15 +36,22 @@ sys.path.insert(0, ROOT)
 
 TOL = 1e-8
 # The mixed solver's cycle per workload: (pre-sweeps, post-sweeps, FP32
-# V-cycles per FP64 refinement step), the fastest measured shape whose solution
-# stays within the error of the V(2,1) x 4 one.  Configuration 3: V(2,1) x 4
-# 8.5 ms, 12 cycles, error 1.4e-9 (V(2,1) x 6 8.3 ms and V(2,2) x 5 8.2 ms stop
-# after two refinement steps with errors of 2.0-2.6e-8; V(2,2) x 3 7.9 ms,
-# 1.3e-8); configuration 6 (refinement): V(2,2) x 6 12.3 ms, 12 cycles,
-# against V(2,1) x 4 20.6 ms, 24 cycles; configuration 2: V(2,1) x 5 2.8 ms
-# against x 2 3.1 ms; 4: V(1,2) x 6 12.2 against V(2,1) x 2 13.2 ms; 5: V(2,1)
-# x 8 34.0 against x 4 36.0 ms.
-MIXED_CYCLE = {1: (2, 1, 4), 2: (2, 1, 5), 3: (2, 1, 4), 4: (1, 2, 6), 5: (2, 1, 8), 6: (2, 2, 6)}
+# V-cycles per FP64 refinement step) and its FP32 sweeps: (over-relaxation
+# factor, rb_order: 1 = red-black order across block faces, 0 = the reference's
+# per-block order); the fastest measured choice whose solution stays within the
+# error of the V(2,1) x 4 Gauss-Seidel one.  Configuration 3: V(2,1) x 3 with
+# omega 1.25 across blocks 5.1 ms, 6 cycles, error 9.2e-10, against V(2,1) x 4
+# Gauss-Seidel per block 8.3 ms, 12 cycles, 1.4e-9 (omega 1.25 per block or
+# across blocks alone: 12 cycles; omega 1.3: 9 cycles; V(1,1) x 3: 9 cycles,
+# 6.0 ms); configuration 2: V(2,1) x 3, omega 1.25 across blocks 2.0 ms against
+# V(2,1) x 5 2.8 ms; 5: V(2,1) x 4, omega 1.25 across blocks 26.5 ms, error
+# 6.0e-8, against V(2,1) x 8 33.4 ms, 2.8e-7.  One block (1): omega 1.25 takes
+# 6 cycles, not 8, but its error grows from 3.7e-8 to 9.5e-7; independent
+# blocks (4) and refinement (6, whose expression-filled levels keep the
+# per-block order): no fewer cycles.  6: V(2,2) x 6 12.3 ms against V(2,1) x 4
+# 20.6 ms; 4: V(1,2) x 6 12.2 against V(2,1) x 2 13.2 ms.
+MIXED_CYCLE = {1: (2, 1, 4), 2: (2, 1, 3), 3: (2, 1, 3), 4: (1, 2, 6), 5: (2, 1, 4), 6: (2, 2, 6)}
+MIXED_SMOOTHER = {1: (1.0, 0), 2: (1.25, 1), 3: (1.25, 1), 4: (1.0, 0), 5: (1.25, 1), 6: (1.0, 0)}
 # Sweeps of the FP64 coarsest level in the mixed solver: enough to converge
 # that level (on the configuration-3 hierarchy 16 leave 14 V-cycles, 32 and 64
 # both 12), so the V-cycle contracts every mode at the rate of its finer
@@ -555,6 +562,10 @@ def main():
             "config": dict(config_of(args.config, prob),
                            precision="FP32 V(%d,%d) RBGS inside FP64 refinement" % MIXED_CYCLE[args.config][:2],
                            inner_cycles=MIXED_CYCLE[args.config][2],
+                           fp32_sweeps="over-relaxation %.2f, %s" % (
+                               MIXED_SMOOTHER[args.config][0],
+                               "red-black order across block faces" if MIXED_SMOOTHER[args.config][1]
+                               else "the reference's per-block red-black order"),
                            coarse="FP64 coarsest level: solved by its pseudo-inverse when it has at most "
                                   "%d cells, else %d RBGS sweeps" % (8 * COARSE_SWEEPS, COARSE_SWEEPS)
                            + ("; coarse coefficients by face sums" if prob.var_coef else ""),
@@ -633,10 +644,12 @@ def build_solver_dev(prob, precision, device, coarse_sweeps=None, coarse_op=None
     if coarse_op is None:
         coarse_op = 1 if (mixed and prob.var_coef) else 0
     ir, ip, inner = MIXED_CYCLE[prob_config(prob)]
+    om, rbo = MIXED_SMOOTHER[prob_config(prob)] if mixed else (0.0, 0)
     s = MultigridSolver(prob.blocks, prob.ngrid, precision=precision, var_coef=prob.var_coef, maxcy=400,
                         device=device, coarse_sweeps=coarse_sweeps, coarse_op=coarse_op,
                         coarse_direct=COARSE_DIRECT and same,
-                        irestr=ir if same else 2, iproln=ip if same else 1, inner_cycles=inner if mixed else 0)
+                        irestr=ir if same else 2, iproln=ip if same else 1, inner_cycles=inner if mixed else 0,
+                        omega=om, rb_order=rbo)
     if prob.var_coef:
         for ib, d in enumerate(prob.dens):
             s.set_density(ib, d)

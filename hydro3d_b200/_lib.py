@@ -68,6 +68,8 @@ class MGDesc(C.Structure):
         ("use_graph", C.c_int32),
         ("coarse_op", C.c_int32),
         ("coarse_direct", C.c_int32),
+        ("rb_order", C.c_int32),
+        ("omega", C.c_float),
         ("blocks", C.POINTER(BlockDesc)),
     ]
 

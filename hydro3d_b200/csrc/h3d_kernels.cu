@@ -27,6 +27,10 @@ namespace {
 // early launched grids hold SM resources the running ones need).
 __device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory"); }
 __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
+// Over-relaxed red-black update of the FP32 inner solve: x + om (gs - x), om
+// the handle's over-relaxation factor (1: Gauss-Seidel up to rounding).  The
+// FP64 sweeps keep the reference's update.
+__device__ __forceinline__ float sorf(float old, float gs, float om) { return fmaf(om, gs - old, old); }
 
 // Launch policy (H3D_PDL): "1" every kernel, "0" none; by default only a
 // kernel of at most kPdlGrid CTAs that follows one of at most kPdlGrid CTAs
@@ -153,7 +157,7 @@ template <typename T, int TX, int TY, int NT, bool VAR, bool ZERO>
 __global__ void __launch_bounds__(NT) k_rbgs(const BlkLev* __restrict__ bls, const Tile* __restrict__ tiles,
                                              int zc, const T* __restrict__ src, T* __restrict__ dst,
                                              const T* __restrict__ rhs, const T* __restrict__ fx,
-                                             const T* __restrict__ fy, const T* __restrict__ fz) {
+                                             const T* __restrict__ fy, const T* __restrict__ fz, float om) {
   pdl_trigger();
   pdl_wait();
   constexpr int RX = TX + 4, RY = TY + 4, RN = RX * RY;
@@ -196,9 +200,11 @@ __global__ void __launch_bounds__(NT) k_rbgs(const BlkLev* __restrict__ bls, con
       long long i = (long long)z * sxy + y * sx + x;
       Coef<T> c = cell_coef<T, VAR>(B, x, y, z, i, FX, FY, FZ);
       T ap = coef_ap(c);
-      P[s] = gs_div(R[i] - (c.aw * P[s - 1] + c.ae * P[s + 1] + c.as * P[s - RX] + c.an * P[s + RX] +
-                            c.ab * Pm[s] + c.at * Pp[s]),
-                    ap);
+      const T gv = gs_div(R[i] - (c.aw * P[s - 1] + c.ae * P[s + 1] + c.as * P[s - RX] + c.an * P[s + RX] +
+                                  c.ab * Pm[s] + c.at * Pp[s]),
+                          ap);
+      if constexpr (sizeof(T) == 4) P[s] = sorf(P[s], gv, om);
+      else P[s] = gv;
     }
   };
   auto black_store = [&](int z) {
@@ -221,6 +227,7 @@ __global__ void __launch_bounds__(NT) k_rbgs(const BlkLev* __restrict__ bls, con
         v = gs_div(R[i] - (c.aw * P[s - 1] + c.ae * P[s + 1] + c.as * P[s - RX] + c.an * P[s + RX] +
                            c.ab * Pm[s] + c.at * Pp[s]),
                    ap);
+        if constexpr (sizeof(T) == 4) v = sorf(P[s], v, om);
       }
       Dz[y * sx + x] = v;
     }
@@ -255,7 +262,7 @@ __global__ void __launch_bounds__(NT) k_rbgs(const BlkLev* __restrict__ bls, con
 // table per CTA.  Ghost pushes as in the window sweep.
 __global__ void __launch_bounds__(256, 3) k_rbgs_zero32(const BlkLev* __restrict__ bls, const Tile* __restrict__ tiles,
                                                      int zc, const float* __restrict__ rhs, float* __restrict__ dst,
-                                                     const long long* __restrict__ push) {
+                                                     const long long* __restrict__ push, float om) {
   pdl_trigger();
   __shared__ float ivtab[64];
   const Tile t = tiles[blockIdx.x];
@@ -340,14 +347,15 @@ __global__ void __launch_bounds__(256, 3) k_rbgs_zero32(const BlkLev* __restrict
       for (int k = 0; k < 4; ++k) {
         const float ivk = k == 0 ? iv_0 : (k == 3 ? iv_3 : iv0);
         if (((par + k) & 1) == 1) {
-          out[k] = hzv[k] * ivk;
+          out[k] = sorf(0.f, hzv[k] * ivk, om);
         } else {
-          const float w = k > 0 ? hzv[k - 1] * (k == 1 ? iv_0 : iv0) : rl * ivw;
-          const float e = k < 3 ? hzv[k + 1] * (k == 2 ? iv_3 : iv0) : rr * ive;
+          const float w = sorf(0.f, k > 0 ? hzv[k - 1] * (k == 1 ? iv_0 : iv0) : rl * ivw, om);
+          const float e = sorf(0.f, k < 3 ? hzv[k + 1] * (k == 2 ? iv_3 : iv0) : rr * ive, om);
           const float aw = k == 0 ? aw0 : ax, ae = k == 3 ? ae3 : ax;
-          const float sum = fmaf(az, htv[k] * ivk, fmaf(az, hbv[k] * ivk, fmaf(ay, hnv[k] * ivk,
-                            fmaf(ay, hsv[k] * ivk, fmaf(ae, e, aw * w)))));
-          out[k] = (hzv[k] - sum) * ivk;
+          const float sum = fmaf(az, sorf(0.f, htv[k] * ivk, om), fmaf(az, sorf(0.f, hbv[k] * ivk, om),
+                            fmaf(ay, sorf(0.f, hnv[k] * ivk, om), fmaf(ay, sorf(0.f, hsv[k] * ivk, om),
+                            fmaf(ae, e, aw * w)))));
+          out[k] = sorf(0.f, (hzv[k] - sum) * ivk, om);
         }
       }
     } else {
@@ -357,19 +365,19 @@ __global__ void __launch_bounds__(256, 3) k_rbgs_zero32(const BlkLev* __restrict
         const int m = wmask(x, y, z);
         const float iv = ivtab[m];
         if (((par + k) & 1) == 1) {
-          out[k] = hzv[k] * iv;
+          out[k] = sorf(0.f, hzv[k] * iv, om);
         } else {
           // red neighbours (zero outside the block's interior)
-          const float w = k > 0 ? hzv[k - 1] * ivtab[wmask(x - 1, y, z)] : (x0 > 1 ? rl * ivtab[wmask(x - 1, y, z)] : 0.f);
-          const float e = k < 3 ? hzv[k + 1] * ivtab[wmask(x + 1, y, z)] : (x + 1 <= nx ? rr * ivtab[wmask(x + 1, y, z)] : 0.f);
-          const float sv = y > 1 ? hsv[k] * ivtab[wmask(x, y - 1, z)] : 0.f;
-          const float nv = y < ny ? hnv[k] * ivtab[wmask(x, y + 1, z)] : 0.f;
-          const float bv = z > 1 ? hbv[k] * ivtab[wmask(x, y, z - 1)] : 0.f;
-          const float tv = z < nz ? htv[k] * ivtab[wmask(x, y, z + 1)] : 0.f;
+          const float w = sorf(0.f, k > 0 ? hzv[k - 1] * ivtab[wmask(x - 1, y, z)] : (x0 > 1 ? rl * ivtab[wmask(x - 1, y, z)] : 0.f), om);
+          const float e = sorf(0.f, k < 3 ? hzv[k + 1] * ivtab[wmask(x + 1, y, z)] : (x + 1 <= nx ? rr * ivtab[wmask(x + 1, y, z)] : 0.f), om);
+          const float sv = sorf(0.f, y > 1 ? hsv[k] * ivtab[wmask(x, y - 1, z)] : 0.f, om);
+          const float nv = sorf(0.f, y < ny ? hnv[k] * ivtab[wmask(x, y + 1, z)] : 0.f, om);
+          const float bv = sorf(0.f, z > 1 ? hbv[k] * ivtab[wmask(x, y, z - 1)] : 0.f, om);
+          const float tv = sorf(0.f, z < nz ? htv[k] * ivtab[wmask(x, y, z + 1)] : 0.f, om);
           const float aw = (m & 1) ? 0.f : ax, ae = (m & 2) ? 0.f : ax, as = (m & 4) ? 0.f : ay,
                       an = (m & 8) ? 0.f : ay, ab = (m & 16) ? 0.f : az, at = (m & 32) ? 0.f : az;
           const float sum = fmaf(at, tv, fmaf(ab, bv, fmaf(an, nv, fmaf(as, sv, fmaf(ae, e, aw * w)))));
-          out[k] = (hzv[k] - sum) * iv;
+          out[k] = sorf(0.f, (hzv[k] - sum) * iv, om);
         }
       }
     }
@@ -395,9 +403,9 @@ __global__ void __launch_bounds__(256, 3) k_rbgs_zero32(const BlkLev* __restrict
 }  // namespace
 
 cudaError_t launch_rbgs_zero32(const BlkLev* bl, const Tile* tiles, int ntiles, int zc, const float* rhs, float* dst,
-                               const long long* push, cudaStream_t st) {
+                               const long long* push, float om, cudaStream_t st) {
   if (ntiles <= 0) return cudaSuccess;
-  pdl_launch(k_rbgs_zero32, ntiles, 256, 0, st, bl, tiles, zc, rhs, dst, push);
+  pdl_launch(k_rbgs_zero32, ntiles, 256, 0, st, bl, tiles, zc, rhs, dst, push, om);
   return cudaGetLastError();
 }
 
@@ -586,6 +594,7 @@ template <typename T, int CP, bool VAR>
 struct RowGs {
   T cw[CP][2], ce[CP][2], cinv[CP][2], cxy[CP][2];
   T cs, cn, az;
+  float om;  // over-relaxation (FP32)
   int ph, nz;
 
   __device__ __forceinline__ void init(const BlkLev& B, int y, int tc, int tpr) {
@@ -632,7 +641,7 @@ struct RowGs {
       T inv;
       if (!VAR && z > 1 && z < nz) inv = m ? cinv[k][1] : cinv[k][0];
       else inv = T(1) / (-(aw + ae + as + an + ab + at));
-      return (rv - sum) * inv;
+      return sorf(P[s], (rv - sum) * inv, om);
     }
   }
 };
@@ -650,7 +659,8 @@ __global__ void __launch_bounds__(TPR*(TY + 2)) k_rbgs_rows(const BlkLev* __rest
                                                            const Tile* __restrict__ tiles, int zc,
                                                            const T* __restrict__ src, T* __restrict__ dst,
                                                            const T* __restrict__ rhs, const T* __restrict__ fx,
-                                                           const T* __restrict__ fy, const T* __restrict__ fz) {
+                                                           const T* __restrict__ fy, const T* __restrict__ fz,
+                                                           float om) {
   pdl_trigger();
   pdl_wait();
   constexpr int SP = 2 * CP * TPR + 4;
@@ -699,6 +709,7 @@ __global__ void __launch_bounds__(TPR*(TY + 2)) k_rbgs_rows(const BlkLev* __rest
   // one cell update in plane z (P), neighbours in Pm (z-1), Pp (z+1)
   RowGs<T, CP, VAR> gs;
   gs.init(B, y, tc, TPR);
+  gs.om = om;
   auto red = [&](int z) {
     if (!row_in) return;
     T* P = ring + (z & 3) * PL;
@@ -850,7 +861,7 @@ __global__ void __launch_bounds__(TPR*(TY + 2)) k_rbgs_tma2(const BlkLev* __rest
                                                            const CUtensorMap* __restrict__ rmaps,
                                                            T* __restrict__ dst, const T* __restrict__ fx,
                                                            const T* __restrict__ fy, const T* __restrict__ fz,
-                                                           int* err) {
+                                                           int* err, float om) {
   pdl_trigger();
   pdl_wait();
   using C = Tma2Cfg<T, TPR, CP, TY, D>;
@@ -916,6 +927,7 @@ __global__ void __launch_bounds__(TPR*(TY + 2)) k_rbgs_tma2(const BlkLev* __rest
   };
   RowGs<T, CP, VAR> gs;
   gs.init(B, y, tc, TPR);
+  gs.om = om;
   auto red = [&](int z) {
     if (!row_in) return;
     T* P = pslot(z);
@@ -1001,7 +1013,7 @@ __global__ void __launch_bounds__(TPR*(TY + 2)) k_rbgs_vec(const BlkLev* __restr
                                                           const Tile* __restrict__ tiles, int zc,
                                                           const CUtensorMap* __restrict__ maps,
                                                           const CUtensorMap* __restrict__ rmaps,
-                                                          float* __restrict__ dst, int* err) {
+                                                          float* __restrict__ dst, int* err, float om) {
   pdl_trigger();
   pdl_wait();
   using C = VecCfg<TPR, GPT, TY, NS, D>;
@@ -1114,11 +1126,11 @@ __global__ void __launch_bounds__(TPR*(TY + 2)) k_rbgs_vec(const BlkLev* __restr
     }
     float4& c = in.c;
     if (q == 0) {
-      c.x = upd(in.side, c.y, in.u.x, in.dn.x, in.bz.x, in.tz.x, in.rh.x, aw0[k], ax, as, an, ab, at, i0);
-      c.z = upd(c.y, c.w, in.u.z, in.dn.z, in.bz.z, in.tz.z, in.rh.z, ax, ax, as, an, ab, at, i12);
+      c.x = sorf(c.x, upd(in.side, c.y, in.u.x, in.dn.x, in.bz.x, in.tz.x, in.rh.x, aw0[k], ax, as, an, ab, at, i0), om);
+      c.z = sorf(c.z, upd(c.y, c.w, in.u.z, in.dn.z, in.bz.z, in.tz.z, in.rh.z, ax, ax, as, an, ab, at, i12), om);
     } else {
-      c.y = upd(c.x, c.z, in.u.y, in.dn.y, in.bz.y, in.tz.y, in.rh.y, ax, ax, as, an, ab, at, i12);
-      c.w = upd(c.z, in.side, in.u.w, in.dn.w, in.bz.w, in.tz.w, in.rh.w, ax, ae3[k], as, an, ab, at, i3);
+      c.y = sorf(c.y, upd(c.x, c.z, in.u.y, in.dn.y, in.bz.y, in.tz.y, in.rh.y, ax, ax, as, an, ab, at, i12), om);
+      c.w = sorf(c.w, upd(c.z, in.side, in.u.w, in.dn.w, in.bz.w, in.tz.w, in.rh.w, ax, ae3[k], as, an, ab, at, i3), om);
     }
   };
 
@@ -1732,15 +1744,15 @@ TileShape tile_shape(int v) { return kShapes[v]; }
 template <typename T, int TX, int TY, int NT>
 static cudaError_t rbgs_dispatch(bool var, bool zero, const BlkLev* bl, const Tile* tiles, int ntiles, int zc,
                                  const T* src, T* dst, const T* rhs, const T* fx, const T* fy, const T* fz,
-                                 cudaStream_t st) {
+                                 float om, cudaStream_t st) {
   if (ntiles <= 0) return cudaSuccess;
   dim3 grid(ntiles), block(NT);
   if (var) {
-    if (zero) pdl_launch(k_rbgs<T, TX, TY, NT, true, true>, grid, block, 0, st, bl, tiles, zc, src, dst, rhs, fx, fy, fz);
-    else pdl_launch(k_rbgs<T, TX, TY, NT, true, false>, grid, block, 0, st, bl, tiles, zc, src, dst, rhs, fx, fy, fz);
+    if (zero) pdl_launch(k_rbgs<T, TX, TY, NT, true, true>, grid, block, 0, st, bl, tiles, zc, src, dst, rhs, fx, fy, fz, om);
+    else pdl_launch(k_rbgs<T, TX, TY, NT, true, false>, grid, block, 0, st, bl, tiles, zc, src, dst, rhs, fx, fy, fz, om);
   } else {
-    if (zero) pdl_launch(k_rbgs<T, TX, TY, NT, false, true>, grid, block, 0, st, bl, tiles, zc, src, dst, rhs, fx, fy, fz);
-    else pdl_launch(k_rbgs<T, TX, TY, NT, false, false>, grid, block, 0, st, bl, tiles, zc, src, dst, rhs, fx, fy, fz);
+    if (zero) pdl_launch(k_rbgs<T, TX, TY, NT, false, true>, grid, block, 0, st, bl, tiles, zc, src, dst, rhs, fx, fy, fz, om);
+    else pdl_launch(k_rbgs<T, TX, TY, NT, false, false>, grid, block, 0, st, bl, tiles, zc, src, dst, rhs, fx, fy, fz, om);
   }
   return cudaGetLastError();
 }
@@ -1763,17 +1775,17 @@ static cudaError_t rows_attr() {
 template <typename T, int TPR, int CP, int TY>
 static cudaError_t rows_dispatch(bool var, bool zero, const BlkLev* bl, const Tile* tiles, int ntiles, int zc,
                                  const T* src, T* dst, const T* rhs, const T* fx, const T* fy, const T* fz,
-                                 cudaStream_t st) {
+                                 float om, cudaStream_t st) {
   if (ntiles <= 0) return cudaSuccess;
   constexpr int NT = TPR * (TY + 2);
   constexpr size_t SM = rows_smem<T, TPR, CP, TY>();
   dim3 grid(ntiles), block(NT);
   if (var) {
-    if (zero) pdl_launch(k_rbgs_rows<T, TPR, CP, TY, true, true>, grid, block, SM, st, bl, tiles, zc, src, dst, rhs, fx, fy, fz);
-    else pdl_launch(k_rbgs_rows<T, TPR, CP, TY, true, false>, grid, block, SM, st, bl, tiles, zc, src, dst, rhs, fx, fy, fz);
+    if (zero) pdl_launch(k_rbgs_rows<T, TPR, CP, TY, true, true>, grid, block, SM, st, bl, tiles, zc, src, dst, rhs, fx, fy, fz, om);
+    else pdl_launch(k_rbgs_rows<T, TPR, CP, TY, true, false>, grid, block, SM, st, bl, tiles, zc, src, dst, rhs, fx, fy, fz, om);
   } else {
-    if (zero) pdl_launch(k_rbgs_rows<T, TPR, CP, TY, false, true>, grid, block, SM, st, bl, tiles, zc, src, dst, rhs, fx, fy, fz);
-    else pdl_launch(k_rbgs_rows<T, TPR, CP, TY, false, false>, grid, block, SM, st, bl, tiles, zc, src, dst, rhs, fx, fy, fz);
+    if (zero) pdl_launch(k_rbgs_rows<T, TPR, CP, TY, false, true>, grid, block, SM, st, bl, tiles, zc, src, dst, rhs, fx, fy, fz, om);
+    else pdl_launch(k_rbgs_rows<T, TPR, CP, TY, false, false>, grid, block, SM, st, bl, tiles, zc, src, dst, rhs, fx, fy, fz, om);
   }
   return cudaGetLastError();
 }
@@ -1800,13 +1812,13 @@ static cudaError_t tma2_attr() {
 template <typename T, int TPR, int CP, int TY, int D0>
 static cudaError_t tma2_dispatch(bool var, const BlkLev* bl, const Tile* tiles, int ntiles, int zc,
                                  const CUtensorMap* maps, const CUtensorMap* rmaps, int* err, T* dst, const T* fx,
-                                 const T* fy, const T* fz, cudaStream_t st) {
+                                 const T* fy, const T* fz, float om, cudaStream_t st) {
   if (ntiles <= 0) return cudaSuccess;
   constexpr int D = tma2_depth<T, TPR, CP, TY, D0>();
   constexpr int NT = TPR * (TY + 2);
   constexpr size_t SM = Tma2Cfg<T, TPR, CP, TY, D>::SMEM;
-  if (var) pdl_launch(k_rbgs_tma2<T, TPR, CP, TY, D, true>, ntiles, NT, SM, st, bl, tiles, zc, maps, rmaps, dst, fx, fy, fz, err);
-  else pdl_launch(k_rbgs_tma2<T, TPR, CP, TY, D, false>, ntiles, NT, SM, st, bl, tiles, zc, maps, rmaps, dst, fx, fy, fz, err);
+  if (var) pdl_launch(k_rbgs_tma2<T, TPR, CP, TY, D, true>, ntiles, NT, SM, st, bl, tiles, zc, maps, rmaps, dst, fx, fy, fz, err, om);
+  else pdl_launch(k_rbgs_tma2<T, TPR, CP, TY, D, false>, ntiles, NT, SM, st, bl, tiles, zc, maps, rmaps, dst, fx, fy, fz, err, om);
   return cudaGetLastError();
 }
 
@@ -1836,13 +1848,13 @@ __device__ __forceinline__ float win_upd(float w, float e, float s, float n, flo
 __device__ __forceinline__ void win_colour(float4& c, const float4& bz, const float4& tz, const float4& u,
                                            const float4& dn, const float4& rh, float l, float r, bool q1, float aw0,
                                            float ae3, float ax, float as, float an, float ab, float at, float iv0,
-                                           float iv12, float iv3) {
+                                           float iv12, float iv3, float om) {
   if (!q1) {
-    c.x = win_upd(l, c.y, u.x, dn.x, bz.x, tz.x, rh.x, aw0, ax, as, an, ab, at, iv0);
-    c.z = win_upd(c.y, c.w, u.z, dn.z, bz.z, tz.z, rh.z, ax, ax, as, an, ab, at, iv12);
+    c.x = sorf(c.x, win_upd(l, c.y, u.x, dn.x, bz.x, tz.x, rh.x, aw0, ax, as, an, ab, at, iv0), om);
+    c.z = sorf(c.z, win_upd(c.y, c.w, u.z, dn.z, bz.z, tz.z, rh.z, ax, ax, as, an, ab, at, iv12), om);
   } else {
-    c.y = win_upd(c.x, c.z, u.y, dn.y, bz.y, tz.y, rh.y, ax, ax, as, an, ab, at, iv12);
-    c.w = win_upd(c.z, r, u.w, dn.w, bz.w, tz.w, rh.w, ax, ae3, as, an, ab, at, iv3);
+    c.y = sorf(c.y, win_upd(c.x, c.z, u.y, dn.y, bz.y, tz.y, rh.y, ax, ax, as, an, ab, at, iv12), om);
+    c.w = sorf(c.w, win_upd(c.z, r, u.w, dn.w, bz.w, tz.w, rh.w, ax, ae3, as, an, ab, at, iv3), om);
   }
 }
 
@@ -1867,7 +1879,7 @@ __global__ void __launch_bounds__(TPR*(TY + 2)) k_rbgs_win(const BlkLev* __restr
                                                           const CUtensorMap* __restrict__ maps,
                                                           const CUtensorMap* __restrict__ rmaps,
                                                           float* __restrict__ dst, int* err,
-                                                          const long long* __restrict__ push) {
+                                                          const long long* __restrict__ push, float om) {
   pdl_trigger();
   using C = VecCfg<TPR, GPT, TY, NS, D>;
   static_assert(TPR <= 32 && (TPR & (TPR - 1)) == 0, "a row is a power-of-two lane segment of one warp");
@@ -2005,12 +2017,12 @@ __global__ void __launch_bounds__(TPR*(TY + 2)) k_rbgs_win(const BlkLev* __restr
   do {                                                                                                           \
     const bool wlo_ = (zz) == 1 && (ph & 16), whi_ = (zz) == nz && (ph & 32);                                    \
     if (!(wlo_ || whi_)) {                                                                                       \
-      win_colour(c, bz, tz, u, dn, rh, l, r, q1, aw0[k], ae3[k], ax, as, an, az, az, i0[k], i12, i3[k]);          \
+      win_colour(c, bz, tz, u, dn, rh, l, r, q1, aw0[k], ae3[k], ax, as, an, az, az, i0[k], i12, i3[k], om);      \
     } else {                                                                                                     \
       win_colour(c, bz, tz, u, dn, rh, l, r, q1, aw0[k], ae3[k], ax, as, an, wlo_ ? 0.f : az, whi_ ? 0.f : az,   \
                  wlo_ ? (whi_ ? i0bt[k] : i0b[k]) : (whi_ ? i0t[k] : i0[k]),                                     \
                  wlo_ ? (whi_ ? i12bt : i12b) : (whi_ ? i12t : i12),                                             \
-                 wlo_ ? (whi_ ? i3bt[k] : i3b[k]) : (whi_ ? i3t[k] : i3[k]));                                    \
+                 wlo_ ? (whi_ ? i3bt[k] : i3b[k]) : (whi_ ? i3t[k] : i3[k]), om);                                \
     }                                                                                                            \
   } while (0)
   auto ld4 = [](const float* p) { return *reinterpret_cast<const float4*>(p); };
@@ -2145,10 +2157,10 @@ static cudaError_t vec_attr() {
 
 template <int TPR, int GPT, int TY, int NS, int D>
 static cudaError_t vec_dispatch(const BlkLev* bl, const Tile* tiles, int ntiles, int zc, const CUtensorMap* maps,
-                                const CUtensorMap* rmaps, int* err, float* dst, cudaStream_t st) {
+                                const CUtensorMap* rmaps, int* err, float* dst, float om, cudaStream_t st) {
   if (ntiles <= 0) return cudaSuccess;
   pdl_launch(k_rbgs_vec<TPR, GPT, TY, NS, D>, ntiles, TPR * (TY + 2), VecCfg<TPR, GPT, TY, NS, D>::SMEM, st, 
-      bl, tiles, zc, maps, rmaps, dst, err);
+      bl, tiles, zc, maps, rmaps, dst, err, om);
   return cudaGetLastError();
 }
 
@@ -2165,16 +2177,16 @@ static cudaError_t win_attr() {
 template <int TPR, int GPT, int TY, int NS, int D, int U>
 static cudaError_t win_dispatch(bool zero, const BlkLev* bl, const Tile* tiles, int ntiles, int zc,
                                 const CUtensorMap* maps, const CUtensorMap* rmaps, int* err, float* dst,
-                                const long long* push, cudaStream_t st) {
+                                const long long* push, float om, cudaStream_t st) {
   static_assert(D + 3 <= NS, "a plane is read until two phases after its own");
   if (ntiles <= 0) return cudaSuccess;
   constexpr size_t SM = VecCfg<TPR, GPT, TY, NS, D>::SMEM;
   if (zero)
     pdl_launch(k_rbgs_win<TPR, GPT, TY, NS, D, true, U>, ntiles, TPR * (TY + 2), SM, st, bl, tiles, zc, maps, rmaps,
-               dst, err, push);
+               dst, err, push, om);
   else
     pdl_launch(k_rbgs_win<TPR, GPT, TY, NS, D, false, U>, ntiles, TPR * (TY + 2), SM, st, bl, tiles, zc, maps, rmaps,
-               dst, err, push);
+               dst, err, push, om);
   return cudaGetLastError();
 }
 
@@ -2268,7 +2280,8 @@ bool rbgs_pushes(int variant, bool var, bool f32) {
 template <typename T>
 cudaError_t launch_rbgs(int variant, bool var, bool zero_src, const BlkLev* bl, const Tile* tiles, int ntiles,
                         int zc, const CUtensorMap* maps, const CUtensorMap* rmaps, int* err, const T* src, T* dst,
-                        const T* rhs, const T* fx, const T* fy, const T* fz, const long long* push, cudaStream_t st) {
+                        const T* rhs, const T* fx, const T* fy, const T* fz, const long long* push, float om,
+                        cudaStream_t st) {
   // ghost pushes need the register-window sweep to run as asked
   if (push && (!rbgs_pushes(variant, var, sizeof(T) == 4) || !maps || !rmaps)) return cudaErrorInvalidValue;
   if (variant >= 0 && variant < num_tile_shapes() && kShapes[variant].tma) {
@@ -2283,31 +2296,31 @@ cudaError_t launch_rbgs(int variant, bool var, bool zero_src, const BlkLev* bl, 
   if constexpr (sizeof(T) == 4) {
     switch (variant) {
 #define X(v, tpr, gpt, ty, ns, d) \
-      case v: return vec_dispatch<tpr, gpt, ty, ns, d>(bl, tiles, ntiles, zc, maps, rmaps, err, reinterpret_cast<float*>(dst), st);
+      case v: return vec_dispatch<tpr, gpt, ty, ns, d>(bl, tiles, ntiles, zc, maps, rmaps, err, reinterpret_cast<float*>(dst), om, st);
       H3D_VEC_SHAPES(X)
 #undef X
 #define X(v, tpr, gpt, ty, ns, d, u) \
-      case v: return win_dispatch<tpr, gpt, ty, ns, d, u>(zero_src, bl, tiles, ntiles, zc, maps, rmaps, err, reinterpret_cast<float*>(dst), push, st);
+      case v: return win_dispatch<tpr, gpt, ty, ns, d, u>(zero_src, bl, tiles, ntiles, zc, maps, rmaps, err, reinterpret_cast<float*>(dst), push, om, st);
       H3D_WIN_SHAPES(X)
 #undef X
       default: break;
     }
   }
   switch (variant) {
-    case 0: return rbgs_dispatch<T, 32, 16, 256>(var, zero_src, bl, tiles, ntiles, zc, src, dst, rhs, fx, fy, fz, st);
-    case 1: return rbgs_dispatch<T, 32, 8, 256>(var, zero_src, bl, tiles, ntiles, zc, src, dst, rhs, fx, fy, fz, st);
-    case 2: return rbgs_dispatch<T, 64, 8, 256>(var, zero_src, bl, tiles, ntiles, zc, src, dst, rhs, fx, fy, fz, st);
-    case 3: return rbgs_dispatch<T, 16, 8, 128>(var, zero_src, bl, tiles, ntiles, zc, src, dst, rhs, fx, fy, fz, st);
-    case 4: return rbgs_dispatch<T, 8, 8, 64>(var, zero_src, bl, tiles, ntiles, zc, src, dst, rhs, fx, fy, fz, st);
-    case 5: return rbgs_dispatch<T, 8, 4, 32>(var, zero_src, bl, tiles, ntiles, zc, src, dst, rhs, fx, fy, fz, st);
-    case 6: return rbgs_dispatch<T, 4, 4, 32>(var, zero_src, bl, tiles, ntiles, zc, src, dst, rhs, fx, fy, fz, st);
-    case 7: return rbgs_dispatch<T, 64, 16, 512>(var, zero_src, bl, tiles, ntiles, zc, src, dst, rhs, fx, fy, fz, st);
+    case 0: return rbgs_dispatch<T, 32, 16, 256>(var, zero_src, bl, tiles, ntiles, zc, src, dst, rhs, fx, fy, fz, om, st);
+    case 1: return rbgs_dispatch<T, 32, 8, 256>(var, zero_src, bl, tiles, ntiles, zc, src, dst, rhs, fx, fy, fz, om, st);
+    case 2: return rbgs_dispatch<T, 64, 8, 256>(var, zero_src, bl, tiles, ntiles, zc, src, dst, rhs, fx, fy, fz, om, st);
+    case 3: return rbgs_dispatch<T, 16, 8, 128>(var, zero_src, bl, tiles, ntiles, zc, src, dst, rhs, fx, fy, fz, om, st);
+    case 4: return rbgs_dispatch<T, 8, 8, 64>(var, zero_src, bl, tiles, ntiles, zc, src, dst, rhs, fx, fy, fz, om, st);
+    case 5: return rbgs_dispatch<T, 8, 4, 32>(var, zero_src, bl, tiles, ntiles, zc, src, dst, rhs, fx, fy, fz, om, st);
+    case 6: return rbgs_dispatch<T, 4, 4, 32>(var, zero_src, bl, tiles, ntiles, zc, src, dst, rhs, fx, fy, fz, om, st);
+    case 7: return rbgs_dispatch<T, 64, 16, 512>(var, zero_src, bl, tiles, ntiles, zc, src, dst, rhs, fx, fy, fz, om, st);
 #define X(v, tpr, cp, ty) \
-    case v: return rows_dispatch<T, tpr, cp, ty>(var, zero_src, bl, tiles, ntiles, zc, src, dst, rhs, fx, fy, fz, st);
+    case v: return rows_dispatch<T, tpr, cp, ty>(var, zero_src, bl, tiles, ntiles, zc, src, dst, rhs, fx, fy, fz, om, st);
     H3D_ROW_SHAPES(X)
 #undef X
 #define X(v, tpr, cp, ty, d) \
-    case v: return tma2_dispatch<T, tpr, cp, ty, d>(var, bl, tiles, ntiles, zc, maps, rmaps, err, dst, fx, fy, fz, st);
+    case v: return tma2_dispatch<T, tpr, cp, ty, d>(var, bl, tiles, ntiles, zc, maps, rmaps, err, dst, fx, fy, fz, om, st);
     H3D_TMA2_SHAPES(X)
 #undef X
     default: return cudaErrorInvalidValue;
@@ -2328,7 +2341,7 @@ template <typename T, bool VAR>
 __device__ void small_relax(const BlkLev* sb, const int* ss, int nb, T* __restrict__ phi, const T* __restrict__ rhs,
                             const T* __restrict__ fx, const T* __restrict__ fy, const T* __restrict__ fz,
                             const uint32_t* __restrict__ fdst, const uint32_t* __restrict__ fsrc, int nfill,
-                            int sweeps, int zero, long long nelems) {
+                            int sweeps, int zero, long long nelems, float om) {
   const int ncell = ss[nb];
   if (zero) {
     for (long long q = threadIdx.x; q < nelems; q += blockDim.x) phi[q] = T(0);
@@ -2347,9 +2360,10 @@ __device__ void small_relax(const BlkLev* sb, const int* ss, int nb, T* __restri
         const Coef<T> cf = cell_coef<T, VAR>(B, x, y, z, i - B.off, VAR ? fx + B.off : nullptr,
                                              VAR ? fy + B.off : nullptr, VAR ? fz + B.off : nullptr);
         const T ap = coef_ap(cf);
-        const T v = gs_div(rhs[i] - (cf.aw * phi[i - 1] + cf.ae * phi[i + 1] + cf.as * phi[i - B.sx] +
-                                     cf.an * phi[i + B.sx] + cf.ab * phi[i - B.sxy] + cf.at * phi[i + B.sxy]),
-                           ap);
+        T v = gs_div(rhs[i] - (cf.aw * phi[i - 1] + cf.ae * phi[i + 1] + cf.as * phi[i - B.sx] +
+                               cf.an * phi[i + B.sx] + cf.ab * phi[i - B.sxy] + cf.at * phi[i + B.sxy]),
+                     ap);
+        if constexpr (sizeof(T) == 4) v = sorf(phi[i], v, om);
         phi[i] = v;
       }
       __syncthreads();
@@ -2368,7 +2382,8 @@ __global__ void __launch_bounds__(1024) k_relax_blocks(const BlkLev* __restrict_
                                                        T* __restrict__ phi, const T* __restrict__ rhs,
                                                        const T* __restrict__ fx, const T* __restrict__ fy,
                                                        const T* __restrict__ fz, const uint32_t* __restrict__ fdst,
-                                                       const uint32_t* __restrict__ fsrc, int sweeps, int zero) {
+                                                       const uint32_t* __restrict__ fsrc, int sweeps, int zero,
+                                                       float om) {
   pdl_trigger();
   const BlkLev B = bls[blockIdx.x];
   const int f0 = fstart[blockIdx.x], f1 = fstart[blockIdx.x + 1];
@@ -2388,9 +2403,10 @@ __global__ void __launch_bounds__(1024) k_relax_blocks(const BlkLev* __restrict_
         const Coef<T> cf = cell_coef<T, VAR>(B, x, y, z, i - B.off, VAR ? fx + B.off : nullptr,
                                              VAR ? fy + B.off : nullptr, VAR ? fz + B.off : nullptr);
         const T ap = coef_ap(cf);
-        const T v = gs_div(rhs[i] - (cf.aw * phi[i - 1] + cf.ae * phi[i + 1] + cf.as * phi[i - B.sx] +
-                                     cf.an * phi[i + B.sx] + cf.ab * phi[i - B.sxy] + cf.at * phi[i + B.sxy]),
-                           ap);
+        T v = gs_div(rhs[i] - (cf.aw * phi[i - 1] + cf.ae * phi[i + 1] + cf.as * phi[i - B.sx] +
+                               cf.an * phi[i + B.sx] + cf.ab * phi[i - B.sxy] + cf.at * phi[i + B.sxy]),
+                     ap);
+        if constexpr (sizeof(T) == 4) v = sorf(phi[i], v, om);
         phi[i] = v;
       }
       __syncthreads();
@@ -2406,7 +2422,7 @@ __global__ void __launch_bounds__(1024) k_relax_small(const BlkLev* __restrict__
                                                       const T* __restrict__ fx, const T* __restrict__ fy,
                                                       const T* __restrict__ fz, const uint32_t* __restrict__ fdst,
                                                       const uint32_t* __restrict__ fsrc, int nfill, int sweeps,
-                                                      int zero, long long nelems) {
+                                                      int zero, long long nelems, float om) {
   pdl_trigger();
   __shared__ BlkLev sb[kSmallLevelBlocks];
   __shared__ int ss[kSmallLevelBlocks + 1];
@@ -2416,7 +2432,7 @@ __global__ void __launch_bounds__(1024) k_relax_small(const BlkLev* __restrict__
   for (int b = threadIdx.x; b <= nb; b += blockDim.x) ss[b] = start[b];
   pdl_wait();
   __syncthreads();
-  small_relax<T, VAR>(sb, ss, nb, phi, rhs, fx, fy, fz, fdst, fsrc, nfill, sweeps, zero, nelems);
+  small_relax<T, VAR>(sb, ss, nb, phi, rhs, fx, fy, fz, fdst, fsrc, nfill, sweeps, zero, nelems, om);
 }
 
 // The fused coarse tail keeps every tail level in shared memory, in a
@@ -2448,8 +2464,9 @@ __device__ __forceinline__ long long global_index(const BlkLev& G, int x, int y,
 // The red then the black cells of one in-place sweep of a tail level; same
 // cell arithmetic as small_relax.
 template <typename T>
-__device__ void tail_colours(const BlkLev* cb, const TailLevel& L, T* phi, const T* rhs) {
+__device__ void tail_colours(const BlkLev* cb, const TailLevel& L, T* phi, const T* rhs, int only = -1) {
   for (int colour = 0; colour < 2; ++colour) {  // red (x+y+z odd) first
+    if (only >= 0 && colour != only) continue;
     const int k0 = colour ? L.nred : 0, k1 = colour ? L.nint : L.nred;
     for (int k = k0 + threadIdx.x; k < k1; k += blockDim.x) {
       const CellRef c = cell_ref(L.cells[k]);
@@ -2457,10 +2474,11 @@ __device__ void tail_colours(const BlkLev* cb, const TailLevel& L, T* phi, const
       const int i = c.i;
       const Coef<T> cf = cell_coef<T, false>(B, c.x, c.y, c.z, i - B.off, nullptr, nullptr, nullptr);
       const T ap = coef_ap(cf);
-      const T v = gs_div(rhs[rhs_index(B, c.x, c.y, c.z)] -
-                             (cf.aw * phi[i - 1] + cf.ae * phi[i + 1] + cf.as * phi[i - B.sx] +
-                              cf.an * phi[i + B.sx] + cf.ab * phi[i - B.sxy] + cf.at * phi[i + B.sxy]),
-                         ap);
+      T v = gs_div(rhs[rhs_index(B, c.x, c.y, c.z)] -
+                       (cf.aw * phi[i - 1] + cf.ae * phi[i + 1] + cf.as * phi[i - B.sx] +
+                        cf.an * phi[i + B.sx] + cf.ab * phi[i - B.sxy] + cf.at * phi[i + B.sxy]),
+                   ap);
+      if constexpr (sizeof(T) == 4) v = sorf(phi[i], v, L.om);
       phi[i] = v;
     }
     __syncthreads();
@@ -2472,6 +2490,14 @@ __device__ void tail_colours(const BlkLev* cb, const TailLevel& L, T* phi, const
 template <typename T>
 __device__ void tail_relax(const BlkLev* cb, const TailLevel& L, T* phi, const T* rhs, int sweeps) {
   for (int it = 0; it < sweeps; ++it) {
+    if (L.rb_global) {  // a fill after each colour: the red-black order across block faces
+      for (int colour = 0; colour < 2; ++colour) {
+        tail_colours<T>(cb, L, phi, rhs, colour);
+        for (int q = threadIdx.x; q < L.nfill; q += blockDim.x) phi[L.fdst[q]] = phi[L.fsrc[q]];
+        __syncthreads();
+      }
+      continue;
+    }
     tail_colours<T>(cb, L, phi, rhs);
     for (int q = threadIdx.x; q < L.nfill; q += blockDim.x) phi[L.fdst[q]] = phi[L.fsrc[q]];
     __syncthreads();
@@ -2773,15 +2799,18 @@ __global__ void __launch_bounds__(kClusterTailThreads) k_coarse_cluster(const Ta
             for (int q = threadIdx.x; q < F.npad; q += blockDim.x) phi[q] = T(0);
             __syncthreads();
           }
+          const int ncol = F.rb_global ? 2 : 1;  // 2: a fill after each colour (order across blocks)
           for (int it = 0; it < op.sweeps; ++it) {
-            tail_colours<T>(fb, F, phi, rhs);
-            cl.sync();  // every block's sweep done
-            for (int q = threadIdx.x; q < F.nfill; q += blockDim.x) {  // (dst, src) pairs of this block
-              const uint32_t dsti = F.fdst[2 * q], src = F.fdst[2 * q + 1];
-              const T* remote = cl.map_shared_rank(phi, (int)(src >> 24));
-              phi[dsti] = remote[src & 0xffffffu];
+            for (int pass = 0; pass < ncol; ++pass) {
+              tail_colours<T>(fb, F, phi, rhs, ncol == 2 ? pass : -1);
+              cl.sync();  // every block's sweep done
+              for (int q = threadIdx.x; q < F.nfill; q += blockDim.x) {  // (dst, src) pairs of this block
+                const uint32_t dsti = F.fdst[2 * q], src = F.fdst[2 * q + 1];
+                const T* remote = cl.map_shared_rank(phi, (int)(src >> 24));
+                phi[dsti] = remote[src & 0xffffffu];
+              }
+              cl.sync();  // every ghost gathered before any interior changes
             }
-            cl.sync();  // every ghost gathered before any interior changes
           }
         };
         if (op.f64) relax(at64(F.s_phi64), (const double*)at64(F.s_rhs64));
@@ -2911,40 +2940,40 @@ cudaError_t launch_coarse_tail(const TailLevel* lv, const TailOp* ops, int nops,
 template <typename T>
 cudaError_t launch_relax_small(bool var, const BlkLev* bl, const int* start, int nb, T* phi, const T* rhs,
                                const T* fx, const T* fy, const T* fz, const uint32_t* fdst, const uint32_t* fsrc,
-                               int nfill, int sweeps, bool zero, long long nelems, cudaStream_t st) {
+                               int nfill, int sweeps, bool zero, long long nelems, float om, cudaStream_t st) {
   if (var)
     pdl_launch(k_relax_small<T, true>, 1, 1024, 0, st, bl, start, nb, phi, rhs, fx, fy, fz, fdst, fsrc, nfill, sweeps,
-               (int)zero, nelems);
+               (int)zero, nelems, om);
   else
     pdl_launch(k_relax_small<T, false>, 1, 1024, 0, st, bl, start, nb, phi, rhs, fx, fy, fz, fdst, fsrc, nfill,
-               sweeps, (int)zero, nelems);
+               sweeps, (int)zero, nelems, om);
   return cudaGetLastError();
 }
 template <typename T>
 cudaError_t launch_relax_blocks(bool var, const BlkLev* bl, int nb, const int* fstart, T* phi, const T* rhs,
                                 const T* fx, const T* fy, const T* fz, const uint32_t* fdst, const uint32_t* fsrc,
-                                int sweeps, bool zero, cudaStream_t st) {
+                                int sweeps, bool zero, float om, cudaStream_t st) {
   if (nb <= 0) return cudaSuccess;
   if (var)
     pdl_launch(k_relax_blocks<T, true>, nb, 1024, 0, st, bl, fstart, phi, rhs, fx, fy, fz, fdst, fsrc, sweeps,
-               (int)zero);
+               (int)zero, om);
   else
     pdl_launch(k_relax_blocks<T, false>, nb, 1024, 0, st, bl, fstart, phi, rhs, fx, fy, fz, fdst, fsrc, sweeps,
-               (int)zero);
+               (int)zero, om);
   return cudaGetLastError();
 }
 template cudaError_t launch_relax_blocks<double>(bool, const BlkLev*, int, const int*, double*, const double*,
                                                  const double*, const double*, const double*, const uint32_t*,
-                                                 const uint32_t*, int, bool, cudaStream_t);
+                                                 const uint32_t*, int, bool, float, cudaStream_t);
 template cudaError_t launch_relax_blocks<float>(bool, const BlkLev*, int, const int*, float*, const float*,
                                                 const float*, const float*, const float*, const uint32_t*,
-                                                const uint32_t*, int, bool, cudaStream_t);
+                                                const uint32_t*, int, bool, float, cudaStream_t);
 template cudaError_t launch_relax_small<double>(bool, const BlkLev*, const int*, int, double*, const double*,
                                                 const double*, const double*, const double*, const uint32_t*,
-                                                const uint32_t*, int, int, bool, long long, cudaStream_t);
+                                                const uint32_t*, int, int, bool, long long, float, cudaStream_t);
 template cudaError_t launch_relax_small<float>(bool, const BlkLev*, const int*, int, float*, const float*,
                                                const float*, const float*, const float*, const uint32_t*,
-                                               const uint32_t*, int, int, bool, long long, cudaStream_t);
+                                               const uint32_t*, int, int, bool, long long, float, cudaStream_t);
 
 template <typename T>
 cudaError_t launch_fill(const uint32_t* dsts, const uint32_t* srcs, int64_t n, T* out, const T* cur, const T* old,
@@ -2953,6 +2982,51 @@ cudaError_t launch_fill(const uint32_t* dsts, const uint32_t* srcs, int64_t n, T
   int g = grid_for(n, 256);
   if (zero_old) pdl_launch(k_fill<T, true>, g, 256, 0, st, dsts, srcs, n, out, cur, old);
   else pdl_launch(k_fill<T, false>, g, 256, 0, st, dsts, srcs, n, out, cur, old);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Red values ahead of an FP32 sweep, for a red-black order across block faces.
+// Inside one sweep a block's black cells read the cells across a block face
+// from its ghost layer, which otherwise holds the values of before the sweep
+// (the reference's order, mgsolver.for:614-615).  Entry e names a red
+// interior cell src[e] of block blk[e] next to a face that another block (or a
+// periodic partner) reads, and the ghost cell dst[e] that shows it there; the
+// red update of src[e] is computed from the iterate (its six neighbours are
+// black, still of before the sweep) and stored at dst[e], in place.  With even
+// block sizes a ghost cell of red colour is read by black cells only, so the
+// sweep's red cells still see their old black neighbours, and no entry reads a
+// cell another entry writes.
+template <bool VAR>
+__global__ void __launch_bounds__(256) k_red_ahead(const uint32_t* __restrict__ dst, const uint32_t* __restrict__ src,
+                                                   const int* __restrict__ blk, int64_t n,
+                                                   const BlkLev* __restrict__ bls, float* __restrict__ phi,
+                                                   const float* __restrict__ rhs, const float* __restrict__ fx,
+                                                   const float* __restrict__ fy, const float* __restrict__ fz,
+                                                   float om) {
+  pdl_trigger();
+  pdl_wait();
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+    const long long gi = src[e];
+    const BlkLev B = bls[blk[e]];
+    const long long i = gi - B.off;
+    const int z = (int)(i / B.sxy), y = (int)((i % B.sxy) / B.sx), x = (int)(i % B.sx);
+    const Coef<float> c = cell_coef<float, VAR>(B, x, y, z, i, VAR ? fx + B.off : nullptr,
+                                                VAR ? fy + B.off : nullptr, VAR ? fz + B.off : nullptr);
+    const float* P = phi + gi;
+    const float sum = fmaf(c.at, P[B.sxy], fmaf(c.ab, P[-B.sxy], fmaf(c.an, P[B.sx], fmaf(c.as, P[-B.sx],
+                      fmaf(c.ae, P[1], c.aw * P[-1])))));
+    phi[dst[e]] = sorf(P[0], (rhs[gi] - sum) * (1.f / coef_ap(c)), om);
+  }
+}
+
+cudaError_t launch_red_ahead(bool var, const uint32_t* dst, const uint32_t* src, const int* blk, int64_t n,
+                             const BlkLev* bl, float* phi, const float* rhs, const float* fx, const float* fy,
+                             const float* fz, float om, cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  const int g = grid_for(n, 256);
+  if (var) pdl_launch(k_red_ahead<true>, g, 256, 0, st, dst, src, blk, n, bl, phi, rhs, fx, fy, fz, om);
+  else pdl_launch(k_red_ahead<false>, g, 256, 0, st, dst, src, blk, n, bl, phi, rhs, fx, fy, fz, om);
   return cudaGetLastError();
 }
 
@@ -4284,10 +4358,10 @@ cudaError_t launch_face_coef(const BlkLev* bl, CellTab ct, const double* dens, c
 // explicit instantiations
 template cudaError_t launch_rbgs<double>(int, bool, bool, const BlkLev*, const Tile*, int, int, const CUtensorMap*,
                                          const CUtensorMap*, int*, const double*, double*, const double*, const double*, const double*,
-                                         const double*, const long long*, cudaStream_t);
+                                         const double*, const long long*, float, cudaStream_t);
 template cudaError_t launch_rbgs<float>(int, bool, bool, const BlkLev*, const Tile*, int, int, const CUtensorMap*,
                                         const CUtensorMap*, int*, const float*, float*, const float*, const float*, const float*,
-                                        const float*, const long long*, cudaStream_t);
+                                        const float*, const long long*, float, cudaStream_t);
 template cudaError_t launch_fill<double>(const uint32_t*, const uint32_t*, int64_t, double*, const double*,
                                          const double*, bool, cudaStream_t);
 template cudaError_t launch_fill<float>(const uint32_t*, const uint32_t*, int64_t, float*, const float*, const float*,

@@ -86,7 +86,7 @@ cudaError_t launch_rbgs(int variant, bool var, bool zero_src, const BlkLev* bl, 
                         int ntiles, int zc, const CUtensorMap* maps, const CUtensorMap* rmaps, int* err,
                         const T* src, T* dst,
                         const T* rhs, const T* fx, const T* fy,
-                        const T* fz, const long long* push, cudaStream_t st);
+                        const T* fz, const long long* push, float om, cudaStream_t st);
 
 constexpr int kSmallLevelBlocks = 64;  // block descriptors the fused small-level kernel caches
 // `sweeps` red-black sweeps of a small level, each followed by its ghost fill,
@@ -115,6 +115,8 @@ struct TailLevel {
   int s_cells, s_fill;  // cluster tail: arena offsets of the staged cell tables and this block's fill pairs
   const double* dense;  // coarsest level solved directly: its pseudo-inverse, dense_n x dense_n, row-major
   int dense_n;
+  float om;             // over-relaxation of the level's FP32 sweeps (1: Gauss-Seidel)
+  int rb_global;        // 1: a ghost fill after each colour (red-black order across block faces)
 };
 enum TailKind {
   kTailRelax = 0,
@@ -157,7 +159,7 @@ cudaError_t launch_coarse_cluster(int nb, const TailLevel* lv, int nlev, const T
 // level (every block's nx a multiple of 4, at most 1024): tiles (block, y0 =
 // first row, z0 = first plane) of 256 / (nx/4) rows and zc planes.
 cudaError_t launch_rbgs_zero32(const BlkLev* bl, const Tile* tiles, int ntiles, int zc, const float* rhs, float* dst,
-                               const long long* push, cudaStream_t st);
+                               const long long* push, float om, cudaStream_t st);
 // Lexicographic Gauss-Seidel (itrsch 1) or line-TDMA (itrsch 2) sweep of
 // every block of a level, one CTA per block (bit-exact wavefront orderings
 // of mgsolver.for:407-549); acoef: level-sized scratch of the TDMA.
@@ -167,12 +169,18 @@ cudaError_t launch_seq_smoother(int itrsch, bool var, bool zero, const BlkLev* b
 template <typename T>
 cudaError_t launch_relax_small(bool var, const BlkLev* bl, const int* start, int nb, T* phi, const T* rhs,
                                const T* fx, const T* fy, const T* fz, const uint32_t* fdst, const uint32_t* fsrc,
-                               int nfill, int sweeps, bool zero, long long nelems, cudaStream_t st);
+                               int nfill, int sweeps, bool zero, long long nelems, float om, cudaStream_t st);
 
 // Ghost gather: out[dst[e]] = (src[e] & old) ? old[src] : cur[src].
 template <typename T>
 cudaError_t launch_fill(const uint32_t* dsts, const uint32_t* srcs, int64_t n, T* out, const T* cur,
                         const T* old, bool zero_old, cudaStream_t st);
+
+// Red updates of the red cells next to block faces, stored at the ghost cells
+// that show them to other blocks (FP32, before a sweep; see k_red_ahead).
+cudaError_t launch_red_ahead(bool var, const uint32_t* dst, const uint32_t* src, const int* blk, int64_t n,
+                             const BlkLev* bl, float* phi, const float* rhs, const float* fx, const float* fy,
+                             const float* fz, float om, cudaStream_t st);
 
 // Residual of the fine level and 8-cell average into the coarse rhs
 // (mgrestr, mgsolver.for:693-756).  zero_phi: fine iterate is zero.
@@ -259,7 +267,7 @@ cudaError_t launch_face_coef_sum(const BlkLev* fine, const BlkLev* coarse, CellT
 template <typename T>
 cudaError_t launch_relax_blocks(bool var, const BlkLev* bl, int nb, const int* fstart, T* phi, const T* rhs,
                                 const T* fx, const T* fy, const T* fz, const uint32_t* fdst, const uint32_t* fsrc,
-                                int sweeps, bool zero, cudaStream_t st);
+                                int sweeps, bool zero, float om, cudaStream_t st);
 
 // Stone's SIP (sipsol.for) on level 1: factor arrays and the residual
 // (level-1 layout, zero outside the interior).

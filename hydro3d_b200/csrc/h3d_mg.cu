@@ -81,6 +81,9 @@ struct Level {
   Halo sweep_push;              // the sweep fill without the faces the register-window sweeps push
   Halo live, live_push;         // the parts of sweep / sweep_push that the next sweep or restriction reads
   bool live_ok = false;         // live fills may stand in for the full fill (FP32 RBGS levels)
+  Halo red;                     // red cells next to block faces and the ghosts that show them (k_red_ahead)
+  int* d_red_blk = nullptr;     // their blocks
+  bool red_ok = false;          // FP32 sweeps of this level take the red-black order across block faces
   long long* d_push = nullptr;  // per block, six ghost push offsets (kNoPush: none)
   bool push_ok = false;
   CUtensorMap* d_maps = nullptr;  // [ty index][0,1: iterate buffer, 2: rhs][block] tensor maps
@@ -187,6 +190,8 @@ struct h3d_mg {
   int dense_n = 0;
   int tail_nops = 0;
   int tail_smem = 0;  // dynamic shared memory of the tail launch
+  float omega = 1.f;       // over-relaxation of the FP32 sweeps (desc.omega)
+  bool rb_global = false;  // FP32 sweeps take the red-black order across block faces (desc.rb_order)
   std::vector<char> tail_zero32, tail_zero64;  // zero flags of the tail levels after the tail
   // the projection (allocated on first use): face velocities u, v, w and
   // ustar, vstar, wstar in the level-1 layout, and the gather table of their
@@ -568,6 +573,13 @@ struct Exec {
     // profiling brackets the full level-1 sweeps (3 words a cell); the first
     // sweep from a zero iterate is another kernel with other bytes
     const bool from_zero = mixed_level(g) ? V.zero32 : V.zero64;
+    if (h->desc.mg_itrsch == 3 && mixed_level(g) && V.red_ok && !V.zero32) {
+      // the red cells next to block faces first: red-black order across blocks
+      CU(launch_red_ahead(h->var, V.red.d_dst, V.red.d_src, V.d_red_blk, V.red.n, V.d_bl, V.phi32[V.cur32], V.rhs32,
+                          V.fx32, V.fy32, V.fz32, h->omega, st));
+      TRY(chk("red ahead", g));
+      h->kernels += 1;
+    }
     if (prof && g == 1 && !from_zero && prof_used + 2 <= prof->size()) {
       e0 = (*prof)[prof_used++];
       e1 = (*prof)[prof_used++];
@@ -606,7 +618,8 @@ struct Exec {
       float* src = V.phi32[V.cur32];
       float* dst = V.phi32[1 - V.cur32];
       const bool push = V.push_ok;
-      CU(launch_rbgs_zero32(V.d_bl, V.d_ztiles, V.nztiles, V.zzc, V.rhs32, dst, push ? V.d_push : nullptr, st));
+      CU(launch_rbgs_zero32(V.d_bl, V.d_ztiles, V.nztiles, V.zzc, V.rhs32, dst, push ? V.d_push : nullptr, h->omega,
+                            st));
       TRY(chk("zero-source sweep fp32", g));
       if (e1) CU(record(e1));
       const Halo& fill = partial && V.live_ok ? (push ? V.live_push : V.live) : (push ? V.sweep_push : V.sweep);
@@ -623,7 +636,7 @@ struct Exec {
       const bool push = V.push_ok && rbgs_pushes(V.variant, h->var, true);
       CU(launch_rbgs<float>(V.variant, h->var, V.zero32, V.d_bl, V.d_tiles, V.ntiles, V.zc, sweep_maps(V, V.cur32),
                             rhs_maps(V), h->d_err, src, dst, V.rhs32,
-                            V.fx32, V.fy32, V.fz32, push ? V.d_push : nullptr, st));
+                            V.fx32, V.fy32, V.fz32, push ? V.d_push : nullptr, h->omega, st));
       TRY(chk("sweep fp32", g));
       if (e1) CU(record(e1));
       const Halo& fill = partial && V.live_ok ? (push ? V.live_push : V.live) : (push ? V.sweep_push : V.sweep);
@@ -636,7 +649,7 @@ struct Exec {
       double* dst = V.phi64[1 - V.cur64];
       CU(launch_rbgs<double>(V.variant, h->var, V.zero64, V.d_bl, V.d_tiles, V.ntiles, V.zc, sweep_maps(V, V.cur64),
                              rhs_maps(V), h->d_err, src, dst, V.rhs64,
-                             V.fx64, V.fy64, V.fz64, nullptr, st));
+                             V.fx64, V.fy64, V.fz64, nullptr, 1.f, st));
       TRY(chk("sweep fp64", g));
       if (e1) CU(record(e1));
       TRY(sweep_fill<double>(V, V.sweep, dst, src, V.zero64, &h->kernels));
@@ -657,12 +670,12 @@ struct Exec {
       if (mixed_level(g)) {
         CU(launch_relax_small<float>(h->var, V.d_bl, V.d_cstart, nb, V.phi32[V.cur32], V.rhs32, V.fx32, V.fy32,
                                      V.fz32, V.sweep.d_dst, V.sweep.d_src, (int)V.sweep.n, it, V.zero32,
-                                     V.geom.n_elems, h->st));
+                                     V.geom.n_elems, h->omega, h->st));
         V.zero32 = false;
       } else {
         CU(launch_relax_small<double>(h->var, V.d_bl, V.d_cstart, nb, V.phi64[V.cur64], V.rhs64, V.fx64, V.fy64,
                                       V.fz64, V.sweep.d_dst, V.sweep.d_src, (int)V.sweep.n, it, V.zero64,
-                                      V.geom.n_elems, h->st));
+                                      V.geom.n_elems, 1.f, h->st));
         V.zero64 = false;
       }
       TRY(chk("relax small", g));
@@ -673,11 +686,11 @@ struct Exec {
       const int nb = (int)V.geom.bl.size();
       if (mixed_level(g)) {
         CU(launch_relax_blocks<float>(h->var, V.d_bl, nb, V.d_lfstart, V.phi32[V.cur32], V.rhs32, V.fx32, V.fy32,
-                                      V.fz32, V.lfill.d_dst, V.lfill.d_src, it, V.zero32, h->st));
+                                      V.fz32, V.lfill.d_dst, V.lfill.d_src, it, V.zero32, h->omega, h->st));
         V.zero32 = false;
       } else {
         CU(launch_relax_blocks<double>(h->var, V.d_bl, nb, V.d_lfstart, V.phi64[V.cur64], V.rhs64, V.fx64, V.fy64,
-                                       V.fz64, V.lfill.d_dst, V.lfill.d_src, it, V.zero64, h->st));
+                                       V.fz64, V.lfill.d_dst, V.lfill.d_src, it, V.zero64, 1.f, h->st));
         V.zero64 = false;
       }
       TRY(chk("relax blocks", g));
@@ -1323,10 +1336,11 @@ int autotune_level(h3d_mg* h, int g) {
         const long long* push = (f32 && V.push_ok && rbgs_pushes(v, h->var, true)) ? V.d_push : nullptr;
         if (f32) CU(launch_rbgs<float>(v, h->var, zero, V.d_bl, V.d_tiles, V.ntiles, zc, sweep_maps(V, V.cur32),
                                        rhs_maps(V), h->d_err, V.phi32[V.cur32],
-                                       V.phi32[1 - V.cur32], V.rhs32, V.fx32, V.fy32, V.fz32, push, h->st));
+                                       V.phi32[1 - V.cur32], V.rhs32, V.fx32, V.fy32, V.fz32, push, h->omega,
+                                       h->st));
         else CU(launch_rbgs<double>(v, h->var, zero, V.d_bl, V.d_tiles, V.ntiles, zc, sweep_maps(V, V.cur64),
                                     rhs_maps(V), h->d_err, V.phi64[V.cur64],
-                                    V.phi64[1 - V.cur64], V.rhs64, V.fx64, V.fy64, V.fz64, nullptr, h->st));
+                                    V.phi64[1 - V.cur64], V.rhs64, V.fx64, V.fy64, V.fz64, nullptr, 1.f, h->st));
         CU(cudaEventRecord(b, h->st));
         {
           cudaError_t e = cudaEventSynchronize(b);
@@ -1355,7 +1369,8 @@ int autotune_level(h3d_mg* h, int g) {
     for (int rep = 0; rep < 6; ++rep) {
       TRY(flush_l2(h));
       CU(cudaEventRecord(a, h->st));
-      CU(launch_rbgs_zero32(V.d_bl, V.d_ztiles, V.nztiles, V.zzc, V.rhs32, V.phi32[1 - V.cur32], push, h->st));
+      CU(launch_rbgs_zero32(V.d_bl, V.d_ztiles, V.nztiles, V.zzc, V.rhs32, V.phi32[1 - V.cur32], push, h->omega,
+                            h->st));
       CU(cudaEventRecord(b, h->st));
       CU(cudaEventSynchronize(b));
       float t;
@@ -1579,10 +1594,42 @@ bool live_entries(const LevelGeom& G, const std::vector<uint32_t>& d, const std:
   return true;
 }
 
+// The red cells among the sources of a level's live fill (every block of even
+// size, so that colours agree across block faces), for k_red_ahead.
+int build_red_ahead(h3d_mg* h, Level& V, const std::vector<uint32_t>& ld, const std::vector<uint32_t>& ls) {
+  const auto& G = V.geom;
+  for (const auto& B : G.bl)
+    if ((B.nx | B.ny | B.nz) & 1) return H3D_OK;
+  std::vector<uint32_t> rd, rs;
+  std::vector<int> rb;
+  for (size_t e = 0; e < ld.size(); ++e) {
+    const long long gi = ls[e] & kIdxMask;
+    for (int q = 0; q < (int)G.bl.size(); ++q) {
+      const BlkLev& B = G.bl[q];
+      if (gi < B.off || gi >= B.off + B.sxy * (B.nz + 2)) continue;
+      const long long l = gi - B.off;
+      const int z = (int)(l / B.sxy), y = (int)((l % B.sxy) / B.sx), x = (int)(l % B.sx);
+      if ((x + y + z) & 1) {  // red
+        rd.push_back(ld[e]);
+        rs.push_back(ls[e]);
+        rb.push_back(q);
+      }
+      break;
+    }
+  }
+  if (rd.empty()) return H3D_OK;
+  TRY(upload_halo(h, V.red, rd, rs));
+  TRY(dalloc(h, &V.d_red_blk, rb.size()));
+  CU(cudaMemcpy(V.d_red_blk, rb.data(), rb.size() * sizeof(int), cudaMemcpyHostToDevice));
+  V.red_ok = true;
+  return H3D_OK;
+}
+
 int build_live(h3d_mg* h, Level& V, const std::vector<uint32_t>& d, const std::vector<uint32_t>& s) {
   std::vector<uint32_t> ld, ls;
   V.live_ok = live_entries(V.geom, d, s, &ld, &ls);
   if (V.live_ok) TRY(upload_halo(h, V.live, ld, ls));
+  if (V.live_ok && h->mixed && h->desc.mg_itrsch == 3 && h->rb_global) TRY(build_red_ahead(h, V, ld, ls));
   return H3D_OK;
 }
 
@@ -1944,6 +1991,8 @@ int build_tail(h3d_mg* h) {
     t.phi64[0] = V.phi64[0];
     t.phi64[1] = V.phi64[1];
     t.rhs64 = V.rhs64;
+    t.om = f32_level(h, q) ? h->omega : 1.f;
+    t.rb_global = f32_level(h, q) && h->rb_global ? 1 : 0;
     t.s_phi32 = plan.s_phi32[k];
     t.s_rhs32 = plan.s_rhs32[k];
     t.s_phi64 = plan.s_phi64[k];
@@ -2261,6 +2310,8 @@ int build_cluster_tail(h3d_mg* h) {
     t.s_fill = l.s_fill;
     t.dense = q == Lv ? h->d_dense : nullptr;
     t.dense_n = q == Lv ? h->dense_n : 0;
+    t.om = f32_level(h, q) ? h->omega : 1.f;
+    t.rb_global = f32_level(h, q) && h->rb_global ? 1 : 0;
     lv.push_back(t);
   }
   // every block's fill list must fit its staged region
@@ -2301,7 +2352,7 @@ int h3d_mg_destroy(h3d_mg* h) {
     void* ps[] = {V.d_bl, V.d_cta_all, V.d_cta_int, V.d_rows_all, V.d_rows_int, V.d_tiles, V.phi64[0], V.phi64[1], V.rhs64, V.phi32[0],
                   V.phi32[1], V.rhs32, V.fx64, V.fy64, V.fz64, V.fx32, V.fy32, V.fz32, V.dens,
                   V.sweep.d_dst, V.sweep.d_src, V.faces.d_dst, V.faces.d_src, V.exch.d_dst, V.exch.d_src,
-                  V.bound.d_dst, V.bound.d_src, V.sweep_push.d_dst, V.sweep_push.d_src, V.live.d_dst, V.live.d_src, V.live_push.d_dst, V.live_push.d_src, V.d_push, V.d_maps, V.d_rmaps, V.d_rtiles, V.d_ptiles, V.d_qtiles, V.d_dtiles, V.d_cstart, V.d_dstart, V.d_pstart, V.seq64, V.seq32, V.d_ztiles, V.lfill.d_dst, V.lfill.d_src, V.d_lfstart,
+                  V.bound.d_dst, V.bound.d_src, V.sweep_push.d_dst, V.sweep_push.d_src, V.live.d_dst, V.live.d_src, V.live_push.d_dst, V.live_push.d_src, V.red.d_dst, V.red.d_src, V.d_red_blk, V.d_push, V.d_maps, V.d_rmaps, V.d_rtiles, V.d_ptiles, V.d_qtiles, V.d_dtiles, V.d_cstart, V.d_dstart, V.d_pstart, V.seq64, V.seq32, V.d_ztiles, V.lfill.d_dst, V.lfill.d_src, V.d_lfstart,
                   V.xs.d_nodes, V.xs.d_dst, V.xs.d_src, V.xe.d_nodes, V.xe.d_dst, V.xe.d_src, V.xscratch, V.d_rsame,
                   V.d_psame, V.d_prows};
     for (void* p : ps) dfree(p);
@@ -2397,6 +2448,9 @@ int h3d_mg_create(h3d_mg** out, const h3d_mg_desc* desc) {
   }
   if (lmr && D.var_coef)
     return fail(nullptr, H3D_ERR_BAD_CONFIG, "local mesh refinement with L_LSM coefficients is not supported");
+  if (!(D.omega >= 0.f && D.omega < 2.f))
+    return fail(nullptr, H3D_ERR_BAD_CONFIG, "omega must be 0 (Gauss-Seidel) or lie in (0, 2)");
+  if (D.rb_order != 0 && D.rb_order != 1) return fail(nullptr, H3D_ERR_BAD_CONFIG, "rb_order must be 0 or 1");
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= D.device || D.device < 0)
     return fail(nullptr, H3D_ERR_NO_DEVICE, "no CUDA device");
@@ -2420,6 +2474,8 @@ int h3d_mg_create(h3d_mg** out, const h3d_mg_desc* desc) {
   h->mixed = D.precision == H3D_PREC_MIXED;
   h->var = D.var_coef != 0;
   h->lmr = lmr;
+  h->omega = D.omega > 0.f ? D.omega : 1.f;  // FP32 levels only
+  h->rb_global = D.rb_order == 1;
   int rc = H3D_OK;
   auto bail = [&](int r) {
     g_create_error = h->last_error;

@@ -62,7 +62,7 @@ class MultigridSolver:
     def __init__(self, blocks: Sequence, ngrd_gl: int, mg_itrsch: int = 3, irestr: int = 2, iproln: int = 1,
                  maxcy: int = 30, precision: str = "fp64", var_coef: bool = False, device: int = 0,
                  coarse_sweeps: int = 0, inner_cycles: int = 0, use_graph: bool = True, coarse_op: int = 0,
-                 coarse_direct: bool = False):
+                 coarse_direct: bool = False, rb_order: int = 0, omega: float = 0.0):
         self.L = _lib.lib()
         self.blocks = list(blocks)
         self._arr = (_lib.BlockDesc * len(self.blocks))(*self.blocks)
@@ -81,6 +81,8 @@ class MultigridSolver:
         desc.use_graph = int(bool(use_graph))
         desc.coarse_op = coarse_op
         desc.coarse_direct = int(bool(coarse_direct))
+        desc.rb_order = int(rb_order)
+        desc.omega = float(omega)
         desc.blocks = self._arr
         self.ngrd = ngrd_gl
         self.precision = precision

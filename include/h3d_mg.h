@@ -79,6 +79,13 @@ typedef struct h3d_mg_desc {
   int32_t coarse_direct;  /* 1: with coarse_sweeps > 0, solve a small coarsest level (at most
                              512 cells, constant coefficients, symmetric) directly by its
                              pseudo-inverse instead of the sweeps; 0: the sweeps */
+  int32_t rb_order;       /* MIXED, FP32 levels: 0 = the reference's order (a block's black
+                             cells see the other blocks' red cells as they were before the
+                             sweep, mgsolver.for:614-615); 1 = red-black order across block
+                             faces (the red cells next to block faces are computed ahead of
+                             the sweep; the coarse tail fills ghosts after each colour) */
+  float omega;            /* MIXED, FP32 levels: over-relaxation factor of the red-black
+                             sweeps, x + omega (gs - x); 0 = 1 (Gauss-Seidel); below 2 */
   const h3d_block_desc* blocks;
 } h3d_mg_desc;
 

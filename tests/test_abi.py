@@ -43,6 +43,14 @@ def test_strerror_and_create_errors(h3d):
     d.mg_itrsch = 4  # smoothers are 1 (GS-lex), 2 (line TDMA) and 3 (red-black GS)
     assert L.h3d_mg_create(C.byref(h), C.byref(d)) == _lib.H3D_ERR_BAD_CONFIG
     assert b"mg_itrsch" in L.h3d_mg_last_error(None)
+    d.mg_itrsch = 3
+    d.omega = 2.5  # over-relaxation of the FP32 sweeps: 0 (Gauss-Seidel) or in (0, 2)
+    assert L.h3d_mg_create(C.byref(h), C.byref(d)) == _lib.H3D_ERR_BAD_CONFIG
+    assert b"omega" in L.h3d_mg_last_error(None)
+    d.omega = 1.25
+    d.rb_order = 2  # 0: the reference's per-block order, 1: across block faces
+    assert L.h3d_mg_create(C.byref(h), C.byref(d)) == _lib.H3D_ERR_BAD_CONFIG
+    assert b"rb_order" in L.h3d_mg_last_error(None)
 
 
 def test_product_does_not_touch_oracle():
