@@ -2993,40 +2993,54 @@ cudaError_t launch_fill(const uint32_t* dsts, const uint32_t* srcs, int64_t n, T
 // interior cell src[e] of block blk[e] next to a face that another block (or a
 // periodic partner) reads, and the ghost cell dst[e] that shows it there; the
 // red update of src[e] is computed from the iterate (its six neighbours are
-// black, still of before the sweep) and stored at dst[e], in place.  With even
+// black, still of before the sweep) and stored at dst[e], in place.  The
+// block tables are staged in shared memory; info[e] carries the cell's block
+// and wall faces, so no index arithmetic is needed.  With even
 // block sizes a ghost cell of red colour is read by black cells only, so the
 // sweep's red cells still see their old black neighbours, and no entry reads a
 // cell another entry writes.
 template <bool VAR>
 __global__ void __launch_bounds__(256) k_red_ahead(const uint32_t* __restrict__ dst, const uint32_t* __restrict__ src,
-                                                   const int* __restrict__ blk, int64_t n,
+                                                   const int* __restrict__ info, int64_t n, int nb,
                                                    const BlkLev* __restrict__ bls, float* __restrict__ phi,
                                                    const float* __restrict__ rhs, const float* __restrict__ fx,
                                                    const float* __restrict__ fy, const float* __restrict__ fz,
                                                    float om) {
+  __shared__ BlkLev sb[kSmallLevelBlocks];
+  const bool staged = nb <= kSmallLevelBlocks;
   pdl_trigger();
+  if (staged)
+    for (int q = threadIdx.x; q < nb; q += blockDim.x) sb[q] = bls[q];
+  __syncthreads();
   pdl_wait();
   for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+    // info: block (bits 0-15) and the cell's wall faces (bits 16-21, W E S N B T)
     const long long gi = src[e];
-    const BlkLev B = bls[blk[e]];
-    const long long i = gi - B.off;
-    const int z = (int)(i / B.sxy), y = (int)((i % B.sxy) / B.sx), x = (int)(i % B.sx);
-    const Coef<float> c = cell_coef<float, VAR>(B, x, y, z, i, VAR ? fx + B.off : nullptr,
-                                                VAR ? fy + B.off : nullptr, VAR ? fz + B.off : nullptr);
+    const int inf = info[e], m = inf >> 16;
+    const BlkLev& B = staged ? sb[inf & 0xffff] : bls[inf & 0xffff];
+    const long long sx = B.sx, sxy = B.sxy;
+    float aw, ae, as, an, ab, at;
+    if (VAR) {
+      aw = fx[gi - 1]; ae = fx[gi]; as = fy[gi - sx]; an = fy[gi]; ab = fz[gi - sxy]; at = fz[gi];
+    } else {
+      const float ax = (float)B.ax, ay = (float)B.ay, az = (float)B.az;
+      aw = (m & 1) ? 0.f : ax; ae = (m & 2) ? 0.f : ax;
+      as = (m & 4) ? 0.f : ay; an = (m & 8) ? 0.f : ay;
+      ab = (m & 16) ? 0.f : az; at = (m & 32) ? 0.f : az;
+    }
     const float* P = phi + gi;
-    const float sum = fmaf(c.at, P[B.sxy], fmaf(c.ab, P[-B.sxy], fmaf(c.an, P[B.sx], fmaf(c.as, P[-B.sx],
-                      fmaf(c.ae, P[1], c.aw * P[-1])))));
-    phi[dst[e]] = sorf(P[0], (rhs[gi] - sum) * (1.f / coef_ap(c)), om);
+    const float sum = fmaf(at, P[sxy], fmaf(ab, P[-sxy], fmaf(an, P[sx], fmaf(as, P[-sx], fmaf(ae, P[1], aw * P[-1])))));
+    phi[dst[e]] = sorf(P[0], (rhs[gi] - sum) * (1.f / -(aw + ae + as + an + ab + at)), om);
   }
 }
 
-cudaError_t launch_red_ahead(bool var, const uint32_t* dst, const uint32_t* src, const int* blk, int64_t n,
+cudaError_t launch_red_ahead(bool var, const uint32_t* dst, const uint32_t* src, const int* info, int64_t n, int nb,
                              const BlkLev* bl, float* phi, const float* rhs, const float* fx, const float* fy,
                              const float* fz, float om, cudaStream_t st) {
   if (n <= 0) return cudaSuccess;
   const int g = grid_for(n, 256);
-  if (var) pdl_launch(k_red_ahead<true>, g, 256, 0, st, dst, src, blk, n, bl, phi, rhs, fx, fy, fz, om);
-  else pdl_launch(k_red_ahead<false>, g, 256, 0, st, dst, src, blk, n, bl, phi, rhs, fx, fy, fz, om);
+  if (var) pdl_launch(k_red_ahead<true>, g, 256, 0, st, dst, src, info, n, nb, bl, phi, rhs, fx, fy, fz, om);
+  else pdl_launch(k_red_ahead<false>, g, 256, 0, st, dst, src, info, n, nb, bl, phi, rhs, fx, fy, fz, om);
   return cudaGetLastError();
 }
 

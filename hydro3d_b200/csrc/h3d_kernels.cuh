@@ -178,7 +178,7 @@ cudaError_t launch_fill(const uint32_t* dsts, const uint32_t* srcs, int64_t n, T
 
 // Red updates of the red cells next to block faces, stored at the ghost cells
 // that show them to other blocks (FP32, before a sweep; see k_red_ahead).
-cudaError_t launch_red_ahead(bool var, const uint32_t* dst, const uint32_t* src, const int* blk, int64_t n,
+cudaError_t launch_red_ahead(bool var, const uint32_t* dst, const uint32_t* src, const int* info, int64_t n, int nb,
                              const BlkLev* bl, float* phi, const float* rhs, const float* fx, const float* fy,
                              const float* fz, float om, cudaStream_t st);
 

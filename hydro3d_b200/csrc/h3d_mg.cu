@@ -82,7 +82,7 @@ struct Level {
   Halo live, live_push;         // the parts of sweep / sweep_push that the next sweep or restriction reads
   bool live_ok = false;         // live fills may stand in for the full fill (FP32 RBGS levels)
   Halo red;                     // red cells next to block faces and the ghosts that show them (k_red_ahead)
-  int* d_red_blk = nullptr;     // their blocks
+  int* d_red_info = nullptr;    // their blocks and wall faces (k_red_ahead)
   bool red_ok = false;          // FP32 sweeps of this level take the red-black order across block faces
   long long* d_push = nullptr;  // per block, six ghost push offsets (kNoPush: none)
   bool push_ok = false;
@@ -575,8 +575,8 @@ struct Exec {
     const bool from_zero = mixed_level(g) ? V.zero32 : V.zero64;
     if (h->desc.mg_itrsch == 3 && mixed_level(g) && V.red_ok && !V.zero32) {
       // the red cells next to block faces first: red-black order across blocks
-      CU(launch_red_ahead(h->var, V.red.d_dst, V.red.d_src, V.d_red_blk, V.red.n, V.d_bl, V.phi32[V.cur32], V.rhs32,
-                          V.fx32, V.fy32, V.fz32, h->omega, st));
+      CU(launch_red_ahead(h->var, V.red.d_dst, V.red.d_src, V.d_red_info, V.red.n, (int)V.geom.bl.size(), V.d_bl,
+                          V.phi32[V.cur32], V.rhs32, V.fx32, V.fy32, V.fz32, h->omega, st));
       TRY(chk("red ahead", g));
       h->kernels += 1;
     }
@@ -1610,17 +1610,19 @@ int build_red_ahead(h3d_mg* h, Level& V, const std::vector<uint32_t>& ld, const 
       const long long l = gi - B.off;
       const int z = (int)(l / B.sxy), y = (int)((l % B.sxy) / B.sx), x = (int)(l % B.sx);
       if ((x + y + z) & 1) {  // red
+        const int m = B.phys & ((x == 1 ? 1 : 0) | (x == B.nx ? 2 : 0) | (y == 1 ? 4 : 0) | (y == B.ny ? 8 : 0) |
+                                (z == 1 ? 16 : 0) | (z == B.nz ? 32 : 0));
         rd.push_back(ld[e]);
         rs.push_back(ls[e]);
-        rb.push_back(q);
+        rb.push_back(q | (m << 16));
       }
       break;
     }
   }
-  if (rd.empty()) return H3D_OK;
+  if (rd.empty() || G.bl.size() > 0xffff) return H3D_OK;
   TRY(upload_halo(h, V.red, rd, rs));
-  TRY(dalloc(h, &V.d_red_blk, rb.size()));
-  CU(cudaMemcpy(V.d_red_blk, rb.data(), rb.size() * sizeof(int), cudaMemcpyHostToDevice));
+  TRY(dalloc(h, &V.d_red_info, rb.size()));
+  CU(cudaMemcpy(V.d_red_info, rb.data(), rb.size() * sizeof(int), cudaMemcpyHostToDevice));
   V.red_ok = true;
   return H3D_OK;
 }
@@ -2352,7 +2354,7 @@ int h3d_mg_destroy(h3d_mg* h) {
     void* ps[] = {V.d_bl, V.d_cta_all, V.d_cta_int, V.d_rows_all, V.d_rows_int, V.d_tiles, V.phi64[0], V.phi64[1], V.rhs64, V.phi32[0],
                   V.phi32[1], V.rhs32, V.fx64, V.fy64, V.fz64, V.fx32, V.fy32, V.fz32, V.dens,
                   V.sweep.d_dst, V.sweep.d_src, V.faces.d_dst, V.faces.d_src, V.exch.d_dst, V.exch.d_src,
-                  V.bound.d_dst, V.bound.d_src, V.sweep_push.d_dst, V.sweep_push.d_src, V.live.d_dst, V.live.d_src, V.live_push.d_dst, V.live_push.d_src, V.red.d_dst, V.red.d_src, V.d_red_blk, V.d_push, V.d_maps, V.d_rmaps, V.d_rtiles, V.d_ptiles, V.d_qtiles, V.d_dtiles, V.d_cstart, V.d_dstart, V.d_pstart, V.seq64, V.seq32, V.d_ztiles, V.lfill.d_dst, V.lfill.d_src, V.d_lfstart,
+                  V.bound.d_dst, V.bound.d_src, V.sweep_push.d_dst, V.sweep_push.d_src, V.live.d_dst, V.live.d_src, V.live_push.d_dst, V.live_push.d_src, V.red.d_dst, V.red.d_src, V.d_red_info, V.d_push, V.d_maps, V.d_rmaps, V.d_rtiles, V.d_ptiles, V.d_qtiles, V.d_dtiles, V.d_cstart, V.d_dstart, V.d_pstart, V.seq64, V.seq32, V.d_ztiles, V.lfill.d_dst, V.lfill.d_src, V.d_lfstart,
                   V.xs.d_nodes, V.xs.d_dst, V.xs.d_src, V.xe.d_nodes, V.xe.d_dst, V.xe.d_src, V.xscratch, V.d_rsame,
                   V.d_psame, V.d_prows};
     for (void* p : ps) dfree(p);
