@@ -605,22 +605,20 @@ def main():
 
 def read_profile_traffic(cfg, variant):
     """DRAM bytes (read + write) per level-1 smoother launch from the committed
-    ncu summary of this workload, when that capture is of the variant the
-    autotuner chose in this run; None otherwise."""
+    ncu summary of this workload (lines `traffic_bytes_per_launch[variant] =
+    bytes`), when it holds a capture of the variant the autotuner chose in this
+    run; None otherwise."""
     p = os.path.join(ROOT, "profiles", "k_rbgs_win_fp32_config3.md")
     if cfg != 3 or not os.path.exists(p):
         return None
-    vals = {}
+    key = "traffic_bytes_per_launch[%d]" % variant
     for ln in open(p):
-        if "=" in ln and ln.split("=")[0].strip() in ("traffic_bytes_per_launch", "smoother_variant"):
-            k, v = ln.split("=", 1)
-            vals[k.strip()] = v.strip()
-    try:
-        if int(vals.get("smoother_variant", -1)) != variant:
-            return None
-        return float(vals["traffic_bytes_per_launch"])
-    except (KeyError, ValueError):
-        return None
+        if "=" in ln and ln.split("=")[0].strip() == key:
+            try:
+                return float(ln.split("=", 1)[1].strip())
+            except ValueError:
+                return None
+    return None
 
 
 def prob_config(prob):
