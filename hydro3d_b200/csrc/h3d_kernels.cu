@@ -1835,26 +1835,30 @@ static cudaError_t tma2_dispatch(bool var, const BlkLev* bl, const Tile* tiles, 
   X(27, 32, 2, 8, 2)       \
   X(28, 8, 1, 16, 2)
 
-// One cell of the seven-point update: (rhs - off-diagonal sum) x diagonal reciprocal.
+// One cell of the seven-point update, over-relaxed: (rhs - off-diagonal sum) x
+// (omega x diagonal reciprocal) + (1 - omega) x old value, one FMA (omega = 1:
+// the Gauss-Seidel value exactly).
 __device__ __forceinline__ float win_upd(float w, float e, float s, float n, float b, float t, float rv, float aw,
-                                         float ae, float as, float an, float ab, float at, float iv) {
+                                         float ae, float as, float an, float ab, float at, float iv, float old,
+                                         float omc) {
   const float sum = fmaf(at, t, fmaf(ab, b, fmaf(an, n, fmaf(as, s, fmaf(ae, e, aw * w)))));
-  return (rv - sum) * iv;
+  return fmaf(rv - sum, iv, omc * old);
 }
 
 // The two cells of one colour of a group of four (positions 0, 2 when q1 is
 // false, else 1, 3).  aw0 / iv0 belong to the first cell of the group, ae3 /
-// iv3 to the last, iv12 to the middle two.
+// iv3 to the last, iv12 to the middle two; the reciprocals carry omega,
+// omc = 1 - omega.
 __device__ __forceinline__ void win_colour(float4& c, const float4& bz, const float4& tz, const float4& u,
                                            const float4& dn, const float4& rh, float l, float r, bool q1, float aw0,
                                            float ae3, float ax, float as, float an, float ab, float at, float iv0,
-                                           float iv12, float iv3, float om) {
+                                           float iv12, float iv3, float omc) {
   if (!q1) {
-    c.x = sorf(c.x, win_upd(l, c.y, u.x, dn.x, bz.x, tz.x, rh.x, aw0, ax, as, an, ab, at, iv0), om);
-    c.z = sorf(c.z, win_upd(c.y, c.w, u.z, dn.z, bz.z, tz.z, rh.z, ax, ax, as, an, ab, at, iv12), om);
+    c.x = win_upd(l, c.y, u.x, dn.x, bz.x, tz.x, rh.x, aw0, ax, as, an, ab, at, iv0, c.x, omc);
+    c.z = win_upd(c.y, c.w, u.z, dn.z, bz.z, tz.z, rh.z, ax, ax, as, an, ab, at, iv12, c.z, omc);
   } else {
-    c.y = sorf(c.y, win_upd(c.x, c.z, u.y, dn.y, bz.y, tz.y, rh.y, ax, ax, as, an, ab, at, iv12), om);
-    c.w = sorf(c.w, win_upd(c.z, r, u.w, dn.w, bz.w, tz.w, rh.w, ax, ae3, as, an, ab, at, iv3), om);
+    c.y = win_upd(c.x, c.z, u.y, dn.y, bz.y, tz.y, rh.y, ax, ax, as, an, ab, at, iv12, c.y, omc);
+    c.w = win_upd(c.z, r, u.w, dn.w, bz.w, tz.w, rh.w, ax, ae3, as, an, ab, at, iv3, c.w, omc);
   }
 }
 
@@ -1950,10 +1954,11 @@ __global__ void __launch_bounds__(TPR*(TY + 2)) k_rbgs_win(const BlkLev* __restr
     aw0[k] = (lft[k] && (ph & 1)) ? 0.f : ax;
     ae3[k] = (rgt[k] && (ph & 2)) ? 0.f : ax;
   }
-  // diagonal reciprocals of the three kinds of cells of a group on interior
-  // planes, the bottom wall plane (b), the top wall plane (t) and a plane that
-  // is both (bt, nz = 1): no division inside the z march
-  auto rcp = [&](float aw, float ae, float ab, float at) { return 1.f / (-(aw + ae + as + an + ab + at)); };
+  // diagonal reciprocals (times omega) of the three kinds of cells of a group
+  // on interior planes, the bottom wall plane (b), the top wall plane (t) and a
+  // plane that is both (bt, nz = 1): no division inside the z march
+  const float omc = 1.f - om;
+  auto rcp = [&](float aw, float ae, float ab, float at) { return om * (1.f / (-(aw + ae + as + an + ab + at))); };
   float i0[GPT], i0b[GPT], i0t[GPT], i0bt[GPT], i3[GPT], i3b[GPT], i3t[GPT], i3bt[GPT];
 #pragma unroll
   for (int k = 0; k < GPT; ++k) {
@@ -2017,12 +2022,12 @@ __global__ void __launch_bounds__(TPR*(TY + 2)) k_rbgs_win(const BlkLev* __restr
   do {                                                                                                           \
     const bool wlo_ = (zz) == 1 && (ph & 16), whi_ = (zz) == nz && (ph & 32);                                    \
     if (!(wlo_ || whi_)) {                                                                                       \
-      win_colour(c, bz, tz, u, dn, rh, l, r, q1, aw0[k], ae3[k], ax, as, an, az, az, i0[k], i12, i3[k], om);      \
+      win_colour(c, bz, tz, u, dn, rh, l, r, q1, aw0[k], ae3[k], ax, as, an, az, az, i0[k], i12, i3[k], omc);     \
     } else {                                                                                                     \
       win_colour(c, bz, tz, u, dn, rh, l, r, q1, aw0[k], ae3[k], ax, as, an, wlo_ ? 0.f : az, whi_ ? 0.f : az,   \
                  wlo_ ? (whi_ ? i0bt[k] : i0b[k]) : (whi_ ? i0t[k] : i0[k]),                                     \
                  wlo_ ? (whi_ ? i12bt : i12b) : (whi_ ? i12t : i12),                                             \
-                 wlo_ ? (whi_ ? i3bt[k] : i3b[k]) : (whi_ ? i3t[k] : i3[k]), om);                                \
+                 wlo_ ? (whi_ ? i3bt[k] : i3b[k]) : (whi_ ? i3t[k] : i3[k]), omc);                               \
     }                                                                                                            \
   } while (0)
   auto ld4 = [](const float* p) { return *reinterpret_cast<const float4*>(p); };
