@@ -1558,23 +1558,28 @@ int h3d_topology(int32_t nblocks, const int32_t* ext, const int32_t* bc, const d
 // fill.  Returns false (no live tables) unless every source is a current
 // interior cell, so that one full fill after any number of live ones leaves
 // the same ghost shell as full fills throughout.
+// Block and (x, y, z) of element gi of a level (blocks in increasing offset).
+bool locate_cell(const LevelGeom& G, long long gi, int* b, int* x, int* y, int* z) {
+  int lo = 0, hi = (int)G.bl.size() - 1, q = -1;
+  while (lo <= hi) {  // last block whose offset is at most gi
+    const int mid = (lo + hi) / 2;
+    if (G.bl[mid].off <= gi) { q = mid; lo = mid + 1; }
+    else hi = mid - 1;
+  }
+  if (q < 0) return false;
+  const BlkLev& B = G.bl[q];
+  const long long l = gi - B.off;
+  if (l >= B.sxy * (B.nz + 2)) return false;
+  *z = (int)(l / B.sxy);
+  *y = (int)((l % B.sxy) / B.sx);
+  *x = (int)(l % B.sx);
+  *b = q;
+  return *x <= B.nx + 1;
+}
+
 bool live_entries(const LevelGeom& G, const std::vector<uint32_t>& d, const std::vector<uint32_t>& s,
                   std::vector<uint32_t>* ld, std::vector<uint32_t>* ls) {
-  const int nb = (int)G.bl.size();
-  auto locate = [&](uint32_t gi, int* b, int* x, int* y, int* z) -> bool {
-    for (int q = 0; q < nb; ++q) {
-      const BlkLev& B = G.bl[q];
-      const long long lo = B.off, hi = B.off + B.sxy * (B.nz + 2);
-      if ((long long)gi < lo || (long long)gi >= hi) continue;
-      const long long l = (long long)gi - lo;
-      *z = (int)(l / B.sxy);
-      *y = (int)((l % B.sxy) / B.sx);
-      *x = (int)(l % B.sx);
-      *b = q;
-      return *x <= B.nx + 1;
-    }
-    return false;
-  };
+  auto locate = [&](uint32_t gi, int* b, int* x, int* y, int* z) { return locate_cell(G, gi, b, x, y, z); };
   ld->clear();
   ls->clear();
   for (size_t e = 0; e < d.size(); ++e) {
@@ -1603,20 +1608,15 @@ int build_red_ahead(h3d_mg* h, Level& V, const std::vector<uint32_t>& ld, const 
   std::vector<uint32_t> rd, rs;
   std::vector<int> rb;
   for (size_t e = 0; e < ld.size(); ++e) {
-    const long long gi = ls[e] & kIdxMask;
-    for (int q = 0; q < (int)G.bl.size(); ++q) {
-      const BlkLev& B = G.bl[q];
-      if (gi < B.off || gi >= B.off + B.sxy * (B.nz + 2)) continue;
-      const long long l = gi - B.off;
-      const int z = (int)(l / B.sxy), y = (int)((l % B.sxy) / B.sx), x = (int)(l % B.sx);
-      if ((x + y + z) & 1) {  // red
-        const int m = B.phys & ((x == 1 ? 1 : 0) | (x == B.nx ? 2 : 0) | (y == 1 ? 4 : 0) | (y == B.ny ? 8 : 0) |
-                                (z == 1 ? 16 : 0) | (z == B.nz ? 32 : 0));
-        rd.push_back(ld[e]);
-        rs.push_back(ls[e]);
-        rb.push_back(q | (m << 16));
-      }
-      break;
+    int q, x, y, z;
+    if (!locate_cell(G, ls[e] & kIdxMask, &q, &x, &y, &z)) return H3D_OK;  // (sources are interior cells)
+    const BlkLev& B = G.bl[q];
+    if ((x + y + z) & 1) {  // red
+      const int m = B.phys & ((x == 1 ? 1 : 0) | (x == B.nx ? 2 : 0) | (y == 1 ? 4 : 0) | (y == B.ny ? 8 : 0) |
+                              (z == 1 ? 16 : 0) | (z == B.nz ? 32 : 0));
+      rd.push_back(ld[e]);
+      rs.push_back(ls[e]);
+      rb.push_back(q | (m << 16));
     }
   }
   if (rd.empty() || G.bl.size() > 0xffff) return H3D_OK;
