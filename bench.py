@@ -44,8 +44,9 @@ TOL = 1e-8
 # Gauss-Seidel per block 8.3 ms, 12 cycles, 1.4e-9 (omega 1.25 per block or
 # across blocks alone: 12 cycles; omega 1.3: 9 cycles; V(1,1) x 3: 9 cycles,
 # 6.0 ms); configuration 2: V(2,1) x 3, omega 1.25 across blocks 2.0 ms against
-# V(2,1) x 5 2.8 ms; 5 (1000:1 density): V(2,1) x 4, omega 1.5 across blocks
-# 17.9 ms, 16 cycles, error 2.1e-8, against V(2,1) x 8 Gauss-Seidel 33.4 ms,
+# V(2,1) x 5 2.8 ms; 5 (1000:1 density, one block: no order across blocks to
+# take): V(2,1) x 4, omega 1.5 17.9 ms, 16 cycles, error 2.1e-8, against
+# V(2,1) x 8 Gauss-Seidel 33.4 ms,
 # 2.8e-7 (omega 1.35-1.6 also 16 cycles, 1.25 24 cycles, 1.7 20 cycles;
 # V(2,2) x 3 with omega 1.6 16.8 ms but error 1.1e-7).  One block (1): omega 1.25 takes
 # 6 cycles, not 8, but its error grows from 3.7e-8 to 9.5e-7; independent
@@ -53,7 +54,7 @@ TOL = 1e-8
 # per-block order): no fewer cycles.  6: V(2,2) x 6 12.3 ms against V(2,1) x 4
 # 20.6 ms; 4: V(1,2) x 6 12.2 against V(2,1) x 2 13.2 ms.
 MIXED_CYCLE = {1: (2, 1, 4), 2: (2, 1, 3), 3: (2, 1, 3), 4: (1, 2, 6), 5: (2, 1, 4), 6: (2, 2, 6)}
-MIXED_SMOOTHER = {1: (1.0, 0), 2: (1.25, 1), 3: (1.25, 1), 4: (1.0, 0), 5: (1.5, 1), 6: (1.0, 0)}
+MIXED_SMOOTHER = {1: (1.0, 0), 2: (1.25, 1), 3: (1.25, 1), 4: (1.0, 0), 5: (1.5, 0), 6: (1.0, 0)}
 # Sweeps of the FP64 coarsest level in the mixed solver: enough to converge
 # that level (on the configuration-3 hierarchy 16 leave 14 V-cycles, 32 and 64
 # both 12), so the V-cycle contracts every mode at the rate of its finer
