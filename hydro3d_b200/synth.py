@@ -153,7 +153,7 @@ def spectral_velocity(rng, shape, box, kmin=1.0, kmax=64.0):
     amp = np.where((kk >= kmin) & (kk <= kmax), np.power(np.maximum(kk, 1e-30), -5.0 / 3.0), 0.0)
     phase = rng.uniform(0.0, 2 * np.pi, amp.shape)
     spec = amp * np.exp(1j * phase)
-    f = np.fft.irfftn(spec, s=shape)
+    f = np.fft.irfftn(spec, s=shape, axes=(0, 1, 2))
     f /= np.sqrt(np.mean(f * f))
     return f
 

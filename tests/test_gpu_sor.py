@@ -4,7 +4,8 @@ red-black order across block faces (rb_order = 1).
   * Two FP32 sweeps of every smoother variant with omega = 1.25 and
     rb_order = 1 are red-black SOR in one colour order over the union of the
     blocks (numpy in FP64: red cells of every block, then black cells of every
-    block, each cell x + omega (gs - x)), within the FP32 tolerance.
+    block, each cell x + omega (gs - x)), within the FP32 tolerance, with walls
+    and with periodic partners (across blocks, and a block its own partner).
   * With those options the configuration-3 layout (4 x 2 x 2 blocks, here of
     32^3) meets 1e-8 in fewer V-cycles than with the reference's per-block
     order and Gauss-Seidel, and its solution is as close to the converged FP64
@@ -19,30 +20,33 @@ from tests.helpers import interior_of_host, mean_removed_rel
 
 pytestmark = pytest.mark.gpu
 
-W = 4
+W, P = 4, 5  # wall, periodic
 FP32_RTOL = 2e-5
 H = 1.0 / 32
 
 
-def _global_rb_sor(u, f, om, sweeps):
-    """Red-black SOR of the cell-centred 7-point operator (walls: zero face
-    coefficient) over a whole (z, y, x) domain, red = x+y+z odd (1-based)."""
+def _global_rb_sor(u, f, om, sweeps, periodic=(False, False, False)):
+    """Red-black SOR of the cell-centred 7-point operator over a whole (z, y, x)
+    domain, red = x+y+z odd (1-based): walls have a zero face coefficient, a
+    periodic axis (x, y, z order) wraps around."""
     a = 1.0 / (H * H)
     shape = u.shape
-    cw = np.full(shape, a); cw[:, :, 0] = 0
-    ce = np.full(shape, a); ce[:, :, -1] = 0
-    cs = np.full(shape, a); cs[:, 0, :] = 0
-    cn = np.full(shape, a); cn[:, -1, :] = 0
-    cb = np.full(shape, a); cb[0] = 0
-    ct = np.full(shape, a); ct[-1] = 0
+    cw = np.full(shape, a); ce = np.full(shape, a)
+    cs = np.full(shape, a); cn = np.full(shape, a)
+    cb = np.full(shape, a); ct = np.full(shape, a)
+    if not periodic[0]:
+        cw[:, :, 0] = 0; ce[:, :, -1] = 0
+    if not periodic[1]:
+        cs[:, 0, :] = 0; cn[:, -1, :] = 0
+    if not periodic[2]:
+        cb[0] = 0; ct[-1] = 0
     ap = -(cw + ce + cs + cn + cb + ct)
     z, y, x = np.indices(shape) + 1
     red = (x + y + z) % 2 == 1
     for _ in range(sweeps):
         for colour in (red, ~red):
-            g = np.pad(u, 1)
-            s = (cw * g[1:-1, 1:-1, :-2] + ce * g[1:-1, 1:-1, 2:] + cs * g[1:-1, :-2, 1:-1] +
-                 cn * g[1:-1, 2:, 1:-1] + cb * g[:-2, 1:-1, 1:-1] + ct * g[2:, 1:-1, 1:-1])
+            s = (cw * np.roll(u, 1, 2) + ce * np.roll(u, -1, 2) + cs * np.roll(u, 1, 1) +
+                 cn * np.roll(u, -1, 1) + cb * np.roll(u, 1, 0) + ct * np.roll(u, -1, 0))
             u = np.where(colour, u + om * ((f - s) / ap - u), u)
     return u
 
@@ -55,8 +59,11 @@ def _part(a, d):
 
 def test_sweeps_are_global_red_black_sor(h3d):
     rng = np.random.default_rng(5)
-    for nblk, n in (((2, 2, 1), (32, 16, 16)), ((2, 1, 2), (64, 12, 8))):
-        blocks = h3d.topology.block_grid(nblk, n, [W] * 6, [H] * 3, 2)
+    for nblk, n, bc in (((2, 2, 1), (32, 16, 16), [W] * 6), ((2, 1, 2), (64, 12, 8), [W] * 6),
+                        ((2, 1, 1), (32, 16, 8), [P, P, W, W, W, W]),      # periodic partners across blocks
+                        ((1, 2, 1), (16, 16, 8), [W, W, P, P, P, P])):     # a block its own partner in z
+        periodic = (bc[0] == P, bc[2] == P, bc[4] == P)
+        blocks = h3d.topology.block_grid(nblk, n, bc, [H] * 3, 2)
         s = h3d.MultigridSolver(blocks, 2, precision="mixed", use_graph=False, omega=1.25, rb_order=1)
         s.coeff()
         shape = (nblk[2] * n[2], nblk[1] * n[1], nblk[0] * n[0])
@@ -69,14 +76,16 @@ def test_sweeps_are_global_red_black_sor(h3d):
                 tried += 1
                 u = rng.standard_normal(shape)
                 f = rng.standard_normal(shape)
+                # every block with its ghost layer cut from the wrapped union: ghosts
+                # across block faces and periodic faces hold the cells they show
+                # (wall ghosts have a zero coefficient)
+                uw = np.pad(u, 1, mode="wrap")
                 for ib, d in enumerate(blocks):
-                    p = np.zeros((d.n[2] + 2, d.n[1] + 2, d.n[0] + 2))
-                    p[1:-1, 1:-1, 1:-1] = _part(u, d)
-                    s.put_level(1, "phi", ib, p)
+                    ox, oy, oz = d.origin
+                    s.put_level(1, "phi", ib, uw[oz:oz + d.n[2] + 2, oy:oy + d.n[1] + 2, ox:ox + d.n[0] + 2])
                     s.put_level(1, "rhs", ib, _part(f, d))
-                s.exchangepp(1)  # ghosts across block faces hold the neighbours' cells
                 s.mgrelax(1, 2)
-                ref = _global_rb_sor(u, f, 1.25, 2)
+                ref = _global_rb_sor(u, f, 1.25, 2, periodic)
                 scale = np.abs(ref).max()
                 for ib, d in enumerate(blocks):
                     got = s.get_level(1, "phi", ib)[1:-1, 1:-1, 1:-1]
