@@ -2346,7 +2346,7 @@ template <typename T, bool VAR>
 __device__ void small_relax(const BlkLev* sb, const int* ss, int nb, T* __restrict__ phi, const T* __restrict__ rhs,
                             const T* __restrict__ fx, const T* __restrict__ fy, const T* __restrict__ fz,
                             const uint32_t* __restrict__ fdst, const uint32_t* __restrict__ fsrc, int nfill,
-                            int sweeps, int zero, long long nelems, float om) {
+                            int sweeps, int zero, long long nelems, float om, int rb) {
   const int ncell = ss[nb];
   if (zero) {
     for (long long q = threadIdx.x; q < nelems; q += blockDim.x) phi[q] = T(0);
@@ -2372,6 +2372,10 @@ __device__ void small_relax(const BlkLev* sb, const int* ss, int nb, T* __restri
         phi[i] = v;
       }
       __syncthreads();
+      if (rb && colour == 1) {  // red-black order across block faces: the new red cells into the ghosts
+        for (int q = threadIdx.x; q < nfill; q += blockDim.x) phi[fdst[q]] = phi[fsrc[q] & kIdxMask];
+        __syncthreads();
+      }
     }
     for (int q = threadIdx.x; q < nfill; q += blockDim.x) phi[fdst[q]] = phi[fsrc[q] & kIdxMask];
     __syncthreads();
@@ -2427,7 +2431,7 @@ __global__ void __launch_bounds__(1024) k_relax_small(const BlkLev* __restrict__
                                                       const T* __restrict__ fx, const T* __restrict__ fy,
                                                       const T* __restrict__ fz, const uint32_t* __restrict__ fdst,
                                                       const uint32_t* __restrict__ fsrc, int nfill, int sweeps,
-                                                      int zero, long long nelems, float om) {
+                                                      int zero, long long nelems, float om, int rb) {
   pdl_trigger();
   __shared__ BlkLev sb[kSmallLevelBlocks];
   __shared__ int ss[kSmallLevelBlocks + 1];
@@ -2437,7 +2441,7 @@ __global__ void __launch_bounds__(1024) k_relax_small(const BlkLev* __restrict__
   for (int b = threadIdx.x; b <= nb; b += blockDim.x) ss[b] = start[b];
   pdl_wait();
   __syncthreads();
-  small_relax<T, VAR>(sb, ss, nb, phi, rhs, fx, fy, fz, fdst, fsrc, nfill, sweeps, zero, nelems, om);
+  small_relax<T, VAR>(sb, ss, nb, phi, rhs, fx, fy, fz, fdst, fsrc, nfill, sweeps, zero, nelems, om, rb);
 }
 
 // The fused coarse tail keeps every tail level in shared memory, in a
@@ -2945,13 +2949,14 @@ cudaError_t launch_coarse_tail(const TailLevel* lv, const TailOp* ops, int nops,
 template <typename T>
 cudaError_t launch_relax_small(bool var, const BlkLev* bl, const int* start, int nb, T* phi, const T* rhs,
                                const T* fx, const T* fy, const T* fz, const uint32_t* fdst, const uint32_t* fsrc,
-                               int nfill, int sweeps, bool zero, long long nelems, float om, cudaStream_t st) {
+                               int nfill, int sweeps, bool zero, long long nelems, float om, bool rb,
+                               cudaStream_t st) {
   if (var)
     pdl_launch(k_relax_small<T, true>, 1, 1024, 0, st, bl, start, nb, phi, rhs, fx, fy, fz, fdst, fsrc, nfill, sweeps,
-               (int)zero, nelems, om);
+               (int)zero, nelems, om, (int)rb);
   else
     pdl_launch(k_relax_small<T, false>, 1, 1024, 0, st, bl, start, nb, phi, rhs, fx, fy, fz, fdst, fsrc, nfill,
-               sweeps, (int)zero, nelems, om);
+               sweeps, (int)zero, nelems, om, (int)rb);
   return cudaGetLastError();
 }
 template <typename T>
@@ -2975,10 +2980,10 @@ template cudaError_t launch_relax_blocks<float>(bool, const BlkLev*, int, const 
                                                 const uint32_t*, int, bool, float, cudaStream_t);
 template cudaError_t launch_relax_small<double>(bool, const BlkLev*, const int*, int, double*, const double*,
                                                 const double*, const double*, const double*, const uint32_t*,
-                                                const uint32_t*, int, int, bool, long long, float, cudaStream_t);
+                                                const uint32_t*, int, int, bool, long long, float, bool, cudaStream_t);
 template cudaError_t launch_relax_small<float>(bool, const BlkLev*, const int*, int, float*, const float*,
                                                const float*, const float*, const float*, const uint32_t*,
-                                               const uint32_t*, int, int, bool, long long, float, cudaStream_t);
+                                               const uint32_t*, int, int, bool, long long, float, bool, cudaStream_t);
 
 template <typename T>
 cudaError_t launch_fill(const uint32_t* dsts, const uint32_t* srcs, int64_t n, T* out, const T* cur, const T* old,

@@ -169,7 +169,8 @@ cudaError_t launch_seq_smoother(int itrsch, bool var, bool zero, const BlkLev* b
 template <typename T>
 cudaError_t launch_relax_small(bool var, const BlkLev* bl, const int* start, int nb, T* phi, const T* rhs,
                                const T* fx, const T* fy, const T* fz, const uint32_t* fdst, const uint32_t* fsrc,
-                               int nfill, int sweeps, bool zero, long long nelems, float om, cudaStream_t st);
+                               int nfill, int sweeps, bool zero, long long nelems, float om, bool rb,
+                               cudaStream_t st);
 
 // Ghost gather: out[dst[e]] = (src[e] & old) ? old[src] : cur[src].
 template <typename T>

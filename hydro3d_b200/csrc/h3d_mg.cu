@@ -670,12 +670,12 @@ struct Exec {
       if (mixed_level(g)) {
         CU(launch_relax_small<float>(h->var, V.d_bl, V.d_cstart, nb, V.phi32[V.cur32], V.rhs32, V.fx32, V.fy32,
                                      V.fz32, V.sweep.d_dst, V.sweep.d_src, (int)V.sweep.n, it, V.zero32,
-                                     V.geom.n_elems, h->omega, h->st));
+                                     V.geom.n_elems, h->omega, h->rb_global, h->st));
         V.zero32 = false;
       } else {
         CU(launch_relax_small<double>(h->var, V.d_bl, V.d_cstart, nb, V.phi64[V.cur64], V.rhs64, V.fx64, V.fy64,
                                       V.fz64, V.sweep.d_dst, V.sweep.d_src, (int)V.sweep.n, it, V.zero64,
-                                      V.geom.n_elems, 1.f, h->st));
+                                      V.geom.n_elems, 1.f, false, h->st));
         V.zero64 = false;
       }
       TRY(chk("relax small", g));
